@@ -1,0 +1,288 @@
+"""galfast_b200 -- B200-native galfast catalog hot path (skygen + photometry +
+kinematics + proper motions) behind a C ABI (include/galfast_b200.h).
+
+The Python layer mirrors the reference's module interface for tests and
+benchmarks: a Skygen object plays the part of the skygen source module
+(integrateCounts / drawSources, src/skygen/skygen.h:47-60) and the module
+functions the osink::process of each postprocessing module.  All compute runs
+in the sm_100a library; there is no CPU fallback: importing this package on a
+machine without the built library raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi as A
+from ._abi import (PencilBeam, Lambert, SkygenConfig, ModelConfig, Extinction, Footprint, Table,
+                   FixedFeHConfig, Bond2010Config, PhotometryConfig, PhotoerrConfig, Vel2pmConfig, ModelInfo)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "_lib", "libgalfast_b200.so")
+
+
+class GalfastError(RuntimeError):
+    pass
+
+
+class Job(C.Structure):
+    _fields_ = [("sky", SkygenConfig), ("pixels", C.POINTER(PencilBeam)), ("npixels", C.c_int32),
+                ("beam_ammin", C.POINTER(C.c_float)), ("ext", Extinction),
+                ("models", C.POINTER(ModelConfig)), ("nmodels", C.c_int32),
+                ("seed48", C.c_uint32), ("nstreams", C.c_int32), ("capacity", C.c_int64), ("nbands", C.c_int32),
+                ("foot", C.POINTER(Footprint)), ("feh", C.POINTER(FixedFeHConfig)),
+                ("kin", C.POINTER(Bond2010Config)), ("phot", C.POINTER(PhotometryConfig)),
+                ("perr", C.POINTER(PhotoerrConfig)), ("v2pm", C.POINTER(Vel2pmConfig)), ("gal2other", C.c_int32)]
+
+
+class CatalogStats(C.Structure):
+    _fields_ = [("expected", C.c_double * 32), ("expected_covered", C.c_double * 32),
+                ("generated", C.c_int64 * 32), ("stored", C.c_int64 * 32), ("batches", C.c_int32),
+                ("norm", C.c_float)]
+
+
+BatchCallback = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.POINTER(Table), C.c_int64)
+
+_lib = None
+
+
+def lib():
+    """The native library; raises GalfastError if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise GalfastError("libgalfast_b200.so is not built: run `python -m galfast_b200.build`")
+        L = C.CDLL(LIBPATH)
+        vp = C.c_void_p
+        L.gf_last_error.restype = C.c_char_p
+        L.gf_ctx_create.argtypes = [C.c_int, C.POINTER(vp)]
+        L.gf_ctx_destroy.argtypes = [vp]
+        L.gf_ctx_sync.argtypes = [vp]
+        L.gf_rng_init.argtypes = [vp, C.c_uint32, C.c_int32]
+        L.gf_rng_seed48_from_cli_seed.argtypes = [C.c_uint64]
+        L.gf_rng_seed48_from_cli_seed.restype = C.c_uint32
+        L.gf_rng_get_state.argtypes = [vp, vp, C.c_int32]
+        L.gf_rng_set_state.argtypes = [vp, vp, C.c_int32]
+        L.gf_skygen_create.argtypes = [vp, C.POINTER(SkygenConfig), C.POINTER(PencilBeam), C.c_int32,
+                                       C.POINTER(C.c_float), C.POINTER(Extinction), C.POINTER(ModelConfig),
+                                       C.c_int32, C.POINTER(vp)]
+        L.gf_skygen_destroy.argtypes = [vp]
+        L.gf_skygen_model_info_get.argtypes = [vp, C.c_int32, C.POINTER(ModelInfo)]
+        L.gf_skygen_model_lf_get.argtypes = [vp, C.c_int32, C.POINTER(C.c_float)]
+        L.gf_skygen_integrate.argtypes = [vp, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double)]
+        L.gf_skygen_set_norm.argtypes = [vp, C.c_int32, C.c_float]
+        L.gf_skygen_draw.argtypes = [vp, C.c_int32, C.POINTER(Table), C.POINTER(C.c_int64), C.POINTER(C.c_int32)]
+        L.gf_table_alloc.argtypes = [vp, C.c_int64, C.c_int32, C.POINTER(Table)]
+        L.gf_table_free.argtypes = [vp, C.POINTER(Table)]
+        L.gf_table_download.argtypes = [vp, C.POINTER(Table), C.POINTER(Table)]
+        L.gf_module_clipper.argtypes = [vp, C.POINTER(Footprint), C.POINTER(Lambert), C.POINTER(Table), C.c_int64, C.c_int64]
+        L.gf_module_fixedfeh.argtypes = [vp, C.POINTER(FixedFeHConfig), C.POINTER(Table), C.c_int64, C.c_int64]
+        L.gf_module_bond2010.argtypes = [vp, C.POINTER(Bond2010Config), C.POINTER(Table), C.c_int64, C.c_int64]
+        L.gf_photometry_create.argtypes = [vp, C.POINTER(PhotometryConfig), C.POINTER(vp)]
+        L.gf_photometry_destroy.argtypes = [vp]
+        L.gf_module_photometry.argtypes = [vp, vp, C.POINTER(Table), C.c_int64, C.c_int64]
+        L.gf_photoerr_create.argtypes = [vp, C.POINTER(PhotoerrConfig), C.POINTER(vp)]
+        L.gf_photoerr_destroy.argtypes = [vp]
+        L.gf_module_photoerrors.argtypes = [vp, vp, C.c_int64, C.POINTER(Table), C.c_int64, C.c_int64]
+        L.gf_module_vel2pm.argtypes = [vp, C.POINTER(Vel2pmConfig), C.POINTER(Table), C.c_int64, C.c_int64]
+        L.gf_module_gal2other.argtypes = [vp, C.c_int32, C.POINTER(Table), C.c_int64, C.c_int64]
+        L.gf_catalog_run.argtypes = [vp, C.POINTER(Job), BatchCallback, vp, C.POINTER(CatalogStats)]
+        L.gf_lambert_init.argtypes = [C.c_double, C.c_double, C.POINTER(Lambert)]
+        L.gf_footprint_pixelize.argtypes = [C.POINTER(Footprint), C.c_double, C.POINTER(Lambert),
+                                            C.POINTER(Extinction), C.POINTER(PencilBeam), C.POINTER(C.c_float),
+                                            C.c_int64, C.POINTER(C.c_int64)]
+        L.gf_photometry_build.argtypes = [C.POINTER(C.c_double), C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                          C.POINTER(C.c_float), C.POINTER(C.c_uint8), C.POINTER(C.c_int32),
+                                          C.POINTER(C.c_int32), C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.gf_multipliers.argtypes = [C.POINTER(C.c_uint32), C.c_int32]
+        L.gf_rng_seed_host.argtypes = [C.c_uint32, C.c_int32, C.POINTER(C.c_uint32)]
+        L.gf_mt19937_outputs.argtypes = [C.c_uint32, C.c_int, C.POINTER(C.c_uint32)]
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != 0:
+        raise GalfastError("galfast_b200 error %d: %s" % (status, lib().gf_last_error().decode()))
+
+
+# ---------------------------------------------------------------------------
+# host tables (numpy views with the library's column layout)
+# ---------------------------------------------------------------------------
+COLUMNS = [  # name, dtype, components (or "bands")
+    ("lb", np.float64, 2), ("projIdx", np.int32, 1), ("projXY", np.float32, 2), ("DM", np.float32, 1),
+    ("absmag", np.float32, 1), ("XYZ", np.float32, 3), ("comp", np.int32, 1), ("Am", np.float32, 1),
+    ("AmInf", np.float32, 1), ("hidden", np.int32, 1), ("FeH", np.float32, 1), ("vcyl", np.float32, 3),
+    ("mags", np.float32, "bands"), ("photoflags", np.int32, 1), ("obsmags", np.float32, "bands"),
+    ("pm", np.float32, 3), ("radec", np.float64, 2),
+]
+SKYGEN_COLUMNS = ["lb", "projIdx", "projXY", "DM", "absmag", "XYZ", "comp", "Am", "AmInf", "hidden"]
+
+
+class HostTable:
+    """A gf_table in host memory backed by numpy arrays; vector columns are (ncomp, capacity)."""
+
+    def __init__(self, capacity, nbands):
+        self.capacity = int(capacity)
+        self.nbands = int(nbands)
+        self.arrays = {}
+        self.t = Table()
+        self.t.capacity = self.capacity
+        self.t.size = 0
+        self.t.nbands = self.nbands
+        for name, dt, ncomp in COLUMNS:
+            k = self.nbands if ncomp == "bands" else ncomp
+            if k == 0:
+                setattr(self.t, name, None)
+                continue
+            a = np.zeros((k, self.capacity), dtype=dt)
+            self.arrays[name] = a
+            setattr(self.t, name, a.ctypes.data)
+
+    @property
+    def size(self):
+        return int(self.t.size)
+
+    def col(self, name):
+        a = self.arrays[name]
+        return a[0, : self.size] if a.shape[0] == 1 else a[:, : self.size]
+
+    def as_dict(self, names=None):
+        return {n: np.array(self.col(n)) for n in (names or self.arrays.keys())}
+
+
+# ---------------------------------------------------------------------------
+# context, generator, modules
+# ---------------------------------------------------------------------------
+class Context:
+    """A CUDA context: one device, one stream, the persistent RNG streams."""
+
+    def __init__(self, device=0):
+        self.h = C.c_void_p()
+        check(lib().gf_ctx_create(device, C.byref(self.h)))
+        self.nstreams = 0
+
+    def close(self):
+        if self.h:
+            lib().gf_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        check(lib().gf_ctx_sync(self.h))
+
+    def rng_init(self, seed48, nstreams=65536):
+        check(lib().gf_rng_init(self.h, seed48, nstreams))
+        self.nstreams = nstreams + (-nstreams) % 64
+
+    def rng_state(self):
+        s = np.zeros(3 * self.nstreams, dtype=np.uint32)
+        check(lib().gf_rng_get_state(self.h, s.ctypes.data, self.nstreams))
+        return s
+
+    def set_rng_state(self, s):
+        s = np.ascontiguousarray(s, dtype=np.uint32)
+        check(lib().gf_rng_set_state(self.h, s.ctypes.data, self.nstreams))
+
+
+class DeviceTable:
+    def __init__(self, ctx, capacity, nbands):
+        self.ctx = ctx
+        self.t = Table()
+        check(lib().gf_table_alloc(ctx.h, capacity, nbands, C.byref(self.t)))
+
+    @property
+    def size(self):
+        return int(self.t.size)
+
+    def download(self, host=None):
+        host = host or HostTable(self.t.capacity, self.t.nbands)
+        check(lib().gf_table_download(self.ctx.h, C.byref(self.t), C.byref(host.t)))
+        return host
+
+    def free(self):
+        lib().gf_table_free(self.ctx.h, C.byref(self.t))
+
+
+class Skygen:
+    """The skygen source module for one workload (os_skygen + one skygenHost per model)."""
+
+    def __init__(self, ctx, w):
+        self.ctx = ctx
+        self.w = w
+        self.h = C.c_void_p()
+        marr = (ModelConfig * len(w.models))(*w.models)
+        self._marr = marr
+        check(lib().gf_skygen_create(ctx.h, C.byref(w.sky), C.cast(w.pixel_array(), C.POINTER(PencilBeam)),
+                                     w.npixels, w.ammin.ctypes.data_as(C.POINTER(C.c_float)), C.byref(w.ext),
+                                     C.cast(marr, C.POINTER(ModelConfig)), len(w.models), C.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().gf_skygen_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self, model):
+        i = ModelInfo()
+        check(lib().gf_skygen_model_info_get(self.h, model, C.byref(i)))
+        return i
+
+    def lf(self, model):
+        n = self.info(model).lf_n
+        a = np.zeros(n, dtype=np.float32)
+        check(lib().gf_skygen_model_lf_get(self.h, model, a.ctypes.data_as(C.POINTER(C.c_float))))
+        return a
+
+    def integrate_counts(self, model, per_pixel=False):
+        e = C.c_double()
+        ec = C.c_double()
+        pp = np.zeros(self.w.npixels) if per_pixel else None
+        check(lib().gf_skygen_integrate(self.h, model, C.byref(e), C.byref(ec),
+                                        pp.ctypes.data_as(C.POINTER(C.c_double)) if pp is not None else None))
+        return e.value, ec.value, pp
+
+    def set_density_norm(self, model, norm):
+        check(lib().gf_skygen_set_norm(self.h, model, norm))
+
+    def draw_sources(self, model, table):
+        n = C.c_int64()
+        d = C.c_int32()
+        check(lib().gf_skygen_draw(self.h, model, C.byref(table.t), C.byref(n), C.byref(d)))
+        return n.value, bool(d.value)
+
+
+def run_catalog(ctx, w, sink=None):
+    """gf_catalog_run: os_skygen::run followed by the module chain for each batch.
+    sink(model, HostTable, row_offset) receives every batch in host memory."""
+    job = w.job(Job)
+    stats = CatalogStats()
+    host_cache = {}
+
+    def cb(user, model, tptr, row_offset):
+        if sink is None:
+            return 0
+        t = tptr.contents
+        key = (t.capacity, t.nbands)
+        if key not in host_cache:
+            host_cache[key] = HostTable(t.capacity, t.nbands)
+        h = host_cache[key]
+        st = lib().gf_table_download(ctx.h, tptr, C.byref(h.t))
+        if st != 0:
+            return 1
+        return 1 if sink(model, h, row_offset) else 0
+
+    ccb = BatchCallback(cb)
+    check(lib().gf_catalog_run(ctx.h, C.byref(job), ccb, None, C.byref(stats)))
+    return stats

@@ -1,0 +1,118 @@
+"""ctypes mirror of include/galfast_b200.h (structures only)."""
+import ctypes as C
+
+GF_OK = 0
+GF_MODEL_EXP_DISK = 1
+GF_MODEL_POWER_LAW_ELLIPSOID = 2
+GF_FRAME_GALPLANE = 0
+GF_FRAME_EXPLICIT = 1
+GF_EXT_NONE = 0
+GF_EXT_SCREEN_CSCB = 1
+GF_FOOT_ALL = 0
+GF_FOOT_LAMBERT_RECT = 1
+GF_FOOT_CAP = 2
+GF_FOOT_LATCUT = 3
+GF_MAX_BANDS = 17
+
+
+class PencilBeam(C.Structure):
+    _fields_ = [("cl", C.c_float), ("cb", C.c_float), ("sl", C.c_float), ("sb", C.c_float),
+                ("coveredFraction", C.c_float), ("dx", C.c_float), ("dA", C.c_float),
+                ("projIdx", C.c_int32), ("X", C.c_float), ("Y", C.c_float), ("extIdx", C.c_int32),
+                ("pad_", C.c_int32)]
+
+
+class Lambert(C.Structure):
+    _fields_ = [("l0", C.c_double), ("b0", C.c_double),
+                ("cl", C.c_float), ("cb", C.c_float), ("sl", C.c_float), ("sb", C.c_float)]
+
+
+class SkygenConfig(C.Structure):
+    _fields_ = [("m0", C.c_float), ("m1", C.c_float), ("dm", C.c_float),
+                ("M0", C.c_float), ("M1", C.c_float),
+                ("dmin", C.c_float), ("dmax", C.c_float),
+                ("nthreads", C.c_int32), ("nstars", C.c_float),
+                ("proj", Lambert * 2)]
+
+
+class ModelConfig(C.Structure):
+    _fields_ = [("type", C.c_int32), ("comp", C.c_int32), ("f", C.c_double),
+                ("l", C.c_double), ("h", C.c_double), ("rcut", C.c_double),
+                ("n", C.c_double), ("ba", C.c_double), ("ca", C.c_double),
+                ("rmin", C.c_double), ("rmax", C.c_double),
+                ("frame", C.c_int32), ("Rg", C.c_double), ("z0", C.c_double),
+                ("T", C.c_double * 3), ("M", C.c_double * 9),
+                ("lf_l", C.c_double), ("lf_b", C.c_double), ("lf_D", C.c_double),
+                ("lf_M", C.POINTER(C.c_double)), ("lf_phi", C.POINTER(C.c_double)), ("lf_n", C.c_int32)]
+
+
+class Extinction(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("A0", C.c_float)]
+
+
+class Footprint(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("proj", C.c_int32),
+                ("a", C.c_double), ("b", C.c_double), ("c", C.c_double), ("d", C.c_double)]
+
+
+class Table(C.Structure):
+    _fields_ = [("capacity", C.c_int64), ("size", C.c_int64), ("nbands", C.c_int32),
+                ("lb", C.c_void_p), ("projIdx", C.c_void_p), ("projXY", C.c_void_p),
+                ("DM", C.c_void_p), ("absmag", C.c_void_p), ("XYZ", C.c_void_p),
+                ("comp", C.c_void_p), ("Am", C.c_void_p), ("AmInf", C.c_void_p),
+                ("hidden", C.c_void_p), ("FeH", C.c_void_p), ("vcyl", C.c_void_p),
+                ("mags", C.c_void_p), ("photoflags", C.c_void_p), ("obsmags", C.c_void_p),
+                ("pm", C.c_void_p), ("radec", C.c_void_p)]
+
+
+class FixedFeHConfig(C.Structure):
+    _fields_ = [("FeH", C.c_float), ("comp_mask", C.c_uint32)]
+
+
+class VMoments(C.Structure):
+    _fields_ = [("m", (C.c_float * 5) * 3), ("ss", (C.c_float * 5) * 6)]
+
+
+class Bond2010Config(C.Structure):
+    _fields_ = [("comp_thin", C.c_uint32), ("comp_thick", C.c_uint32), ("comp_halo", C.c_uint32),
+                ("fk", C.c_float), ("disk_1", VMoments), ("disk_2", VMoments), ("halo", VMoments),
+                ("M", C.c_float * 9), ("T", C.c_float * 3)]
+
+
+class PhotometryConfig(C.Structure):
+    _fields_ = [("nbands", C.c_int32), ("bidx", C.c_int32), ("reddening", C.c_float * GF_MAX_BANDS),
+                ("nFeH", C.c_int32), ("nMr", C.c_int32), ("tcFeH", C.c_float * 2), ("tcMr", C.c_float * 2),
+                ("colors", C.POINTER(C.c_float)), ("eflags", C.POINTER(C.c_uint8)), ("comp_mask", C.c_uint32)]
+
+
+class PhotoerrConfig(C.Structure):
+    _fields_ = [("nbands", C.c_int32), ("nknots", C.c_int32),
+                ("mag", C.POINTER(C.c_double)), ("sigma", C.POINTER(C.c_double)), ("seed", C.c_uint64)]
+
+
+class Vel2pmConfig(C.Structure):
+    _fields_ = [("coordsys", C.c_int32), ("vLSR", C.c_float), ("u0", C.c_float), ("v0", C.c_float),
+                ("w0", C.c_float), ("Rg", C.c_float)]
+
+
+class ModelInfo(C.Structure):
+    _fields_ = [("m0", C.c_float), ("m1", C.c_float), ("dm", C.c_float), ("M0", C.c_float),
+                ("M1", C.c_float), ("dM", C.c_float), ("nm", C.c_int32), ("nM", C.c_int32),
+                ("npixels", C.c_int32), ("nthreads", C.c_int32), ("f", C.c_float),
+                ("lf_x0", C.c_float), ("lf_inv_dx", C.c_float), ("lf_n", C.c_int32), ("norm", C.c_float)]
+
+
+# exported symbols of libgalfast_b200.so declared in include/galfast_b200.h
+EXPORTS = [
+    "gf_last_error", "gf_ctx_create", "gf_ctx_destroy", "gf_ctx_sync",
+    "gf_rng_init", "gf_rng_seed48_from_cli_seed", "gf_rng_get_state", "gf_rng_set_state",
+    "gf_skygen_create", "gf_skygen_destroy", "gf_skygen_model_info_get", "gf_skygen_model_lf_get",
+    "gf_skygen_integrate", "gf_skygen_set_norm", "gf_skygen_draw",
+    "gf_table_alloc", "gf_table_free", "gf_table_download",
+    "gf_module_clipper", "gf_module_fixedfeh", "gf_module_bond2010",
+    "gf_photometry_create", "gf_photometry_destroy", "gf_module_photometry",
+    "gf_photoerr_create", "gf_photoerr_destroy", "gf_module_photoerrors",
+    "gf_module_vel2pm", "gf_module_gal2other",
+    "gf_lambert_init", "gf_footprint_pixelize", "gf_photometry_build",
+    "gf_multipliers", "gf_rng_seed_host", "gf_mt19937_outputs",
+]

@@ -1,0 +1,68 @@
+"""Build the galfast_b200 native library for sm_100a.
+
+    python -m galfast_b200.build          # or galfast_b200.build.build()
+
+compiles every CUDA and C++ source under galfast_b200/csrc into
+galfast_b200/_lib/libgalfast_b200.so and writes the stream-multiplier table
+(safeprimes_65536.bin) next to it.  Device code is compiled with -fmad=false
+and host code with -ffp-contract=off: the catalog's Poisson draws depend on the
+exact float results of the reference's expressions, so no multiply-add may be
+fused unless the source asks for it (gf_math.h uses explicit fma).
+"""
+import ctypes
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "_lib")
+LIBNAME = "libgalfast_b200.so"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+SOURCES = ["gf_skygen.cu", "gf_modules.cu", "gf_api.cu", "gf_host.cpp", "gf_safeprimes.cpp"]
+
+
+def nvcc_path():
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(cand):
+        raise RuntimeError("nvcc not found")
+    return cand
+
+
+def build(verbose=False, extra=None):
+    os.makedirs(LIBDIR, exist_ok=True)
+    out = os.path.join(LIBDIR, LIBNAME)
+    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    cmd = [nvcc_path(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
+           "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
+           "-shared", "-o", out, *srcs, "-ldl"]
+    if extra:
+        cmd[1:1] = list(extra)
+    if verbose:
+        print(" ".join(cmd))
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc build of %s failed" % LIBNAME)
+    write_multiplier_table(out)
+    return out
+
+
+def write_multiplier_table(libpath):
+    """Regenerate the 65536 stream multipliers (primality tests, ~5 s) once."""
+    fn = os.path.join(LIBDIR, "safeprimes_65536.bin")
+    if os.path.exists(fn) and os.path.getsize(fn) == 65536 * 4:
+        return fn
+    lib = ctypes.CDLL(libpath)
+    buf = (ctypes.c_uint32 * 65536)()
+    if lib.gf_multipliers(buf, 65536) != 0:
+        raise RuntimeError("multiplier generation failed")
+    with open(fn, "wb") as f:
+        f.write(bytes(buf))
+    return fn
+
+
+if __name__ == "__main__":
+    print(build(verbose=True))

@@ -1,0 +1,909 @@
+/*
+ * gf_api.cu -- the C ABI (include/galfast_b200.h) and the host orchestration
+ * of the catalog path on one B200.
+ */
+#include "gf_launch.h"
+#include "gf_host.h"
+#include "gf_safeprimes.h"
+
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+gf_status fail(gf_status s, const std::string &msg)
+{
+    g_err = msg;
+    return s;
+}
+
+#define GF_CUDA(call)                                                                        \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            return fail(e_ == cudaErrorMemoryAllocation ? GF_E_OOM : GF_E_CUDA,              \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                  \
+        }                                                                                    \
+    } while (0)
+
+#define GF_TRY(call)                         \
+    do {                                     \
+        gf_status s_ = (call);               \
+        if (s_ != GF_OK) return s_;          \
+    } while (0)
+
+template <typename T>
+gf_status dev_alloc(T **p, size_t n)
+{
+    *p = nullptr;
+    if (n == 0) return GF_OK;
+    GF_CUDA(cudaMalloc((void **)p, n * sizeof(T)));
+    return GF_OK;
+}
+
+template <typename T>
+void dev_free(T *&p)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+}  // namespace
+
+struct gf_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t *d_rng = nullptr;           /* persistent streams [3][rng_nstreams] */
+    int32_t rng_nstreams = 0;
+    uint32_t *d_mult = nullptr;
+    JumpTables jt = {nullptr, nullptr};
+    unsigned long long *d_counters = nullptr;   /* [0] record count, [1] visible count */
+    unsigned long long *h_counters = nullptr;   /* pinned */
+};
+
+struct ModelState {
+    gfh::HostModel hm;
+    float *d_lf = nullptr;
+    bool crawl_init = false;
+    bool done = false;
+    CrawlState st{};
+    CrawlState snap{};
+    void *st_mem = nullptr, *snap_mem = nullptr;
+    double expected = 0, expected_covered = 0;
+    int64_t drawn = 0;
+};
+
+struct gf_skygen {
+    gf_ctx *ctx = nullptr;
+    gf_skygen_config cfg{};
+    SkyGeom geom{};
+    gf_pencil_beam *d_pixels = nullptr;
+    float *d_ammin = nullptr;
+    std::vector<ModelState> models;
+    /* per-launch buffers */
+    int64_t *d_limits = nullptr;
+    int64_t *h_nstars = nullptr;         /* pinned [nthreads] */
+    uint32_t *d_rng_snap = nullptr;      /* [3][nthreads] */
+    StarRecord *d_rec = nullptr, *d_rec2 = nullptr;
+    int64_t rec_cap = 0;
+    /* placement + sort buffers (rec_cap rows) */
+    double *d_lb = nullptr;
+    int32_t *d_projIdx = nullptr, *d_hidden = nullptr;
+    float *d_projXY = nullptr, *d_DM = nullptr, *d_absmag = nullptr, *d_XYZ = nullptr, *d_Am = nullptr, *d_AmInf = nullptr;
+    uint64_t *d_key = nullptr, *d_key2 = nullptr;
+    uint32_t *d_idx = nullptr, *d_idx2 = nullptr;
+    void *d_sort_temp = nullptr;
+    size_t sort_temp_bytes = 0;
+    int nthreads = 0;
+};
+
+namespace {
+
+/* CrawlState arrays carved from one allocation */
+gf_status alloc_crawl_state(int n, CrawlState &st, void **mem)
+{
+    size_t words = (size_t)n * 12 + (size_t)n * 2;   /* 11 int/float fields + one int64 */
+    GF_CUDA(cudaMalloc(mem, words * 4 + 16));
+    char *p = (char *)*mem;
+    auto take = [&](size_t bytes) { char *r = p; p += bytes; return r; };
+    st.status = (int32_t *)take(4 * (size_t)n);
+    st.blk_ilb = (int32_t *)take(4 * (size_t)n);
+    st.blk_k = (int32_t *)take(4 * (size_t)n);
+    st.pos = (int32_t *)take(4 * (size_t)n);
+    st.ndraw = (int32_t *)take(4 * (size_t)n);
+    st.cur_ilb = (int32_t *)take(4 * (size_t)n);
+    st.cur_im = (int32_t *)take(4 * (size_t)n);
+    st.cur_iM = (int32_t *)take(4 * (size_t)n);
+    st.D = (float *)take(4 * (size_t)n);
+    st.Am = (float *)take(4 * (size_t)n);
+    st.ms = (float *)take(4 * (size_t)n);
+    p = (char *)(((uintptr_t)p + 15) & ~(uintptr_t)15);
+    st.nstars = (int64_t *)take(8 * (size_t)n);
+    return GF_OK;
+}
+
+size_t crawl_state_bytes(int n) { return (size_t)n * 12 * 4 + (size_t)n * 8 + 16; }
+
+gf_status ensure_rec_capacity(gf_skygen *s, int64_t need)
+{
+    if (need <= s->rec_cap) return GF_OK;
+    int64_t cap = std::max<int64_t>(need, s->rec_cap * 3 / 2);
+    cap = std::max<int64_t>(cap, 4096);
+    dev_free(s->d_rec); dev_free(s->d_rec2);
+    dev_free(s->d_lb); dev_free(s->d_projIdx); dev_free(s->d_hidden);
+    dev_free(s->d_projXY); dev_free(s->d_DM); dev_free(s->d_absmag); dev_free(s->d_XYZ);
+    dev_free(s->d_Am); dev_free(s->d_AmInf);
+    dev_free(s->d_key); dev_free(s->d_key2); dev_free(s->d_idx); dev_free(s->d_idx2);
+    if (s->d_sort_temp) cudaFree(s->d_sort_temp);
+    s->d_sort_temp = nullptr;
+    s->rec_cap = 0;
+    GF_TRY(dev_alloc(&s->d_rec, cap));
+    GF_TRY(dev_alloc(&s->d_rec2, cap));
+    GF_TRY(dev_alloc(&s->d_lb, 2 * cap));
+    GF_TRY(dev_alloc(&s->d_projIdx, cap));
+    GF_TRY(dev_alloc(&s->d_hidden, cap));
+    GF_TRY(dev_alloc(&s->d_projXY, 2 * cap));
+    GF_TRY(dev_alloc(&s->d_DM, cap));
+    GF_TRY(dev_alloc(&s->d_absmag, cap));
+    GF_TRY(dev_alloc(&s->d_XYZ, 3 * cap));
+    GF_TRY(dev_alloc(&s->d_Am, cap));
+    GF_TRY(dev_alloc(&s->d_AmInf, cap));
+    GF_TRY(dev_alloc(&s->d_key, cap));
+    GF_TRY(dev_alloc(&s->d_key2, cap));
+    GF_TRY(dev_alloc(&s->d_idx, cap));
+    GF_TRY(dev_alloc(&s->d_idx2, cap));
+    size_t tb = 0;
+    GF_CUDA(gfk::sort_temp_bytes(cap, &tb));
+    GF_CUDA(cudaMalloc(&s->d_sort_temp, tb + 256));
+    s->sort_temp_bytes = tb + 256;
+    s->rec_cap = cap;
+    return GF_OK;
+}
+
+gfk::LaunchCrawl crawl_launch(gf_skygen *s, ModelState &ms)
+{
+    gfk::LaunchCrawl L;
+    memset(&L, 0, sizeof(L));
+    L.m = ms.hm.m;
+    L.m.lf = ms.d_lf;
+    L.g = s->geom;
+    L.st = ms.st;
+    L.rng = s->ctx->d_rng;
+    L.rng_nstreams = s->ctx->rng_nstreams;
+    L.jt = s->ctx->jt;
+    L.stream_begin = 0;
+    L.stream_end = s->nthreads;
+    L.limits = s->d_limits;
+    L.rec = s->d_rec;
+    L.rec_capacity = s->rec_cap;
+    L.rec_count = s->ctx->d_counters;
+    L.err = s->ctx->d_counters + 2;
+    return L;
+}
+
+/* save / restore the crawl state and the crawl streams of one model */
+gf_status snapshot(gf_skygen *s, ModelState &ms, bool restore)
+{
+    cudaStream_t st = s->ctx->stream;
+    const int N = s->nthreads, NS = s->ctx->rng_nstreams;
+    size_t bytes = crawl_state_bytes(N);
+    if (restore) GF_CUDA(cudaMemcpyAsync(ms.st_mem, ms.snap_mem, bytes, cudaMemcpyDeviceToDevice, st));
+    else GF_CUDA(cudaMemcpyAsync(ms.snap_mem, ms.st_mem, bytes, cudaMemcpyDeviceToDevice, st));
+    for (int k = 0; k < 3; k++) {
+        uint32_t *live = s->ctx->d_rng + (size_t)k * NS;
+        uint32_t *saved = s->d_rng_snap + (size_t)k * N;
+        if (restore) GF_CUDA(cudaMemcpyAsync(live, saved, 4 * (size_t)N, cudaMemcpyDeviceToDevice, st));
+        else GF_CUDA(cudaMemcpyAsync(saved, live, 4 * (size_t)N, cudaMemcpyDeviceToDevice, st));
+    }
+    return GF_OK;
+}
+
+/* restore streams [t, n) of a model's crawl state and streams from the snapshot */
+__global__ void restore_tail(CrawlState st, CrawlState snap, uint32_t *rng, int32_t NS, const uint32_t *rng_snap, int32_t n, int32_t t)
+{
+    int i = t + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    st.status[i] = snap.status[i]; st.blk_ilb[i] = snap.blk_ilb[i]; st.blk_k[i] = snap.blk_k[i]; st.pos[i] = snap.pos[i];
+    st.ndraw[i] = snap.ndraw[i]; st.cur_ilb[i] = snap.cur_ilb[i]; st.cur_im[i] = snap.cur_im[i]; st.cur_iM[i] = snap.cur_iM[i];
+    st.D[i] = snap.D[i]; st.Am[i] = snap.Am[i]; st.ms[i] = snap.ms[i]; st.nstars[i] = 0;
+    for (int k = 0; k < 3; k++) rng[(size_t)k * NS + i] = rng_snap[(size_t)k * n + i];
+}
+
+__global__ void filter_records(const StarRecord *in, int64_t n, int32_t stream_end, StarRecord *out, unsigned long long *count)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        StarRecord r = in[i];
+        if (r.stream < stream_end) {
+            unsigned long long k = atomicAdd(count, 1ull);
+            out[k] = r;
+        }
+    }
+}
+
+__global__ void set_limits(int64_t *lim, int n, int32_t t, int64_t Lt)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    lim[i] = (i < t) ? 0 : (i == t ? Lt : 0);
+}
+
+__global__ void fill_i64(int64_t *p, int n, int64_t v)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+gf_status check_ctx(gf_ctx *ctx)
+{
+    if (!ctx) return fail(GF_E_INVALID, "null context");
+    GF_CUDA(cudaSetDevice(ctx->device));
+    return GF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *gf_last_error(void) { return g_err.c_str(); }
+
+gf_status gf_ctx_create(int device, gf_ctx **out)
+{
+    if (!out) return fail(GF_E_INVALID, "null output");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return fail(GF_E_CUDA, "no CUDA device available");
+    if (device < 0 || device >= ndev) return fail(GF_E_INVALID, "device index out of range");
+    GF_CUDA(cudaSetDevice(device));
+    gf_ctx *c = new gf_ctx();
+    c->device = device;
+    cudaError_t ce = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaMalloc(&c->d_counters, 64);
+    if (ce == cudaSuccess) ce = cudaMallocHost(&c->h_counters, 64);
+    if (ce != cudaSuccess) {
+        delete c;
+        return fail(GF_E_CUDA, std::string("context setup: ") + cudaGetErrorString(ce));
+    }
+    *out = c;
+    return GF_OK;
+}
+
+gf_status gf_ctx_destroy(gf_ctx *ctx)
+{
+    if (!ctx) return GF_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    dev_free(ctx->d_rng);
+    dev_free(ctx->d_mult);
+    dev_free(ctx->jt.lo);
+    dev_free(ctx->jt.hi);
+    dev_free(ctx->d_counters);
+    if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return GF_OK;
+}
+
+gf_status gf_ctx_sync(gf_ctx *ctx)
+{
+    GF_TRY(check_ctx(ctx));
+    GF_CUDA(cudaStreamSynchronize(ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_rng_init(gf_ctx *ctx, uint32_t seed48, int32_t nstreams)
+{
+    GF_TRY(check_ctx(ctx));
+    if (nstreams <= 0 || nstreams > GF_MAX_STREAMS) return fail(GF_E_INVALID, "nstreams must be in [1, 65536]");
+    if (nstreams % 64) nstreams += 64 - nstreams % 64;     /* roundUpModulo (cuda_rng.h:468) */
+    const std::vector<uint32_t> &mult = gfh::multipliers();
+    if (!ctx->d_mult) {
+        GF_TRY(dev_alloc(&ctx->d_mult, GF_MAX_STREAMS));
+        GF_CUDA(cudaMemcpy(ctx->d_mult, mult.data(), 4 * (size_t)GF_MAX_STREAMS, cudaMemcpyHostToDevice));
+        GF_TRY(dev_alloc(&ctx->jt.lo, (size_t)GF_MAX_STREAMS * 32));
+        GF_TRY(dev_alloc(&ctx->jt.hi, (size_t)GF_MAX_STREAMS * 32));
+        GF_CUDA(gfk::launch_jump_tables(ctx->d_mult, GF_MAX_STREAMS, ctx->jt.lo, ctx->jt.hi, ctx->stream));
+    }
+    std::vector<uint32_t> h(3 * (size_t)nstreams);
+    gfh::seed_streams(seed48, nstreams, mult.data(), h.data());
+    if (ctx->rng_nstreams != nstreams) {
+        dev_free(ctx->d_rng);
+        GF_TRY(dev_alloc(&ctx->d_rng, 3 * (size_t)nstreams));
+        ctx->rng_nstreams = nstreams;
+    }
+    GF_CUDA(cudaMemcpyAsync(ctx->d_rng, h.data(), 4 * h.size(), cudaMemcpyHostToDevice, ctx->stream));
+    GF_CUDA(cudaStreamSynchronize(ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_rng_get_state(gf_ctx *ctx, uint32_t *host_state, int32_t nstreams)
+{
+    GF_TRY(check_ctx(ctx));
+    if (nstreams != ctx->rng_nstreams) return fail(GF_E_INVALID, "stream count mismatch");
+    GF_CUDA(cudaMemcpyAsync(host_state, ctx->d_rng, 12 * (size_t)nstreams, cudaMemcpyDeviceToHost, ctx->stream));
+    GF_CUDA(cudaStreamSynchronize(ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_rng_set_state(gf_ctx *ctx, const uint32_t *host_state, int32_t nstreams)
+{
+    GF_TRY(check_ctx(ctx));
+    if (nstreams != ctx->rng_nstreams) return fail(GF_E_INVALID, "stream count mismatch");
+    GF_CUDA(cudaMemcpyAsync(ctx->d_rng, host_state, 12 * (size_t)nstreams, cudaMemcpyHostToDevice, ctx->stream));
+    GF_CUDA(cudaStreamSynchronize(ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_skygen_destroy(gf_skygen *s);
+
+gf_status gf_skygen_create(gf_ctx *ctx, const gf_skygen_config *cfg, const gf_pencil_beam *pixels, int32_t npixels,
+                           const float *beam_ammin, const gf_extinction *ext, const gf_model_config *models,
+                           int32_t nmodels, gf_skygen **out)
+{
+    GF_TRY(check_ctx(ctx));
+    if (!cfg || !pixels || npixels <= 0 || !models || nmodels <= 0 || !out) return fail(GF_E_INVALID, "invalid skygen arguments");
+    for (int i = 0; i < npixels; i++) {
+        if (pixels[i].projIdx < 0 || pixels[i].projIdx > 1) return fail(GF_E_INVALID, "pixel projIdx must be 0 or 1");
+        if (beam_ammin && (pixels[i].extIdx < 0 || pixels[i].extIdx >= npixels)) return fail(GF_E_INVALID, "pixel extIdx out of range");
+    }
+    std::vector<gfh::HostModel> hms;
+    std::string err;
+    if (!gfh::setup_models(*cfg, npixels, models, nmodels, hms, err)) return fail(GF_E_INVALID, err);
+    gf_skygen *s = new gf_skygen();
+    s->ctx = ctx;
+    s->cfg = *cfg;
+    s->nthreads = cfg->nthreads;
+    gf_status st = GF_OK;
+    auto bail = [&](gf_status code) { gf_skygen_destroy(s); return code; };
+    if ((st = dev_alloc(&s->d_pixels, npixels)) != GF_OK) return bail(st);
+    cudaMemcpy(s->d_pixels, pixels, sizeof(gf_pencil_beam) * (size_t)npixels, cudaMemcpyHostToDevice);
+    if (beam_ammin) {
+        if ((st = dev_alloc(&s->d_ammin, npixels)) != GF_OK) return bail(st);
+        cudaMemcpy(s->d_ammin, beam_ammin, 4 * (size_t)npixels, cudaMemcpyHostToDevice);
+    }
+    s->geom.pixels = s->d_pixels;
+    s->geom.npixels = npixels;
+    s->geom.ammin = s->d_ammin;
+    s->geom.ext_kind = ext ? ext->kind : GF_EXT_NONE;
+    s->geom.A0 = ext ? ext->A0 : 0.f;
+    s->geom.proj[0] = cfg->proj[0];
+    s->geom.proj[1] = cfg->proj[1];
+    s->models.resize(nmodels);
+    for (int i = 0; i < nmodels; i++) {
+        ModelState &ms = s->models[i];
+        ms.hm = hms[i];
+        if ((st = dev_alloc(&ms.d_lf, ms.hm.lf.size())) != GF_OK) return bail(st);
+        cudaMemcpy(ms.d_lf, ms.hm.lf.data(), 4 * ms.hm.lf.size(), cudaMemcpyHostToDevice);
+        if ((st = alloc_crawl_state(s->nthreads, ms.st, &ms.st_mem)) != GF_OK) return bail(st);
+        if ((st = alloc_crawl_state(s->nthreads, ms.snap, &ms.snap_mem)) != GF_OK) return bail(st);
+    }
+    if ((st = dev_alloc(&s->d_limits, s->nthreads)) != GF_OK) return bail(st);
+    if ((st = dev_alloc(&s->d_rng_snap, 3 * (size_t)s->nthreads)) != GF_OK) return bail(st);
+    if (cudaMallocHost(&s->h_nstars, 8 * (size_t)s->nthreads) != cudaSuccess) return bail(fail(GF_E_OOM, "pinned allocation"));
+    cudaError_t ce = cudaGetLastError();
+    if (ce != cudaSuccess) return bail(fail(GF_E_CUDA, cudaGetErrorString(ce)));
+    *out = s;
+    return GF_OK;
+}
+
+gf_status gf_skygen_destroy(gf_skygen *s)
+{
+    if (!s) return GF_OK;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    for (auto &ms : s->models) {
+        dev_free(ms.d_lf);
+        if (ms.st_mem) cudaFree(ms.st_mem);
+        if (ms.snap_mem) cudaFree(ms.snap_mem);
+    }
+    dev_free(s->d_pixels); dev_free(s->d_ammin); dev_free(s->d_limits); dev_free(s->d_rng_snap);
+    if (s->h_nstars) cudaFreeHost(s->h_nstars);
+    dev_free(s->d_rec); dev_free(s->d_rec2);
+    dev_free(s->d_lb); dev_free(s->d_projIdx); dev_free(s->d_hidden);
+    dev_free(s->d_projXY); dev_free(s->d_DM); dev_free(s->d_absmag); dev_free(s->d_XYZ);
+    dev_free(s->d_Am); dev_free(s->d_AmInf);
+    dev_free(s->d_key); dev_free(s->d_key2); dev_free(s->d_idx); dev_free(s->d_idx2);
+    if (s->d_sort_temp) cudaFree(s->d_sort_temp);
+    delete s;
+    return GF_OK;
+}
+
+gf_status gf_skygen_model_info_get(gf_skygen *s, int32_t model, gf_skygen_model_info *info)
+{
+    if (!s || model < 0 || model >= (int)s->models.size() || !info) return fail(GF_E_INVALID, "invalid model");
+    const SkyModel &m = s->models[model].hm.m;
+    info->m0 = m.m0; info->m1 = m.m1; info->dm = m.dm; info->M0 = m.M0; info->M1 = m.M1; info->dM = m.dM;
+    info->nm = m.nm; info->nM = m.nM; info->npixels = m.npixels; info->nthreads = m.nthreads;
+    info->f = m.f; info->lf_x0 = m.lf_x0; info->lf_inv_dx = m.lf_inv_dx; info->lf_n = m.lf_n;
+    info->norm = m.norm;
+    return GF_OK;
+}
+
+gf_status gf_skygen_model_lf_get(gf_skygen *s, int32_t model, float *lf)
+{
+    if (!s || model < 0 || model >= (int)s->models.size() || !lf) return fail(GF_E_INVALID, "invalid model");
+    const std::vector<float> &v = s->models[model].hm.lf;
+    std::copy(v.begin(), v.end(), lf);
+    return GF_OK;
+}
+
+gf_status gf_skygen_set_norm(gf_skygen *s, int32_t model, float norm)
+{
+    if (!s || model < 0 || model >= (int)s->models.size()) return fail(GF_E_INVALID, "invalid model");
+    ModelState &ms = s->models[model];
+    ms.hm.m.norm = norm;
+    ms.expected *= norm;
+    ms.expected_covered *= norm;
+    return GF_OK;
+}
+
+gf_status gf_skygen_integrate(gf_skygen *s, int32_t model, double *expected, double *expected_covered, double *per_pixel)
+{
+    if (!s || model < 0 || model >= (int)s->models.size()) return fail(GF_E_INVALID, "invalid model");
+    GF_TRY(check_ctx(s->ctx));
+    ModelState &ms = s->models[model];
+    cudaStream_t st = s->ctx->stream;
+    const int N = s->nthreads;
+    const int npix = s->geom.npixels;
+    double *d_counts = nullptr, *d_cov = nullptr, *d_pp = nullptr;
+    GF_TRY(dev_alloc(&d_counts, N));
+    GF_TRY(dev_alloc(&d_cov, N));
+    if (per_pixel) GF_TRY(dev_alloc(&d_pp, npix));
+    GF_CUDA(cudaMemsetAsync(d_counts, 0, 8 * (size_t)N, st));
+    GF_CUDA(cudaMemsetAsync(d_cov, 0, 8 * (size_t)N, st));
+    if (d_pp) GF_CUDA(cudaMemsetAsync(d_pp, 0, 8 * (size_t)npix, st));
+    gfk::LaunchCrawl L = crawl_launch(s, ms);
+    L.counts = d_counts;
+    L.countsCovered = d_cov;
+    L.per_pixel = d_pp;
+    const SkyModel &m = ms.hm.m;
+    const long long kmax = (long long)m.nm * m.nM;
+    if (kmax % GF_BLOCK == 0) {
+        /* blocks never straddle pixels: one crawl over all pixels visits the same
+         * bins with the same anchors as the reference's pixel-block launches */
+        L.pix_base = 0;
+        GF_CUDA(gfk::launch_crawl(L, 0, st));
+    } else {
+        /* pixel blocks of 2^21 / nthreads pixels (skyconfig_impl.h:344-387) */
+        const int PIXBLOCK = 1024 * 1024 * 2 / N;
+        if (PIXBLOCK < 1) return fail(GF_E_UNSUPPORTED, "nthreads too large for pixel blocking");
+        for (int p0 = 0; p0 < npix; p0 += PIXBLOCK) {
+            int p1 = std::min(p0 + PIXBLOCK, npix);
+            L.g.pixels = s->d_pixels + p0;
+            L.g.npixels = p1 - p0;
+            L.pix_base = p0;
+            GF_CUDA(gfk::launch_crawl(L, 0, st));
+        }
+    }
+    std::vector<double> hc(N), hv(N);
+    GF_CUDA(cudaMemcpyAsync(hc.data(), d_counts, 8 * (size_t)N, cudaMemcpyDeviceToHost, st));
+    GF_CUDA(cudaMemcpyAsync(hv.data(), d_cov, 8 * (size_t)N, cudaMemcpyDeviceToHost, st));
+    if (per_pixel) GF_CUDA(cudaMemcpyAsync(per_pixel, d_pp, 8 * (size_t)npix, cudaMemcpyDeviceToHost, st));
+    GF_CUDA(cudaStreamSynchronize(st));
+    dev_free(d_counts); dev_free(d_cov); dev_free(d_pp);
+    double e = 0, ec = 0;
+    for (int i = 0; i < N; i++) { e += hc[i]; ec += hv[i]; }
+    ms.expected = e;
+    ms.expected_covered = ec;
+    if (expected) *expected = e;
+    if (expected_covered) *expected_covered = ec;
+    return GF_OK;
+}
+
+gf_status gf_skygen_draw(gf_skygen *s, int32_t model, gf_table *out, int64_t *n_generated, int32_t *done)
+{
+    if (!s || model < 0 || model >= (int)s->models.size() || !out || !n_generated || !done) return fail(GF_E_INVALID, "invalid arguments");
+    GF_TRY(check_ctx(s->ctx));
+    if (s->ctx->rng_nstreams < s->nthreads) return fail(GF_E_STATE, "gf_rng_init with at least nthreads streams must precede gf_skygen_draw");
+    if (out->capacity <= 0) return fail(GF_E_INVALID, "output table has no capacity");
+    ModelState &ms = s->models[model];
+    cudaStream_t st = s->ctx->stream;
+    const int N = s->nthreads;
+    const int64_t C = out->capacity;
+    if (ms.done) { out->size = 0; *n_generated = 0; *done = 1; return GF_OK; }
+    if (!ms.crawl_init) {
+        GF_CUDA(cudaMemsetAsync(ms.st_mem, 0, crawl_state_bytes(N), st));
+        ms.crawl_init = true;
+    }
+    GF_CUDA(cudaMemsetAsync(ms.st.nstars, 0, 8 * (size_t)N, st));
+    GF_CUDA(cudaMemsetAsync(s->ctx->d_counters + 2, 0, 8, st));
+    GF_TRY(snapshot(s, ms, false));
+    /* first guess of the record buffer: the stars still expected, or the capacity */
+    double remaining = std::max(0.0, ms.expected - (double)ms.drawn);
+    int64_t guess = (int64_t)std::min<double>((double)C, remaining * 1.05 + 6.0 * sqrt(remaining + 1.0) + 1024.0);
+    GF_TRY(ensure_rec_capacity(s, std::max<int64_t>(guess, 4096)));
+
+    const int fb = (N + 255) / 256;
+    int64_t total = 0;
+    for (;;) {
+        fill_i64<<<fb, 256, 0, st>>>(s->d_limits, N, C);
+        GF_CUDA(cudaMemsetAsync(s->ctx->d_counters, 0, 16, st));
+        gfk::LaunchCrawl L = crawl_launch(s, ms);
+        GF_CUDA(gfk::launch_crawl(L, 1, st));
+        GF_CUDA(cudaMemcpyAsync(s->ctx->h_counters, s->ctx->d_counters, 8, cudaMemcpyDeviceToHost, st));
+        GF_CUDA(cudaMemcpyAsync(s->h_nstars, ms.st.nstars, 8 * (size_t)N, cudaMemcpyDeviceToHost, st));
+        GF_CUDA(cudaStreamSynchronize(st));
+        total = (int64_t)s->ctx->h_counters[0];
+        if (total <= s->rec_cap) break;
+        /* more stars than the record buffer holds: grow and redo from the snapshot */
+        GF_TRY(snapshot(s, ms, true));
+        GF_CUDA(cudaMemsetAsync(ms.st.nstars, 0, 8 * (size_t)N, st));
+        GF_TRY(ensure_rec_capacity(s, total));
+    }
+    /* streams fill the batch in stream order (the CPU path's thread order) */
+    int64_t cum = 0;
+    int t = -1;
+    for (int i = 0; i < N; i++) {
+        if (cum + s->h_nstars[i] >= C) { t = i; break; }
+        cum += s->h_nstars[i];
+    }
+    int64_t nbatch;
+    bool generated_all;
+    if (t < 0) {
+        nbatch = total;
+        generated_all = true;
+    } else {
+        /* keep the records of streams before t, rerun t with the room left and
+         * let every later stream stop at its first star (skygen.cu.h:366-373) */
+        GF_CUDA(cudaMemsetAsync(s->ctx->d_counters, 0, 8, st));
+        int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)gfk::sm_count() * 16);
+        if (total > 0) filter_records<<<std::max(blocks, 1), 256, 0, st>>>(s->d_rec, total, t, s->d_rec2, s->ctx->d_counters);
+        std::swap(s->d_rec, s->d_rec2);
+        /* streams < t keep the state they reached in the speculative run */
+        if (N - t > 0)
+            restore_tail<<<(N - t + 255) / 256, 256, 0, st>>>(ms.st, ms.snap, s->ctx->d_rng, s->ctx->rng_nstreams,
+                                                              s->d_rng_snap, N, t);
+        set_limits<<<fb, 256, 0, st>>>(s->d_limits, N, t, C - cum);
+        gfk::LaunchCrawl L = crawl_launch(s, ms);
+        L.stream_begin = t;
+        GF_CUDA(gfk::launch_crawl(L, 1, st));
+        GF_CUDA(cudaMemcpyAsync(s->ctx->h_counters, s->ctx->d_counters, 8, cudaMemcpyDeviceToHost, st));
+        GF_CUDA(cudaStreamSynchronize(st));
+        nbatch = (int64_t)s->ctx->h_counters[0];
+        if (nbatch != C) return fail(GF_E_CUDA, "batch rerun produced an unexpected star count");
+        generated_all = false;
+    }
+    (void)cum;
+    /* placement, sort by (hidden, l, b, DM, M, Am), truncation at the first hidden row */
+    GF_CUDA(cudaMemsetAsync(s->ctx->d_counters + 1, 0, 8, st));
+    gfk::LaunchPlace P;
+    P.m = ms.hm.m;
+    P.m.lf = ms.d_lf;
+    P.g = s->geom;
+    P.rec = s->d_rec;
+    P.n = nbatch;
+    P.lb = s->d_lb; P.projIdx = s->d_projIdx; P.projXY = s->d_projXY; P.DM = s->d_DM; P.absmag = s->d_absmag;
+    P.XYZ = s->d_XYZ; P.Am = s->d_Am; P.AmInf = s->d_AmInf; P.hidden = s->d_hidden; P.key = s->d_key;
+    P.nvis = s->ctx->d_counters + 1;
+    GF_CUDA(gfk::launch_place(P, st));
+    GF_CUDA(cudaMemcpyAsync(s->ctx->h_counters + 1, s->ctx->d_counters + 1, 8, cudaMemcpyDeviceToHost, st));
+    GF_CUDA(cudaStreamSynchronize(st));
+    int64_t nvis = (int64_t)s->ctx->h_counters[1];
+    GF_CUDA(cudaMemcpy(s->ctx->h_counters + 2, s->ctx->d_counters + 2, 8, cudaMemcpyDeviceToHost));
+    if (s->ctx->h_counters[2]) return fail(GF_E_INVALID, "a bin has an infinite expected star count");
+    gfk::LaunchSort S;
+    S.n = nbatch;
+    S.nvisible = nvis;
+    S.key_in = s->d_key; S.key_out = s->d_key2; S.idx_in = s->d_idx; S.idx_out = s->d_idx2;
+    S.temp = s->d_sort_temp; S.temp_bytes = s->sort_temp_bytes;
+    S.lb = s->d_lb; S.projIdx = s->d_projIdx; S.projXY = s->d_projXY; S.DM = s->d_DM; S.absmag = s->d_absmag;
+    S.XYZ = s->d_XYZ; S.Am = s->d_Am; S.AmInf = s->d_AmInf; S.comp = ms.hm.m.comp;
+    S.out = *out;
+    GF_CUDA(gfk::launch_sort_gather(S, st));
+    GF_CUDA(cudaStreamSynchronize(st));
+    out->size = nvis;
+    ms.drawn += nbatch;
+    *n_generated = nbatch;
+    *done = generated_all ? 1 : 0;
+    if (generated_all) ms.done = true;
+    return GF_OK;
+}
+
+/* ---------------- tables ---------------- */
+
+gf_status gf_table_alloc(gf_ctx *ctx, int64_t capacity, int32_t nbands, gf_table *t)
+{
+    GF_TRY(check_ctx(ctx));
+    if (!t || capacity <= 0 || nbands < 0 || nbands > GF_MAX_BANDS) return fail(GF_E_INVALID, "invalid table arguments");
+    memset(t, 0, sizeof(*t));
+    t->capacity = capacity;
+    t->nbands = nbands;
+    size_t n = (size_t)capacity;
+    GF_TRY(dev_alloc(&t->lb, 2 * n));
+    GF_TRY(dev_alloc(&t->projIdx, n));
+    GF_TRY(dev_alloc(&t->projXY, 2 * n));
+    GF_TRY(dev_alloc(&t->DM, n));
+    GF_TRY(dev_alloc(&t->absmag, n));
+    GF_TRY(dev_alloc(&t->XYZ, 3 * n));
+    GF_TRY(dev_alloc(&t->comp, n));
+    GF_TRY(dev_alloc(&t->Am, n));
+    GF_TRY(dev_alloc(&t->AmInf, n));
+    GF_TRY(dev_alloc(&t->hidden, n));
+    GF_TRY(dev_alloc(&t->FeH, n));
+    GF_TRY(dev_alloc(&t->vcyl, 3 * n));
+    if (nbands) {
+        GF_TRY(dev_alloc(&t->mags, (size_t)nbands * n));
+        GF_TRY(dev_alloc(&t->obsmags, (size_t)nbands * n));
+    }
+    GF_TRY(dev_alloc(&t->photoflags, n));
+    GF_TRY(dev_alloc(&t->pm, 3 * n));
+    GF_TRY(dev_alloc(&t->radec, 2 * n));
+    /* module columns start at zero so that rows a module skips are defined */
+    GF_CUDA(cudaMemsetAsync(t->FeH, 0, 4 * n, ctx->stream));
+    GF_CUDA(cudaMemsetAsync(t->vcyl, 0, 12 * n, ctx->stream));
+    if (nbands) {
+        GF_CUDA(cudaMemsetAsync(t->mags, 0, 4 * (size_t)nbands * n, ctx->stream));
+        GF_CUDA(cudaMemsetAsync(t->obsmags, 0, 4 * (size_t)nbands * n, ctx->stream));
+    }
+    GF_CUDA(cudaMemsetAsync(t->photoflags, 0, 4 * n, ctx->stream));
+    GF_CUDA(cudaMemsetAsync(t->pm, 0, 12 * n, ctx->stream));
+    GF_CUDA(cudaMemsetAsync(t->radec, 0, 16 * n, ctx->stream));
+    GF_CUDA(cudaStreamSynchronize(ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_table_free(gf_ctx *ctx, gf_table *t)
+{
+    if (!ctx || !t) return GF_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    dev_free(t->lb); dev_free(t->projIdx); dev_free(t->projXY); dev_free(t->DM); dev_free(t->absmag);
+    dev_free(t->XYZ); dev_free(t->comp); dev_free(t->Am); dev_free(t->AmInf); dev_free(t->hidden);
+    dev_free(t->FeH); dev_free(t->vcyl); dev_free(t->mags); dev_free(t->photoflags); dev_free(t->obsmags);
+    dev_free(t->pm); dev_free(t->radec);
+    memset(t, 0, sizeof(*t));
+    return GF_OK;
+}
+
+gf_status gf_table_download(gf_ctx *ctx, const gf_table *dev, gf_table *host)
+{
+    GF_TRY(check_ctx(ctx));
+    if (!dev || !host) return fail(GF_E_INVALID, "null table");
+    if (host->capacity < dev->size) return fail(GF_E_INVALID, "host table too small");
+    const size_t n = (size_t)dev->size, P = (size_t)dev->capacity, H = (size_t)host->capacity;
+    cudaStream_t st = ctx->stream;
+    auto cp = [&](void *h, const void *d, size_t elem, int ncomp) -> gf_status {
+        if (!h || !d || n == 0) return GF_OK;
+        for (int k = 0; k < ncomp; k++)
+            GF_CUDA(cudaMemcpyAsync((char *)h + k * H * elem, (const char *)d + k * P * elem, n * elem, cudaMemcpyDeviceToHost, st));
+        return GF_OK;
+    };
+    GF_TRY(cp(host->lb, dev->lb, 8, 2));
+    GF_TRY(cp(host->projIdx, dev->projIdx, 4, 1));
+    GF_TRY(cp(host->projXY, dev->projXY, 4, 2));
+    GF_TRY(cp(host->DM, dev->DM, 4, 1));
+    GF_TRY(cp(host->absmag, dev->absmag, 4, 1));
+    GF_TRY(cp(host->XYZ, dev->XYZ, 4, 3));
+    GF_TRY(cp(host->comp, dev->comp, 4, 1));
+    GF_TRY(cp(host->Am, dev->Am, 4, 1));
+    GF_TRY(cp(host->AmInf, dev->AmInf, 4, 1));
+    GF_TRY(cp(host->hidden, dev->hidden, 4, 1));
+    GF_TRY(cp(host->FeH, dev->FeH, 4, 1));
+    GF_TRY(cp(host->vcyl, dev->vcyl, 4, 3));
+    GF_TRY(cp(host->mags, dev->mags, 4, dev->nbands));
+    GF_TRY(cp(host->photoflags, dev->photoflags, 4, 1));
+    GF_TRY(cp(host->obsmags, dev->obsmags, 4, dev->nbands));
+    GF_TRY(cp(host->pm, dev->pm, 4, 3));
+    GF_TRY(cp(host->radec, dev->radec, 8, 2));
+    GF_CUDA(cudaStreamSynchronize(st));
+    host->size = dev->size;
+    return GF_OK;
+}
+
+/* ---------------- modules ---------------- */
+
+static gf_status row_range(const gf_table *t, int64_t begin, int64_t end)
+{
+    if (!t || begin < 0 || end < begin || end > t->capacity) return fail(GF_E_INVALID, "invalid row range");
+    return GF_OK;
+}
+
+gf_status gf_module_clipper(gf_ctx *ctx, const gf_footprint *foot, const gf_lambert proj[2], gf_table *t, int64_t begin, int64_t end)
+{
+    (void)proj;
+    GF_TRY(check_ctx(ctx));
+    GF_TRY(row_range(t, begin, end));
+    if (!foot) return fail(GF_E_INVALID, "null footprint");
+    GF_CUDA(gfk::launch_clipper(*foot, *t, begin, end, ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_module_fixedfeh(gf_ctx *ctx, const gf_fixedfeh_config *cfg, gf_table *t, int64_t begin, int64_t end)
+{
+    GF_TRY(check_ctx(ctx));
+    GF_TRY(row_range(t, begin, end));
+    if (!cfg) return fail(GF_E_INVALID, "null config");
+    GF_CUDA(gfk::launch_fixedfeh(*cfg, *t, begin, end, ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_module_bond2010(gf_ctx *ctx, const gf_bond2010_config *cfg, gf_table *t, int64_t begin, int64_t end)
+{
+    GF_TRY(check_ctx(ctx));
+    GF_TRY(row_range(t, begin, end));
+    if (!cfg) return fail(GF_E_INVALID, "null config");
+    if (!ctx->d_rng) return fail(GF_E_STATE, "gf_rng_init must precede gf_module_bond2010");
+    int64_t n = end - begin;
+    if ((n + 255) / 256 > ctx->rng_nstreams) return fail(GF_E_INVALID, "more than 256 rows per stream");
+    GF_CUDA(gfk::launch_bond2010(*cfg, ctx->d_rng, ctx->rng_nstreams, *t, begin, end, ctx->stream));
+    return GF_OK;
+}
+
+struct gf_photometry {
+    gfk::PhotTables tab;
+    float *d_colors = nullptr;
+    uint8_t *d_eflags = nullptr;
+};
+
+struct gf_photoerr {
+    gfk::PerrTables tab;
+    double *d_mag = nullptr, *d_sigma = nullptr;
+};
+
+gf_status gf_photometry_create(gf_ctx *ctx, const gf_photometry_config *cfg, gf_photometry **out)
+{
+    GF_TRY(check_ctx(ctx));
+    if (!cfg || !out || cfg->nbands < 2 || cfg->nbands > GF_MAX_BANDS || cfg->bidx < 0 || cfg->bidx >= cfg->nbands ||
+        cfg->nFeH < 1 || cfg->nMr < 1 || !cfg->colors || !cfg->eflags)
+        return fail(GF_E_INVALID, "invalid photometry configuration");
+    gf_photometry *p = new gf_photometry();
+    size_t n = (size_t)(cfg->nbands - 1) * cfg->nMr * cfg->nFeH;
+    if (dev_alloc(&p->d_colors, n) != GF_OK || dev_alloc(&p->d_eflags, n) != GF_OK) {
+        dev_free(p->d_colors); dev_free(p->d_eflags); delete p;
+        return fail(GF_E_OOM, "photometry tables");
+    }
+    cudaMemcpy(p->d_colors, cfg->colors, 4 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(p->d_eflags, cfg->eflags, n, cudaMemcpyHostToDevice);
+    gfk::PhotTables &T = p->tab;
+    T.nbands = cfg->nbands; T.bidx = cfg->bidx; T.nFeH = cfg->nFeH; T.nMr = cfg->nMr;
+    for (int i = 0; i < GF_MAX_BANDS; i++) T.reddening[i] = cfg->reddening[i];
+    T.tcFeH[0] = cfg->tcFeH[0]; T.tcFeH[1] = cfg->tcFeH[1]; T.tcMr[0] = cfg->tcMr[0]; T.tcMr[1] = cfg->tcMr[1];
+    T.colors = p->d_colors; T.eflags = p->d_eflags; T.comp_mask = cfg->comp_mask;
+    *out = p;
+    return GF_OK;
+}
+
+gf_status gf_photometry_destroy(gf_photometry *p)
+{
+    if (!p) return GF_OK;
+    dev_free(p->d_colors); dev_free(p->d_eflags);
+    delete p;
+    return GF_OK;
+}
+
+gf_status gf_module_photometry(gf_ctx *ctx, const gf_photometry *p, gf_table *t, int64_t begin, int64_t end)
+{
+    GF_TRY(check_ctx(ctx));
+    GF_TRY(row_range(t, begin, end));
+    if (!p) return fail(GF_E_INVALID, "null photometry");
+    if (t->nbands < p->tab.nbands) return fail(GF_E_INVALID, "table has fewer bands than the photometric system");
+    GF_CUDA(gfk::launch_photometry(p->tab, *t, begin, end, ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_photoerr_create(gf_ctx *ctx, const gf_photoerr_config *cfg, gf_photoerr **out)
+{
+    GF_TRY(check_ctx(ctx));
+    if (!cfg || !out || cfg->nbands < 1 || cfg->nbands > GF_MAX_BANDS || cfg->nknots < 2 || !cfg->mag || !cfg->sigma)
+        return fail(GF_E_INVALID, "invalid photometric error configuration");
+    gf_photoerr *p = new gf_photoerr();
+    size_t n = (size_t)cfg->nbands * cfg->nknots;
+    if (dev_alloc(&p->d_mag, n) != GF_OK || dev_alloc(&p->d_sigma, n) != GF_OK) {
+        dev_free(p->d_mag); dev_free(p->d_sigma); delete p;
+        return fail(GF_E_OOM, "photometric error tables");
+    }
+    cudaMemcpy(p->d_mag, cfg->mag, 8 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(p->d_sigma, cfg->sigma, 8 * n, cudaMemcpyHostToDevice);
+    p->tab.nbands = cfg->nbands; p->tab.nknots = cfg->nknots; p->tab.mag = p->d_mag; p->tab.sigma = p->d_sigma;
+    p->tab.seed = cfg->seed;
+    *out = p;
+    return GF_OK;
+}
+
+gf_status gf_photoerr_destroy(gf_photoerr *p)
+{
+    if (!p) return GF_OK;
+    dev_free(p->d_mag); dev_free(p->d_sigma);
+    delete p;
+    return GF_OK;
+}
+
+gf_status gf_module_photoerrors(gf_ctx *ctx, const gf_photoerr *p, int64_t row_offset, gf_table *t, int64_t begin, int64_t end)
+{
+    GF_TRY(check_ctx(ctx));
+    GF_TRY(row_range(t, begin, end));
+    if (!p) return fail(GF_E_INVALID, "null photometric errors");
+    if (t->nbands < p->tab.nbands) return fail(GF_E_INVALID, "table has fewer bands than the error model");
+    GF_CUDA(gfk::launch_photoerrors(p->tab, row_offset, *t, begin, end, ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_module_vel2pm(gf_ctx *ctx, const gf_vel2pm_config *cfg, gf_table *t, int64_t begin, int64_t end)
+{
+    GF_TRY(check_ctx(ctx));
+    GF_TRY(row_range(t, begin, end));
+    if (!cfg) return fail(GF_E_INVALID, "null config");
+    GF_CUDA(gfk::launch_vel2pm(*cfg, *t, begin, end, ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_module_gal2other(gf_ctx *ctx, int32_t coordsys, gf_table *t, int64_t begin, int64_t end)
+{
+    GF_TRY(check_ctx(ctx));
+    GF_TRY(row_range(t, begin, end));
+    GF_CUDA(gfk::launch_gal2other(coordsys, *t, begin, end, ctx->stream));
+    return GF_OK;
+}
+
+/* ---------------- the catalog path ---------------- */
+
+gf_status gf_catalog_run(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, void *user, gf_catalog_stats *stats)
+{
+    GF_TRY(check_ctx(ctx));
+    if (!job || job->nmodels <= 0 || job->nmodels > GF_MAX_MODELS || job->capacity <= 0) return fail(GF_E_INVALID, "invalid job");
+    if (job->capacity > (int64_t)256 * GF_MAX_STREAMS) return fail(GF_E_INVALID, "capacity above 256 rows x 65536 streams");
+    gf_catalog_stats local;
+    gf_catalog_stats &S = stats ? *stats : local;
+    memset(&S, 0, sizeof(S));
+    S.norm = 1.f;
+    if (job->nstreams > 0) GF_TRY(gf_rng_init(ctx, job->seed48, job->nstreams));
+    if (!ctx->d_rng) return fail(GF_E_STATE, "no random streams: set nstreams or call gf_rng_init");
+    /* models in component order (os_skygen.cpp:392-399) */
+    std::vector<gf_model_config> models(job->models, job->models + job->nmodels);
+    std::stable_sort(models.begin(), models.end(), [](const gf_model_config &a, const gf_model_config &b) { return a.comp < b.comp; });
+    gf_skygen *sky = nullptr;
+    GF_TRY(gf_skygen_create(ctx, &job->sky, job->pixels, job->npixels, job->beam_ammin, &job->ext, models.data(),
+                            (int32_t)models.size(), &sky));
+    struct Guard {
+        gf_ctx *ctx; gf_skygen *sky; gf_table t; gf_photometry *ph; gf_photoerr *pe;
+        ~Guard() { gf_table_free(ctx, &t); gf_photometry_destroy(ph); gf_photoerr_destroy(pe); gf_skygen_destroy(sky); }
+    } g{ctx, sky, gf_table(), nullptr, nullptr};
+    memset(&g.t, 0, sizeof(g.t));
+    /* integrate every model first (os_skygen.cpp:875-880) */
+    double total = 0;
+    for (int i = 0; i < (int)models.size(); i++) {
+        GF_TRY(gf_skygen_integrate(sky, i, &S.expected[i], &S.expected_covered[i], nullptr));
+        total += S.expected_covered[i];
+    }
+    if (job->sky.nstars != 0.f) {
+        /* forced normalisation (os_skygen.cpp:886-901) */
+        double norm = job->sky.nstars / total;
+        S.norm = (float)norm;
+        for (int i = 0; i < (int)models.size(); i++) GF_TRY(gf_skygen_set_norm(sky, i, (float)norm));
+    }
+    GF_TRY(gf_table_alloc(ctx, job->capacity, job->nbands, &g.t));
+    if (job->phot) GF_TRY(gf_photometry_create(ctx, job->phot, &g.ph));
+    if (job->perr) GF_TRY(gf_photoerr_create(ctx, job->perr, &g.pe));
+    int64_t row_offset = 0;
+    for (int i = 0; i < (int)models.size(); i++) {
+        int32_t done = 0;
+        while (!done) {
+            int64_t ngen = 0;
+            GF_TRY(gf_skygen_draw(sky, i, &g.t, &ngen, &done));
+            S.generated[i] += ngen;
+            const int64_t n = g.t.size;
+            if (n == 0) continue;
+            S.batches++;
+            /* the module chain in pipeline order (pipeline.h:75-88) */
+            if (job->foot) GF_TRY(gf_module_clipper(ctx, job->foot, job->sky.proj, &g.t, 0, n));
+            if (job->feh) GF_TRY(gf_module_fixedfeh(ctx, job->feh, &g.t, 0, n));
+            if (job->kin) GF_TRY(gf_module_bond2010(ctx, job->kin, &g.t, 0, n));
+            if (g.ph) GF_TRY(gf_module_photometry(ctx, g.ph, &g.t, 0, n));
+            if (g.pe) GF_TRY(gf_module_photoerrors(ctx, g.pe, row_offset, &g.t, 0, n));
+            if (job->v2pm) GF_TRY(gf_module_vel2pm(ctx, job->v2pm, &g.t, 0, n));
+            if (job->gal2other) GF_TRY(gf_module_gal2other(ctx, job->gal2other, &g.t, 0, n));
+            GF_CUDA(cudaStreamSynchronize(ctx->stream));
+            S.stored[i] += n;
+            if (cb && cb(user, models[i].comp, &g.t, row_offset) != 0) return fail(GF_E_STATE, "stopped by the batch callback");
+            row_offset += n;
+        }
+    }
+    return GF_OK;
+}
+
+}  /* extern "C" */

@@ -1,0 +1,560 @@
+/*
+ * gf_host.cpp -- host setup of the catalog generator: binning, luminosity
+ * functions, model frames and normalisation, stream seeding, footprint
+ * pixelisation and photometric-system tables.
+ */
+#include "gf_host.h"
+#include "gf_math.h"
+#include "gf_safeprimes.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <dlfcn.h>
+#include <map>
+#include <mutex>
+
+namespace gfh {
+
+/* ---------------- random number seeding ---------------- */
+
+void MT19937::seed(uint32_t s)
+{
+    mt[0] = s;
+    for (int i = 1; i < 624; i++) mt[i] = 1812433253u * (mt[i - 1] ^ (mt[i - 1] >> 30)) + (uint32_t)i;
+    mti = 624;
+}
+
+uint32_t MT19937::next()
+{
+    static const uint32_t mag01[2] = {0u, 0x9908b0dfu};
+    if (mti >= 624) {
+        int k;
+        for (k = 0; k < 624 - 397; k++) {
+            uint32_t y = (mt[k] & 0x80000000u) | (mt[k + 1] & 0x7fffffffu);
+            mt[k] = mt[k + 397] ^ (y >> 1) ^ mag01[y & 1u];
+        }
+        for (; k < 623; k++) {
+            uint32_t y = (mt[k] & 0x80000000u) | (mt[k + 1] & 0x7fffffffu);
+            mt[k] = mt[k + (397 - 624)] ^ (y >> 1) ^ mag01[y & 1u];
+        }
+        uint32_t y = (mt[623] & 0x80000000u) | (mt[0] & 0x7fffffffu);
+        mt[623] = mt[396] ^ (y >> 1) ^ mag01[y & 1u];
+        mti = 0;
+    }
+    uint32_t y = mt[mti++];
+    y ^= (y >> 11);
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= (y >> 18);
+    return y;
+}
+
+void seed_streams(uint32_t seed48, int nstreams, const uint32_t *mult, uint32_t *state)
+{
+    Rand48 r;
+    r.srand(seed48);
+    for (int i = 0; i < nstreams; i++) {
+        uint32_t prime = mult[i];
+        state[i] = prime;
+        /* (int)(drand48() * prime): x86 cvttsd2si gives INT_MIN out of range */
+        double t = r.drand() * prime;
+        int32_t c = (t >= 2147483648.0) ? INT32_MIN : (int32_t)t;
+        state[nstreams + i] = (uint32_t)c;
+        state[2 * nstreams + i] = r.lrand();
+    }
+}
+
+static std::string library_dir()
+{
+    Dl_info info;
+    if (dladdr((void *)&library_dir, &info) && info.dli_fname) {
+        std::string p(info.dli_fname);
+        size_t s = p.rfind('/');
+        if (s != std::string::npos) return p.substr(0, s);
+    }
+    return ".";
+}
+
+const std::vector<uint32_t> &multipliers()
+{
+    static std::vector<uint32_t> tab;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        tab.resize(GF_MAX_STREAMS);
+        std::string fn = library_dir() + "/safeprimes_65536.bin";
+        FILE *f = fopen(fn.c_str(), "rb");
+        bool ok = false;
+        if (f) {
+            ok = fread(tab.data(), 4, GF_MAX_STREAMS, f) == GF_MAX_STREAMS;
+            fclose(f);
+        }
+        if (!ok) gf_safeprimes_generate(tab.data(), GF_MAX_STREAMS);
+    });
+    return tab;
+}
+
+/* ---------------- model setup ---------------- */
+
+/* gsl_interp_linear evaluation with linear extrapolation (spline.cpp:59-65) */
+double interp_linear(const std::vector<double> &xa, const std::vector<double> &ya, double x)
+{
+    int n = (int)xa.size();
+    int lo = 0, hi = n - 1;
+    while (hi > lo + 1) {
+        int mid = (hi + lo) / 2;
+        if (xa[mid] > x) hi = mid; else lo = mid;
+    }
+    double dx = xa[lo + 1] - xa[lo];
+    if (dx > 0.0) return ya[lo] + (x - xa[lo]) / dx * (ya[lo + 1] - ya[lo]);
+    return 0.0;
+}
+
+namespace {
+
+void reset_absmag(SkyModel &m, float M0, float M1, float dM)
+{
+    /* os_skygen.cpp:401-407 */
+    m.M0 = M0; m.M1 = M1; m.dM = dM;
+    m.nM = (int)round((m.M1 - m.M0) / m.dM);
+    m.M1 -= 0.5 * m.dM;
+}
+
+float rho_host(const SkyModel &m, float x, float y, float z)
+{
+    float vx = x + m.T[0], vy = y + m.T[1], vz = z + m.T[2];
+    float wx = m.M[0] * vx + m.M[1] * vy + m.M[2] * vz;
+    float wy = m.M[3] * vx + m.M[4] * vy + m.M[5] * vz;
+    float wz = m.M[6] * vx + m.M[7] * vy + m.M[8] * vz;
+    if (m.type == GF_MODEL_EXP_DISK) {
+        float r2 = wx * wx + wy * wy;
+        if (m.r_cut2 != 0.f && r2 + wz * wz > m.r_cut2) return 0.f;
+        return m.f * gfm::expf_(-sqrtf(r2) / m.l - fabsf(wz) / m.h);
+    }
+    float DSq = wx * wx + wy * wy + wz * wz;
+    if (m.rmaxSq != 0.f && (DSq < m.rminSq || DSq >= m.rmaxSq)) return 0.f;
+    float ty = wy / m.ba, tz = wz / m.ca;
+    float rSq = wx * wx + ty * ty + tz * tz;
+    return m.f * gfm::powf_(rSq, 0.5f * m.n);
+}
+
+}  // namespace
+
+bool setup_models(const gf_skygen_config &cfg, int npixels, const gf_model_config *mc, int nmodels,
+                  std::vector<HostModel> &out, std::string &err)
+{
+    if (cfg.dm <= 0.f || !(cfg.m1 > cfg.m0) || !(cfg.M1 > cfg.M0)) { err = "invalid magnitude binning"; return false; }
+    if (cfg.nthreads <= 0 || cfg.nthreads > 65536) { err = "nthreads must be in [1, 65536]"; return false; }
+    SkyModel base;
+    memset(&base, 0, sizeof(base));
+    /* load_skyPixelizationConfig (os_skygen.cpp:409-430) */
+    base.dmin = cfg.dmin;
+    base.dmax = cfg.dmax;
+    base.dm = cfg.dm;
+    base.m1 = cfg.m1;
+    reset_absmag(base, cfg.M0, cfg.M1, cfg.dm);
+    base.nm = (int)round((cfg.m1 - cfg.m0) / cfg.dm);
+    base.m0 = cfg.m0 + 0.5 * cfg.dm;
+    base.npixels = npixels;
+    base.nthreads = cfg.nthreads;
+    base.norm = 1.f;
+
+    out.clear();
+    for (int i = 0; i < nmodels; i++) {
+        const gf_model_config &c = mc[i];
+        HostModel hm;
+        SkyModel &m = hm.m;
+        m = base;
+        if (c.type != GF_MODEL_EXP_DISK && c.type != GF_MODEL_POWER_LAW_ELLIPSOID) { err = "unknown model type"; return false; }
+        if (c.comp < 0 || c.comp > 31) { err = "component id must be in [0, 31]"; return false; }
+        m.type = c.type;
+        m.comp = c.comp;
+        /* frame: load_transform (transform.cpp:345-388) */
+        if (c.frame == GF_FRAME_EXPLICIT) {
+            for (int k = 0; k < 3; k++) m.T[k] = (float)c.T[k];
+            for (int k = 0; k < 9; k++) m.M[k] = (float)c.M[k];
+        } else {
+            double Rg = c.Rg, z0 = c.z0;
+            double sina = -z0 / Rg, cosa = sqrt(1 - sina * sina);
+            /* centre of the galplane frame in galactic cartesian coordinates (transform.cpp:194-213) */
+            double cx = cosa * 0.0 - sina * 0.0, cz = sina * 0.0 + cosa * 0.0;
+            double ctr[3] = {Rg - cx, -0.0, cz};
+            for (int k = 0; k < 3; k++) m.T[k] = (float)-ctr[k];
+            double R[9] = {-cosa, 0, sina, 0, -1, 0, sina, 0, cosa};
+            for (int k = 0; k < 9; k++) m.M[k] = (float)R[k];
+        }
+        if (c.type == GF_MODEL_EXP_DISK) {
+            if (!(c.l > 0) || !(c.h > 0)) { err = "exponential disk needs l > 0 and h > 0"; return false; }
+            m.l = (float)c.l;
+            m.h = (float)c.h;
+        } else {
+            m.n = (float)c.n;
+            m.ba = (float)c.ba;
+            m.ca = (float)c.ca;
+        }
+        m.r_cut2 = 0.f;
+        m.rminSq = m.rmaxSq = 0.f;
+        /* luminosity function (cux.cpp:336-384) */
+        if (c.lf_n <= 0 || !c.lf_M || !c.lf_phi) {
+            hm.lf.assign(2, 1.f);
+            m.lf_x0 = -100.f;
+            m.lf_inv_dx = (float)(1. / (100. - -100.));
+        } else {
+            if (c.lf_n < 2) { err = "LF needs at least 2 knots"; return false; }
+            std::vector<double> X, Y;
+            X.push_back(-123);
+            Y.push_back(0.f);
+            for (int k = 0; k < c.lf_n; k++) { X.push_back(c.lf_M[k]); Y.push_back(c.lf_phi[k]); }
+            double xrange = X.back() - X[1];
+            X[0] = X[1] - 1e-5 * xrange;
+            X.push_back(X.back() + 1e-5 * xrange);
+            Y.push_back(0.f);
+            const int nsamp = 1024;
+            double X0 = X[0], X1 = X.back(), dX = (X1 - X0) / (nsamp - 1);
+            hm.lf.resize(nsamp);
+            for (int k = 0; k < nsamp; k++) hm.lf[k] = (float)interp_linear(X, Y, X0 + k * dX);
+            m.lf_x0 = (float)X0;
+            m.lf_inv_dx = (float)(1. / dX);
+        }
+        m.lf_n = (int)hm.lf.size();
+        /* normalisation at the LF sampling point (model_lib.h:68-95) */
+        const double d2r = 0.01745329251994329576923691;
+        float lfl = (float)c.lf_l, lfb = (float)c.lf_b, lfD = (float)c.lf_D;
+        double rl = lfl * d2r, rb = lfb * d2r;
+        float cl = (float)gfm::cos_d(rl), cb = (float)gfm::cos_d(rb), sl = (float)gfm::sin_d(rl), sb = (float)gfm::sin_d(rb);
+        float px = lfD * cl * cb, py = lfD * sl * cb, pz = lfD * sb;
+        m.f = 1.f;
+        float norm = rho_host(m, px, py, pz);
+        if (!(norm != 0.f && std::isnormal(norm))) { err = "density is zero at the LF sampling point"; return false; }
+        float f0 = (float)c.f;
+        m.f = f0 / norm;
+        if (c.type == GF_MODEL_EXP_DISK) {
+            float rc = (float)c.rcut;
+            m.r_cut2 = rc * rc;
+        } else {
+            float rmin = (float)c.rmin, rmax = (float)c.rmax;
+            m.rminSq = rmin * rmin;
+            m.rmaxSq = rmax * rmax;
+        }
+        /* absolute magnitude hint from the LF range (skyconfig_impl.h:257-263, model_lib.h:97-112) */
+        float hM0 = m.M0, hM1 = m.M1 + 0.5 * m.dM;
+        float X0 = m.lf_x0;
+        float X1 = double(m.lf_n - 1) / m.lf_inv_dx + X0;
+        bool hint = false;
+        if (X0 > hM0) { hint = true; hM0 = X0; }
+        if (X1 < hM1) { hint = true; hM1 = X1; }
+        if (hint) reset_absmag(m, hM0, hM1, m.dM);
+        if (m.nm <= 0 || m.nM <= 0) { err = "empty magnitude grid"; return false; }
+        if ((long long)m.nm * m.nM > 0x3fffffff) { err = "magnitude grid too large"; return false; }
+        if (m.nm > 32767 || m.nM > 32767) { err = "magnitude grid dimension above 32767"; return false; }
+        m.lf = nullptr;
+        out.push_back(hm);
+    }
+    return true;
+}
+
+}  // namespace gfh
+
+/* ------------------------------------------------------------------ */
+/* Host-only C entry points                                            */
+/* ------------------------------------------------------------------ */
+extern "C" {
+
+uint32_t gf_rng_seed48_from_cli_seed(uint64_t seed)
+{
+    /* rng_gsl_t(seed) with gsl_rng_default = mt19937 (gpu.h:362-382), then
+     * (uint32_t)(seeder.uniform() * (1 << 24)) (cux.cpp:409) */
+    gfh::MT19937 mt;
+    uint32_t s = (uint32_t)seed;
+    if (s == 0) s = 4357;       /* GSL's mt19937 treats seed 0 as 4357 */
+    mt.seed(s);
+    double u = mt.next() / 4294967296.0;
+    float fu = (float)u;
+    return (uint32_t)(fu * (float)(1 << 24));
+}
+
+void gf_mt19937_outputs(uint32_t seed, int n, uint32_t *out)
+{
+    gfh::MT19937 mt;
+    mt.seed(seed);
+    for (int i = 0; i < n; i++) out[i] = mt.next();
+}
+
+void gf_rng_seed_host(uint32_t seed48, int32_t nstreams, uint32_t *state)
+{
+    gfh::seed_streams(seed48, nstreams, gfh::multipliers().data(), state);
+}
+
+int gf_multipliers(uint32_t *out, int32_t n)
+{
+    if (n < 0 || n > GF_MAX_STREAMS) return GF_E_INVALID;
+    const std::vector<uint32_t> &m = gfh::multipliers();
+    std::copy(m.begin(), m.begin() + n, out);
+    return GF_OK;
+}
+
+}  /* extern "C" */
+
+/* ------------------------------------------------------------------ */
+/* Footprint pixelisation (host setup; the reference builds its pixel  */
+/* list from GPC polygons, os_skygen.cpp:130-283 -- here footprints    */
+/* are analytic and coverage is measured by supersampling).            */
+/* ------------------------------------------------------------------ */
+namespace {
+
+const double kD2R = 0.01745329251994329576923691;
+
+/* lambert deprojection in double precision (skygen.h:131-146 with double x, y) */
+void deproject_d(const gf_lambert &p, double x, double y, double &l, double &b)
+{
+    double r2 = x * x + y * y;
+    if (r2 == 0.) { b = p.b0; l = 0.; return; }
+    double ir = 1. / sqrt(r2);
+    double sc = 1. / ir * sqrt(1. - 0.25 * r2);
+    double cc = 1. - 0.5 * r2;
+    b = gfm::asin_d(cc * (double)p.sb + y * sc * (double)p.cb * ir);
+    l = p.l0 + gfm::atan2_d(x * sc, (double)p.cb * cc / ir - y * (double)p.sb * sc);
+}
+
+struct FootTest {
+    gf_footprint f;
+    double cb0, sb0, l0, cosr;
+    explicit FootTest(const gf_footprint &ff) : f(ff)
+    {
+        l0 = f.a * kD2R;
+        cb0 = gfm::cos_d(f.b * kD2R);
+        sb0 = gfm::sin_d(f.b * kD2R);
+        cosr = gfm::cos_d(f.c * kD2R);
+    }
+    /* is the point (l, b) (radians), seen in projection `proj` at (x, y), inside? */
+    bool inside(int proj, double x, double y, double l, double b) const
+    {
+        switch (f.kind) {
+        case GF_FOOT_ALL: return true;
+        case GF_FOOT_LAMBERT_RECT: return proj == f.proj && x >= f.a && x < f.b && y >= f.c && y < f.d;
+        case GF_FOOT_CAP: return gfm::sin_d(b) * sb0 + gfm::cos_d(b) * cb0 * gfm::cos_d(l - l0) >= cosr;
+        case GF_FOOT_LATCUT: return fabs(b) > f.a * kD2R;
+        }
+        return false;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+gf_status gf_lambert_init(double l0_deg, double b0_deg, gf_lambert *p)
+{
+    /* lambert::init (skygen.h:115-120) */
+    p->l0 = l0_deg * kD2R;
+    p->b0 = b0_deg * kD2R;
+    p->cl = (float)gfm::cos_d(p->l0);
+    p->cb = (float)gfm::cos_d(p->b0);
+    p->sl = (float)gfm::sin_d(p->l0);
+    p->sb = (float)gfm::sin_d(p->b0);
+    return GF_OK;
+}
+
+/* Pixelise a footprint on the Lambert grids of the two hemispheres (cell side
+ * dx_deg in degrees of Lambert coordinate, grid anchored at the pole).  A point
+ * belongs to the north grid when b >= 0 and to the south grid otherwise.
+ * beam_ammin (nullable) receives the minimum screen extinction over each cell.
+ * Call with pixels == NULL to count. */
+gf_status gf_footprint_pixelize(const gf_footprint *foot, double dx_deg, const gf_lambert proj[2],
+                                const gf_extinction *ext, gf_pencil_beam *pixels, float *beam_ammin,
+                                int64_t max_pixels, int64_t *npixels)
+{
+    if (!foot || !npixels || !(dx_deg > 0)) return GF_E_INVALID;
+    const double dx = dx_deg * kD2R;
+    const float dxf = (float)dx;
+    FootTest ft(*foot);
+    const int SS = 16;                       /* supersampling per axis at the boundary */
+    int64_t n = 0;
+    for (int h = 0; h < 2; h++) {
+        /* bounding box of the footprint in this hemisphere's Lambert plane */
+        double xmin = -M_SQRT2, xmax = M_SQRT2, ymin = -M_SQRT2, ymax = M_SQRT2;
+        if (foot->kind == GF_FOOT_LAMBERT_RECT) {
+            if (foot->proj != h) continue;
+            xmin = foot->a; xmax = foot->b; ymin = foot->c; ymax = foot->d;
+        } else if (foot->kind == GF_FOOT_LATCUT) {
+            double R = 2 * gfm::sin_d(0.5 * (90. - foot->a) * kD2R);
+            xmin = ymin = -R; xmax = ymax = R;
+        } else if (foot->kind == GF_FOOT_CAP) {
+            /* project boundary samples of the cap that fall in this hemisphere */
+            double bx0 = 1e9, bx1 = -1e9, by0 = 1e9, by1 = -1e9;
+            bool any = false;
+            const gf_lambert &p = proj[h];
+            double lc = foot->a * kD2R, bc = foot->b * kD2R, r = foot->c * kD2R;
+            for (int k = 0; k <= 4096; k++) {
+                double rr = (k == 4096) ? 0.0 : r;
+                double az = 2 * M_PI * k / 4096.0;
+                /* destination point at distance rr, azimuth az from (lc, bc) */
+                double sb = gfm::sin_d(bc) * gfm::cos_d(rr) + gfm::cos_d(bc) * gfm::sin_d(rr) * gfm::cos_d(az);
+                double b = gfm::asin_d(sb);
+                double l = lc + gfm::atan2_d(gfm::sin_d(az) * gfm::sin_d(rr) * gfm::cos_d(bc), gfm::cos_d(rr) - gfm::sin_d(bc) * sb);
+                if ((h == 0) != (b >= 0)) continue;
+                /* forward Lambert projection about the pole */
+                double cll0 = gfm::cos_d(l - p.l0);
+                double sll0 = gfm::sin_d(l - p.l0);
+                double kp = 1.414213562373095 * sqrt(1. / (1. + (double)p.sb * gfm::sin_d(b) + (double)p.cb * gfm::cos_d(b) * cll0));
+                double x = kp * gfm::cos_d(b) * sll0;
+                double y = kp * ((double)p.cb * gfm::sin_d(b) - (double)p.sb * gfm::cos_d(b) * cll0);
+                bx0 = std::min(bx0, x); bx1 = std::max(bx1, x); by0 = std::min(by0, y); by1 = std::max(by1, y);
+                any = true;
+            }
+            /* the cap may reach the equator: then its hemisphere part is bounded by the cap samples and the rim */
+            if (!any) continue;
+            double pad = 2 * dx;
+            xmin = std::max(-M_SQRT2, bx0 - pad); xmax = std::min(M_SQRT2, bx1 + pad);
+            ymin = std::max(-M_SQRT2, by0 - pad); ymax = std::min(M_SQRT2, by1 + pad);
+            /* a cap containing the pole covers the origin */
+            double dpole = (h == 0 ? 90. - foot->b : 90. + foot->b);
+            if (dpole <= foot->c) { xmin = std::min(xmin, -dx); xmax = std::max(xmax, dx); ymin = std::min(ymin, -dx); ymax = std::max(ymax, dx); }
+        }
+        long long i0 = (long long)floor(xmin / dx), i1 = (long long)ceil(xmax / dx);
+        long long j0 = (long long)floor(ymin / dx), j1 = (long long)ceil(ymax / dx);
+        for (long long i = i0; i < i1; i++) {
+            for (long long j = j0; j < j1; j++) {
+                double cx0 = i * dx, cy0 = j * dx;
+                /* reject cells entirely outside the Lambert disk of the hemisphere */
+                double nx = std::max(cx0, std::min(0.0, cx0 + dx)), ny = std::max(cy0, std::min(0.0, cy0 + dx));
+                double rmin2 = nx * nx + ny * ny;
+                if (rmin2 > 2.0) continue;
+                /* coverage: corners + centre decide interior cells; boundary cells are supersampled */
+                int in_corners = 0;
+                for (int c = 0; c < 5; c++) {
+                    double px = (c == 4) ? cx0 + 0.5 * dx : cx0 + (c & 1) * dx * 0.999999;
+                    double py = (c == 4) ? cy0 + 0.5 * dx : cy0 + ((c >> 1) & 1) * dx * 0.999999;
+                    if (px * px + py * py > 2.0) continue;
+                    double l, b;
+                    deproject_d(proj[h], px, py, l, b);
+                    bool hemi = (h == 0) ? (b >= 0) : (b < 0);
+                    if (hemi && ft.inside(h, px, py, l, b)) in_corners++;
+                }
+                double cov;
+                if (in_corners == 5 && foot->kind != GF_FOOT_CAP && foot->kind != GF_FOOT_LATCUT) {
+                    cov = 1.0;
+                } else {
+                    int cnt = 0;
+                    for (int a = 0; a < SS; a++) {
+                        for (int bq = 0; bq < SS; bq++) {
+                            double px = cx0 + (a + 0.5) * dx / SS, py = cy0 + (bq + 0.5) * dx / SS;
+                            if (px * px + py * py > 2.0) continue;
+                            double l, b;
+                            deproject_d(proj[h], px, py, l, b);
+                            bool hemi = (h == 0) ? (b >= 0) : (b < 0);
+                            if (hemi && ft.inside(h, px, py, l, b)) cnt++;
+                        }
+                    }
+                    if (foot->kind == GF_FOOT_LAMBERT_RECT) {
+                        /* exact overlap of two rectangles */
+                        double ox = std::max(0.0, std::min(cx0 + dx, foot->b) - std::max(cx0, foot->a));
+                        double oy = std::max(0.0, std::min(cy0 + dx, foot->d) - std::max(cy0, foot->c));
+                        cov = ox * oy / (dx * dx);
+                    } else {
+                        cov = (double)cnt / (SS * SS);
+                    }
+                }
+                if (cov <= 0.0) continue;
+                if (pixels && n < max_pixels) {
+                    double X = cx0 + 0.5 * dx, Y = cy0 + 0.5 * dx;
+                    double l, b;
+                    deproject_d(proj[h], X, Y, l, b);
+                    gf_pencil_beam &pb = pixels[n];
+                    memset(&pb, 0, sizeof(pb));
+                    pb.cl = (float)gfm::cos_d(l); pb.cb = (float)gfm::cos_d(b);
+                    pb.sl = (float)gfm::sin_d(l); pb.sb = (float)gfm::sin_d(b);
+                    pb.coveredFraction = (float)cov;
+                    pb.dx = dxf;
+                    pb.dA = dxf * dxf;
+                    pb.projIdx = h;
+                    pb.X = (float)X;
+                    pb.Y = (float)Y;
+                    pb.extIdx = (int32_t)n;
+                    if (beam_ammin) {
+                        float am = 0.f;
+                        if (ext && ext->kind == GF_EXT_SCREEN_CSCB) {
+                            double sbmax = 1.0 - 0.5 * rmin2;          /* sin|b| at the cell point nearest the pole */
+                            am = (float)(ext->A0 / sbmax * (1.0 - 1e-6));
+                        }
+                        beam_ammin[n] = am;
+                    }
+                }
+                n++;
+            }
+        }
+    }
+    *npixels = n;
+    return (pixels && n > max_pixels) ? GF_E_INVALID : GF_OK;
+}
+
+/* Resample a photometric system table (rows Mr, FeH, c_1..c_ncolors) to the
+ * colour/extrapolation-flag grids of os_photometry::construct
+ * (photometry_host.cpp:233-344).  Call with colors == NULL to get the sizes. */
+gf_status gf_photometry_build(const double *rows, int32_t nrows, int32_t ncolors, double dFeH, double dMr,
+                              float *colors, uint8_t *eflags, int32_t *nFeH_out, int32_t *nMr_out,
+                              float tcFeH[2], float tcMr[2])
+{
+    if (!rows || nrows < 1 || ncolors < 1 || ncolors >= GF_MAX_BANDS || !(dFeH > 0) || !(dMr > 0)) return GF_E_INVALID;
+    const int w = 2 + ncolors;
+    std::map<double, std::vector<const double *>> v;
+    for (int r = 0; r < nrows; r++) v[rows[(size_t)r * w + 1]].push_back(rows + (size_t)r * w);
+    double FeH0 = v.begin()->first, FeH1 = v.rbegin()->first;
+    double Mr0 = rows[0], Mr1 = rows[0];
+    for (int r = 0; r < nrows; r++) { Mr0 = std::min(Mr0, rows[(size_t)r * w]); Mr1 = std::max(Mr1, rows[(size_t)r * w]); }
+    int nFeH = (int)((FeH1 - FeH0) / dFeH + 1);
+    int nMr = (int)((Mr1 - Mr0) / dMr + 1);
+    /* texcoord_from_range(0, n, x0, x0 + n*dx) in float (cux.cpp:389-397) */
+    auto tc_range = [](float imgx, float imgy, float x, float y, float out[2]) {
+        out[0] = (-imgy * x + imgx * y) / (imgx - imgy);
+        out[1] = (imgx - imgy) / (x - y);
+    };
+    tc_range(0, (float)nFeH, (float)FeH0, (float)(FeH0 + nFeH * dFeH), tcFeH);
+    tc_range(0, (float)nMr, (float)Mr0, (float)(Mr0 + nMr * dMr), tcMr);
+    *nFeH_out = nFeH;
+    *nMr_out = nMr;
+    if (!colors) return GF_OK;
+    /* per-FeH colour(Mr) knots, sorted by Mr */
+    struct Line { double FeH; std::vector<double> Mr; std::vector<std::vector<double>> c; double Mrmin, Mrmax; };
+    std::vector<Line> lines;
+    std::vector<double> vFeH;
+    for (auto &kv : v) {
+        Line L;
+        L.FeH = kv.first;
+        std::vector<const double *> rs = kv.second;
+        std::stable_sort(rs.begin(), rs.end(), [](const double *a, const double *b) { return a[0] < b[0]; });
+        L.c.resize(ncolors);
+        for (const double *r : rs) {
+            L.Mr.push_back(r[0]);
+            for (int ic = 0; ic < ncolors; ic++) L.c[ic].push_back(r[2 + ic]);
+        }
+        L.Mrmin = L.Mr.front();
+        L.Mrmax = L.Mr.back();
+        lines.push_back(L);
+        vFeH.push_back(L.FeH);
+    }
+    std::vector<double> vcol(lines.size()), vecol(lines.size());
+    for (int ic = 0; ic < ncolors; ic++) {
+        for (int m = 0; m < nMr; m++) {
+            double Mr = Mr0 + m * dMr;
+            for (size_t k = 0; k < lines.size(); k++) {
+                const Line &L = lines[k];
+                vcol[k] = L.Mr.size() > 1 ? gfh::interp_linear(L.Mr, L.c[ic], Mr) : L.c[ic][0];
+                vecol[k] = (L.Mrmin > Mr || Mr > L.Mrmax) ? 1.0 : 0.0;
+            }
+            for (int f = 0; f < nFeH; f++) {
+                double FeH = FeH0 + f * dFeH;
+                float color = (float)(lines.size() > 1 ? gfh::interp_linear(vFeH, vcol, FeH) : vcol[0]);
+                double ef = lines.size() > 1 ? gfh::interp_linear(vFeH, vecol, FeH) : vecol[0];
+                bool eflag = vFeH.front() > FeH || FeH > vFeH.back() || ef != 0.;
+                size_t off = ((size_t)ic * nMr + m) * nFeH + f;
+                colors[off] = color;
+                eflags[off] = eflag ? 1 : 0;
+            }
+        }
+    }
+    return GF_OK;
+}
+
+}  /* extern "C" */

@@ -1,0 +1,84 @@
+/*
+ * gf_launch.h -- launch descriptors of the sm_100a kernels, used by the host
+ * orchestration (gf_api.cu).
+ */
+#pragma once
+#include <cuda_runtime.h>
+#include "gf_internal.h"
+
+namespace gfk {
+
+struct LaunchCrawl {
+    SkyModel m;
+    SkyGeom g;
+    CrawlState st;
+    uint32_t *rng;
+    int32_t rng_nstreams;
+    JumpTables jt;
+    int32_t stream_begin, stream_end;
+    const int64_t *limits;
+    StarRecord *rec;
+    int64_t rec_capacity;
+    unsigned long long *rec_count;
+    unsigned long long *err;
+    double *counts, *countsCovered, *per_pixel;
+    int32_t pix_base;
+};
+
+struct LaunchPlace {
+    SkyModel m;
+    SkyGeom g;
+    const StarRecord *rec;
+    int64_t n;
+    double *lb;
+    int32_t *projIdx;
+    float *projXY, *DM, *absmag, *XYZ, *Am, *AmInf;
+    int32_t *hidden;
+    uint64_t *key;
+    unsigned long long *nvis;
+};
+
+struct LaunchSort {
+    int64_t n, nvisible;
+    uint64_t *key_in, *key_out;
+    uint32_t *idx_in, *idx_out;
+    void *temp;
+    size_t temp_bytes;
+    const double *lb;
+    const int32_t *projIdx;
+    const float *projXY, *DM, *absmag, *XYZ, *Am, *AmInf;
+    int32_t comp;
+    gf_table out;
+};
+
+int sm_count();
+cudaError_t launch_crawl(const LaunchCrawl &L, int draw, cudaStream_t s);
+cudaError_t launch_place(const LaunchPlace &L, cudaStream_t s);
+cudaError_t sort_temp_bytes(int64_t n, size_t *bytes);
+cudaError_t launch_sort_gather(const LaunchSort &L, cudaStream_t s);
+cudaError_t launch_jump_tables(const uint32_t *mult, int n, uint64_t *lo, uint64_t *hi, cudaStream_t s);
+
+/* modules (gf_modules.cu) */
+cudaError_t launch_clipper(const gf_footprint &foot, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
+cudaError_t launch_fixedfeh(const gf_fixedfeh_config &c, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
+cudaError_t launch_bond2010(const gf_bond2010_config &c, uint32_t *rng, int32_t rng_nstreams, gf_table t,
+                            int64_t begin, int64_t end, cudaStream_t s);
+struct PhotTables {
+    int32_t nbands, bidx, nFeH, nMr;
+    float reddening[GF_MAX_BANDS];
+    float tcFeH[2], tcMr[2];
+    const float *colors;          /* device */
+    const uint8_t *eflags;        /* device */
+    uint32_t comp_mask;
+};
+cudaError_t launch_photometry(const PhotTables &c, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
+struct PerrTables {
+    int32_t nbands, nknots;
+    const double *mag, *sigma;    /* device */
+    uint64_t seed;
+};
+cudaError_t launch_photoerrors(const PerrTables &c, int64_t row_offset, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
+cudaError_t launch_vel2pm(const gf_vel2pm_config &c, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
+cudaError_t launch_gal2other(int32_t coordsys, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
+
+}  // namespace gfk

@@ -1,0 +1,412 @@
+/*
+ * gf_modules.cu -- sm_100a kernels of the postprocessing modules on the
+ * catalog path.  Each restates the reference kernel named beside it with the
+ * portable math of gf_math.h; expressions keep the reference's types and
+ * evaluation order (the library is compiled with -fmad=false).
+ *
+ *   clipper_kernel     os_clipper::process (src/skygen/os_skygen.cpp:999-1044), analytic footprints
+ *   fixedfeh_kernel    os_fixedFeH_kernel (src/modules/fixedFeH_gpu.cu.h:34-50)
+ *   bond2010_kernel    os_Bond2010_kernel (src/modules/Bond2010_gpu.cu.h:81-218)
+ *   photometry_kernel  os_photometry_kernel (src/modules/photometry_gpu.cu.h:87-174)
+ *   photoerr_kernel    os_photometricErrors::process (photometricErrors_host.cpp:112-131)
+ *   vel2pm_kernel      os_vel2pm_kernel (src/modules/vel2pm_gpu.cu.h:253-301)
+ *   gal2other_kernel   os_gal2other_kernel (src/modules/gal2other_gpu.cu.h:62-96)
+ */
+#include "gf_launch.h"
+#include "gf_math.h"
+#include "gf_rng.h"
+
+namespace gfk {
+
+static const double D2R = 0.01745329251994329576923691;
+
+static int grid_for(int64_t n, int threads)
+{
+    int64_t b = (n + threads - 1) / threads;
+    int64_t cap = (int64_t)sm_count() * 32;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+/* ---------------- clipper ---------------- */
+__global__ void clipper_kernel(gf_footprint foot, gf_table t, int64_t begin, int64_t end)
+{
+    const int64_t P = t.capacity;
+    for (int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < end; row += (int64_t)gridDim.x * blockDim.x) {
+        if (t.hidden[row]) continue;
+        bool in = true;
+        if (foot.kind == GF_FOOT_LAMBERT_RECT) {
+            float x = t.projXY[row], y = t.projXY[P + row];
+            in = t.projIdx[row] == foot.proj && x >= foot.a && x < foot.b && y >= foot.c && y < foot.d;
+        } else if (foot.kind == GF_FOOT_CAP) {
+            double l = t.lb[row] * D2R, b = t.lb[P + row] * D2R;
+            double l0 = foot.a * D2R, b0 = foot.b * D2R;
+            double cosd = gfm::sin_d(b) * gfm::sin_d(b0) + gfm::cos_d(b) * gfm::cos_d(b0) * gfm::cos_d(l - l0);
+            in = cosd >= gfm::cos_d(foot.c * D2R);
+        } else if (foot.kind == GF_FOOT_LATCUT) {
+            in = fabs(t.lb[P + row]) > foot.a;
+        }
+        if (!in) t.hidden[row] = 1;
+    }
+}
+
+cudaError_t launch_clipper(const gf_footprint &foot, gf_table t, int64_t begin, int64_t end, cudaStream_t s)
+{
+    if (end <= begin || foot.kind == GF_FOOT_ALL) return cudaSuccess;
+    clipper_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(foot, t, begin, end);
+    return cudaGetLastError();
+}
+
+/* ---------------- fixedFeH ---------------- */
+__global__ void fixedfeh_kernel(gf_fixedfeh_config c, gf_table t, int64_t begin, int64_t end)
+{
+    for (int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < end; row += (int64_t)gridDim.x * blockDim.x) {
+        if (t.hidden[row]) continue;
+        int cmp = t.comp[row];
+        if (!((c.comp_mask >> cmp) & 1u)) continue;
+        t.FeH[row] = c.FeH;
+    }
+}
+
+cudaError_t launch_fixedfeh(const gf_fixedfeh_config &c, gf_table t, int64_t begin, int64_t end, cudaStream_t s)
+{
+    if (end <= begin) return cudaSuccess;
+    fixedfeh_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(c, t, begin, end);
+    return cudaGetLastError();
+}
+
+/* ---------------- Bond2010 kinematics ---------------- */
+__device__ __forceinline__ float modfun(float Rsquared, float Z, const float *val)
+{
+    /* a + b|Z|^c + d R^e, Bond2010_gpu.cu.h:106-110 */
+    return val[0] + val[1] * gfm::powf_(fabsf(Z), val[2]) + val[3] * gfm::powf_(Rsquared, (float)(0.5 * (double)val[4]));
+}
+
+__device__ __forceinline__ void trivar_gauss(float y[3], const float sg[6], gfr::Mwc &rng)
+{
+    /* Cholesky draw, Bond2010_gpu.cu.h:81-103 */
+    float s11 = sg[0], s12 = sg[1], s13 = sg[2], s22 = sg[3], s23 = sg[4], s33 = sg[5];
+    float b10 = s12;      float b11 = s22 * s22;
+    float b20 = s13;      float b21 = s23;      float b22 = s33 * s33;
+    float a00 = s11; float oneDivA00 = 1.0f / a00;
+    float a10 = b10 * oneDivA00;
+    float a11 = sqrtf(b11 - a10 * a10);
+    float a20 = b20 * oneDivA00;
+    float a21 = (b21 - a20 * a10) / a11;
+    float a22 = sqrtf(b22 - a20 * a20 - a21 * a21);
+    float z0 = rng.gaussian(1.0f);
+    float z1 = rng.gaussian(1.0f);
+    float z2 = rng.gaussian(1.0f);
+    y[0] += a00 * z0;
+    y[1] += a10 * z0 + a11 * z1;
+    y[2] += a20 * z0 + a21 * z1 + a22 * z2;
+}
+
+__device__ __forceinline__ void draw_moments(float v[3], float R2, float Z, const gf_vmoments &mo, bool disk, gfr::Mwc &rng)
+{
+    for (int i = 0; i < 3; i++) v[i] = modfun(R2, Z, mo.m[i]);
+    if (disk && v[1] > 0.f) v[1] = 0.f;
+    float sg[6];
+    for (int i = 0; i < 6; i++) sg[i] = modfun(R2, Z, mo.ss[i]);
+    trivar_gauss(v, sg, rng);
+}
+
+__global__ void __launch_bounds__(128) bond2010_kernel(const gf_bond2010_config par, uint32_t *rng, int32_t NS, gf_table t,
+                                                        int64_t begin, int64_t end, int64_t nchunks)
+{
+    const int64_t P = t.capacity;
+    int64_t th = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (th >= nchunks) return;
+    gfr::Mwc r;
+    r.a = rng[th]; r.c = rng[NS + th]; r.x = rng[2 * NS + th];
+    int64_t rb = begin + 256 * th, re = begin + 256 * (th + 1);
+    if (re > end) re = end;
+    for (int64_t row = rb; row < re; row++) {
+        if (t.hidden[row]) continue;
+        const int cmp = t.comp[row];
+        float vx = t.XYZ[row] + par.T[0], vy = t.XYZ[P + row] + par.T[1], vz = t.XYZ[2 * P + row] + par.T[2];
+        float wx = par.M[0] * vx + par.M[1] * vy + par.M[2] * vz;
+        float wy = par.M[3] * vx + par.M[4] * vy + par.M[5] * vz;
+        float wz = par.M[6] * vx + par.M[7] * vy + par.M[8] * vz;
+        const float R2 = (float)(1e-6 * (double)(wx * wx + wy * wy));
+        const float Z = (float)(1e-3 * (double)wz);
+        float v[3];
+        if (((par.comp_thin | par.comp_thick) >> cmp) & 1u) {
+            float pu = r.uniform();
+            const gf_vmoments &disk = pu < par.fk ? par.disk_1 : par.disk_2;
+            draw_moments(v, R2, Z, disk, true, r);
+        } else if ((par.comp_halo >> cmp) & 1u) {
+            draw_moments(v, R2, Z, par.halo, false, r);
+            float invR = 1.f / sqrtf(R2 + Z * Z);
+            float cosa = sqrtf(R2) * invR;
+            float sina = Z * invR;
+            float vR = cosa * v[0] - sina * v[1];
+            float vZ = sina * v[0] + cosa * v[1];
+            v[0] = vR;
+            v[1] = v[2];
+            v[2] = vZ;
+        } else {
+            continue;
+        }
+        t.vcyl[row] = v[0];
+        t.vcyl[P + row] = v[1];
+        t.vcyl[2 * P + row] = v[2];
+    }
+    rng[NS + th] = r.c;
+    rng[2 * NS + th] = r.x;
+}
+
+cudaError_t launch_bond2010(const gf_bond2010_config &c, uint32_t *rng, int32_t NS, gf_table t, int64_t begin, int64_t end,
+                            cudaStream_t s)
+{
+    if (end <= begin) return cudaSuccess;
+    int64_t n = end - begin;
+    int64_t nchunks = n / 256 + (n % 256 ? 1 : 0);
+    if (nchunks > NS) return cudaErrorInvalidValue;
+    bond2010_kernel<<<(int)((nchunks + 127) / 128), 128, 0, s>>>(c, rng, NS, t, begin, end, nchunks);
+    return cudaGetLastError();
+}
+
+/* ---------------- photometry ---------------- */
+__device__ __forceinline__ uint32_t brev(uint32_t a) { return __brev(a); }
+
+__global__ void __launch_bounds__(256) photometry_kernel(PhotTables lt, gf_table t, int64_t begin, int64_t end)
+{
+    const int64_t P = t.capacity;
+    const int ncolors = lt.nbands - 1;
+    for (int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < end; row += (int64_t)gridDim.x * blockDim.x) {
+        if (t.hidden[row]) continue;
+        int cmp = t.comp[row];
+        if (!((lt.comp_mask >> cmp) & 1u)) continue;
+        float fFeH = t.FeH[row];
+        float fMr = t.absmag[row];
+        uint32_t flag = 0;
+        float c[GF_MAX_BANDS];
+        if (!(fMr >= 99.999f)) {
+            float xi = (fFeH - lt.tcFeH[0]) * lt.tcFeH[1] + 0.5f;
+            float yi = (fMr - lt.tcMr[0]) * lt.tcMr[1] + 0.5f;
+            if (xi < 0.f) xi = 0.f; else if (xi >= (float)lt.nFeH) xi = (float)lt.nFeH - 1;
+            if (yi < 0.f) yi = 0.f; else if (yi >= (float)lt.nMr) yi = (float)lt.nMr - 1;
+            uint32_t i = (uint32_t)xi, j = (uint32_t)yi;
+            for (int ic = 0; ic < ncolors; ic++) {
+                size_t off = ((size_t)ic * lt.nMr + j) * lt.nFeH + i;
+                c[ic] = lt.colors[off];
+                flag |= ((uint32_t)(lt.eflags[off] != 0)) << ic;
+            }
+            for (int b = 0; b <= ncolors; b++) {
+                float M = fMr;
+                if (b < lt.bidx) { for (int q = b; q != lt.bidx; q++) M += c[q]; }
+                if (b > lt.bidx) { for (int q = lt.bidx; q != b; q++) M -= c[q]; }
+                t.mags[b * P + row] = gfm::exp10f_(-0.4f * M);
+            }
+        }
+        bool fl = false;
+        for (int q = lt.bidx - 1; q >= 0; q--) {
+            fl = fl || (flag & (1u << q));
+            flag |= ((uint32_t)fl) << q;
+        }
+        fl = false;
+        for (int q = lt.bidx; q < ncolors; q++) {
+            fl = fl || (flag & (1u << q));
+            flag |= ((uint32_t)fl) << q << 1;
+        }
+        flag &= ~(1u << lt.bidx);
+        flag = brev(flag);
+        flag >>= (8 * sizeof(flag) - ncolors - 1);
+        t.photoflags[row] = (int32_t)flag;
+        float dm = t.DM[row];
+        float Am0 = t.Am[row];
+        for (int b = 0; b <= ncolors; b++) {
+            float Msys = -2.5f * gfm::log10f_(t.mags[b * P + row]);
+            float msys = dm + Msys;
+            float Am = Am0 * lt.reddening[b];
+            t.mags[b * P + row] = msys + Am;
+        }
+    }
+}
+
+cudaError_t launch_photometry(const PhotTables &c, gf_table t, int64_t begin, int64_t end, cudaStream_t s)
+{
+    if (end <= begin) return cudaSuccess;
+    photometry_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(c, t, begin, end);
+    return cudaGetLastError();
+}
+
+/* ---------------- photometric errors ---------------- */
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw 2011) */
+__device__ __forceinline__ void philox(uint32_t ctr[4], uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, ctr[0]), lo0 = 0xD2511F53u * ctr[0];
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, ctr[2]), lo1 = 0xCD9E8D57u * ctr[2];
+        uint32_t n0 = hi1 ^ ctr[1] ^ k0;
+        uint32_t n2 = hi0 ^ ctr[3] ^ k1;
+        ctr[0] = n0; ctr[1] = lo1; ctr[2] = n2; ctr[3] = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+}
+
+__device__ __forceinline__ double error_normal(uint64_t seed, uint64_t row, uint32_t band)
+{
+    uint32_t ctr[4] = {(uint32_t)row, (uint32_t)(row >> 32), band, 0x67616c66u};
+    philox(ctr, (uint32_t)seed, (uint32_t)(seed >> 32));
+    uint64_t a = ((uint64_t)ctr[0] << 21) ^ (ctr[1] >> 11);
+    uint64_t b = ((uint64_t)ctr[2] << 21) ^ (ctr[3] >> 11);
+    double u1 = ((double)(a & ((1ull << 53) - 1)) + 1.0) * 0x1p-53;
+    double u2 = (double)(b & ((1ull << 53) - 1)) * 0x1p-53;
+    double r = sqrt(-2.0 * gfm::log_d(u1));
+    return r * gfm::cos_d(6.283185307179586 * u2);
+}
+
+__device__ __forceinline__ double linear_eval(const double *xa, const double *ya, int n, double x)
+{
+    int ilo = 0, ihi = n - 1;
+    while (ihi > ilo + 1) {
+        int i = (ihi + ilo) / 2;
+        if (xa[i] > x) ihi = i; else ilo = i;
+    }
+    double x_lo = xa[ilo], x_hi = xa[ilo + 1];
+    double y_lo = ya[ilo], y_hi = ya[ilo + 1];
+    double dx = x_hi - x_lo;
+    if (dx > 0.0) return y_lo + (x - x_lo) / dx * (y_hi - y_lo);
+    return 0.0;
+}
+
+__global__ void __launch_bounds__(256) photoerr_kernel(PerrTables c, int64_t row_offset, gf_table t, int64_t begin, int64_t end)
+{
+    const int64_t P = t.capacity;
+    for (int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < end; row += (int64_t)gridDim.x * blockDim.x) {
+        if (t.hidden[row]) continue;
+        for (int b = 0; b < c.nbands; b++) {
+            float mag = t.mags[b * P + row];
+            float sigma = (float)linear_eval(c.mag + (size_t)b * c.nknots, c.sigma + (size_t)b * c.nknots, c.nknots, mag);
+            double z = error_normal(c.seed, (uint64_t)(row_offset + row), (uint32_t)b);
+            t.obsmags[b * P + row] = mag + (float)((double)sigma * z);
+        }
+    }
+}
+
+cudaError_t launch_photoerrors(const PerrTables &c, int64_t row_offset, gf_table t, int64_t begin, int64_t end, cudaStream_t s)
+{
+    if (end <= begin) return cudaSuccess;
+    photoerr_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(c, row_offset, t, begin, end);
+    return cudaGetLastError();
+}
+
+/* ---------------- vel2pm ---------------- */
+__device__ __forceinline__ void vel_xyz2lbr(float &vl, float &vb, float &vr, const float vx, const float vy, const float vz,
+                                            const float l, const float b)
+{
+    float cl = gfm::cosf_(l), sl = gfm::sinf_(l), cb = gfm::cosf_(b), sb = gfm::sinf_(b);
+    float tmp;
+    vl = -vx * sl + vy * cl;
+    tmp = vx * cl + vy * sl;
+    vr = cb * tmp + vz * sb;
+    vb = -sb * tmp + vz * cb;
+}
+
+__device__ __forceinline__ void transform_pm(float &vlout, float &vbout, float l, float b, float vl, float vb,
+                                             const double ce, const double se, const double l0)
+{
+    double cb = gfm::cos_d((double)b);
+    double sb = gfm::sin_d((double)b);
+    double cl = gfm::cos_d((double)l - l0);
+    double sl = gfm::sin_d((double)l - l0);
+    double tmp1 = cb * se - ce * sb * sl;
+    double tmp2 = ce * sb - cb * se * sl;
+    double tmp4 = cb * cl;
+    double tmp3 = sb * se + cb * ce * sl;
+    if (fabs(tmp3) > 0.9999999) {
+        vlout = vbout = 999.99f;
+    } else {
+        double denom1 = 1. / (tmp4 * tmp4 + tmp2 * tmp2);
+        double cd = sqrt(1. - tmp3 * tmp3);
+        vl = (float)((double)vl / cb);
+        vlout = (float)((-ce * cl * (double)vb + cb * tmp1 * (double)vl) * denom1);
+        vbout = (float)((tmp1 * (double)vb + cb * ce * cl * (double)vl) / cd);
+        vlout = (float)((double)vlout * cd);
+    }
+}
+
+__global__ void __launch_bounds__(256) vel2pm_kernel(gf_vel2pm_config par, gf_table t, int64_t begin, int64_t end)
+{
+    const int64_t P = t.capacity;
+    const double ce = 0.88998740217659689, se = 0.45598511375586859, l0 = D2R * 32.932;
+    for (int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < end; row += (int64_t)gridDim.x * blockDim.x) {
+        if (t.hidden[row]) continue;
+        float l = 0.017453292519943295769f * (float)t.lb[row];
+        float b = 0.017453292519943295769f * (float)t.lb[P + row];
+        float X = par.Rg - t.XYZ[row];
+        float Y = -t.XYZ[P + row];
+        float Z = t.XYZ[2 * P + row];
+        float vx = t.vcyl[row], vy = t.vcyl[P + row], vz = t.vcyl[2 * P + row];
+        /* vel_cyl2xyz */
+        float rho = sqrtf(X * X + Y * Y);
+        float cphi = X / rho;
+        float sphi = Y / rho;
+        float px = -sphi * vy + cphi * vx;
+        float py = cphi * vy + sphi * vx;
+        float pz = vz;
+        px -= par.u0;
+        py -= par.v0 + par.vLSR;
+        pz -= par.w0;
+        float ix = -px, iy = -py, iz = pz;
+        vel_xyz2lbr(px, py, pz, ix, iy, iz, l, b);
+        float D = sqrtf((8000.f - X) * (8000.f - X) + Y * Y + Z * Z);
+        px = (float)((double)px / (4.74 * (double)D * 1e-3));
+        py = (float)((double)py / (4.74 * (double)D * 1e-3));
+        if (par.coordsys == 1) {
+            float ivl = px, ivb = py;
+            transform_pm(px, py, l, b, ivl, ivb, ce, se, l0);
+        } else if (par.coordsys != 0) {
+            px = py = pz = -9.99f;
+        }
+        t.pm[row] = px;
+        t.pm[P + row] = py;
+        t.pm[2 * P + row] = pz;
+    }
+}
+
+cudaError_t launch_vel2pm(const gf_vel2pm_config &c, gf_table t, int64_t begin, int64_t end, cudaStream_t s)
+{
+    if (end <= begin) return cudaSuccess;
+    vel2pm_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(c, t, begin, end);
+    return cudaGetLastError();
+}
+
+/* ---------------- gal2other ---------------- */
+__global__ void __launch_bounds__(256) gal2other_kernel(int32_t coordsys, gf_table t, int64_t begin, int64_t end)
+{
+    const int64_t P = t.capacity;
+    const double angp = D2R * 192.859508333, l0 = D2R * 32.932;
+    const double ce = 0.88998740217659689, se = 0.45598511375586859;
+    const double pi2 = 2 * 3.14159265358979323846264338;
+    for (int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < end; row += (int64_t)gridDim.x * blockDim.x) {
+        if (t.hidden[row]) continue;
+        double lx = t.lb[row] * D2R, ly = t.lb[P + row] * D2R;
+        double rx, ry;
+        if (coordsys == 1) {
+            const double cb = gfm::cos_d(ly), sb = gfm::sin_d(ly);
+            const double cl = gfm::cos_d(lx - l0), sl = gfm::sin_d(lx - l0);
+            rx = gfm::atan2_d(cb * cl, sb * ce - cb * se * sl) + angp;
+            ry = gfm::asin_d(cb * ce * sl + sb * se);
+            while (rx < 0.) rx += pi2;
+            while (rx >= pi2) rx -= pi2;
+        } else {
+            rx = ry = -9999.;
+        }
+        t.radec[row] = rx / D2R;
+        t.radec[P + row] = ry / D2R;
+    }
+}
+
+cudaError_t launch_gal2other(int32_t coordsys, gf_table t, int64_t begin, int64_t end, cudaStream_t s)
+{
+    if (end <= begin) return cudaSuccess;
+    gal2other_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(coordsys, t, begin, end);
+    return cudaGetLastError();
+}
+
+}  // namespace gfk

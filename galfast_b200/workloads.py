@@ -1,0 +1,347 @@
+"""Synthetic catalog workloads with the shapes of galfast's configurations.
+
+Everything here is host-side setup: footprints are pixelised by the native
+library (gf_footprint_pixelize), the luminosity function, colour loci and
+error curves are generated from closed-form expressions with fixed seeds.
+
+    config 1  10x10 deg patch at the north galactic pole, 0.25 deg pixels, 15 < r < 21
+    config 2  whole sky with |b| > 10 deg, 0.1 deg pixels, 14 < r < 22, 16M-star batches
+    config 4  4096 pencil beams (batched form), per-request model variants and seeds
+"""
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import _abi as A
+
+D2R = math.pi / 180.0
+
+# SDSS-like extinction-to-reddening ratios A_b / E(B-V) for u g r i z
+SDSS_AE = np.array([5.155, 3.793, 2.751, 2.086, 1.479])
+SDSS_M5 = np.array([22.5, 23.0, 23.0, 23.0, 22.2])
+
+
+def lf_table():
+    """Mr from 3 to 15 in 0.1 mag steps, log10 phi rising linearly from -3.5 to -2.0."""
+    M = np.round(np.arange(121) * 0.1 + 3.0, 10)
+    phi = 10.0 ** (-3.5 + 1.5 * (M - 3.0) / 12.0)
+    return M.astype(np.float64), phi.astype(np.float64)
+
+
+def color_coefficients(nbands=5, seed=20240611):
+    """Cubic colour-magnitude relations c_i(Mr) = sum_k a_ik t^k, t = (Mr - 9)/6, for
+    the colours band_i - band_(i+1); base colours of a main-sequence-like locus."""
+    rng = np.random.default_rng(seed)
+    a = rng.normal(0.0, 0.1, size=(nbands - 1, 4))
+    base = np.array([1.2, 0.45, 0.18, 0.08, 0.05][: nbands - 1])
+    slope = np.array([0.6, 0.55, 0.35, 0.2, 0.15][: nbands - 1])
+    a[:, 0] += base
+    a[:, 1] += slope
+    return a
+
+
+def photosys_rows(coef, Mr0=3.0, Mr1=15.0, dMr=0.01, FeHs=(-3.0, 1.0)):
+    """A photosys-format table (Mr, FeH, c_1..c_n) sampled every dMr."""
+    n = int(round((Mr1 - Mr0) / dMr)) + 1
+    Mr = np.round(Mr0 + np.arange(n) * dMr, 10)
+    t = (Mr - 9.0) / 6.0
+    cols = np.stack([sum(c[k] * t ** k for k in range(4)) for c in coef], axis=1)
+    rows = []
+    for feh in FeHs:
+        rows.append(np.column_stack([Mr, np.full(n, feh), cols]))
+    return np.ascontiguousarray(np.concatenate(rows), dtype=np.float64)
+
+
+def error_knots(m5):
+    """sigma(m) = 0.005 + 0.04 * 10^(0.4 (m - m5)) tabulated from 0 to 40 in 0.01 steps,
+    accumulating m exactly as os_modelPhotoErrors::construct (photometricErrors_host.cpp:236-240)."""
+    mags = []
+    m = 0.0
+    while m < 40:
+        mags.append(m)
+        m += 0.01
+    mags = np.array(mags)
+    sig = np.stack([0.005 + 0.04 * 10.0 ** (0.4 * (mags - mm)) for mm in m5])
+    return np.ascontiguousarray(np.tile(mags, (len(m5), 1))), np.ascontiguousarray(sig)
+
+
+def galplane_frame(Rg=8000.0, z0=25.0):
+    """The galplane rotation and translation as float32 (transform.cpp:122-135, 194-213)."""
+    sina = -z0 / Rg
+    cosa = math.sqrt(1 - sina * sina)
+    M = np.array([-cosa, 0, sina, 0, -1, 0, sina, 0, cosa], dtype=np.float32)
+    T = np.array([-Rg, 0.0, -0.0], dtype=np.float32)
+    return M, T
+
+
+def bond2010_config(disk_sigma=(35.0, 25.0, 20.0), halo_sigma=(140.0, 100.0, 95.0), Rg=8000.0, z0=25.0):
+    """Bond et al. (2010) kinematics with constant dispersions (Bond2010_host.cpp:142-227 layout)."""
+    cfg = A.Bond2010Config()
+    cfg.comp_thin, cfg.comp_thick, cfg.comp_halo = 1, 2, 4
+    fk = 3.0
+    cfg.fk = fk / (1.0 + fk)
+
+    def setv(arr, vals):
+        for i in range(5):
+            arr[i] = vals[i] if i < len(vals) else 0.0
+
+    d1 = cfg.disk_1
+    setv(d1.m[0], [0])                       # vR
+    setv(d1.m[1], [-194, 19.2, 1.25])        # vPhi
+    setv(d1.m[2], [0])                       # vZ
+    setv(d1.ss[0], [disk_sigma[0]])          # sigmaR
+    setv(d1.ss[1], [0])
+    setv(d1.ss[2], [0])
+    setv(d1.ss[3], [disk_sigma[1]])          # sigmaPhi1
+    setv(d1.ss[4], [0])
+    setv(d1.ss[5], [disk_sigma[2]])          # sigmaZ
+    C.memmove(C.addressof(cfg.disk_2), C.addressof(cfg.disk_1), C.sizeof(A.VMoments))
+    cfg.disk_2.m[1][0] += 34.0               # DeltavPhi
+    setv(cfg.disk_2.ss[3], [disk_sigma[1]])  # sigmaPhi2
+    h = cfg.halo
+    for i in range(3):
+        setv(h.m[i], [0])
+    setv(h.ss[0], [halo_sigma[0]])           # HsigmaR
+    setv(h.ss[1], [0])
+    setv(h.ss[2], [0])
+    setv(h.ss[3], [halo_sigma[2]])           # HsigmaTh
+    setv(h.ss[4], [0])
+    setv(h.ss[5], [halo_sigma[1]])           # HsigmaPhi
+    M, T = galplane_frame(Rg, z0)
+    for i in range(9):
+        cfg.M[i] = float(M[i])
+    for i in range(3):
+        cfg.T[i] = float(T[i])
+    return cfg
+
+
+@dataclass
+class Workload:
+    """One catalog request: generator inputs plus the module chain."""
+    sky: A.SkygenConfig
+    pixels: np.ndarray                 # structured bytes of gf_pencil_beam
+    npixels: int
+    ammin: np.ndarray
+    ext: A.Extinction
+    models: List[A.ModelConfig]
+    seed48: int
+    nstreams: int
+    capacity: int
+    nbands: int
+    foot: Optional[A.Footprint] = None
+    feh: Optional[A.FixedFeHConfig] = None
+    kin: Optional[A.Bond2010Config] = None
+    phot: Optional[A.PhotometryConfig] = None
+    perr: Optional[A.PhotoerrConfig] = None
+    v2pm: Optional[A.Vel2pmConfig] = None
+    gal2other: int = 0
+    keep: list = field(default_factory=list)   # keeps ctypes buffers alive
+
+    def pixel_array(self):
+        return (A.PencilBeam * self.npixels).from_buffer(self.pixels)
+
+    def job(self, lib_types):
+        """The gf_job structure (lib_types: galfast_b200.Job)."""
+        j = lib_types()
+        j.sky = self.sky
+        j.pixels = C.cast(self.pixel_array(), C.POINTER(A.PencilBeam))
+        j.npixels = self.npixels
+        j.beam_ammin = self.ammin.ctypes.data_as(C.POINTER(C.c_float))
+        j.ext = self.ext
+        marr = (A.ModelConfig * len(self.models))(*self.models)
+        self.keep.append(marr)
+        j.models = C.cast(marr, C.POINTER(A.ModelConfig))
+        j.nmodels = len(self.models)
+        j.seed48 = self.seed48
+        j.nstreams = self.nstreams
+        j.capacity = self.capacity
+        j.nbands = self.nbands
+        for name in ("foot", "feh", "kin", "phot", "perr", "v2pm"):
+            v = getattr(self, name)
+            if v is not None:
+                setattr(j, name, C.pointer(v))
+        j.gal2other = self.gal2other
+        return j
+
+
+def _lambert_pair(lib):
+    pr = (A.Lambert * 2)()
+    lib.gf_lambert_init(C.c_double(90.0), C.c_double(90.0), C.byref(pr[0]))
+    lib.gf_lambert_init(C.c_double(270.0), C.c_double(-90.0), C.byref(pr[1]))
+    return pr
+
+
+def pixelize(lib, foot, dx_deg, proj, ext):
+    n = C.c_int64(0)
+    st = lib.gf_footprint_pixelize(C.byref(foot), C.c_double(dx_deg), proj, C.byref(ext), None, None, C.c_int64(0), C.byref(n))
+    if st != 0:
+        raise RuntimeError("pixelisation failed")
+    npix = n.value
+    buf = bytearray(C.sizeof(A.PencilBeam) * max(npix, 1))
+    pix = (A.PencilBeam * max(npix, 1)).from_buffer(buf)
+    ammin = np.zeros(max(npix, 1), dtype=np.float32)
+    st = lib.gf_footprint_pixelize(C.byref(foot), C.c_double(dx_deg), proj, C.byref(ext), pix,
+                                   ammin.ctypes.data_as(C.POINTER(C.c_float)), C.c_int64(npix), C.byref(n))
+    if st != 0:
+        raise RuntimeError("pixelisation failed")
+    return buf, npix, ammin
+
+
+def _model(kind, comp, f, Rg, z0, lfM, lfphi, **kw):
+    m = A.ModelConfig()
+    m.type = kind
+    m.comp = comp
+    m.f = f
+    m.frame = A.GF_FRAME_GALPLANE
+    m.Rg, m.z0 = Rg, z0
+    m.lf_M = lfM.ctypes.data_as(C.POINTER(C.c_double))
+    m.lf_phi = lfphi.ctypes.data_as(C.POINTER(C.c_double))
+    m.lf_n = len(lfM)
+    m.ba = 1.0
+    m.ca = 1.0
+    for k, v in kw.items():
+        setattr(m, k, v)
+    return m
+
+
+def build_workload(lib, *, foot, dx_deg, m0, m1, nthreads=7680, seed48=42, capacity=1 << 20,
+                   thin_h=300.0, halo_q=0.64, with_modules=True, nbands=5, m5=SDSS_M5,
+                   perr_seed=0x5eed, M0=3.0, M1=15.0, ext_E=0.02):
+    proj = _lambert_pair(lib)
+    ext = A.Extinction()
+    ext.kind = A.GF_EXT_SCREEN_CSCB if ext_E > 0 else A.GF_EXT_NONE
+    ext.A0 = float(SDSS_AE[2] * ext_E)
+    pixbuf, npix, ammin = pixelize(lib, foot, dx_deg, proj, ext)
+    sky = A.SkygenConfig()
+    sky.m0, sky.m1, sky.dm = m0, m1, 0.05
+    sky.M0, sky.M1 = M0, M1
+    sky.dmin = sky.dmax = 0.0
+    sky.nthreads = nthreads
+    sky.nstars = 0.0
+    sky.proj[0], sky.proj[1] = proj[0], proj[1]
+    lfM, lfphi = lf_table()
+    Rg, z0 = 8000.0, 25.0
+    models = [
+        _model(A.GF_MODEL_EXP_DISK, 0, 1.0, Rg, z0, lfM, lfphi, l=2600.0, h=thin_h),
+        _model(A.GF_MODEL_EXP_DISK, 1, 0.12, Rg, z0, lfM, lfphi, l=3600.0, h=900.0),
+        _model(A.GF_MODEL_POWER_LAW_ELLIPSOID, 2, 0.005, Rg, z0, lfM, lfphi, n=-2.77, ca=halo_q, ba=1.0),
+    ]
+    w = Workload(sky=sky, pixels=pixbuf, npixels=npix, ammin=ammin, ext=ext, models=models, seed48=seed48,
+                 nstreams=65536, capacity=capacity, nbands=nbands if with_modules else 0, foot=foot)
+    w.keep += [lfM, lfphi, proj]
+    if not with_modules:
+        return w
+    feh = A.FixedFeHConfig()
+    feh.FeH = 0.0
+    feh.comp_mask = 0xFFFFFFFF
+    w.feh = feh
+    w.kin = bond2010_config(Rg=Rg, z0=z0)
+    coef = color_coefficients(nbands)
+    rows = photosys_rows(coef)
+    nFeH = C.c_int32(0)
+    nMr = C.c_int32(0)
+    tcF = (C.c_float * 2)()
+    tcM = (C.c_float * 2)()
+    st = lib.gf_photometry_build(rows.ctypes.data_as(C.POINTER(C.c_double)), rows.shape[0], nbands - 1,
+                                 C.c_double(0.01), C.c_double(0.01), None, None, C.byref(nFeH), C.byref(nMr), tcF, tcM)
+    if st != 0:
+        raise RuntimeError("photometry build failed")
+    ncol = nbands - 1
+    colors = np.zeros(ncol * nMr.value * nFeH.value, dtype=np.float32)
+    eflags = np.zeros(ncol * nMr.value * nFeH.value, dtype=np.uint8)
+    lib.gf_photometry_build(rows.ctypes.data_as(C.POINTER(C.c_double)), rows.shape[0], ncol,
+                            C.c_double(0.01), C.c_double(0.01), colors.ctypes.data_as(C.POINTER(C.c_float)),
+                            eflags.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(nFeH), C.byref(nMr), tcF, tcM)
+    ph = A.PhotometryConfig()
+    ph.nbands = nbands
+    ph.bidx = 2
+    red = np.ones(A.GF_MAX_BANDS, dtype=np.float32)
+    red[:nbands] = (SDSS_AE[:nbands] / SDSS_AE[2]).astype(np.float32) if nbands <= 5 else 1.0
+    for i in range(A.GF_MAX_BANDS):
+        ph.reddening[i] = float(red[i])
+    ph.nFeH, ph.nMr = nFeH.value, nMr.value
+    ph.tcFeH[0], ph.tcFeH[1] = tcF[0], tcF[1]
+    ph.tcMr[0], ph.tcMr[1] = tcM[0], tcM[1]
+    ph.colors = colors.ctypes.data_as(C.POINTER(C.c_float))
+    ph.eflags = eflags.ctypes.data_as(C.POINTER(C.c_uint8))
+    ph.comp_mask = 0xFFFFFFFF
+    w.phot = ph
+    mk, sg = error_knots(list(m5)[:nbands])
+    pe = A.PhotoerrConfig()
+    pe.nbands = nbands
+    pe.nknots = mk.shape[1]
+    pe.mag = mk.ctypes.data_as(C.POINTER(C.c_double))
+    pe.sigma = sg.ctypes.data_as(C.POINTER(C.c_double))
+    pe.seed = perr_seed
+    w.perr = pe
+    v = A.Vel2pmConfig()
+    v.coordsys = 1
+    v.vLSR, v.u0, v.v0, v.w0, v.Rg = -220.0, -10.0, -5.3, 7.2, Rg
+    w.v2pm = v
+    w.gal2other = 1
+    w.keep += [rows, colors, eflags, mk, sg]
+    return w
+
+
+def config1(lib, **kw):
+    """10x10 deg patch centred on the north galactic pole, 0.25 deg pixels, 15 < r < 21."""
+    half = 5.0 * D2R
+    foot = A.Footprint()
+    foot.kind = A.GF_FOOT_LAMBERT_RECT
+    foot.proj = 0
+    foot.a, foot.b, foot.c, foot.d = -half, half, -half, half
+    return build_workload(lib, foot=foot, dx_deg=0.25, m0=15.0, m1=21.0, **kw)
+
+
+def config2(lib, **kw):
+    """The whole sky with |b| > 10 deg, 0.1 deg pixels, 14 < r < 22."""
+    foot = A.Footprint()
+    foot.kind = A.GF_FOOT_LATCUT
+    foot.a = 10.0
+    kw.setdefault("capacity", 1 << 24)
+    return build_workload(lib, foot=foot, dx_deg=0.1, m0=14.0, m1=22.0, **kw)
+
+
+def cap_footprint(l_deg, b_deg, r_deg):
+    foot = A.Footprint()
+    foot.kind = A.GF_FOOT_CAP
+    foot.a, foot.b, foot.c = l_deg, b_deg, r_deg
+    return foot
+
+
+def splitmix64(x):
+    x = (x + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+    z = x
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+    return z ^ (z >> 31)
+
+
+def config4_requests(n=4096, seed=1234567):
+    """Parameters of the batched form: pencil beams with |b| > 5 deg, radius log-uniform in
+    [0.5, 5] deg, r_max uniform in [19, 24], thin-disk h in [250, 350] pc, halo q in [0.55, 0.75]."""
+    out = []
+    for r in range(n):
+        s = splitmix64(seed + r)
+        g = np.random.default_rng(s)
+        while True:
+            z = g.uniform(-1, 1)
+            b = math.degrees(math.asin(z))
+            if abs(b) > 5.0:
+                break
+        l = g.uniform(0, 360)
+        rad = math.exp(g.uniform(math.log(0.5), math.log(5.0)))
+        rmax = g.uniform(19, 24)
+        h = g.uniform(250, 350)
+        q = g.uniform(0.55, 0.75)
+        out.append(dict(l=l, b=b, r=rad, rmax=rmax, h=h, q=q, seed48=s & 0xFFFFFFFF))
+    return out
+
+
+def config4_workload(lib, req, **kw):
+    foot = cap_footprint(req["l"], req["b"], req["r"])
+    return build_workload(lib, foot=foot, dx_deg=0.1, m0=14.0, m1=req["rmax"], thin_h=req["h"],
+                          halo_q=req["q"], seed48=req["seed48"], **kw)

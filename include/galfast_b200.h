@@ -1,0 +1,387 @@
+/*
+ * galfast_b200.h -- C ABI of the B200-native galfast catalog-generation hot path.
+ *
+ * The library replaces the compute behind galfast's skygen source module and
+ * the postprocessing modules that follow it on the catalog path:
+ *
+ *   reference interface (mjuric/galfast)                      entry point here
+ *   ------------------------------------------------------    ------------------------------
+ *   skygenInterface::init / initRNG (src/skygen/skygen.h:47-60,
+ *     src/skygen/skyconfig_impl.h:244-305, src/common/cux.cpp:404-435)
+ *                                                             gf_rng_init, gf_skygen_create
+ *   skygenInterface::integrateCounts (skyconfig_impl.h:323-429)
+ *                                                             gf_skygen_integrate
+ *   skygenInterface::setDensityNorm (skyconfig_impl.h:308-320) gf_skygen_set_norm
+ *   skygenInterface::drawSources, one output batch per call
+ *     (skyconfig_impl.h:435-545, kernel skygen.cu.h:469-618)  gf_skygen_draw
+ *   osink::process of the modules (src/pipeline.h:98-110) and their kernels
+ *     fixedFeH (src/modules/fixedFeH_host.cpp:49-70)          gf_module_fixedfeh
+ *     Bond2010 (src/modules/Bond2010_host.cpp:70-90)          gf_module_bond2010
+ *     photometry (src/modules/photometry_host.cpp:363-395)    gf_module_photometry
+ *     photometricErrors (photometricErrors_host.cpp:112-131)  gf_module_photoerrors
+ *     vel2pm (src/modules/vel2pm_host.cpp:58-74)              gf_module_vel2pm
+ *     gal2other (src/modules/gal2other_host.cpp)              gf_module_gal2other
+ *     clipper (src/skygen/os_skygen.cpp:999-1044)             gf_module_clipper
+ *   os_skygen::run + drawSources + the module chain
+ *     (os_skygen.cpp:866-932, pipeline.cpp:1143-1227)         gf_catalog_run
+ *
+ * All pointers are plain host or device pointers, all sizes are element
+ * counts, and every entry point returns a gf_status; gf_last_error() returns
+ * a description of the last failure on the calling thread.  A gf_ctx owns one
+ * CUDA stream on one device and is used by one host thread at a time.
+ */
+#ifndef GALFAST_B200_H
+#define GALFAST_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GF_ABI_VERSION 1
+
+typedef enum {
+    GF_OK = 0,
+    GF_E_INVALID = -1,      /* bad argument or configuration */
+    GF_E_OOM = -2,          /* device or host allocation failed */
+    GF_E_CUDA = -3,         /* CUDA runtime error */
+    GF_E_TIMEOUT = -4,      /* a bounded device wait gave up */
+    GF_E_UNSUPPORTED = -5,  /* configuration outside what this build implements */
+    GF_E_STATE = -6         /* call out of sequence */
+} gf_status;
+
+/* ------------------------------------------------------------------ */
+/* Geometry (layouts mirror the reference's device structs)            */
+/* ------------------------------------------------------------------ */
+
+/* A pencil beam (sky pixel); mirrors struct pencilBeam, src/skygen/skygen.h:89-103. */
+typedef struct gf_pencil_beam {
+    float cl, cb, sl, sb;      /* cos/sin of the pixel centre (l, b) */
+    float coveredFraction;     /* fraction of the pixel inside the footprint */
+    float dx, dA;              /* side (radians, Lambert units) and area dx*dx */
+    int32_t projIdx;           /* 0 = north, 1 = south Lambert projection */
+    float X, Y;                /* Lambert coordinates of the centre */
+    int32_t extIdx;            /* row of the per-beam minimum-extinction table */
+    int32_t pad_;
+} gf_pencil_beam;
+
+/* Lambert azimuthal equal-area projection; mirrors class lambert, skygen.h:108-147. */
+typedef struct gf_lambert {
+    double l0, b0;             /* pole (radians) */
+    float cl, cb, sl, sb;      /* cos/sin of the pole, as floats */
+} gf_lambert;
+
+/* ------------------------------------------------------------------ */
+/* skygen configuration                                                */
+/* ------------------------------------------------------------------ */
+
+/* Raw binning keys of the skygen module (os_skygen.cpp:409-430): the library
+ * applies the half-bin shifts and the luminosity-function hint itself. */
+typedef struct gf_skygen_config {
+    float m0, m1, dm;          /* apparent magnitude range and bin (keys m0/r0, m1/r1, dm) */
+    float M0, M1;              /* absolute magnitude range (keys M0/ri0, M1/ri1); dM = dm */
+    float dmin, dmax;          /* distance limits in pc (0, 0 = none) */
+    int32_t nthreads;          /* crawl streams (reference grid*block, default 120*64 = 7680) */
+    float nstars;              /* forced mean star count over all models (0 = from the model) */
+    gf_lambert proj[2];        /* north/south projections */
+} gf_skygen_config;
+
+typedef enum {
+    GF_MODEL_EXP_DISK = 1,                 /* src/skygen/model_expDisk.h */
+    GF_MODEL_POWER_LAW_ELLIPSOID = 2       /* src/skygen/model_powerLawEllipsoid.h */
+} gf_model_type;
+
+typedef enum {
+    GF_FRAME_GALPLANE = 0,     /* center = orientation = galplane (transform.cpp:122-135) */
+    GF_FRAME_EXPLICIT = 1      /* T and M given directly: xyz' = M (xyz + T) */
+} gf_frame_kind;
+
+/* A density model (model_*.cpp load()).  Parameters are the config-file values. */
+typedef struct gf_model_config {
+    int32_t type;              /* gf_model_type */
+    int32_t comp;              /* sequential component id (0-based) */
+    double f;                  /* key f: density at the LF sampling point */
+    double l, h, rcut;         /* exponential disk: scale length, height, cylindrical cutoff (0 = none) */
+    double n, ba, ca;          /* power-law ellipsoid: index, b/a, c/a */
+    double rmin, rmax;         /* power-law ellipsoid radial limits (0, 0 = none) */
+    int32_t frame;             /* gf_frame_kind */
+    double Rg, z0;             /* galplane frame: Sun's distance to the centre and height */
+    double T[3];               /* explicit frame translation */
+    double M[9];               /* explicit frame rotation, row major */
+    double lf_l, lf_b, lf_D;   /* where the LF was sampled (keys lf_l, lf_b, lf_D) */
+    const double *lf_M;        /* LF knots (absolute magnitude); NULL = constant LF of 1 */
+    const double *lf_phi;      /* LF values */
+    int32_t lf_n;              /* number of knots */
+} gf_model_config;
+
+typedef enum {
+    GF_EXT_NONE = 0,           /* zero extinction (os_skygen.cpp:701-706) */
+    GF_EXT_SCREEN_CSCB = 1     /* Am = A0 / |sin b| in the bootstrap band at every distance */
+} gf_extinction_kind;
+
+typedef struct gf_extinction {
+    int32_t kind;
+    float A0;                  /* bootstrap-band extinction towards the pole */
+} gf_extinction;
+
+/* Footprints of the analytic clipper (stars outside are flagged hidden). */
+typedef enum {
+    GF_FOOT_ALL = 0,           /* no clipping */
+    GF_FOOT_LAMBERT_RECT = 1,  /* x0 <= X < x1, y0 <= Y < y1 in projection proj */
+    GF_FOOT_CAP = 2,           /* angular distance from (l, b) <= r (degrees) */
+    GF_FOOT_LATCUT = 3         /* |b| > bmin (degrees) */
+} gf_footprint_kind;
+
+typedef struct gf_footprint {
+    int32_t kind;
+    int32_t proj;
+    double a, b, c, d;         /* RECT: x0 x1 y0 y1; CAP: l b r; LATCUT: bmin */
+} gf_footprint;
+
+/* ------------------------------------------------------------------ */
+/* Output table: structure of arrays, row index fastest                */
+/* (src/common/column.h:131-136, built-in schema otable.cpp:719-745)   */
+/* Vector columns are stored component-major: col[k*pitch + row].      */
+/* ------------------------------------------------------------------ */
+#define GF_MAX_BANDS 17
+
+typedef struct gf_table {
+    int64_t capacity;          /* rows allocated (the pitch of vector columns) */
+    int64_t size;              /* rows in use */
+    int32_t nbands;            /* bands of the photometric system (0 = none) */
+    /* skygen columns (os_skygen.cpp:838-858) */
+    double  *lb;               /* [2]: l, b (degrees) */
+    int32_t *projIdx;
+    float   *projXY;           /* [2] */
+    float   *DM;
+    float   *absmag;           /* absolute magnitude in the bootstrap band */
+    float   *XYZ;              /* [3] heliocentric, pc */
+    int32_t *comp;
+    float   *Am, *AmInf;
+    int32_t *hidden;
+    /* module columns */
+    float   *FeH;
+    float   *vcyl;             /* [3] vR, vPhi, vZ (km/s) */
+    float   *mags;             /* [nbands] true magnitudes */
+    int32_t *photoflags;
+    float   *obsmags;          /* [nbands] magnitudes with photometric errors */
+    float   *pm;               /* [3] mu_l/mu_ra, mu_b/mu_dec (mas/yr), v_r (km/s) */
+    double  *radec;            /* [2] (degrees) */
+} gf_table;
+
+/* ------------------------------------------------------------------ */
+/* Module configurations (mirror the reference module data structs)    */
+/* ------------------------------------------------------------------ */
+
+typedef struct gf_fixedfeh_config {        /* fixedFeH_host.cpp:25-70 */
+    float FeH;
+    uint32_t comp_mask;                    /* bit c set: apply to component c */
+} gf_fixedfeh_config;
+
+typedef struct gf_vmoments {               /* Bond2010_gpu.cu.h:29-34 */
+    float m[3][5];                         /* means: coefficients (a,b,c,d,e) of a + b|Z|^c + d R^e */
+    float ss[6][5];                        /* dispersion tensor s11^.5 s12 s13 s22^.5 s23 s33^.5 */
+} gf_vmoments;
+
+typedef struct gf_bond2010_config {        /* os_Bond2010_data, Bond2010_gpu.cu.h:36-51 */
+    uint32_t comp_thin, comp_thick, comp_halo;   /* component bit masks */
+    float fk;                              /* probability of the first disk Gaussian */
+    gf_vmoments disk_1, disk_2, halo;
+    float M[9];                            /* galactic -> galplane rotation (row major) */
+    float T[3];
+} gf_bond2010_config;
+
+typedef struct gf_photometry_config {      /* os_photometry_data + isochrone textures */
+    int32_t nbands;                        /* ncolors + 1 */
+    int32_t bidx;                          /* bootstrap band index */
+    float reddening[GF_MAX_BANDS];
+    int32_t nFeH, nMr;                     /* texture size */
+    float tcFeH[2], tcMr[2];               /* texture coordinates (x0, 1/dx) */
+    const float *colors;                   /* [ncolors][nMr][nFeH] */
+    const uint8_t *eflags;                 /* [ncolors][nMr][nFeH], 1 = extrapolated */
+    uint32_t comp_mask;
+} gf_photometry_config;
+
+typedef struct gf_photoerr_config {        /* os_photometricErrors: sigma(m) per band */
+    int32_t nbands;
+    int32_t nknots;                        /* knots per band */
+    const double *mag;                     /* [nbands][nknots] */
+    const double *sigma;                   /* [nbands][nknots] */
+    uint64_t seed;                         /* key of the counter-based Gaussian draws */
+} gf_photoerr_config;
+
+typedef struct gf_vel2pm_config {          /* os_vel2pm_data, vel2pm_gpu.cu.h:26-34 */
+    int32_t coordsys;                      /* 0 = GAL (pmlb), 1 = EQU (pmradec) */
+    float vLSR, u0, v0, w0;
+    float Rg;
+} gf_vel2pm_config;
+
+/* ------------------------------------------------------------------ */
+/* Opaque handles                                                     */
+/* ------------------------------------------------------------------ */
+typedef struct gf_ctx gf_ctx;
+typedef struct gf_skygen gf_skygen;
+typedef struct gf_photometry gf_photometry;
+typedef struct gf_photoerr gf_photoerr;
+
+/* Description of the last error on this thread. */
+const char *gf_last_error(void);
+
+/* Create a context on CUDA device `device`. */
+gf_status gf_ctx_create(int device, gf_ctx **out);
+gf_status gf_ctx_destroy(gf_ctx *ctx);
+/* Block until all work queued on the context's stream is done. */
+gf_status gf_ctx_sync(gf_ctx *ctx);
+
+/* ---- persistent multiply-with-carry streams (cux.cpp:404-435, cuda_rng.h:466-497) ---- */
+
+/* Seed nstreams (<= 65536, rounded up to a multiple of 64) streams from the
+ * srand48 seed `seed48`, the value the reference derives as
+ * (uint32)(seeder.uniform() * 2^24) from its GSL generator. */
+gf_status gf_rng_init(gf_ctx *ctx, uint32_t seed48, int32_t nstreams);
+/* The srand48 seed the reference derives from a galfast command-line seed
+ * (GSL's default mt19937 seeded with `seed`, first uniform, times 2^24). */
+uint32_t gf_rng_seed48_from_cli_seed(uint64_t seed);
+/* Copy the stream states to/from host memory: [3][nstreams] words a, c, x. */
+gf_status gf_rng_get_state(gf_ctx *ctx, uint32_t *host_state, int32_t nstreams);
+gf_status gf_rng_set_state(gf_ctx *ctx, const uint32_t *host_state, int32_t nstreams);
+
+/* ---- skygen ---- */
+
+/* Build the generator for a footprint pixelisation and a list of models
+ * (os_skygen::construct + skygenHost<T>::init for each model). */
+gf_status gf_skygen_create(gf_ctx *ctx, const gf_skygen_config *cfg,
+                           const gf_pencil_beam *pixels, int32_t npixels,
+                           const float *beam_ammin,          /* [npixels] minimum extinction per beam, or NULL */
+                           const gf_extinction *ext,
+                           const gf_model_config *models, int32_t nmodels,
+                           gf_skygen **out);
+gf_status gf_skygen_destroy(gf_skygen *sky);
+
+/* Derived per-model binning after the LF hint (skygenParams after init). */
+typedef struct gf_skygen_model_info {
+    float m0, m1, dm, M0, M1, dM;
+    int32_t nm, nM, npixels, nthreads;
+    float f;                               /* renormalised density factor */
+    float lf_x0, lf_inv_dx;                /* LF texture coordinates */
+    int32_t lf_n;
+    float norm;
+} gf_skygen_model_info;
+gf_status gf_skygen_model_info_get(gf_skygen *sky, int32_t model, gf_skygen_model_info *info);
+/* Copy the resampled LF of a model (lf_n floats) to host memory. */
+gf_status gf_skygen_model_lf_get(gf_skygen *sky, int32_t model, float *lf);
+
+/* Expected star counts of one model over all pixels (integrateCounts).
+ * per_pixel (nullable, host, npixels doubles) receives the covered counts per beam. */
+gf_status gf_skygen_integrate(gf_skygen *sky, int32_t model,
+                              double *expected, double *expected_covered,
+                              double *per_pixel);
+gf_status gf_skygen_set_norm(gf_skygen *sky, int32_t model, float norm);
+
+/* Draw the next output batch of one model into the device table `out`
+ * (capacity rows).  The batch follows the reference CPU path: streams fill
+ * the table in stream order; the batch is sorted by (hidden, l, b, DM, M, Am)
+ * and truncated at the first hidden row.  *n_generated receives the stars
+ * drawn in the batch (before truncation), out->size the rows kept, *done = 1
+ * after the model's last batch.  Between calls the caller may run modules
+ * that consume the streams (gf_module_bond2010), as the reference pipeline does. */
+gf_status gf_skygen_draw(gf_skygen *sky, int32_t model, gf_table *out,
+                         int64_t *n_generated, int32_t *done);
+
+/* ---- device tables ---- */
+gf_status gf_table_alloc(gf_ctx *ctx, int64_t capacity, int32_t nbands, gf_table *t);
+gf_status gf_table_free(gf_ctx *ctx, gf_table *t);
+/* Copy rows [0, t->size) of every allocated column to a host table with the same capacity layout. */
+gf_status gf_table_download(gf_ctx *ctx, const gf_table *dev, gf_table *host);
+
+/* ---- modules: process rows [begin, end) of a device table ---- */
+gf_status gf_module_clipper(gf_ctx *ctx, const gf_footprint *foot, const gf_lambert proj[2],
+                            gf_table *t, int64_t begin, int64_t end);
+gf_status gf_module_fixedfeh(gf_ctx *ctx, const gf_fixedfeh_config *cfg, gf_table *t, int64_t begin, int64_t end);
+gf_status gf_module_bond2010(gf_ctx *ctx, const gf_bond2010_config *cfg, gf_table *t, int64_t begin, int64_t end);
+/* Photometry: upload the colour grids once (os_photometry::construct), then process batches. */
+gf_status gf_photometry_create(gf_ctx *ctx, const gf_photometry_config *cfg, gf_photometry **out);
+gf_status gf_photometry_destroy(gf_photometry *p);
+gf_status gf_module_photometry(gf_ctx *ctx, const gf_photometry *p, gf_table *t, int64_t begin, int64_t end);
+/* Photometric errors: sigma(m) knots per band; the Gaussian deviate of (row, band) is
+ * keyed by (seed, row_offset + row, band), so batches reproduce a single run. */
+gf_status gf_photoerr_create(gf_ctx *ctx, const gf_photoerr_config *cfg, gf_photoerr **out);
+gf_status gf_photoerr_destroy(gf_photoerr *p);
+gf_status gf_module_photoerrors(gf_ctx *ctx, const gf_photoerr *p, int64_t row_offset,
+                                gf_table *t, int64_t begin, int64_t end);
+gf_status gf_module_vel2pm(gf_ctx *ctx, const gf_vel2pm_config *cfg, gf_table *t, int64_t begin, int64_t end);
+gf_status gf_module_gal2other(gf_ctx *ctx, int32_t coordsys, gf_table *t, int64_t begin, int64_t end);
+
+/* ---- the catalog path: os_skygen::run + drawSources + the module chain ---- */
+
+typedef struct gf_job {
+    gf_skygen_config sky;
+    const gf_pencil_beam *pixels;
+    int32_t npixels;
+    const float *beam_ammin;                   /* [npixels] or NULL */
+    gf_extinction ext;
+    const gf_model_config *models;             /* run in component order */
+    int32_t nmodels;
+    uint32_t seed48;                           /* srand48 seed of the persistent streams */
+    int32_t nstreams;                          /* streams to seed (0 = keep the context's streams) */
+    int64_t capacity;                          /* rows per output batch (the otable capacity, KBATCH) */
+    int32_t nbands;                            /* bands of the output table (photometry) */
+    const gf_footprint *foot;                  /* clipper; NULL = no clipping */
+    const gf_fixedfeh_config *feh;             /* NULL = module absent */
+    const gf_bond2010_config *kin;
+    const gf_photometry_config *phot;
+    const gf_photoerr_config *perr;
+    const gf_vel2pm_config *v2pm;
+    int32_t gal2other;                         /* 0 = absent, 1 = equatorial (radec) */
+} gf_job;
+
+#define GF_MAX_MODELS 32
+typedef struct gf_catalog_stats {
+    double expected[GF_MAX_MODELS];            /* integrateCounts: stars to generate */
+    double expected_covered[GF_MAX_MODELS];    /* ... within the footprint */
+    int64_t generated[GF_MAX_MODELS];          /* stars drawn (before truncation) */
+    int64_t stored[GF_MAX_MODELS];             /* rows passed down the module chain */
+    int32_t batches;
+    float norm;                                /* density normalisation applied (1 = none) */
+} gf_catalog_stats;
+
+/* Called once per output batch with the device table after all modules ran;
+ * row_offset is the number of rows delivered before this batch.  A nonzero
+ * return stops the run (gf_catalog_run then returns GF_E_STATE). */
+typedef int (*gf_batch_callback)(void *user, int32_t model, const gf_table *dev_batch, int64_t row_offset);
+
+gf_status gf_catalog_run(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, void *user, gf_catalog_stats *stats);
+
+/* ---- host-side setup helpers (no GPU needed) ---- */
+
+/* Lambert projection with pole (l0, b0) in degrees (lambert::init, skygen.h:115-120). */
+gf_status gf_lambert_init(double l0_deg, double b0_deg, gf_lambert *p);
+/* Pixelise a footprint on the two hemispheres' Lambert grids (cell side dx_deg
+ * degrees, grid anchored at each pole; b >= 0 belongs to the north grid), with
+ * the covered fraction of each cell and, for the screen extinction, the minimum
+ * extinction over the cell.  Replaces the GPC footprint pixelisation of
+ * os_skygen::load_footprints (os_skygen.cpp:239-283) for analytic footprints.
+ * Call with pixels == NULL to count. */
+gf_status gf_footprint_pixelize(const gf_footprint *foot, double dx_deg, const gf_lambert proj[2],
+                                const gf_extinction *ext, gf_pencil_beam *pixels, float *beam_ammin,
+                                int64_t max_pixels, int64_t *npixels);
+/* Resample a photometric-system table (rows: Mr, FeH, c_1..c_ncolors) to the colour
+ * and extrapolation-flag grids of os_photometry::construct (photometry_host.cpp:233-344).
+ * colors/eflags: [ncolors][nMr][nFeH]; call with colors == NULL for the sizes. */
+gf_status gf_photometry_build(const double *rows, int32_t nrows, int32_t ncolors, double dFeH, double dMr,
+                              float *colors, uint8_t *eflags, int32_t *nFeH, int32_t *nMr,
+                              float tcFeH[2], float tcMr[2]);
+/* The stream multipliers a_i (safe primes a_i 2^32 - 1, cuda_rng.h:466-497). */
+int gf_multipliers(uint32_t *out, int32_t n);
+/* The seeded stream states [3][nstreams] that gf_rng_init uploads. */
+void gf_rng_seed_host(uint32_t seed48, int32_t nstreams, uint32_t *state);
+/* First n outputs of MT19937 seeded with `seed` (the GSL default generator's core). */
+void gf_mt19937_outputs(uint32_t seed, int n, uint32_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GALFAST_B200_H */

@@ -1,0 +1,1326 @@
+/*
+ * gf_oracle.cpp -- sequential CPU restatement of mjuric/galfast's catalog hot
+ * path.  TEST INFRASTRUCTURE: loaded only by the test suite, smoke() and the
+ * CPU-baseline leg of bench.py, as the checker or as the timed CPU baseline.
+ *
+ * It follows the reference's CPU build: the skygen kernel's emulated threads
+ * run one after another (src/skygen/skygen.cu.h:119-151), atomicAdd is a plain
+ * add (skygen.cu.h:153), textures are sampled at the nearest texel
+ * (src/common/cux.h:778-810, 849-874), and every expression keeps the types
+ * and evaluation order of the reference source (x86 SSE arithmetic, no FMA
+ * contraction).  With -DOR_PORTABLE the elementary functions come from
+ * galfast_b200/csrc/gf_math.h (bit-comparable with the GPU); otherwise from the
+ * host libm, as in the reference's own build.
+ */
+#include "../include/galfast_b200.h"
+#include "../galfast_b200/csrc/gf_math.h"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <thread>
+
+#ifdef OR_PORTABLE
+#define OR_EXPF gfm::expf_
+#define OR_LOGF gfm::logf_
+#define OR_LOG10F gfm::log10f_
+#define OR_EXP10F gfm::exp10f_
+#define OR_POWF gfm::powf_
+#define OR_TANF gfm::tanf_
+#define OR_SINF gfm::sinf_
+#define OR_COSF gfm::cosf_
+#define OR_SIN gfm::sin_d
+#define OR_COS gfm::cos_d
+#define OR_ASIN gfm::asin_d
+#define OR_ATAN2 gfm::atan2_d
+#define OR_EXP gfm::exp_d
+#define OR_LOG gfm::log_d
+#else
+#define OR_EXPF ::expf
+#define OR_LOGF ::logf
+#define OR_LOG10F ::log10f
+#define OR_EXP10F ::exp10f
+#define OR_POWF ::powf
+#define OR_TANF ::tanf
+#define OR_SINF ::sinf
+#define OR_COSF ::cosf
+#define OR_SIN ::sin
+#define OR_COS ::cos
+#define OR_ASIN ::asin
+#define OR_ATAN2 ::atan2
+#define OR_EXP ::exp
+#define OR_LOG ::log
+#endif
+
+namespace {
+
+const double dbl_pi = 3.14159265358979323846264338;
+const double dbl_d2r = 0.01745329251994329576923691;   /* module_lib.h:41-43 */
+const double dbl_r2d = 57.2957795130823208767981548;
+const float POGSON = 0.4605170185988091f;              /* skygen.cu.h:466 */
+const int BLOCK = 10;                                   /* skygen.cu.h:467 */
+
+/* ------------------------------------------------------------------ */
+/* Multiply-with-carry stream and samplers: src/common/cuda_rng.h      */
+/* ------------------------------------------------------------------ */
+struct Rng {
+    uint32_t a, c, xn;
+    /* cuda_rng.h:439-463 */
+    float uniform()
+    {
+        uint64_t xnew = (uint64_t)a * xn + c;
+        c = (uint32_t)(xnew >> 32);
+        xn = (uint32_t)((xnew << 32) >> 32);
+        return 2.32830643708e-10f * xn;
+    }
+    /* cuda_rng.h:158-163 */
+    float uniform_pos()
+    {
+        float x;
+        do { x = uniform(); } while (x == 0.f);
+        return x;
+    }
+    /* cuda_rng.h:165-182 (float square root, as the device build evaluates it) */
+    float gaussian(const float sigma)
+    {
+        float x, y, r2;
+        do {
+            x = -1.f + 2.f * uniform();
+            y = -1.f + 2.f * uniform();
+            r2 = x * x + y * y;
+        } while (r2 > 1.0f || r2 == 0.f || r2 == 4.f);
+        return sigma * y * sqrtf(-2.0f * OR_LOGF(r2) / r2);
+    }
+    /* cuda_rng.h:185-208 */
+    float gamma_large(const float aa)
+    {
+        float sqa, x, y, v;
+        sqa = sqrtf(2 * aa - 1);
+        do {
+            do {
+                y = OR_TANF((float)(M_PI * uniform()));
+                x = sqa * y + aa - 1;
+            } while (x <= 0);
+            v = uniform();
+        } while (v > (1 + y * y) * OR_EXPF((aa - 1) * OR_LOGF(x / (aa - 1)) - sqa * y));
+        return x;
+    }
+    /* cuda_rng.h:211-235 */
+    float gamma_int(const unsigned int aa)
+    {
+        if (aa < 3) {
+            unsigned int i;
+            float prod = 1;
+            for (i = 0; i < aa; i++) prod *= uniform_pos();
+            return -OR_LOGF(prod);
+        }
+        return gamma_large((float)aa);
+    }
+    /* cuda_rng.h:238-264 */
+    float gamma_frac(const float aa)
+    {
+        float p, q, x, u, v;
+        p = (float)(M_E / (aa + M_E));
+        do {
+            u = uniform();
+            v = uniform_pos();
+            if (u < p) {
+                x = (float)OR_EXP((1 / aa) * OR_LOG(v));
+                q = (float)OR_EXP(-x);
+            } else {
+                x = (float)(1 - OR_LOG(v));
+                q = (float)OR_EXP((aa - 1) * OR_LOG(x));
+            }
+        } while (uniform() >= q);
+        return x;
+    }
+    /* cuda_rng.h:276-297 */
+    float gamma(const float aa, const float b)
+    {
+        unsigned int na = (unsigned int)floorf(aa);
+        if (aa >= 4294967295.f) return b * (gamma_large(floorf(aa)) + gamma_frac(aa - floorf(aa)));
+        else if (aa == (float)na) return b * gamma_int(na);
+        else if (na == 0) return b * gamma_frac(aa);
+        else return b * (gamma_int(na) + gamma_frac(aa - na));
+    }
+    /* cuda_rng.h:299-305 */
+    float beta(const float aa, const float b)
+    {
+        float x1 = gamma(aa, 1.0);
+        float x2 = gamma(b, 1.0);
+        return x1 / (x1 + x2);
+    }
+    /* cuda_rng.h:308-340 */
+    unsigned int binomial(float p, unsigned int n)
+    {
+        unsigned int i, aa, b, k = 0;
+        while (n > 10) {
+            float X;
+            aa = 1 + (n / 2);
+            b = 1 + n - aa;
+            X = beta((float)aa, (float)b);
+            if (X >= p) {
+                n = aa - 1;
+                p /= X;
+            } else {
+                k += aa;
+                n = b - 1;
+                p = (p - X) / (1 - X);
+            }
+        }
+        for (i = 0; i < n; i++) {
+            float u = uniform();
+            if (u < p) k++;
+        }
+        return k;
+    }
+    /* cuda_rng.h:344-376 */
+    unsigned int poisson(float mu)
+    {
+        float emu;
+        float prod = 1.0;
+        unsigned int k = 0;
+        while (mu > 10) {
+            unsigned int m = (unsigned int)(mu * (7.0 / 8.0));
+            float X = gamma_int(m);
+            if (X >= mu) return k + binomial(mu / X, m - 1);
+            k += m;
+            mu -= X;
+        }
+        emu = OR_EXPF(-mu);
+        do {
+            prod *= uniform();
+            k++;
+        } while (prod > emu);
+        return k - 1;
+    }
+};
+
+/* rng_base::load/store: gstate[i*nstreams + tid] (cuda_rng.h:45-69) */
+struct RngState {
+    uint32_t *g;
+    int nstreams;
+    Rng load(int tid) const { Rng r; r.a = g[tid]; r.c = g[nstreams + tid]; r.xn = g[2 * nstreams + tid]; return r; }
+    void store(int tid, const Rng &r) const { g[tid] = r.a; g[nstreams + tid] = r.c; g[2 * nstreams + tid] = r.xn; }
+};
+
+/* ------------------------------------------------------------------ */
+/* GSL linear interpolation (spline.cpp:59-65, gsl_interp_linear)     */
+/* evaluated with the index search of gsl_interp_bsearch and linear    */
+/* extrapolation beyond the end knots.                                 */
+/* ------------------------------------------------------------------ */
+double linear_eval(const double *xa, const double *ya, int n, double x)
+{
+    int ilo = 0, ihi = n - 1;
+    while (ihi > ilo + 1) {
+        int i = (ihi + ilo) / 2;
+        if (xa[i] > x) ihi = i; else ilo = i;
+    }
+    double x_lo = xa[ilo], x_hi = xa[ilo + 1];
+    double y_lo = ya[ilo], y_hi = ya[ilo + 1];
+    double dx = x_hi - x_lo;
+    if (dx > 0.0) return y_lo + (x - x_lo) / dx * (y_hi - y_lo);
+    return 0.0;
+}
+
+/* direction (module_lib.h:87-114): cos/sin evaluated in double, stored as float */
+struct Dir { float cl, cb, sl, sb; };
+Dir make_dir(double l, double b)
+{
+    Dir d;
+    d.cl = (float)OR_COS(l); d.cb = (float)OR_COS(b);
+    d.sl = (float)OR_SIN(l); d.sb = (float)OR_SIN(b);
+    return d;
+}
+
+struct F3 { float x, y, z; };
+
+/* ------------------------------------------------------------------ */
+/* Density models (model_expDisk.h:71-121, model_powerLawEllipsoid.h:60-105) */
+/* ------------------------------------------------------------------ */
+struct Model {
+    int type, comp;
+    float f, l, h, r_cut2;
+    float n, ba, ca, rminSq, rmaxSq;
+    float T[3];
+    float M[3][3];
+    std::vector<float> lf;
+    float lf_x0, lf_inv_dx;
+    /* skygenParams of this model after init() (skyconfig_impl.h:244-297) */
+    float m0, m1, dm, M0, M1, dM, dmin, dmax;
+    int npixels, nm, nM, nthreads;
+    float norm;
+    double nstarsExpectedToGenerate, nstarsExpected;
+
+    float rho(float x, float y, float z) const
+    {
+        /* transform(v, T, M) (module_lib.h:133-146) */
+        float vx = x + T[0], vy = y + T[1], vz = z + T[2];
+        float wx = M[0][0] * vx + M[0][1] * vy + M[0][2] * vz;
+        float wy = M[1][0] * vx + M[1][1] * vy + M[1][2] * vz;
+        float wz = M[2][0] * vx + M[2][1] * vy + M[2][2] * vz;
+        if (type == GF_MODEL_EXP_DISK) {
+            float r2 = wx * wx + wy * wy;
+            if (r_cut2 && r2 + wz * wz > r_cut2) return 0.f;
+            float r = sqrtf(r2);
+            float rho = f * OR_EXPF(-r / l - fabsf(wz) / h);
+            return rho;
+        } else {
+            float DSq = wx * wx + wy * wy + wz * wz;
+            if (rmaxSq && (DSq < rminSq || DSq >= rmaxSq)) return 0.f;
+            float ty = wy / ba, tz = wz / ca;
+            float rSq = wx * wx + ty * ty + tz * tz;
+            float rho = f * OR_POWF(rSq, 0.5f * n);
+            return rho;
+        }
+    }
+    /* TEX1D on the CPU: nearest texel with clamping (cux.h:778-792, 849-855) */
+    float lf_sample(float Mabs) const
+    {
+        float xi = (Mabs - lf_x0) * lf_inv_dx + 0.5f;
+        float i = xi;
+        if (i < 0.f) i = 0.f;
+        else if (i >= (float)lf.size()) i = (float)lf.size() - 1;
+        return lf[(uint32_t)i];
+    }
+};
+
+/* reset_absmag (os_skygen.cpp:401-407) */
+void reset_absmag(Model &m, float M0, float M1, float dM)
+{
+    m.M0 = M0; m.M1 = M1; m.dM = dM;
+    m.nM = (int)round((m.M1 - m.M0) / m.dM);
+    m.M1 -= 0.5 * m.dM;
+}
+
+/* galplane frame: xxx2galxyz + get_gal2xxx_matrix (transform.cpp:100-135, 194-213, 345-388) */
+void load_transform(const gf_model_config &c, float T[3], float M[3][3])
+{
+    if (c.frame == GF_FRAME_EXPLICIT) {
+        for (int i = 0; i < 3; i++) T[i] = (float)c.T[i];
+        for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) M[i][j] = (float)c.M[3 * i + j];
+        return;
+    }
+    double Rg = c.Rg, z0 = c.z0;
+    double v[3] = {0., 0., 0.};
+    double sina = -z0 / Rg, cosa = sqrt(1 - sina * sina);
+    double x = cosa * v[0] - sina * v[2];
+    double z = sina * v[0] + cosa * v[2];
+    v[0] = Rg - x;
+    v[1] = -v[1];
+    v[2] = z;
+    T[0] = (float)-v[0]; T[1] = (float)-v[1]; T[2] = (float)-v[2];
+    double go[3][3];
+    go[0][0] = -cosa; go[0][1] = 0; go[0][2] = sina;
+    go[1][0] = 0;     go[1][1] = -1; go[1][2] = 0;
+    go[2][0] = sina;  go[2][1] = 0; go[2][2] = cosa;
+    for (int i = 0; i < 3; i++) for (int j = 0; j < 3; j++) M[i][j] = (float)go[i][j];
+}
+
+/* load_resample_and_clip_texture_1D + construct_texture_by_resampling_1D (cux.cpp:336-384),
+ * or load_constant_texture_1D(1, -100, 100) (cux.cpp:310-318) without a LF table. */
+void load_lf(Model &m, const gf_model_config &c)
+{
+    if (c.lf_n <= 0 || !c.lf_M) {
+        m.lf.assign(2, 1.f);
+        m.lf_x0 = -100.f;
+        m.lf_inv_dx = (float)(1. / (100. - -100.));
+        return;
+    }
+    std::vector<double> X, Y;
+    X.push_back(-123); Y.push_back(0.f);
+    for (int i = 0; i < c.lf_n; i++) { X.push_back(c.lf_M[i]); Y.push_back(c.lf_phi[i]); }
+    double xrange = X.back() - X[1];
+    X[0] = X[1] - 1e-5 * xrange;
+    X.push_back(X.back() + 1e-5 * xrange);
+    Y.push_back(0.f);
+    int ndata = (int)X.size(), nsamp = 1024;
+    m.lf.resize(nsamp);
+    double X0 = X[0], X1 = X[ndata - 1], dX = (X1 - X0) / (nsamp - 1);
+    for (int i = 0; i != nsamp; i++) {
+        m.lf[i] = (float)linear_eval(X.data(), Y.data(), ndata, X0 + i * dX);
+    }
+    m.lf_x0 = (float)X0;
+    m.lf_inv_dx = (float)(1. / dX);
+}
+
+/* ------------------------------------------------------------------ */
+/* skygen                                                              */
+/* ------------------------------------------------------------------ */
+struct Pixel : gf_pencil_beam {};
+
+/* runtime_state<Model> (skygen.h:184-257) */
+struct KState {
+    std::vector<int> cont, ilb, im, iM, k, bc, ndraw;
+    std::vector<F3> pos;
+    std::vector<float> D, Am, ms;
+    std::vector<gf_pencil_beam> pix;
+    void alloc(int n)
+    {
+        cont.assign(n, 0); ilb.assign(n, 0); im.assign(n, 0); iM.assign(n, 0); k.assign(n, 0);
+        bc.assign(n, 0); ndraw.assign(n, 0); pos.assign(n, F3{0, 0, 0});
+        D.assign(n, 0); Am.assign(n, 0); ms.assign(n, 0); pix.assign(n, gf_pencil_beam());
+    }
+};
+
+struct Sky {
+    gf_skygen_config cfg;
+    std::vector<gf_pencil_beam> pixels;
+    std::vector<float> ammin;
+    gf_extinction ext;
+    std::vector<Model> models;
+    std::vector<KState> ks;            /* per model draw state */
+    std::vector<char> ks_alloc;
+};
+
+/* The constant part of one kernel launch (skygenGPU<T> in __constant__ memory). */
+struct Launch {
+    const Sky *sky;
+    const Model *m;
+    int npixels;
+    const gf_pencil_beam *pixels;
+    int stopstars;
+    /* draw */
+    int *nstars;
+    gf_table *out;
+    KState *ks;
+    RngState rng;
+    /* integrate */
+    double *counts, *countsCovered;
+    float *countsCoveredPerBeam;   /* [nthreads][npixels] */
+    float *maxCount;
+};
+
+/* skygen.cu.h:257-300 */
+void diagIndexToIJ(int &ilb, int &i, int &j, int &k, const int x, const int y)
+{
+    int kmax = x * y;
+    if (k >= kmax) {
+        ilb += k / kmax;
+        k %= kmax;
+    }
+    int l = x < y ? x : y;
+    int m = x < y ? y : x;
+    int d;
+    if (2 * k < l * (l - 1)) {
+        d = int(0.5 * (sqrtf(1 + 8 * k) - 1));
+        i = k - d * (d + 1) / 2;
+    } else if (2 * k < l * (2 * m + 1 - l)) {
+        if (x >= y) {
+            int ka = k - y * (y - 1) / 2;
+            d = int(ka / y) + (y - 1);
+            i = (ka % y) + d - (y - 1);
+        } else {
+            int ka = k - x * (x - 1) / 2;
+            d = int(ka / x) + (x - 1);
+            i = ka % x;
+        }
+    } else {
+        int ka = x * y - k - 1;
+        int dd = int(0.5 * (sqrtf(1 + 8 * ka) - 1));
+        d = (x + y - 2) - dd;
+        i = (x - 1) - (ka - dd * (dd + 1) / 2);
+    }
+    j = d - i;
+}
+
+/* skygen.cu.h:307-358 */
+bool advance(const Launch &L, int &ilb, int &i, int &j, gf_pencil_beam &dir, const int x, const int y)
+{
+    i++; j--;
+    if (j < 0) {
+        if (i < y) { j += i + 1; i = 0; }
+        else { i -= (y - 1); j += y; }
+    } else if (i >= x) {
+        if (x > y) {
+            i -= y - j - 2; j = y - 1;
+        } else {
+            if (j + 1 < y - x) { i -= x; j += x + 1; }
+            else { i = x - y + j + 2; j = y - 1; }
+        }
+        if (i == x) {
+            ilb++;
+            if (ilb != L.npixels) dir = L.pixels[ilb];
+        }
+    } else {
+        return false;
+    }
+    return true;
+}
+
+/* The minimum extinction along a beam (ext_beam texture, os_skygen.cpp:742-797). */
+float beam_extinction(const Launch &L, const gf_pencil_beam &pix)
+{
+    if (L.sky->ext.kind == GF_EXT_NONE || L.sky->ammin.empty()) return 0.f;
+    return L.sky->ammin[pix.extIdx];
+}
+
+/* Extinction towards a star (sampleExtinction, skygen.cu.h:199-208) for the screen model. */
+float star_extinction(const Launch &L, const Dir &d)
+{
+    if (L.sky->ext.kind == GF_EXT_SCREEN_CSCB) return L.sky->ext.A0 / fabsf(d.sb);
+    return 0.f;
+}
+
+/* skygen.cu.h:216-229 */
+F3 compute_pos(const Launch &L, float &D, float &Am, float M, const int im, const gf_pencil_beam &pix)
+{
+    const Model &m = *L.m;
+    float mm = m.m0 + im * m.dm;
+    float DM = mm - M;
+    D = OR_POWF(10.f, 0.2f * DM + 1.f);
+    Am = beam_extinction(L, pix);
+    F3 p;
+    p.x = D * pix.cl * pix.cb;
+    p.y = D * pix.sl * pix.cb;
+    p.z = D * pix.sb;
+    return p;
+}
+
+/* lambert::deproject (skygen.h:131-146) */
+void deproject(const gf_lambert &p, double &l, double &b, const float x, const float y)
+{
+    double r2 = x * x + y * y;
+    if (r2 == 0.) { b = p.b0; l = 0.; return; }
+    double ir = 1. / sqrt(r2);
+    double sc = 1. / ir * sqrt(1. - 0.25 * r2);
+    double cc = 1. - 0.5 * r2;
+    b = OR_ASIN(cc * p.sb + y * sc * p.cb * ir);
+    l = p.l0 + OR_ATAN2(x * sc, p.cb * cc / ir - y * p.sb * sc);
+}
+
+/* skygen.cu.h:366-457 */
+void draw_stars(const Launch &L, Rng &rng, int &ndraw, const float &M, const int &im, const gf_pencil_beam &pix, float AmMin)
+{
+    if (!ndraw) return;
+    const Model &m = *L.m;
+    gf_table &s = *L.out;
+    const int64_t P = s.capacity;
+    int idx = *L.nstars; *L.nstars += ndraw;          /* CPU atomicAdd, skygen.cu.h:153 */
+    for (; ndraw && idx < L.stopstars; idx++, ndraw--) {
+        float x = pix.X, y = pix.Y;
+        x += pix.dx * (rng.uniform() - 0.5f);
+        y += pix.dx * (rng.uniform() - 0.5f);
+        if (x * x + y * y > 2.f) {
+            s.hidden[idx] = 1;
+            continue;
+        }
+        s.projIdx[idx] = pix.projIdx;
+        s.projXY[idx] = x;
+        s.projXY[P + idx] = y;
+        double l, b;
+        deproject(L.sky->cfg.proj[pix.projIdx], l, b, x, y);
+        Dir dir2 = make_dir(l, b);
+        l *= dbl_r2d;
+        if (l < 0.) l += 360.;
+        if (l > 360.) l -= 360.;
+        b *= dbl_r2d;
+        s.lb[idx] = l;
+        s.lb[P + idx] = b;
+        float Mtmp, mtmp, DM;
+        s.absmag[idx] = Mtmp = M + m.dM * (rng.uniform() - 0.5f);
+        mtmp = m.m0 + m.dm * (im + rng.uniform() - 0.5f);
+        DM = mtmp - Mtmp;
+        s.DM[idx] = DM;
+        float D = OR_POWF(10, 0.2f * DM + 1.f);
+        s.XYZ[idx] = D * dir2.cl * dir2.cb;
+        s.XYZ[P + idx] = D * dir2.sl * dir2.cb;
+        s.XYZ[2 * P + idx] = D * dir2.sb;
+        s.comp[idx] = m.comp;
+        float Am0, Am1;
+        s.Am[idx] = Am0 = star_extinction(L, dir2);
+        Am1 = star_extinction(L, dir2);
+        s.AmInf[idx] = Am1 > Am0 ? Am1 : Am0;
+        s.hidden[idx] = (mtmp + Am0 > m.m1) ? 1 : 0;
+        if (AmMin > Am0) s.AmInf[idx] = -AmMin;
+    }
+}
+
+/* skygenGPU<T>::kernel<draw> (skygen.cu.h:469-618) for one emulated thread */
+void kernel(const Launch &L, int draw, int tid)
+{
+    const Model &mdl = *L.m;
+    const int nthreads = mdl.nthreads, nm = mdl.nm, nM = mdl.nM;
+    int ilb, im = 0, iM = 0, k, ndraw = 0;
+    F3 pos = {0, 0, 0};
+    gf_pencil_beam pix = gf_pencil_beam();
+    float Am = 0;
+    double count = 0.f, countCovered = 0.f;
+    float maxCount1 = 0.;
+    int bc = 0;
+    float D = 0;
+    float ms = 0;
+    Rng rng = {0, 0, 0};
+
+    ilb = 0;
+    k = BLOCK * (tid - nthreads);
+    if (draw) {
+        KState &ks = *L.ks;
+        if (ks.cont[tid]) {
+            ilb = ks.ilb[tid]; im = ks.im[tid]; iM = ks.iM[tid]; k = ks.k[tid]; bc = ks.bc[tid];
+            pos = ks.pos[tid]; pix = ks.pix[tid]; D = ks.D[tid]; Am = ks.Am[tid]; ms = ks.ms[tid];
+            ndraw = ks.ndraw[tid];
+        }
+        if (ilb >= L.npixels) return;
+        rng = L.rng.load(tid);
+        if (ndraw) {
+            float M = mdl.M1 - iM * mdl.dM;
+            draw_stars(L, rng, ndraw, M, im, pix, Am);
+        }
+    }
+
+    double rhoBeam = 0.f;
+    int ilbPrev = 0;
+    while (ndraw == 0) {
+        bool moved;
+        if (bc == 0) {
+            bc = BLOCK;
+            k += BLOCK * nthreads;
+            diagIndexToIJ(ilb, im, iM, k, nm, nM);
+            if (ilb >= L.npixels) break;
+            pix = L.pixels[ilb];
+            moved = true;
+        } else {
+            moved = advance(L, ilb, im, iM, pix, nm, nM);
+        }
+        bc--;
+
+        float M = mdl.M1 - iM * mdl.dM;
+        if (moved) {
+            if (ilb >= L.npixels) break;
+            pos = compute_pos(L, D, Am, M, im, pix);
+            ms = mdl.rho(pos.x, pos.y, pos.z);
+        }
+
+        if ((mdl.dmin || mdl.dmax) && (mdl.dmin > D || mdl.dmax <= D)) continue;
+
+        float m = mdl.m0 + mdl.dm * im + Am;
+        if (m > mdl.m1) continue;
+
+        float rho = mdl.lf_sample(M) * ms;
+        rho *= mdl.norm;
+        rho *= D * D * D;
+        rho *= pix.dA * POGSON * mdl.dm * mdl.dM;
+
+        if (draw) {
+            if (ndraw == 0) ndraw = rng.poisson(rho);
+            draw_stars(L, rng, ndraw, M, im, pix, Am);
+        } else {
+            if (ilbPrev != ilb) {
+                L.countsCoveredPerBeam[(size_t)tid * L.npixels + ilbPrev] = (float)rhoBeam;
+                rhoBeam = 0.f;
+                ilbPrev = ilb;
+            }
+            count += rho;
+            countCovered += rho * pix.coveredFraction;
+            rhoBeam += rho * pix.coveredFraction;
+            if (maxCount1 < rho) maxCount1 = rho;
+        }
+    }
+
+    if (!draw) {
+        L.countsCoveredPerBeam[(size_t)tid * L.npixels + ilbPrev] = (float)rhoBeam;
+        L.counts[tid] = count;
+        L.countsCovered[tid] = countCovered;
+        L.maxCount[tid] = maxCount1;
+    } else {
+        KState &ks = *L.ks;
+        ks.ilb[tid] = ilb; ks.im[tid] = im; ks.iM[tid] = iM; ks.k[tid] = k; ks.bc[tid] = bc;
+        ks.pos[tid] = pos; ks.pix[tid] = pix; ks.D[tid] = D; ks.Am[tid] = Am; ks.ms[tid] = ms;
+        ks.ndraw[tid] = ndraw;
+        ks.cont[tid] = 1;
+        L.rng.store(tid, rng);
+    }
+}
+
+thread_local std::string g_err;
+
+int g_nthreads_cpu = 1;     /* host threads used by the parallel loops (or_set_threads) */
+
+/* Run f(i) for i in [0, n) on g_nthreads_cpu host threads (interleaved assignment). */
+template <typename F>
+void parallel_for(int n, F f)
+{
+    int nt = std::max(1, std::min(g_nthreads_cpu, n));
+    if (nt == 1) { for (int i = 0; i < n; i++) f(i); return; }
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; t++)
+        th.emplace_back([&, t]() { for (int i = t; i < n; i += nt) f(i); });
+    for (auto &x : th) x.join();
+}
+
+/* star_comp (skyconfig_impl.h:34-68) */
+struct StarComp {
+    const gf_table *t;
+    bool operator()(const size_t a, const size_t b) const
+    {
+        const int64_t P = t->capacity;
+        const double *lb = t->lb;
+        int ha = t->hidden[a], hb = t->hidden[b];
+        if (ha != hb) return ha < hb;
+        if (lb[a] != lb[b]) return lb[a] < lb[b];
+        if (lb[P + a] != lb[P + b]) return lb[P + a] < lb[P + b];
+        if (t->DM[a] != t->DM[b]) return t->DM[a] < t->DM[b];
+        if (t->absmag[a] != t->absmag[b]) return t->absmag[a] < t->absmag[b];
+        return t->Am[a] < t->Am[b];
+    }
+};
+
+template <typename T>
+void permute(T *col, const std::vector<size_t> &s, int64_t n)
+{
+    std::vector<T> tmp(col, col + n);
+    for (int64_t i = 0; i < n; i++) col[i] = tmp[s[i]];
+}
+
+/* ------------------------------------------------------------------ */
+/* Modules                                                              */
+/* ------------------------------------------------------------------ */
+
+/* sampleColors with nearest-texel 2-D lookup (photometry_gpu.cu.h:40-70) */
+struct Phot {
+    const gf_photometry_config *c;
+    float tex(int color, float FeH, float Mr, bool &flag) const
+    {
+        float xi = (FeH - c->tcFeH[0]) * c->tcFeH[1] + 0.5f;
+        float yi = (Mr - c->tcMr[0]) * c->tcMr[1] + 0.5f;
+        if (xi < 0.f) xi = 0.f; else if (xi >= (float)c->nFeH) xi = (float)c->nFeH - 1;
+        if (yi < 0.f) yi = 0.f; else if (yi >= (float)c->nMr) yi = (float)c->nMr - 1;
+        uint32_t i = (uint32_t)xi, j = (uint32_t)yi;
+        size_t off = ((size_t)color * c->nMr + j) * c->nFeH + i;
+        flag = c->eflags[off] != 0;
+        return c->colors[off];
+    }
+};
+
+uint32_t brev32(uint32_t a)     /* photometry_gpu.cu.h:76-84 */
+{
+    a = ((a >> 1) & 0x55555555) + ((a & 0x55555555) << 1);
+    a = ((a >> 2) & 0x33333333) + ((a & 0x33333333) << 2);
+    a = ((a >> 4) & 0x0F0F0F0F) + ((a & 0x0F0F0F0F) << 4);
+    a = ((a >> 8) & 0x00FF00FF) + ((a & 0x00FF00FF) << 8);
+    a = (a >> 16) + (a << 16);
+    return a;
+}
+
+/* Philox4x32-10 (Salmon et al. 2011, "Parallel random numbers: as easy as 1, 2, 3") */
+void philox4x32_10(uint32_t ctr[4], const uint32_t key_in[2])
+{
+    uint32_t k0 = key_in[0], k1 = key_in[1];
+    for (int r = 0; r < 10; r++) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * ctr[0];
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * ctr[2];
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ ctr[1] ^ k0;
+        uint32_t n1 = lo1;
+        uint32_t n2 = hi0 ^ ctr[3] ^ k1;
+        uint32_t n3 = lo0;
+        ctr[0] = n0; ctr[1] = n1; ctr[2] = n2; ctr[3] = n3;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+}
+
+/* Standard normal deviate for (seed, row, band): Box-Muller on two 53-bit uniforms. */
+double error_normal(uint64_t seed, uint64_t row, uint32_t band)
+{
+    uint32_t ctr[4] = {(uint32_t)row, (uint32_t)(row >> 32), band, 0x67616c66u};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    philox4x32_10(ctr, key);
+    uint64_t a = ((uint64_t)ctr[0] << 21) ^ (ctr[1] >> 11);
+    uint64_t b = ((uint64_t)ctr[2] << 21) ^ (ctr[3] >> 11);
+    double u1 = ((double)(a & ((1ull << 53) - 1)) + 1.0) * 0x1p-53;   /* (0, 1] */
+    double u2 = (double)(b & ((1ull << 53) - 1)) * 0x1p-53;           /* [0, 1) */
+    double r = sqrt(-2.0 * OR_LOG(u1));
+    return r * OR_COS(6.283185307179586 * u2);
+}
+
+/* vel2pm_gpu.cu.h:52-61 */
+void vel_xyz2lbr(float &vl, float &vb, float &vr, const float vx, const float vy, const float vz, const float l, const float b)
+{
+    float cl, sl, cb, sb;
+    cl = OR_COSF(l); sl = OR_SINF(l); cb = OR_COSF(b); sb = OR_SINF(b);
+    float tmp;
+    vl = -vx * sl + vy * cl;
+    tmp = vx * cl + vy * sl;
+    vr = cb * tmp + vz * sb;
+    vb = -sb * tmp + vz * cb;
+}
+
+/* vel2pm_gpu.cu.h:89-97 */
+void vel_cyl2xyz(float &vx, float &vy, float &vz, const float vr, const float vphi, const float vz0, const float X, const float Y)
+{
+    float rho = sqrtf(X * X + Y * Y);
+    float cphi = X / rho;
+    float sphi = Y / rho;
+    vx = -sphi * vphi + cphi * vr;
+    vy = cphi * vphi + sphi * vr;
+    vz = vz0;
+}
+
+/* galequ constants (module_lib.h:60-71) */
+const double GE_angp = dbl_d2r * 192.859508333;
+const double GE_l0 = dbl_d2r * 32.932;
+const double GE_ce = 0.88998740217659689;
+const double GE_se = 0.45598511375586859;
+
+/* vel2pm_gpu.cu.h:109-137 */
+void transform_pm(float &vlout, float &vbout, float l, float b, float vl, float vb, const double ce, const double se, const double l0)
+{
+    double cb = OR_COS(b);
+    double sb = OR_SIN(b);
+    double cl = OR_COS(l - l0);
+    double sl = OR_SIN(l - l0);
+    double tmp1 = cb * se - ce * sb * sl;
+    double tmp2 = ce * sb - cb * se * sl;
+    double tmp4 = cb * cl;
+    double tmp3 = sb * se + cb * ce * sl;
+    if (fabs(tmp3) > 0.9999999) {
+        vlout = vbout = 999.99;
+    } else {
+        double denom1 = 1. / (tmp4 * tmp4 + tmp2 * tmp2);
+        double cd = sqrt(1. - tmp3 * tmp3);
+        vl /= cb;
+        vlout = (-ce * cl * vb + cb * tmp1 * vl) * denom1;
+        vbout = (tmp1 * vb + cb * ce * cl * vl) / cd;
+        vlout *= cd;
+    }
+}
+
+}  // namespace
+
+/* ================================================================== */
+/* C API                                                               */
+/* ================================================================== */
+extern "C" {
+
+const char *or_last_error(void) { return g_err.c_str(); }
+
+/* Number of host threads for the loops over independent streams (default 1). */
+void or_set_threads(int n) { g_nthreads_cpu = n < 1 ? 1 : n; }
+
+int or_math_portable(void)
+{
+#ifdef OR_PORTABLE
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+/* Seeding of the persistent streams (cux.cpp:404-414, cuda_rng.h:466-497) with
+ * glibc's srand48/drand48/lrand48.  `primes` holds the stream multipliers.
+ * (int)(drand48()*prime) uses the x86 conversion: out-of-range values become INT_MIN. */
+int or_rng_seed(uint32_t seed, int32_t nstreams, const uint32_t *primes, uint32_t *state)
+{
+    if (nstreams % 64) nstreams += 64 - nstreams % 64;
+    srand48(seed);
+    for (int i = 0; i != nstreams; i++) {
+        uint32_t prime = primes[i];
+        state[i] = prime;
+        double t = drand48() * prime;
+        int32_t cv = (t >= 2147483648.0) ? INT32_MIN : (int32_t)t;
+        state[nstreams + i] = (uint32_t)cv;
+        state[2 * nstreams + i] = (uint32_t)lrand48();
+    }
+    return nstreams;
+}
+
+/* n uniforms of one stream (for the known-answer tests) */
+void or_mwc_uniforms(uint32_t *a, uint32_t *c, uint32_t *x, int n, float *out)
+{
+    Rng r = {*a, *c, *x};
+    for (int i = 0; i < n; i++) out[i] = r.uniform();
+    *a = r.a; *c = r.c; *x = r.xn;
+}
+
+/* n Poisson / Gaussian draws of one stream */
+void or_mwc_poisson(uint32_t *a, uint32_t *c, uint32_t *x, const float *mu, int n, uint32_t *out)
+{
+    Rng r = {*a, *c, *x};
+    for (int i = 0; i < n; i++) out[i] = r.poisson(mu[i]);
+    *a = r.a; *c = r.c; *x = r.xn;
+}
+void or_mwc_gaussian(uint32_t *a, uint32_t *c, uint32_t *x, float sigma, int n, float *out)
+{
+    Rng r = {*a, *c, *x};
+    for (int i = 0; i < n; i++) out[i] = r.gaussian(sigma);
+    *a = r.a; *c = r.c; *x = r.xn;
+}
+
+void *or_skygen_create(const gf_skygen_config *cfg, const gf_pencil_beam *pixels, int32_t npixels,
+                       const float *beam_ammin, const gf_extinction *ext,
+                       const gf_model_config *mc, int32_t nmodels)
+{
+    Sky *s = new Sky();
+    s->cfg = *cfg;
+    s->pixels.assign(pixels, pixels + npixels);
+    if (beam_ammin) s->ammin.assign(beam_ammin, beam_ammin + npixels);
+    s->ext = ext ? *ext : gf_extinction{GF_EXT_NONE, 0.f};
+
+    /* load_skyPixelizationConfig (os_skygen.cpp:409-430) */
+    float M0 = cfg->M0, M1 = cfg->M1, m0 = cfg->m0, m1 = cfg->m1, dm = cfg->dm, dM = dm;
+    Model base = Model();
+    base.dmin = cfg->dmin; base.dmax = cfg->dmax;
+    base.m1 = m1; base.dm = dm;
+    reset_absmag(base, M0, M1, dM);
+    base.nm = (int)round((m1 - m0) / dm);
+    base.m0 = m0 + 0.5 * dm;
+    base.npixels = npixels;
+    base.nthreads = cfg->nthreads;
+
+    for (int i = 0; i < nmodels; i++) {
+        const gf_model_config &c = mc[i];
+        Model m = base;
+        m.type = c.type;
+        m.comp = c.comp;
+        m.norm = 1.f;
+        load_transform(c, m.T, m.M);
+        m.l = (float)c.l; m.h = (float)c.h; m.r_cut2 = 0.f;
+        m.n = (float)c.n; m.ba = (float)c.ba; m.ca = (float)c.ca;
+        m.rminSq = m.rmaxSq = 0.f;
+        /* load_lf (model_lib.h:68-95) */
+        load_lf(m, c);
+        float lfx = (float)c.lf_l, lfy = (float)c.lf_b, lfz = (float)c.lf_D;
+        Dir d = make_dir(lfx * dbl_d2r, lfy * dbl_d2r);
+        F3 lfc = {lfz * d.cl * d.cb, lfz * d.sl * d.cb, lfz * d.sb};
+        m.f = 1.f;
+        float norm = m.rho(lfc.x, lfc.y, lfc.z);
+        if (!(norm != 0.f && std::isnormal(norm))) {
+            g_err = "LF normalisation point has zero density";
+            delete s;
+            return nullptr;
+        }
+        float f0 = (float)c.f;
+        m.f = f0 / norm;
+        if (c.type == GF_MODEL_EXP_DISK) {
+            float rc = (float)c.rcut;
+            m.r_cut2 = rc * rc;
+        } else {
+            float rmin = (float)c.rmin, rmax = (float)c.rmax;
+            m.rminSq = rmin * rmin;
+            m.rmaxSq = rmax * rmax;
+        }
+        /* skygenHost<T>::init (skyconfig_impl.h:257-263): LF hint */
+        float hM0 = m.M0, hM1 = m.M1 + 0.5 * m.dM;
+        float X0 = m.lf_x0;
+        float X1 = double(m.lf.size() - 1) / m.lf_inv_dx + X0;
+        bool ret = false;
+        if (X0 > hM0) { ret = true; hM0 = X0; }
+        if (X1 < hM1) { ret = true; hM1 = X1; }
+        if (ret) reset_absmag(m, hM0, hM1, m.dM);
+        m.nstarsExpected = m.nstarsExpectedToGenerate = 0;
+        s->models.push_back(m);
+    }
+    s->ks.resize(nmodels);
+    s->ks_alloc.assign(nmodels, 0);
+    return s;
+}
+
+void or_skygen_destroy(void *h) { delete (Sky *)h; }
+
+int or_skygen_model_info(void *h, int32_t mi, gf_skygen_model_info *info)
+{
+    Sky *s = (Sky *)h;
+    const Model &m = s->models[mi];
+    info->m0 = m.m0; info->m1 = m.m1; info->dm = m.dm; info->M0 = m.M0; info->M1 = m.M1; info->dM = m.dM;
+    info->nm = m.nm; info->nM = m.nM; info->npixels = m.npixels; info->nthreads = m.nthreads;
+    info->f = m.f; info->lf_x0 = m.lf_x0; info->lf_inv_dx = m.lf_inv_dx; info->lf_n = (int)m.lf.size();
+    info->norm = m.norm;
+    return 0;
+}
+
+int or_skygen_model_lf(void *h, int32_t mi, float *lf)
+{
+    Sky *s = (Sky *)h;
+    std::copy(s->models[mi].lf.begin(), s->models[mi].lf.end(), lf);
+    return 0;
+}
+
+/* integrateCounts (skyconfig_impl.h:323-429), pixel blocks of PIXBLOCK */
+int or_skygen_integrate(void *h, int32_t mi, double *expected, double *expected_covered, double *per_pixel)
+{
+    Sky *s = (Sky *)h;
+    Model &m = s->models[mi];
+    const int N = m.nthreads;
+    const int lastpix = m.npixels;
+    const int PIXBLOCK = 1024 * 1024 * 2 / N;
+    std::vector<double> counts(N), countsCovered(N);
+    std::vector<float> maxCount(N);
+    double nE = 0, nEC = 0;
+    int startpix = 0;
+    while (startpix < lastpix) {
+        int endpix = std::min(startpix + PIXBLOCK, lastpix);
+        int npix = endpix - startpix;
+        std::vector<float> ccpb((size_t)N * npix, 0.f);
+        Launch L = {};
+        L.sky = s; L.m = &m; L.npixels = npix; L.pixels = s->pixels.data() + startpix;
+        L.counts = counts.data(); L.countsCovered = countsCovered.data();
+        L.countsCoveredPerBeam = ccpb.data(); L.maxCount = maxCount.data();
+        std::fill(counts.begin(), counts.end(), 0.);
+        std::fill(countsCovered.begin(), countsCovered.end(), 0.);
+        parallel_for(N, [&](int tid) { kernel(L, 0, tid); });
+        for (int i = 0; i != N; i++) { nE += counts[i]; nEC += countsCovered[i]; }
+        if (per_pixel) {
+            for (int px = 0; px < npix; px++) {
+                double rho = 0;
+                for (int th = 0; th != N; th++) rho += ccpb[(size_t)th * npix + px];
+                per_pixel[startpix + px] = rho;
+            }
+        }
+        startpix = endpix;
+    }
+    m.nstarsExpectedToGenerate = nE;
+    m.nstarsExpected = nEC;
+    if (expected) *expected = nE;
+    if (expected_covered) *expected_covered = nEC;
+    return 0;
+}
+
+/* setDensityNorm (skyconfig_impl.h:308-320) */
+int or_skygen_set_norm(void *h, int32_t mi, float norm)
+{
+    Sky *s = (Sky *)h;
+    Model &m = s->models[mi];
+    m.norm = norm;
+    m.nstarsExpected *= norm;
+    m.nstarsExpectedToGenerate *= norm;
+    return 0;
+}
+
+/* One iteration of drawSources' batch loop (skyconfig_impl.h:445-515):
+ * draw into the host table t (capacity rows), sort, truncate.  rng_state is
+ * the persistent [3][nstreams] stream state, updated in place. */
+int or_skygen_draw(void *h, int32_t mi, uint32_t *rng_state, int32_t nstreams, gf_table *t,
+                   int64_t *n_generated, int32_t *done)
+{
+    Sky *s = (Sky *)h;
+    Model &m = s->models[mi];
+    if (!s->ks_alloc[mi]) { s->ks[mi].alloc(m.nthreads); s->ks_alloc[mi] = 1; }
+    int nstars = 0;
+    Launch L = {};
+    L.sky = s; L.m = &m; L.npixels = m.npixels; L.pixels = s->pixels.data();
+    L.stopstars = (int)t->capacity;
+    L.nstars = &nstars;
+    L.out = t;
+    L.ks = &s->ks[mi];
+    L.rng.g = rng_state; L.rng.nstreams = nstreams;
+    for (int tid = 0; tid < m.nthreads; tid++) kernel(L, 1, tid);
+    int stars_generated = std::min(nstars, L.stopstars);
+    int generated_all = stars_generated < L.stopstars;
+
+    /* sort by (hidden, l, b, DM, M, Am) and truncate at the first hidden row */
+    std::vector<size_t> idx(stars_generated);
+    for (int i = 0; i < stars_generated; i++) idx[i] = i;
+    t->size = stars_generated;
+    StarComp sc = {t};
+    std::sort(idx.begin(), idx.end(), sc);
+    const int64_t P = t->capacity;
+    permute(t->lb, idx, stars_generated); permute(t->lb + P, idx, stars_generated);
+    permute(t->projIdx, idx, stars_generated);
+    permute(t->projXY, idx, stars_generated); permute(t->projXY + P, idx, stars_generated);
+    permute(t->Am, idx, stars_generated); permute(t->AmInf, idx, stars_generated);
+    permute(t->XYZ, idx, stars_generated); permute(t->XYZ + P, idx, stars_generated); permute(t->XYZ + 2 * P, idx, stars_generated);
+    permute(t->comp, idx, stars_generated);
+    permute(t->absmag, idx, stars_generated);
+    permute(t->DM, idx, stars_generated);
+    permute(t->hidden, idx, stars_generated);
+    int32_t *h0 = std::upper_bound(t->hidden, t->hidden + stars_generated, 0);
+    t->size = h0 - t->hidden;
+    *n_generated = stars_generated;
+    *done = generated_all;
+    return 0;
+}
+
+/* Per-stream star counts of a full single-batch draw, without writing rows
+ * (diagnostics for the batch tests): out[tid] = stars drawn by thread tid. */
+
+/* ---- modules on a host table, rows [begin, end) ---- */
+
+/* os_clipper::process (os_skygen.cpp:999-1044) with an analytic footprint */
+int or_module_clipper(const gf_footprint *foot, const gf_lambert *proj, gf_table *t, int64_t begin, int64_t end)
+{
+    (void)proj;
+    const int64_t P = t->capacity;
+    for (int64_t row = begin; row < end; row++) {
+        if (t->hidden[row]) continue;
+        bool in = true;
+        if (foot->kind == GF_FOOT_LAMBERT_RECT) {
+            float x = t->projXY[row], y = t->projXY[P + row];
+            in = t->projIdx[row] == foot->proj && x >= foot->a && x < foot->b && y >= foot->c && y < foot->d;
+        } else if (foot->kind == GF_FOOT_CAP) {
+            double l = t->lb[row] * dbl_d2r, b = t->lb[P + row] * dbl_d2r;
+            double l0 = foot->a * dbl_d2r, b0 = foot->b * dbl_d2r;
+            double cosd = OR_SIN(b) * OR_SIN(b0) + OR_COS(b) * OR_COS(b0) * OR_COS(l - l0);
+            in = cosd >= OR_COS(foot->c * dbl_d2r);
+        } else if (foot->kind == GF_FOOT_LATCUT) {
+            in = fabs(t->lb[P + row]) > foot->a;
+        }
+        if (!in) t->hidden[row] = 1;
+    }
+    return 0;
+}
+
+/* os_fixedFeH_kernel (fixedFeH_gpu.cu.h:34-50) */
+int or_module_fixedfeh(const gf_fixedfeh_config *c, gf_table *t, int64_t begin, int64_t end)
+{
+    for (int64_t row = begin; row < end; row++) {
+        if (t->hidden[row]) continue;
+        int cmp = t->comp[row];
+        if (!((c->comp_mask >> cmp) & 1u)) continue;
+        t->FeH[row] = c->FeH;
+    }
+    return 0;
+}
+
+/* os_Bond2010_kernel (Bond2010_gpu.cu.h:81-218): thread t owns rows
+ * [begin + 256 t, begin + 256 (t+1)) and stream t of the persistent state. */
+static float modfun(float Rsquared, float Z, const float val[5])
+{
+    return val[0] + val[1] * OR_POWF(fabsf(Z), val[2]) + val[3] * OR_POWF(Rsquared, (float)(0.5 * val[4]));
+}
+
+static void trivar_gaussK_draw(float y[3], float s11, float s12, float s13, float s22, float s23, float s33, Rng &rng)
+{
+    float b10 = s12;      float b11 = s22 * s22;
+    float b20 = s13;      float b21 = s23;      float b22 = s33 * s33;
+    float a00 = s11; float oneDivA00 = 1.0f / a00;
+    float a10 = (b10) * oneDivA00;
+    float a11 = sqrtf(b11 - a10 * a10);
+    float a20 = (b20) * oneDivA00;
+    float a21 = (b21 - a20 * a10) / a11;
+    float a22 = sqrtf(b22 - a20 * a20 - a21 * a21);
+    float z0 = rng.gaussian(1.0f);
+    float z1 = rng.gaussian(1.0f);
+    float z2 = rng.gaussian(1.0f);
+    y[0] += a00 * z0;
+    y[1] += a10 * z0 + a11 * z1;
+    y[2] += a20 * z0 + a21 * z1 + a22 * z2;
+}
+
+static void add_dispersion(float v[3], float Rsquared, float Z, const float ellip[6][5], Rng &rng)
+{
+    float sigma[6];
+    for (int i = 0; i < 6; i++) sigma[i] = modfun(Rsquared, Z, ellip[i]);
+    trivar_gaussK_draw(v, sigma[0], sigma[1], sigma[2], sigma[3], sigma[4], sigma[5], rng);
+}
+
+static void compute_means(float v[3], float Rsquared, float Z, const float means[3][5])
+{
+    for (int i = 0; i < 3; i++) v[i] = modfun(Rsquared, Z, means[i]);
+}
+
+int or_module_bond2010(const gf_bond2010_config *par, uint32_t *rng_state, int32_t nstreams,
+                       gf_table *t, int64_t begin, int64_t end)
+{
+    const int64_t P = t->capacity;
+    RngState rs = {rng_state, nstreams};
+    int64_t n = end - begin;
+    int64_t nth = n / 256 + (n % 256 ? 1 : 0);
+    if (nth > nstreams) { g_err = "Bond2010: more than 256*nstreams rows"; return -1; }
+    for (int64_t th = 0; th < nth; th++) {
+        Rng rng = rs.load((int)th);
+        int64_t rb = begin + 256 * th, re = std::min(begin + 256 * (th + 1), end);
+        for (int64_t row = rb; row < re; row++) {
+            if (t->hidden[row]) continue;
+            const int cmp = t->comp[row];
+            float vx = t->XYZ[row] + par->T[0], vy = t->XYZ[P + row] + par->T[1], vz = t->XYZ[2 * P + row] + par->T[2];
+            float wx = par->M[0] * vx + par->M[1] * vy + par->M[2] * vz;
+            float wy = par->M[3] * vx + par->M[4] * vy + par->M[5] * vz;
+            float wz = par->M[6] * vx + par->M[7] * vy + par->M[8] * vz;
+            const float Rsquared = (float)(1e-6 * (wx * wx + wy * wy));
+            const float Z = (float)(1e-3 * wz);
+            float tmp[3];
+            if (((par->comp_thin | par->comp_thick) >> cmp) & 1u) {
+                float p = rng.uniform();
+                const gf_vmoments &disk = p < par->fk ? par->disk_1 : par->disk_2;
+                compute_means(tmp, Rsquared, Z, disk.m);
+                if (tmp[1] > 0.) tmp[1] = 0.;
+                add_dispersion(tmp, Rsquared, Z, disk.ss, rng);
+            } else if ((par->comp_halo >> cmp) & 1u) {
+                compute_means(tmp, Rsquared, Z, par->halo.m);
+                add_dispersion(tmp, Rsquared, Z, par->halo.ss, rng);
+                float invR = 1.f / sqrtf(Rsquared + Z * Z);
+                float cosa = sqrtf(Rsquared) * invR;
+                float sina = Z * invR;
+                float vR = cosa * tmp[0] - sina * tmp[1];
+                float vZ = sina * tmp[0] + cosa * tmp[1];
+                tmp[0] = vR;
+                tmp[1] = tmp[2];
+                tmp[2] = vZ;
+            } else {
+                continue;
+            }
+            t->vcyl[row] = tmp[0];
+            t->vcyl[P + row] = tmp[1];
+            t->vcyl[2 * P + row] = tmp[2];
+        }
+        rs.store((int)th, rng);
+    }
+    return 0;
+}
+
+/* os_photometry_kernel (photometry_gpu.cu.h:87-174) for single stars (nabsmag = 1) */
+int or_module_photometry(const gf_photometry_config *lt, gf_table *t, int64_t begin, int64_t end)
+{
+    const int64_t P = t->capacity;
+    const int ncolors = lt->nbands - 1;
+    Phot ph = {lt};
+    float c[GF_MAX_BANDS];
+    for (int64_t row = begin; row < end; row++) {
+        if (t->hidden[row]) continue;
+        int cmp = t->comp[row];
+        if (!((lt->comp_mask >> cmp) & 1u)) continue;
+        float fFeH = t->FeH[row];
+        uint32_t flag = 0;
+        float fMr = t->absmag[row];
+        if (!(fMr >= 99.999f)) {
+            for (int ic = 0; ic < ncolors; ic++) {
+                bool fl;
+                c[ic] = ph.tex(ic, fFeH, fMr, fl);
+                flag |= ((uint32_t)fl) << ic;
+            }
+            for (int b = 0; b <= ncolors; b++) {
+                float M = fMr;
+                if (b < lt->bidx) { for (int i = b; i != lt->bidx; i++) M += c[i]; }
+                if (b > lt->bidx) { for (int i = lt->bidx; i != b; i++) M -= c[i]; }
+                float L = OR_EXP10F(-0.4f * M);
+                t->mags[b * P + row] = L;
+            }
+        }
+        bool fl = false;
+        for (int i = lt->bidx - 1; i >= 0; i--) {
+            uint32_t mask = 1u << i;
+            fl = fl || (flag & mask);
+            flag |= ((uint32_t)fl) << i;
+        }
+        fl = false;
+        for (int i = lt->bidx; i < ncolors; i++) {
+            uint32_t mask = 1u << i;
+            fl = fl || (flag & mask);
+            flag |= ((uint32_t)fl) << i << 1;
+        }
+        flag &= ~(1u << lt->bidx);
+        flag = brev32(flag);
+        flag >>= (8 * sizeof(flag) - ncolors - 1);
+        t->photoflags[row] = (int32_t)flag;
+        float dm = t->DM[row];
+        float Am0 = t->Am[row];
+        for (int b = 0; b <= ncolors; b++) {
+            float Msys = -2.5f * OR_LOG10F(t->mags[b * P + row]);
+            float msys = dm + Msys;
+            float Am = Am0 * lt->reddening[b];
+            t->mags[b * P + row] = msys + Am;
+        }
+    }
+    return 0;
+}
+
+/* os_photometricErrors::process (photometricErrors_host.cpp:112-131) with
+ * counter-based Gaussian deviates keyed by (seed, row_offset + row, band). */
+int or_module_photoerrors(const gf_photoerr_config *c, int64_t row_offset, gf_table *t, int64_t begin, int64_t end)
+{
+    const int64_t P = t->capacity;
+    for (int b = 0; b < c->nbands; b++) {
+        const double *mk = c->mag + (size_t)b * c->nknots, *sk = c->sigma + (size_t)b * c->nknots;
+        for (int64_t row = begin; row < end; row++) {
+            if (t->hidden[row]) continue;
+            float mag = t->mags[b * P + row];
+            float sigma = (float)linear_eval(mk, sk, c->nknots, mag);
+            double z = error_normal(c->seed, (uint64_t)(row_offset + row), (uint32_t)b);
+            t->obsmags[b * P + row] = mag + (float)(sigma * z);
+        }
+    }
+    return 0;
+}
+
+/* os_vel2pm_kernel (vel2pm_gpu.cu.h:221-301) */
+int or_module_vel2pm(const gf_vel2pm_config *par, gf_table *t, int64_t begin, int64_t end)
+{
+    const int64_t P = t->capacity;
+    for (int64_t row = begin; row < end; row++) {
+        if (t->hidden[row]) continue;
+        float l = 0.017453292519943295769f * (float)t->lb[row];
+        float b = 0.017453292519943295769f * (float)t->lb[P + row];
+        float X = par->Rg - t->XYZ[row];
+        float Y = -t->XYZ[P + row];
+        float Z = t->XYZ[2 * P + row];
+        float vx = t->vcyl[row], vy = t->vcyl[P + row], vz = t->vcyl[2 * P + row];
+        float px, py, pz;
+        vel_cyl2xyz(px, py, pz, vx, vy, vz, X, Y);
+        px -= par->u0;
+        py -= par->v0 + par->vLSR;
+        pz -= par->w0;
+        vel_xyz2lbr(px, py, pz, -px, -py, pz, l, b);
+        float D = sqrtf((8000.f - X) * (8000.f - X) + Y * Y + Z * Z);
+        px = (float)(px / (4.74 * D * 1e-3));
+        py = (float)(py / (4.74 * D * 1e-3));
+        if (par->coordsys == 1) {
+            transform_pm(px, py, l, b, px, py, GE_ce, GE_se, GE_l0);
+        } else if (par->coordsys != 0) {
+            px = py = pz = -9.99f;
+        }
+        t->pm[row] = px;
+        t->pm[P + row] = py;
+        t->pm[2 * P + row] = pz;
+    }
+    return 0;
+}
+
+/* os_gal2other_kernel (gal2other_gpu.cu.h:39-96) */
+int or_module_gal2other(int32_t coordsys, gf_table *t, int64_t begin, int64_t end)
+{
+    const int64_t P = t->capacity;
+    const double pi2 = 2 * dbl_pi;
+    for (int64_t row = begin; row < end; row++) {
+        if (t->hidden[row]) continue;
+        double lx = t->lb[row] * dbl_d2r, ly = t->lb[P + row] * dbl_d2r;
+        double rx, ry;
+        if (coordsys == 1) {
+            const double cb = OR_COS(ly);
+            const double sb = OR_SIN(ly);
+            const double cl = OR_COS(lx - GE_l0);
+            const double sl = OR_SIN(lx - GE_l0);
+            rx = OR_ATAN2(cb * cl, sb * GE_ce - cb * GE_se * sl) + GE_angp;
+            ry = OR_ASIN(cb * GE_ce * sl + sb * GE_se);
+            while (rx < 0.) rx += pi2;
+            while (rx >= pi2) rx -= pi2;
+        } else {
+            rx = ry = -9999.;
+        }
+        t->radec[row] = rx / dbl_d2r;
+        t->radec[P + row] = ry / dbl_d2r;
+    }
+    return 0;
+}
+
+/* vcyl2pm on explicit inputs (for the golden-file and known-answer tests) */
+void or_vcyl2pm(const gf_vel2pm_config *par, int n, const double *l_deg, const double *b_deg,
+                const float *X, const float *Y, const float *Z, const float *vx, const float *vy, const float *vz,
+                float *out /* [n][3] */)
+{
+    for (int i = 0; i < n; i++) {
+        float l = 0.017453292519943295769f * (float)l_deg[i];
+        float b = 0.017453292519943295769f * (float)b_deg[i];
+        float px, py, pz;
+        vel_cyl2xyz(px, py, pz, vx[i], vy[i], vz[i], X[i], Y[i]);
+        px -= par->u0;
+        py -= par->v0 + par->vLSR;
+        pz -= par->w0;
+        vel_xyz2lbr(px, py, pz, -px, -py, pz, l, b);
+        float D = sqrtf((8000.f - X[i]) * (8000.f - X[i]) + Y[i] * Y[i] + Z[i] * Z[i]);
+        px = (float)(px / (4.74 * D * 1e-3));
+        py = (float)(py / (4.74 * D * 1e-3));
+        if (par->coordsys == 1) transform_pm(px, py, l, b, px, py, GE_ce, GE_se, GE_l0);
+        out[3 * i] = px; out[3 * i + 1] = py; out[3 * i + 2] = pz;
+    }
+}
+
+double or_error_normal(uint64_t seed, uint64_t row, uint32_t band) { return error_normal(seed, row, band); }
+
+}  /* extern "C" */

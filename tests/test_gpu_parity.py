@@ -1,0 +1,173 @@
+"""GPU parity: the sm_100a library against the CPU oracle (the reference CPU
+path restated) on the same seeded inputs, through the C ABI.
+
+Per-bin expected counts, Poisson draws and every skygen column must be
+bit-exact; the module columns are required to agree within 1e-5 relative
+(they are computed with the same portable math, so they are normally exact).
+"""
+import numpy as np
+import pytest
+
+import galfast_b200 as G
+from galfast_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SKY_COLS = ["lb", "projIdx", "projXY", "DM", "absmag", "XYZ", "comp", "Am", "AmInf", "hidden"]
+MODULE_COLS = ["FeH", "vcyl", "mags", "photoflags", "obsmags", "pm", "radec"]
+RTOL = 1e-5
+
+
+def small_patch(lib, half_deg=2.5, **kw):
+    import math
+    from galfast_b200 import _abi as A
+    half = half_deg * math.pi / 180
+    foot = A.Footprint()
+    foot.kind = A.GF_FOOT_LAMBERT_RECT
+    foot.proj = 0
+    foot.a, foot.b, foot.c, foot.d = -half, half, -half, half
+    return W.build_workload(lib, foot=foot, dx_deg=0.25, m0=15.0, m1=kw.pop("m1", 21.0), **kw)
+
+
+def assert_same(g, o, names, exact=True):
+    for n in names:
+        a, b = g[n], o[n]
+        assert a.shape == b.shape, n
+        if exact:
+            if a.dtype.kind == "f":
+                same = (a == b) | (np.isnan(a) & np.isnan(b))
+                assert same.all(), "%s differs in %d of %d values" % (n, (~same).sum(), same.size)
+            else:
+                assert np.array_equal(a, b), n
+        else:
+            if a.dtype.kind == "f":
+                np.testing.assert_allclose(a, b, rtol=RTOL, atol=1e-6, err_msg=n)
+            else:
+                assert np.array_equal(a, b), n
+
+
+def test_seed_parity(ctx, multipliers):
+    ctx.rng_init(42, 65536)
+    assert np.array_equal(ctx.rng_state(), O.seed_streams(42, multipliers))
+
+
+@pytest.mark.parametrize("nthreads", [7680, 640, 33])
+def test_integrate_parity(ctx, lib, nthreads):
+    w = small_patch(lib, nthreads=nthreads, with_modules=False)
+    sky = G.Skygen(ctx, w)
+    osk = O.OracleSkygen(w)
+    for m in range(3):
+        ge, gc, gp = sky.integrate_counts(m, per_pixel=True)
+        oe, oc, op = osk.integrate_counts(m, per_pixel=True)
+        assert ge == pytest.approx(oe, rel=1e-12)
+        assert gc == pytest.approx(oc, rel=1e-12)
+        np.testing.assert_allclose(gp, op, rtol=1e-6)
+
+
+def test_integrate_straddling_blocks(ctx, lib):
+    """nm * nM not a multiple of 10: blocks run past the end of a pixel and the
+    reference's pixel blocking changes the anchors (skyconfig_impl.h:344-387)."""
+    w = small_patch(lib, half_deg=1.0, nthreads=300, with_modules=False, m1=21.05, M1=14.9)
+    sky = G.Skygen(ctx, w)
+    osk = O.OracleSkygen(w)
+    inf = sky.info(0)
+    assert (inf.nm * inf.nM) % 10 != 0
+    for m in range(3):
+        ge, gc, _ = sky.integrate_counts(m)
+        oe, oc, _ = osk.integrate_counts(m)
+        assert ge == pytest.approx(oe, rel=1e-12)
+
+
+def draw_all(ctx, w, multipliers, capacity, between=None):
+    """Draw every model batch by batch on both sides and compare each batch."""
+    ctx.rng_init(w.seed48, 65536)
+    ostate = O.seed_streams(w.seed48, multipliers)
+    sky = G.Skygen(ctx, w)
+    osk = O.OracleSkygen(w)
+    for m in range(3):
+        sky.integrate_counts(m)
+        osk.integrate_counts(m)
+    dt = G.DeviceTable(ctx, capacity, 0)
+    ht = G.HostTable(capacity, 0)
+    nb = 0
+    total = 0
+    try:
+        for m in range(3):
+            while True:
+                ng, dg = sky.draw_sources(m, dt)
+                no, do = osk.draw_sources(m, ostate, ht)
+                assert (ng, dg) == (no, do)
+                g = dt.download()
+                assert g.size == ht.size
+                assert_same(g.as_dict(SKY_COLS), ht.as_dict(SKY_COLS), SKY_COLS)
+                N = w.sky.nthreads
+                gs = ctx.rng_state().reshape(3, -1)[:, :N]
+                os_ = ostate.reshape(3, -1)[:, :N]
+                assert np.array_equal(gs, os_), "stream states differ after a batch"
+                nb += 1
+                total += ht.size
+                if dg:
+                    break
+    finally:
+        dt.free()
+    return nb, total
+
+
+def test_draw_single_batch(ctx, lib, multipliers):
+    w = small_patch(lib, with_modules=False)
+    nb, total = draw_all(ctx, w, multipliers, capacity=1 << 18)
+    assert nb == 3 and total > 1000
+
+
+@pytest.mark.parametrize("nthreads,capacity", [(7680, 3000), (97, 1777)])
+def test_draw_multi_batch(ctx, lib, multipliers, nthreads, capacity):
+    w = small_patch(lib, half_deg=1.5, nthreads=nthreads, with_modules=False)
+    nb, total = draw_all(ctx, w, multipliers, capacity=capacity)
+    assert nb > 3
+
+
+def test_draw_straddling_blocks(ctx, lib, multipliers):
+    w = small_patch(lib, half_deg=1.0, nthreads=300, with_modules=False, m1=21.05, M1=14.9)
+    nb, total = draw_all(ctx, w, multipliers, capacity=1 << 16)
+    assert total > 100
+
+
+def run_both(ctx, w, multipliers):
+    gb, ob = [], []
+
+    def gsink(model, t, off):
+        gb.append((model, off, t.as_dict()))
+
+    def osink(model, t, off):
+        ob.append((model, off, t.as_dict()))
+
+    gs = G.run_catalog(ctx, w, gsink)
+    os_, _ = O.run_catalog(w, multipliers, sink=osink)
+    return gs, os_, gb, ob
+
+
+@pytest.mark.parametrize("capacity", [1 << 18, 4000])
+def test_catalog_parity(ctx, lib, multipliers, capacity):
+    """The whole path -- skygen, clipper, fixedFeH, Bond2010 (sharing the streams
+    between batches), photometry, photometric errors, vel2pm, gal2other."""
+    w = small_patch(lib, capacity=capacity)
+    gs, os_, gb, ob = run_both(ctx, w, multipliers)
+    assert len(gb) == len(ob) > 0
+    for (gm, go, g), (om, oo, o) in zip(gb, ob):
+        assert (gm, go) == (om, oo)
+        assert_same(g, o, SKY_COLS)
+        assert_same(g, o, MODULE_COLS, exact=False)
+    for m in range(3):
+        assert gs.generated[m] == os_["generated"][m]
+
+
+def test_config1_catalog(ctx, lib, multipliers):
+    """Configuration 1 in full (about 1e5 stars)."""
+    w = W.config1(lib)
+    gs, os_, gb, ob = run_both(ctx, w, multipliers)
+    n = sum(len(g["DM"]) for _, _, g in gb)
+    assert 5e4 < n < 2e5
+    for (gm, go, g), (om, oo, o) in zip(gb, ob):
+        assert_same(g, o, SKY_COLS)
+        assert_same(g, o, MODULE_COLS, exact=False)
