@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Catalog-generation throughput of galfast_b200 on B200 (stars/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config config2]
+
+A step is one complete catalog request through gf_catalog_run: seeding of the
+65536 persistent MWC streams, the integrate pass of the three density models,
+every 16M-row output batch of each model (Poisson draws, placement, sort) and
+the module chain (clipper, fixedFeH, Bond2010, photometry, photometric errors,
+vel2pm, gal2other).  The default workload is the full-scale plain form: the
+whole sky at |b| > 10 deg in 0.1 deg pixels, 14 < r < 22 (3.41e6 pixels,
+3.9e11 bins, about 2.9e8 stars).
+
+`value` is device-resident throughput (the catalog stays in HBM); `e2e` is the
+same request with every batch copied to pinned host memory inside the timed
+region.  Multi-GPU runs are replicas (one independent request per rank, seed
+offset by rank, scaling "weak").  The CPU baseline is the reference path
+restated in C++ (oracle/, libm flavour) on a fixed 1/1000 subset of the
+pixels, single-threaded like the reference's CPU build.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "stars/s end-to-end on 1 B200, batched vs plain at fixed accuracy; p50/p99 latency"
+
+# nominal per-SM issue rates of B200 (148 SMs): FP32 lanes, special-function units, FP64 lanes
+B200_SMS = 148
+FP32_PER_SM, SFU_PER_SM, FP64_PER_SM = 128, 16, 64
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, path):
+        self.path = path
+        self.p = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + q, "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.p is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        loaded = [x for x in sm if smax and x > 0.5 * smax] or sm
+        return {"sm_mhz": float(np.median(loaded)) if loaded else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(G, W, name, rank=0):
+    L = G.lib()
+    if name == "config2":
+        w = W.config2(L, seed48=42 + rank)
+        desc = "config2: whole sky |b|>10 deg, 0.1 deg pixels, 14<r<22, thin+thick disk+halo, ugriz, 16M-row batches"
+    elif name == "config1":
+        w = W.config1(L, seed48=42 + rank)
+        desc = "config1: 10x10 deg NGP patch, 0.25 deg pixels, 15<r<21"
+    else:
+        raise SystemExit("unknown config " + name)
+    return w, desc
+
+
+def model_bins(w):
+    """bins and diagonals of the three models (same binning for each)."""
+    nm = int(round((w.sky.m1 - w.sky.m0) / w.sky.dm))
+    nM = int(round((w.sky.M1 - w.sky.M0) / w.sky.dm))
+    return len(w.models) * w.npixels * nm * nM, len(w.models) * w.npixels * (nm + nM - 1)
+
+
+def cpu_baseline(G, W, O, w_full, flavour="l"):
+    """The reference CPU path (oracle, libm) on every 1000th pixel of the workload."""
+    import copy
+    mult = np.zeros(65536, dtype=np.uint32)
+    G.lib().gf_multipliers(mult.ctypes.data_as(C.POINTER(C.c_uint32)), 65536)
+    sub = copy.copy(w_full)
+    idx = np.arange(0, w_full.npixels, 1000)
+    pix = np.frombuffer(w_full.pixels, dtype=np.uint8).reshape(w_full.npixels, -1)[idx].copy()
+    # renumber the per-beam extinction rows
+    pb = (G.PencilBeam * len(idx)).from_buffer(pix)
+    for k in range(len(idx)):
+        pb[k].extIdx = k
+    sub.pixels = bytearray(pix.tobytes())
+    sub.npixels = len(idx)
+    sub.ammin = np.ascontiguousarray(w_full.ammin[idx])
+    sub.keep = list(w_full.keep)
+    t0 = time.perf_counter()
+    stats, _ = O.run_catalog(sub, mult, flavour=flavour)
+    dt = time.perf_counter() - t0
+    stars = sum(stats["stored"].values())
+    return stars / dt, stars, dt, len(idx)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="config2")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900))
+
+    import galfast_b200 as G
+    from galfast_b200 import workloads as W
+
+    if args.impl == "reference":
+        from oracle import oracle as O
+        if rank != 0:
+            if dist is not None:
+                dist.destroy_process_group()
+            return
+        w, desc = workload(G, W, args.config)
+        vals = []
+        for i in range(args.warmup + args.steps):
+            v, stars, dt, npx = cpu_baseline(G, W, O, w)
+            if i >= args.warmup:
+                vals.append((v, dt))
+        value = float(np.mean([v for v, _ in vals]))
+        line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "stars/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean([d for _, d in vals])),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": desc, "sample": "every 1000th pixel (%d pixels), full module chain" % npx},
+                "cpu_baseline": {"value": value, "unit": "stars/s", "cores": 1, "kind": "port",
+                                 "sample": "every 1000th pixel of the workload, single-threaded restatement (libm)"},
+                "e2e": {"value": value, "unit": "stars/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    device = local_rank if world > 1 else 0
+    ctx = G.Context(device)
+    w, desc = workload(G, W, args.config, rank)
+    L = G.lib()
+
+    def step(host_sink=None):
+        ctx.mark(0)
+        st = G.run_catalog(ctx, w, host_sink)
+        ctx.mark(1)
+        ms = ctx.elapsed_ms(0, 1)
+        return ms, st
+
+    for _ in range(args.warmup):
+        step()
+
+    # ---- timed region: device-resident catalog ----
+    ctx.profile(True)
+    ctx.profile_read()
+    if dist is not None:
+        dist.barrier()
+    ctx.sync()
+    n0 = L.gf_launch_count()
+    times, stars = [], []
+    clock = ClockSampler(os.path.join(ROOT, "gpurun_out", "bench_clocks_rank%d.csv" % rank)) if os.path.isdir(
+        os.path.join(ROOT, "gpurun_out")) else ClockSampler("/tmp/bench_clocks.csv")
+    with clock:
+        for _ in range(args.steps):
+            ms, st = step()
+            times.append(ms)
+            stars.append(sum(st.stored[i] for i in range(len(w.models))))
+    ctx.sync()
+    launches = L.gf_launch_count() - n0
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    total_ms = float(np.sum(times))
+    if dist is not None:
+        import torch
+        t = torch.tensor([total_ms, float(np.sum(stars))], dtype=torch.float64, device="cuda")
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        total_ms_all, stars_all = float(tmax[0]), float(t[1])
+    else:
+        total_ms_all, stars_all = total_ms, float(np.sum(stars))
+    value = stars_all / (total_ms_all / 1e3)
+
+    # ---- e2e: every batch copied to pinned host memory inside the timed region ----
+    e2e = None
+    if args.e2e_steps > 0:
+        import torch
+        cache = {}
+        d2h = [0]
+
+        def sink(model, t, off):
+            return 0
+
+        def make_pinned_sink():
+            # host tables in page-locked memory; the library copies each batch into them
+            def cb(user, model, tptr, row_offset):
+                tb = tptr.contents
+                key = (tb.capacity, tb.nbands)
+                if key not in cache:
+                    h = G.HostTable.__new__(G.HostTable)
+                    h.capacity, h.nbands, h.arrays = int(tb.capacity), int(tb.nbands), {}
+                    h.t = G.Table()
+                    h.t.capacity, h.t.nbands = tb.capacity, tb.nbands
+                    for name, dt, nc in G.COLUMNS:
+                        k = h.nbands if nc == "bands" else nc
+                        if k == 0:
+                            continue
+                        buf = torch.empty(k * h.capacity * np.dtype(dt).itemsize, dtype=torch.uint8, pin_memory=True)
+                        a = buf.numpy().view(dt).reshape(k, h.capacity)
+                        h.arrays[name] = (a, buf)
+                        setattr(h.t, name, a.ctypes.data)
+                    cache[key] = h
+                h = cache[key]
+                if L.gf_table_download(ctx.h, tptr, C.byref(h.t)) != 0:
+                    return 1
+                row_bytes = sum((tb.nbands if nc == "bands" else nc) * np.dtype(dt).itemsize for _, dt, nc in G.COLUMNS)
+                d2h[0] += int(tb.size) * row_bytes
+                return 0
+            return G.BatchCallback(cb)
+
+        ccb = make_pinned_sink()
+        job = w.job(G.Job)
+        e2e_times = []
+        e2e_stars = []
+        for _ in range(args.e2e_steps):
+            d2h[0] = 0
+            stt = G.CatalogStats()
+            ctx.mark(2)
+            G.check(L.gf_catalog_run(ctx.h, C.byref(job), ccb, None, C.byref(stt)))
+            ctx.mark(3)
+            e2e_times.append(ctx.elapsed_ms(2, 3))
+            e2e_stars.append(sum(stt.stored[i] for i in range(len(w.models))))
+        h2d = w.npixels * C.sizeof(G.PencilBeam) + w.ammin.nbytes + 3 * 1024 * 4 + 12 * 65536
+        if w.phot is not None:
+            h2d += w.phot.nMr * w.phot.nFeH * (w.nbands - 1) * 5
+        if w.perr is not None:
+            h2d += 2 * 8 * w.perr.nbands * w.perr.nknots
+        e2e = {"value": float(np.sum(e2e_stars)) / (float(np.sum(e2e_times)) / 1e3) * (world if world > 1 else 1),
+               "unit": "stars/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h[0])}
+
+    # ---- roofline of the dominant kernel (the draw crawl) ----
+    pk, pk_kind = peaks()
+    bins, diags = model_bins(w)
+    nsteps = args.steps
+    draw_ms = prof.get("draw_window", (0, 0))[0] + prof.get("draw_rerun", (0, 0))[0]
+    draw_launches = prof.get("draw_window", (0, 0))[1] + prof.get("draw_rerun", (0, 0))[1]
+    stars_step = float(np.mean(stars))
+    gen_stars = stars_step
+    # algorithmic work of the draw pass per step (per-bin / per-diagonal / per-star counts of the reference kernel)
+    fp32 = 6.0 * bins + 60.0 * diags + 250.0 * gen_stars
+    sfu = 1.0 * bins + 6.0 * diags + 40.0 * gen_stars
+    fp64 = 150.0 * gen_stars
+    bytes_alg = 32.0 * gen_stars + 48.0 * w.npixels * len(w.models)       # star records written + beams read
+    t_draw = draw_ms / 1e3 / nsteps if draw_ms else float("nan")
+    clk = (pk.get("sm_max_mhz") or 1965.0) * 1e6
+    pf32, psfu, pf64 = B200_SMS * FP32_PER_SM * clk, B200_SMS * SFU_PER_SM * clk, B200_SMS * FP64_PER_SM * clk
+    t_roof = max(fp32 / pf32, sfu / psfu, fp64 / pf64, bytes_alg / (pk["hbm_gbs"] * 1e9))
+    achieved_gbs = bytes_alg / t_draw / 1e9 if t_draw == t_draw else None
+    roofline = {"bound": "hbm", "kernel": "crawl_kernel<1> (draw pass)", "achieved": achieved_gbs,
+                "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": (achieved_gbs / pk["hbm_gbs"]) if achieved_gbs else None,
+                "traffic": None, "peak_source": pk_kind,
+                "algorithmic_bytes_per_launch": bytes_alg * nsteps / max(draw_launches, 1),
+                "avg_launch_ms": draw_ms / max(draw_launches, 1)}
+    compute_roofline = {"bound": "sfu/fp32 issue (nominal)", "kernel": "crawl_kernel<1> (draw pass)",
+                        "t_bound_s": t_roof, "t_measured_s": t_draw, "frac": t_roof / t_draw if t_draw == t_draw else None,
+                        "fp32_ops": fp32, "sfu_ops": sfu, "fp64_ops": fp64,
+                        "peaks": {"fp32_ops_per_s": pf32, "sfu_ops_per_s": psfu, "fp64_ops_per_s": pf64,
+                                  "clock_mhz": clk / 1e6}}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        from oracle import oracle as O
+        v, s_, dt, npx = cpu_baseline(G, W, O, w)
+        cpu = {"value": v, "unit": "stars/s", "cores": 1, "kind": "port",
+               "sample": "every 1000th pixel (%d pixels) of the workload, full module chain, %.1f s" % (npx, dt)}
+
+    if rank == 0:
+        lat = np.array(times) / 1e3
+        line = {"metric": METRIC, "value": value, "unit": "stars/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": float(np.mean(times)), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": desc, "pixels": w.npixels, "bins_per_step": bins,
+                           "stars_per_step": stars_step, "batch_rows": w.capacity, "nthreads": w.sky.nthreads,
+                           "parallelism": "replicas" if world > 1 else "single request",
+                           "l2": "inputs larger than L2 (164 MB pixel list, 10+ GB catalog per step)",
+                           "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99))},
+                "e2e": e2e, "roofline": roofline, "compute_roofline": compute_roofline, "cpu_baseline": cpu,
+                "gpu_launches": int(launches), "clocks": clock.summary(),
+                "phases_ms_per_step": {k: v[0] / nsteps for k, v in prof.items()}}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -58,6 +58,11 @@ def lib():
         L.gf_ctx_create.argtypes = [C.c_int, C.POINTER(vp)]
         L.gf_ctx_destroy.argtypes = [vp]
         L.gf_ctx_sync.argtypes = [vp]
+        L.gf_ctx_mark.argtypes = [vp, C.c_int32]
+        L.gf_ctx_elapsed.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(C.c_float)]
+        L.gf_launch_count.restype = C.c_int64
+        L.gf_profile_enable.argtypes = [vp, C.c_int32]
+        L.gf_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
         L.gf_rng_init.argtypes = [vp, C.c_uint32, C.c_int32]
         L.gf_rng_seed48_from_cli_seed.argtypes = [C.c_uint64]
         L.gf_rng_seed48_from_cli_seed.restype = C.c_uint32
@@ -117,6 +122,8 @@ COLUMNS = [  # name, dtype, components (or "bands")
     ("mags", np.float32, "bands"), ("photoflags", np.int32, 1), ("obsmags", np.float32, "bands"),
     ("pm", np.float32, 3), ("radec", np.float64, 2),
 ]
+PROFILE_PHASES = ["integrate", "draw_window", "draw_rerun", "place", "sort", "clipper", "fixedfeh", "bond2010",
+                  "photometry", "photoerrors", "vel2pm", "gal2other"]
 SKYGEN_COLUMNS = ["lb", "projIdx", "projXY", "DM", "absmag", "XYZ", "comp", "Am", "AmInf", "hidden"]
 
 
@@ -176,6 +183,25 @@ class Context:
 
     def sync(self):
         check(lib().gf_ctx_sync(self.h))
+
+    def mark(self, slot):
+        """Record device event `slot` on the library's stream."""
+        check(lib().gf_ctx_mark(self.h, slot))
+
+    def profile(self, on=True):
+        check(lib().gf_profile_enable(self.h, 1 if on else 0))
+
+    def profile_read(self):
+        """{phase: (milliseconds, launches)} accumulated since the last read."""
+        ms = (C.c_double * 12)()
+        n = (C.c_int64 * 12)()
+        check(lib().gf_profile_read(self.h, ms, n))
+        return {PROFILE_PHASES[i]: (ms[i], n[i]) for i in range(12) if n[i]}
+
+    def elapsed_ms(self, a, b):
+        ms = C.c_float()
+        check(lib().gf_ctx_elapsed(self.h, a, b, C.byref(ms)))
+        return ms.value
 
     def rng_init(self, seed48, nstreams=65536):
         check(lib().gf_rng_init(self.h, seed48, nstreams))

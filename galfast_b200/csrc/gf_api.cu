@@ -65,11 +65,44 @@ struct gf_ctx {
     JumpTables jt = {nullptr, nullptr};
     unsigned long long *d_counters = nullptr;   /* [0] record count, [1] visible count */
     unsigned long long *h_counters = nullptr;   /* pinned */
+    cudaEvent_t ev[16] = {};
+    /* phase profiler */
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
+    double prof_ms[GF_PROF_NPHASES] = {};
+    int64_t prof_n[GF_PROF_NPHASES] = {};
 };
+
+namespace {
+cudaEvent_t prof_event(gf_ctx *c)
+{
+    if (!c->ev_pool.empty()) { cudaEvent_t e = c->ev_pool.back(); c->ev_pool.pop_back(); return e; }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+/* brackets the kernels of one phase with events when profiling is enabled */
+struct ProfScope {
+    gf_ctx *c; int kind; cudaEvent_t a = nullptr;
+    ProfScope(gf_ctx *c_, int k) : c(c_), kind(k)
+    {
+        if (c->prof) { a = prof_event(c); cudaEventRecord(a, c->stream); }
+    }
+    ~ProfScope()
+    {
+        if (!a) return;
+        cudaEvent_t b = prof_event(c);
+        cudaEventRecord(b, c->stream);
+        c->prof_pending.push_back({kind, {a, b}});
+    }
+};
+}  // namespace
 
 struct ModelState {
     gfh::HostModel hm;
     float *d_lf = nullptr;
+    float *d_Dtab = nullptr;                 /* D[im][iM] */
     bool crawl_init = false;
     bool done = false;
     CrawlState st{};
@@ -77,6 +110,9 @@ struct ModelState {
     void *st_mem = nullptr, *snap_mem = nullptr;
     double expected = 0, expected_covered = 0;
     int64_t drawn = 0;
+    std::vector<double> stream_expected;     /* per-stream expected stars (integrate pass) */
+    std::vector<int64_t> stream_drawn;       /* stars drawn per stream so far */
+    int first_active = 0;                    /* streams before it have finished */
 };
 
 struct gf_skygen {
@@ -130,12 +166,24 @@ gf_status alloc_crawl_state(int n, CrawlState &st, void **mem)
 
 size_t crawl_state_bytes(int n) { return (size_t)n * 12 * 4 + (size_t)n * 8 + 16; }
 
-gf_status ensure_rec_capacity(gf_skygen *s, int64_t need)
+gf_status ensure_rec_capacity(gf_skygen *s, int64_t need, int64_t keep)
 {
     if (need <= s->rec_cap) return GF_OK;
     int64_t cap = std::max<int64_t>(need, s->rec_cap * 3 / 2);
     cap = std::max<int64_t>(cap, 4096);
-    dev_free(s->d_rec); dev_free(s->d_rec2);
+    StarRecord *old = s->d_rec;
+    s->d_rec = nullptr;
+    if (keep > 0 && old) {
+        StarRecord *nr = nullptr;
+        GF_TRY(dev_alloc(&nr, cap));
+        GF_CUDA(cudaMemcpyAsync(nr, old, sizeof(StarRecord) * (size_t)keep, cudaMemcpyDeviceToDevice, s->ctx->stream));
+        GF_CUDA(cudaStreamSynchronize(s->ctx->stream));
+        dev_free(old);
+        s->d_rec = nr;
+    } else {
+        dev_free(old);
+    }
+    dev_free(s->d_rec2);
     dev_free(s->d_lb); dev_free(s->d_projIdx); dev_free(s->d_hidden);
     dev_free(s->d_projXY); dev_free(s->d_DM); dev_free(s->d_absmag); dev_free(s->d_XYZ);
     dev_free(s->d_Am); dev_free(s->d_AmInf);
@@ -143,7 +191,7 @@ gf_status ensure_rec_capacity(gf_skygen *s, int64_t need)
     if (s->d_sort_temp) cudaFree(s->d_sort_temp);
     s->d_sort_temp = nullptr;
     s->rec_cap = 0;
-    GF_TRY(dev_alloc(&s->d_rec, cap));
+    if (!s->d_rec) GF_TRY(dev_alloc(&s->d_rec, cap));
     GF_TRY(dev_alloc(&s->d_rec2, cap));
     GF_TRY(dev_alloc(&s->d_lb, 2 * cap));
     GF_TRY(dev_alloc(&s->d_projIdx, cap));
@@ -184,6 +232,7 @@ gfk::LaunchCrawl crawl_launch(gf_skygen *s, ModelState &ms)
     L.rec_capacity = s->rec_cap;
     L.rec_count = s->ctx->d_counters;
     L.err = s->ctx->d_counters + 2;
+    L.Dtab = ms.d_Dtab;
     return L;
 }
 
@@ -204,6 +253,24 @@ gf_status snapshot(gf_skygen *s, ModelState &ms, bool restore)
     return GF_OK;
 }
 
+/* copy streams [a, b) of the crawl state and of the crawl streams between live and snapshot */
+__global__ void copy_state_range(CrawlState dst, CrawlState src, uint32_t *rng_dst, int32_t dst_pitch,
+                                 const uint32_t *rng_src, int32_t src_pitch, int32_t a, int32_t b)
+{
+    int i = a + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= b) return;
+    dst.status[i] = src.status[i]; dst.blk_ilb[i] = src.blk_ilb[i]; dst.blk_k[i] = src.blk_k[i]; dst.pos[i] = src.pos[i];
+    dst.ndraw[i] = src.ndraw[i]; dst.cur_ilb[i] = src.cur_ilb[i]; dst.cur_im[i] = src.cur_im[i]; dst.cur_iM[i] = src.cur_iM[i];
+    dst.D[i] = src.D[i]; dst.Am[i] = src.Am[i]; dst.ms[i] = src.ms[i]; dst.nstars[i] = 0;
+    for (int k = 0; k < 3; k++) rng_dst[(size_t)k * dst_pitch + i] = rng_src[(size_t)k * src_pitch + i];
+}
+
+__global__ void fill_range(int64_t *p, int n, int a, int b, int64_t v)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && i >= a && i < b) p[i] = v;
+}
+
 /* restore streams [t, n) of a model's crawl state and streams from the snapshot */
 __global__ void restore_tail(CrawlState st, CrawlState snap, uint32_t *rng, int32_t NS, const uint32_t *rng_snap, int32_t n, int32_t t)
 {
@@ -213,6 +280,19 @@ __global__ void restore_tail(CrawlState st, CrawlState snap, uint32_t *rng, int3
     st.ndraw[i] = snap.ndraw[i]; st.cur_ilb[i] = snap.cur_ilb[i]; st.cur_im[i] = snap.cur_im[i]; st.cur_iM[i] = snap.cur_iM[i];
     st.D[i] = snap.D[i]; st.Am[i] = snap.Am[i]; st.ms[i] = snap.ms[i]; st.nstars[i] = 0;
     for (int k = 0; k < 3; k++) rng[(size_t)k * NS + i] = rng_snap[(size_t)k * n + i];
+}
+
+gf_status snapshot_range(gf_skygen *s, ModelState &ms, int a, int b, bool restore)
+{
+    if (b <= a) return GF_OK;
+    const int N = s->nthreads, NS = s->ctx->rng_nstreams;
+    int blocks = (b - a + 255) / 256;
+    if (restore)
+        copy_state_range<<<blocks, 256, 0, s->ctx->stream>>>(ms.st, ms.snap, s->ctx->d_rng, NS, s->d_rng_snap, N, a, b);
+    else
+        copy_state_range<<<blocks, 256, 0, s->ctx->stream>>>(ms.snap, ms.st, s->d_rng_snap, N, s->ctx->d_rng, NS, a, b);
+    GF_CUDA(cudaGetLastError());
+    return GF_OK;
 }
 
 __global__ void filter_records(const StarRecord *in, int64_t n, int32_t stream_end, StarRecord *out, unsigned long long *count)
@@ -284,6 +364,9 @@ gf_status gf_ctx_destroy(gf_ctx *ctx)
     dev_free(ctx->jt.hi);
     dev_free(ctx->d_counters);
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
+    for (auto &e : ctx->ev) if (e) cudaEventDestroy(e);
+    for (auto &p : ctx->prof_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
+    for (auto &e : ctx->ev_pool) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return GF_OK;
@@ -293,6 +376,56 @@ gf_status gf_ctx_sync(gf_ctx *ctx)
 {
     GF_TRY(check_ctx(ctx));
     GF_CUDA(cudaStreamSynchronize(ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_ctx_mark(gf_ctx *ctx, int32_t slot)
+{
+    GF_TRY(check_ctx(ctx));
+    if (slot < 0 || slot >= 16) return fail(GF_E_INVALID, "event slot out of range");
+    if (!ctx->ev[slot]) GF_CUDA(cudaEventCreate(&ctx->ev[slot]));
+    GF_CUDA(cudaEventRecord(ctx->ev[slot], ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_ctx_elapsed(gf_ctx *ctx, int32_t from, int32_t to, float *ms)
+{
+    GF_TRY(check_ctx(ctx));
+    if (from < 0 || from >= 16 || to < 0 || to >= 16 || !ctx->ev[from] || !ctx->ev[to] || !ms)
+        return fail(GF_E_INVALID, "event slots not recorded");
+    GF_CUDA(cudaEventSynchronize(ctx->ev[to]));
+    GF_CUDA(cudaEventElapsedTime(ms, ctx->ev[from], ctx->ev[to]));
+    return GF_OK;
+}
+
+int64_t gf_launch_count(void) { return gfk::launches(); }
+
+gf_status gf_profile_enable(gf_ctx *ctx, int32_t on)
+{
+    GF_TRY(check_ctx(ctx));
+    ctx->prof = on != 0;
+    return GF_OK;
+}
+
+gf_status gf_profile_read(gf_ctx *ctx, double *ms, int64_t *launches)
+{
+    GF_TRY(check_ctx(ctx));
+    GF_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (auto &p : ctx->prof_pending) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, p.second.first, p.second.second);
+        ctx->prof_ms[p.first] += t;
+        ctx->prof_n[p.first] += 1;
+        ctx->ev_pool.push_back(p.second.first);
+        ctx->ev_pool.push_back(p.second.second);
+    }
+    ctx->prof_pending.clear();
+    for (int i = 0; i < GF_PROF_NPHASES; i++) {
+        if (ms) ms[i] = ctx->prof_ms[i];
+        if (launches) launches[i] = ctx->prof_n[i];
+        ctx->prof_ms[i] = 0;
+        ctx->prof_n[i] = 0;
+    }
     return GF_OK;
 }
 
@@ -379,6 +512,8 @@ gf_status gf_skygen_create(gf_ctx *ctx, const gf_skygen_config *cfg, const gf_pe
         ms.hm = hms[i];
         if ((st = dev_alloc(&ms.d_lf, ms.hm.lf.size())) != GF_OK) return bail(st);
         cudaMemcpy(ms.d_lf, ms.hm.lf.data(), 4 * ms.hm.lf.size(), cudaMemcpyHostToDevice);
+        if ((st = dev_alloc(&ms.d_Dtab, (size_t)ms.hm.m.nm * ms.hm.m.nM)) != GF_OK) return bail(st);
+        if (gfk::launch_dtab(ms.hm.m, ms.d_Dtab, ctx->stream) != cudaSuccess) return bail(fail(GF_E_CUDA, "distance table"));
         if ((st = alloc_crawl_state(s->nthreads, ms.st, &ms.st_mem)) != GF_OK) return bail(st);
         if ((st = alloc_crawl_state(s->nthreads, ms.snap, &ms.snap_mem)) != GF_OK) return bail(st);
     }
@@ -398,6 +533,7 @@ gf_status gf_skygen_destroy(gf_skygen *s)
     cudaStreamSynchronize(s->ctx->stream);
     for (auto &ms : s->models) {
         dev_free(ms.d_lf);
+        dev_free(ms.d_Dtab);
         if (ms.st_mem) cudaFree(ms.st_mem);
         if (ms.snap_mem) cudaFree(ms.snap_mem);
     }
@@ -467,6 +603,7 @@ gf_status gf_skygen_integrate(gf_skygen *s, int32_t model, double *expected, dou
         /* blocks never straddle pixels: one crawl over all pixels visits the same
          * bins with the same anchors as the reference's pixel-block launches */
         L.pix_base = 0;
+        ProfScope ps(s->ctx, GF_PROF_INTEGRATE);
         GF_CUDA(gfk::launch_crawl(L, 0, st));
     } else {
         /* pixel blocks of 2^21 / nthreads pixels (skyconfig_impl.h:344-387) */
@@ -477,6 +614,7 @@ gf_status gf_skygen_integrate(gf_skygen *s, int32_t model, double *expected, dou
             L.g.pixels = s->d_pixels + p0;
             L.g.npixels = p1 - p0;
             L.pix_base = p0;
+            ProfScope ps(s->ctx, GF_PROF_INTEGRATE);
             GF_CUDA(gfk::launch_crawl(L, 0, st));
         }
     }
@@ -488,6 +626,7 @@ gf_status gf_skygen_integrate(gf_skygen *s, int32_t model, double *expected, dou
     dev_free(d_counts); dev_free(d_cov); dev_free(d_pp);
     double e = 0, ec = 0;
     for (int i = 0; i < N; i++) { e += hc[i]; ec += hv[i]; }
+    if (kmax % GF_BLOCK == 0) ms.stream_expected = hc;   /* the draw crawl assigns the same bins to the same streams */
     ms.expected = e;
     ms.expected_covered = ec;
     if (expected) *expected = e;
@@ -506,69 +645,113 @@ gf_status gf_skygen_draw(gf_skygen *s, int32_t model, gf_table *out, int64_t *n_
     const int N = s->nthreads;
     const int64_t C = out->capacity;
     if (ms.done) { out->size = 0; *n_generated = 0; *done = 1; return GF_OK; }
-    if (!ms.crawl_init) {
+    const bool first_batch = !ms.crawl_init;
+    if (first_batch) {
         GF_CUDA(cudaMemsetAsync(ms.st_mem, 0, crawl_state_bytes(N), st));
         ms.crawl_init = true;
+        ms.stream_drawn.assign(N, 0);
     }
     GF_CUDA(cudaMemsetAsync(ms.st.nstars, 0, 8 * (size_t)N, st));
-    GF_CUDA(cudaMemsetAsync(s->ctx->d_counters + 2, 0, 8, st));
-    GF_TRY(snapshot(s, ms, false));
-    /* first guess of the record buffer: the stars still expected, or the capacity */
-    double remaining = std::max(0.0, ms.expected - (double)ms.drawn);
-    int64_t guess = (int64_t)std::min<double>((double)C, remaining * 1.05 + 6.0 * sqrt(remaining + 1.0) + 1024.0);
-    GF_TRY(ensure_rec_capacity(s, std::max<int64_t>(guess, 4096)));
-
+    GF_CUDA(cudaMemsetAsync(s->ctx->d_counters, 0, 24, st));
+    GF_TRY(ensure_rec_capacity(s, C + C / 2 + 65536, 0));
     const int fb = (N + 255) / 256;
-    int64_t total = 0;
-    for (;;) {
-        fill_i64<<<fb, 256, 0, st>>>(s->d_limits, N, C);
-        GF_CUDA(cudaMemsetAsync(s->ctx->d_counters, 0, 16, st));
-        gfk::LaunchCrawl L = crawl_launch(s, ms);
-        GF_CUDA(gfk::launch_crawl(L, 1, st));
-        GF_CUDA(cudaMemcpyAsync(s->ctx->h_counters, s->ctx->d_counters, 8, cudaMemcpyDeviceToHost, st));
-        GF_CUDA(cudaMemcpyAsync(s->h_nstars, ms.st.nstars, 8 * (size_t)N, cudaMemcpyDeviceToHost, st));
-        GF_CUDA(cudaStreamSynchronize(st));
-        total = (int64_t)s->ctx->h_counters[0];
-        if (total <= s->rec_cap) break;
-        /* more stars than the record buffer holds: grow and redo from the snapshot */
-        GF_TRY(snapshot(s, ms, true));
-        GF_CUDA(cudaMemsetAsync(ms.st.nstars, 0, 8 * (size_t)N, st));
-        GF_TRY(ensure_rec_capacity(s, total));
-    }
-    /* streams fill the batch in stream order (the CPU path's thread order) */
-    int64_t cum = 0;
+
+    /* The batch is filled by streams in stream order (the CPU path runs the
+     * emulated threads one after another).  Streams run speculatively in
+     * windows predicted from their expected counts; the window that reaches
+     * the capacity fixes the boundary stream t. */
+    const bool have_pred = (int)ms.stream_expected.size() == N;
+    int64_t cum = 0;          /* stars of streams before the current window position */
     int t = -1;
-    for (int i = 0; i < N; i++) {
-        if (cum + s->h_nstars[i] >= C) { t = i; break; }
-        cum += s->h_nstars[i];
+    int w_lo = ms.first_active, w_hi = w_lo;
+    while (w_lo < N) {
+        /* window end: enough expected stars to fill the remaining capacity with margin */
+        int64_t room = C - cum;
+        if (have_pred) {
+            double need = (double)room + 6.0 * sqrt((double)room) + 256.0, acc = 0.0;
+            w_hi = w_lo;
+            while (w_hi < N && acc < need) {
+                double rem = ms.stream_expected[w_hi] * (double)ms.hm.m.norm - (double)ms.stream_drawn[w_hi];
+                acc += rem > 0 ? rem : 0.0;
+                w_hi++;
+            }
+            w_hi = std::min(N, std::max(w_hi + 16, w_lo + 32));
+        } else {
+            w_hi = N;
+        }
+        unsigned long long rec_before = 0;
+        GF_CUDA(cudaMemcpyAsync(&s->ctx->h_counters[0], s->ctx->d_counters, 8, cudaMemcpyDeviceToHost, st));
+        GF_CUDA(cudaStreamSynchronize(st));
+        rec_before = s->ctx->h_counters[0];
+        GF_TRY(snapshot_range(s, ms, w_lo, w_hi, false));
+        for (;;) {
+            fill_range<<<fb, 256, 0, st>>>(s->d_limits, N, w_lo, w_hi, room);
+            gfk::LaunchCrawl L = crawl_launch(s, ms);
+            L.stream_begin = w_lo;
+            L.stream_end = w_hi;
+            {
+                ProfScope ps(s->ctx, GF_PROF_DRAW_WINDOW);
+                GF_CUDA(gfk::launch_crawl(L, 1, st));
+            }
+            GF_CUDA(cudaMemcpyAsync(s->ctx->h_counters, s->ctx->d_counters, 8, cudaMemcpyDeviceToHost, st));
+            GF_CUDA(cudaMemcpyAsync(s->h_nstars + w_lo, ms.st.nstars + w_lo, 8 * (size_t)(w_hi - w_lo), cudaMemcpyDeviceToHost, st));
+            GF_CUDA(cudaStreamSynchronize(st));
+            int64_t total = (int64_t)s->ctx->h_counters[0];
+            if (total <= s->rec_cap) break;
+            /* the window drew more stars than the record buffer holds: grow it and redo the window */
+            GF_TRY(snapshot_range(s, ms, w_lo, w_hi, true));
+            GF_TRY(ensure_rec_capacity(s, total + total / 4, (int64_t)rec_before));
+            unsigned long long rb = rec_before;
+            GF_CUDA(cudaMemcpyAsync(s->ctx->d_counters, &rb, 8, cudaMemcpyHostToDevice, st));
+        }
+        for (int i = w_lo; i < w_hi; i++) {
+            if (cum + s->h_nstars[i] >= C) { t = i; break; }
+            cum += s->h_nstars[i];
+        }
+        if (t >= 0) break;
+        w_lo = w_hi;
     }
     int64_t nbatch;
     bool generated_all;
     if (t < 0) {
-        nbatch = total;
+        GF_CUDA(cudaMemcpyAsync(s->ctx->h_counters, s->ctx->d_counters, 8, cudaMemcpyDeviceToHost, st));
+        GF_CUDA(cudaStreamSynchronize(st));
+        nbatch = (int64_t)s->ctx->h_counters[0];
         generated_all = true;
+        for (int i = ms.first_active; i < N; i++) ms.stream_drawn[i] += s->h_nstars[i];
+        ms.first_active = N;
     } else {
-        /* keep the records of streams before t, rerun t with the room left and
-         * let every later stream stop at its first star (skygen.cu.h:366-373) */
+        /* keep the records of streams before t; rerun t with the room left; every
+         * later stream stops at its first star (skygen.cu.h:366-373).  Streams after
+         * the window reached their first star in the first batch already. */
+        GF_CUDA(cudaMemcpyAsync(s->ctx->h_counters, s->ctx->d_counters, 8, cudaMemcpyDeviceToHost, st));
+        GF_CUDA(cudaStreamSynchronize(st));
+        int64_t total = (int64_t)s->ctx->h_counters[0];
         GF_CUDA(cudaMemsetAsync(s->ctx->d_counters, 0, 8, st));
         int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)gfk::sm_count() * 16);
         if (total > 0) filter_records<<<std::max(blocks, 1), 256, 0, st>>>(s->d_rec, total, t, s->d_rec2, s->ctx->d_counters);
         std::swap(s->d_rec, s->d_rec2);
-        /* streams < t keep the state they reached in the speculative run */
-        if (N - t > 0)
-            restore_tail<<<(N - t + 255) / 256, 256, 0, st>>>(ms.st, ms.snap, s->ctx->d_rng, s->ctx->rng_nstreams,
-                                                              s->d_rng_snap, N, t);
+        GF_TRY(snapshot_range(s, ms, t, w_hi, true));
+        const int r_hi = first_batch ? N : w_hi;
         set_limits<<<fb, 256, 0, st>>>(s->d_limits, N, t, C - cum);
         gfk::LaunchCrawl L = crawl_launch(s, ms);
         L.stream_begin = t;
-        GF_CUDA(gfk::launch_crawl(L, 1, st));
+        L.stream_end = r_hi;
+        {
+            ProfScope ps(s->ctx, GF_PROF_DRAW_RERUN);
+            GF_CUDA(gfk::launch_crawl(L, 1, st));
+        }
         GF_CUDA(cudaMemcpyAsync(s->ctx->h_counters, s->ctx->d_counters, 8, cudaMemcpyDeviceToHost, st));
         GF_CUDA(cudaStreamSynchronize(st));
         nbatch = (int64_t)s->ctx->h_counters[0];
         if (nbatch != C) return fail(GF_E_CUDA, "batch rerun produced an unexpected star count");
         generated_all = false;
+        for (int i = ms.first_active; i < t; i++) ms.stream_drawn[i] += s->h_nstars[i];
+        ms.stream_drawn[t] += C - cum;
+        ms.first_active = t;
     }
-    (void)cum;
+    GF_CUDA(cudaMemcpy(s->ctx->h_counters + 2, s->ctx->d_counters + 2, 8, cudaMemcpyDeviceToHost));
+    if (s->ctx->h_counters[2]) return fail(GF_E_INVALID, "a bin has an infinite expected star count");
     /* placement, sort by (hidden, l, b, DM, M, Am), truncation at the first hidden row */
     GF_CUDA(cudaMemsetAsync(s->ctx->d_counters + 1, 0, 8, st));
     gfk::LaunchPlace P;
@@ -580,12 +763,13 @@ gf_status gf_skygen_draw(gf_skygen *s, int32_t model, gf_table *out, int64_t *n_
     P.lb = s->d_lb; P.projIdx = s->d_projIdx; P.projXY = s->d_projXY; P.DM = s->d_DM; P.absmag = s->d_absmag;
     P.XYZ = s->d_XYZ; P.Am = s->d_Am; P.AmInf = s->d_AmInf; P.hidden = s->d_hidden; P.key = s->d_key;
     P.nvis = s->ctx->d_counters + 1;
-    GF_CUDA(gfk::launch_place(P, st));
+    {
+        ProfScope ps(s->ctx, GF_PROF_PLACE);
+        GF_CUDA(gfk::launch_place(P, st));
+    }
     GF_CUDA(cudaMemcpyAsync(s->ctx->h_counters + 1, s->ctx->d_counters + 1, 8, cudaMemcpyDeviceToHost, st));
     GF_CUDA(cudaStreamSynchronize(st));
     int64_t nvis = (int64_t)s->ctx->h_counters[1];
-    GF_CUDA(cudaMemcpy(s->ctx->h_counters + 2, s->ctx->d_counters + 2, 8, cudaMemcpyDeviceToHost));
-    if (s->ctx->h_counters[2]) return fail(GF_E_INVALID, "a bin has an infinite expected star count");
     gfk::LaunchSort S;
     S.n = nbatch;
     S.nvisible = nvis;
@@ -594,7 +778,10 @@ gf_status gf_skygen_draw(gf_skygen *s, int32_t model, gf_table *out, int64_t *n_
     S.lb = s->d_lb; S.projIdx = s->d_projIdx; S.projXY = s->d_projXY; S.DM = s->d_DM; S.absmag = s->d_absmag;
     S.XYZ = s->d_XYZ; S.Am = s->d_Am; S.AmInf = s->d_AmInf; S.comp = ms.hm.m.comp;
     S.out = *out;
-    GF_CUDA(gfk::launch_sort_gather(S, st));
+    {
+        ProfScope ps(s->ctx, GF_PROF_SORT);
+        GF_CUDA(gfk::launch_sort_gather(S, st));
+    }
     GF_CUDA(cudaStreamSynchronize(st));
     out->size = nvis;
     ms.drawn += nbatch;
@@ -709,6 +896,7 @@ gf_status gf_module_clipper(gf_ctx *ctx, const gf_footprint *foot, const gf_lamb
     GF_TRY(check_ctx(ctx));
     GF_TRY(row_range(t, begin, end));
     if (!foot) return fail(GF_E_INVALID, "null footprint");
+    ProfScope ps(ctx, GF_PROF_CLIPPER);
     GF_CUDA(gfk::launch_clipper(*foot, *t, begin, end, ctx->stream));
     return GF_OK;
 }
@@ -718,6 +906,7 @@ gf_status gf_module_fixedfeh(gf_ctx *ctx, const gf_fixedfeh_config *cfg, gf_tabl
     GF_TRY(check_ctx(ctx));
     GF_TRY(row_range(t, begin, end));
     if (!cfg) return fail(GF_E_INVALID, "null config");
+    ProfScope ps(ctx, GF_PROF_FEH);
     GF_CUDA(gfk::launch_fixedfeh(*cfg, *t, begin, end, ctx->stream));
     return GF_OK;
 }
@@ -730,6 +919,7 @@ gf_status gf_module_bond2010(gf_ctx *ctx, const gf_bond2010_config *cfg, gf_tabl
     if (!ctx->d_rng) return fail(GF_E_STATE, "gf_rng_init must precede gf_module_bond2010");
     int64_t n = end - begin;
     if ((n + 255) / 256 > ctx->rng_nstreams) return fail(GF_E_INVALID, "more than 256 rows per stream");
+    ProfScope ps(ctx, GF_PROF_BOND2010);
     GF_CUDA(gfk::launch_bond2010(*cfg, ctx->d_rng, ctx->rng_nstreams, *t, begin, end, ctx->stream));
     return GF_OK;
 }
@@ -782,6 +972,7 @@ gf_status gf_module_photometry(gf_ctx *ctx, const gf_photometry *p, gf_table *t,
     GF_TRY(row_range(t, begin, end));
     if (!p) return fail(GF_E_INVALID, "null photometry");
     if (t->nbands < p->tab.nbands) return fail(GF_E_INVALID, "table has fewer bands than the photometric system");
+    ProfScope ps(ctx, GF_PROF_PHOTOMETRY);
     GF_CUDA(gfk::launch_photometry(p->tab, *t, begin, end, ctx->stream));
     return GF_OK;
 }
@@ -819,6 +1010,7 @@ gf_status gf_module_photoerrors(gf_ctx *ctx, const gf_photoerr *p, int64_t row_o
     GF_TRY(row_range(t, begin, end));
     if (!p) return fail(GF_E_INVALID, "null photometric errors");
     if (t->nbands < p->tab.nbands) return fail(GF_E_INVALID, "table has fewer bands than the error model");
+    ProfScope ps(ctx, GF_PROF_PHOTOERR);
     GF_CUDA(gfk::launch_photoerrors(p->tab, row_offset, *t, begin, end, ctx->stream));
     return GF_OK;
 }
@@ -828,6 +1020,7 @@ gf_status gf_module_vel2pm(gf_ctx *ctx, const gf_vel2pm_config *cfg, gf_table *t
     GF_TRY(check_ctx(ctx));
     GF_TRY(row_range(t, begin, end));
     if (!cfg) return fail(GF_E_INVALID, "null config");
+    ProfScope ps(ctx, GF_PROF_VEL2PM);
     GF_CUDA(gfk::launch_vel2pm(*cfg, *t, begin, end, ctx->stream));
     return GF_OK;
 }
@@ -836,6 +1029,7 @@ gf_status gf_module_gal2other(gf_ctx *ctx, int32_t coordsys, gf_table *t, int64_
 {
     GF_TRY(check_ctx(ctx));
     GF_TRY(row_range(t, begin, end));
+    ProfScope ps(ctx, GF_PROF_GAL2OTHER);
     GF_CUDA(gfk::launch_gal2other(coordsys, *t, begin, end, ctx->stream));
     return GF_OK;
 }

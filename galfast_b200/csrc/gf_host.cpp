@@ -421,40 +421,46 @@ gf_status gf_footprint_pixelize(const gf_footprint *foot, double dx_deg, const g
                 double nx = std::max(cx0, std::min(0.0, cx0 + dx)), ny = std::max(cy0, std::min(0.0, cy0 + dx));
                 double rmin2 = nx * nx + ny * ny;
                 if (rmin2 > 2.0) continue;
-                /* coverage: corners + centre decide interior cells; boundary cells are supersampled */
-                int in_corners = 0;
-                for (int c = 0; c < 5; c++) {
-                    double px = (c == 4) ? cx0 + 0.5 * dx : cx0 + (c & 1) * dx * 0.999999;
-                    double py = (c == 4) ? cy0 + 0.5 * dx : cy0 + ((c >> 1) & 1) * dx * 0.999999;
-                    if (px * px + py * py > 2.0) continue;
+                /* coverage: corners + centre decide interior and exterior cells; mixed
+                 * cells (and cells that could hold a footprint smaller than a cell) are
+                 * supersampled */
+                auto in_point = [&](double px, double py) -> bool {
+                    double r2 = px * px + py * py;
+                    if (r2 > 2.0) return false;
+                    if (foot->kind == GF_FOOT_LATCUT) {
+                        /* pole projections: sin|b| = 1 - r^2/2 */
+                        return 1.0 - 0.5 * r2 > gfm::sin_d(foot->a * kD2R);
+                    }
+                    if (foot->kind == GF_FOOT_LAMBERT_RECT) return ft.inside(h, px, py, 0, 0);
                     double l, b;
                     deproject_d(proj[h], px, py, l, b);
                     bool hemi = (h == 0) ? (b >= 0) : (b < 0);
-                    if (hemi && ft.inside(h, px, py, l, b)) in_corners++;
+                    return hemi && ft.inside(h, px, py, l, b);
+                };
+                int in_corners = 0;
+                for (int c = 0; c < 5; c++) {
+                    double px = (c == 4) ? cx0 + 0.5 * dx : cx0 + (c & 1) * dx;
+                    double py = (c == 4) ? cy0 + 0.5 * dx : cy0 + ((c >> 1) & 1) * dx;
+                    if (in_point(px, py)) in_corners++;
                 }
+                bool tiny = foot->kind == GF_FOOT_CAP && foot->c * kD2R < 3 * dx;
                 double cov;
-                if (in_corners == 5 && foot->kind != GF_FOOT_CAP && foot->kind != GF_FOOT_LATCUT) {
+                if (foot->kind == GF_FOOT_LAMBERT_RECT) {
+                    /* exact overlap of two rectangles */
+                    double ox = std::max(0.0, std::min(cx0 + dx, foot->b) - std::max(cx0, foot->a));
+                    double oy = std::max(0.0, std::min(cy0 + dx, foot->d) - std::max(cy0, foot->c));
+                    cov = ox * oy / (dx * dx);
+                    if (cx0 * cx0 + cy0 * cy0 > 2.0 && in_corners == 0) cov = 0.0;
+                } else if (in_corners == 5 && !tiny) {
                     cov = 1.0;
+                } else if (in_corners == 0 && !tiny) {
+                    cov = 0.0;
                 } else {
                     int cnt = 0;
-                    for (int a = 0; a < SS; a++) {
-                        for (int bq = 0; bq < SS; bq++) {
-                            double px = cx0 + (a + 0.5) * dx / SS, py = cy0 + (bq + 0.5) * dx / SS;
-                            if (px * px + py * py > 2.0) continue;
-                            double l, b;
-                            deproject_d(proj[h], px, py, l, b);
-                            bool hemi = (h == 0) ? (b >= 0) : (b < 0);
-                            if (hemi && ft.inside(h, px, py, l, b)) cnt++;
-                        }
-                    }
-                    if (foot->kind == GF_FOOT_LAMBERT_RECT) {
-                        /* exact overlap of two rectangles */
-                        double ox = std::max(0.0, std::min(cx0 + dx, foot->b) - std::max(cx0, foot->a));
-                        double oy = std::max(0.0, std::min(cy0 + dx, foot->d) - std::max(cy0, foot->c));
-                        cov = ox * oy / (dx * dx);
-                    } else {
-                        cov = (double)cnt / (SS * SS);
-                    }
+                    for (int a = 0; a < SS; a++)
+                        for (int bq = 0; bq < SS; bq++)
+                            if (in_point(cx0 + (a + 0.5) * dx / SS, cy0 + (bq + 0.5) * dx / SS)) cnt++;
+                    cov = (double)cnt / (SS * SS);
                 }
                 if (cov <= 0.0) continue;
                 if (pixels && n < max_pixels) {

@@ -23,6 +23,7 @@ struct LaunchCrawl {
     unsigned long long *err;
     double *counts, *countsCovered, *per_pixel;
     int32_t pix_base;
+    const float *Dtab;
 };
 
 struct LaunchPlace {
@@ -52,10 +53,14 @@ struct LaunchSort {
 };
 
 int sm_count();
+/* count of kernel launches issued by the library (for the benchmark's launch census) */
+void count_launches(int n);
+long long launches();
 cudaError_t launch_crawl(const LaunchCrawl &L, int draw, cudaStream_t s);
 cudaError_t launch_place(const LaunchPlace &L, cudaStream_t s);
 cudaError_t sort_temp_bytes(int64_t n, size_t *bytes);
 cudaError_t launch_sort_gather(const LaunchSort &L, cudaStream_t s);
+cudaError_t launch_dtab(const SkyModel &m, float *D, cudaStream_t s);
 cudaError_t launch_jump_tables(const uint32_t *mult, int n, uint64_t *lo, uint64_t *hi, cudaStream_t s);
 
 /* modules (gf_modules.cu) */

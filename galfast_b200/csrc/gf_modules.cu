@@ -55,6 +55,7 @@ cudaError_t launch_clipper(const gf_footprint &foot, gf_table t, int64_t begin, 
 {
     if (end <= begin || foot.kind == GF_FOOT_ALL) return cudaSuccess;
     clipper_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(foot, t, begin, end);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -73,6 +74,7 @@ cudaError_t launch_fixedfeh(const gf_fixedfeh_config &c, gf_table t, int64_t beg
 {
     if (end <= begin) return cudaSuccess;
     fixedfeh_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(c, t, begin, end);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -165,6 +167,7 @@ cudaError_t launch_bond2010(const gf_bond2010_config &c, uint32_t *rng, int32_t 
     int64_t nchunks = n / 256 + (n % 256 ? 1 : 0);
     if (nchunks > NS) return cudaErrorInvalidValue;
     bond2010_kernel<<<(int)((nchunks + 127) / 128), 128, 0, s>>>(c, rng, NS, t, begin, end, nchunks);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -230,6 +233,7 @@ cudaError_t launch_photometry(const PhotTables &c, gf_table t, int64_t begin, in
 {
     if (end <= begin) return cudaSuccess;
     photometry_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(c, t, begin, end);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -292,6 +296,7 @@ cudaError_t launch_photoerrors(const PerrTables &c, int64_t row_offset, gf_table
 {
     if (end <= begin) return cudaSuccess;
     photoerr_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(c, row_offset, t, begin, end);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -373,6 +378,7 @@ cudaError_t launch_vel2pm(const gf_vel2pm_config &c, gf_table t, int64_t begin, 
 {
     if (end <= begin) return cudaSuccess;
     vel2pm_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(c, t, begin, end);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -406,6 +412,7 @@ cudaError_t launch_gal2other(int32_t coordsys, gf_table t, int64_t begin, int64_
 {
     if (end <= begin) return cudaSuccess;
     gal2other_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(coordsys, t, begin, end);
+    count_launches(1);
     return cudaGetLastError();
 }
 

@@ -24,6 +24,7 @@
 #include "gf_crawl.cuh"
 #include "gf_rng.h"
 #include <cub/cub.cuh>
+#include <atomic>
 
 namespace gfk {
 
@@ -44,6 +45,7 @@ struct CrawlParams {
     double *counts, *countsCovered;
     double *per_pixel;
     int32_t pix_base;              /* first pixel of this launch within the generator's pixel list */
+    const float *Dtab;             /* distances D[im][iM] of the model's bins */
 };
 
 __device__ __forceinline__ uint64_t shfl64(uint64_t v, int src)
@@ -77,62 +79,33 @@ __device__ __forceinline__ bool surely_empty(float u, float mu)
     return u <= (1.0f - mu) - 3.0e-7f;
 }
 
-/* Enumerate the bins of one block (the block starting at local index k0 in pixel
- * ilb0) into per-position arrays.  alive[s] = 0 once the crawl has left the
- * last pixel; moved[s] marks the anchor bins. */
-struct BlockBins {
-    int ilb[GF_BLOCK];
-    short im[GF_BLOCK], iM[GF_BLOCK];
-    bool moved[GF_BLOCK], alive[GF_BLOCK];
+/* The bin at position s of the block starting at local index k0 in pixel ilb0,
+ * by following advance() from the block start (skygen.cu.h:307-358).  Also
+ * returns whether the bin is alive (the crawl has not left the last pixel) and
+ * the last anchor bin at or after position s_from (-1 if none). */
+struct BinPos {
+    int ilb, im, iM;
+    bool alive;
+    int anchor_s;
 };
 
-__device__ __forceinline__ void enumerate_block(int ilb0, int k0, int x, int y, int npix, BlockBins &b)
+__device__ BinPos bin_at(int ilb0, int k0, int s, int s_from, int x, int y, int npix)
 {
-    const int kmax = x * y;
-    if (ilb0 >= npix) {
-#pragma unroll
-        for (int s = 0; s < GF_BLOCK; s++) b.alive[s] = false;
-        return;
-    }
+    BinPos r;
     int i, j;
-    if (k0 + GF_BLOCK - 1 < kmax) {
-        gfc::diag_to_ij(k0, x, y, i, j);
-#pragma unroll
-        for (int s = 0; s < GF_BLOCK; s++) {
-            if (s > 0) {
-                /* step along the diagonal; recompute at a diagonal end */
-                int ni = i + 1, nj = j - 1;
-                if (nj < 0 || ni >= x) gfc::diag_to_ij(k0 + s, x, y, ni, nj);
-                i = ni; j = nj;
-            }
-            b.ilb[s] = ilb0;
-            b.im[s] = (short)i;
-            b.iM[s] = (short)j;
-            b.moved[s] = (s == 0) || i == 0 || j == y - 1;
-            b.alive[s] = true;
-        }
-        return;
+    gfc::diag_to_ij(k0, x, y, i, j);
+    int ilb = ilb0;
+    bool alive = ilb0 < npix;
+    int anc = (s_from <= 0) ? 0 : -1;
+    for (int q = 1; q <= s; q++) {
+        bool inc;
+        bool mv = gfc::advance(i, j, x, y, inc);
+        if (inc) ilb++;
+        if (mv && ilb >= npix) alive = false;
+        if (mv && q >= s_from) anc = q;
     }
-    /* block runs past the end of the pixel: follow advance() exactly */
-    {
-        int ilb = ilb0;
-        bool dead = false;
-        gfc::diag_to_ij(k0, x, y, i, j);
-        for (int s = 0; s < GF_BLOCK; s++) {
-            bool mv = true;
-            if (s > 0 && !dead) {
-                bool inc;
-                mv = gfc::advance(i, j, x, y, inc);
-                if (inc) ilb++;
-                if (mv && ilb >= npix) dead = true;
-            }
-            b.ilb[s] = ilb;
-            b.im[s] = (short)i;
-            b.iM[s] = (short)j;
-            b.moved[s] = mv;
-            b.alive[s] = !dead;
-        }
-    }
+    r.ilb = ilb; r.im = i; r.iM = j; r.alive = alive; r.anchor_s = anc;
+    return r;
 }
 
 /* State of the crawl cursor of one stream, uniform across its warp. */
@@ -182,20 +155,23 @@ __device__ void draw_stars(const CrawlParams &P, int tid, int lane, gfr::Mwc &r,
     ndraw -= todo;
 }
 
-/* The anchor of bin s of a lane's block: the last anchor bin at or before s. */
-__device__ gfc::Anchor anchor_at(const CrawlParams &P, const BlockBins &b, int s, int s_begin, bool carried_ok,
-                                 const gfc::Anchor &carried)
+/* Anchor quantities with the distance taken from the per-model table
+ * D[im][iM] = powf(10, 0.2 DM + 1) (identical to compute_pos, skygen.cu.h:216-229). */
+__device__ __forceinline__ gfc::Anchor anchor(const CrawlParams &P, const gf_pencil_beam &pix, int im, int iM)
 {
-    int sa = s;
-    while (sa > s_begin && !b.moved[sa]) sa--;
-    if (!b.moved[sa] && carried_ok) return carried;
     const SkyModel &m = P.m;
-    float M = m.M1 - (float)b.iM[sa] * m.dM;
-    return gfc::compute_anchor(m, P.g, P.g.pixels[b.ilb[sa]], b.im[sa], M);
+    gfc::Anchor a;
+    a.D = P.Dtab[im * m.nM + iM];
+    a.Am = gfc::beam_extinction(P.g, pix);
+    float x = a.D * pix.cl * pix.cb;
+    float y = a.D * pix.sl * pix.cb;
+    float z = a.D * pix.sb;
+    a.ms = gfc::model_rho(m, x, y, z);
+    return a;
 }
 
 template <int DRAW>
-__device__ void crawl_stream(const CrawlParams &P, const float *lf, int tid, int lane)
+__device__ void crawl_stream(const CrawlParams &P, const float *lf, float *mu_sm, int tid, int lane)
 {
     const SkyModel &m = P.m;
     const int x = m.nm, y = m.nM, kmax = x * y, N = m.nthreads;
@@ -239,164 +215,170 @@ __device__ void crawl_stream(const CrawlParams &P, const float *lf, int tid, int
             draw_stars(P, tid, lane, r, c.ndraw, nstars, limit, c.cur_ilb, c.cur_im, c.cur_iM, c.anc.Am);
             v = r.v();
         }
-        (void)0;
     }
 
     double cnt_sum = 0.0, cov_sum = 0.0;
     bool finished = false;
-    /* per-pixel accumulation (integrate, optional) */
     int pp_ilb = -1;
     double pp_sum = 0.0;
+    const long long step = (long long)GF_BLOCK * N;
 
     while (!(DRAW && c.ndraw)) {
         /* ---------- phase A: bins, anchors and mu of 32 blocks ---------- */
-        const long long step = (long long)GF_BLOCK * N;
         long long kk = (long long)c.blk_k + (long long)lane * step;
-        int my_k = (int)(kk % kmax);
-        int my_q = (int)(kk / kmax);
-        int drift = gfc::block_drift(my_k, x, y);
-        /* exclusive prefix of the drifts */
+        const int my_k = (int)(kk % kmax);
+        const int my_q = (int)(kk / kmax);
+        const int drift = gfc::block_drift(my_k, x, y);
         int dsum = drift;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             int t = __shfl_up_sync(0xffffffffu, dsum, o);
             if (lane >= o) dsum += t;
         }
-        int dexcl = dsum - drift;
-        int dtot = __shfl_sync(0xffffffffu, dsum, 31);
+        const int dexcl = dsum - drift;
+        const int dtot = __shfl_sync(0xffffffffu, dsum, 31);
         long long my_ilb_ll = (long long)c.blk_ilb + my_q + dexcl;
-        int my_ilb = my_ilb_ll > npix ? npix : (int)my_ilb_ll;
-        int s_begin = (lane == 0) ? c.pos : 0;
+        const int my_ilb = my_ilb_ll > npix ? npix : (int)my_ilb_ll;
+        const int s_begin = (lane == 0) ? c.pos : 0;
+        const bool fast = my_k + GF_BLOCK - 1 < kmax;
 
-        BlockBins b;
-        enumerate_block(my_ilb, my_k, x, y, npix, b);
-
-        float mu[GF_BLOCK];
+        /* mu of bin s of this lane at mu_sm[s * 32 + lane] (conflict-free) */
+#define MU(s_) mu_sm[(s_) * 32 + lane]
         gfc::Anchor anc = c.anc;       /* lane 0 inherits the carried anchor */
-        bool have_anc = (lane == 0);
-        bool lane_end = false;         /* the crawl ends within or before this block */
-#pragma unroll
-        for (int s = 0; s < GF_BLOCK; s++) {
-            mu[s] = gfc::cut_marker();
-            if (s < s_begin) continue;
-            if (!b.alive[s]) { lane_end = true; continue; }
-            if (lane_end) continue;
-            float M = m.M1 - (float)b.iM[s] * m.dM;
-            const gf_pencil_beam &pix = P.g.pixels[b.ilb[s]];
-            if (b.moved[s] || !have_anc) {
-                anc = gfc::compute_anchor(m, P.g, pix, b.im[s], M);
-                have_anc = true;
-            }
-            mu[s] = gfc::bin_mu(m, lf, anc, pix.dA, b.im[s], M);
-            if (!DRAW && !gfc::is_cut(mu[s])) {
-                cnt_sum += (double)mu[s];
-                float cov = mu[s] * pix.coveredFraction;
-                cov_sum += (double)cov;
-                if (P.per_pixel) {
-                    if (b.ilb[s] != pp_ilb) {
-                        if (pp_ilb >= 0) atomicAdd(&P.per_pixel[pp_ilb + P.pix_base], pp_sum);
-                        pp_ilb = b.ilb[s];
-                        pp_sum = 0.0;
-                    }
-                    pp_sum += (double)cov;
-                }
-            }
-        }
-        if (my_ilb >= npix) lane_end = true;
-        unsigned end_mask = __ballot_sync(0xffffffffu, lane_end);
-
-        if (!DRAW) {
-            if (end_mask) break;
-            /* next window */
-            long long nk = (long long)c.blk_k + 32LL * step;
-            c.blk_ilb = (int)((long long)c.blk_ilb + nk / kmax + dtot);
-            c.blk_k = (int)(nk % kmax);
-            c.pos = 0;
-            continue;
-        }
-
-        /* ---------- phase B: speculative uniforms ---------- */
-        int cnt = 0;
-#pragma unroll
-        for (int s = 0; s < GF_BLOCK; s++) cnt += gfc::is_cut(mu[s]) ? 0 : 1;
-        int csum = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, csum, o);
-            if (lane >= o) csum += t;
-        }
-        int off = csum - cnt;
-        uint64_t w = jump(v, off, jlo, jhi, a, p);
-        int ev_s = -1;
-        uint64_t w_before = w;
-#pragma unroll
-        for (int s = 0; s < GF_BLOCK; s++) {
-            if (ev_s < 0 && !gfc::is_cut(mu[s])) {
-                uint64_t wb = w;
-                float u = mwc_step(w, a);
-                float mus = mu[s];
-                if (!surely_empty(u, mus)) {
-                    if (mus > 10.f || u > gfm::expf_(-mus)) { ev_s = s; w_before = wb; }
-                }
-            }
-        }
-        unsigned ev_mask = __ballot_sync(0xffffffffu, ev_s >= 0);
-        if (ev_mask == 0) {
-            v = shfl64(w, 31);
-            if (end_mask) { finished = true; break; }
-            long long nk = (long long)c.blk_k + 32LL * step;
-            c.blk_ilb = (int)((long long)c.blk_ilb + nk / kmax + dtot);
-            c.blk_k = (int)(nk % kmax);
-            c.pos = 0;
-            continue;
-        }
-        /* ---------- an event: the first lane with stars ---------- */
-        int f = __ffs(ev_mask) - 1;
-        int es = __shfl_sync(0xffffffffu, ev_s, f);
-        uint64_t vb = shfl64(w_before, f);
-        float emu = __shfl_sync(0xffffffffu, mu[0], f);
-#pragma unroll
-        for (int s = 1; s < GF_BLOCK; s++) {
-            float t = __shfl_sync(0xffffffffu, mu[s], f);
-            if (s == es) emu = t;
-        }
-        int f_ilb = __shfl_sync(0xffffffffu, my_ilb, f);
-        int f_k = __shfl_sync(0xffffffffu, my_k, f);
-        int f_sbeg = (f == 0) ? c.pos : 0;
-        /* the event bin and its anchor, recomputed warp-uniformly */
-        BlockBins fb;
-        enumerate_block(f_ilb, f_k, x, y, npix, fb);
-        gfc::Anchor ea = anchor_at(P, fb, es, f_sbeg, f == 0, c.anc);
-        /* an infinite expected count would never leave the sampler's gamma
-         * reduction loop: report it and end the stream */
-        if (!(emu < 3.0e38f)) {
-            if (lane == 0) atomicOr(P.err, 1ull);
-            finished = true;
-            break;
-        }
-        /* Poisson draw with the state before the event bin's first uniform */
-        r.a = a;
-        r.set_v(vb);
-        c.ndraw = (int)r.poisson(emu);
-        c.cur_ilb = fb.ilb[es];
-        c.cur_im = fb.im[es];
-        c.cur_iM = fb.iM[es];
-        c.anc = ea;
-        /* the cursor moves to the bin after the event */
+        bool lane_end = my_ilb >= npix;
         {
-            long long fk = (long long)c.blk_k + (long long)f * step;
-            int fdrift = __shfl_sync(0xffffffffu, dexcl, f);
-            c.blk_ilb = (int)((long long)c.blk_ilb + fk / kmax + fdrift);
-            c.blk_k = (int)(fk % kmax);
-            c.pos = es + 1;
+            int i = 0, j = 0, ilb = my_ilb;
+            bool dead = lane_end;
+            if (!dead) gfc::diag_to_ij(my_k, x, y, i, j);
+#pragma unroll 1
+            for (int s = 0; s < GF_BLOCK; s++) {
+                bool moved = true;
+                if (s > 0 && !dead) {
+                    if (fast) {
+                        int ni = i + 1, nj = j - 1;
+                        if (nj < 0 || ni >= x) gfc::diag_to_ij(my_k + s, x, y, ni, nj);
+                        i = ni; j = nj;
+                        moved = (i == 0) || (j == y - 1);
+                    } else {
+                        bool inc;
+                        moved = gfc::advance(i, j, x, y, inc);
+                        if (inc) ilb++;
+                        if (moved && ilb >= npix) dead = true;
+                    }
+                }
+                float mus = gfc::cut_marker();
+                if (dead) lane_end = true;
+                if (!dead && s >= s_begin) {
+                    const gf_pencil_beam pix = P.g.pixels[ilb];
+                    if (moved || (s == s_begin && lane != 0)) anc = anchor(P, pix, i, j);
+                    const float M = m.M1 - (float)j * m.dM;
+                    mus = gfc::bin_mu(m, lf, anc, pix.dA, i, M);
+                    if (!DRAW && !gfc::is_cut(mus)) {
+                        cnt_sum += (double)mus;
+                        float cov = mus * pix.coveredFraction;
+                        cov_sum += (double)cov;
+                        if (P.per_pixel) {
+                            if (ilb != pp_ilb) {
+                                if (pp_ilb >= 0) atomicAdd(&P.per_pixel[pp_ilb + P.pix_base], pp_sum);
+                                pp_ilb = ilb;
+                                pp_sum = 0.0;
+                            }
+                            pp_sum += (double)cov;
+                        }
+                    }
+                }
+                if (DRAW) MU(s) = mus;
+            }
         }
-        draw_stars(P, tid, lane, r, c.ndraw, nstars, limit, c.cur_ilb, c.cur_im, c.cur_iM, c.anc.Am);
-        v = r.v();
-        /* the window restarts after the event bin; if ndraw remains the stream pauses */
+        const unsigned end_mask = __ballot_sync(0xffffffffu, lane_end);
+        __syncwarp();
+
+        if (DRAW) {
+            /* ---------- phase B: uniforms, restarted after each bin with stars ---------- */
+            int lane_lo = s_begin;          /* first bin of the lane not yet consumed */
+            for (;;) {
+                int cnt = 0;
+#pragma unroll
+                for (int s = 0; s < GF_BLOCK; s++) cnt += (s >= lane_lo && !gfc::is_cut(MU(s))) ? 1 : 0;
+                int csum = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    int t = __shfl_up_sync(0xffffffffu, csum, o);
+                    if (lane >= o) csum += t;
+                }
+                uint64_t w = jump(v, csum - cnt, jlo, jhi, a, p);
+                int ev_s = -1;
+                uint64_t w_before = w;
+                float ev_mu = 0.f;
+#pragma unroll
+                for (int s = 0; s < GF_BLOCK; s++) {
+                    const float mus = MU(s);
+                    if (ev_s < 0 && s >= lane_lo && !gfc::is_cut(mus)) {
+                        uint64_t wb = w;
+                        float u = mwc_step(w, a);
+                        if (!surely_empty(u, mus)) {
+                            if (mus > 10.f || u > gfm::expf_(-mus)) { ev_s = s; w_before = wb; ev_mu = mus; }
+                        }
+                    }
+                }
+                const unsigned ev_mask = __ballot_sync(0xffffffffu, ev_s >= 0);
+                if (ev_mask == 0) {
+                    v = shfl64(w, 31);
+                    break;
+                }
+                /* the first lane with stars: its bin goes through the reference's sampler */
+                const int f = __ffs(ev_mask) - 1;
+                const int es = __shfl_sync(0xffffffffu, ev_s, f);
+                const uint64_t vb = shfl64(w_before, f);
+                const float emu = __shfl_sync(0xffffffffu, ev_mu, f);
+                const int f_ilb = __shfl_sync(0xffffffffu, my_ilb, f);
+                const int f_k = __shfl_sync(0xffffffffu, my_k, f);
+                const int f_sbeg = (f == 0) ? c.pos : 0;
+                const BinPos eb = bin_at(f_ilb, f_k, es, f_sbeg, x, y, npix);
+                if (!(emu < 3.0e38f)) {
+                    /* an infinite expected count would never leave the sampler's gamma loop */
+                    if (lane == 0) atomicOr(P.err, 1ull);
+                    finished = true;
+                    break;
+                }
+                r.a = a;
+                r.set_v(vb);
+                c.ndraw = (int)r.poisson(emu);
+                c.cur_ilb = eb.ilb;
+                c.cur_im = eb.im;
+                c.cur_iM = eb.iM;
+                const float AmMin = gfc::beam_extinction(P.g, P.g.pixels[eb.ilb]);
+                draw_stars(P, tid, lane, r, c.ndraw, nstars, limit, c.cur_ilb, c.cur_im, c.cur_iM, AmMin);
+                v = r.v();
+                if (c.ndraw) {
+                    /* the table is full: pause right after the event bin, with its anchor */
+                    long long fk = (long long)c.blk_k + (long long)f * step;
+                    const int fdrift = __shfl_sync(0xffffffffu, dexcl, f);
+                    c.blk_ilb = (int)((long long)c.blk_ilb + fk / kmax + fdrift);
+                    c.blk_k = (int)(fk % kmax);
+                    if (eb.anchor_s >= 0) {
+                        const BinPos ab = bin_at(f_ilb, f_k, eb.anchor_s, 0, x, y, npix);
+                        c.anc = anchor(P, P.g.pixels[ab.ilb], ab.im, ab.iM);
+                    }
+                    c.pos = es + 1;
+                    break;
+                }
+                /* continue with the bins after the event */
+                if (lane < f) lane_lo = GF_BLOCK;
+                else if (lane == f) lane_lo = es + 1;
+            }
+            if (finished || c.ndraw) break;
+        }
+#undef MU
+        if (end_mask) { finished = true; break; }
+        /* next window: 32 blocks further */
+        long long nk = (long long)c.blk_k + 32LL * step;
+        c.blk_ilb = (int)((long long)c.blk_ilb + nk / kmax + dtot);
+        c.blk_k = (int)(nk % kmax);
+        c.pos = 0;
     }
 
     if (!DRAW) {
-        /* warp reduction of the partial sums */
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             cnt_sum += __shfl_xor_sync(0xffffffffu, cnt_sum, o);
@@ -427,13 +409,27 @@ template <int DRAW>
 __global__ void __launch_bounds__(128) crawl_kernel(CrawlParams P)
 {
     extern __shared__ float s_lf[];
+    __shared__ float s_mu[128 / 32][GF_BLOCK * 32];
     for (int i = threadIdx.x; i < P.m.lf_n; i += blockDim.x) s_lf[i] = P.m.lf[i];
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int tid = P.stream_begin + warp; tid < P.stream_end; tid += nwarps)
-        crawl_stream<DRAW>(P, s_lf, tid, lane);
+        crawl_stream<DRAW>(P, s_lf, s_mu[threadIdx.x >> 5], tid, lane);
+}
+
+/* D[im][iM] = powf(10, 0.2 DM + 1) with DM = (m0 + im dm) - (M1 - iM dM), skygen.cu.h:219-222 */
+__global__ void dtab_kernel(SkyModel m, float *D)
+{
+    int n = m.nm * m.nM;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        int im = q / m.nM, iM = q - im * m.nM;
+        float M = m.M1 - (float)iM * m.dM;
+        float mm = m.m0 + (float)im * m.dm;
+        float DM = mm - M;
+        D[q] = gfm::powf_(10.f, 0.2f * DM + 1.f);
+    }
 }
 
 /* ------------------------------------------------------------------ */
@@ -598,6 +594,10 @@ __global__ void iota_kernel(uint32_t *idx, int64_t n)
 
 namespace gfk {
 
+static std::atomic<long long> g_launches(0);
+void count_launches(int n) { g_launches += n; }
+long long launches() { return g_launches.load(); }
+
 static int sm_count_cached = 0;
 int sm_count()
 {
@@ -630,6 +630,7 @@ static CrawlParams make_params(const LaunchCrawl &L)
     P.countsCovered = L.countsCovered;
     P.per_pixel = L.per_pixel;
     P.pix_base = L.pix_base;
+    P.Dtab = L.Dtab;
     return P;
 }
 
@@ -644,6 +645,7 @@ cudaError_t launch_crawl(const LaunchCrawl &L, int draw, cudaStream_t s)
     size_t smem = (size_t)L.m.lf_n * sizeof(float);
     if (draw) crawl_kernel<1><<<blocks, threads, smem, s>>>(P);
     else crawl_kernel<0><<<blocks, threads, smem, s>>>(P);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -657,6 +659,7 @@ cudaError_t launch_place(const LaunchPlace &L, cudaStream_t s)
     P.nvis = L.nvis;
     int blocks = (int)std::min<int64_t>((L.n + 255) / 256, (int64_t)sm_count() * 16);
     place_kernel<<<blocks, 256, 0, s>>>(P);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -682,6 +685,7 @@ cudaError_t launch_sort_gather(const LaunchSort &L, cudaStream_t s)
     G.lb = L.lb; G.projIdx = L.projIdx; G.projXY = L.projXY; G.DM = L.DM; G.absmag = L.absmag;
     G.XYZ = L.XYZ; G.Am = L.Am; G.AmInf = L.AmInf; G.comp = L.comp; G.out = L.out;
     gather_kernel<<<blocks, 256, 0, s>>>(G);
+    count_launches(3);     /* iota, tie, gather (the radix sort itself is CUB's) */
     return cudaGetLastError();
 }
 
@@ -710,6 +714,14 @@ __global__ void jump_table_kernel(const uint32_t *mult, int n, uint64_t *lo, uin
         hi[(size_t)s * 32 + l] = h;                       /* a^(32 l - 3) */
         h = gfr::mulmod_generic(h, a32, p);
     }
+}
+
+cudaError_t launch_dtab(const SkyModel &m, float *D, cudaStream_t s)
+{
+    int n = m.nm * m.nM;
+    dtab_kernel<<<(n + 255) / 256, 256, 0, s>>>(m, D);
+    count_launches(1);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_jump_tables(const uint32_t *mult, int n, uint64_t *lo, uint64_t *hi, cudaStream_t s)

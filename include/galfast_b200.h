@@ -234,6 +234,24 @@ gf_status gf_ctx_create(int device, gf_ctx **out);
 gf_status gf_ctx_destroy(gf_ctx *ctx);
 /* Block until all work queued on the context's stream is done. */
 gf_status gf_ctx_sync(gf_ctx *ctx);
+/* Device-side timing on the context's stream: record event `slot` (0..15),
+ * and read the elapsed milliseconds between two recorded slots. */
+gf_status gf_ctx_mark(gf_ctx *ctx, int32_t slot);
+gf_status gf_ctx_elapsed(gf_ctx *ctx, int32_t from, int32_t to, float *ms);
+/* Number of this library's kernels launched by the process so far. */
+int64_t gf_launch_count(void);
+
+/* Per-phase device time (like the reference's kernelRunSwatch, gpu.h:251-254):
+ * when enabled, every kernel phase is bracketed by CUDA events on the context's
+ * stream; gf_profile_read returns the accumulated milliseconds and launch
+ * counts per phase (GF_PROF_*) and resets them. */
+enum {
+    GF_PROF_INTEGRATE = 0, GF_PROF_DRAW_WINDOW = 1, GF_PROF_DRAW_RERUN = 2, GF_PROF_PLACE = 3,
+    GF_PROF_SORT = 4, GF_PROF_CLIPPER = 5, GF_PROF_FEH = 6, GF_PROF_BOND2010 = 7, GF_PROF_PHOTOMETRY = 8,
+    GF_PROF_PHOTOERR = 9, GF_PROF_VEL2PM = 10, GF_PROF_GAL2OTHER = 11, GF_PROF_NPHASES = 12
+};
+gf_status gf_profile_enable(gf_ctx *ctx, int32_t on);
+gf_status gf_profile_read(gf_ctx *ctx, double *ms, int64_t *launches);
 
 /* ---- persistent multiply-with-carry streams (cux.cpp:404-435, cuda_rng.h:466-497) ---- */
 
