@@ -56,6 +56,10 @@ void dev_free(T *&p)
 
 }  // namespace
 
+namespace gfk {
+void set_last_error(const std::string &msg) { g_err = msg; }
+}
+
 struct gf_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;

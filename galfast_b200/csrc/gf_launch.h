@@ -4,6 +4,7 @@
  */
 #pragma once
 #include <cuda_runtime.h>
+#include <string>
 #include "gf_internal.h"
 
 namespace gfk {
@@ -53,6 +54,8 @@ struct LaunchSort {
 };
 
 int sm_count();
+/* set the message returned by gf_last_error() on this thread */
+void set_last_error(const std::string &msg);
 /* count of kernel launches issued by the library (for the benchmark's launch census) */
 void count_launches(int n);
 long long launches();

@@ -372,6 +372,26 @@ typedef int (*gf_batch_callback)(void *user, int32_t model, const gf_table *dev_
 
 gf_status gf_catalog_run(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, void *user, gf_catalog_stats *stats);
 
+/* ---- expected counts without device allocation ---- */
+
+/* Expected star counts of ONE density model over a footprint, computed with
+ * the integrate pass of gf_skygen_integrate but without allocating device
+ * memory: for hosts that own all of the GPU's memory themselves (a framework
+ * with its own arena, or a process that must not call cudaMalloc/cudaFree
+ * while it runs).  No counterpart in the reference: galfast allocates its
+ * buffers itself (skyconfig_impl.h:196-241).
+ *   d_pixels, d_beam_ammin   caller's device buffers (d_beam_ammin may be NULL)
+ *   d_result                 caller's device buffer of 2 doubles: expected, expected within the footprint
+ *   cuda_stream              cudaStream_t to run on (NULL = default stream); synchronised before return
+ * The scratch (per-stream partial sums, LF, distance table) is a fixed 1.3 MB
+ * __device__ array of the library: at most 65536 streams, 1024 LF samples and
+ * 65536 (m, M) bins per pixel; larger requests are rejected with GF_E_INVALID.
+ * The first call on each device looks up the array's address (make it before any
+ * stream capture); calls share the array, so calls that overlap on the GPU race. */
+gf_status gf_skygen_integrate_static(const gf_skygen_config *cfg, const gf_pencil_beam *d_pixels, int32_t npixels,
+                                     const float *d_beam_ammin, const gf_extinction *ext,
+                                     const gf_model_config *model, double *d_result, void *cuda_stream);
+
 /* ---- host-side setup helpers (no GPU needed) ---- */
 
 /* Lambert projection with pole (l0, b0) in degrees (lambert::init, skygen.h:115-120). */
