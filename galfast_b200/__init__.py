@@ -103,6 +103,8 @@ def lib():
         L.gf_multipliers.argtypes = [C.POINTER(C.c_uint32), C.c_int32]
         L.gf_rng_seed_host.argtypes = [C.c_uint32, C.c_int32, C.POINTER(C.c_uint32)]
         L.gf_mt19937_outputs.argtypes = [C.c_uint32, C.c_int, C.POINTER(C.c_uint32)]
+        L.gf_skygen_setup_host.argtypes = [C.POINTER(SkygenConfig), C.c_int32, C.POINTER(ModelConfig), C.c_int32,
+                                           C.POINTER(ModelInfo), C.POINTER(C.c_float)]
         _lib = L
     return _lib
 

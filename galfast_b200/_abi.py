@@ -115,5 +115,6 @@ EXPORTS = [
     "gf_photoerr_create", "gf_photoerr_destroy", "gf_module_photoerrors",
     "gf_module_vel2pm", "gf_module_gal2other",
     "gf_lambert_init", "gf_footprint_pixelize", "gf_photometry_build",
-    "gf_multipliers", "gf_rng_seed_host", "gf_mt19937_outputs",
+    "gf_multipliers", "gf_rng_seed_host", "gf_mt19937_outputs", "gf_skygen_setup_host",
+    "gf_skygen_integrate_static",
 ]

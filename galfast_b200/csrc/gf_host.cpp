@@ -286,6 +286,26 @@ void gf_rng_seed_host(uint32_t seed48, int32_t nstreams, uint32_t *state)
     gfh::seed_streams(seed48, nstreams, gfh::multipliers().data(), state);
 }
 
+/* Host-only model setup (binning, LF resampling, frames, normalisation): the
+ * derived parameters and LF of each model, as gf_skygen_create computes them. */
+gf_status gf_skygen_setup_host(const gf_skygen_config *cfg, int32_t npixels, const gf_model_config *models, int32_t nmodels,
+                               gf_skygen_model_info *info, float *lf /* [nmodels][1024] or NULL */)
+{
+    std::vector<gfh::HostModel> hms;
+    std::string err;
+    if (!cfg || !models || nmodels <= 0 || !info) return GF_E_INVALID;
+    if (!gfh::setup_models(*cfg, npixels, models, nmodels, hms, err)) return GF_E_INVALID;
+    for (int i = 0; i < nmodels; i++) {
+        const SkyModel &m = hms[i].m;
+        gf_skygen_model_info &o = info[i];
+        o.m0 = m.m0; o.m1 = m.m1; o.dm = m.dm; o.M0 = m.M0; o.M1 = m.M1; o.dM = m.dM;
+        o.nm = m.nm; o.nM = m.nM; o.npixels = m.npixels; o.nthreads = m.nthreads;
+        o.f = m.f; o.lf_x0 = m.lf_x0; o.lf_inv_dx = m.lf_inv_dx; o.lf_n = m.lf_n; o.norm = m.norm;
+        if (lf) std::copy(hms[i].lf.begin(), hms[i].lf.end(), lf + (size_t)i * 1024);
+    }
+    return GF_OK;
+}
+
 int gf_multipliers(uint32_t *out, int32_t n)
 {
     if (n < 0 || n > GF_MAX_STREAMS) return GF_E_INVALID;

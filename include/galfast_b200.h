@@ -411,6 +411,9 @@ gf_status gf_footprint_pixelize(const gf_footprint *foot, double dx_deg, const g
 gf_status gf_photometry_build(const double *rows, int32_t nrows, int32_t ncolors, double dFeH, double dMr,
                               float *colors, uint8_t *eflags, int32_t *nFeH, int32_t *nMr,
                               float tcFeH[2], float tcMr[2]);
+/* The model setup of gf_skygen_create on the host alone: info[nmodels], lf[nmodels][1024] (nullable). */
+gf_status gf_skygen_setup_host(const gf_skygen_config *cfg, int32_t npixels, const gf_model_config *models, int32_t nmodels,
+                               gf_skygen_model_info *info, float *lf);
 /* The stream multipliers a_i (safe primes a_i 2^32 - 1, cuda_rng.h:466-497). */
 int gf_multipliers(uint32_t *out, int32_t n);
 /* The seeded stream states [3][nstreams] that gf_rng_init uploads. */

@@ -1323,4 +1323,55 @@ void or_vcyl2pm(const gf_vel2pm_config *par, int n, const double *l_deg, const d
 
 double or_error_normal(uint64_t seed, uint64_t row, uint32_t band) { return error_normal(seed, row, band); }
 
+/* elementary functions of this flavour on arrays (for the accuracy tests):
+ * kind 0 expf, 1 logf, 2 log10f, 3 exp10f, 4 sinf, 5 cosf, 6 tanf, 7 powf(x, y) */
+void or_math_f(int kind, int n, const float *x, const float *y, float *out)
+{
+    for (int i = 0; i < n; i++) {
+        switch (kind) {
+        case 0: out[i] = OR_EXPF(x[i]); break;
+        case 1: out[i] = OR_LOGF(x[i]); break;
+        case 2: out[i] = OR_LOG10F(x[i]); break;
+        case 3: out[i] = OR_EXP10F(x[i]); break;
+        case 4: out[i] = OR_SINF(x[i]); break;
+        case 5: out[i] = OR_COSF(x[i]); break;
+        case 6: out[i] = OR_TANF(x[i]); break;
+        case 7: out[i] = OR_POWF(x[i], y[i]); break;
+        }
+    }
+}
+/* kind 0 exp, 1 log, 2 sin, 3 cos, 4 asin, 5 atan2(x, y) */
+void or_math_d(int kind, int n, const double *x, const double *y, double *out)
+{
+    for (int i = 0; i < n; i++) {
+        switch (kind) {
+        case 0: out[i] = OR_EXP(x[i]); break;
+        case 1: out[i] = OR_LOG(x[i]); break;
+        case 2: out[i] = OR_SIN(x[i]); break;
+        case 3: out[i] = OR_COS(x[i]); break;
+        case 4: out[i] = OR_ASIN(x[i]); break;
+        case 5: out[i] = OR_ATAN2(x[i], y[i]); break;
+        }
+    }
+}
+
+/* the crawl's bin order: diagIndexToIJ of k and advance() from it (skygen.cu.h:257-358) */
+void or_diag(int k, int x, int y, int *i, int *j)
+{
+    int ilb = 0, kk = k;
+    diagIndexToIJ(ilb, *i, *j, kk, x, y);
+}
+int or_advance(int *i, int *j, int x, int y)
+{
+    Launch L = {};
+    gf_pencil_beam pix;
+    int ilb = 0;
+    L.npixels = 1 << 30;
+    std::vector<gf_pencil_beam> dummy(2);
+    L.pixels = dummy.data();
+    L.npixels = 2;
+    bool mv = advance(L, ilb, *i, *j, pix, x, y);
+    return (mv ? 1 : 0) | (ilb ? 2 : 0);
+}
+
 }  /* extern "C" */

@@ -1,0 +1,190 @@
+"""Host logic and the C ABI (CPU only): the library loads and exports every
+function include/galfast_b200.h declares; the safe-prime multipliers are
+regenerated exactly; the portable math library is accurate; the host model
+setup equals the oracle's; the footprint pixelisation has the configurations'
+sizes; and the crawl's bin enumeration is a bijection."""
+import ctypes as C
+import math
+import os
+import re
+
+import numpy as np
+import pytest
+
+import galfast_b200 as G
+from galfast_b200 import workloads as W, _abi as A
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "galfast_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = set(re.findall(r"\b(gf_[a-z0-9_]+)\s*\(", src))
+    return sorted(n for n in names if not n.endswith("_callback"))
+
+
+def test_library_exports_every_declared_function(lib):
+    import subprocess
+    out = subprocess.run(["nm", "-D", "--defined-only", G.LIBPATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (gf_\w+)", out))
+    missing = [n for n in declared_functions() if n not in exported]
+    assert not missing, missing
+    for n in A.EXPORTS:
+        assert n in exported, n
+
+
+def test_struct_layouts():
+    assert C.sizeof(A.PencilBeam) == 48
+    assert C.sizeof(A.Lambert) == 32
+    assert C.sizeof(A.Bond2010Config) == 4 * (4 + 3 * 45 + 12)
+
+
+def test_safeprime_multipliers_are_safe(multipliers):
+    def is_prime(n):
+        if n < 2:
+            return False
+        for p in (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37):
+            if n % p == 0:
+                return n == p
+        d, s = n - 1, 0
+        while d % 2 == 0:
+            d //= 2
+            s += 1
+        for a in (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37):
+            x = pow(a, d, n)
+            if x in (1, n - 1):
+                continue
+            for _ in range(s - 1):
+                x = x * x % n
+                if x == n - 1:
+                    break
+            else:
+                return False
+        return True
+    rng = np.random.default_rng(3)
+    for i in list(rng.integers(0, 65536, size=200)) + [0, 17157, 17158, 54734, 54735, 65535]:
+        a = int(multipliers[i])
+        assert is_prime(a * 2 ** 32 - 1) and is_prime(a * 2 ** 31 - 1), i
+    # the three enumerations: increasing from 1, decreasing below 2^31 and below 2^32
+    assert np.all(np.diff(multipliers[:17158].astype(np.int64)) > 0)
+    assert np.all(np.diff(multipliers[17158:54735].astype(np.int64)) < 0) and multipliers[17158] < 2 ** 31
+    assert np.all(np.diff(multipliers[54735:].astype(np.int64)) < 0) and multipliers[54735] > 2 ** 31
+
+
+@pytest.mark.skipif(not os.path.exists("/root/reference/data/safeprimes32.txt"), reason="reference tree not present")
+def test_safeprime_multipliers_equal_reference_table(multipliers):
+    ref = np.loadtxt("/root/reference/data/safeprimes32.txt", dtype=np.uint64, max_rows=65536)
+    assert np.array_equal(ref[:, 0].astype(np.uint32), multipliers)
+    assert np.array_equal(ref[:, 1], ref[:, 0] * 2 ** 32 - 1)
+
+
+def ulp_diff32(a, b):
+    ai = np.asarray(a, dtype=np.float32).view(np.int32).astype(np.int64)
+    bi = np.asarray(b, dtype=np.float32).view(np.int32).astype(np.int64)
+    ai = np.where(ai < 0, np.int64(-2 ** 31) - ai, ai)
+    bi = np.where(bi < 0, np.int64(-2 ** 31) - bi, bi)
+    return np.abs(ai - bi)
+
+
+def test_portable_math_single_precision():
+    """gf_math.h float functions are correctly rounded (vs float64 numpy) in all but rare cases."""
+    L = O.load("p")
+    rng = np.random.default_rng(11)
+    n = 200000
+    cases = [
+        (0, rng.uniform(-87, 88, n).astype(np.float32), None, lambda x, y: np.exp(x.astype(np.float64))),
+        (1, np.exp(rng.uniform(-80, 80, n)).astype(np.float32), None, lambda x, y: np.log(x.astype(np.float64))),
+        (2, np.exp(rng.uniform(-80, 80, n)).astype(np.float32), None, lambda x, y: np.log10(x.astype(np.float64))),
+        (3, rng.uniform(-37, 37, n).astype(np.float32), None, lambda x, y: 10.0 ** x.astype(np.float64)),
+        (4, rng.uniform(-7, 7, n).astype(np.float32), None, lambda x, y: np.sin(x.astype(np.float64))),
+        (5, rng.uniform(-7, 7, n).astype(np.float32), None, lambda x, y: np.cos(x.astype(np.float64))),
+        (6, rng.uniform(0, 3.1415, n).astype(np.float32), None, lambda x, y: np.tan(x.astype(np.float64))),
+        (7, rng.uniform(0, 100, n).astype(np.float32), rng.uniform(-10, 10, n).astype(np.float32),
+         lambda x, y: x.astype(np.float64) ** y.astype(np.float64)),
+    ]
+    for kind, x, y, ref in cases:
+        yy = y if y is not None else np.zeros_like(x)
+        out = np.zeros_like(x)
+        L.or_math_f(kind, n, x.ctypes.data, yy.ctypes.data, out.ctypes.data)
+        r = ref(x, yy).astype(np.float32)
+        d = ulp_diff32(out, r)
+        assert d.max() <= 1, kind
+        assert (d != 0).mean() < 1e-4, kind
+
+
+def test_portable_math_double_precision():
+    L = O.load("p")
+    rng = np.random.default_rng(12)
+    n = 100000
+    for kind, x, y, ref, tol in [
+        (0, rng.uniform(-700, 700, n), None, np.exp, 2e-16),
+        (1, np.exp(rng.uniform(-700, 700, n)), None, np.log, 1e-15),
+        (2, rng.uniform(-10, 10, n), None, np.sin, 1e-15),
+        (3, rng.uniform(-10, 10, n), None, np.cos, 1e-15),
+        (4, rng.uniform(-1, 1, n), None, np.arcsin, 1e-15),
+        (5, rng.uniform(-1, 1, n), rng.uniform(-1, 1, n), np.arctan2, 1e-15),
+    ]:
+        yy = y if y is not None else np.zeros_like(x)
+        out = np.zeros_like(x)
+        L.or_math_d(kind, n, x.ctypes.data, yy.ctypes.data, out.ctypes.data)
+        r = ref(x, yy) if kind == 5 else ref(x)
+        err = np.abs(out - r) / np.maximum(np.abs(r), 1e-300)
+        assert np.nanmax(err) < 4 * tol + 1e-300, kind
+
+
+def test_host_model_setup_equals_oracle(lib):
+    w = W.config1(lib, with_modules=False)
+    n = len(w.models)
+    info = (G.ModelInfo * n)()
+    lf = np.zeros((n, 1024), dtype=np.float32)
+    marr = (G.ModelConfig * n)(*w.models)
+    assert lib.gf_skygen_setup_host(C.byref(w.sky), w.npixels, marr, n, info,
+                                    lf.ctypes.data_as(C.POINTER(C.c_float))) == 0
+    osk = O.OracleSkygen(w)
+    for i in range(n):
+        oi = osk.info(i)
+        for f in ("m0", "m1", "dm", "M0", "M1", "dM", "nm", "nM", "f", "lf_x0", "lf_inv_dx", "lf_n"):
+            assert getattr(info[i], f) == getattr(oi, f), (i, f)
+        assert np.array_equal(lf[i, :info[i].lf_n], osk.lf(i))
+    # the LF hint restricts the absolute-magnitude grid to the tabulated range (model_lib.h:97-112)
+    assert info[0].nM == 240 and info[0].nm == 120
+
+
+def test_pixelisation_sizes(lib):
+    w1 = W.config1(lib, with_modules=False)
+    assert w1.npixels == 1600
+    pix = np.frombuffer(w1.pixels, dtype=np.float32).reshape(-1, 12)
+    assert np.all(pix[:, 4] == 1.0)                  # fully covered
+    X, Y = pix[:, 8], pix[:, 9]
+    half = 5 * math.pi / 180
+    assert np.all(np.abs(X) < half) and np.all(np.abs(Y) < half)
+    w2 = W.config2(lib, with_modules=False)
+    assert abs(w2.npixels - 3.41e6) / 3.41e6 < 0.01
+    # the screen extinction's beam minimum never exceeds the extinction anywhere in the cell
+    cb = np.frombuffer(w2.pixels, dtype=np.float32).reshape(-1, 12)
+    sb = np.abs(cb[:, 3])
+    assert np.all(w2.ammin <= w2.ext.A0 / sb * (1 + 1e-6))
+
+
+def test_crawl_bin_order_is_a_bijection():
+    """diagIndexToIJ enumerates every (m, M) bin once along diagonals of constant DM,
+    and advance() steps to the next index (skygen.cu.h:231-358)."""
+    L = O.load("p")
+    for x, y in [(7, 5), (5, 7), (6, 6), (1, 4), (4, 1), (12, 31)]:
+        seen = set()
+        for k in range(x * y):
+            i, j = C.c_int(), C.c_int()
+            L.or_diag(k, x, y, C.byref(i), C.byref(j))
+            assert 0 <= i.value < x and 0 <= j.value < y
+            seen.add((i.value, j.value))
+            if k + 1 < x * y:
+                i2, j2 = C.c_int(), C.c_int()
+                L.or_diag(k + 1, x, y, C.byref(i2), C.byref(j2))
+                ii, jj = C.c_int(i.value), C.c_int(j.value)
+                L.or_advance(C.byref(ii), C.byref(jj), x, y)
+                assert (ii.value, jj.value) == (i2.value, j2.value), (x, y, k)
+                assert i2.value + j2.value >= i.value + j.value
+        assert len(seen) == x * y

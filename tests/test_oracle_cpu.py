@@ -1,0 +1,100 @@
+"""Properties of the CPU oracle itself (CPU only, small workloads).
+
+* the portable-math flavour agrees with the libm flavour (the reference's own
+  CPU build) on expected counts to 1e-6 and on the drawn stars up to rare
+  ulp-level differences;
+* batching is transparent when no module consumes the streams between batches:
+  the stars of a many-batch run are exactly the stars of a single-batch run;
+* with Bond2010 consuming the same streams between batches the catalog depends
+  on the batch size, as in the reference (skyconfig_impl.h:445-534);
+* the integrate pass is independent of the crawl's stream count.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import galfast_b200 as G
+from galfast_b200 import workloads as W, _abi as A
+from oracle import oracle as O
+
+
+def patch(lib, half_deg=1.0, **kw):
+    half = half_deg * math.pi / 180
+    foot = A.Footprint()
+    foot.kind = A.GF_FOOT_LAMBERT_RECT
+    foot.proj = 0
+    foot.a, foot.b, foot.c, foot.d = -half, half, -half, half
+    return W.build_workload(lib, foot=foot, dx_deg=0.25, m0=15.0, m1=kw.pop("m1", 20.0), **kw)
+
+
+def collect(w, mult, flavour="p"):
+    rows = []
+    O.run_catalog(w, mult, flavour=flavour, sink=lambda m, t, off: rows.append(t.as_dict(G.SKYGEN_COLUMNS)))
+    return rows
+
+
+def star_set(rows, exact_lb=True):
+    """(comp, l, b, DM, M) of every star; without exact_lb, l and b are rounded to 1e-9 deg
+    (the two math flavours differ in the last bits of asin/atan2)."""
+    keys = []
+    for r in rows:
+        for k in range(len(r["DM"])):
+            l, b = r["lb"][0][k], r["lb"][1][k]
+            if not exact_lb:
+                l, b = round(l, 9), round(b, 9)
+            keys.append((r["comp"][k], l, b, r["DM"][k], r["absmag"][k]))
+    return sorted(keys)
+
+
+def test_flavours_agree(lib, multipliers):
+    w = patch(lib, with_modules=False)
+    p, l = O.OracleSkygen(w, "p"), O.OracleSkygen(w, "l")
+    for m in range(3):
+        ep, _, _ = p.integrate_counts(m)
+        el, _, _ = l.integrate_counts(m)
+        assert ep == pytest.approx(el, rel=1e-6)
+    sp = star_set(collect(w, multipliers, "p"), exact_lb=False)
+    sl = star_set(collect(w, multipliers, "l"), exact_lb=False)
+    assert abs(len(sp) - len(sl)) <= max(3, 1e-3 * len(sp))
+    common = len(set(sp) & set(sl))
+    assert common >= 0.97 * len(sp)
+
+
+def test_batching_is_transparent_without_stream_consumers(lib, multipliers):
+    w1 = patch(lib, with_modules=False, capacity=1 << 16)
+    w2 = patch(lib, with_modules=False, capacity=997)
+    r1, r2 = collect(w1, multipliers), collect(w2, multipliers)
+    assert len(r1) == 3 and len(r2) > len(r1)
+    assert star_set(r1) == star_set(r2)
+
+
+def test_batching_changes_the_catalog_when_bond2010_shares_the_streams(lib, multipliers):
+    """With two streams each holding ~1000 stars, a 1024-row batch stops stream 0 part-way;
+    Bond2010 then draws from streams 0-3 before the crawl resumes, so the rest differs."""
+    w1 = patch(lib, half_deg=2.0, nthreads=2, capacity=1 << 16)
+    w2 = patch(lib, half_deg=2.0, nthreads=2, capacity=1024)
+    r1, r2 = collect(w1, multipliers), collect(w2, multipliers)
+    s1, s2 = set(star_set(r1)), set(star_set(r2))
+    assert len(r2) > len(r1)
+    assert s1 != s2
+    assert len(s1 & s2) > 500        # the stars before the first batch boundary agree
+
+
+def test_expected_counts_do_not_depend_on_the_stream_count(lib):
+    e = []
+    for nthreads in (7680, 333, 64):
+        w = patch(lib, nthreads=nthreads, with_modules=False)
+        sk = O.OracleSkygen(w)
+        e.append([sk.integrate_counts(m)[0] for m in range(3)])
+    np.testing.assert_allclose(e[0], e[1], rtol=1e-12)
+    np.testing.assert_allclose(e[0], e[2], rtol=1e-12)
+
+
+def test_draw_count_is_consistent_with_expectation(lib, multipliers):
+    w = patch(lib, half_deg=2.0, with_modules=False)
+    sk = O.OracleSkygen(w)
+    exp = sum(sk.integrate_counts(m)[0] for m in range(3))
+    st, _ = O.run_catalog(w, multipliers)
+    gen = sum(st["generated"].values())
+    assert abs(gen - exp) < 5 * math.sqrt(exp)
