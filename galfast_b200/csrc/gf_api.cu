@@ -141,17 +141,26 @@ struct gf_skygen {
     void *d_sort_temp = nullptr;
     size_t sort_temp_bytes = 0;
     int nthreads = 0;
+    /* checkpoints of the last speculative window (see gf_skygen_draw) */
+    Checkpoint *d_ck = nullptr;
+    int32_t ck_cap = 0;
+    uint32_t *d_ck_count = nullptr;
+    unsigned long long *d_ck_sel = nullptr;
+    int64_t *d_keep = nullptr;
 };
 
 namespace {
 
 /* CrawlState arrays carved from one allocation */
+size_t crawl_state_bytes(int n) { return (size_t)n * (8 * 4 + 16 + 8) + 256; }
+
 gf_status alloc_crawl_state(int n, CrawlState &st, void **mem)
 {
-    size_t words = (size_t)n * 12 + (size_t)n * 2;   /* 11 int/float fields + one int64 */
-    GF_CUDA(cudaMalloc(mem, words * 4 + 16));
+    GF_CUDA(cudaMalloc(mem, crawl_state_bytes(n)));
     char *p = (char *)*mem;
-    auto take = [&](size_t bytes) { char *r = p; p += bytes; return r; };
+    auto take = [&](size_t bytes) { char *r = p; p += (bytes + 15) & ~(size_t)15; return r; };
+    st.anc = (AnchorX *)take(16 * (size_t)n);
+    st.nstars = (int64_t *)take(8 * (size_t)n);
     st.status = (int32_t *)take(4 * (size_t)n);
     st.blk_ilb = (int32_t *)take(4 * (size_t)n);
     st.blk_k = (int32_t *)take(4 * (size_t)n);
@@ -160,15 +169,8 @@ gf_status alloc_crawl_state(int n, CrawlState &st, void **mem)
     st.cur_ilb = (int32_t *)take(4 * (size_t)n);
     st.cur_im = (int32_t *)take(4 * (size_t)n);
     st.cur_iM = (int32_t *)take(4 * (size_t)n);
-    st.D = (float *)take(4 * (size_t)n);
-    st.Am = (float *)take(4 * (size_t)n);
-    st.ms = (float *)take(4 * (size_t)n);
-    p = (char *)(((uintptr_t)p + 15) & ~(uintptr_t)15);
-    st.nstars = (int64_t *)take(8 * (size_t)n);
     return GF_OK;
 }
-
-size_t crawl_state_bytes(int n) { return (size_t)n * 12 * 4 + (size_t)n * 8 + 16; }
 
 gf_status ensure_rec_capacity(gf_skygen *s, int64_t need, int64_t keep)
 {
@@ -265,7 +267,7 @@ __global__ void copy_state_range(CrawlState dst, CrawlState src, uint32_t *rng_d
     if (i >= b) return;
     dst.status[i] = src.status[i]; dst.blk_ilb[i] = src.blk_ilb[i]; dst.blk_k[i] = src.blk_k[i]; dst.pos[i] = src.pos[i];
     dst.ndraw[i] = src.ndraw[i]; dst.cur_ilb[i] = src.cur_ilb[i]; dst.cur_im[i] = src.cur_im[i]; dst.cur_iM[i] = src.cur_iM[i];
-    dst.D[i] = src.D[i]; dst.Am[i] = src.Am[i]; dst.ms[i] = src.ms[i]; dst.nstars[i] = 0;
+    dst.anc[i] = src.anc[i]; dst.nstars[i] = 0;
     for (int k = 0; k < 3; k++) rng_dst[(size_t)k * dst_pitch + i] = rng_src[(size_t)k * src_pitch + i];
 }
 
@@ -282,7 +284,7 @@ __global__ void restore_tail(CrawlState st, CrawlState snap, uint32_t *rng, int3
     if (i >= n) return;
     st.status[i] = snap.status[i]; st.blk_ilb[i] = snap.blk_ilb[i]; st.blk_k[i] = snap.blk_k[i]; st.pos[i] = snap.pos[i];
     st.ndraw[i] = snap.ndraw[i]; st.cur_ilb[i] = snap.cur_ilb[i]; st.cur_im[i] = snap.cur_im[i]; st.cur_iM[i] = snap.cur_iM[i];
-    st.D[i] = snap.D[i]; st.Am[i] = snap.Am[i]; st.ms[i] = snap.ms[i]; st.nstars[i] = 0;
+    st.anc[i] = snap.anc[i]; st.nstars[i] = 0;
     for (int k = 0; k < 3; k++) rng[(size_t)k * NS + i] = rng_snap[(size_t)k * n + i];
 }
 
@@ -299,14 +301,75 @@ gf_status snapshot_range(gf_skygen *s, ModelState &ms, int a, int b, bool restor
     return GF_OK;
 }
 
-__global__ void filter_records(const StarRecord *in, int64_t n, int32_t stream_end, StarRecord *out, unsigned long long *count)
+/* keep the records of streams before t, and the first keep_t[0] stars of stream t */
+__global__ void filter_records(const StarRecord *in, int64_t n, int32_t t, const int64_t *keep_t, StarRecord *out,
+                               unsigned long long *count)
 {
+    const int64_t kt = *keep_t;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         StarRecord r = in[i];
-        if (r.stream < stream_end) {
+        if (r.stream < t || (r.stream == t && (int64_t)r.seq < kt)) {
             unsigned long long k = atomicAdd(count, 1ull);
             out[k] = r;
         }
+    }
+}
+
+/* ---- checkpoints: resume a stream just before one of its bins with stars ---- */
+__device__ void apply_checkpoint(const Checkpoint &ck, int s, CrawlState st, uint32_t *rng, int32_t NS)
+{
+    st.status[s] = 1;
+    st.blk_ilb[s] = ck.blk_ilb;
+    st.blk_k[s] = ck.blk_k;
+    st.pos[s] = ck.pos;
+    st.ndraw[s] = 0;
+    st.anc[s] = ck.anc;
+    st.nstars[s] = ck.nstars;
+    rng[(size_t)NS + s] = (uint32_t)(ck.v >> 32);
+    rng[2 * (size_t)NS + s] = (uint32_t)ck.v;
+}
+
+/* the latest checkpoint of stream t with at most Lt stars before it */
+__global__ void select_checkpoint(const Checkpoint *ck, const uint32_t *count, int32_t cap, int32_t t, int64_t Lt,
+                                  unsigned long long *sel)
+{
+    const uint32_t n = min(*count, (uint32_t)cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Checkpoint &c = ck[i];
+        if (c.stream == t && (int64_t)c.nstars <= Lt)
+            atomicMax(sel, ((unsigned long long)(c.nstars + 1) << 32) | i);
+    }
+}
+
+/* stream t resumes from its selected checkpoint, or from the window snapshot if it has none;
+ * keep[0] = the number of its stars that stay in the batch */
+__global__ void resume_boundary_stream(const Checkpoint *ck, const unsigned long long *sel, int32_t t, CrawlState st,
+                                       CrawlState snap, uint32_t *rng, int32_t NS, const uint32_t *rng_snap, int32_t N,
+                                       int64_t *keep)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const unsigned long long sv = *sel;
+    if (sv) {
+        const Checkpoint c = ck[(uint32_t)sv];
+        apply_checkpoint(c, t, st, rng, NS);
+        *keep = c.nstars;
+    } else {
+        st.status[t] = snap.status[t]; st.blk_ilb[t] = snap.blk_ilb[t]; st.blk_k[t] = snap.blk_k[t]; st.pos[t] = snap.pos[t];
+        st.ndraw[t] = snap.ndraw[t]; st.cur_ilb[t] = snap.cur_ilb[t]; st.cur_im[t] = snap.cur_im[t]; st.cur_iM[t] = snap.cur_iM[t];
+        st.anc[t] = snap.anc[t]; st.nstars[t] = 0;
+        for (int k = 0; k < 3; k++) rng[(size_t)k * NS + t] = rng_snap[(size_t)k * N + t];
+        *keep = 0;
+    }
+}
+
+/* first batch: streams in (t, w_hi) go back to their first bin with stars */
+__global__ void resume_at_first_star(const Checkpoint *ck, const uint32_t *count, int32_t cap, int32_t t, int32_t w_hi,
+                                     CrawlState st, uint32_t *rng, int32_t NS)
+{
+    const uint32_t n = min(*count, (uint32_t)cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Checkpoint c = ck[i];
+        if (c.stream > t && c.stream < w_hi && c.nstars == 0) apply_checkpoint(c, c.stream, st, rng, NS);
     }
 }
 
@@ -443,7 +506,7 @@ gf_status gf_rng_init(gf_ctx *ctx, uint32_t seed48, int32_t nstreams)
         GF_TRY(dev_alloc(&ctx->d_mult, GF_MAX_STREAMS));
         GF_CUDA(cudaMemcpy(ctx->d_mult, mult.data(), 4 * (size_t)GF_MAX_STREAMS, cudaMemcpyHostToDevice));
         GF_TRY(dev_alloc(&ctx->jt.lo, (size_t)GF_MAX_STREAMS * 32));
-        GF_TRY(dev_alloc(&ctx->jt.hi, (size_t)GF_MAX_STREAMS * 32));
+        GF_TRY(dev_alloc(&ctx->jt.hi, (size_t)GF_MAX_STREAMS * GF_JUMP_HI));
         GF_CUDA(gfk::launch_jump_tables(ctx->d_mult, GF_MAX_STREAMS, ctx->jt.lo, ctx->jt.hi, ctx->stream));
     }
     std::vector<uint32_t> h(3 * (size_t)nstreams);
@@ -549,6 +612,7 @@ gf_status gf_skygen_destroy(gf_skygen *s)
     dev_free(s->d_Am); dev_free(s->d_AmInf);
     dev_free(s->d_key); dev_free(s->d_key2); dev_free(s->d_idx); dev_free(s->d_idx2);
     if (s->d_sort_temp) cudaFree(s->d_sort_temp);
+    dev_free(s->d_ck); dev_free(s->d_ck_count); dev_free(s->d_ck_sel); dev_free(s->d_keep);
     delete s;
     return GF_OK;
 }
@@ -659,6 +723,21 @@ gf_status gf_skygen_draw(gf_skygen *s, int32_t model, gf_table *out, int64_t *n_
     GF_CUDA(cudaMemsetAsync(s->ctx->d_counters, 0, 24, st));
     GF_TRY(ensure_rec_capacity(s, C + C / 2 + 65536, 0));
     const int fb = (N + 255) / 256;
+    /* checkpoints: one at each stream's first bin with stars and one every kCkEvery stars */
+    const int kCkEvery = 64;
+    {
+        const int64_t want = (int64_t)N + (C + C / 2 + 65536) / kCkEvery + 4096;
+        if (want > s->ck_cap) {
+            dev_free(s->d_ck);
+            GF_TRY(dev_alloc(&s->d_ck, (size_t)want));
+            s->ck_cap = (int32_t)want;
+        }
+        if (!s->d_ck_count) {
+            GF_TRY(dev_alloc(&s->d_ck_count, 4));
+            GF_TRY(dev_alloc(&s->d_ck_sel, 1));
+            GF_TRY(dev_alloc(&s->d_keep, 1));
+        }
+    }
 
     /* The batch is filled by streams in stream order (the CPU path runs the
      * emulated threads one after another).  Streams run speculatively in
@@ -690,14 +769,20 @@ gf_status gf_skygen_draw(gf_skygen *s, int32_t model, gf_table *out, int64_t *n_
         GF_TRY(snapshot_range(s, ms, w_lo, w_hi, false));
         for (;;) {
             fill_range<<<fb, 256, 0, st>>>(s->d_limits, N, w_lo, w_hi, room);
+            GF_CUDA(cudaMemsetAsync(s->d_ck_count, 0, 4, st));
             gfk::LaunchCrawl L = crawl_launch(s, ms);
             L.stream_begin = w_lo;
             L.stream_end = w_hi;
+            L.ck = s->d_ck;
+            L.ck_count = s->d_ck_count;
+            L.ck_capacity = s->ck_cap;
+            L.ck_every = kCkEvery;
             {
                 ProfScope ps(s->ctx, GF_PROF_DRAW_WINDOW);
                 GF_CUDA(gfk::launch_crawl(L, 1, st));
             }
             GF_CUDA(cudaMemcpyAsync(s->ctx->h_counters, s->ctx->d_counters, 8, cudaMemcpyDeviceToHost, st));
+            GF_CUDA(cudaMemcpyAsync(s->ctx->h_counters + 4, s->d_ck_count, 4, cudaMemcpyDeviceToHost, st));
             GF_CUDA(cudaMemcpyAsync(s->h_nstars + w_lo, ms.st.nstars + w_lo, 8 * (size_t)(w_hi - w_lo), cudaMemcpyDeviceToHost, st));
             GF_CUDA(cudaStreamSynchronize(st));
             int64_t total = (int64_t)s->ctx->h_counters[0];
@@ -725,21 +810,45 @@ gf_status gf_skygen_draw(gf_skygen *s, int32_t model, gf_table *out, int64_t *n_
         for (int i = ms.first_active; i < N; i++) ms.stream_drawn[i] += s->h_nstars[i];
         ms.first_active = N;
     } else {
-        /* keep the records of streams before t; rerun t with the room left; every
-         * later stream stops at its first star (skygen.cu.h:366-373).  Streams after
-         * the window reached their first star in the first batch already. */
+        /* The batch ends inside stream t: it keeps the stars of the streams before
+         * t and the first C - cum stars of t, and every later stream stops at its
+         * first star (skygen.cu.h:366-373).  Stream t resumes from its latest
+         * checkpoint at or below that count and re-draws only the stars after it;
+         * in the first batch, the later streams of the window resume at their
+         * first bin with stars and the streams after the window run up to theirs. */
         GF_CUDA(cudaMemcpyAsync(s->ctx->h_counters, s->ctx->d_counters, 8, cudaMemcpyDeviceToHost, st));
         GF_CUDA(cudaStreamSynchronize(st));
-        int64_t total = (int64_t)s->ctx->h_counters[0];
+        const int64_t total = (int64_t)s->ctx->h_counters[0];
+        const bool ck_ok = (int64_t)(uint32_t)s->ctx->h_counters[4] <= (int64_t)s->ck_cap;
+        const int64_t Lt = C - cum;
+        const uint32_t NS = (uint32_t)s->ctx->rng_nstreams;
         GF_CUDA(cudaMemsetAsync(s->ctx->d_counters, 0, 8, st));
+        int r_lo = t, r_hi;
+        if (ck_ok) {
+            GF_CUDA(cudaMemsetAsync(s->d_ck_sel, 0, 8, st));
+            select_checkpoint<<<gfk::sm_count() * 4, 256, 0, st>>>(s->d_ck, s->d_ck_count, s->ck_cap, t, Lt, s->d_ck_sel);
+            resume_boundary_stream<<<1, 32, 0, st>>>(s->d_ck, s->d_ck_sel, t, ms.st, ms.snap, s->ctx->d_rng, (int32_t)NS,
+                                                      s->d_rng_snap, N, s->d_keep);
+            if (first_batch) {
+                resume_at_first_star<<<gfk::sm_count() * 4, 256, 0, st>>>(s->d_ck, s->d_ck_count, s->ck_cap, t, w_hi,
+                                                                        ms.st, s->ctx->d_rng, (int32_t)NS);
+                r_hi = N;
+            } else {
+                GF_TRY(snapshot_range(s, ms, t + 1, w_hi, true));
+                r_hi = t + 1;
+            }
+            gfk::count_launches(first_batch ? 3 : 2);
+        } else {
+            GF_TRY(snapshot_range(s, ms, t, w_hi, true));
+            GF_CUDA(cudaMemsetAsync(s->d_keep, 0, 8, st));
+            r_hi = first_batch ? N : w_hi;
+        }
         int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)gfk::sm_count() * 16);
-        if (total > 0) filter_records<<<std::max(blocks, 1), 256, 0, st>>>(s->d_rec, total, t, s->d_rec2, s->ctx->d_counters);
+        if (total > 0) filter_records<<<std::max(blocks, 1), 256, 0, st>>>(s->d_rec, total, t, s->d_keep, s->d_rec2, s->ctx->d_counters);
         std::swap(s->d_rec, s->d_rec2);
-        GF_TRY(snapshot_range(s, ms, t, w_hi, true));
-        const int r_hi = first_batch ? N : w_hi;
-        set_limits<<<fb, 256, 0, st>>>(s->d_limits, N, t, C - cum);
+        set_limits<<<fb, 256, 0, st>>>(s->d_limits, N, t, Lt);
         gfk::LaunchCrawl L = crawl_launch(s, ms);
-        L.stream_begin = t;
+        L.stream_begin = r_lo;
         L.stream_end = r_hi;
         {
             ProfScope ps(s->ctx, GF_PROF_DRAW_RERUN);
@@ -751,7 +860,7 @@ gf_status gf_skygen_draw(gf_skygen *s, int32_t model, gf_table *out, int64_t *n_
         if (nbatch != C) return fail(GF_E_CUDA, "batch rerun produced an unexpected star count");
         generated_all = false;
         for (int i = ms.first_active; i < t; i++) ms.stream_drawn[i] += s->h_nstars[i];
-        ms.stream_drawn[t] += C - cum;
+        ms.stream_drawn[t] += Lt;
         ms.first_active = t;
     }
     GF_CUDA(cudaMemcpy(s->ctx->h_counters + 2, s->ctx->d_counters + 2, 8, cudaMemcpyDeviceToHost));

@@ -41,6 +41,56 @@ __device__ __forceinline__ void diag_to_ij(int k, const int x, const int y, int 
     j = d - i;
 }
 
+/* diag_to_ij with the divisions of the middle region done by FastDiv. */
+__device__ __forceinline__ void diag_to_ij_fast(int k, const int x, const int y, const FastDiv &fx, const FastDiv &fy,
+                                                int &i, int &j)
+{
+    int l = x < y ? x : y;
+    int m = x < y ? y : x;
+    int d;
+    if (2 * k < l * (l - 1)) {
+        d = int(0.5 * (double)(sqrtf((float)(1 + 8 * k)) - 1));
+        i = k - d * (d + 1) / 2;
+    } else if (2 * k < l * (2 * m + 1 - l)) {
+        if (x >= y) {
+            int ka = k - y * (y - 1) / 2;
+            int q = (int)((__umulhi((uint32_t)ka, fy.mul) + (uint32_t)ka) >> fy.shift);
+            d = q + (y - 1);
+            i = (ka - q * y) + d - (y - 1);
+        } else {
+            int ka = k - x * (x - 1) / 2;
+            int q = (int)((__umulhi((uint32_t)ka, fx.mul) + (uint32_t)ka) >> fx.shift);
+            d = q + (x - 1);
+            i = ka - q * x;
+        }
+    } else {
+        int ka = x * y - k - 1;
+        int dd = int(0.5 * (double)(sqrtf((float)(1 + 8 * ka)) - 1));
+        d = (x + y - 2) - dd;
+        i = (x - 1) - (ka - dd * (dd + 1) / 2);
+    }
+    j = d - i;
+}
+
+/* One step along the bin order inside a pixel: the next bin on the diagonal,
+ * or the first bin of the next diagonal d+1 = i+j+1, which starts at
+ * i = max(0, d+1 - (y-1)) (the same successor advance() computes, minus the
+ * pixel change).  Returns whether a new diagonal starts. */
+__device__ __forceinline__ bool step_in_pixel(int &i, int &j, const int x, const int y)
+{
+    int ni = i + 1, nj = j - 1;
+    bool wrap = (nj < 0) | (ni >= x);
+    if (wrap) {
+        int d1 = i + j + 1;
+        ni = d1 - (y - 1);
+        ni = ni > 0 ? ni : 0;
+        nj = d1 - ni;
+    }
+    i = ni;
+    j = nj;
+    return wrap;
+}
+
 /* advance (skygen.cu.h:307-358) without the pixel reload: returns whether the
  * step moved to a new diagonal; *pix_inc is set when the pixel index grows. */
 __device__ __forceinline__ bool advance(int &i, int &j, const int x, const int y, bool &pix_inc)
@@ -82,23 +132,22 @@ __device__ __forceinline__ int block_drift(int k0, const int x, const int y)
 
 /* Anchor quantities of a bin (compute_pos + Model::setpos, skygen.cu.h:216-229,
  * model_expDisk.h:71-115, model_powerLawEllipsoid.h:60-99). */
-struct Anchor {
-    float D, Am, ms;
-};
-
 __device__ __forceinline__ float beam_extinction(const SkyGeom &g, const gf_pencil_beam &pix)
 {
     if (g.ext_kind == GF_EXT_NONE || g.ammin == nullptr) return 0.f;
     return g.ammin[pix.extIdx];
 }
 
+/* Model density at the heliocentric position (x, y, z); MODEL is the
+ * compile-time model kind (GF_MODEL_EXP_DISK or GF_MODEL_POWER_LAW_ELLIPSOID). */
+template <int MODEL>
 __device__ __forceinline__ float model_rho(const SkyModel &m, float x, float y, float z)
 {
     float vx = x + m.T[0], vy = y + m.T[1], vz = z + m.T[2];
     float wx = m.M[0] * vx + m.M[1] * vy + m.M[2] * vz;
     float wy = m.M[3] * vx + m.M[4] * vy + m.M[5] * vz;
     float wz = m.M[6] * vx + m.M[7] * vy + m.M[8] * vz;
-    if (m.type == GF_MODEL_EXP_DISK) {
+    if (MODEL == GF_MODEL_EXP_DISK) {
         float r2 = wx * wx + wy * wy;
         if (m.r_cut2 != 0.f && r2 + wz * wz > m.r_cut2) return 0.f;
         float r = sqrtf(r2);
@@ -112,17 +161,34 @@ __device__ __forceinline__ float model_rho(const SkyModel &m, float x, float y, 
     }
 }
 
-__device__ __forceinline__ Anchor compute_anchor(const SkyModel &m, const SkyGeom &g, const gf_pencil_beam &pix, int im, float M)
+/* Distance of the bin (im, iM): DM = (m0 + im dm) - (M1 - iM dM), D = powf(10, 0.2 DM + 1)
+ * (skygen.cu.h:219-222).  After advance() leaves a pixel the reference keeps
+ * crawling with im >= nm ("garbage" bins of a block that straddles two pixels);
+ * those are evaluated directly instead of from the table. */
+__device__ __forceinline__ float bin_distance(const SkyModel &m, const float *Dtab, int im, int iM)
 {
-    Anchor a;
-    float mm = m.m0 + (float)im * m.dm;
-    float DM = mm - M;
-    a.D = gfm::powf_(10.f, 0.2f * DM + 1.f);
-    a.Am = beam_extinction(g, pix);
-    float x = a.D * pix.cl * pix.cb;
-    float y = a.D * pix.sl * pix.cb;
-    float z = a.D * pix.sb;
-    a.ms = model_rho(m, x, y, z);
+    if ((unsigned)im < (unsigned)m.nm && (unsigned)iM < (unsigned)m.nM) return Dtab[im * m.nM + iM];
+    const float M = m.M1 - (float)iM * m.dM;
+    const float mm = m.m0 + (float)im * m.dm;
+    return gfm::powf_(10.f, 0.2f * (mm - M) + 1.f);
+}
+
+/* Anchor quantities in the per-bin form (AnchorX) for the bin (ilb, im, iM). */
+template <int MODEL>
+__device__ __forceinline__ AnchorX anchor_x(const SkyModel &m, const SkyGeom &g, const float *Dtab, int ilb, int im, int iM)
+{
+    const gf_pencil_beam pix = g.pixels[ilb];
+    AnchorX a;
+    const float D = bin_distance(m, Dtab, im, iM);
+    const float Am = beam_extinction(g, pix);
+    float x = D * pix.cl * pix.cb;
+    float y = D * pix.sl * pix.cb;
+    float z = D * pix.sb;
+    a.ms = model_rho<MODEL>(m, x, y, z);
+    const bool dcut = (m.dmin != 0.f || m.dmax != 0.f) && (m.dmin > D || m.dmax <= D);
+    a.Am = dcut ? __int_as_float(0x7f800000) : Am;
+    a.D3 = D * D * D;
+    a.K = pix.dA * GF_POGSON * m.dm * m.dM;
     return a;
 }
 
@@ -140,18 +206,15 @@ __device__ __forceinline__ float lf_sample(const SkyModel &m, const float *lf, f
 __device__ __forceinline__ float cut_marker() { return __int_as_float(0x7fc0dead); }
 __device__ __forceinline__ bool is_cut(float mu) { return __float_as_int(mu) == 0x7fc0dead; }
 
-/* Expected count of a bin, or the cut marker if the bin is cut (skygen.cu.h:551-565). */
-__device__ __forceinline__ float bin_mu(const SkyModel &m, const float *lf, const Anchor &a, float dA, int im, float M)
+/* Expected count of a bin from its anchor, the LF value at its absolute
+ * magnitude and m0 + dm*im (the two per-model tables), or the cut marker. */
+__device__ __forceinline__ float bin_mu_x(const AnchorX &a, float lfv, float mrow, float norm, float m1)
 {
-    if ((m.dmin != 0.f || m.dmax != 0.f) && (m.dmin > a.D || m.dmax <= a.D)) return cut_marker();
-    float mm = m.m0 + m.dm * (float)im + a.Am;
-    if (mm > m.m1) return cut_marker();
-    float rho = lf_sample(m, lf, M) * a.ms;
-    rho *= m.norm;
-    rho *= a.D * a.D * a.D;
-    rho *= dA * GF_POGSON * m.dm * m.dM;
-    return rho;
+    float rho = lfv * a.ms;
+    rho *= norm;
+    rho *= a.D3;
+    rho *= a.K;
+    return (mrow + a.Am > m1) ? cut_marker() : rho;
 }
-
 
 }  // namespace gfc

@@ -38,11 +38,22 @@ struct SkyGeom {
 
 /* A star drawn by the crawl, to be placed by the star kernel. */
 struct StarRecord {
-    int32_t stream;
+    int32_t stream;                /* crawl stream; (request << 16) | stream in a multi-request launch */
     int32_t ilb;                   /* pixel */
     int16_t im, iM;                /* bin */
-    float AmMin;                   /* beam extinction at the bin's anchor */
+    int32_t seq;                   /* ordinal of the star among its stream's stars in this batch */
     float u[4];                    /* uniforms x, y, M, m (u[2..3] = 0 if hidden by x^2+y^2>2) */
+};
+
+/* Anchor quantities of a bin in the form the per-bin loop consumes:
+ *   Am  beam extinction, or +inf when the anchor's distance is outside [dmin, dmax)
+ *   ms  model density at the anchor position
+ *   D3  D*D*D
+ *   K   dA * POGSON * dm * dM of the anchor's pixel
+ * so that mu = ((((LF(M) * ms) * norm) * D3) * K), cut when m + Am > m1
+ * (skygen.cu.h:551-565, the same float operations in the same order). */
+struct AnchorX {
+    float Am, ms, D3, K;
 };
 
 /* Per-stream crawl state (structure of arrays over the crawl streams).
@@ -55,13 +66,45 @@ struct CrawlState {
     int32_t *pos;                  /* next bin within the current block, 0..10 */
     int32_t *ndraw;                /* stars still to draw for the last processed bin */
     int32_t *cur_ilb, *cur_im, *cur_iM;   /* last processed bin */
-    float *D, *Am, *ms;            /* anchor of the last processed bin */
+    AnchorX *anc;                  /* anchor in effect at the cursor */
     int64_t *nstars;               /* stars drawn by the stream in the current batch */
 };
 
-/* Multiplier tables for jump-ahead: for stream s, lane l holds
- * a^(l-3) mod p and a^(32 l - 3) mod p (scaled multipliers of gfr::mwc_mulmod_scaled). */
+/* Resumable position of a stream just before one of its bins with stars:
+ * restarting the crawl from it replays that bin's Poisson draw. */
+struct Checkpoint {
+    int32_t stream;                /* as StarRecord::stream */
+    int32_t nstars;                /* stars the stream had drawn in the batch before this bin */
+    int32_t blk_ilb, blk_k, pos;   /* cursor: block start pixel, block start index, bin in block */
+    int32_t pad;
+    AnchorX anc;                   /* anchor in effect at the bin */
+    uint64_t v;                    /* stream state c*2^32 + x before the bin's first uniform */
+};
+
+/* Division by a loop-invariant divisor d >= 1 for numerators below 2^31:
+ * n / d = (umulhi(n, mul) + n) >> shift with shift = ceil(log2 d) and
+ * mul = floor(2^32 (2^shift - d) / d) + 1 (Granlund and Montgomery, "Division
+ * by invariant integers using multiplication", 1994, the round-up variant). */
+struct FastDiv {
+    uint32_t d, mul, shift;
+};
+
+static inline FastDiv make_fastdiv(uint32_t d)
+{
+    FastDiv f;
+    f.d = d;
+    uint32_t s = 0;
+    while ((1ull << s) < (unsigned long long)d) s++;
+    f.shift = s;
+    f.mul = (uint32_t)((((1ull << 32) * ((1ull << s) - d)) / d) + 1);
+    return f;
+}
+
+/* Multiplier tables for jump-ahead: for stream s, lo[s][l] = a^(l-3) mod p
+ * (l < 32) and hi[s][h] = a^(32 h - 3) mod p (h < 64), the scaled multipliers
+ * of gfr::mwc_mulmod_scaled; two products jump any distance below 2048. */
+#define GF_JUMP_HI 64
 struct JumpTables {
     uint64_t *lo;                  /* [nstreams][32] */
-    uint64_t *hi;                  /* [nstreams][32] */
+    uint64_t *hi;                  /* [nstreams][GF_JUMP_HI] */
 };

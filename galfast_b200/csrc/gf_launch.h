@@ -25,6 +25,9 @@ struct LaunchCrawl {
     double *counts, *countsCovered, *per_pixel;
     int32_t pix_base;
     const float *Dtab;
+    Checkpoint *ck;                /* draw: checkpoints at the first bin with stars and every ck_every stars */
+    uint32_t *ck_count;
+    int32_t ck_capacity, ck_every;
 };
 
 struct LaunchPlace {

@@ -32,9 +32,11 @@ namespace gfr {
 
 struct Mwc {
     uint32_t a, c, x;
+    uint32_t used;          /* uniforms drawn since the caller last cleared it */
 
     GFR_HD float uniform()
     {
+        used++;
         uint64_t t = (uint64_t)a * x + c;
         c = (uint32_t)(t >> 32);
         x = (uint32_t)t;

@@ -8,18 +8,23 @@
  *
  * Parallel layout.  The reference runs one thread per RNG stream; each stream
  * crawls blocks of 10 consecutive diagonal bins, jumping 10*nthreads bins
- * ahead between blocks.  Here one warp owns one stream and lane l owns block
- * j+l of it: the bin enumeration, the per-diagonal anchor (distance, extinction,
- * model density) and each bin's expected count mu are evaluated for 32 blocks
- * (320 bins) at once.  Only the uniforms are sequential: the MWC stream is a
- * Lehmer generator modulo its safe prime, so lane l jumps directly to the
- * uniform its first bin would consume if every earlier bin drew zero stars
- * (two 128-bit modular multiplications), then walks its block with plain MWC
- * steps.  The first lane that finds a bin with stars ("event": u > exp(-mu),
- * or mu > 10) hands that bin to the whole warp, which runs the reference's
- * Poisson sampler and star draws sequentially, and the window restarts right
- * after it.  Results are bin-for-bin and draw-for-draw those of the reference
- * CPU path.
+ * ahead between blocks.  Here one CTA of 4 warps owns one stream and thread L
+ * owns block j+L of it, a window of 128 blocks (1280 bins):
+ *   pass 1  each thread lists the anchor bins of its block (block start and
+ *           diagonal starts); the warp evaluates them compacted, one anchor
+ *           per lane (distance, extinction, model density: the expensive part);
+ *   pass 2  each thread computes the expected count mu of its 10 bins from
+ *           the anchors and two per-model shared-memory tables (LF at each
+ *           absolute-magnitude row, m at each apparent-magnitude row);
+ *   phase B only the uniforms are sequential: the MWC stream is a Lehmer
+ *           generator modulo its safe prime, so thread L jumps directly to the
+ *           uniform its first bin would consume if every earlier bin drew zero
+ *           stars (two 128-bit modular multiplications) and walks its block with
+ *           plain MWC steps.  The first thread that finds a bin with stars
+ *           (u > exp(-mu), or mu > 10) hands the bin to its warp, which runs the
+ *           reference's Poisson sampler and star draws, and the window restarts
+ *           right after it.
+ * Results are bin-for-bin and draw-for-draw those of the reference CPU path.
  */
 #include "gf_crawl.cuh"
 #include "gf_rng.h"
@@ -28,31 +33,58 @@
 
 namespace gfk {
 
-struct CrawlParams {
+/* One model crawl of one request: everything the CTA of a stream needs. */
+struct CrawlJob {
     SkyModel m;
     SkyGeom g;
     CrawlState st;
     uint32_t *rng;                 /* persistent stream state [3][rng_nstreams] */
     int32_t rng_nstreams;
-    JumpTables jt;
-    int32_t stream_begin, stream_end;
+    int32_t pix_base;              /* first pixel of this launch within the generator's pixel list */
     const int64_t *limits;         /* per-stream star limit for this launch (draw) */
+    double *counts, *countsCovered;   /* integrate outputs, per stream */
+    double *per_pixel;             /* integrate output, per pixel (optional) */
+    const float *Dtab;             /* distances D[im][iM] of the model's bins */
+    FastDiv fx, fy;                /* division by nm and by nM */
+    int32_t job_id;                /* bits 16.. of StarRecord::stream */
+    int32_t pad;
+};
+
+struct CrawlParams {
+    CrawlJob job0;                 /* the job of a single-request launch */
+    const CrawlJob *jobs;          /* multi-request launch: device job table, or null */
+    const uint32_t *items;         /* multi-request launch: (job << 16) | stream per CTA item */
+    int32_t nitems;                /* streams (CTA items) in the launch */
+    int32_t stream_begin;          /* single-request launch: stream of item 0 */
+    JumpTables jt;
     StarRecord *rec;
     int64_t rec_capacity;
     unsigned long long *rec_count;
     unsigned long long *err;       /* set when a bin's expected count is infinite */
-    /* integrate outputs */
-    double *counts, *countsCovered;
-    double *per_pixel;
-    int32_t pix_base;              /* first pixel of this launch within the generator's pixel list */
-    const float *Dtab;             /* distances D[im][iM] of the model's bins */
+    Checkpoint *ck;                /* draw: checkpoint buffer, or null */
+    uint32_t *ck_count;
+    int32_t ck_capacity, ck_every;
 };
+
+#define GF_CW 4                    /* warps per stream */
+#define GF_WIN (GF_CW * 32)        /* blocks of a stream evaluated together (one per thread) */
+#define FULLMASK 0xffffffffu
 
 __device__ __forceinline__ uint64_t shfl64(uint64_t v, int src)
 {
-    uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)v, src);
-    uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(v >> 32), src);
+    uint32_t lo = __shfl_sync(FULLMASK, (uint32_t)v, src);
+    uint32_t hi = __shfl_sync(FULLMASK, (uint32_t)(v >> 32), src);
     return ((uint64_t)hi << 32) | lo;
+}
+
+__device__ __forceinline__ int warp_incl_scan(int v, int lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(FULLMASK, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
 }
 
 /* One MWC step on the combined state v = c*2^32 + x. */
@@ -63,13 +95,13 @@ __device__ __forceinline__ float mwc_step(uint64_t &v, uint32_t a)
     return GF_MWC_SCALE * (float)(uint32_t)t;
 }
 
-/* v * a^n mod p for 0 <= n < 1024 using the lane-held scaled powers. */
-__device__ __forceinline__ uint64_t jump(uint64_t v, int n, uint64_t jlo, uint64_t jhi, uint32_t a, uint64_t p)
+/* v * a^n mod p for 0 <= n < 2048 from the stream's scaled powers
+ * lo[l] = a^(l-3) and hi[h] = a^(32 h - 3) (L1-resident, 768 bytes per stream). */
+__device__ __forceinline__ uint64_t jump(uint64_t v, int n, const uint64_t *lo, const uint64_t *hi, uint32_t a)
 {
-    uint64_t ml = shfl64(jlo, n & 31);
-    uint64_t mh = shfl64(jhi, (n >> 5) & 31);
-    uint64_t w = gfr::mwc_mulmod_scaled(ml, v, a, p);
-    return gfr::mwc_mulmod_scaled(mh, w, a, p);
+    const uint64_t p = ((uint64_t)a << 32) - 1;
+    const uint64_t w = gfr::mwc_mulmod_scaled(__ldg(lo + (n & 31)), v, a, p);
+    return gfr::mwc_mulmod_scaled(__ldg(hi + (n >> 5)), w, a, p);
 }
 
 /* Lower bound of expf(-mu) used to accept "no star" without evaluating expf:
@@ -81,62 +113,100 @@ __device__ __forceinline__ bool surely_empty(float u, float mu)
 
 /* The bin at position s of the block starting at local index k0 in pixel ilb0,
  * by following advance() from the block start (skygen.cu.h:307-358).  Also
- * returns whether the bin is alive (the crawl has not left the last pixel) and
- * the last anchor bin at or after position s_from (-1 if none). */
+ * returns the last anchor bin at or after position s_from (-1 if none). */
 struct BinPos {
     int ilb, im, iM;
-    bool alive;
     int anchor_s;
 };
 
-__device__ BinPos bin_at(int ilb0, int k0, int s, int s_from, int x, int y, int npix)
+__device__ BinPos bin_at(int ilb0, int k0, int s, int s_from, int x, int y)
 {
     BinPos r;
     int i, j;
     gfc::diag_to_ij(k0, x, y, i, j);
     int ilb = ilb0;
-    bool alive = ilb0 < npix;
     int anc = (s_from <= 0) ? 0 : -1;
     for (int q = 1; q <= s; q++) {
         bool inc;
         bool mv = gfc::advance(i, j, x, y, inc);
         if (inc) ilb++;
-        if (mv && ilb >= npix) alive = false;
         if (mv && q >= s_from) anc = q;
     }
-    r.ilb = ilb; r.im = i; r.iM = j; r.alive = alive; r.anchor_s = anc;
+    r.ilb = ilb; r.im = i; r.iM = j; r.anchor_s = anc;
     return r;
 }
 
-/* State of the crawl cursor of one stream, uniform across its warp. */
+/* Crawl cursor of one stream, identical in every thread of its CTA. */
 struct Cursor {
     int blk_ilb, blk_k, pos;
     int ndraw;
     int cur_ilb, cur_im, cur_iM;
-    gfc::Anchor anc;
+    AnchorX anc;
 };
 
-/* Draw up to ndraw stars of the bin (ilb, im, M) while the stream is under its
- * limit (draw_stars, skygen.cu.h:366-457); uniforms are recorded for the
- * placement kernel.  Executed identically by all lanes; lane 0 writes. */
-__device__ void draw_stars(const CrawlParams &P, int tid, int lane, gfr::Mwc &r, int &ndraw, int64_t &nstars,
-                           int64_t limit, int ilb, int im, int iM, float AmMin)
+#define GF_RECBUF 64               /* star records staged in shared memory per stream */
+
+template <int DRAW>
+struct CrawlSmem {
+    CrawlJob job;
+    float4 slot[GF_WIN * GF_BLOCK];           /* anchor inputs (pixel, i<<16|j), then AnchorX; thread L owns [10L, 10L+10) */
+    uint16_t dense[GF_WIN * GF_BLOCK];        /* compacted list of the window's anchor slots */
+    float mu[DRAW ? GF_CW : 1][GF_BLOCK][32]; /* mu of bin s of each thread's block */
+    StarRecord recbuf[DRAW ? GF_RECBUF : 1];
+    int nrec;
+    int wtot[GF_CW];
+    int wev[GF_CW];
+    int scan[GF_CW];
+    unsigned long long v_end;
+    /* stream state shared by the CTA; written by one thread between barriers */
+    Cursor cur;
+    unsigned long long v;
+    unsigned long long mult;       /* scaled a^(k-1) after a bin with stars that drew k uniforms */
+    long long nstars, limit;
+    int next_ck, flag, fL, es;
+    double red[2][GF_CW];
+};
+
+/* Write the staged star records to the global buffer (one warp, all lanes). */
+template <int DRAW>
+__device__ void flush_records(const CrawlParams &P, CrawlSmem<DRAW> &S, int lane)
+{
+    __syncwarp();
+    const int n = S.nrec;
+    if (n == 0) return;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(P.rec_count, (unsigned long long)n);
+    base = __shfl_sync(FULLMASK, base, 0);
+    for (int q = lane; q < n; q += 32) {
+        const unsigned long long slot = base + q;
+        if (slot < (unsigned long long)P.rec_capacity) P.rec[slot] = S.recbuf[q];
+    }
+    __syncwarp();
+    if (lane == 0) S.nrec = 0;
+    __syncwarp();
+}
+
+/* Draw up to ndraw stars of the bin (ilb, im, iM) while the stream is under its
+ * limit (draw_stars, skygen.cu.h:366-457); the uniforms are staged as star
+ * records for the placement kernel.  Executed identically by all lanes of one
+ * warp; lane 0 writes. */
+template <int DRAW>
+__device__ void draw_stars(const CrawlParams &P, CrawlSmem<DRAW> &S, int sid, int lane, gfr::Mwc &r, int &ndraw,
+                           long long &nstars, long long limit, int ilb, int im, int iM)
 {
     if (!ndraw) return;
-    int64_t room = limit - nstars;
-    int todo = (int)(room < (int64_t)ndraw ? (room > 0 ? room : 0) : ndraw);
+    const CrawlJob &J = S.job;
+    long long room = limit - nstars;
+    int todo = (int)(room < (long long)ndraw ? (room > 0 ? room : 0) : ndraw);
     if (todo <= 0) return;
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(P.rec_count, (unsigned long long)todo);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    const gf_pencil_beam pix = P.g.pixels[ilb];
+    const gf_pencil_beam pix = J.g.pixels[ilb];
     for (int n = 0; n < todo; n++) {
         StarRecord rec;
-        rec.stream = tid;
-        rec.ilb = ilb + P.pix_base;
+        rec.stream = sid;
+        rec.ilb = ilb + J.pix_base;
         rec.im = (short)im;
         rec.iM = (short)iM;
-        rec.AmMin = AmMin;
+        rec.seq = (int32_t)(nstars + n);
         rec.u[0] = r.uniform();
         rec.u[1] = r.uniform();
         float x = pix.X, y = pix.Y;
@@ -148,275 +218,515 @@ __device__ void draw_stars(const CrawlParams &P, int tid, int lane, gfr::Mwc &r,
             rec.u[2] = r.uniform();
             rec.u[3] = r.uniform();
         }
-        unsigned long long slot = base + n;
-        if (lane == 0 && slot < (unsigned long long)P.rec_capacity) P.rec[slot] = rec;
+        __syncwarp();
+        const int k = S.nrec;
+        __syncwarp();
+        if (lane == 0) { S.recbuf[k] = rec; S.nrec = k + 1; }
+        if (k + 1 == GF_RECBUF) flush_records(P, S, lane);
     }
     nstars += todo;
     ndraw -= todo;
 }
 
-/* Anchor quantities with the distance taken from the per-model table
- * D[im][iM] = powf(10, 0.2 DM + 1) (identical to compute_pos, skygen.cu.h:216-229). */
-__device__ __forceinline__ gfc::Anchor anchor(const CrawlParams &P, const gf_pencil_beam &pix, int im, int iM)
+__device__ __forceinline__ AnchorX ax_from(const float4 t) { AnchorX a; a.Am = t.x; a.ms = t.y; a.D3 = t.z; a.K = t.w; return a; }
+
+template <int MODEL>
+__device__ __noinline__ AnchorX anchor_cold(const SkyModel &m, const SkyGeom &g, const float *Dtab, int ilb, int im, int iM)
 {
-    const SkyModel &m = P.m;
-    gfc::Anchor a;
-    a.D = P.Dtab[im * m.nM + iM];
-    a.Am = gfc::beam_extinction(P.g, pix);
-    float x = a.D * pix.cl * pix.cb;
-    float y = a.D * pix.sl * pix.cb;
-    float z = a.D * pix.sb;
-    a.ms = gfc::model_rho(m, x, y, z);
-    return a;
+    return gfc::anchor_x<MODEL>(m, g, Dtab, ilb, im, iM);
 }
 
-template <int DRAW>
-__device__ void crawl_stream(const CrawlParams &P, const float *lf, float *mu_sm, int tid, int lane)
+/* Non-surely-empty bins: the exact test of the reference's sampler, u > exp(-mu)
+ * or mu > 10 (the branch that does not compare with exp(-mu) at all). */
+__device__ __noinline__ bool has_stars(float u, float mu)
 {
-    const SkyModel &m = P.m;
-    const int x = m.nm, y = m.nM, kmax = x * y, N = m.nthreads;
-    const int npix = P.g.npixels;
-    const CrawlState &st = P.st;
+    return mu > 10.f || u > gfm::expf_(-mu);
+}
 
-    Cursor c;
-    int status = DRAW ? st.status[tid] : 0;
-    if (status == 2) return;
-    if (status == 0) {
-        long long k = (long long)GF_BLOCK * tid;
-        c.blk_ilb = (int)(k / kmax);
-        c.blk_k = (int)(k % kmax);
-        c.pos = 0;
-        c.ndraw = 0;
-        c.cur_ilb = c.cur_im = c.cur_iM = 0;
-        c.anc.D = c.anc.Am = c.anc.ms = 0.f;
+/* A bin with stars found by phase B: thread fL = 32 fw + fl of the CTA, bin es of
+ * its block.  Runs the reference's Poisson sampler and star draws for it on the
+ * calling warp (all lanes, identical control flow), records a checkpoint when
+ * one is due, and leaves the outcome in S (flag 0: continue, 1: the stream
+ * reached its limit and pauses after the bin, 2: stop on an infinite expected
+ * count).  For a block inside one pixel the bin and its anchor are found by
+ * stepping from the block start and reading the window's anchor slots. */
+template <int DRAW, int MODEL>
+__device__ __noinline__ void handle_event(const CrawlParams &P, CrawlSmem<DRAW> &S, int sid, int lane, int fL, int es,
+                                          uint64_t vb, float emu, int f_ilb, int f_k, int f_i0, int f_j0, bool f_fast,
+                                          uint32_t a, const uint64_t *jlo, const uint64_t *jhi)
+{
+    const CrawlJob &J = S.job;
+    const SkyModel &m = J.m;
+    const int x = m.nm, y = m.nM;
+    const int f_sbeg = (fL == 0) ? S.cur.pos : 0;
+    int e_ilb, e_im, e_iM;
+    AnchorX anc_es = S.cur.anc;
+    if (f_fast) {
+        int ci = f_i0, cj = f_j0, n = (f_sbeg == 0) ? 0 : -1;
+        for (int s = 1; s <= es; s++) {
+            if (gfc::step_in_pixel(ci, cj, x, y) && s >= f_sbeg) n++;
+        }
+        e_ilb = f_ilb; e_im = ci; e_iM = cj;
+        if (n >= 0) anc_es = ax_from(S.slot[fL * GF_BLOCK + n]);
     } else {
-        c.blk_ilb = st.blk_ilb[tid]; c.blk_k = st.blk_k[tid]; c.pos = st.pos[tid];
-        c.ndraw = st.ndraw[tid];
-        c.cur_ilb = st.cur_ilb[tid]; c.cur_im = st.cur_im[tid]; c.cur_iM = st.cur_iM[tid];
-        c.anc.D = st.D[tid]; c.anc.Am = st.Am[tid]; c.anc.ms = st.ms[tid];
-    }
-
-    uint32_t a = 0;
-    uint64_t p = 0, v = 0, jlo = 0, jhi = 0;
-    int64_t nstars = 0, limit = 0;
-    gfr::Mwc r;
-    if (DRAW) {
-        const int NS = P.rng_nstreams;
-        a = P.rng[tid];
-        r.a = a; r.c = P.rng[NS + tid]; r.x = P.rng[2 * NS + tid];
-        p = r.p();
-        v = r.v();
-        jlo = P.jt.lo[(size_t)tid * 32 + lane];
-        jhi = P.jt.hi[(size_t)tid * 32 + lane];
-        nstars = st.nstars[tid];
-        limit = P.limits[tid];
-        /* finish the draw that did not complete before the table filled (skygen.cu.h:497-502) */
-        if (c.ndraw) {
-            draw_stars(P, tid, lane, r, c.ndraw, nstars, limit, c.cur_ilb, c.cur_im, c.cur_iM, c.anc.Am);
-            v = r.v();
+        const BinPos eb = bin_at(f_ilb, f_k, es, f_sbeg, x, y);
+        e_ilb = eb.ilb; e_im = eb.im; e_iM = eb.iM;
+        if (eb.anchor_s >= 0) {
+            const BinPos ab = bin_at(f_ilb, f_k, eb.anchor_s, 0, x, y);
+            anc_es = anchor_cold<MODEL>(m, J.g, J.Dtab, ab.ilb, ab.im, ab.iM);
         }
     }
+    int flag = 0, nd = 0;
+    long long ns = S.nstars;
+    int nck = S.next_ck;
+    uint64_t vnew = vb;
+    if (!(emu < 3.0e38f)) {
+        /* an infinite expected count would never leave the sampler's gamma loop */
+        if (lane == 0) atomicOr(P.err, 1ull);
+        flag = 2;
+    } else {
+        if (P.ck && ns >= nck) {
+            if (lane == 0) {
+                const uint32_t slot = atomicAdd(P.ck_count, 1u);
+                if (slot < (uint32_t)P.ck_capacity) {
+                    Checkpoint ck;
+                    ck.stream = sid; ck.nstars = (int32_t)ns;
+                    ck.blk_ilb = f_ilb; ck.blk_k = f_k; ck.pos = es; ck.pad = 0;
+                    ck.anc = anc_es; ck.v = vb;
+                    P.ck[slot] = ck;
+                }
+            }
+            nck = (int)ns + P.ck_every;
+        }
+        gfr::Mwc r;
+        r.a = a;
+        r.set_v(vb);
+        r.used = 0;
+        nd = (int)r.poisson(emu);
+        draw_stars<DRAW>(P, S, sid, lane, r, nd, ns, S.limit, e_ilb, e_im, e_iM);
+        vnew = r.v();
+        if (nd) flag = 1;             /* the stream reached its limit: pause right after the bin */
+        /* The walk assumed one uniform for this bin; it drew r.used >= 1.  Every later
+         * bin's start state moves by a^(used-1): the scaled multiplier of that power. */
+        const uint64_t p = ((uint64_t)a << 32) - 1;
+        uint32_t n = r.used - 1;
+        uint64_t ms = __ldg(jlo);                                 /* scaled a^0 */
+        if (n >= 2048) {
+            const uint64_t m2047 = gfr::mwc_mulmod_scaled(__ldg(jlo + 31), __ldg(jhi + 63), a, p);
+            while (n >= 2047) { ms = gfr::mwc_mulmod_scaled(ms, m2047, a, p); n -= 2047; }
+        }
+        ms = gfr::mwc_mulmod_scaled(ms, gfr::mwc_mulmod_scaled(__ldg(jlo + (n & 31)), __ldg(jhi + (n >> 5)), a, p), a, p);
+        if (lane == 0) S.mult = ms;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        S.v = vnew; S.nstars = ns; S.flag = flag; S.fL = fL; S.es = es; S.next_ck = nck;
+        S.cur.ndraw = nd; S.cur.cur_ilb = e_ilb; S.cur.cur_im = e_im; S.cur.cur_iM = e_iM;
+        if (flag == 1) {
+            S.cur.blk_ilb = f_ilb; S.cur.blk_k = f_k; S.cur.pos = es + 1;
+            S.cur.anc = anc_es;
+        }
+    }
+    __syncwarp();
+}
+
+/* Finish the draw that did not complete before the previous batch filled
+ * (skygen.cu.h:497-502); warp 0. */
+template <int DRAW>
+__device__ __noinline__ void finish_pending(const CrawlParams &P, CrawlSmem<DRAW> &S, int sid, int lane, uint32_t a)
+{
+    gfr::Mwc r;
+    r.a = a;
+    r.set_v(S.v);
+    int nd = S.cur.ndraw;
+    long long ns = S.nstars;
+    draw_stars<DRAW>(P, S, sid, lane, r, nd, ns, S.limit, S.cur.cur_ilb, S.cur.cur_im, S.cur.cur_iM);
+    __syncwarp();
+    if (lane == 0) { S.v = r.v(); S.nstars = ns; S.cur.ndraw = nd; S.next_ck = (int)ns; }
+    __syncwarp();
+}
+
+/* A block that runs past the end of its pixel (possible only when nm*nM is not
+ * a multiple of 10): follow advance() bin by bin with the anchors inline.
+ * Returns whether the crawl left the last pixel inside the block. */
+template <int DRAW, int MODEL>
+__device__ __noinline__ bool slow_block(CrawlSmem<DRAW> &S, const float *LFM, const float *MMr, int L, int i0, int j0,
+                                        int my_ilb, int s_begin, uint32_t &live, double &cnt_sum, double &cov_sum)
+{
+    const CrawlJob &J = S.job;
+    const SkyModel &m = J.m;
+    const int x = m.nm, y = m.nM, npix = J.g.npixels;
+    int i = i0, j = j0, ilb = my_ilb;
+    bool dd = false, ended = false;
+    AnchorX A = S.cur.anc;
+    float cf = 0.f;
+    for (int s = 0; s < GF_BLOCK; s++) {
+        bool moved = true;
+        if (s > 0 && !dd) {
+            bool pinc;
+            moved = gfc::advance(i, j, x, y, pinc);
+            if (pinc) ilb++;
+            if (moved && ilb >= npix) dd = true;
+        }
+        if (dd) ended = true;
+        float mus = gfc::cut_marker();
+        if (!dd && s >= s_begin) {
+            if (moved) {
+                A = gfc::anchor_x<MODEL>(m, J.g, J.Dtab, ilb, i, j);
+                if (!DRAW) cf = J.g.pixels[ilb].coveredFraction;
+            }
+            /* i (and j) can leave the grid after a pixel change: see bin_distance */
+            const float lfv = ((unsigned)j < (unsigned)y) ? LFM[j] : gfc::lf_sample(m, m.lf, m.M1 - (float)j * m.dM);
+            const float mrow = ((unsigned)i < (unsigned)x) ? MMr[i] : m.m0 + m.dm * (float)i;
+            mus = gfc::bin_mu_x(A, lfv, mrow, m.norm, m.m1);
+        }
+        const bool ok = !gfc::is_cut(mus);
+        if (DRAW) {
+            S.mu[L >> 5][s][L & 31] = mus;
+            live |= ok ? (1u << s) : 0u;
+        } else if (ok) {
+            cnt_sum += (double)mus;
+            const double cv = (double)(mus * cf);
+            cov_sum += cv;
+            if (J.per_pixel) atomicAdd(&J.per_pixel[ilb + J.pix_base], cv);
+        }
+    }
+    return ended;
+}
+
+/* Crawl of one stream by one CTA (integrate when DRAW = 0, Poisson draw when
+ * DRAW = 1).  Thread L of the CTA owns block j+L of the stream's window. */
+template <int DRAW, int MODEL>
+__device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float *LFM, const float *MMr, int tid)
+{
+    const CrawlJob &J = S.job;
+    const SkyModel &m = J.m;
+    const int L = threadIdx.x, warp = L >> 5, lane = L & 31;
+    const int x = m.nm, y = m.nM, kmax = x * y;
+    const int npix = J.g.npixels;
+    const float norm = m.norm, m1 = m.m1;
+    const CrawlState &st = J.st;
+    const long long step = (long long)GF_BLOCK * m.nthreads;
+    const long long offL = (long long)L * step;
+    const int qL = (int)(offL / kmax), rL = (int)(offL % kmax);
+    const long long offW = (long long)GF_WIN * step;
+    const int QW = (int)(offW / kmax), RW = (int)(offW % kmax);
+    const int sid = (J.job_id << 16) | tid;
+
+    const int status = DRAW ? st.status[tid] : 0;
+    if (status == 2) return;
+    if (L == 0) {
+        Cursor &c = S.cur;
+        if (status == 0) {
+            long long k = (long long)GF_BLOCK * tid;
+            c.blk_ilb = (int)(k / kmax);
+            c.blk_k = (int)(k % kmax);
+            c.pos = 0;
+            c.ndraw = 0;
+            c.cur_ilb = c.cur_im = c.cur_iM = 0;
+            c.anc.Am = c.anc.ms = c.anc.D3 = c.anc.K = 0.f;
+        } else {
+            c.blk_ilb = st.blk_ilb[tid]; c.blk_k = st.blk_k[tid]; c.pos = st.pos[tid];
+            c.ndraw = st.ndraw[tid];
+            c.cur_ilb = st.cur_ilb[tid]; c.cur_im = st.cur_im[tid]; c.cur_iM = st.cur_iM[tid];
+            c.anc = st.anc[tid];
+        }
+        if (DRAW) {
+            const int NS = J.rng_nstreams;
+            S.v = ((uint64_t)J.rng[NS + tid] << 32) | J.rng[2 * NS + tid];
+            S.nstars = st.nstars[tid];
+            S.limit = J.limits[tid];
+            S.next_ck = (int)S.nstars;
+            S.nrec = 0;
+        }
+    }
+    __syncthreads();
+
+    uint32_t a = 0;
+    uint64_t v = 0;
+    const uint64_t *jlo = nullptr, *jhi = nullptr;
+    if (DRAW) {
+        a = J.rng[tid];
+        jlo = P.jt.lo + (size_t)tid * 32;
+        jhi = P.jt.hi + (size_t)tid * GF_JUMP_HI;
+        if (S.cur.ndraw) {
+            if (warp == 0) finish_pending<DRAW>(P, S, sid, lane, a);
+            __syncthreads();
+        }
+        v = S.v;
+    }
+    int blk_ilb = S.cur.blk_ilb, blk_k = S.cur.blk_k, pos = S.cur.pos;
 
     double cnt_sum = 0.0, cov_sum = 0.0;
     bool finished = false;
-    int pp_ilb = -1;
-    double pp_sum = 0.0;
-    const long long step = (long long)GF_BLOCK * N;
 
-    while (!(DRAW && c.ndraw)) {
-        /* ---------- phase A: bins, anchors and mu of 32 blocks ---------- */
-        long long kk = (long long)c.blk_k + (long long)lane * step;
-        const int my_k = (int)(kk % kmax);
-        const int my_q = (int)(kk / kmax);
-        const int drift = gfc::block_drift(my_k, x, y);
-        int dsum = drift;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, dsum, o);
-            if (lane >= o) dsum += t;
-        }
-        const int dexcl = dsum - drift;
-        const int dtot = __shfl_sync(0xffffffffu, dsum, 31);
-        long long my_ilb_ll = (long long)c.blk_ilb + my_q + dexcl;
-        const int my_ilb = my_ilb_ll > npix ? npix : (int)my_ilb_ll;
-        const int s_begin = (lane == 0) ? c.pos : 0;
+    while (!(DRAW && S.cur.ndraw)) {
+        /* ---------- the window: block j+L of the stream for thread L ---------- */
+        int my_k = blk_k + rL, my_q = qL;
+        if (my_k >= kmax) { my_k -= kmax; my_q++; }
         const bool fast = my_k + GF_BLOCK - 1 < kmax;
+        const int drift = fast ? 0 : gfc::block_drift(my_k, x, y);
+        int dexcl = 0, dtot = 0;
+        if (__syncthreads_or(drift != 0)) {
+            const int inc = warp_incl_scan(drift, lane);
+            if (lane == 31) S.scan[warp] = inc;
+            __syncthreads();
+            int woff = 0;
+            for (int q = 0; q < GF_CW; q++) {
+                const int t = S.scan[q];
+                woff += (q < warp) ? t : 0;
+                dtot += t;
+            }
+            dexcl = woff + inc - drift;
+            __syncthreads();
+        }
+        const long long ilb_ll = (long long)blk_ilb + my_q + dexcl;
+        const int my_ilb = ilb_ll > npix ? npix : (int)ilb_ll;
+        const int s_begin = (L == 0) ? pos : 0;
+        const bool dead0 = my_ilb >= npix;
+        bool lane_end = dead0;
 
-        /* mu of bin s of this lane at mu_sm[s * 32 + lane] (conflict-free) */
-#define MU(s_) mu_sm[(s_) * 32 + lane]
-        gfc::Anchor anc = c.anc;       /* lane 0 inherits the carried anchor */
-        bool lane_end = my_ilb >= npix;
-        {
-            int i = 0, j = 0, ilb = my_ilb;
-            bool dead = lane_end;
-            if (!dead) gfc::diag_to_ij(my_k, x, y, i, j);
-#pragma unroll 1
-            for (int s = 0; s < GF_BLOCK; s++) {
-                bool moved = true;
-                if (s > 0 && !dead) {
-                    if (fast) {
-                        int ni = i + 1, nj = j - 1;
-                        if (nj < 0 || ni >= x) gfc::diag_to_ij(my_k + s, x, y, ni, nj);
-                        i = ni; j = nj;
-                        moved = (i == 0) || (j == y - 1);
-                    } else {
-                        bool inc;
-                        moved = gfc::advance(i, j, x, y, inc);
-                        if (inc) ilb++;
-                        if (moved && ilb >= npix) dead = true;
-                    }
+        /* ---------- pass 1: anchor bins of the block, evaluated compacted over the CTA ---------- */
+        int i0 = 0, j0 = 0;
+        if (!dead0) gfc::diag_to_ij_fast(my_k, x, y, J.fx, J.fy, i0, j0);
+        const int base = L * GF_BLOCK;
+        int na = 0;
+        if (!dead0 && fast) {
+            int ci = i0, cj = j0, s = 0;
+            if (s_begin == 0) {
+                S.slot[base] = make_float4(__int_as_float(my_ilb), __int_as_float((ci << 16) | cj), 0.f, 0.f);
+                na = 1;
+            }
+            for (;;) {
+                const int rem = min(cj, x - 1 - ci) + 1;     /* bins left on this diagonal */
+                s += rem;
+                if (s >= GF_BLOCK) break;
+                const int d1 = ci + cj + 1;
+                ci = max(0, d1 - (y - 1));
+                cj = d1 - ci;
+                if (s >= s_begin) {
+                    S.slot[base + na] = make_float4(__int_as_float(my_ilb), __int_as_float((ci << 16) | cj), 0.f, 0.f);
+                    na++;
                 }
-                float mus = gfc::cut_marker();
-                if (dead) lane_end = true;
-                if (!dead && s >= s_begin) {
-                    const gf_pencil_beam pix = P.g.pixels[ilb];
-                    if (moved || (s == s_begin && lane != 0)) anc = anchor(P, pix, i, j);
-                    const float M = m.M1 - (float)j * m.dM;
-                    mus = gfc::bin_mu(m, lf, anc, pix.dA, i, M);
-                    if (!DRAW && !gfc::is_cut(mus)) {
-                        cnt_sum += (double)mus;
-                        float cov = mus * pix.coveredFraction;
-                        cov_sum += (double)cov;
-                        if (P.per_pixel) {
-                            if (ilb != pp_ilb) {
-                                if (pp_ilb >= 0) atomicAdd(&P.per_pixel[pp_ilb + P.pix_base], pp_sum);
-                                pp_ilb = ilb;
-                                pp_sum = 0.0;
-                            }
-                            pp_sum += (double)cov;
-                        }
-                    }
-                }
-                if (DRAW) MU(s) = mus;
             }
         }
-        const unsigned end_mask = __ballot_sync(0xffffffffu, lane_end);
-        __syncwarp();
+        {
+            const int inc = warp_incl_scan(na, lane);
+            if (lane == 31) S.scan[warp] = inc;
+            __syncthreads();
+            int woff = 0, T = 0;
+            for (int q = 0; q < GF_CW; q++) {
+                const int t = S.scan[q];
+                woff += (q < warp) ? t : 0;
+                T += t;
+            }
+            const int excl = woff + inc - na;
+            for (int n = 0; n < na; n++) S.dense[excl + n] = (uint16_t)(base + n);
+            __syncthreads();
+            for (int d = L; d < T; d += GF_WIN) {
+                const int sl = S.dense[d];
+                const float4 in = S.slot[sl];
+                const int ij = __float_as_int(in.y);
+                const AnchorX ax = gfc::anchor_x<MODEL>(m, J.g, J.Dtab, __float_as_int(in.x), ij >> 16, ij & 0xffff);
+                S.slot[sl] = make_float4(ax.Am, ax.ms, ax.D3, ax.K);
+            }
+            __syncthreads();
+        }
+
+        /* ---------- pass 2: expected count of every bin ---------- */
+        uint32_t live = 0;                 /* bins with an expected count (not cut) */
+        if (!dead0 && fast) {
+            int ci = i0, cj = j0, n = (s_begin == 0) ? 0 : -1;
+            AnchorX A = (s_begin == 0) ? ax_from(S.slot[base]) : S.cur.anc;
+            const float cf = DRAW ? 0.f : J.g.pixels[my_ilb].coveredFraction;
+            double bcov = 0.0;
+#pragma unroll
+            for (int s = 0; s < GF_BLOCK; s++) {
+                if (s > 0) {
+                    const bool wrap = gfc::step_in_pixel(ci, cj, x, y);
+                    if (wrap && s >= s_begin) { n++; A = ax_from(S.slot[base + n]); }
+                }
+                float mus = gfc::cut_marker();
+                if (s >= s_begin) mus = gfc::bin_mu_x(A, LFM[cj], MMr[ci], norm, m1);
+                const bool ok = !gfc::is_cut(mus);
+                if (DRAW) {
+                    S.mu[warp][s][lane] = mus;
+                    live |= ok ? (1u << s) : 0u;
+                } else if (ok) {
+                    cnt_sum += (double)mus;
+                    const double cv = (double)(mus * cf);
+                    cov_sum += cv;
+                    bcov += cv;
+                }
+            }
+            if (!DRAW && J.per_pixel) atomicAdd(&J.per_pixel[my_ilb + J.pix_base], bcov);
+        } else if (!dead0) {
+            if (slow_block<DRAW, MODEL>(S, LFM, MMr, L, i0, j0, my_ilb, s_begin, live, cnt_sum, cov_sum)) lane_end = true;
+        }
+        const int any_end = __syncthreads_or(lane_end);
 
         if (DRAW) {
             /* ---------- phase B: uniforms, restarted after each bin with stars ---------- */
-            int lane_lo = s_begin;          /* first bin of the lane not yet consumed */
+            /* start state of each thread's first bin, if no bin before it has stars */
+            const uint32_t act0 = s_begin >= GF_BLOCK ? 0u : ((live >> s_begin) << s_begin);
+            uint32_t act = act0;
+            uint64_t wst;
+            {
+                const int cnt = __popc(act);
+                const int inc = warp_incl_scan(cnt, lane);
+                if (lane == 31) S.wtot[warp] = inc;
+                __syncthreads();
+                int woff = 0;
+                for (int q = 0; q < GF_CW; q++) woff += (q < warp) ? S.wtot[q] : 0;
+                wst = jump(v, woff + inc - cnt, jlo, jhi, a);
+            }
+            const uint64_t pmod = ((uint64_t)a << 32) - 1;
             for (;;) {
-                int cnt = 0;
-#pragma unroll
-                for (int s = 0; s < GF_BLOCK; s++) cnt += (s >= lane_lo && !gfc::is_cut(MU(s))) ? 1 : 0;
-                int csum = cnt;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    int t = __shfl_up_sync(0xffffffffu, csum, o);
-                    if (lane >= o) csum += t;
-                }
-                uint64_t w = jump(v, csum - cnt, jlo, jhi, a, p);
                 int ev_s = -1;
-                uint64_t w_before = w;
+                uint64_t w = wst, w_before = 0;
                 float ev_mu = 0.f;
+                if (act) {
 #pragma unroll
-                for (int s = 0; s < GF_BLOCK; s++) {
-                    const float mus = MU(s);
-                    if (ev_s < 0 && s >= lane_lo && !gfc::is_cut(mus)) {
-                        uint64_t wb = w;
-                        float u = mwc_step(w, a);
-                        if (!surely_empty(u, mus)) {
-                            if (mus > 10.f || u > gfm::expf_(-mus)) { ev_s = s; w_before = wb; ev_mu = mus; }
+                    for (int s = 0; s < GF_BLOCK; s++) {
+                        if (ev_s < 0 && ((act >> s) & 1u)) {
+                            const float mus = S.mu[warp][s][lane];
+                            const uint64_t wb = w;
+                            const float u = mwc_step(w, a);
+                            if (!surely_empty(u, mus) && has_stars(u, mus)) {
+                                ev_s = s;
+                                w_before = wb;
+                                ev_mu = mus;
+                            }
                         }
                     }
                 }
-                const unsigned ev_mask = __ballot_sync(0xffffffffu, ev_s >= 0);
-                if (ev_mask == 0) {
-                    v = shfl64(w, 31);
+                const unsigned evm = __ballot_sync(FULLMASK, ev_s >= 0);
+                if (lane == 0) S.wev[warp] = evm ? (__ffs(evm) - 1) : -1;
+                if (L == GF_WIN - 1) S.v_end = w;
+                __syncthreads();
+                int fw = -1, fl = 0;
+                for (int q = 0; q < GF_CW; q++) {
+                    const int e = S.wev[q];
+                    if (fw < 0 && e >= 0) { fw = q; fl = e; }
+                }
+                if (fw < 0) {
+                    v = S.v_end;
                     break;
                 }
-                /* the first lane with stars: its bin goes through the reference's sampler */
-                const int f = __ffs(ev_mask) - 1;
-                const int es = __shfl_sync(0xffffffffu, ev_s, f);
-                const uint64_t vb = shfl64(w_before, f);
-                const float emu = __shfl_sync(0xffffffffu, ev_mu, f);
-                const int f_ilb = __shfl_sync(0xffffffffu, my_ilb, f);
-                const int f_k = __shfl_sync(0xffffffffu, my_k, f);
-                const int f_sbeg = (f == 0) ? c.pos : 0;
-                const BinPos eb = bin_at(f_ilb, f_k, es, f_sbeg, x, y, npix);
-                if (!(emu < 3.0e38f)) {
-                    /* an infinite expected count would never leave the sampler's gamma loop */
-                    if (lane == 0) atomicOr(P.err, 1ull);
-                    finished = true;
+                if (warp == fw) {
+                    const int es = __shfl_sync(FULLMASK, ev_s, fl);
+                    const uint64_t vb = shfl64(w_before, fl);
+                    const float emu = __shfl_sync(FULLMASK, ev_mu, fl);
+                    const int f_ilb = __shfl_sync(FULLMASK, my_ilb, fl);
+                    const int f_k = __shfl_sync(FULLMASK, my_k, fl);
+                    const int f_i0 = __shfl_sync(FULLMASK, i0, fl);
+                    const int f_j0 = __shfl_sync(FULLMASK, j0, fl);
+                    const bool f_fast = __shfl_sync(FULLMASK, fast ? 1 : 0, fl) != 0;
+                    handle_event<DRAW, MODEL>(P, S, sid, lane, fw * 32 + fl, es, vb, emu, f_ilb, f_k, f_i0, f_j0, f_fast,
+                                              a, jlo, jhi);
+                }
+                __syncthreads();
+                const int flag = S.flag;
+                if (flag) {
+                    v = S.v;
+                    if (flag == 2) finished = true;
                     break;
                 }
-                r.a = a;
-                r.set_v(vb);
-                c.ndraw = (int)r.poisson(emu);
-                c.cur_ilb = eb.ilb;
-                c.cur_im = eb.im;
-                c.cur_iM = eb.iM;
-                const float AmMin = gfc::beam_extinction(P.g, P.g.pixels[eb.ilb]);
-                draw_stars(P, tid, lane, r, c.ndraw, nstars, limit, c.cur_ilb, c.cur_im, c.cur_iM, AmMin);
-                v = r.v();
-                if (c.ndraw) {
-                    /* the table is full: pause right after the event bin, with its anchor */
-                    long long fk = (long long)c.blk_k + (long long)f * step;
-                    const int fdrift = __shfl_sync(0xffffffffu, dexcl, f);
-                    c.blk_ilb = (int)((long long)c.blk_ilb + fk / kmax + fdrift);
-                    c.blk_k = (int)(fk % kmax);
-                    if (eb.anchor_s >= 0) {
-                        const BinPos ab = bin_at(f_ilb, f_k, eb.anchor_s, 0, x, y, npix);
-                        c.anc = anchor(P, P.g.pixels[ab.ilb], ab.im, ab.iM);
-                    }
-                    c.pos = es + 1;
-                    break;
+                /* continue with the bins after the one with stars: the thread that had it
+                 * resumes from the state after the draw, later threads shift by a^(used-1) */
+                const int fL = fw * 32 + fl;
+                if (L < fL) {
+                    act = 0u;
+                } else if (L == fL) {
+                    const int lo = S.es + 1;
+                    act = lo >= GF_BLOCK ? 0u : ((live >> lo) << lo);
+                    wst = S.v;
+                } else {
+                    wst = gfr::mwc_mulmod_scaled(S.mult, wst, a, pmod);
                 }
-                /* continue with the bins after the event */
-                if (lane < f) lane_lo = GF_BLOCK;
-                else if (lane == f) lane_lo = es + 1;
             }
-            if (finished || c.ndraw) break;
+            if (finished || S.cur.ndraw) break;
         }
-#undef MU
-        if (end_mask) { finished = true; break; }
-        /* next window: 32 blocks further */
-        long long nk = (long long)c.blk_k + 32LL * step;
-        c.blk_ilb = (int)((long long)c.blk_ilb + nk / kmax + dtot);
-        c.blk_k = (int)(nk % kmax);
-        c.pos = 0;
+        if (any_end) { finished = true; break; }
+        /* next window */
+        int nk = blk_k + RW, carry = 0;
+        if (nk >= kmax) { nk -= kmax; carry = 1; }
+        blk_ilb = blk_ilb + QW + carry + dtot;
+        blk_k = nk;
+        pos = 0;
+        if (L == 0) S.cur.pos = 0;        /* read by the event handler of the next window */
     }
 
     if (!DRAW) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
-            cnt_sum += __shfl_xor_sync(0xffffffffu, cnt_sum, o);
-            cov_sum += __shfl_xor_sync(0xffffffffu, cov_sum, o);
+            cnt_sum += __shfl_xor_sync(FULLMASK, cnt_sum, o);
+            cov_sum += __shfl_xor_sync(FULLMASK, cov_sum, o);
         }
-        if (P.per_pixel && pp_ilb >= 0) atomicAdd(&P.per_pixel[pp_ilb + P.pix_base], pp_sum);
-        if (lane == 0) {
-            P.counts[tid] += cnt_sum;
-            P.countsCovered[tid] += cov_sum;
+        if (lane == 0) { S.red[0][warp] = cnt_sum; S.red[1][warp] = cov_sum; }
+        __syncthreads();
+        if (L == 0) {
+            double e = 0.0, ec = 0.0;
+            for (int q = 0; q < GF_CW; q++) { e += S.red[0][q]; ec += S.red[1][q]; }
+            J.counts[tid] += e;
+            J.countsCovered[tid] += ec;
         }
         return;
     }
 
-    if (lane == 0) {
+    __syncthreads();
+    if (warp == 0) flush_records<DRAW>(P, S, lane);
+    if (L == 0) {
+        const Cursor &c = S.cur;
+        const bool paused = c.ndraw != 0;
         st.status[tid] = finished ? 2 : 1;
-        st.blk_ilb[tid] = c.blk_ilb; st.blk_k[tid] = c.blk_k; st.pos[tid] = c.pos;
+        st.blk_ilb[tid] = paused ? c.blk_ilb : blk_ilb;
+        st.blk_k[tid] = paused ? c.blk_k : blk_k;
+        st.pos[tid] = paused ? c.pos : pos;
         st.ndraw[tid] = c.ndraw;
         st.cur_ilb[tid] = c.cur_ilb; st.cur_im[tid] = c.cur_im; st.cur_iM[tid] = c.cur_iM;
-        st.D[tid] = c.anc.D; st.Am[tid] = c.anc.Am; st.ms[tid] = c.anc.ms;
-        st.nstars[tid] = nstars;
-        const int NS = P.rng_nstreams;
-        P.rng[NS + tid] = (uint32_t)(v >> 32);
-        P.rng[2 * NS + tid] = (uint32_t)v;
+        st.anc[tid] = c.anc;
+        st.nstars[tid] = S.nstars;
+        const int NS = J.rng_nstreams;
+        J.rng[NS + tid] = (uint32_t)(v >> 32);
+        J.rng[2 * NS + tid] = (uint32_t)v;
     }
 }
 
-template <int DRAW>
-__global__ void __launch_bounds__(128) crawl_kernel(CrawlParams P)
+/* Per-model tables in shared memory: LF(M) of every absolute-magnitude row
+ * (nearest texel, cux.h:778-792) and m0 + dm*im of every apparent-magnitude row. */
+__device__ void fill_tables(const SkyModel &m, float *LFM, float *MMr)
 {
-    extern __shared__ float s_lf[];
-    __shared__ float s_mu[128 / 32][GF_BLOCK * 32];
-    for (int i = threadIdx.x; i < P.m.lf_n; i += blockDim.x) s_lf[i] = P.m.lf[i];
-    __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int tid = P.stream_begin + warp; tid < P.stream_end; tid += nwarps)
-        crawl_stream<DRAW>(P, s_lf, s_mu[threadIdx.x >> 5], tid, lane);
+    for (int q = threadIdx.x; q < m.nM; q += blockDim.x) LFM[q] = gfc::lf_sample(m, m.lf, m.M1 - (float)q * m.dM);
+    for (int q = threadIdx.x; q < m.nm; q += blockDim.x) MMr[q] = m.m0 + m.dm * (float)q;
+}
+
+template <int DRAW, int MODEL>
+__global__ void __launch_bounds__(GF_WIN, DRAW ? 4 : 6) crawl_kernel(CrawlParams P)
+{
+    extern __shared__ float s_tab[];
+    __shared__ CrawlSmem<DRAW> S;
+    int loaded = -1;
+    for (int it = blockIdx.x; it < P.nitems; it += gridDim.x) {
+        int job = 0, tid;
+        if (P.items) {
+            const uint32_t w = P.items[it];
+            job = (int)(w >> 16);
+            tid = (int)(w & 0xffffu);
+        } else {
+            tid = P.stream_begin + it;
+        }
+        if (job != loaded) {
+            __syncthreads();
+            const int *src = P.jobs ? (const int *)&P.jobs[job] : (const int *)&P.job0;
+            for (int q = threadIdx.x; q < (int)(sizeof(CrawlJob) / 4); q += blockDim.x) ((int *)&S.job)[q] = src[q];
+            __syncthreads();
+            fill_tables(S.job.m, s_tab, s_tab + S.job.m.nM);
+            loaded = job;
+        }
+        __syncthreads();
+        crawl_item<DRAW, MODEL>(P, S, s_tab, s_tab + S.job.m.nM, tid);
+    }
 }
 
 /* D[im][iM] = powf(10, 0.2 DM + 1) with DM = (m0 + im dm) - (M1 - iM dM), skygen.cu.h:219-222 */
@@ -506,7 +816,9 @@ __global__ void __launch_bounds__(256) place_kernel(PlaceParams P)
         float Am0 = (P.g.ext_kind == GF_EXT_SCREEN_CSCB) ? P.g.A0 / fabsf(sb) : 0.f;
         float AmInf = Am0;
         int hid = (mtmp + Am0 > m.m1) ? 1 : 0;
-        if (rec.AmMin > Am0) AmInf = -rec.AmMin;
+        /* the beam extinction at the bin's anchor (draw_stars, skygen.cu.h:437-446) */
+        const float AmMin = gfc::beam_extinction(P.g, pix);
+        if (AmMin > Am0) AmInf = -AmMin;
         P.Am[i] = Am0;
         P.AmInf[i] = AmInf;
         P.hidden[i] = hid;
@@ -610,41 +922,63 @@ int sm_count()
     return sm_count_cached;
 }
 
-static CrawlParams make_params(const LaunchCrawl &L)
+static void fill_job(CrawlJob &J, const LaunchCrawl &L)
 {
-    CrawlParams P;
-    P.m = L.m;
-    P.g = L.g;
-    P.st = L.st;
-    P.rng = L.rng;
-    P.rng_nstreams = L.rng_nstreams;
-    P.jt = L.jt;
-    P.stream_begin = L.stream_begin;
-    P.stream_end = L.stream_end;
-    P.limits = L.limits;
-    P.rec = L.rec;
-    P.rec_capacity = L.rec_capacity;
-    P.rec_count = L.rec_count;
-    P.err = L.err;
-    P.counts = L.counts;
-    P.countsCovered = L.countsCovered;
-    P.per_pixel = L.per_pixel;
-    P.pix_base = L.pix_base;
-    P.Dtab = L.Dtab;
-    return P;
+    memset(&J, 0, sizeof(J));
+    J.m = L.m;
+    J.g = L.g;
+    J.st = L.st;
+    J.rng = L.rng;
+    J.rng_nstreams = L.rng_nstreams;
+    J.pix_base = L.pix_base;
+    J.limits = L.limits;
+    J.counts = L.counts;
+    J.countsCovered = L.countsCovered;
+    J.per_pixel = L.per_pixel;
+    J.Dtab = L.Dtab;
+    J.fx = make_fastdiv((uint32_t)L.m.nm);
+    J.fy = make_fastdiv((uint32_t)L.m.nM);
+    J.job_id = 0;
+}
+
+/* one launch of crawl_kernel: one CTA per stream (the hardware scheduler balances them) */
+template <int DRAW, int MODEL>
+static cudaError_t start_crawl(const CrawlParams &P, size_t smem, cudaStream_t s)
+{
+    static bool attr_set = false;       /* the per-model tables may exceed the 48 KB default */
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(crawl_kernel<DRAW, MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    crawl_kernel<DRAW, MODEL><<<P.nitems, GF_WIN, smem, s>>>(P);
+    return cudaSuccess;
 }
 
 cudaError_t launch_crawl(const LaunchCrawl &L, int draw, cudaStream_t s)
 {
-    CrawlParams P = make_params(L);
-    int nstreams = L.stream_end - L.stream_begin;
-    if (nstreams <= 0) return cudaSuccess;
-    const int threads = 128;
-    int warps_per_block = threads / 32;
-    int blocks = (nstreams + warps_per_block - 1) / warps_per_block;
-    size_t smem = (size_t)L.m.lf_n * sizeof(float);
-    if (draw) crawl_kernel<1><<<blocks, threads, smem, s>>>(P);
-    else crawl_kernel<0><<<blocks, threads, smem, s>>>(P);
+    CrawlParams P;
+    memset(&P, 0, sizeof(P));
+    fill_job(P.job0, L);
+    P.nitems = L.stream_end - L.stream_begin;
+    P.stream_begin = L.stream_begin;
+    P.jt = L.jt;
+    P.rec = L.rec;
+    P.rec_capacity = L.rec_capacity;
+    P.rec_count = L.rec_count;
+    P.err = L.err;
+    P.ck = L.ck;
+    P.ck_count = L.ck_count;
+    P.ck_capacity = L.ck_capacity;
+    P.ck_every = L.ck_every > 0 ? L.ck_every : 64;
+    if (P.nitems <= 0) return cudaSuccess;
+    const size_t smem = (size_t)(L.m.nm + L.m.nM) * sizeof(float);
+    if (smem > 64 * 1024) return cudaErrorInvalidValue;
+    const bool disk = L.m.type == GF_MODEL_EXP_DISK;
+    cudaError_t e;
+    if (draw) e = disk ? start_crawl<1, GF_MODEL_EXP_DISK>(P, smem, s) : start_crawl<1, GF_MODEL_POWER_LAW_ELLIPSOID>(P, smem, s);
+    else e = disk ? start_crawl<0, GF_MODEL_EXP_DISK>(P, smem, s) : start_crawl<0, GF_MODEL_POWER_LAW_ELLIPSOID>(P, smem, s);
+    if (e != cudaSuccess) return e;
     count_launches(1);
     return cudaGetLastError();
 }
@@ -710,8 +1044,8 @@ __global__ void jump_table_kernel(const uint32_t *mult, int n, uint64_t *lo, uin
     for (int l = 32; l < 35; l++) tt = gfr::mulmod_generic(tt, a, p);
     a32 = tt;
     uint64_t h = b3;
-    for (int l = 0; l < 32; l++) {
-        hi[(size_t)s * 32 + l] = h;                       /* a^(32 l - 3) */
+    for (int l = 0; l < GF_JUMP_HI; l++) {
+        hi[(size_t)s * GF_JUMP_HI + l] = h;               /* a^(32 l - 3) */
         h = gfr::mulmod_generic(h, a32, p);
     }
 }
