@@ -2,7 +2,7 @@
  * gf_api.cu -- the C ABI (include/galfast_b200.h) and the host orchestration
  * of the catalog path on one B200.
  */
-#include "gf_launch.h"
+#include "gf_ctx.h"
 #include "gf_host.h"
 #include "gf_safeprimes.h"
 
@@ -13,7 +13,7 @@
 #include <string>
 #include <vector>
 
-namespace {
+namespace gfa {
 
 thread_local std::string g_err;
 
@@ -23,85 +23,36 @@ gf_status fail(gf_status s, const std::string &msg)
     return s;
 }
 
-#define GF_CUDA(call)                                                                        \
-    do {                                                                                     \
-        cudaError_t e_ = (call);                                                             \
-        if (e_ != cudaSuccess) {                                                             \
-            return fail(e_ == cudaErrorMemoryAllocation ? GF_E_OOM : GF_E_CUDA,              \
-                        std::string(#call) + ": " + cudaGetErrorString(e_));                  \
-        }                                                                                    \
-    } while (0)
-
-#define GF_TRY(call)                         \
-    do {                                     \
-        gf_status s_ = (call);               \
-        if (s_ != GF_OK) return s_;          \
-    } while (0)
-
-template <typename T>
-gf_status dev_alloc(T **p, size_t n)
+gf_status check_ctx(gf_ctx *ctx)
 {
-    *p = nullptr;
-    if (n == 0) return GF_OK;
-    GF_CUDA(cudaMalloc((void **)p, n * sizeof(T)));
+    if (!ctx) return fail(GF_E_INVALID, "null context");
+    GF_CUDA(cudaSetDevice(ctx->device));
     return GF_OK;
 }
 
-template <typename T>
-void dev_free(T *&p)
+gf_status ensure_multipliers(gf_ctx *ctx)
 {
-    if (p) cudaFree(p);
-    p = nullptr;
+    if (ctx->d_mult) return GF_OK;
+    const std::vector<uint32_t> &mult = gfh::multipliers();
+    GF_TRY(dev_alloc(&ctx->d_mult, GF_MAX_STREAMS));
+    GF_CUDA(cudaMemcpy(ctx->d_mult, mult.data(), 4 * (size_t)GF_MAX_STREAMS, cudaMemcpyHostToDevice));
+    GF_TRY(dev_alloc(&ctx->jt.lo, (size_t)GF_MAX_STREAMS * 32));
+    GF_TRY(dev_alloc(&ctx->jt.hi, (size_t)GF_MAX_STREAMS * GF_JUMP_HI));
+    GF_CUDA(gfk::launch_jump_tables(ctx->d_mult, GF_MAX_STREAMS, ctx->jt.lo, ctx->jt.hi, ctx->stream));
+    return GF_OK;
 }
 
-}  // namespace
+}  // namespace gfa
+
+using gfa::fail;
+using gfa::dev_alloc;
+using gfa::dev_free;
+using gfa::check_ctx;
+using gfa::ProfScope;
 
 namespace gfk {
-void set_last_error(const std::string &msg) { g_err = msg; }
+void set_last_error(const std::string &msg) { gfa::g_err = msg; }
 }
-
-struct gf_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    uint32_t *d_rng = nullptr;           /* persistent streams [3][rng_nstreams] */
-    int32_t rng_nstreams = 0;
-    uint32_t *d_mult = nullptr;
-    JumpTables jt = {nullptr, nullptr};
-    unsigned long long *d_counters = nullptr;   /* [0] record count, [1] visible count */
-    unsigned long long *h_counters = nullptr;   /* pinned */
-    cudaEvent_t ev[16] = {};
-    /* phase profiler */
-    bool prof = false;
-    std::vector<cudaEvent_t> ev_pool;
-    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
-    double prof_ms[GF_PROF_NPHASES] = {};
-    int64_t prof_n[GF_PROF_NPHASES] = {};
-};
-
-namespace {
-cudaEvent_t prof_event(gf_ctx *c)
-{
-    if (!c->ev_pool.empty()) { cudaEvent_t e = c->ev_pool.back(); c->ev_pool.pop_back(); return e; }
-    cudaEvent_t e = nullptr;
-    cudaEventCreate(&e);
-    return e;
-}
-/* brackets the kernels of one phase with events when profiling is enabled */
-struct ProfScope {
-    gf_ctx *c; int kind; cudaEvent_t a = nullptr;
-    ProfScope(gf_ctx *c_, int k) : c(c_), kind(k)
-    {
-        if (c->prof) { a = prof_event(c); cudaEventRecord(a, c->stream); }
-    }
-    ~ProfScope()
-    {
-        if (!a) return;
-        cudaEvent_t b = prof_event(c);
-        cudaEventRecord(b, c->stream);
-        c->prof_pending.push_back({kind, {a, b}});
-    }
-};
-}  // namespace
 
 struct ModelState {
     gfh::HostModel hm;
@@ -386,18 +337,11 @@ __global__ void fill_i64(int64_t *p, int n, int64_t v)
     if (i < n) p[i] = v;
 }
 
-gf_status check_ctx(gf_ctx *ctx)
-{
-    if (!ctx) return fail(GF_E_INVALID, "null context");
-    GF_CUDA(cudaSetDevice(ctx->device));
-    return GF_OK;
-}
-
 }  // namespace
 
 extern "C" {
 
-const char *gf_last_error(void) { return g_err.c_str(); }
+const char *gf_last_error(void) { return gfa::g_err.c_str(); }
 
 gf_status gf_ctx_create(int device, gf_ctx **out)
 {
@@ -502,13 +446,7 @@ gf_status gf_rng_init(gf_ctx *ctx, uint32_t seed48, int32_t nstreams)
     if (nstreams <= 0 || nstreams > GF_MAX_STREAMS) return fail(GF_E_INVALID, "nstreams must be in [1, 65536]");
     if (nstreams % 64) nstreams += 64 - nstreams % 64;     /* roundUpModulo (cuda_rng.h:468) */
     const std::vector<uint32_t> &mult = gfh::multipliers();
-    if (!ctx->d_mult) {
-        GF_TRY(dev_alloc(&ctx->d_mult, GF_MAX_STREAMS));
-        GF_CUDA(cudaMemcpy(ctx->d_mult, mult.data(), 4 * (size_t)GF_MAX_STREAMS, cudaMemcpyHostToDevice));
-        GF_TRY(dev_alloc(&ctx->jt.lo, (size_t)GF_MAX_STREAMS * 32));
-        GF_TRY(dev_alloc(&ctx->jt.hi, (size_t)GF_MAX_STREAMS * GF_JUMP_HI));
-        GF_CUDA(gfk::launch_jump_tables(ctx->d_mult, GF_MAX_STREAMS, ctx->jt.lo, ctx->jt.hi, ctx->stream));
-    }
+    GF_TRY(gfa::ensure_multipliers(ctx));
     std::vector<uint32_t> h(3 * (size_t)nstreams);
     gfh::seed_streams(seed48, nstreams, mult.data(), h.data());
     if (ctx->rng_nstreams != nstreams) {

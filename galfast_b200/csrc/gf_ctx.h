@@ -1,0 +1,100 @@
+/*
+ * gf_ctx.h -- the library context and the host-side error and allocation
+ * helpers shared by the C ABI files (gf_api.cu, gf_multi.cu).
+ */
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include <utility>
+#include <vector>
+#include "gf_launch.h"
+
+namespace gfa {
+
+/* record the message returned by gf_last_error() and pass the status through */
+gf_status fail(gf_status s, const std::string &msg);
+
+template <typename T>
+void dev_free(T *&p)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+}  // namespace gfa
+
+#define GF_CUDA(call)                                                                        \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            return gfa::fail(e_ == cudaErrorMemoryAllocation ? GF_E_OOM : GF_E_CUDA,         \
+                             std::string(#call) + ": " + cudaGetErrorString(e_));             \
+        }                                                                                    \
+    } while (0)
+
+#define GF_TRY(call)                         \
+    do {                                     \
+        gf_status s_ = (call);               \
+        if (s_ != GF_OK) return s_;          \
+    } while (0)
+
+namespace gfa {
+template <typename T>
+gf_status dev_alloc(T **p, size_t n)
+{
+    *p = nullptr;
+    if (n == 0) return GF_OK;
+    GF_CUDA(cudaMalloc((void **)p, n * sizeof(T)));
+    return GF_OK;
+}
+}  // namespace gfa
+
+struct gf_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t *d_rng = nullptr;           /* persistent streams [3][rng_nstreams] */
+    int32_t rng_nstreams = 0;
+    uint32_t *d_mult = nullptr;
+    JumpTables jt = {nullptr, nullptr};
+    unsigned long long *d_counters = nullptr;   /* [0] record count, [1] visible count, [2] error flag */
+    unsigned long long *h_counters = nullptr;   /* pinned */
+    cudaEvent_t ev[16] = {};
+    /* phase profiler */
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
+    double prof_ms[GF_PROF_NPHASES] = {};
+    int64_t prof_n[GF_PROF_NPHASES] = {};
+};
+
+namespace gfa {
+
+gf_status check_ctx(gf_ctx *ctx);
+/* multipliers and jump tables of all 65536 streams on the context's device */
+gf_status ensure_multipliers(gf_ctx *ctx);
+
+inline cudaEvent_t prof_event(gf_ctx *c)
+{
+    if (!c->ev_pool.empty()) { cudaEvent_t e = c->ev_pool.back(); c->ev_pool.pop_back(); return e; }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+/* brackets the kernels of one phase with events when profiling is enabled */
+struct ProfScope {
+    gf_ctx *c; int kind; cudaEvent_t a = nullptr;
+    ProfScope(gf_ctx *c_, int k) : c(c_), kind(k)
+    {
+        if (c->prof) { a = prof_event(c); cudaEventRecord(a, c->stream); }
+    }
+    ~ProfScope()
+    {
+        if (!a) return;
+        cudaEvent_t b = prof_event(c);
+        cudaEventRecord(b, c->stream);
+        c->prof_pending.push_back({kind, {a, b}});
+    }
+};
+
+}  // namespace gfa

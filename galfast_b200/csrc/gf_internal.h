@@ -108,3 +108,21 @@ struct JumpTables {
     uint64_t *lo;                  /* [nstreams][32] */
     uint64_t *hi;                  /* [nstreams][GF_JUMP_HI] */
 };
+
+/* One model crawl of one request: everything the CTA of a stream needs. */
+struct CrawlJob {
+    SkyModel m;
+    SkyGeom g;
+    CrawlState st;
+    uint32_t *rng;                 /* persistent stream state [3][rng_nstreams] */
+    int32_t rng_nstreams;
+    int32_t pix_base;              /* first pixel of this launch within the generator's pixel list */
+    const int64_t *limits;         /* per-stream star limit for this launch (draw) */
+    double *counts, *countsCovered;   /* integrate outputs, per stream */
+    double *per_pixel;             /* integrate output, per pixel (optional) */
+    const float *Dtab;             /* distances D[im][iM] of the model's bins */
+    FastDiv fx, fy;                /* division by nm and by nM */
+    int32_t job_id;                /* bits 16.. of StarRecord::stream */
+    int32_t pad;
+    int64_t limit_all;             /* star limit of every stream when limits is null */
+};

@@ -56,6 +56,37 @@ struct LaunchSort {
     gf_table out;
 };
 
+/* one model pass over many requests: jobs[k] per request, items (job << 16) | stream */
+struct LaunchCrawlMulti {
+    const CrawlJob *jobs;          /* device */
+    const uint32_t *items;         /* device, in the order the work queue hands them out */
+    int32_t nitems;
+    uint32_t *counter;             /* device work-queue counter */
+    int32_t model_type;            /* GF_MODEL_* shared by all jobs */
+    int32_t max_tab;               /* max over jobs of nm + nM */
+    JumpTables jt;
+    StarRecord *rec;
+    int64_t rec_capacity;
+    unsigned long long *rec_count, *err;
+};
+
+struct LaunchPlaceMulti {
+    const CrawlJob *jobs;
+    const int32_t *job_slot;       /* output position of each request */
+    const StarRecord *rec;
+    int64_t n;
+    double *lb;
+    int32_t *projIdx;
+    float *projXY, *DM, *absmag, *XYZ, *Am, *AmInf;
+    int32_t *hidden;
+    uint64_t *key, *key_b;
+    uint32_t *idx_a, *idx_b, *slot_a, *slot_b;
+    int slot_bits;
+    void *temp;
+    size_t temp_bytes;
+    int64_t *seg_begin, *vis_end, *seg_end;     /* per slot, preset to zero by the caller */
+};
+
 int sm_count();
 /* set the message returned by gf_last_error() on this thread */
 void set_last_error(const std::string &msg);
@@ -68,6 +99,12 @@ cudaError_t sort_temp_bytes(int64_t n, size_t *bytes);
 cudaError_t launch_sort_gather(const LaunchSort &L, cudaStream_t s);
 cudaError_t launch_dtab(const SkyModel &m, float *D, cudaStream_t s);
 cudaError_t launch_jump_tables(const uint32_t *mult, int n, uint64_t *lo, uint64_t *hi, cudaStream_t s);
+cudaError_t launch_seed_streams(const uint32_t *seeds, int njobs, const uint32_t *mult, int NS, uint32_t *rng, cudaStream_t s);
+cudaError_t launch_crawl_multi(const LaunchCrawlMulti &L, int draw, cudaStream_t s);
+cudaError_t sort_temp_bytes_multi(int64_t n, size_t *bytes);
+cudaError_t launch_place_sort_multi(const LaunchPlaceMulti &L, cudaStream_t s);
+cudaError_t launch_tie_gather_multi(const LaunchPlaceMulti &L, const int64_t *row_begin, const int32_t *slot_comp,
+                                    gf_table out, int32_t *row_slot, cudaStream_t s);
 
 /* modules (gf_modules.cu) */
 cudaError_t launch_clipper(const gf_footprint &foot, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
@@ -91,5 +128,19 @@ struct PerrTables {
 cudaError_t launch_photoerrors(const PerrTables &c, int64_t row_offset, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
 cudaError_t launch_vel2pm(const gf_vel2pm_config &c, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
 cudaError_t launch_gal2other(int32_t coordsys, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
+
+/* module kernels over the rows of many requests (row_slot: the request slot of each row) */
+struct MultiRows {
+    const int32_t *row_slot;       /* [rows] */
+    const int64_t *slot_row_begin; /* [nslots] first row of each slot */
+    const int32_t *slot_job;       /* [nslots] request index of each slot */
+};
+cudaError_t launch_clipper_multi(const gf_footprint *foot_by_job, MultiRows R, gf_table t, int64_t begin, int64_t end,
+                                 cudaStream_t s);
+cudaError_t launch_bond2010_multi(const gf_bond2010_config &c, uint32_t *rng_all, int32_t NS, MultiRows R,
+                                  const int64_t *slot_chunk_begin, int32_t nslots, int64_t nchunks,
+                                  const int64_t *slot_rows, gf_table t, cudaStream_t s);
+cudaError_t launch_photoerrors_multi(const PerrTables &c, const uint64_t *seed_by_job, const int64_t *catalog_offset_by_job,
+                                     MultiRows R, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
 
 }  // namespace gfk

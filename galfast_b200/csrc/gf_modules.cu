@@ -30,12 +30,11 @@ static int grid_for(int64_t n, int threads)
 }
 
 /* ---------------- clipper ---------------- */
-__global__ void clipper_kernel(gf_footprint foot, gf_table t, int64_t begin, int64_t end)
+__device__ __forceinline__ void clip_row(const gf_footprint &foot, gf_table &t, int64_t row)
 {
     const int64_t P = t.capacity;
-    for (int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < end; row += (int64_t)gridDim.x * blockDim.x) {
-        if (t.hidden[row]) continue;
-        bool in = true;
+    if (t.hidden[row]) return;
+    bool in = true;
         if (foot.kind == GF_FOOT_LAMBERT_RECT) {
             float x = t.projXY[row], y = t.projXY[P + row];
             in = t.projIdx[row] == foot.proj && x >= foot.a && x < foot.b && y >= foot.c && y < foot.d;
@@ -48,7 +47,30 @@ __global__ void clipper_kernel(gf_footprint foot, gf_table t, int64_t begin, int
             in = fabs(t.lb[P + row]) > foot.a;
         }
         if (!in) t.hidden[row] = 1;
+}
+
+__global__ void clipper_kernel(gf_footprint foot, gf_table t, int64_t begin, int64_t end)
+{
+    for (int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < end; row += (int64_t)gridDim.x * blockDim.x)
+        clip_row(foot, t, row);
+}
+
+/* each row clipped by its own request's footprint */
+__global__ void clipper_multi_kernel(const gf_footprint *foot_by_job, MultiRows R, gf_table t, int64_t begin, int64_t end)
+{
+    for (int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < end; row += (int64_t)gridDim.x * blockDim.x) {
+        const gf_footprint &f = foot_by_job[R.slot_job[R.row_slot[row]]];
+        if (f.kind != GF_FOOT_ALL) clip_row(f, t, row);
     }
+}
+
+cudaError_t launch_clipper_multi(const gf_footprint *foot_by_job, MultiRows R, gf_table t, int64_t begin, int64_t end,
+                                 cudaStream_t s)
+{
+    if (end <= begin) return cudaSuccess;
+    clipper_multi_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(foot_by_job, R, t, begin, end);
+    count_launches(1);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_clipper(const gf_footprint &foot, gf_table t, int64_t begin, int64_t end, cudaStream_t s)
@@ -114,12 +136,11 @@ __device__ __forceinline__ void draw_moments(float v[3], float R2, float Z, cons
     trivar_gauss(v, sg, rng);
 }
 
-__global__ void __launch_bounds__(128) bond2010_kernel(const gf_bond2010_config par, uint32_t *rng, int32_t NS, gf_table t,
-                                                        int64_t begin, int64_t end, int64_t nchunks)
+/* rows [begin + 256 th, min(begin + 256 (th + 1), end)) with stream th (Bond2010_gpu.cu.h:179, 217) */
+__device__ __forceinline__ void bond2010_chunk(const gf_bond2010_config &par, uint32_t *rng, int32_t NS, gf_table &t,
+                                               int64_t begin, int64_t end, int64_t th)
 {
     const int64_t P = t.capacity;
-    int64_t th = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (th >= nchunks) return;
     gfr::Mwc r;
     r.a = rng[th]; r.c = rng[NS + th]; r.x = rng[2 * NS + th];
     int64_t rb = begin + 256 * th, re = begin + 256 * (th + 1);
@@ -157,6 +178,41 @@ __global__ void __launch_bounds__(128) bond2010_kernel(const gf_bond2010_config 
     }
     rng[NS + th] = r.c;
     rng[2 * NS + th] = r.x;
+}
+
+__global__ void __launch_bounds__(128) bond2010_kernel(const gf_bond2010_config par, uint32_t *rng, int32_t NS, gf_table t,
+                                                        int64_t begin, int64_t end, int64_t nchunks)
+{
+    int64_t th = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (th >= nchunks) return;
+    bond2010_chunk(par, rng, NS, t, begin, end, th);
+}
+
+/* the 256-row chunks of every request, each drawing from its request's streams */
+__global__ void __launch_bounds__(128) bond2010_multi_kernel(const gf_bond2010_config par, uint32_t *rng_all, int32_t NS,
+                                                              MultiRows R, const int64_t *slot_chunk_begin, int32_t nslots,
+                                                              int64_t nchunks, const int64_t *slot_rows, gf_table t)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nchunks) return;
+    int lo = 0, hi = nslots - 1;          /* last slot whose first chunk is <= c */
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (slot_chunk_begin[mid] <= c) lo = mid; else hi = mid - 1;
+    }
+    const int64_t b = R.slot_row_begin[lo];
+    bond2010_chunk(par, rng_all + (size_t)R.slot_job[lo] * 3 * NS, NS, t, b, b + slot_rows[lo], c - slot_chunk_begin[lo]);
+}
+
+cudaError_t launch_bond2010_multi(const gf_bond2010_config &c, uint32_t *rng_all, int32_t NS, MultiRows R,
+                                  const int64_t *slot_chunk_begin, int32_t nslots, int64_t nchunks,
+                                  const int64_t *slot_rows, gf_table t, cudaStream_t s)
+{
+    if (nchunks <= 0) return cudaSuccess;
+    bond2010_multi_kernel<<<(unsigned)((nchunks + 127) / 128), 128, 0, s>>>(c, rng_all, NS, R, slot_chunk_begin, nslots,
+                                                                          nchunks, slot_rows, t);
+    count_launches(1);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_bond2010(const gf_bond2010_config &c, uint32_t *rng, int32_t NS, gf_table t, int64_t begin, int64_t end,
@@ -278,18 +334,43 @@ __device__ __forceinline__ double linear_eval(const double *xa, const double *ya
     return 0.0;
 }
 
-__global__ void __launch_bounds__(256) photoerr_kernel(PerrTables c, int64_t row_offset, gf_table t, int64_t begin, int64_t end)
+/* observed magnitudes of one row; catalog_row numbers the row within its request's catalog */
+__device__ __forceinline__ void photoerr_row(const PerrTables &c, uint64_t seed, int64_t catalog_row, gf_table &t, int64_t row)
 {
     const int64_t P = t.capacity;
-    for (int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < end; row += (int64_t)gridDim.x * blockDim.x) {
-        if (t.hidden[row]) continue;
-        for (int b = 0; b < c.nbands; b++) {
-            float mag = t.mags[b * P + row];
-            float sigma = (float)linear_eval(c.mag + (size_t)b * c.nknots, c.sigma + (size_t)b * c.nknots, c.nknots, mag);
-            double z = error_normal(c.seed, (uint64_t)(row_offset + row), (uint32_t)b);
-            t.obsmags[b * P + row] = mag + (float)((double)sigma * z);
-        }
+    if (t.hidden[row]) return;
+    for (int b = 0; b < c.nbands; b++) {
+        float mag = t.mags[b * P + row];
+        float sigma = (float)linear_eval(c.mag + (size_t)b * c.nknots, c.sigma + (size_t)b * c.nknots, c.nknots, mag);
+        double z = error_normal(seed, (uint64_t)catalog_row, (uint32_t)b);
+        t.obsmags[b * P + row] = mag + (float)((double)sigma * z);
     }
+}
+
+__global__ void __launch_bounds__(256) photoerr_kernel(PerrTables c, int64_t row_offset, gf_table t, int64_t begin, int64_t end)
+{
+    for (int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < end; row += (int64_t)gridDim.x * blockDim.x)
+        photoerr_row(c, c.seed, row_offset + row, t, row);
+}
+
+__global__ void __launch_bounds__(256) photoerr_multi_kernel(PerrTables c, const uint64_t *seed_by_job,
+                                                              const int64_t *catalog_offset_by_job, MultiRows R, gf_table t,
+                                                              int64_t begin, int64_t end)
+{
+    for (int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < end; row += (int64_t)gridDim.x * blockDim.x) {
+        const int sl = R.row_slot[row];
+        const int job = R.slot_job[sl];
+        photoerr_row(c, seed_by_job[job], catalog_offset_by_job[job] + (row - R.slot_row_begin[sl]), t, row);
+    }
+}
+
+cudaError_t launch_photoerrors_multi(const PerrTables &c, const uint64_t *seed_by_job, const int64_t *catalog_offset_by_job,
+                                     MultiRows R, gf_table t, int64_t begin, int64_t end, cudaStream_t s)
+{
+    if (end <= begin) return cudaSuccess;
+    photoerr_multi_kernel<<<grid_for(end - begin, 256), 256, 0, s>>>(c, seed_by_job, catalog_offset_by_job, R, t, begin, end);
+    count_launches(1);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_photoerrors(const PerrTables &c, int64_t row_offset, gf_table t, int64_t begin, int64_t end, cudaStream_t s)

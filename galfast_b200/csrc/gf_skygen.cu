@@ -33,23 +33,6 @@
 
 namespace gfk {
 
-/* One model crawl of one request: everything the CTA of a stream needs. */
-struct CrawlJob {
-    SkyModel m;
-    SkyGeom g;
-    CrawlState st;
-    uint32_t *rng;                 /* persistent stream state [3][rng_nstreams] */
-    int32_t rng_nstreams;
-    int32_t pix_base;              /* first pixel of this launch within the generator's pixel list */
-    const int64_t *limits;         /* per-stream star limit for this launch (draw) */
-    double *counts, *countsCovered;   /* integrate outputs, per stream */
-    double *per_pixel;             /* integrate output, per pixel (optional) */
-    const float *Dtab;             /* distances D[im][iM] of the model's bins */
-    FastDiv fx, fy;                /* division by nm and by nM */
-    int32_t job_id;                /* bits 16.. of StarRecord::stream */
-    int32_t pad;
-};
-
 struct CrawlParams {
     CrawlJob job0;                 /* the job of a single-request launch */
     const CrawlJob *jobs;          /* multi-request launch: device job table, or null */
@@ -64,6 +47,7 @@ struct CrawlParams {
     Checkpoint *ck;                /* draw: checkpoint buffer, or null */
     uint32_t *ck_count;
     int32_t ck_capacity, ck_every;
+    uint32_t *next_item;           /* persistent launch: work-queue counter (items taken in order), or null */
 };
 
 #define GF_CW 4                    /* warps per stream */
@@ -435,7 +419,7 @@ __device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float
             const int NS = J.rng_nstreams;
             S.v = ((uint64_t)J.rng[NS + tid] << 32) | J.rng[2 * NS + tid];
             S.nstars = st.nstars[tid];
-            S.limit = J.limits[tid];
+            S.limit = J.limits ? J.limits[tid] : J.limit_all;
             S.next_ck = (int)S.nstars;
             S.nrec = 0;
         }
@@ -701,13 +685,25 @@ __device__ void fill_tables(const SkyModel &m, float *LFM, float *MMr)
     for (int q = threadIdx.x; q < m.nm; q += blockDim.x) MMr[q] = m.m0 + m.dm * (float)q;
 }
 
+/* next work item of a CTA: a static stride, or the shared queue of a persistent launch */
+__device__ __forceinline__ int next_work_item(const CrawlParams &P, int *slot, int it)
+{
+    if (!P.next_item) return it + gridDim.x;
+    __syncthreads();
+    if (threadIdx.x == 0) *slot = (int)atomicAdd(P.next_item, 1u);
+    __syncthreads();
+    return *slot;
+}
+
 template <int DRAW, int MODEL>
 __global__ void __launch_bounds__(GF_WIN, DRAW ? 4 : 6) crawl_kernel(CrawlParams P)
 {
     extern __shared__ float s_tab[];
     __shared__ CrawlSmem<DRAW> S;
+    __shared__ int s_item;
     int loaded = -1;
-    for (int it = blockIdx.x; it < P.nitems; it += gridDim.x) {
+    int it = P.next_item ? next_work_item(P, &s_item, 0) : (int)blockIdx.x;
+    for (; it < P.nitems; it = next_work_item(P, &s_item, it)) {
         int job = 0, tid;
         if (P.items) {
             const uint32_t w = P.items[it];
@@ -773,58 +769,64 @@ __device__ __forceinline__ void deproject(const gf_lambert &p, double &l, double
     l = p.l0 + gfm::atan2_d((double)x * sc, (double)p.cb * cc / ir - (double)(y * p.sb) * sc);
 }
 
-__global__ void __launch_bounds__(256) place_kernel(PlaceParams P)
+/* Placement of one star record (draw_stars, skygen.cu.h:376-456) into row i of
+ * the unsorted columns; returns whether the star is visible. */
+__device__ __forceinline__ int place_one(const SkyModel &m, const SkyGeom &g, const StarRecord &rec, int64_t i, int64_t n,
+                                         const PlaceParams &P)
 {
     const double r2d = 57.2957795130823208767981548;
+    const gf_pencil_beam pix = g.pixels[rec.ilb];
+    float M = m.M1 - (float)rec.iM * m.dM;
+    float x = pix.X, y = pix.Y;
+    x += pix.dx * (rec.u[0] - 0.5f);
+    y += pix.dx * (rec.u[1] - 0.5f);
+    if (x * x + y * y > 2.f) {
+        P.hidden[i] = 1;
+        P.key[i] = ~0ull;
+        return 0;
+    }
+    P.projIdx[i] = pix.projIdx;
+    P.projXY[i] = x;
+    P.projXY[n + i] = y;
+    double l, b;
+    deproject(g.proj[pix.projIdx], l, b, x, y);
+    float cl = (float)gfm::cos_d(l), cb = (float)gfm::cos_d(b);
+    float sl = (float)gfm::sin_d(l), sb = (float)gfm::sin_d(b);
+    l *= r2d;
+    if (l < 0.) l += 360.;
+    if (l > 360.) l -= 360.;
+    b *= r2d;
+    P.lb[i] = l;
+    P.lb[n + i] = b;
+    float Mtmp = M + m.dM * (rec.u[2] - 0.5f);
+    float mtmp = m.m0 + m.dm * ((float)rec.im + rec.u[3] - 0.5f);
+    float DM = mtmp - Mtmp;
+    P.absmag[i] = Mtmp;
+    P.DM[i] = DM;
+    float D = gfm::powf_(10.f, 0.2f * DM + 1.f);
+    P.XYZ[i] = D * cl * cb;
+    P.XYZ[n + i] = D * sl * cb;
+    P.XYZ[2 * n + i] = D * sb;
+    float Am0 = (g.ext_kind == GF_EXT_SCREEN_CSCB) ? g.A0 / fabsf(sb) : 0.f;
+    float AmInf = Am0;
+    int hid = (mtmp + Am0 > m.m1) ? 1 : 0;
+    /* the beam extinction at the bin's anchor (draw_stars, skygen.cu.h:437-446) */
+    const float AmMin = gfc::beam_extinction(g, pix);
+    if (AmMin > Am0) AmInf = -AmMin;
+    P.Am[i] = Am0;
+    P.AmInf[i] = AmInf;
+    P.hidden[i] = hid;
+    /* l >= 0 here (-0.0 compares equal to 0.0 and maps to key 0) */
+    P.key[i] = hid ? ~0ull : (l == 0.0 ? 0ull : (uint64_t)__double_as_longlong(l));
+    return hid ? 0 : 1;
+}
+
+__global__ void __launch_bounds__(256) place_kernel(PlaceParams P)
+{
     unsigned vis_local = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += (int64_t)gridDim.x * blockDim.x) {
         const StarRecord rec = P.rec[i];
-        const SkyModel &m = P.m;
-        const gf_pencil_beam pix = P.g.pixels[rec.ilb];
-        const int64_t n = P.n;
-        float M = m.M1 - (float)rec.iM * m.dM;
-        float x = pix.X, y = pix.Y;
-        x += pix.dx * (rec.u[0] - 0.5f);
-        y += pix.dx * (rec.u[1] - 0.5f);
-        if (x * x + y * y > 2.f) {
-            P.hidden[i] = 1;
-            P.key[i] = ~0ull;
-            continue;
-        }
-        P.projIdx[i] = pix.projIdx;
-        P.projXY[i] = x;
-        P.projXY[n + i] = y;
-        double l, b;
-        deproject(P.g.proj[pix.projIdx], l, b, x, y);
-        float cl = (float)gfm::cos_d(l), cb = (float)gfm::cos_d(b);
-        float sl = (float)gfm::sin_d(l), sb = (float)gfm::sin_d(b);
-        l *= r2d;
-        if (l < 0.) l += 360.;
-        if (l > 360.) l -= 360.;
-        b *= r2d;
-        P.lb[i] = l;
-        P.lb[n + i] = b;
-        float Mtmp = M + m.dM * (rec.u[2] - 0.5f);
-        float mtmp = m.m0 + m.dm * ((float)rec.im + rec.u[3] - 0.5f);
-        float DM = mtmp - Mtmp;
-        P.absmag[i] = Mtmp;
-        P.DM[i] = DM;
-        float D = gfm::powf_(10.f, 0.2f * DM + 1.f);
-        P.XYZ[i] = D * cl * cb;
-        P.XYZ[n + i] = D * sl * cb;
-        P.XYZ[2 * n + i] = D * sb;
-        float Am0 = (P.g.ext_kind == GF_EXT_SCREEN_CSCB) ? P.g.A0 / fabsf(sb) : 0.f;
-        float AmInf = Am0;
-        int hid = (mtmp + Am0 > m.m1) ? 1 : 0;
-        /* the beam extinction at the bin's anchor (draw_stars, skygen.cu.h:437-446) */
-        const float AmMin = gfc::beam_extinction(P.g, pix);
-        if (AmMin > Am0) AmInf = -AmMin;
-        P.Am[i] = Am0;
-        P.AmInf[i] = AmInf;
-        P.hidden[i] = hid;
-        /* l >= 0 here (-0.0 compares equal to 0.0 and maps to key 0) */
-        P.key[i] = hid ? ~0ull : (l == 0.0 ? 0ull : (uint64_t)__double_as_longlong(l));
-        vis_local += hid ? 0u : 1u;
+        vis_local += (unsigned)place_one(P.m, P.g, rec, i, P.n, P);
     }
     /* warp-aggregated count of visible stars */
     for (int o = 16; o > 0; o >>= 1) vis_local += __shfl_xor_sync(0xffffffffu, vis_local, o);
@@ -1062,6 +1064,258 @@ cudaError_t launch_jump_tables(const uint32_t *mult, int n, uint64_t *lo, uint64
 {
     jump_table_kernel<<<(n + 127) / 128, 128, 0, s>>>(mult, n, lo, hi);
     return cudaGetLastError();
+}
+
+}  // namespace gfk
+
+/* ------------------------------------------------------------------ */
+/* Device side of the multi-request run (gf_catalog_run_multi)        */
+/* ------------------------------------------------------------------ */
+namespace gfk {
+
+/* x_n of the 48-bit LCG behind drand48/lrand48 (x' = 0x5DEECE66D x + 11 mod 2^48)
+ * after n steps from x0, by composing the affine map with itself. */
+__device__ __forceinline__ uint64_t lcg48_jump(uint64_t x0, uint64_t n)
+{
+    const uint64_t M = (1ull << 48) - 1;
+    uint64_t acc_a = 1, acc_c = 0, cur_a = 0x5DEECE66Dull, cur_c = 0xBull;
+    while (n) {
+        if (n & 1) {
+            acc_a = (acc_a * cur_a) & M;
+            acc_c = (acc_c * cur_a + cur_c) & M;
+        }
+        cur_c = (cur_c * cur_a + cur_c) & M;
+        cur_a = (cur_a * cur_a) & M;
+        n >>= 1;
+    }
+    return (acc_a * x0 + acc_c) & M;
+}
+
+/* The stream states of many requests at once, identical to gfh::seed_streams:
+ * srand48(seed); per stream i in order: c = (int)(drand48() * a_i) (x86 gives
+ * INT_MIN out of range), x = lrand48() (cux.cpp:404-414). */
+__global__ void seed_streams_kernel(const uint32_t *seeds, int njobs, const uint32_t *mult, int NS, uint32_t *rng)
+{
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (int64_t)njobs * NS) return;
+    const int j = (int)(g / NS), i = (int)(g % NS);
+    const uint64_t x0 = ((uint64_t)seeds[j] << 16) | 0x330Eull;
+    const uint64_t x1 = lcg48_jump(x0, 2ull * i + 1);
+    const uint64_t x2 = (0x5DEECE66Dull * x1 + 0xBull) & ((1ull << 48) - 1);
+    const uint32_t prime = mult[i];
+    const double t = ((double)x1 * 0x1p-48) * (double)prime;
+    const int32_t c = (t >= 2147483648.0) ? INT32_MIN : (int32_t)t;
+    uint32_t *r = rng + (size_t)j * 3 * NS;
+    r[i] = prime;
+    r[NS + i] = (uint32_t)c;
+    r[2 * NS + i] = (uint32_t)(x2 >> 17);
+}
+
+cudaError_t launch_seed_streams(const uint32_t *seeds, int njobs, const uint32_t *mult, int NS, uint32_t *rng, cudaStream_t s)
+{
+    const int64_t n = (int64_t)njobs * NS;
+    if (n <= 0) return cudaSuccess;
+    seed_streams_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(seeds, njobs, mult, NS, rng);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+template <int DRAW, int MODEL>
+static cudaError_t start_crawl_persistent(const CrawlParams &P, size_t smem, cudaStream_t s)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(crawl_kernel<DRAW, MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, crawl_kernel<DRAW, MODEL>, GF_WIN, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    int grid = sm_count() * per_sm;
+    if (grid > P.nitems) grid = P.nitems;
+    crawl_kernel<DRAW, MODEL><<<grid, GF_WIN, smem, s>>>(P);
+    return cudaSuccess;
+}
+
+cudaError_t launch_crawl_multi(const LaunchCrawlMulti &L, int draw, cudaStream_t s)
+{
+    if (L.nitems <= 0) return cudaSuccess;
+    CrawlParams P;
+    memset(&P, 0, sizeof(P));
+    P.jobs = L.jobs;
+    P.items = L.items;
+    P.nitems = L.nitems;
+    P.next_item = L.counter;
+    P.jt = L.jt;
+    P.rec = L.rec;
+    P.rec_capacity = L.rec_capacity;
+    P.rec_count = L.rec_count;
+    P.err = L.err;
+    P.ck_every = 64;
+    const size_t smem = (size_t)L.max_tab * sizeof(float);
+    if (smem > 64 * 1024) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(L.counter, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    const bool disk = L.model_type == GF_MODEL_EXP_DISK;
+    if (draw) e = disk ? start_crawl_persistent<1, GF_MODEL_EXP_DISK>(P, smem, s) : start_crawl_persistent<1, GF_MODEL_POWER_LAW_ELLIPSOID>(P, smem, s);
+    else e = disk ? start_crawl_persistent<0, GF_MODEL_EXP_DISK>(P, smem, s) : start_crawl_persistent<0, GF_MODEL_POWER_LAW_ELLIPSOID>(P, smem, s);
+    if (e != cudaSuccess) return e;
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+/* placement of the records of many requests; slotkey = output position of the record's request */
+__global__ void __launch_bounds__(256) place_multi_kernel(PlaceParams P, const CrawlJob *jobs, const int32_t *job_slot,
+                                                          uint32_t *slotkey)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const StarRecord rec = P.rec[i];
+        const int job = rec.stream >> 16;
+        const CrawlJob &J = jobs[job];
+        place_one(J.m, J.g, rec, i, P.n, P);
+        slotkey[i] = (uint32_t)job_slot[job];
+    }
+}
+
+__global__ void gather_u32_kernel(const uint32_t *src, const uint32_t *idx, uint32_t *dst, int64_t n)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[idx[i]];
+}
+
+__global__ void gather_u64_kernel(const uint64_t *src, const uint32_t *idx, uint64_t *dst, int64_t n)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[idx[i]];
+}
+
+/* per output slot: first sorted position, end of its visible rows (hidden rows
+ * carry the largest key and sort last within the slot) and end of the slot */
+__global__ void segment_bounds_kernel(const uint32_t *slot, const uint64_t *key, int64_t n, int64_t *seg_begin,
+                                      int64_t *vis_end, int64_t *seg_end)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t sl = slot[i];
+        const bool first = (i == 0) || slot[i - 1] != sl;
+        const bool last = (i + 1 == n) || slot[i + 1] != sl;
+        if (first) seg_begin[sl] = i;
+        if (last) seg_end[sl] = i + 1;
+        const bool hid = key[i] == ~0ull;
+        if (hid && (first || key[i - 1] != ~0ull)) vis_end[sl] = i;
+        if (!hid && last) vis_end[sl] = i + 1;
+    }
+}
+
+/* runs of equal (slot, l) ordered by (b, DM, M, Am) (star_comp, skyconfig_impl.h:58-67) */
+__global__ void tie_multi_kernel(const uint64_t *key, const uint32_t *slot, uint32_t *idx, int64_t n, const double *lb,
+                                 const float *DM, const float *absmag, const float *Am, int64_t pitch)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (key[i] == ~0ull) continue;
+        if (i + 1 >= n || key[i] != key[i + 1] || slot[i] != slot[i + 1]) continue;
+        if (i > 0 && key[i - 1] == key[i] && slot[i - 1] == slot[i]) continue;
+        int64_t e = i + 1;
+        while (e + 1 < n && key[e + 1] == key[i] && slot[e + 1] == slot[i]) e++;
+        for (int64_t q = i + 1; q <= e; q++) {
+            uint32_t cur = idx[q];
+            int64_t r = q - 1;
+            while (r >= i) {
+                uint32_t o = idx[r];
+                bool less;
+                if (lb[pitch + cur] != lb[pitch + o]) less = lb[pitch + cur] < lb[pitch + o];
+                else if (DM[cur] != DM[o]) less = DM[cur] < DM[o];
+                else if (absmag[cur] != absmag[o]) less = absmag[cur] < absmag[o];
+                else less = Am[cur] < Am[o];
+                if (!less) break;
+                idx[r + 1] = o;
+                r--;
+            }
+            idx[r + 1] = cur;
+        }
+    }
+}
+
+/* visible rows of each slot into the output table at row_begin[slot]; row_slot maps rows back */
+__global__ void __launch_bounds__(256) gather_multi_kernel(GatherParams G, const uint32_t *slot, const int64_t *seg_begin,
+                                                           const int64_t *vis_end, const int64_t *row_begin,
+                                                           const int32_t *slot_comp, int32_t *row_slot)
+{
+    const int64_t P = G.out.capacity, S = G.src_pitch;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < G.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t sl = slot[i];
+        if (i >= vis_end[sl]) continue;
+        const int64_t o = row_begin[sl] + (i - seg_begin[sl]);
+        const uint32_t s = G.idx[i];
+        G.out.lb[o] = G.lb[s];
+        G.out.lb[P + o] = G.lb[S + s];
+        G.out.projIdx[o] = G.projIdx[s];
+        G.out.projXY[o] = G.projXY[s];
+        G.out.projXY[P + o] = G.projXY[S + s];
+        G.out.DM[o] = G.DM[s];
+        G.out.absmag[o] = G.absmag[s];
+        G.out.XYZ[o] = G.XYZ[s];
+        G.out.XYZ[P + o] = G.XYZ[S + s];
+        G.out.XYZ[2 * P + o] = G.XYZ[2 * S + s];
+        G.out.comp[o] = slot_comp[sl];
+        G.out.Am[o] = G.Am[s];
+        G.out.AmInf[o] = G.AmInf[s];
+        G.out.hidden[o] = 0;
+        row_slot[o] = (int32_t)sl;
+    }
+}
+
+cudaError_t launch_place_sort_multi(const LaunchPlaceMulti &L, cudaStream_t s)
+{
+    if (L.n <= 0) return cudaSuccess;
+    const int blocks = (int)std::min<int64_t>((L.n + 255) / 256, (int64_t)sm_count() * 16);
+    PlaceParams P;
+    memset(&P, 0, sizeof(P));
+    P.rec = L.rec; P.n = L.n;
+    P.lb = L.lb; P.projIdx = L.projIdx; P.projXY = L.projXY; P.DM = L.DM; P.absmag = L.absmag;
+    P.XYZ = L.XYZ; P.Am = L.Am; P.AmInf = L.AmInf; P.hidden = L.hidden; P.key = L.key;
+    place_multi_kernel<<<blocks, 256, 0, s>>>(P, L.jobs, L.job_slot, L.slot_a);
+    iota_kernel<<<blocks, 256, 0, s>>>(L.idx_a, L.n);
+    /* by l, then (stable) by slot: the records of each request in star_comp order */
+    size_t tb = L.temp_bytes;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(L.temp, tb, L.key, L.key_b, L.idx_a, L.idx_b, (int)L.n, 0, 64, s);
+    if (e != cudaSuccess) return e;
+    gather_u32_kernel<<<blocks, 256, 0, s>>>(L.slot_a, L.idx_b, L.slot_b, L.n);
+    tb = L.temp_bytes;
+    e = cub::DeviceRadixSort::SortPairs(L.temp, tb, L.slot_b, L.slot_a, L.idx_b, L.idx_a, (int)L.n, 0, L.slot_bits, s);
+    if (e != cudaSuccess) return e;
+    gather_u64_kernel<<<blocks, 256, 0, s>>>(L.key, L.idx_a, L.key_b, L.n);
+    segment_bounds_kernel<<<blocks, 256, 0, s>>>(L.slot_a, L.key_b, L.n, L.seg_begin, L.vis_end, L.seg_end);
+    count_launches(6);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tie_gather_multi(const LaunchPlaceMulti &L, const int64_t *row_begin, const int32_t *slot_comp,
+                                    gf_table out, int32_t *row_slot, cudaStream_t s)
+{
+    if (L.n <= 0) return cudaSuccess;
+    const int blocks = (int)std::min<int64_t>((L.n + 255) / 256, (int64_t)sm_count() * 16);
+    tie_multi_kernel<<<blocks, 256, 0, s>>>(L.key_b, L.slot_a, L.idx_a, L.n, L.lb, L.DM, L.absmag, L.Am, L.n);
+    GatherParams G;
+    G.idx = L.idx_a; G.n = L.n; G.src_pitch = L.n;
+    G.lb = L.lb; G.projIdx = L.projIdx; G.projXY = L.projXY; G.DM = L.DM; G.absmag = L.absmag;
+    G.XYZ = L.XYZ; G.Am = L.Am; G.AmInf = L.AmInf; G.comp = 0; G.out = out;
+    gather_multi_kernel<<<blocks, 256, 0, s>>>(G, L.slot_a, L.seg_begin, L.vis_end, row_begin, slot_comp, row_slot);
+    count_launches(2);
+    return cudaGetLastError();
+}
+
+cudaError_t sort_temp_bytes_multi(int64_t n, size_t *bytes)
+{
+    size_t a = 0, b = 0;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, a, (const uint64_t *)nullptr, (uint64_t *)nullptr,
+                                                    (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)n);
+    if (e != cudaSuccess) return e;
+    e = cub::DeviceRadixSort::SortPairs(nullptr, b, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                        (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)n);
+    *bytes = a > b ? a : b;
+    return e;
 }
 
 }  // namespace gfk
