@@ -42,6 +42,7 @@ class CatalogStats(C.Structure):
 
 
 BatchCallback = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.POINTER(Table), C.c_int64)
+MultiCallback = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.POINTER(Table), C.POINTER(C.c_int64), C.POINTER(C.c_int64))
 
 _lib = None
 
@@ -93,6 +94,7 @@ def lib():
         L.gf_module_vel2pm.argtypes = [vp, C.POINTER(Vel2pmConfig), C.POINTER(Table), C.c_int64, C.c_int64]
         L.gf_module_gal2other.argtypes = [vp, C.c_int32, C.POINTER(Table), C.c_int64, C.c_int64]
         L.gf_catalog_run.argtypes = [vp, C.POINTER(Job), BatchCallback, vp, C.POINTER(CatalogStats)]
+        L.gf_catalog_run_multi.argtypes = [vp, C.POINTER(Job), C.c_int32, MultiCallback, vp, C.POINTER(CatalogStats)]
         L.gf_lambert_init.argtypes = [C.c_double, C.c_double, C.POINTER(Lambert)]
         L.gf_footprint_pixelize.argtypes = [C.POINTER(Footprint), C.c_double, C.POINTER(Lambert),
                                             C.POINTER(Extinction), C.POINTER(PencilBeam), C.POINTER(C.c_float),
@@ -159,6 +161,14 @@ class HostTable:
 
     def as_dict(self, names=None):
         return {n: np.array(self.col(n)) for n in (names or self.arrays.keys())}
+
+    def rows(self, a, b, names=None):
+        """Copies of rows [a, b) of every column (vector columns as (ncomp, b - a))."""
+        out = {}
+        for n in (names or self.arrays.keys()):
+            x = self.arrays[n]
+            out[n] = np.array(x[0, a:b] if x.shape[0] == 1 else x[:, a:b])
+        return out
 
 
 # ---------------------------------------------------------------------------
@@ -314,3 +324,40 @@ def run_catalog(ctx, w, sink=None):
     ccb = BatchCallback(cb)
     check(lib().gf_catalog_run(ctx.h, C.byref(job), ccb, None, C.byref(stats)))
     return stats
+
+
+def run_catalog_multi(ctx, workloads, sink=None, device_sink=None):
+    """gf_catalog_run_multi: the catalogs of many requests generated together.
+
+    sink(job, model, rows) receives each request's rows of each model in host
+    memory as a dict of column arrays (one download per model pass, then a split
+    by request);
+    device_sink(model, table_ptr, row_begin, row_count) sees the device table
+    instead.  Returns the per-request CatalogStats."""
+    n = len(workloads)
+    jobs = (Job * n)(*[w.job(Job) for w in workloads])
+    stats = (CatalogStats * n)()
+    cache = {}
+
+    def cb(user, model, tptr, rb, rc):
+        if device_sink is not None:
+            if device_sink(model, tptr, rb, rc):
+                return 1
+        if sink is None:
+            return 0
+        t = tptr.contents
+        key = (t.capacity, t.nbands)
+        if key not in cache:
+            cache[key] = HostTable(t.capacity, t.nbands)
+        h = cache[key]
+        if lib().gf_table_download(ctx.h, tptr, C.byref(h.t)) != 0:
+            return 1
+        for j in range(n):
+            if rc[j] > 0:
+                if sink(j, model, h.rows(rb[j], rb[j] + rc[j])):
+                    return 1
+        return 0
+
+    ccb = MultiCallback(cb)
+    check(lib().gf_catalog_run_multi(ctx.h, jobs, n, ccb, None, stats))
+    return list(stats)

@@ -193,23 +193,6 @@ gfk::LaunchCrawl crawl_launch(gf_skygen *s, ModelState &ms)
     return L;
 }
 
-/* save / restore the crawl state and the crawl streams of one model */
-gf_status snapshot(gf_skygen *s, ModelState &ms, bool restore)
-{
-    cudaStream_t st = s->ctx->stream;
-    const int N = s->nthreads, NS = s->ctx->rng_nstreams;
-    size_t bytes = crawl_state_bytes(N);
-    if (restore) GF_CUDA(cudaMemcpyAsync(ms.st_mem, ms.snap_mem, bytes, cudaMemcpyDeviceToDevice, st));
-    else GF_CUDA(cudaMemcpyAsync(ms.snap_mem, ms.st_mem, bytes, cudaMemcpyDeviceToDevice, st));
-    for (int k = 0; k < 3; k++) {
-        uint32_t *live = s->ctx->d_rng + (size_t)k * NS;
-        uint32_t *saved = s->d_rng_snap + (size_t)k * N;
-        if (restore) GF_CUDA(cudaMemcpyAsync(live, saved, 4 * (size_t)N, cudaMemcpyDeviceToDevice, st));
-        else GF_CUDA(cudaMemcpyAsync(saved, live, 4 * (size_t)N, cudaMemcpyDeviceToDevice, st));
-    }
-    return GF_OK;
-}
-
 /* copy streams [a, b) of the crawl state and of the crawl streams between live and snapshot */
 __global__ void copy_state_range(CrawlState dst, CrawlState src, uint32_t *rng_dst, int32_t dst_pitch,
                                  const uint32_t *rng_src, int32_t src_pitch, int32_t a, int32_t b)
@@ -226,17 +209,6 @@ __global__ void fill_range(int64_t *p, int n, int a, int b, int64_t v)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n && i >= a && i < b) p[i] = v;
-}
-
-/* restore streams [t, n) of a model's crawl state and streams from the snapshot */
-__global__ void restore_tail(CrawlState st, CrawlState snap, uint32_t *rng, int32_t NS, const uint32_t *rng_snap, int32_t n, int32_t t)
-{
-    int i = t + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    st.status[i] = snap.status[i]; st.blk_ilb[i] = snap.blk_ilb[i]; st.blk_k[i] = snap.blk_k[i]; st.pos[i] = snap.pos[i];
-    st.ndraw[i] = snap.ndraw[i]; st.cur_ilb[i] = snap.cur_ilb[i]; st.cur_im[i] = snap.cur_im[i]; st.cur_iM[i] = snap.cur_iM[i];
-    st.anc[i] = snap.anc[i]; st.nstars[i] = 0;
-    for (int k = 0; k < 3; k++) rng[(size_t)k * NS + i] = rng_snap[(size_t)k * n + i];
 }
 
 gf_status snapshot_range(gf_skygen *s, ModelState &ms, int a, int b, bool restore)
@@ -329,12 +301,6 @@ __global__ void set_limits(int64_t *lim, int n, int32_t t, int64_t Lt)
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     lim[i] = (i < t) ? 0 : (i == t ? Lt : 0);
-}
-
-__global__ void fill_i64(int64_t *p, int n, int64_t v)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) p[i] = v;
 }
 
 }  // namespace
@@ -974,17 +940,6 @@ gf_status gf_module_bond2010(gf_ctx *ctx, const gf_bond2010_config *cfg, gf_tabl
     GF_CUDA(gfk::launch_bond2010(*cfg, ctx->d_rng, ctx->rng_nstreams, *t, begin, end, ctx->stream));
     return GF_OK;
 }
-
-struct gf_photometry {
-    gfk::PhotTables tab;
-    float *d_colors = nullptr;
-    uint8_t *d_eflags = nullptr;
-};
-
-struct gf_photoerr {
-    gfk::PerrTables tab;
-    double *d_mag = nullptr, *d_sigma = nullptr;
-};
 
 gf_status gf_photometry_create(gf_ctx *ctx, const gf_photometry_config *cfg, gf_photometry **out)
 {

@@ -67,6 +67,17 @@ struct gf_ctx {
     int64_t prof_n[GF_PROF_NPHASES] = {};
 };
 
+struct gf_photometry {
+    gfk::PhotTables tab;
+    float *d_colors = nullptr;
+    uint8_t *d_eflags = nullptr;
+};
+
+struct gf_photoerr {
+    gfk::PerrTables tab;
+    double *d_mag = nullptr, *d_sigma = nullptr;
+};
+
 namespace gfa {
 
 gf_status check_ctx(gf_ctx *ctx);

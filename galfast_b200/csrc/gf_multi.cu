@@ -1,0 +1,595 @@
+/*
+ * gf_multi.cu -- many catalog requests per pass: gf_catalog_run_multi.
+ *
+ * The plain path (gf_catalog_run) generates one request at a time.  A small
+ * request -- a pencil beam of a few hundred pixels -- keeps only a fraction of
+ * the GPU busy: its crawl has 7680 short streams, and every launch, sort and
+ * module pass has fixed costs.  Here every pass runs over all requests at
+ * once:
+ *
+ *   seeding     the 65536 streams of every request, on the GPU (seed_streams_kernel)
+ *   integrate   one persistent crawl per model over the (request, stream) work queue
+ *   draw        one persistent crawl per model over the same queue, requests in
+ *               decreasing size so that the queue ends on small work
+ *   place/sort  all records at once, sorted by (request, star_comp order)
+ *   modules     one launch per module over the rows of all requests; Bond2010 and
+ *               the photometric errors use each row's own request (its streams,
+ *               its seed and catalog row numbers)
+ *
+ * Each request's catalog is the one gf_catalog_run produces for it alone, bit
+ * for bit, as long as every model's stars fit one output batch (the batch
+ * boundary rules of the plain path do not arise).  Requests whose expected
+ * counts come near their batch capacity, or whose grid makes crawl blocks
+ * straddle pixels (nm*nM not a multiple of 10), run through gf_catalog_run
+ * after the batched passes.
+ */
+#include "gf_ctx.h"
+#include "gf_host.h"
+#include "gf_safeprimes.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <tuple>
+#include <vector>
+
+using gfa::dev_alloc;
+using gfa::dev_free;
+using gfa::fail;
+using gfa::ProfScope;
+
+namespace {
+
+/* device allocations released together */
+struct Pool {
+    std::vector<void *> ptrs;
+    template <typename T>
+    gf_status alloc(T **p, size_t n)
+    {
+        GF_TRY(dev_alloc(p, n));
+        if (*p) ptrs.push_back((void *)*p);
+        return GF_OK;
+    }
+    ~Pool()
+    {
+        for (void *p : ptrs) cudaFree(p);
+    }
+};
+
+/* a buffer that only grows */
+template <typename T>
+struct Grow {
+    T *p = nullptr;
+    size_t n = 0;
+    gf_status need(size_t m)
+    {
+        if (m <= n) return GF_OK;
+        dev_free(p);
+        n = 0;
+        GF_TRY(dev_alloc(&p, m));
+        n = m;
+        return GF_OK;
+    }
+    ~Grow() { dev_free(p); }
+};
+
+/* content signature of the photometry and error tables of a request (the error
+ * seed is per request and not part of it) */
+std::string module_signature(const gf_job &J)
+{
+    std::string sig;
+    auto add = [&](const void *p, size_t n) { sig.append((const char *)p, n); };
+    if (J.phot) {
+        gf_photometry_config c = *J.phot;
+        const size_t n = (size_t)(c.nbands > 1 ? c.nbands - 1 : 0) * (size_t)c.nMr * (size_t)c.nFeH;
+        const float *colors = c.colors;
+        const uint8_t *eflags = c.eflags;
+        c.colors = nullptr;
+        c.eflags = nullptr;
+        sig += "P";
+        add(&c, sizeof(c));
+        if (colors) add(colors, 4 * n);
+        if (eflags) add(eflags, n);
+    }
+    if (J.perr) {
+        gf_photoerr_config c = *J.perr;
+        const size_t n = (size_t)c.nbands * (size_t)c.nknots;
+        const double *mag = c.mag, *sigma = c.sigma;
+        c.mag = c.sigma = nullptr;
+        c.seed = 0;
+        sig += "E";
+        add(&c, sizeof(c));
+        if (mag) add(mag, 8 * n);
+        if (sigma) add(sigma, 8 * n);
+    }
+    return sig;
+}
+
+bool same_cfg(const void *a, const void *b, size_t n)
+{
+    if (!a || !b) return a == b;
+    return memcmp(a, b, n) == 0;
+}
+
+struct ReqInfo {
+    std::vector<gfh::HostModel> hm;    /* models in component order */
+    std::vector<gf_model_config> mc;
+    int64_t pix_off = 0;
+    bool plain = false;
+    int group = 0;
+    int slot = -1;
+    double cost = 0;
+};
+
+/* CrawlState slices of one request inside the arrays of all requests */
+CrawlState slice(const CrawlState &a, size_t off)
+{
+    CrawlState s;
+    s.status = a.status + off; s.blk_ilb = a.blk_ilb + off; s.blk_k = a.blk_k + off; s.pos = a.pos + off;
+    s.ndraw = a.ndraw + off; s.cur_ilb = a.cur_ilb + off; s.cur_im = a.cur_im + off; s.cur_iM = a.cur_iM + off;
+    s.anc = a.anc + off; s.nstars = a.nstars + off;
+    return s;
+}
+
+struct PlainForward {
+    gf_multi_callback cb;
+    void *user;
+    int32_t njobs, job;
+    std::vector<int64_t> begin, count;
+};
+
+int forward_plain_batch(void *u, int32_t model, const gf_table *dev, int64_t row_offset)
+{
+    (void)row_offset;
+    PlainForward *f = (PlainForward *)u;
+    if (!f->cb) return 0;
+    std::fill(f->begin.begin(), f->begin.end(), 0);
+    std::fill(f->count.begin(), f->count.end(), 0);
+    f->count[f->job] = dev->size;
+    return f->cb(f->user, model, dev, f->begin.data(), f->count.data());
+}
+
+}  // namespace
+
+extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, void *user,
+                                          gf_catalog_stats *stats)
+{
+    GF_TRY(gfa::check_ctx(ctx));
+    if (!jobs || njobs <= 0 || njobs > 32767) return fail(GF_E_INVALID, "njobs must be in [1, 32767]");
+    const gf_job &J0 = jobs[0];
+    const int N = J0.sky.nthreads;
+    const int nmod = J0.nmodels;
+    if (N <= 0 || N > GF_MAX_STREAMS) return fail(GF_E_INVALID, "nthreads must be in [1, 65536]");
+    if (nmod <= 0 || nmod > GF_MAX_MODELS) return fail(GF_E_INVALID, "invalid model count");
+    int NS = 0, nbands = 0;
+    for (int j = 0; j < njobs; j++) {
+        const gf_job &J = jobs[j];
+        if (J.sky.nthreads != N || J.nmodels != nmod)
+            return fail(GF_E_INVALID, "all requests of a multi-request run need the same nthreads and model count");
+        if (!J.pixels || J.npixels <= 0 || !J.models) return fail(GF_E_INVALID, "request without pixels or models");
+        if (J.sky.nstars != 0.f) return fail(GF_E_UNSUPPORTED, "forced star counts (nstars) need gf_catalog_run");
+        if (J.nstreams <= 0) return fail(GF_E_INVALID, "every request of a multi-request run seeds its own streams (nstreams > 0)");
+        if (J.capacity <= 0 || J.capacity > (int64_t)256 * GF_MAX_STREAMS) return fail(GF_E_INVALID, "invalid capacity");
+        int ns = J.nstreams > GF_MAX_STREAMS ? GF_MAX_STREAMS : J.nstreams;
+        if (ns % 64) ns += 64 - ns % 64;
+        if (ns < N) return fail(GF_E_INVALID, "nstreams below nthreads");
+        if (J.kin && (J.capacity + 255) / 256 > ns) return fail(GF_E_INVALID, "capacity above 256 rows per stream (Bond2010)");
+        NS = std::max(NS, ns);
+        nbands = std::max(nbands, (int)J.nbands);
+        if (!!J.feh != !!J0.feh || !!J.kin != !!J0.kin || !!J.v2pm != !!J0.v2pm || J.gal2other != J0.gal2other ||
+            !!J.phot != !!J0.phot || !!J.perr != !!J0.perr)
+            return fail(GF_E_INVALID, "all requests of a multi-request run need the same modules");
+        if (!same_cfg(J.feh, J0.feh, sizeof(gf_fixedfeh_config)) || !same_cfg(J.kin, J0.kin, sizeof(gf_bond2010_config)) ||
+            !same_cfg(J.v2pm, J0.v2pm, sizeof(gf_vel2pm_config)))
+            return fail(GF_E_INVALID, "fixedFeH, Bond2010 and vel2pm configurations must agree across requests");
+    }
+    GF_TRY(gfa::ensure_multipliers(ctx));
+    cudaStream_t st = ctx->stream;
+
+    std::vector<gf_catalog_stats> local(njobs);
+    gf_catalog_stats *S = stats ? stats : local.data();
+    for (int j = 0; j < njobs; j++) {
+        memset(&S[j], 0, sizeof(gf_catalog_stats));
+        S[j].norm = 1.f;
+    }
+
+    /* ---- host set-up of every request ---- */
+    std::vector<ReqInfo> R(njobs);
+    int64_t pix_total = 0;
+    std::map<std::string, int> groups;          /* module-table signature -> group */
+    std::vector<int> group_rep;                 /* a request of each group */
+    for (int j = 0; j < njobs; j++) {
+        const gf_job &J = jobs[j];
+        ReqInfo &q = R[j];
+        q.mc.assign(J.models, J.models + nmod);
+        std::stable_sort(q.mc.begin(), q.mc.end(), [](const gf_model_config &a, const gf_model_config &b) { return a.comp < b.comp; });
+        std::string err;
+        if (!gfh::setup_models(J.sky, J.npixels, q.mc.data(), nmod, q.hm, err)) return fail(GF_E_INVALID, err);
+        for (int i = 0; i < nmod; i++) {
+            if (q.hm[i].m.type != R[0].hm[i].m.type)
+                return fail(GF_E_INVALID, "model kinds must agree across requests (in component order)");
+            const long long kmax = (long long)q.hm[i].m.nm * q.hm[i].m.nM;
+            if (kmax % GF_BLOCK) q.plain = true;
+            if (q.hm[i].m.nm + q.hm[i].m.nM > 16384) q.plain = true;
+        }
+        q.pix_off = pix_total;
+        pix_total += J.npixels;
+        q.cost = (double)J.npixels * q.hm[0].m.nm;
+        const std::string key = module_signature(J);
+        auto it = groups.find(key);
+        if (it == groups.end()) {
+            it = groups.insert({key, (int)groups.size()}).first;
+            group_rep.push_back(j);
+        }
+        q.group = it->second;
+    }
+
+    Pool pool;
+    gf_pencil_beam *d_pix = nullptr;
+    float *d_ammin = nullptr, *d_lf = nullptr;
+    GF_TRY(pool.alloc(&d_pix, (size_t)pix_total));
+    GF_TRY(pool.alloc(&d_ammin, (size_t)pix_total));
+    GF_TRY(pool.alloc(&d_lf, (size_t)njobs * nmod * 1024));
+    {
+        std::vector<float> lf((size_t)njobs * nmod * 1024, 0.f);
+        for (int j = 0; j < njobs; j++) {
+            GF_CUDA(cudaMemcpyAsync(d_pix + R[j].pix_off, jobs[j].pixels, sizeof(gf_pencil_beam) * (size_t)jobs[j].npixels,
+                                    cudaMemcpyHostToDevice, st));
+            if (jobs[j].beam_ammin)
+                GF_CUDA(cudaMemcpyAsync(d_ammin + R[j].pix_off, jobs[j].beam_ammin, 4 * (size_t)jobs[j].npixels,
+                                        cudaMemcpyHostToDevice, st));
+            for (int i = 0; i < nmod; i++)
+                std::copy(R[j].hm[i].lf.begin(), R[j].hm[i].lf.end(), lf.begin() + ((size_t)j * nmod + i) * 1024);
+        }
+        GF_CUDA(cudaMemcpyAsync(d_lf, lf.data(), 4 * lf.size(), cudaMemcpyHostToDevice, st));
+        GF_CUDA(cudaStreamSynchronize(st));
+    }
+    /* distance tables D[im][iM], shared by the requests with the same magnitude grid */
+    std::map<std::tuple<float, float, float, float, int>, std::pair<int, float *>> dtabs;
+    for (int j = 0; j < njobs; j++)
+        for (int i = 0; i < nmod; i++) {
+            const SkyModel &m = R[j].hm[i].m;
+            auto k = std::make_tuple(m.m0, m.dm, m.M1, m.dM, m.nM);
+            auto &e = dtabs[k];
+            e.first = std::max(e.first, m.nm);
+        }
+    for (auto &kv : dtabs) {
+        SkyModel m;
+        memset(&m, 0, sizeof(m));
+        m.m0 = std::get<0>(kv.first); m.dm = std::get<1>(kv.first); m.M1 = std::get<2>(kv.first); m.dM = std::get<3>(kv.first);
+        m.nM = std::get<4>(kv.first);
+        m.nm = kv.second.first;
+        GF_TRY(pool.alloc(&kv.second.second, (size_t)m.nm * m.nM));
+        GF_CUDA(gfk::launch_dtab(m, kv.second.second, st));
+    }
+    auto dtab_of = [&](const SkyModel &m) { return dtabs[std::make_tuple(m.m0, m.dm, m.M1, m.dM, m.nM)].second; };
+
+    /* ---- streams of every request ---- */
+    uint32_t *d_rng = nullptr, *d_rng_snap = nullptr, *d_seeds = nullptr;
+    GF_TRY(pool.alloc(&d_rng, (size_t)njobs * 3 * NS));
+    GF_TRY(pool.alloc(&d_rng_snap, (size_t)njobs * 3 * NS));
+    GF_TRY(pool.alloc(&d_seeds, (size_t)njobs));
+    {
+        std::vector<uint32_t> seeds(njobs);
+        for (int j = 0; j < njobs; j++) seeds[j] = jobs[j].seed48;
+        GF_CUDA(cudaMemcpyAsync(d_seeds, seeds.data(), 4 * (size_t)njobs, cudaMemcpyHostToDevice, st));
+        GF_CUDA(gfk::launch_seed_streams(d_seeds, njobs, ctx->d_mult, NS, d_rng, st));
+    }
+
+    /* ---- per-(request, stream) state ---- */
+    const size_t nall = (size_t)njobs * N;
+    CrawlState cs;
+    {
+        char *base = nullptr;
+        const size_t bytes = nall * (8 * 4 + 16 + 8) + 256;
+        GF_TRY(pool.alloc(&base, bytes));
+        char *p = base;
+        auto take = [&](size_t b) { char *r = p; p += (b + 15) & ~(size_t)15; return r; };
+        cs.anc = (AnchorX *)take(16 * nall);
+        cs.nstars = (int64_t *)take(8 * nall);
+        cs.status = (int32_t *)take(4 * nall); cs.blk_ilb = (int32_t *)take(4 * nall); cs.blk_k = (int32_t *)take(4 * nall);
+        cs.pos = (int32_t *)take(4 * nall); cs.ndraw = (int32_t *)take(4 * nall); cs.cur_ilb = (int32_t *)take(4 * nall);
+        cs.cur_im = (int32_t *)take(4 * nall); cs.cur_iM = (int32_t *)take(4 * nall);
+    }
+    const size_t cs_bytes = nall * (8 * 4 + 16 + 8) + 256;
+    char *cs_base = (char *)cs.anc;
+    double *d_counts = nullptr;
+    CrawlJob *d_jobs = nullptr;
+    uint32_t *d_items = nullptr, *d_counter = nullptr;
+    GF_TRY(pool.alloc(&d_counts, 2 * nall));
+    GF_TRY(pool.alloc(&d_jobs, (size_t)njobs));
+    GF_TRY(pool.alloc(&d_items, nall));
+    GF_TRY(pool.alloc(&d_counter, 1));
+
+    auto crawl_job = [&](int j, int i) {
+        CrawlJob c;
+        memset(&c, 0, sizeof(c));
+        c.m = R[j].hm[i].m;
+        c.m.lf = d_lf + ((size_t)j * nmod + i) * 1024;
+        c.g.pixels = d_pix + R[j].pix_off;
+        c.g.npixels = jobs[j].npixels;
+        c.g.ammin = jobs[j].beam_ammin ? d_ammin + R[j].pix_off : nullptr;
+        c.g.ext_kind = jobs[j].ext.kind;
+        c.g.A0 = jobs[j].ext.A0;
+        c.g.proj[0] = jobs[j].sky.proj[0];
+        c.g.proj[1] = jobs[j].sky.proj[1];
+        c.st = slice(cs, (size_t)j * N);
+        c.rng = d_rng + (size_t)j * 3 * NS;
+        c.rng_nstreams = NS;
+        c.counts = d_counts + (size_t)j * N;
+        c.countsCovered = d_counts + nall + (size_t)j * N;
+        c.Dtab = dtab_of(c.m);
+        c.fx = make_fastdiv((uint32_t)c.m.nm);
+        c.fy = make_fastdiv((uint32_t)c.m.nM);
+        c.job_id = j;
+        c.limit_all = jobs[j].capacity;
+        return c;
+    };
+    /* work items: requests in decreasing size, all streams of each */
+    auto upload_items = [&](const std::vector<int> &order, int32_t *nitems) -> gf_status {
+        std::vector<uint32_t> items;
+        items.reserve(order.size() * N);
+        for (int j : order)
+            for (int t = 0; t < N; t++) items.push_back(((uint32_t)j << 16) | (uint32_t)t);
+        GF_CUDA(cudaMemcpyAsync(d_items, items.data(), 4 * items.size(), cudaMemcpyHostToDevice, st));
+        GF_CUDA(cudaStreamSynchronize(st));
+        *nitems = (int32_t)items.size();
+        return GF_OK;
+    };
+    std::vector<int> order_all(njobs);
+    for (int j = 0; j < njobs; j++) order_all[j] = j;
+    std::stable_sort(order_all.begin(), order_all.end(), [&](int a, int b) { return R[a].cost > R[b].cost; });
+    auto max_tab = [&](int i, const std::vector<int> &js) {
+        int mt = 0;
+        for (int j : js) mt = std::max(mt, R[j].hm[i].m.nm + R[j].hm[i].m.nM);
+        return mt;
+    };
+
+    /* ---- integrate every model of every request (os_skygen.cpp:875-880) ---- */
+    std::vector<CrawlJob> hj(njobs);
+    std::vector<double> hc(2 * nall);
+    std::vector<int> integ;
+    for (int j : order_all)
+        if (!R[j].plain) integ.push_back(j);
+    int32_t nitems = 0;
+    if (!integ.empty()) GF_TRY(upload_items(integ, &nitems));
+    for (int i = 0; i < nmod && !integ.empty(); i++) {
+        for (int j = 0; j < njobs; j++) hj[j] = crawl_job(j, i);
+        GF_CUDA(cudaMemcpyAsync(d_jobs, hj.data(), sizeof(CrawlJob) * (size_t)njobs, cudaMemcpyHostToDevice, st));
+        GF_CUDA(cudaMemsetAsync(d_counts, 0, 16 * nall, st));
+        gfk::LaunchCrawlMulti L;
+        memset(&L, 0, sizeof(L));
+        L.jobs = d_jobs; L.items = d_items; L.nitems = nitems; L.counter = d_counter;
+        L.model_type = R[integ[0]].hm[i].m.type;
+        L.max_tab = max_tab(i, integ);
+        L.jt = ctx->jt;
+        {
+            ProfScope ps(ctx, GF_PROF_INTEGRATE);
+            GF_CUDA(gfk::launch_crawl_multi(L, 0, st));
+        }
+        GF_CUDA(cudaMemcpyAsync(hc.data(), d_counts, 16 * nall, cudaMemcpyDeviceToHost, st));
+        GF_CUDA(cudaStreamSynchronize(st));
+        for (int j : integ) {
+            double e = 0, ec = 0;
+            for (int t = 0; t < N; t++) {
+                e += hc[(size_t)j * N + t];
+                ec += hc[nall + (size_t)j * N + t];
+            }
+            S[j].expected[i] = e;
+            S[j].expected_covered[i] = ec;
+            /* room for the Poisson spread of the model's stars in one batch */
+            if (e + 8.0 * sqrt(e) + 1024.0 >= (double)jobs[j].capacity) R[j].plain = true;
+        }
+    }
+
+    /* ---- requests generated together, in output order (by module group) ---- */
+    std::vector<int> batched, slot_job;
+    for (int j : order_all)
+        if (!R[j].plain) batched.push_back(j);
+    slot_job = batched;
+    std::stable_sort(slot_job.begin(), slot_job.end(), [&](int a, int b) { return R[a].group != R[b].group ? R[a].group < R[b].group : a < b; });
+    const int nslots = (int)slot_job.size();
+    for (int s = 0; s < nslots; s++) R[slot_job[s]].slot = s;
+    std::vector<int32_t> job_slot(njobs, 0);
+    for (int j = 0; j < njobs; j++) job_slot[j] = R[j].slot < 0 ? 0 : R[j].slot;
+
+    if (nslots > 0) {
+        GF_TRY(upload_items(batched, &nitems));
+        int32_t *d_job_slot = nullptr, *d_slot_job = nullptr, *d_slot_comp = nullptr;
+        int64_t *d_seg = nullptr, *d_row_begin = nullptr, *d_slot_rows = nullptr, *d_chunk_begin = nullptr, *d_catoff = nullptr;
+        uint64_t *d_pseed = nullptr;
+        gf_footprint *d_foot = nullptr;
+        GF_TRY(pool.alloc(&d_job_slot, (size_t)njobs));
+        GF_TRY(pool.alloc(&d_slot_job, (size_t)nslots));
+        GF_TRY(pool.alloc(&d_slot_comp, (size_t)nslots));
+        GF_TRY(pool.alloc(&d_seg, 3 * (size_t)nslots));
+        GF_TRY(pool.alloc(&d_row_begin, (size_t)nslots + 1));
+        GF_TRY(pool.alloc(&d_slot_rows, (size_t)nslots));
+        GF_TRY(pool.alloc(&d_chunk_begin, (size_t)nslots));
+        GF_TRY(pool.alloc(&d_catoff, (size_t)njobs));
+        GF_TRY(pool.alloc(&d_pseed, (size_t)njobs));
+        GF_TRY(pool.alloc(&d_foot, (size_t)njobs));
+        GF_CUDA(cudaMemcpyAsync(d_job_slot, job_slot.data(), 4 * (size_t)njobs, cudaMemcpyHostToDevice, st));
+        GF_CUDA(cudaMemcpyAsync(d_slot_job, slot_job.data(), 4 * (size_t)nslots, cudaMemcpyHostToDevice, st));
+        bool any_foot = false;
+        std::vector<gf_footprint> foot(njobs);
+        std::vector<uint64_t> pseed(njobs, 0);
+        for (int j = 0; j < njobs; j++) {
+            memset(&foot[j], 0, sizeof(gf_footprint));
+            if (jobs[j].foot) { foot[j] = *jobs[j].foot; any_foot = any_foot || foot[j].kind != GF_FOOT_ALL; }
+            if (jobs[j].perr) pseed[j] = jobs[j].perr->seed;
+        }
+        GF_CUDA(cudaMemcpyAsync(d_foot, foot.data(), sizeof(gf_footprint) * (size_t)njobs, cudaMemcpyHostToDevice, st));
+        GF_CUDA(cudaMemcpyAsync(d_pseed, pseed.data(), 8 * (size_t)njobs, cudaMemcpyHostToDevice, st));
+        /* photometry and photometric-error tables of each module group */
+        struct GroupMods { gf_photometry *ph = nullptr; gf_photoerr *pe = nullptr; };
+        std::vector<GroupMods> gm(groups.size());
+        struct ModGuard {
+            std::vector<GroupMods> *g;
+            ~ModGuard() { for (auto &x : *g) { gf_photometry_destroy(x.ph); gf_photoerr_destroy(x.pe); } }
+        } mod_guard{&gm};
+        for (int g = 0; g < (int)group_rep.size(); g++) {
+            const gf_job &J = jobs[group_rep[g]];
+            if (J.phot) GF_TRY(gf_photometry_create(ctx, J.phot, &gm[g].ph));
+            if (J.perr) GF_TRY(gf_photoerr_create(ctx, J.perr, &gm[g].pe));
+        }
+
+        /* growing buffers of the draw passes */
+        Grow<StarRecord> rec;
+        Grow<double> lb;
+        Grow<int32_t> projIdx, hidden, row_slot;
+        Grow<float> projXY, DMc, absmag, XYZ, Am, AmInf;
+        Grow<uint64_t> key, key_b;
+        Grow<uint32_t> idx_a, idx_b, slot_a, slot_b;
+        Grow<char> temp;
+        gf_table out;
+        memset(&out, 0, sizeof(out));
+        struct TableGuard { gf_ctx *c; gf_table *t; ~TableGuard() { gf_table_free(c, t); } } tg{ctx, &out};
+        std::vector<int64_t> catoff(njobs, 0);
+        int slot_bits = 1;
+        while ((1 << slot_bits) < nslots) slot_bits++;
+
+        for (int i = 0; i < nmod; i++) {
+            for (int j = 0; j < njobs; j++) hj[j] = crawl_job(j, i);
+            GF_CUDA(cudaMemcpyAsync(d_jobs, hj.data(), sizeof(CrawlJob) * (size_t)njobs, cudaMemcpyHostToDevice, st));
+            double want = 65536;
+            for (int j : batched) want += S[j].expected[i] + 8.0 * sqrt(S[j].expected[i]) + 1024.0;
+            int64_t cap = (int64_t)want;
+            GF_CUDA(cudaMemcpyAsync(d_rng_snap, d_rng, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
+            int64_t nrec = 0;
+            for (;;) {
+                GF_TRY(rec.need((size_t)cap));
+                GF_CUDA(cudaMemsetAsync(cs_base, 0, cs_bytes, st));
+                GF_CUDA(cudaMemsetAsync(ctx->d_counters, 0, 24, st));
+                gfk::LaunchCrawlMulti L;
+                memset(&L, 0, sizeof(L));
+                L.jobs = d_jobs; L.items = d_items; L.nitems = nitems; L.counter = d_counter;
+                L.model_type = R[batched[0]].hm[i].m.type;
+                L.max_tab = max_tab(i, batched);
+                L.jt = ctx->jt;
+                L.rec = rec.p; L.rec_capacity = (int64_t)rec.n;
+                L.rec_count = ctx->d_counters; L.err = ctx->d_counters + 2;
+                {
+                    ProfScope ps(ctx, GF_PROF_DRAW_WINDOW);
+                    GF_CUDA(gfk::launch_crawl_multi(L, 1, st));
+                }
+                GF_CUDA(cudaMemcpyAsync(ctx->h_counters, ctx->d_counters, 24, cudaMemcpyDeviceToHost, st));
+                GF_CUDA(cudaStreamSynchronize(st));
+                nrec = (int64_t)ctx->h_counters[0];
+                if (ctx->h_counters[2]) return fail(GF_E_INVALID, "a bin has an infinite expected star count");
+                if (nrec <= (int64_t)rec.n) break;
+                /* more stars than the buffer holds: restore the streams and draw again */
+                GF_CUDA(cudaMemcpyAsync(d_rng, d_rng_snap, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
+                cap = nrec + nrec / 8 + 65536;
+            }
+            /* placement and the (request, star_comp) sort */
+            const size_t n = (size_t)std::max<int64_t>(nrec, 1);
+            GF_TRY(lb.need(2 * n)); GF_TRY(projIdx.need(n)); GF_TRY(hidden.need(n)); GF_TRY(projXY.need(2 * n));
+            GF_TRY(DMc.need(n)); GF_TRY(absmag.need(n)); GF_TRY(XYZ.need(3 * n)); GF_TRY(Am.need(n)); GF_TRY(AmInf.need(n));
+            GF_TRY(key.need(n)); GF_TRY(key_b.need(n)); GF_TRY(idx_a.need(n)); GF_TRY(idx_b.need(n));
+            GF_TRY(slot_a.need(n)); GF_TRY(slot_b.need(n));
+            size_t tb = 0;
+            GF_CUDA(gfk::sort_temp_bytes_multi((int64_t)n, &tb));
+            GF_TRY(temp.need(tb + 256));
+            GF_CUDA(cudaMemsetAsync(d_seg, 0, 24 * (size_t)nslots, st));
+            gfk::LaunchPlaceMulti PL;
+            memset(&PL, 0, sizeof(PL));
+            PL.jobs = d_jobs; PL.job_slot = d_job_slot; PL.rec = rec.p; PL.n = nrec;
+            PL.lb = lb.p; PL.projIdx = projIdx.p; PL.projXY = projXY.p; PL.DM = DMc.p; PL.absmag = absmag.p;
+            PL.XYZ = XYZ.p; PL.Am = Am.p; PL.AmInf = AmInf.p; PL.hidden = hidden.p; PL.key = key.p; PL.key_b = key_b.p;
+            PL.idx_a = idx_a.p; PL.idx_b = idx_b.p; PL.slot_a = slot_a.p; PL.slot_b = slot_b.p; PL.slot_bits = slot_bits;
+            PL.temp = temp.p; PL.temp_bytes = temp.n;
+            PL.seg_begin = d_seg; PL.vis_end = d_seg + nslots; PL.seg_end = d_seg + 2 * nslots;
+            {
+                ProfScope ps(ctx, GF_PROF_SORT);
+                GF_CUDA(gfk::launch_place_sort_multi(PL, st));
+            }
+            std::vector<int64_t> seg(3 * (size_t)nslots);
+            GF_CUDA(cudaMemcpyAsync(seg.data(), d_seg, 24 * (size_t)nslots, cudaMemcpyDeviceToHost, st));
+            GF_CUDA(cudaStreamSynchronize(st));
+            std::vector<int64_t> row_begin(nslots + 1, 0), slot_rows(nslots), chunk_begin(nslots);
+            std::vector<int32_t> slot_comp(nslots);
+            int64_t nchunks = 0;
+            for (int s = 0; s < nslots; s++) {
+                const int j = slot_job[s];
+                const int64_t gen = seg[2 * nslots + s] - seg[s];
+                const int64_t vis = gen > 0 ? seg[nslots + s] - seg[s] : 0;
+                if (gen >= jobs[j].capacity)
+                    return fail(GF_E_STATE, "a request drew a full output batch in the multi-request run; run it with gf_catalog_run");
+                S[j].generated[i] = gen;
+                S[j].stored[i] = vis;
+                if (vis > 0) S[j].batches++;
+                slot_rows[s] = vis;
+                row_begin[s + 1] = row_begin[s] + vis;
+                chunk_begin[s] = nchunks;
+                nchunks += (vis + 255) / 256;
+                slot_comp[s] = R[j].hm[i].m.comp;
+            }
+            const int64_t total = row_begin[nslots];
+            if (out.capacity < std::max<int64_t>(total, 1)) {
+                gf_table_free(ctx, &out);
+                GF_TRY(gf_table_alloc(ctx, std::max<int64_t>(total + total / 8, 1024), nbands, &out));
+            }
+            GF_TRY(row_slot.need((size_t)out.capacity));
+            GF_CUDA(cudaMemcpyAsync(d_row_begin, row_begin.data(), 8 * (size_t)(nslots + 1), cudaMemcpyHostToDevice, st));
+            GF_CUDA(cudaMemcpyAsync(d_slot_rows, slot_rows.data(), 8 * (size_t)nslots, cudaMemcpyHostToDevice, st));
+            GF_CUDA(cudaMemcpyAsync(d_chunk_begin, chunk_begin.data(), 8 * (size_t)nslots, cudaMemcpyHostToDevice, st));
+            GF_CUDA(cudaMemcpyAsync(d_slot_comp, slot_comp.data(), 4 * (size_t)nslots, cudaMemcpyHostToDevice, st));
+            GF_CUDA(cudaMemcpyAsync(d_catoff, catoff.data(), 8 * (size_t)njobs, cudaMemcpyHostToDevice, st));
+            {
+                ProfScope ps(ctx, GF_PROF_SORT);
+                GF_CUDA(gfk::launch_tie_gather_multi(PL, d_row_begin, d_slot_comp, out, row_slot.p, st));
+            }
+            out.size = total;
+            /* the module chain in pipeline order (pipeline.h:75-88) over every request's rows */
+            gfk::MultiRows MR;
+            MR.row_slot = row_slot.p; MR.slot_row_begin = d_row_begin; MR.slot_job = d_slot_job;
+            if (total > 0) {
+                if (any_foot) {
+                    ProfScope ps(ctx, GF_PROF_CLIPPER);
+                    GF_CUDA(gfk::launch_clipper_multi(d_foot, MR, out, 0, total, st));
+                }
+                if (J0.feh) GF_TRY(gf_module_fixedfeh(ctx, J0.feh, &out, 0, total));
+                if (J0.kin) {
+                    ProfScope ps(ctx, GF_PROF_BOND2010);
+                    GF_CUDA(gfk::launch_bond2010_multi(*J0.kin, d_rng, NS, MR, d_chunk_begin, nslots, nchunks, d_slot_rows, out, st));
+                }
+                int s0 = 0;
+                while (s0 < nslots) {
+                    const int g = R[slot_job[s0]].group;
+                    int s1 = s0;
+                    while (s1 < nslots && R[slot_job[s1]].group == g) s1++;
+                    const int64_t b = row_begin[s0], e = row_begin[s1];
+                    if (gm[g].ph) GF_TRY(gf_module_photometry(ctx, gm[g].ph, &out, b, e));
+                    if (gm[g].pe) {
+                        ProfScope ps(ctx, GF_PROF_PHOTOERR);
+                        GF_CUDA(gfk::launch_photoerrors_multi(gm[g].pe->tab, d_pseed, d_catoff, MR, out, b, e, st));
+                    }
+                    s0 = s1;
+                }
+                if (J0.v2pm) GF_TRY(gf_module_vel2pm(ctx, J0.v2pm, &out, 0, total));
+                if (J0.gal2other) GF_TRY(gf_module_gal2other(ctx, J0.gal2other, &out, 0, total));
+            }
+            GF_CUDA(cudaStreamSynchronize(st));
+            if (cb) {
+                std::vector<int64_t> rb(njobs, 0), rc(njobs, 0);
+                for (int s = 0; s < nslots; s++) { rb[slot_job[s]] = row_begin[s]; rc[slot_job[s]] = slot_rows[s]; }
+                if (cb(user, R[batched[0]].hm[i].m.comp, &out, rb.data(), rc.data()) != 0)
+                    return fail(GF_E_STATE, "stopped by the batch callback");
+            }
+            for (int s = 0; s < nslots; s++) catoff[slot_job[s]] += slot_rows[s];
+        }
+    }
+
+    /* ---- requests that need the batch rules of the plain path ---- */
+    for (int j = 0; j < njobs; j++) {
+        if (!R[j].plain) continue;
+        PlainForward f;
+        f.cb = cb; f.user = user; f.njobs = njobs; f.job = j;
+        f.begin.assign(njobs, 0);
+        f.count.assign(njobs, 0);
+        GF_TRY(gf_catalog_run(ctx, &jobs[j], forward_plain_batch, &f, &S[j]));
+    }
+    return GF_OK;
+}

@@ -22,6 +22,9 @@ D2R = math.pi / 180.0
 # SDSS-like extinction-to-reddening ratios A_b / E(B-V) for u g r i z
 SDSS_AE = np.array([5.155, 3.793, 2.751, 2.086, 1.479])
 SDSS_M5 = np.array([22.5, 23.0, 23.0, 23.0, 22.2])
+# LSST-like u g r i z y: the same ratios plus y, 5-sigma depths one magnitude deeper
+LSST_AE = np.array([5.155, 3.793, 2.751, 2.086, 1.479, 1.263])
+LSST_M5 = np.array([23.5, 24.0, 24.0, 24.0, 23.2, 22.9])
 
 
 def lf_table():
@@ -36,8 +39,8 @@ def color_coefficients(nbands=5, seed=20240611):
     the colours band_i - band_(i+1); base colours of a main-sequence-like locus."""
     rng = np.random.default_rng(seed)
     a = rng.normal(0.0, 0.1, size=(nbands - 1, 4))
-    base = np.array([1.2, 0.45, 0.18, 0.08, 0.05][: nbands - 1])
-    slope = np.array([0.6, 0.55, 0.35, 0.2, 0.15][: nbands - 1])
+    base = np.array([1.2, 0.45, 0.18, 0.08, 0.05, 0.04][: nbands - 1])
+    slope = np.array([0.6, 0.55, 0.35, 0.2, 0.15, 0.1][: nbands - 1])
     a[:, 0] += base
     a[:, 1] += slope
     return a
@@ -259,7 +262,8 @@ def build_workload(lib, *, foot, dx_deg, m0, m1, nthreads=7680, seed48=42, capac
     ph.nbands = nbands
     ph.bidx = 2
     red = np.ones(A.GF_MAX_BANDS, dtype=np.float32)
-    red[:nbands] = (SDSS_AE[:nbands] / SDSS_AE[2]).astype(np.float32) if nbands <= 5 else 1.0
+    AE = SDSS_AE if nbands <= 5 else LSST_AE
+    red[:nbands] = (AE[:nbands] / AE[2]).astype(np.float32)
     for i in range(A.GF_MAX_BANDS):
         ph.reddening[i] = float(red[i])
     ph.nFeH, ph.nMr = nFeH.value, nMr.value

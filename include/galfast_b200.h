@@ -372,6 +372,30 @@ typedef int (*gf_batch_callback)(void *user, int32_t model, const gf_table *dev_
 
 gf_status gf_catalog_run(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, void *user, gf_catalog_stats *stats);
 
+/* ---- many requests per pass ---- */
+
+/* Called once per model with the device table holding that model's rows of
+ * every request: the rows of request j are [row_begin[j], row_begin[j] +
+ * row_count[j]) (njobs entries each, host memory).  Requests that run alone
+ * (below) deliver their batches through the same callback with only their own
+ * entry nonzero.  A nonzero return stops the run (GF_E_STATE). */
+typedef int (*gf_multi_callback)(void *user, int32_t model, const gf_table *dev_rows, const int64_t *row_begin,
+                                 const int64_t *row_count);
+
+/* The catalogs of njobs independent requests (os_skygen::run + the module
+ * chain of each, as gf_catalog_run), generated together: every crawl, sort
+ * and module pass covers all requests at once.  Each request's rows are those
+ * gf_catalog_run produces for it alone, bit for bit.  A request whose expected
+ * stars of some model reach its batch capacity (within 8 sigma), or whose grid
+ * has nm*nM not a multiple of 10, runs alone through gf_catalog_run after the
+ * others.  All requests need the same nthreads, model kinds (in component
+ * order) and fixedFeH/Bond2010/vel2pm/gal2other settings, nstreams > 0 and
+ * nstars = 0; footprints, models, grids, seeds, capacities and photometry may
+ * differ.  stats: njobs entries or NULL.  No counterpart in the reference,
+ * which generates one catalog per process (os_skygen.cpp:866-932). */
+gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, void *user,
+                               gf_catalog_stats *stats);
+
 /* ---- expected counts without device allocation ---- */
 
 /* Expected star counts of ONE density model over a footprint, computed with

@@ -1,0 +1,98 @@
+"""gf_catalog_run_multi against gf_catalog_run (B200): every request's catalog
+is the one it gets alone, bit for bit, whether it was generated together with
+the others or (capacity too small for one batch) ran alone inside the multi
+call.  Requests differ in footprint, depth, model parameters, seed, capacity
+and photometric system."""
+import numpy as np
+import pytest
+
+import galfast_b200 as G
+from galfast_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+SKY = ["lb", "projIdx", "projXY", "DM", "absmag", "XYZ", "comp", "Am", "AmInf", "hidden"]
+MODULE = ["FeH", "vcyl", "mags", "photoflags", "obsmags", "pm", "radec"]
+
+
+def requests(lib, n=7):
+    reqs = W.config4_requests(n, seed=777)
+    ws = []
+    for k, r in enumerate(reqs):
+        r = dict(r)
+        r["r"] = 0.4 + 0.25 * k            # 0.4 .. 1.9 deg caps
+        r["rmax"] = 19.0 + 0.4 * k
+        kw = {}
+        if k % 3 == 2:
+            kw = dict(nbands=6, m5=W.LSST_M5)
+        w = W.config4_workload(lib, r, capacity=1 << 20, **kw)
+        ws.append(w)
+    # one request whose stars need several batches: it runs alone inside the multi call
+    ws[1].capacity = 400
+    return ws
+
+
+def catalog_alone(ctx, w):
+    per_model = {}
+
+    def sink(model, t, off):
+        d = t.as_dict()
+        per_model.setdefault(model, []).append(d)
+    st = G.run_catalog(ctx, w, sink=sink)
+    out = {}
+    for m, parts in per_model.items():
+        out[m] = {k: np.concatenate([p[k] for p in parts], axis=-1) for k in parts[0]}
+    return out, st
+
+
+def test_multi_request_rows_equal_standalone(lib):
+    ws = requests(lib)
+    ctx = G.Context(0)
+    got = {}
+
+    def sink(j, model, rows):
+        got.setdefault(j, {}).setdefault(model, []).append(rows)
+    stats = G.run_catalog_multi(ctx, ws, sink=sink)
+    assert len(got) == len(ws)
+    for j, w in enumerate(ws):
+        ref, st = catalog_alone(ctx, w)
+        assert sorted(ref) == sorted(got[j]), j
+        for m in ref:
+            parts = got[j][m]
+            mine = {k: np.concatenate([p[k] for p in parts], axis=-1) for k in parts[0]}
+            a, b = ref[m], mine
+            assert a["DM"].shape == b["DM"].shape, (j, m)
+            for c in SKY:
+                np.testing.assert_array_equal(a[c], b[c], err_msg="%s request %d model %d" % (c, j, m))
+            vis = a["hidden"] == 0
+            for c in MODULE:
+                if c not in a or a[c].size == 0:
+                    continue
+                x, y = a[c], b[c]
+                if c in ("mags", "obsmags"):
+                    y = y[: x.shape[0]]             # the shared table holds the most bands of any request
+                np.testing.assert_array_equal(x[..., vis], y[..., vis], err_msg="%s request %d model %d" % (c, j, m))
+        for i in range(3):
+            assert stats[j].expected[i] == st.expected[i]
+            assert stats[j].generated[i] == st.generated[i]
+        if j == 1:
+            assert stats[j].batches > 3        # the small-capacity request kept the plain batch rules
+    ctx.close()
+
+
+def test_multi_request_is_repeatable(lib):
+    ws = requests(lib, n=4)
+    ctx = G.Context(0)
+    runs = []
+    for _ in range(2):
+        got = {}
+
+        def sink(j, model, rows):
+            got.setdefault((j, model), []).append(rows["lb"].copy())
+        G.run_catalog_multi(ctx, ws, sink=sink)
+        runs.append(got)
+    assert runs[0].keys() == runs[1].keys()
+    for k in runs[0]:
+        for x, y in zip(runs[0][k], runs[1][k]):
+            np.testing.assert_array_equal(x, y)
+    ctx.close()
