@@ -1,22 +1,26 @@
 #!/usr/bin/env python
 """Catalog-generation throughput of galfast_b200 on B200 (stars/s).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config config2]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config config4]
 
-A step is one complete catalog request through gf_catalog_run: seeding of the
-65536 persistent MWC streams, the integrate pass of the three density models,
-every 16M-row output batch of each model (Poisson draws, placement, sort) and
-the module chain (clipper, fixedFeH, Bond2010, photometry, photometric errors,
-vel2pm, gal2other).  The default workload is the full-scale plain form: the
-whole sky at |b| > 10 deg in 0.1 deg pixels, 14 < r < 22 (3.41e6 pixels,
-3.9e11 bins, about 2.9e8 stars).
+Default workload: the batched form (config 4).  4096 independent catalog
+requests -- pencil beams with |b| > 5 deg, radii log-uniform in [0.5, 5] deg,
+r_max uniform in [19, 24], per-request thin-disk scale height and halo
+flattening, each with its own seed -- and the full module chain (clipper,
+fixedFeH, Bond2010, ugriz photometry, photometric errors, vel2pm, gal2other).
+A step generates all 4096 catalogs through gf_catalog_run_multi (one pass per
+model over every request).  The plain path -- gf_catalog_run, one request at a
+time -- is timed beside it on a fixed sample of the same requests (every 16th),
+and both lines' stars are catalog rows.
 
-`value` is device-resident throughput (the catalog stays in HBM); `e2e` is the
-same request with every batch copied to pinned host memory inside the timed
-region.  Multi-GPU runs are replicas (one independent request per rank, seed
-offset by rank, scaling "weak").  The CPU baseline is the reference path
-restated in C++ (oracle/, libm flavour) on a fixed 1/1000 subset of the
-pixels, single-threaded like the reference's CPU build.
+`value` keeps the catalogs in HBM (the call copies its host inputs in);
+`e2e` also copies every request's rows to pinned host memory inside the timed
+region.  --config config2 / config1 time the plain single-request path on the
+full-sky and NGP-patch workloads instead.  Multi-GPU runs are replicas (each
+rank its own 4096 requests, seeds offset by rank, scaling "weak").  The CPU
+baseline is the reference path restated in C++ (oracle/, libm flavour) on a
+fixed sample of the same workload, single-threaded like the reference's CPU
+build; --impl reference runs it on all host cores.
 """
 import argparse
 import ctypes as C
@@ -112,6 +116,66 @@ def workload(G, W, name, rank=0):
     return w, desc
 
 
+C4_NREQ = 4096
+C4_CAPACITY = 1 << 22          # rows per output batch of each request
+C4_PLAIN_STRIDE = 16           # the plain path is timed on every 16th request
+
+
+def config4_set(G, W, rank=0, nreq=C4_NREQ):
+    reqs = W.config4_requests(nreq, seed=1234567 + nreq * rank)
+    ws = W.config4_workloads(G.lib(), reqs, capacity=C4_CAPACITY)
+    desc = ("config4: %d pencil beams, centres uniform at |b|>5 deg, radius log-uniform 0.5-5 deg, 0.1 deg pixels, "
+            "14<r<U(19,24), thin-disk h U(250,350), halo q U(0.55,0.75), own seed each, ugriz, full module chain" % nreq)
+    return ws, desc
+
+
+def set_bins(ws):
+    b = d = 0
+    for w in ws:
+        bb, dd = model_bins(w)
+        b += bb
+        d += dd
+    return b, d
+
+
+def pinned_table(G, capacity, nbands):
+    """A HostTable whose columns are page-locked (the library's downloads run at full PCIe speed)."""
+    import torch
+    h = G.HostTable.__new__(G.HostTable)
+    h.capacity, h.nbands, h.arrays, h.keep = int(capacity), int(nbands), {}, []
+    h.t = G.Table()
+    h.t.capacity, h.t.nbands = capacity, nbands
+    for name, dt, nc in G.COLUMNS:
+        k = h.nbands if nc == "bands" else nc
+        if k == 0:
+            continue
+        buf = torch.empty(k * h.capacity * np.dtype(dt).itemsize, dtype=torch.uint8, pin_memory=True)
+        a = buf.numpy().view(dt).reshape(k, h.capacity)
+        h.arrays[name] = a
+        h.keep.append(buf)
+        setattr(h.t, name, a.ctypes.data)
+    return h
+
+
+def row_bytes(G, nbands):
+    return sum((nbands if nc == "bands" else nc) * np.dtype(dt).itemsize for _, dt, nc in G.COLUMNS)
+
+
+def cpu_baseline_set(G, O, ws, threads=1, budget_s=12.0):
+    """The reference CPU path (oracle, libm) on the set's first requests, in order,
+    until budget_s of CPU work (at least one request)."""
+    mult = np.zeros(65536, dtype=np.uint32)
+    G.lib().gf_multipliers(mult.ctypes.data_as(C.POINTER(C.c_uint32)), 65536)
+    stars, t_all, k = 0, 0.0, 0
+    while k < len(ws) and (k == 0 or t_all < budget_s):
+        t0 = time.perf_counter()
+        st, _ = O.run_catalog(ws[k], mult, flavour="l", threads=threads)
+        t_all += time.perf_counter() - t0
+        stars += sum(st["stored"].values())
+        k += 1
+    return stars / t_all, stars, t_all, k
+
+
 def model_bins(w):
     """bins and diagonals of the three models (same binning for each)."""
     nm = int(round((w.sky.m1 - w.sky.m0) / w.sky.dm))
@@ -119,7 +183,7 @@ def model_bins(w):
     return len(w.models) * w.npixels * nm * nM, len(w.models) * w.npixels * (nm + nM - 1)
 
 
-def cpu_baseline(G, W, O, w_full, flavour="l"):
+def cpu_baseline(G, W, O, w_full, flavour="l", threads=1):
     """The reference CPU path (oracle, libm) on every 1000th pixel of the workload."""
     import copy
     mult = np.zeros(65536, dtype=np.uint32)
@@ -136,7 +200,7 @@ def cpu_baseline(G, W, O, w_full, flavour="l"):
     sub.ammin = np.ascontiguousarray(w_full.ammin[idx])
     sub.keep = list(w_full.keep)
     t0 = time.perf_counter()
-    stats, _ = O.run_catalog(sub, mult, flavour=flavour)
+    stats, _ = O.run_catalog(sub, mult, flavour=flavour, threads=threads)
     dt = time.perf_counter() - t0
     stars = sum(stats["stored"].values())
     return stars / dt, stars, dt, len(idx)
@@ -145,11 +209,11 @@ def cpu_baseline(G, W, O, w_full, flavour="l"):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="config2")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--config", default="config4", choices=["config4", "config2", "config1"])
+    ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
@@ -173,19 +237,26 @@ def main():
             if dist is not None:
                 dist.destroy_process_group()
             return
-        w, desc = workload(G, W, args.config)
+        threads = os.cpu_count() or 1
+        if args.config == "config4":
+            ws, desc = config4_set(G, W, 0, nreq=8)
+            sample_fn = lambda: cpu_baseline_set(G, O, ws[:2], threads=threads, budget_s=0.0)
+            sample_desc = "the first 2 requests of the config-4 set, all modules, %d threads" % threads
+        else:
+            w, desc = workload(G, W, args.config)
+            sample_fn = lambda: cpu_baseline(G, W, O, w, threads=threads)
+            sample_desc = "every 1000th pixel of the workload, all modules, %d threads" % threads
         vals = []
         for i in range(args.warmup + args.steps):
-            v, stars, dt, npx = cpu_baseline(G, W, O, w)
+            v, stars, dt, npx = sample_fn()
             if i >= args.warmup:
                 vals.append((v, dt))
         value = float(np.mean([v for v, _ in vals]))
         line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "stars/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean([d for _, d in vals])),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": desc, "sample": "every 1000th pixel (%d pixels), full module chain" % npx},
-                "cpu_baseline": {"value": value, "unit": "stars/s", "cores": 1, "kind": "port",
-                                 "sample": "every 1000th pixel of the workload, single-threaded restatement (libm)"},
+                "config": {"workload": desc, "sample": sample_desc},
+                "cpu_baseline": {"value": value, "unit": "stars/s", "cores": threads, "kind": "port", "sample": sample_desc},
                 "e2e": {"value": value, "unit": "stars/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         if dist is not None:
@@ -194,6 +265,190 @@ def main():
 
     device = local_rank if world > 1 else 0
     ctx = G.Context(device)
+    if args.config == "config4":
+        bench_multi(args, G, W, ctx, rank, world, dist)
+    else:
+        bench_single(args, G, W, ctx, rank, world, dist)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+
+
+def clock_sampler(rank):
+    d = os.path.join(ROOT, "gpurun_out")
+    return ClockSampler(os.path.join(d, "bench_clocks_rank%d.csv" % rank) if os.path.isdir(d) else "/tmp/bench_clocks.csv")
+
+
+def reduce_max_sum(dist, tmax, tsum):
+    """(max over ranks of tmax, sum over ranks of tsum)"""
+    if dist is None:
+        return tmax, tsum
+    import torch
+    t = torch.tensor([tmax, tsum], dtype=torch.float64, device="cuda")
+    a, b = t[:1].clone(), t[1:].clone()
+    dist.all_reduce(a, op=dist.ReduceOp.MAX)
+    dist.all_reduce(b, op=dist.ReduceOp.SUM)
+    return float(a[0]), float(b[0])
+
+
+def draw_rooflines(pk, pk_kind, bins, diags, stars_step, npix_models, draw_ms, draw_launches, nsteps):
+    """HBM roofline of the draw crawl (algorithmic bytes: star records written and
+    beams read) and its issue roofline (per-bin / per-diagonal / per-star work of
+    the reference kernel against nominal B200 FP32, SFU and FP64 rates)."""
+    fp32 = 6.0 * bins + 60.0 * diags + 250.0 * stars_step
+    sfu = 1.0 * bins + 6.0 * diags + 40.0 * stars_step
+    fp64 = 150.0 * stars_step
+    bytes_alg = 32.0 * stars_step + 48.0 * npix_models
+    t_draw = draw_ms / 1e3 / nsteps if draw_ms else float("nan")
+    clk = (pk.get("sm_max_mhz") or 1965.0) * 1e6
+    pf32, psfu, pf64 = B200_SMS * FP32_PER_SM * clk, B200_SMS * SFU_PER_SM * clk, B200_SMS * FP64_PER_SM * clk
+    t_roof = max(fp32 / pf32, sfu / psfu, fp64 / pf64, bytes_alg / (pk["hbm_gbs"] * 1e9))
+    achieved = bytes_alg / t_draw / 1e9 if t_draw == t_draw else None
+    roofline = {"bound": "hbm", "kernel": "crawl_kernel<1> (draw pass)", "achieved": achieved,
+                "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": (achieved / pk["hbm_gbs"]) if achieved else None,
+                "traffic": None, "peak_source": pk_kind,
+                "algorithmic_bytes_per_launch": bytes_alg * nsteps / max(draw_launches, 1),
+                "avg_launch_ms": draw_ms / max(draw_launches, 1)}
+    compute = {"bound": "sfu/fp32 issue (nominal)", "kernel": "crawl_kernel<1> (draw pass)",
+               "t_bound_s": t_roof, "t_measured_s": t_draw, "frac": t_roof / t_draw if t_draw == t_draw else None,
+               "fp32_ops": fp32, "sfu_ops": sfu, "fp64_ops": fp64,
+               "peaks": {"fp32_ops_per_s": pf32, "sfu_ops_per_s": psfu, "fp64_ops_per_s": pf64, "clock_mhz": clk / 1e6}}
+    return roofline, compute
+
+
+def bench_multi(args, G, W, ctx, rank, world, dist):
+    """config 4: every request through gf_catalog_run_multi, the plain path on a sample."""
+    L = G.lib()
+    ws, desc = config4_set(G, W, rank)
+    n = len(ws)
+    jobs = (G.Job * n)(*[w.job(G.Job) for w in ws])
+    stats = (G.CatalogStats * n)()
+    nmod = len(ws[0].models)
+
+    def rows_of(st_list):
+        return sum(st.stored[i] for st in st_list for i in range(nmod))
+
+    NULL_MULTI = G.MultiCallback()
+    NULL_BATCH = G.BatchCallback()
+
+    def step(cb=None):
+        ctx.mark(0)
+        G.check(L.gf_catalog_run_multi(ctx.h, jobs, n, cb if cb is not None else NULL_MULTI, None, stats))
+        ctx.mark(1)
+        return ctx.elapsed_ms(0, 1), rows_of(stats)
+
+    for _ in range(args.warmup):
+        step()
+
+    # ---- timed region: batched, catalogs resident in HBM ----
+    ctx.profile(True)
+    ctx.profile_read()
+    if dist is not None:
+        dist.barrier()
+    ctx.sync()
+    n0 = L.gf_launch_count()
+    times, rows = [], []
+    clock = clock_sampler(rank)
+    with clock:
+        for _ in range(args.steps):
+            ms, r = step()
+            times.append(ms)
+            rows.append(r)
+    ctx.sync()
+    launches = L.gf_launch_count() - n0
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    total_ms, total_rows = reduce_max_sum(dist, float(np.sum(times)), float(np.sum(rows)))
+    value = total_rows / (total_ms / 1e3)
+    generated = sum(st.generated[i] for st in stats for i in range(nmod))
+
+    # ---- plain path: one request at a time (gf_catalog_run) on every 16th request ----
+    sample = list(range(0, n, C4_PLAIN_STRIDE))
+    st1 = G.CatalogStats()
+    for j in sample[:3]:
+        G.check(L.gf_catalog_run(ctx.h, C.byref(jobs[j]), NULL_BATCH, None, C.byref(st1)))
+    plain_ms, plain_rows = [], []
+    for j in sample:
+        ctx.mark(4)
+        G.check(L.gf_catalog_run(ctx.h, C.byref(jobs[j]), NULL_BATCH, None, C.byref(st1)))
+        ctx.mark(5)
+        plain_ms.append(ctx.elapsed_ms(4, 5))
+        plain_rows.append(rows_of([st1]))
+    pm, pr = reduce_max_sum(dist, float(np.sum(plain_ms)), float(np.sum(plain_rows)))
+    plain_value = pr / (pm / 1e3)
+
+    # ---- e2e: every request's rows copied to pinned host memory inside the timed region ----
+    e2e = None
+    if args.e2e_steps > 0:
+        nb_max = max(w.nbands for w in ws)
+        stage = {nb_max: pinned_table(G, C4_CAPACITY, nb_max)}      # page-locked, allocated before timing
+        d2h = [0]
+
+        def cb(user, model, tptr, rb, rc):
+            tb = tptr.contents
+            if tb.nbands not in stage:
+                stage.clear()
+                stage[tb.nbands] = pinned_table(G, C4_CAPACITY, tb.nbands)
+            h = stage[tb.nbands]
+            rbytes = row_bytes(G, tb.nbands)
+            for j in range(n):
+                if rc[j] > 0:
+                    if L.gf_table_download_rows(ctx.h, tptr, rb[j], rb[j] + rc[j], C.byref(h.t)) != 0:
+                        return 1
+                    d2h[0] += int(rc[j]) * rbytes
+            return 0
+        ccb = G.MultiCallback(cb)
+        e_ms, e_rows = [], []
+        for _ in range(args.e2e_steps):
+            d2h[0] = 0
+            ms, r = step(ccb)
+            e_ms.append(ms)
+            e_rows.append(r)
+        em, er = reduce_max_sum(dist, float(np.sum(e_ms)), float(np.sum(e_rows)))
+        h2d = sum(w.npixels * (C.sizeof(G.PencilBeam) + 4) + nmod * 1024 * 4 for w in ws)
+        e2e = {"value": er / (em / 1e3), "unit": "stars/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h[0])}
+
+    pk, pk_kind = peaks()
+    bins, diags = set_bins(ws)
+    draw_ms = prof.get("draw_window", (0, 0))[0]
+    draw_launches = prof.get("draw_window", (0, 0))[1]
+    roofline, compute = draw_rooflines(pk, pk_kind, bins, diags, generated, nmod * sum(w.npixels for w in ws),
+                                       draw_ms, draw_launches, args.steps)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        from oracle import oracle as O
+        v, s_, dt, k = cpu_baseline_set(G, O, ws, threads=1)
+        cpu = {"value": v, "unit": "stars/s", "cores": 1, "kind": "port",
+               "sample": "the first %d requests of the set, full module chain, single-threaded restatement (libm), %.1f s" % (k, dt)}
+
+    if rank == 0:
+        lat = np.array(times) / 1e3
+        plat = np.array(plain_ms) / 1e3
+        line = {"metric": METRIC, "value": value, "unit": "stars/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": float(np.mean(times)), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": desc, "requests": n, "pixels": int(sum(w.npixels for w in ws)),
+                           "bins_per_step": bins, "stars_per_step": float(np.mean(rows)), "generated_per_step": generated,
+                           "batch_rows_per_request": C4_CAPACITY, "nthreads": ws[0].sky.nthreads,
+                           "parallelism": "replicas" if world > 1 else "batched (gf_catalog_run_multi)",
+                           "l2": "inputs larger than L2 (%.0f MB of pencil beams, tens of GB of catalog per step)"
+                                 % (sum(w.npixels for w in ws) * 52 / 1e6),
+                           "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+                           "latency_note": "batched: every request of a step completes at the step's end"},
+                "plain": {"value": plain_value, "unit": "stars/s", "sample": "every %dth request (%d requests) through "
+                          "gf_catalog_run, one at a time" % (C4_PLAIN_STRIDE, len(sample)),
+                          "latency_p50_s": float(np.percentile(plat, 50)), "latency_p99_s": float(np.percentile(plat, 99))},
+                "batched_over_plain": value / plain_value if plain_value else None,
+                "e2e": e2e, "roofline": roofline, "compute_roofline": compute, "cpu_baseline": cpu,
+                "gpu_launches": int(launches), "clocks": clock.summary(),
+                "phases_ms_per_step": {k: v[0] / args.steps for k, v in prof.items()}}
+        print(json.dumps(line))
+
+
+def bench_single(args, G, W, ctx, rank, world, dist):
+    """config 1 / config 2: one request per step through gf_catalog_run."""
     w, desc = workload(G, W, args.config, rank)
     L = G.lib()
 
@@ -345,10 +600,6 @@ def main():
                 "gpu_launches": int(launches), "clocks": clock.summary(),
                 "phases_ms_per_step": {k: v[0] / nsteps for k, v in prof.items()}}
         print(json.dumps(line))
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
-    ctx.close()
 
 
 if __name__ == "__main__":

@@ -95,6 +95,8 @@ def lib():
         L.gf_module_gal2other.argtypes = [vp, C.c_int32, C.POINTER(Table), C.c_int64, C.c_int64]
         L.gf_catalog_run.argtypes = [vp, C.POINTER(Job), BatchCallback, vp, C.POINTER(CatalogStats)]
         L.gf_catalog_run_multi.argtypes = [vp, C.POINTER(Job), C.c_int32, MultiCallback, vp, C.POINTER(CatalogStats)]
+        L.gf_multi_set_memory_budget.argtypes = [vp, C.c_int64]
+        L.gf_table_download_rows.argtypes = [vp, C.POINTER(Table), C.c_int64, C.c_int64, C.POINTER(Table)]
         L.gf_lambert_init.argtypes = [C.c_double, C.c_double, C.POINTER(Lambert)]
         L.gf_footprint_pixelize.argtypes = [C.POINTER(Footprint), C.c_double, C.POINTER(Lambert),
                                             C.POINTER(Extinction), C.POINTER(PencilBeam), C.POINTER(C.c_float),
@@ -214,6 +216,10 @@ class Context:
         ms = C.c_float()
         check(lib().gf_ctx_elapsed(self.h, a, b, C.byref(ms)))
         return ms.value
+
+    def set_multi_budget(self, nbytes):
+        """Device bytes per chunk of gf_catalog_run_multi (0 = 60% of free memory)."""
+        check(lib().gf_multi_set_memory_budget(self.h, int(nbytes)))
 
     def rng_init(self, seed48, nstreams=65536):
         check(lib().gf_rng_init(self.h, seed48, nstreams))

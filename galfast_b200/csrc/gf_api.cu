@@ -335,6 +335,7 @@ gf_status gf_ctx_destroy(gf_ctx *ctx)
     if (!ctx) return GF_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    gfa::free_multi_ws(ctx);
     dev_free(ctx->d_rng);
     dev_free(ctx->d_mult);
     dev_free(ctx->jt.lo);
@@ -864,17 +865,20 @@ gf_status gf_table_free(gf_ctx *ctx, gf_table *t)
     return GF_OK;
 }
 
-gf_status gf_table_download(gf_ctx *ctx, const gf_table *dev, gf_table *host)
+gf_status gf_table_download_rows(gf_ctx *ctx, const gf_table *dev, int64_t begin, int64_t end, gf_table *host)
 {
     GF_TRY(check_ctx(ctx));
     if (!dev || !host) return fail(GF_E_INVALID, "null table");
-    if (host->capacity < dev->size) return fail(GF_E_INVALID, "host table too small");
-    const size_t n = (size_t)dev->size, P = (size_t)dev->capacity, H = (size_t)host->capacity;
+    if (begin < 0 || end < begin || end > dev->capacity) return fail(GF_E_INVALID, "invalid row range");
+    if (host->capacity < end - begin) return fail(GF_E_INVALID, "host table too small");
+    if (host->nbands < dev->nbands && (host->mags || host->obsmags)) return fail(GF_E_INVALID, "host table has fewer bands");
+    const size_t n = (size_t)(end - begin), P = (size_t)dev->capacity, H = (size_t)host->capacity, b0 = (size_t)begin;
     cudaStream_t st = ctx->stream;
     auto cp = [&](void *h, const void *d, size_t elem, int ncomp) -> gf_status {
         if (!h || !d || n == 0) return GF_OK;
         for (int k = 0; k < ncomp; k++)
-            GF_CUDA(cudaMemcpyAsync((char *)h + k * H * elem, (const char *)d + k * P * elem, n * elem, cudaMemcpyDeviceToHost, st));
+            GF_CUDA(cudaMemcpyAsync((char *)h + k * H * elem, (const char *)d + (k * P + b0) * elem, n * elem,
+                                    cudaMemcpyDeviceToHost, st));
         return GF_OK;
     };
     GF_TRY(cp(host->lb, dev->lb, 8, 2));
@@ -895,8 +899,14 @@ gf_status gf_table_download(gf_ctx *ctx, const gf_table *dev, gf_table *host)
     GF_TRY(cp(host->pm, dev->pm, 4, 3));
     GF_TRY(cp(host->radec, dev->radec, 8, 2));
     GF_CUDA(cudaStreamSynchronize(st));
-    host->size = dev->size;
+    host->size = end - begin;
     return GF_OK;
+}
+
+gf_status gf_table_download(gf_ctx *ctx, const gf_table *dev, gf_table *host)
+{
+    if (!dev) return fail(GF_E_INVALID, "null table");
+    return gf_table_download_rows(ctx, dev, 0, dev->size, host);
 }
 
 /* ---------------- modules ---------------- */

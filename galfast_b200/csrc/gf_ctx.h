@@ -9,6 +9,8 @@
 #include <vector>
 #include "gf_launch.h"
 
+struct MultiWS;
+
 namespace gfa {
 
 /* record the message returned by gf_last_error() and pass the status through */
@@ -65,6 +67,8 @@ struct gf_ctx {
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_pending;
     double prof_ms[GF_PROF_NPHASES] = {};
     int64_t prof_n[GF_PROF_NPHASES] = {};
+    int64_t multi_budget = 0;            /* device bytes per multi-request chunk (0: 60% of free memory) */
+    MultiWS *multi_ws = nullptr;         /* buffers of gf_catalog_run_multi kept between calls */
 };
 
 struct gf_photometry {
@@ -81,6 +85,7 @@ struct gf_photoerr {
 namespace gfa {
 
 gf_status check_ctx(gf_ctx *ctx);
+void free_multi_ws(gf_ctx *ctx);
 /* multipliers and jump tables of all 65536 streams on the context's device */
 gf_status ensure_multipliers(gf_ctx *ctx);
 

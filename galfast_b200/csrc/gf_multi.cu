@@ -132,6 +132,54 @@ CrawlState slice(const CrawlState &a, size_t off)
     return s;
 }
 
+}  // namespace
+
+/* Device buffers of gf_catalog_run_multi, kept by the context between calls
+ * (they only grow), so that repeated runs do not allocate. */
+struct MultiWS {
+    Grow<float> ammin;
+    Grow<int64_t> catoff;
+    Grow<int64_t> chunk_begin;
+    Grow<uint32_t> counter;
+    Grow<double> counts;
+    Grow<char> cs;
+    Grow<gf_footprint> foot;
+    Grow<uint32_t> items;
+    Grow<int32_t> job_slot;
+    Grow<CrawlJob> jobs;
+    Grow<float> lf;
+    Grow<gf_pencil_beam> pix;
+    Grow<uint64_t> pseed;
+    Grow<uint32_t> rng;
+    Grow<uint32_t> rng_snap;
+    Grow<int64_t> row_begin;
+    Grow<uint32_t> seeds;
+    Grow<int64_t> seg;
+    Grow<int32_t> slot_comp;
+    Grow<int32_t> slot_job;
+    Grow<int64_t> slot_rows;
+    Grow<StarRecord> rec;
+    Grow<double> lb;
+    Grow<int32_t> projIdx, hidden, row_slot;
+    Grow<float> projXY, DMc, absmag, XYZ, Am, AmInf;
+    Grow<uint64_t> key, key_b;
+    Grow<uint32_t> idx_a, idx_b, slot_a, slot_b;
+    Grow<char> temp;
+    gf_table out;
+    MultiWS() { memset(&out, 0, sizeof(out)); }
+};
+
+namespace gfa {
+void free_multi_ws(gf_ctx *ctx)
+{
+    if (!ctx->multi_ws) return;
+    gf_table_free(ctx, &ctx->multi_ws->out);
+    delete ctx->multi_ws;
+    ctx->multi_ws = nullptr;
+}
+}  // namespace gfa
+
+namespace {
 struct PlainForward {
     gf_multi_callback cb;
     void *user;
@@ -226,11 +274,16 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
     }
 
     Pool pool;
+    if (!ctx->multi_ws) ctx->multi_ws = new MultiWS();
+    MultiWS &ws = *ctx->multi_ws;
     gf_pencil_beam *d_pix = nullptr;
     float *d_ammin = nullptr, *d_lf = nullptr;
-    GF_TRY(pool.alloc(&d_pix, (size_t)pix_total));
-    GF_TRY(pool.alloc(&d_ammin, (size_t)pix_total));
-    GF_TRY(pool.alloc(&d_lf, (size_t)njobs * nmod * 1024));
+    GF_TRY(ws.pix.need((size_t)pix_total));
+    d_pix = ws.pix.p;
+    GF_TRY(ws.ammin.need((size_t)pix_total));
+    d_ammin = ws.ammin.p;
+    GF_TRY(ws.lf.need((size_t)njobs * nmod * 1024));
+    d_lf = ws.lf.p;
     {
         std::vector<float> lf((size_t)njobs * nmod * 1024, 0.f);
         for (int j = 0; j < njobs; j++) {
@@ -267,9 +320,12 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
 
     /* ---- streams of every request ---- */
     uint32_t *d_rng = nullptr, *d_rng_snap = nullptr, *d_seeds = nullptr;
-    GF_TRY(pool.alloc(&d_rng, (size_t)njobs * 3 * NS));
-    GF_TRY(pool.alloc(&d_rng_snap, (size_t)njobs * 3 * NS));
-    GF_TRY(pool.alloc(&d_seeds, (size_t)njobs));
+    GF_TRY(ws.rng.need((size_t)njobs * 3 * NS));
+    d_rng = ws.rng.p;
+    GF_TRY(ws.rng_snap.need((size_t)njobs * 3 * NS));
+    d_rng_snap = ws.rng_snap.p;
+    GF_TRY(ws.seeds.need((size_t)njobs));
+    d_seeds = ws.seeds.p;
     {
         std::vector<uint32_t> seeds(njobs);
         for (int j = 0; j < njobs; j++) seeds[j] = jobs[j].seed48;
@@ -283,7 +339,8 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
     {
         char *base = nullptr;
         const size_t bytes = nall * (8 * 4 + 16 + 8) + 256;
-        GF_TRY(pool.alloc(&base, bytes));
+        GF_TRY(ws.cs.need(bytes));
+    base = ws.cs.p;
         char *p = base;
         auto take = [&](size_t b) { char *r = p; p += (b + 15) & ~(size_t)15; return r; };
         cs.anc = (AnchorX *)take(16 * nall);
@@ -297,10 +354,14 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
     double *d_counts = nullptr;
     CrawlJob *d_jobs = nullptr;
     uint32_t *d_items = nullptr, *d_counter = nullptr;
-    GF_TRY(pool.alloc(&d_counts, 2 * nall));
-    GF_TRY(pool.alloc(&d_jobs, (size_t)njobs));
-    GF_TRY(pool.alloc(&d_items, nall));
-    GF_TRY(pool.alloc(&d_counter, 1));
+    GF_TRY(ws.counts.need(2 * nall));
+    d_counts = ws.counts.p;
+    GF_TRY(ws.jobs.need((size_t)njobs));
+    d_jobs = ws.jobs.p;
+    GF_TRY(ws.items.need(nall));
+    d_items = ws.items.p;
+    GF_TRY(ws.counter.need(1));
+    d_counter = ws.counter.p;
 
     auto crawl_job = [&](int j, int i) {
         CrawlJob c;
@@ -383,36 +444,62 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
         }
     }
 
-    /* ---- requests generated together, in output order (by module group) ---- */
-    std::vector<int> batched, slot_job;
+    /* ---- requests generated together ---- */
+    std::vector<int> batched_all;
     for (int j : order_all)
-        if (!R[j].plain) batched.push_back(j);
-    slot_job = batched;
-    std::stable_sort(slot_job.begin(), slot_job.end(), [&](int a, int b) { return R[a].group != R[b].group ? R[a].group < R[b].group : a < b; });
-    const int nslots = (int)slot_job.size();
-    for (int s = 0; s < nslots; s++) R[slot_job[s]].slot = s;
-    std::vector<int32_t> job_slot(njobs, 0);
-    for (int j = 0; j < njobs; j++) job_slot[j] = R[j].slot < 0 ? 0 : R[j].slot;
+        if (!R[j].plain) batched_all.push_back(j);
+    /* chunks of requests whose draw passes fit the memory budget: records, placement,
+     * sort and output columns take about kStarBytes per star of the largest model */
+    const double kStarBytes = 320.0;
+    int64_t budget = ctx->multi_budget;
+    if (budget <= 0) {
+        size_t fr = 0, tot = 0;
+        GF_CUDA(cudaMemGetInfo(&fr, &tot));
+        budget = (int64_t)(0.6 * (double)fr);
+    }
+    std::vector<std::vector<int>> chunks;
+    {
+        double used = 0;
+        for (int j : batched_all) {
+            double mx = 0;
+            for (int i = 0; i < nmod; i++) mx = std::max(mx, S[j].expected[i] + 8.0 * sqrt(S[j].expected[i]) + 1024.0);
+            const double need = mx * kStarBytes;
+            if (chunks.empty() || (used + need > (double)budget && !chunks.back().empty())) {
+                chunks.emplace_back();
+                used = 0;
+            }
+            chunks.back().push_back(j);
+            used += need;
+        }
+    }
 
-    if (nslots > 0) {
-        GF_TRY(upload_items(batched, &nitems));
-        int32_t *d_job_slot = nullptr, *d_slot_job = nullptr, *d_slot_comp = nullptr;
-        int64_t *d_seg = nullptr, *d_row_begin = nullptr, *d_slot_rows = nullptr, *d_chunk_begin = nullptr, *d_catoff = nullptr;
-        uint64_t *d_pseed = nullptr;
-        gf_footprint *d_foot = nullptr;
-        GF_TRY(pool.alloc(&d_job_slot, (size_t)njobs));
-        GF_TRY(pool.alloc(&d_slot_job, (size_t)nslots));
-        GF_TRY(pool.alloc(&d_slot_comp, (size_t)nslots));
-        GF_TRY(pool.alloc(&d_seg, 3 * (size_t)nslots));
-        GF_TRY(pool.alloc(&d_row_begin, (size_t)nslots + 1));
-        GF_TRY(pool.alloc(&d_slot_rows, (size_t)nslots));
-        GF_TRY(pool.alloc(&d_chunk_begin, (size_t)nslots));
-        GF_TRY(pool.alloc(&d_catoff, (size_t)njobs));
-        GF_TRY(pool.alloc(&d_pseed, (size_t)njobs));
-        GF_TRY(pool.alloc(&d_foot, (size_t)njobs));
-        GF_CUDA(cudaMemcpyAsync(d_job_slot, job_slot.data(), 4 * (size_t)njobs, cudaMemcpyHostToDevice, st));
-        GF_CUDA(cudaMemcpyAsync(d_slot_job, slot_job.data(), 4 * (size_t)nslots, cudaMemcpyHostToDevice, st));
-        bool any_foot = false;
+    std::vector<int32_t> job_slot(njobs, 0);
+    int32_t *d_job_slot = nullptr, *d_slot_job = nullptr, *d_slot_comp = nullptr;
+    int64_t *d_seg = nullptr, *d_row_begin = nullptr, *d_slot_rows = nullptr, *d_chunk_begin = nullptr, *d_catoff = nullptr;
+    uint64_t *d_pseed = nullptr;
+    gf_footprint *d_foot = nullptr;
+    GF_TRY(ws.job_slot.need((size_t)njobs));
+    d_job_slot = ws.job_slot.p;
+    GF_TRY(ws.slot_job.need((size_t)njobs));
+    d_slot_job = ws.slot_job.p;
+    GF_TRY(ws.slot_comp.need((size_t)njobs));
+    d_slot_comp = ws.slot_comp.p;
+    GF_TRY(ws.seg.need(3 * (size_t)njobs));
+    d_seg = ws.seg.p;
+    GF_TRY(ws.row_begin.need((size_t)njobs + 1));
+    d_row_begin = ws.row_begin.p;
+    GF_TRY(ws.slot_rows.need((size_t)njobs));
+    d_slot_rows = ws.slot_rows.p;
+    GF_TRY(ws.chunk_begin.need((size_t)njobs));
+    d_chunk_begin = ws.chunk_begin.p;
+    GF_TRY(ws.catoff.need((size_t)njobs));
+    d_catoff = ws.catoff.p;
+    GF_TRY(ws.pseed.need((size_t)njobs));
+    d_pseed = ws.pseed.p;
+    GF_TRY(ws.foot.need((size_t)njobs));
+    d_foot = ws.foot.p;
+    bool any_foot = false;
+    {
         std::vector<gf_footprint> foot(njobs);
         std::vector<uint64_t> pseed(njobs, 0);
         for (int j = 0; j < njobs; j++) {
@@ -422,31 +509,42 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
         }
         GF_CUDA(cudaMemcpyAsync(d_foot, foot.data(), sizeof(gf_footprint) * (size_t)njobs, cudaMemcpyHostToDevice, st));
         GF_CUDA(cudaMemcpyAsync(d_pseed, pseed.data(), 8 * (size_t)njobs, cudaMemcpyHostToDevice, st));
-        /* photometry and photometric-error tables of each module group */
-        struct GroupMods { gf_photometry *ph = nullptr; gf_photoerr *pe = nullptr; };
-        std::vector<GroupMods> gm(groups.size());
-        struct ModGuard {
-            std::vector<GroupMods> *g;
-            ~ModGuard() { for (auto &x : *g) { gf_photometry_destroy(x.ph); gf_photoerr_destroy(x.pe); } }
-        } mod_guard{&gm};
+        GF_CUDA(cudaStreamSynchronize(st));
+    }
+    /* photometry and photometric-error tables of each module group */
+    struct GroupMods { gf_photometry *ph = nullptr; gf_photoerr *pe = nullptr; };
+    std::vector<GroupMods> gm(groups.size());
+    struct ModGuard {
+        std::vector<GroupMods> *g;
+        ~ModGuard() { for (auto &x : *g) { gf_photometry_destroy(x.ph); gf_photoerr_destroy(x.pe); } }
+    } mod_guard{&gm};
+    if (!batched_all.empty())
         for (int g = 0; g < (int)group_rep.size(); g++) {
             const gf_job &J = jobs[group_rep[g]];
             if (J.phot) GF_TRY(gf_photometry_create(ctx, J.phot, &gm[g].ph));
             if (J.perr) GF_TRY(gf_photoerr_create(ctx, J.perr, &gm[g].pe));
         }
 
-        /* growing buffers of the draw passes */
-        Grow<StarRecord> rec;
-        Grow<double> lb;
-        Grow<int32_t> projIdx, hidden, row_slot;
-        Grow<float> projXY, DMc, absmag, XYZ, Am, AmInf;
-        Grow<uint64_t> key, key_b;
-        Grow<uint32_t> idx_a, idx_b, slot_a, slot_b;
-        Grow<char> temp;
-        gf_table out;
-        memset(&out, 0, sizeof(out));
-        struct TableGuard { gf_ctx *c; gf_table *t; ~TableGuard() { gf_table_free(c, t); } } tg{ctx, &out};
-        std::vector<int64_t> catoff(njobs, 0);
+    /* growing buffers of the draw passes */
+    auto &rec = ws.rec;
+    auto &lb = ws.lb;
+    auto &projIdx = ws.projIdx, &hidden = ws.hidden, &row_slot = ws.row_slot;
+    auto &projXY = ws.projXY, &DMc = ws.DMc, &absmag = ws.absmag, &XYZ = ws.XYZ, &Am = ws.Am, &AmInf = ws.AmInf;
+    auto &key = ws.key, &key_b = ws.key_b;
+    auto &idx_a = ws.idx_a, &idx_b = ws.idx_b, &slot_a = ws.slot_a, &slot_b = ws.slot_b;
+    auto &temp = ws.temp;
+    gf_table &out = ws.out;
+    std::vector<int64_t> catoff(njobs, 0);
+
+    for (const std::vector<int> &batched : chunks) {
+        /* output order of the chunk: by module group, then request */
+        std::vector<int> slot_job = batched;
+        std::stable_sort(slot_job.begin(), slot_job.end(), [&](int a, int b) { return R[a].group != R[b].group ? R[a].group < R[b].group : a < b; });
+        const int nslots = (int)slot_job.size();
+        for (int sl = 0; sl < nslots; sl++) job_slot[slot_job[sl]] = sl;
+        GF_CUDA(cudaMemcpyAsync(d_job_slot, job_slot.data(), 4 * (size_t)njobs, cudaMemcpyHostToDevice, st));
+        GF_CUDA(cudaMemcpyAsync(d_slot_job, slot_job.data(), 4 * (size_t)nslots, cudaMemcpyHostToDevice, st));
+        GF_TRY(upload_items(batched, &nitems));
         int slot_bits = 1;
         while ((1 << slot_bits) < nslots) slot_bits++;
 
@@ -527,7 +625,7 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
                 slot_comp[s] = R[j].hm[i].m.comp;
             }
             const int64_t total = row_begin[nslots];
-            if (out.capacity < std::max<int64_t>(total, 1)) {
+            if (out.capacity < std::max<int64_t>(total, 1) || out.nbands < nbands) {
                 gf_table_free(ctx, &out);
                 GF_TRY(gf_table_alloc(ctx, std::max<int64_t>(total + total / 8, 1024), nbands, &out));
             }
@@ -591,5 +689,13 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
         f.count.assign(njobs, 0);
         GF_TRY(gf_catalog_run(ctx, &jobs[j], forward_plain_batch, &f, &S[j]));
     }
+    return GF_OK;
+}
+
+extern "C" gf_status gf_multi_set_memory_budget(gf_ctx *ctx, int64_t bytes)
+{
+    GF_TRY(gfa::check_ctx(ctx));
+    if (bytes < 0) return fail(GF_E_INVALID, "negative memory budget");
+    ctx->multi_budget = bytes;
     return GF_OK;
 }

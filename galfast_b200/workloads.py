@@ -210,6 +210,41 @@ def _model(kind, comp, f, Rg, z0, lfM, lfphi, **kw):
     return m
 
 
+_TABLES = {}
+
+
+def _module_tables(lib, nbands, m5):
+    """Photometry and photometric-error tables of one photometric system, built once
+    per process and shared by every request that uses the system."""
+    key = (nbands, m5)
+    if key in _TABLES:
+        return _TABLES[key]
+    coef = color_coefficients(nbands)
+    rows = photosys_rows(coef)
+    nFeH = C.c_int32(0)
+    nMr = C.c_int32(0)
+    tcF = (C.c_float * 2)()
+    tcM = (C.c_float * 2)()
+    st = lib.gf_photometry_build(rows.ctypes.data_as(C.POINTER(C.c_double)), rows.shape[0], nbands - 1,
+                                 C.c_double(0.01), C.c_double(0.01), None, None, C.byref(nFeH), C.byref(nMr), tcF, tcM)
+    if st != 0:
+        raise RuntimeError("photometry build failed")
+    ncol = nbands - 1
+    colors = np.zeros(ncol * nMr.value * nFeH.value, dtype=np.float32)
+    eflags = np.zeros(ncol * nMr.value * nFeH.value, dtype=np.uint8)
+    lib.gf_photometry_build(rows.ctypes.data_as(C.POINTER(C.c_double)), rows.shape[0], ncol,
+                            C.c_double(0.01), C.c_double(0.01), colors.ctypes.data_as(C.POINTER(C.c_float)),
+                            eflags.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(nFeH), C.byref(nMr), tcF, tcM)
+    red = np.ones(A.GF_MAX_BANDS, dtype=np.float32)
+    AE = SDSS_AE if nbands <= 5 else LSST_AE
+    red[:nbands] = (AE[:nbands] / AE[2]).astype(np.float32)
+    mk, sg = error_knots(list(m5))
+    t = dict(rows=rows, colors=colors, eflags=eflags, nFeH=nFeH.value, nMr=nMr.value, tcF=(tcF[0], tcF[1]),
+             tcM=(tcM[0], tcM[1]), red=red, mk=mk, sg=sg)
+    _TABLES[key] = t
+    return t
+
+
 def build_workload(lib, *, foot, dx_deg, m0, m1, nthreads=7680, seed48=42, capacity=1 << 20,
                    thin_h=300.0, halo_q=0.64, with_modules=True, nbands=5, m5=SDSS_M5,
                    perr_seed=0x5eed, M0=3.0, M1=15.0, ext_E=0.02):
@@ -242,38 +277,20 @@ def build_workload(lib, *, foot, dx_deg, m0, m1, nthreads=7680, seed48=42, capac
     feh.comp_mask = 0xFFFFFFFF
     w.feh = feh
     w.kin = bond2010_config(Rg=Rg, z0=z0)
-    coef = color_coefficients(nbands)
-    rows = photosys_rows(coef)
-    nFeH = C.c_int32(0)
-    nMr = C.c_int32(0)
-    tcF = (C.c_float * 2)()
-    tcM = (C.c_float * 2)()
-    st = lib.gf_photometry_build(rows.ctypes.data_as(C.POINTER(C.c_double)), rows.shape[0], nbands - 1,
-                                 C.c_double(0.01), C.c_double(0.01), None, None, C.byref(nFeH), C.byref(nMr), tcF, tcM)
-    if st != 0:
-        raise RuntimeError("photometry build failed")
-    ncol = nbands - 1
-    colors = np.zeros(ncol * nMr.value * nFeH.value, dtype=np.float32)
-    eflags = np.zeros(ncol * nMr.value * nFeH.value, dtype=np.uint8)
-    lib.gf_photometry_build(rows.ctypes.data_as(C.POINTER(C.c_double)), rows.shape[0], ncol,
-                            C.c_double(0.01), C.c_double(0.01), colors.ctypes.data_as(C.POINTER(C.c_float)),
-                            eflags.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(nFeH), C.byref(nMr), tcF, tcM)
+    tabs = _module_tables(lib, nbands, tuple(float(x) for x in list(m5)[:nbands]))
     ph = A.PhotometryConfig()
     ph.nbands = nbands
     ph.bidx = 2
-    red = np.ones(A.GF_MAX_BANDS, dtype=np.float32)
-    AE = SDSS_AE if nbands <= 5 else LSST_AE
-    red[:nbands] = (AE[:nbands] / AE[2]).astype(np.float32)
     for i in range(A.GF_MAX_BANDS):
-        ph.reddening[i] = float(red[i])
-    ph.nFeH, ph.nMr = nFeH.value, nMr.value
-    ph.tcFeH[0], ph.tcFeH[1] = tcF[0], tcF[1]
-    ph.tcMr[0], ph.tcMr[1] = tcM[0], tcM[1]
-    ph.colors = colors.ctypes.data_as(C.POINTER(C.c_float))
-    ph.eflags = eflags.ctypes.data_as(C.POINTER(C.c_uint8))
+        ph.reddening[i] = float(tabs["red"][i])
+    ph.nFeH, ph.nMr = tabs["nFeH"], tabs["nMr"]
+    ph.tcFeH[0], ph.tcFeH[1] = tabs["tcF"][0], tabs["tcF"][1]
+    ph.tcMr[0], ph.tcMr[1] = tabs["tcM"][0], tabs["tcM"][1]
+    ph.colors = tabs["colors"].ctypes.data_as(C.POINTER(C.c_float))
+    ph.eflags = tabs["eflags"].ctypes.data_as(C.POINTER(C.c_uint8))
     ph.comp_mask = 0xFFFFFFFF
     w.phot = ph
-    mk, sg = error_knots(list(m5)[:nbands])
+    mk, sg = tabs["mk"], tabs["sg"]
     pe = A.PhotoerrConfig()
     pe.nbands = nbands
     pe.nknots = mk.shape[1]
@@ -286,7 +303,7 @@ def build_workload(lib, *, foot, dx_deg, m0, m1, nthreads=7680, seed48=42, capac
     v.vLSR, v.u0, v.v0, v.w0, v.Rg = -220.0, -10.0, -5.3, 7.2, Rg
     w.v2pm = v
     w.gal2other = 1
-    w.keep += [rows, colors, eflags, mk, sg]
+    w.keep += [tabs]
     return w
 
 
@@ -341,11 +358,23 @@ def config4_requests(n=4096, seed=1234567):
         rmax = g.uniform(19, 24)
         h = g.uniform(250, 350)
         q = g.uniform(0.55, 0.75)
-        out.append(dict(l=l, b=b, r=rad, rmax=rmax, h=h, q=q, seed48=s & 0xFFFFFFFF))
+        out.append(dict(l=l, b=b, r=rad, rmax=rmax, h=h, q=q, seed48=s & 0xFFFFFFFF, perr_seed=splitmix64(s)))
     return out
 
 
 def config4_workload(lib, req, **kw):
     foot = cap_footprint(req["l"], req["b"], req["r"])
+    kw.setdefault("perr_seed", req.get("perr_seed", 0x5eed))
     return build_workload(lib, foot=foot, dx_deg=0.1, m0=14.0, m1=req["rmax"], thin_h=req["h"],
                           halo_q=req["q"], seed48=req["seed48"], **kw)
+
+
+def config4_workloads(lib, reqs, threads=None, **kw):
+    """config4_workload for many requests on a thread pool (the pixelisation is
+    native code and runs without the interpreter lock)."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    _module_tables(lib, kw.get("nbands", 5), tuple(float(x) for x in list(kw.get("m5", SDSS_M5))[:kw.get("nbands", 5)]))
+    n = threads or min(32, os.cpu_count() or 1)
+    with ThreadPoolExecutor(max_workers=n) as ex:
+        return list(ex.map(lambda r: config4_workload(lib, r, **kw), reqs))

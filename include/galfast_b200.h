@@ -313,6 +313,9 @@ gf_status gf_table_alloc(gf_ctx *ctx, int64_t capacity, int32_t nbands, gf_table
 gf_status gf_table_free(gf_ctx *ctx, gf_table *t);
 /* Copy rows [0, t->size) of every allocated column to a host table with the same capacity layout. */
 gf_status gf_table_download(gf_ctx *ctx, const gf_table *dev, gf_table *host);
+/* rows [begin, end) of a device table into rows [0, end - begin) of a host table
+ * (one request's rows of a gf_catalog_run_multi table, for instance) */
+gf_status gf_table_download_rows(gf_ctx *ctx, const gf_table *dev, int64_t begin, int64_t end, gf_table *host);
 
 /* ---- modules: process rows [begin, end) of a device table ---- */
 gf_status gf_module_clipper(gf_ctx *ctx, const gf_footprint *foot, const gf_lambert proj[2],
@@ -395,6 +398,13 @@ typedef int (*gf_multi_callback)(void *user, int32_t model, const gf_table *dev_
  * which generates one catalog per process (os_skygen.cpp:866-932). */
 gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, void *user,
                                gf_catalog_stats *stats);
+
+/* Device memory that one chunk of a multi-request run may use for its draw
+ * passes (records, placement, sort and output columns, about 320 bytes per
+ * expected star of a request's largest model).  Requests are generated in
+ * consecutive chunks that fit; the callback then sees each chunk's rows.
+ * 0 (the default) = 60% of the free device memory at the start of the run. */
+gf_status gf_multi_set_memory_budget(gf_ctx *ctx, int64_t bytes);
 
 /* ---- expected counts without device allocation ---- */
 

@@ -80,19 +80,22 @@ def test_multi_request_rows_equal_standalone(lib):
     ctx.close()
 
 
-def test_multi_request_is_repeatable(lib):
+def test_multi_request_is_repeatable_and_chunking_is_transparent(lib):
+    """A second run gives the same rows; so does a run whose memory budget puts every
+    request in a chunk of its own."""
     ws = requests(lib, n=4)
     ctx = G.Context(0)
     runs = []
-    for _ in range(2):
+    for budget in (0, 0, 1):
+        ctx.set_multi_budget(budget)
         got = {}
 
         def sink(j, model, rows):
             got.setdefault((j, model), []).append(rows["lb"].copy())
         G.run_catalog_multi(ctx, ws, sink=sink)
         runs.append(got)
-    assert runs[0].keys() == runs[1].keys()
-    for k in runs[0]:
-        for x, y in zip(runs[0][k], runs[1][k]):
-            np.testing.assert_array_equal(x, y)
+    for other in runs[1:]:
+        assert runs[0].keys() == other.keys()
+        for k in runs[0]:
+            np.testing.assert_array_equal(np.concatenate(runs[0][k], axis=-1), np.concatenate(other[k], axis=-1))
     ctx.close()
