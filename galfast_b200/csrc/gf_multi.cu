@@ -74,34 +74,42 @@ struct Grow {
     ~Grow() { dev_free(p); }
 };
 
-/* content signature of the photometry and error tables of a request (the error
- * seed is per request and not part of it) */
+/* a page-locked host buffer that only grows */
+template <typename T>
+struct HostGrow {
+    T *p = nullptr;
+    size_t n = 0;
+    gf_status need(size_t m)
+    {
+        if (m <= n) return GF_OK;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        GF_CUDA(cudaMallocHost((void **)&p, m * sizeof(T)));
+        n = m;
+        return GF_OK;
+    }
+    ~HostGrow()
+    {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+/* module-group key of a request (the error seed is per request and not part of it) */
 std::string module_signature(const gf_job &J)
 {
+    /* the configuration bytes, table pointers included: requests built from one
+     * photometric system share its tables and land in one group */
     std::string sig;
-    auto add = [&](const void *p, size_t n) { sig.append((const char *)p, n); };
     if (J.phot) {
-        gf_photometry_config c = *J.phot;
-        const size_t n = (size_t)(c.nbands > 1 ? c.nbands - 1 : 0) * (size_t)c.nMr * (size_t)c.nFeH;
-        const float *colors = c.colors;
-        const uint8_t *eflags = c.eflags;
-        c.colors = nullptr;
-        c.eflags = nullptr;
         sig += "P";
-        add(&c, sizeof(c));
-        if (colors) add(colors, 4 * n);
-        if (eflags) add(eflags, n);
+        sig.append((const char *)J.phot, sizeof(gf_photometry_config));
     }
     if (J.perr) {
         gf_photoerr_config c = *J.perr;
-        const size_t n = (size_t)c.nbands * (size_t)c.nknots;
-        const double *mag = c.mag, *sigma = c.sigma;
-        c.mag = c.sigma = nullptr;
         c.seed = 0;
         sig += "E";
-        add(&c, sizeof(c));
-        if (mag) add(mag, 8 * n);
-        if (sigma) add(sigma, 8 * n);
+        sig.append((const char *)&c, sizeof(c));
     }
     return sig;
 }
@@ -166,6 +174,7 @@ struct MultiWS {
     Grow<uint32_t> idx_a, idx_b, slot_a, slot_b;
     Grow<char> temp;
     gf_table out;
+    HostGrow<char> h_stage;              /* page-locked staging of uploads and downloads */
     MultiWS() { memset(&out, 0, sizeof(out)); }
 };
 
@@ -285,17 +294,24 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
     GF_TRY(ws.lf.need((size_t)njobs * nmod * 1024));
     d_lf = ws.lf.p;
     {
-        std::vector<float> lf((size_t)njobs * nmod * 1024, 0.f);
+        /* one page-locked staging area: all pixels, then the per-beam extinction, then the LFs */
+        const size_t pb = sizeof(gf_pencil_beam) * (size_t)pix_total, ab = 4 * (size_t)pix_total;
+        const size_t lb_ = 4 * (size_t)njobs * nmod * 1024;
+        GF_TRY(ws.h_stage.need(pb + ab + lb_));
+        char *h = ws.h_stage.p;
+        gf_pencil_beam *hp = (gf_pencil_beam *)h;
+        float *ha = (float *)(h + pb), *hl = (float *)(h + pb + ab);
+        memset(hl, 0, lb_);
         for (int j = 0; j < njobs; j++) {
-            GF_CUDA(cudaMemcpyAsync(d_pix + R[j].pix_off, jobs[j].pixels, sizeof(gf_pencil_beam) * (size_t)jobs[j].npixels,
-                                    cudaMemcpyHostToDevice, st));
-            if (jobs[j].beam_ammin)
-                GF_CUDA(cudaMemcpyAsync(d_ammin + R[j].pix_off, jobs[j].beam_ammin, 4 * (size_t)jobs[j].npixels,
-                                        cudaMemcpyHostToDevice, st));
+            memcpy(hp + R[j].pix_off, jobs[j].pixels, sizeof(gf_pencil_beam) * (size_t)jobs[j].npixels);
+            if (jobs[j].beam_ammin) memcpy(ha + R[j].pix_off, jobs[j].beam_ammin, 4 * (size_t)jobs[j].npixels);
+            else memset(ha + R[j].pix_off, 0, 4 * (size_t)jobs[j].npixels);
             for (int i = 0; i < nmod; i++)
-                std::copy(R[j].hm[i].lf.begin(), R[j].hm[i].lf.end(), lf.begin() + ((size_t)j * nmod + i) * 1024);
+                std::copy(R[j].hm[i].lf.begin(), R[j].hm[i].lf.end(), hl + ((size_t)j * nmod + i) * 1024);
         }
-        GF_CUDA(cudaMemcpyAsync(d_lf, lf.data(), 4 * lf.size(), cudaMemcpyHostToDevice, st));
+        GF_CUDA(cudaMemcpyAsync(d_pix, hp, pb, cudaMemcpyHostToDevice, st));
+        GF_CUDA(cudaMemcpyAsync(d_ammin, ha, ab, cudaMemcpyHostToDevice, st));
+        GF_CUDA(cudaMemcpyAsync(d_lf, hl, lb_, cudaMemcpyHostToDevice, st));
         GF_CUDA(cudaStreamSynchronize(st));
     }
     /* distance tables D[im][iM], shared by the requests with the same magnitude grid */
@@ -389,13 +405,15 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
     };
     /* work items: requests in decreasing size, all streams of each */
     auto upload_items = [&](const std::vector<int> &order, int32_t *nitems) -> gf_status {
-        std::vector<uint32_t> items;
-        items.reserve(order.size() * N);
+        const size_t cnt = order.size() * (size_t)N;
+        GF_TRY(ws.h_stage.need(4 * cnt));
+        uint32_t *items = (uint32_t *)ws.h_stage.p;
+        size_t k = 0;
         for (int j : order)
-            for (int t = 0; t < N; t++) items.push_back(((uint32_t)j << 16) | (uint32_t)t);
-        GF_CUDA(cudaMemcpyAsync(d_items, items.data(), 4 * items.size(), cudaMemcpyHostToDevice, st));
+            for (int t = 0; t < N; t++) items[k++] = ((uint32_t)j << 16) | (uint32_t)t;
+        GF_CUDA(cudaMemcpyAsync(d_items, items, 4 * cnt, cudaMemcpyHostToDevice, st));
         GF_CUDA(cudaStreamSynchronize(st));
-        *nitems = (int32_t)items.size();
+        *nitems = (int32_t)cnt;
         return GF_OK;
     };
     std::vector<int> order_all(njobs);
@@ -429,8 +447,10 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
             ProfScope ps(ctx, GF_PROF_INTEGRATE);
             GF_CUDA(gfk::launch_crawl_multi(L, 0, st));
         }
-        GF_CUDA(cudaMemcpyAsync(hc.data(), d_counts, 16 * nall, cudaMemcpyDeviceToHost, st));
+        GF_TRY(ws.h_stage.need(16 * nall));
+        GF_CUDA(cudaMemcpyAsync(ws.h_stage.p, d_counts, 16 * nall, cudaMemcpyDeviceToHost, st));
         GF_CUDA(cudaStreamSynchronize(st));
+        memcpy(hc.data(), ws.h_stage.p, 16 * nall);
         for (int j : integ) {
             double e = 0, ec = 0;
             for (int t = 0; t < N; t++) {
