@@ -122,7 +122,7 @@ C4_PLAIN_STRIDE = 16           # the plain path is timed on every 16th request
 
 
 def config4_set(G, W, rank=0, nreq=C4_NREQ):
-    reqs = W.config4_requests(nreq, seed=1234567 + nreq * rank)
+    reqs = W.config4_requests(nreq, seed=1234567 + C4_NREQ * rank)
     ws = W.config4_workloads(G.lib(), reqs, capacity=C4_CAPACITY)
     desc = ("config4: %d pencil beams, centres uniform at |b|>5 deg, radius log-uniform 0.5-5 deg, 0.1 deg pixels, "
             "14<r<U(19,24), thin-disk h U(250,350), halo q U(0.55,0.75), own seed each, ugriz, full module chain" % nreq)
@@ -215,6 +215,7 @@ def main():
     ap.add_argument("--config", default="config4", choices=["config4", "config2", "config1"])
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--requests", type=int, default=C4_NREQ, help="config4: requests per step (a prefix of the set)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -320,7 +321,7 @@ def draw_rooflines(pk, pk_kind, bins, diags, stars_step, npix_models, draw_ms, d
 def bench_multi(args, G, W, ctx, rank, world, dist):
     """config 4: every request through gf_catalog_run_multi, the plain path on a sample."""
     L = G.lib()
-    ws, desc = config4_set(G, W, rank)
+    ws, desc = config4_set(G, W, rank, nreq=args.requests)
     n = len(ws)
     jobs = (G.Job * n)(*[w.job(G.Job) for w in ws])
     stats = (G.CatalogStats * n)()
