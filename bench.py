@@ -212,7 +212,9 @@ def main():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="config4", choices=["config4", "config2", "config1"])
+    ap.add_argument("--config", default="config4", choices=["config4", "config5", "config2", "config1"])
+    ap.add_argument("--rates", default="10,30,100,300,1000", help="config5: arrival rates (requests/s)")
+    ap.add_argument("--serve-requests", type=int, default=32, help="config5: requests per rate")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--requests", type=int, default=C4_NREQ, help="config4: requests per step (a prefix of the set)")
@@ -268,6 +270,8 @@ def main():
     ctx = G.Context(device)
     if args.config == "config4":
         bench_multi(args, G, W, ctx, rank, world, dist)
+    elif args.config == "config5":
+        bench_serve(args, G, W, ctx, rank, world, dist)
     else:
         bench_single(args, G, W, ctx, rank, world, dist)
     if dist is not None:
@@ -445,6 +449,58 @@ def bench_multi(args, G, W, ctx, rank, world, dist):
                 "e2e": e2e, "roofline": roofline, "compute_roofline": compute, "cpu_baseline": cpu,
                 "gpu_launches": int(launches), "clocks": clock.summary(),
                 "phases_ms_per_step": {k: v[0] / args.steps for k, v in prof.items()}}
+        print(json.dumps(line))
+
+
+def bench_serve(args, G, W, ctx, rank, world, dist):
+    """config 5: a Poisson request stream through gf_server (continuous batching) at each rate."""
+    L = G.lib()
+    rates = [float(x) for x in args.rates.split(",")]
+    n = args.serve_requests
+    # one request set: the same footprints at every rate, arrival times scaled by the rate
+    base = W.config5_requests(n, 1.0, seed=99 + rank)
+    ws = W.config5_workloads(L, base)
+    # warm-up: the first requests through a server, untimed
+    srv = G.Server(0, workers=2, memory_budget=150 * 2 ** 30, max_batch=512)
+    for w in ws[: min(4, n)]:
+        srv.submit(w)
+    srv.drain()
+    srv.close()
+    results = []
+    n0 = L.gf_launch_count()
+    clock = clock_sampler(rank)
+    with clock:
+        for rate in rates:
+            srv = G.Server(0, workers=2, memory_budget=150 * 2 ** 30, max_batch=512)
+            t0 = time.perf_counter()
+            for r, w in zip(base, ws):
+                t_arr = r["t"] / rate
+                while time.perf_counter() - t0 < t_arr:
+                    time.sleep(0.0005)
+                srv.submit(w)
+            srv.drain()
+            lat = np.array([srv.finished[i] - srv.submitted[i] for i in srv.submitted])
+            rows = sum(st.stored[i] for st in srv.stats.values() for i in range(len(ws[0].models)))
+            span = max(srv.finished.values()) - min(srv.submitted.values())
+            bad = [i for i, s_ in srv.status.items() if s_ != 0]
+            srv.close()
+            results.append({"rate_per_s": rate, "requests": n, "failed": len(bad), "rows": int(rows),
+                            "stars_per_s": rows / span, "latency_p50_s": float(np.percentile(lat, 50)),
+                            "latency_p99_s": float(np.percentile(lat, 99)), "makespan_s": span})
+    launches = L.gf_launch_count() - n0
+    total_rows = sum(r["rows"] for r in results)
+    total_span = sum(r["makespan_s"] for r in results)
+    if rank == 0:
+        line = {"metric": METRIC, "value": total_rows / total_span, "unit": "stars/s", "n_gpus": world,
+                "steps": len(rates), "warmup": 1, "ms_per_step": 1e3 * total_span / len(rates), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "config5: Poisson arrivals, caps and lon/lat rectangles of log-uniform 1-1000 deg^2 at |b|>10 deg, "
+                                       "0.1 deg pixels, 14<r<U(20,25), half ugriz / half ugrizy (m5 one mag deeper), own seeds; "
+                                       "gf_server with 2 workers, 150 GiB budget",
+                           "requests_per_rate": n, "pixels": int(sum(w.npixels for w in ws)),
+                           "latency": "submit to completion, host wall clock", "l2": "inputs and catalogs larger than L2"},
+                "serving": results, "gpu_launches": int(launches), "clocks": clock.summary(),
+                "e2e": None, "roofline": None, "cpu_baseline": None}
         print(json.dumps(line))
 
 

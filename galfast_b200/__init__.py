@@ -42,6 +42,8 @@ class CatalogStats(C.Structure):
 
 
 BatchCallback = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.POINTER(Table), C.c_int64)
+ServerRows = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.POINTER(Table), C.c_int64, C.c_int64)
+ServerDone = C.CFUNCTYPE(None, C.c_void_p, C.c_int64, C.c_int32, C.POINTER(CatalogStats))
 MultiCallback = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.POINTER(Table), C.POINTER(C.c_int64), C.POINTER(C.c_int64))
 
 _lib = None
@@ -97,6 +99,10 @@ def lib():
         L.gf_catalog_run_multi.argtypes = [vp, C.POINTER(Job), C.c_int32, MultiCallback, vp, C.POINTER(CatalogStats)]
         L.gf_multi_set_memory_budget.argtypes = [vp, C.c_int64]
         L.gf_table_download_rows.argtypes = [vp, C.POINTER(Table), C.c_int64, C.c_int64, C.POINTER(Table)]
+        L.gf_server_create.argtypes = [C.c_int32, C.c_int32, C.c_int64, C.c_int32, C.POINTER(vp)]
+        L.gf_server_submit.argtypes = [vp, C.POINTER(Job), ServerRows, ServerDone, vp, C.POINTER(C.c_int64)]
+        L.gf_server_drain.argtypes = [vp]
+        L.gf_server_destroy.argtypes = [vp]
         L.gf_lambert_init.argtypes = [C.c_double, C.c_double, C.POINTER(Lambert)]
         L.gf_footprint_pixelize.argtypes = [C.POINTER(Footprint), C.c_double, C.POINTER(Lambert),
                                             C.POINTER(Extinction), C.POINTER(PencilBeam), C.POINTER(C.c_float),
@@ -367,3 +373,70 @@ def run_catalog_multi(ctx, workloads, sink=None, device_sink=None):
     ccb = MultiCallback(cb)
     check(lib().gf_catalog_run_multi(ctx.h, jobs, n, ccb, None, stats))
     return list(stats)
+
+
+class Server:
+    """gf_server: continuous batching of catalog requests on one device.
+
+    submit(w) queues a workload; keep_rows=True keeps each request's rows in host
+    memory (a dict per model of column arrays).  Completion wall-clock times are
+    recorded for latency.  Callbacks run on the server's worker threads."""
+
+    def __init__(self, device=0, workers=2, memory_budget=150 * 2 ** 30, max_batch=512, keep_rows=False):
+        import threading
+        import time as _time
+        self._time = _time
+        self.h = C.c_void_p()
+        check(lib().gf_server_create(device, workers, int(memory_budget), max_batch, C.byref(self.h)))
+        self.keep_rows = keep_rows
+        self.lock = threading.Lock()
+        self.jobs = {}
+        self.submitted, self.finished, self.status, self.stats, self.rows = {}, {}, {}, {}, {}
+        self._stage = {}
+
+        def on_rows(user, rid, model, wctx, tptr, begin, count):
+            if not self.keep_rows:
+                return 0
+            t = tptr.contents
+            h = HostTable(max(int(count), 1), t.nbands)
+            if lib().gf_table_download_rows(wctx, tptr, begin, begin + count, C.byref(h.t)) != 0:
+                return 1
+            with self.lock:
+                self.rows.setdefault(rid, {}).setdefault(model, []).append(h.rows(0, int(count)))
+            return 0
+
+        def on_done(user, rid, status, stats):
+            t = self._time.perf_counter()
+            st = CatalogStats()
+            C.memmove(C.byref(st), stats, C.sizeof(CatalogStats))
+            with self.lock:
+                self.finished[rid] = t
+                self.status[rid] = status
+                self.stats[rid] = st
+
+        self._rows_cb = ServerRows(on_rows)
+        self._done_cb = ServerDone(on_done)
+
+    def submit(self, w):
+        job = w.job(Job)
+        rid = C.c_int64()
+        t = self._time.perf_counter()
+        check(lib().gf_server_submit(self.h, C.byref(job), self._rows_cb, self._done_cb, None, C.byref(rid)))
+        with self.lock:
+            self.jobs[rid.value] = (job, w)
+            self.submitted[rid.value] = t
+        return rid.value
+
+    def drain(self):
+        check(lib().gf_server_drain(self.h))
+
+    def close(self):
+        if self.h:
+            lib().gf_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -21,7 +21,7 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIBNAME = "libgalfast_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-SOURCES = ["gf_skygen.cu", "gf_modules.cu", "gf_api.cu", "gf_static.cu", "gf_multi.cu", "gf_host.cpp", "gf_safeprimes.cpp"]
+SOURCES = ["gf_skygen.cu", "gf_modules.cu", "gf_api.cu", "gf_static.cu", "gf_multi.cu", "gf_server.cpp", "gf_host.cpp", "gf_safeprimes.cpp"]
 
 
 def nvcc_path():
@@ -37,7 +37,7 @@ def build(verbose=False, extra=None):
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     cmd = [nvcc_path(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
            "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
-           "-shared", "-o", out, *srcs, "-ldl"]
+           "-shared", "-o", out, *srcs, "-ldl", "-lpthread"]
     if extra:
         cmd[1:1] = list(extra)
     if verbose:

@@ -337,6 +337,15 @@ void deproject_d(const gf_lambert &p, double x, double y, double &l, double &b)
     l = p.l0 + gfm::atan2_d(x * sc, (double)p.cb * cc / ir - y * (double)p.sb * sc);
 }
 
+/* galactic longitude/latitude rectangle, degrees; l in any turn */
+static bool lb_rect_inside(const gf_footprint &f, double l, double b)
+{
+    if (!(b >= f.c && b < f.d)) return false;
+    l = fmod(l, 360.0);
+    if (l < 0) l += 360.0;
+    return (f.a <= f.b) ? (l >= f.a && l < f.b) : (l >= f.a || l < f.b);
+}
+
 struct FootTest {
     gf_footprint f;
     double cb0, sb0, l0, cosr;
@@ -355,6 +364,7 @@ struct FootTest {
         case GF_FOOT_LAMBERT_RECT: return proj == f.proj && x >= f.a && x < f.b && y >= f.c && y < f.d;
         case GF_FOOT_CAP: return gfm::sin_d(b) * sb0 + gfm::cos_d(b) * cb0 * gfm::cos_d(l - l0) >= cosr;
         case GF_FOOT_LATCUT: return fabs(b) > f.a * kD2R;
+        case GF_FOOT_LB_RECT: return lb_rect_inside(f, l / kD2R, b / kD2R);
         }
         return false;
     }
@@ -400,20 +410,13 @@ gf_status gf_footprint_pixelize(const gf_footprint *foot, double dx_deg, const g
         } else if (foot->kind == GF_FOOT_LATCUT) {
             double R = 2 * gfm::sin_d(0.5 * (90. - foot->a) * kD2R);
             xmin = ymin = -R; xmax = ymax = R;
-        } else if (foot->kind == GF_FOOT_CAP) {
-            /* project boundary samples of the cap that fall in this hemisphere */
+        } else if (foot->kind == GF_FOOT_CAP || foot->kind == GF_FOOT_LB_RECT) {
+            /* project boundary samples of the footprint that fall in this hemisphere */
             double bx0 = 1e9, bx1 = -1e9, by0 = 1e9, by1 = -1e9;
             bool any = false;
             const gf_lambert &p = proj[h];
-            double lc = foot->a * kD2R, bc = foot->b * kD2R, r = foot->c * kD2R;
-            for (int k = 0; k <= 4096; k++) {
-                double rr = (k == 4096) ? 0.0 : r;
-                double az = 2 * M_PI * k / 4096.0;
-                /* destination point at distance rr, azimuth az from (lc, bc) */
-                double sb = gfm::sin_d(bc) * gfm::cos_d(rr) + gfm::cos_d(bc) * gfm::sin_d(rr) * gfm::cos_d(az);
-                double b = gfm::asin_d(sb);
-                double l = lc + gfm::atan2_d(gfm::sin_d(az) * gfm::sin_d(rr) * gfm::cos_d(bc), gfm::cos_d(rr) - gfm::sin_d(bc) * sb);
-                if ((h == 0) != (b >= 0)) continue;
+            auto add_point = [&](double l, double b) {
+                if ((h == 0) != (b >= 0)) return;
                 /* forward Lambert projection about the pole */
                 double cll0 = gfm::cos_d(l - p.l0);
                 double sll0 = gfm::sin_d(l - p.l0);
@@ -422,15 +425,44 @@ gf_status gf_footprint_pixelize(const gf_footprint *foot, double dx_deg, const g
                 double y = kp * ((double)p.cb * gfm::sin_d(b) - (double)p.sb * gfm::cos_d(b) * cll0);
                 bx0 = std::min(bx0, x); bx1 = std::max(bx1, x); by0 = std::min(by0, y); by1 = std::max(by1, y);
                 any = true;
+            };
+            if (foot->kind == GF_FOOT_CAP) {
+                double lc = foot->a * kD2R, bc = foot->b * kD2R, r = foot->c * kD2R;
+                for (int k = 0; k <= 4096; k++) {
+                    double rr = (k == 4096) ? 0.0 : r;
+                    double az = 2 * M_PI * k / 4096.0;
+                    /* destination point at distance rr, azimuth az from (lc, bc) */
+                    double sb = gfm::sin_d(bc) * gfm::cos_d(rr) + gfm::cos_d(bc) * gfm::sin_d(rr) * gfm::cos_d(az);
+                    double b = gfm::asin_d(sb);
+                    double l = lc + gfm::atan2_d(gfm::sin_d(az) * gfm::sin_d(rr) * gfm::cos_d(bc), gfm::cos_d(rr) - gfm::sin_d(bc) * sb);
+                    add_point(l, b);
+                }
+            } else {
+                double l0 = foot->a, l1 = foot->b < foot->a ? foot->b + 360.0 : foot->b;
+                double b0 = std::max(foot->c, -90.0), b1 = std::min(foot->d, 90.0);
+                for (int k = 0; k <= 2048; k++) {
+                    double t = k / 2048.0;
+                    double l = (l0 + t * (l1 - l0)) * kD2R, b = (b0 + t * (b1 - b0)) * kD2R;
+                    add_point(l, b0 * kD2R);
+                    add_point(l, b1 * kD2R);
+                    add_point(l0 * kD2R, b);
+                    add_point(l1 * kD2R, b);
+                    add_point(0.5 * (l0 + l1) * kD2R, b);
+                }
             }
-            /* the cap may reach the equator: then its hemisphere part is bounded by the cap samples and the rim */
+            /* a footprint that reaches the equator is also bounded by the rim: its inside points at b = 0 */
+            for (int k = 0; k < 8192; k++) {
+                const double l = 2 * M_PI * k / 8192.0, b = (h == 0) ? 0.0 : -1e-12;
+                if (ft.inside(h, 0.0, 0.0, l, b)) add_point(l, b);
+            }
             if (!any) continue;
             double pad = 2 * dx;
             xmin = std::max(-M_SQRT2, bx0 - pad); xmax = std::min(M_SQRT2, bx1 + pad);
             ymin = std::max(-M_SQRT2, by0 - pad); ymax = std::min(M_SQRT2, by1 + pad);
-            /* a cap containing the pole covers the origin */
-            double dpole = (h == 0 ? 90. - foot->b : 90. + foot->b);
-            if (dpole <= foot->c) { xmin = std::min(xmin, -dx); xmax = std::max(xmax, dx); ymin = std::min(ymin, -dx); ymax = std::max(ymax, dx); }
+            /* a footprint containing the pole covers the origin */
+            bool pole = (foot->kind == GF_FOOT_CAP) ? ((h == 0 ? 90. - foot->b : 90. + foot->b) <= foot->c)
+                                                    : (h == 0 ? foot->d >= 90. : foot->c <= -90.);
+            if (pole) { xmin = std::min(xmin, -dx); xmax = std::max(xmax, dx); ymin = std::min(ymin, -dx); ymax = std::max(ymax, dx); }
         }
         long long i0 = (long long)floor(xmin / dx), i1 = (long long)ceil(xmax / dx);
         long long j0 = (long long)floor(ymin / dx), j1 = (long long)ceil(ymax / dx);

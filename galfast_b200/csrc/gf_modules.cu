@@ -45,6 +45,9 @@ __device__ __forceinline__ void clip_row(const gf_footprint &foot, gf_table &t, 
             in = cosd >= gfm::cos_d(foot.c * D2R);
         } else if (foot.kind == GF_FOOT_LATCUT) {
             in = fabs(t.lb[P + row]) > foot.a;
+        } else if (foot.kind == GF_FOOT_LB_RECT) {
+            const double l = t.lb[row], b = t.lb[P + row];
+            in = b >= foot.c && b < foot.d && ((foot.a <= foot.b) ? (l >= foot.a && l < foot.b) : (l >= foot.a || l < foot.b));
         }
         if (!in) t.hidden[row] = 1;
 }

@@ -7,6 +7,8 @@ error curves are generated from closed-form expressions with fixed seeds.
     config 1  10x10 deg patch at the north galactic pole, 0.25 deg pixels, 15 < r < 21
     config 2  whole sky with |b| > 10 deg, 0.1 deg pixels, 14 < r < 22, 16M-star batches
     config 4  4096 pencil beams (batched form), per-request model variants and seeds
+    config 5  served requests: Poisson arrivals, caps and lon/lat rectangles of 1-1000 deg^2,
+              14 < r < U(20, 25), SDSS-like or LSST-like photometry
 """
 import ctypes as C
 import math
@@ -378,3 +380,64 @@ def config4_workloads(lib, reqs, threads=None, **kw):
     n = threads or min(32, os.cpu_count() or 1)
     with ThreadPoolExecutor(max_workers=n) as ex:
         return list(ex.map(lambda r: config4_workload(lib, r, **kw), reqs))
+
+
+def lb_rect_footprint(l0, l1, b0, b1):
+    foot = A.Footprint()
+    foot.kind = A.GF_FOOT_LB_RECT
+    foot.a, foot.b, foot.c, foot.d = l0 % 360.0, l1 % 360.0, b0, b1
+    return foot
+
+
+def config5_requests(n, rate, seed=99, area=(1.0, 1000.0), rmax=(20.0, 25.0)):
+    """The served request stream: arrival times of a Poisson process of the given rate
+    (requests/s), footprint areas log-uniform in `area` deg^2, caps or galactic
+    lon/lat rectangles (half each) at random centres with |b| > 10 deg, depth r_max
+    uniform in `rmax`, half SDSS-like ugriz and half LSST-like ugrizy, own seeds."""
+    g = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(n):
+        t += g.exponential(1.0 / rate)
+        while True:
+            z = g.uniform(-1, 1)
+            b = math.degrees(math.asin(z))
+            if abs(b) > 10.0:
+                break
+        l = g.uniform(0, 360)
+        A_deg2 = math.exp(g.uniform(math.log(area[0]), math.log(area[1])))
+        a_sr = A_deg2 * D2R * D2R
+        if g.uniform() < 0.5:
+            shape = dict(kind="cap", r=math.degrees(math.acos(1.0 - a_sr / (2 * math.pi))))
+        else:
+            db = math.sqrt(A_deg2)
+            b0 = max(-90.0, b - 0.5 * db)
+            b1 = min(90.0, b + 0.5 * db)
+            dl = math.degrees(a_sr / (math.sin(math.radians(b1)) - math.sin(math.radians(b0))))
+            shape = dict(kind="rect", l0=l - 0.5 * min(dl, 359.0), l1=l + 0.5 * min(dl, 359.0), b0=b0, b1=b1)
+        s = splitmix64(seed * 1000003 + k)
+        out.append(dict(t=t, l=l, b=b, area=A_deg2, rmax=g.uniform(*rmax), lsst=bool(g.uniform() < 0.5),
+                        seed48=s & 0xFFFFFFFF, perr_seed=splitmix64(s), **shape))
+    return out
+
+
+def config5_workload(lib, req, capacity=1 << 24, **kw):
+    if req["kind"] == "cap":
+        foot = cap_footprint(req["l"], req["b"], req["r"])
+    else:
+        foot = lb_rect_footprint(req["l0"], req["l1"], req["b0"], req["b1"])
+    if req["lsst"]:
+        kw.setdefault("nbands", 6)
+        kw.setdefault("m5", LSST_M5)
+    return build_workload(lib, foot=foot, dx_deg=0.1, m0=14.0, m1=req["rmax"], seed48=req["seed48"],
+                          perr_seed=req["perr_seed"], capacity=capacity, **kw)
+
+
+def config5_workloads(lib, reqs, threads=None, **kw):
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    for nb, m5 in ((5, SDSS_M5), (6, LSST_M5)):
+        _module_tables(lib, nb, tuple(float(x) for x in m5))
+    n = threads or min(32, os.cpu_count() or 1)
+    with ThreadPoolExecutor(max_workers=n) as ex:
+        return list(ex.map(lambda r: config5_workload(lib, r, **kw), reqs))

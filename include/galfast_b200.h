@@ -131,13 +131,14 @@ typedef enum {
     GF_FOOT_ALL = 0,           /* no clipping */
     GF_FOOT_LAMBERT_RECT = 1,  /* x0 <= X < x1, y0 <= Y < y1 in projection proj */
     GF_FOOT_CAP = 2,           /* angular distance from (l, b) <= r (degrees) */
-    GF_FOOT_LATCUT = 3         /* |b| > bmin (degrees) */
+    GF_FOOT_LATCUT = 3,        /* |b| > bmin (degrees) */
+    GF_FOOT_LB_RECT = 4        /* l0 <= l < l1 (degrees, through 360 when l0 > l1), b0 <= b < b1 */
 } gf_footprint_kind;
 
 typedef struct gf_footprint {
     int32_t kind;
     int32_t proj;
-    double a, b, c, d;         /* RECT: x0 x1 y0 y1; CAP: l b r; LATCUT: bmin */
+    double a, b, c, d;         /* RECT: x0 x1 y0 y1; CAP: l b r; LATCUT: bmin; LB_RECT: l0 l1 b0 b1 */
 } gf_footprint;
 
 /* ------------------------------------------------------------------ */
@@ -405,6 +406,32 @@ gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, g
  * consecutive chunks that fit; the callback then sees each chunk's rows.
  * 0 (the default) = 60% of the free device memory at the start of the run. */
 gf_status gf_multi_set_memory_budget(gf_ctx *ctx, int64_t bytes);
+
+/* ---- serving: continuous batching of requests ---- */
+
+typedef struct gf_server gf_server;
+/* rows [begin, begin + count) of dev hold this request's rows of one model
+ * (called on a worker thread; ctx is that worker's context, for downloads such as
+ * gf_table_download_rows; a nonzero return fails the request's batch) */
+typedef int (*gf_server_rows)(void *user, int64_t request, int32_t model, gf_ctx *ctx, const gf_table *dev, int64_t begin,
+                              int64_t count);
+/* the request is complete (status GF_OK) or failed; stats are the request's own */
+typedef void (*gf_server_done)(void *user, int64_t request, gf_status status, const gf_catalog_stats *stats);
+
+/* A request server on one device: nworkers worker threads, each with its own
+ * context and CUDA stream, take the compatible requests waiting at the head of
+ * the queue and generate them together (gf_catalog_run_multi) within their
+ * share of memory_budget bytes of device memory; requests that arrive while
+ * others run are taken by the next free worker, so batches overlap on the GPU.
+ * max_batch caps the requests of one batch.  No counterpart in the reference. */
+gf_status gf_server_create(int32_t device, int32_t nworkers, int64_t memory_budget, int32_t max_batch, gf_server **out);
+/* Queue one request; the job and everything it points to must stay valid until
+ * its done callback.  *request receives its id. */
+gf_status gf_server_submit(gf_server *s, const gf_job *job, gf_server_rows rows, gf_server_done done, void *user,
+                           int64_t *request);
+/* Wait until every submitted request is done; returns the first error seen. */
+gf_status gf_server_drain(gf_server *s);
+gf_status gf_server_destroy(gf_server *s);
 
 /* ---- expected counts without device allocation ---- */
 
