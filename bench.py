@@ -212,7 +212,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="config4", choices=["config4", "config5", "config2", "config1"])
+    ap.add_argument("--config", default="config4", choices=["config4", "config5", "config3", "config2", "config1"])
     ap.add_argument("--rates", default="10,30,100,300,1000", help="config5: arrival rates (requests/s)")
     ap.add_argument("--serve-requests", type=int, default=32, help="config5: requests per rate")
     ap.add_argument("--e2e-steps", type=int, default=1)
@@ -272,6 +272,8 @@ def main():
         bench_multi(args, G, W, ctx, rank, world, dist)
     elif args.config == "config5":
         bench_serve(args, G, W, ctx, rank, world, dist)
+    elif args.config == "config3":
+        bench_precision(args, G, W, ctx, rank, world, dist)
     else:
         bench_single(args, G, W, ctx, rank, world, dist)
     if dist is not None:
@@ -449,6 +451,70 @@ def bench_multi(args, G, W, ctx, rank, world, dist):
                 "e2e": e2e, "roofline": roofline, "compute_roofline": compute, "cpu_baseline": cpu,
                 "gpu_launches": int(launches), "clocks": clock.summary(),
                 "phases_ms_per_step": {k: v[0] / args.steps for k, v in prof.items()}}
+        print(json.dumps(line))
+
+
+def bench_precision(args, G, W, ctx, rank, world, dist):
+    """config 3: FP32 (as generated, Kahan per pixel) against FP64 expected counts on the
+    full-sky workload, and the placed stars' DM distribution against the FP64 expectation."""
+    L = G.lib()
+    w, desc = workload(G, W, "config2", rank)
+    sk = G.Skygen(ctx, w)
+    reps, hist = [], None
+    t0 = time.perf_counter()
+    for m in range(len(w.models)):
+        rep, p32, p64, h = sk.precision(m)
+        reps.append({"model": m, "expected32": rep.expected32, "expected64": rep.expected64,
+                     "total_rel_err": rep.total_rel_err, "bin_max_rel_err": rep.bin_max_rel_err,
+                     "bin_mean_rel_err": rep.bin_mean_rel_err, "pixel_max_rel_err": rep.pixel_max_rel_err,
+                     "pixel_mean_rel_err": rep.pixel_mean_rel_err, "bins": int(rep.bins)})
+        hist = h if hist is None else hist + h
+    t_prec = time.perf_counter() - t0
+    info = sk.info(0)
+    sk.close()
+    # placed stars: DM of every stored row, against the FP64 expected DM distribution
+    edges = np.arange(info.m0 - info.M1 - 0.5 * info.dm - 0.2, info.m1 - info.M0 + 0.2, 0.01)
+    counts = np.zeros(len(edges) - 1)
+    dm_host = {}
+
+    def cb(user, model, tptr, off):
+        t = tptr.contents
+        n = int(t.size)
+        if n not in dm_host:
+            dm_host.clear()
+            dm_host[n] = np.zeros(n, dtype=np.float32)
+        h = G.Table()
+        h.capacity, h.nbands = n, t.nbands
+        h.DM = dm_host[n].ctypes.data
+        if L.gf_table_download_rows(ctx.h, tptr, 0, n, C.byref(h)) != 0:
+            return 1
+        counts[:] += np.histogram(dm_host[n], bins=edges)[0]
+        return 0
+    stats = G.CatalogStats()
+    G.check(L.gf_catalog_run(ctx.h, C.byref(w.job(G.Job)), G.BatchCallback(cb), None, C.byref(stats)))
+    # expected: diagonal d has DM = m0 - M1 + d dm; a star's DM spreads triangularly over +-dm
+    d_dm = (info.m0 - info.M1) + np.arange(len(hist)) * info.dm
+    centers = 0.5 * (edges[1:] + edges[:-1])
+    expct = np.zeros_like(centers)
+    for dmc, hv in zip(d_dm, hist):
+        tri = np.clip(1.0 - np.abs(centers - dmc) / info.dm, 0.0, None)
+        if tri.sum() > 0:
+            expct += hv * tri / tri.sum()
+    cdf_o = np.cumsum(counts) / counts.sum()
+    cdf_e = np.cumsum(expct) / expct.sum()
+    ks = float(np.max(np.abs(cdf_o - cdf_e)))
+    if rank == 0:
+        worst = max(r["total_rel_err"] for r in reps)
+        line = {"metric": "expected-count error of the FP32 path against FP64 (max over models, relative)",
+                "value": worst, "unit": "relative error", "n_gpus": world, "steps": 1, "warmup": 0,
+                "ms_per_step": 1e3 * t_prec, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 vs f64", "data": "synthetic",
+                "config": {"workload": "config3: " + desc, "pixels": w.npixels},
+                "precision": reps,
+                "dm_distribution": {"stars": float(counts.sum()), "expected_fp64": float(hist.sum()), "ks": ks,
+                                    "ks_sqrt_n": ks * math.sqrt(counts.sum()),
+                                    "note": "stored (visible) rows against all expected stars; hidden rows are not stored"},
+                "e2e": None, "roofline": None, "cpu_baseline": None, "gpu_launches": None}
         print(json.dumps(line))
 
 

@@ -103,6 +103,8 @@ def lib():
         L.gf_server_submit.argtypes = [vp, C.POINTER(Job), ServerRows, ServerDone, vp, C.POINTER(C.c_int64)]
         L.gf_server_drain.argtypes = [vp]
         L.gf_server_destroy.argtypes = [vp]
+        L.gf_skygen_precision.argtypes = [vp, C.c_int32, C.POINTER(A.PrecisionReport), C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.gf_lambert_init.argtypes = [C.c_double, C.c_double, C.POINTER(Lambert)]
         L.gf_footprint_pixelize.argtypes = [C.POINTER(Footprint), C.c_double, C.POINTER(Lambert),
                                             C.POINTER(Extinction), C.POINTER(PencilBeam), C.POINTER(C.c_float),
@@ -302,6 +304,18 @@ class Skygen:
         check(lib().gf_skygen_integrate(self.h, model, C.byref(e), C.byref(ec),
                                         pp.ctypes.data_as(C.POINTER(C.c_double)) if pp is not None else None))
         return e.value, ec.value, pp
+
+    def precision(self, model):
+        """gf_skygen_precision: (report, per-pixel FP32 sums, per-pixel FP64 sums, FP64 counts per DM row)."""
+        i = self.info(model)
+        rep = A.PrecisionReport()
+        p32 = np.zeros(self.w.npixels)
+        p64 = np.zeros(self.w.npixels)
+        hist = np.zeros(i.nm + i.nM - 1)
+        dp = C.POINTER(C.c_double)
+        check(lib().gf_skygen_precision(self.h, model, C.byref(rep), p32.ctypes.data_as(dp), p64.ctypes.data_as(dp),
+                                        hist.ctypes.data_as(dp)))
+        return rep, p32, p64, hist
 
     def set_density_norm(self, model, norm):
         check(lib().gf_skygen_set_norm(self.h, model, norm))

@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -604,6 +605,62 @@ gf_status gf_skygen_integrate(gf_skygen *s, int32_t model, double *expected, dou
     ms.expected_covered = ec;
     if (expected) *expected = e;
     if (expected_covered) *expected_covered = ec;
+    return GF_OK;
+}
+
+gf_status gf_skygen_precision(gf_skygen *s, int32_t model, gf_precision_report *rep, double *per_pixel32,
+                              double *per_pixel64, double *dm_hist64)
+{
+    if (!s || model < 0 || model >= (int)s->models.size() || !rep) return fail(GF_E_INVALID, "invalid arguments");
+    GF_TRY(check_ctx(s->ctx));
+    ModelState &ms = s->models[model];
+    SkyModel m = ms.hm.m;
+    m.lf = ms.d_lf;
+    if (((long long)m.nm * m.nM) % GF_BLOCK) return fail(GF_E_UNSUPPORTED, "nm*nM must be a multiple of 10");
+    cudaStream_t st = s->ctx->stream;
+    const int npix = s->geom.npixels, nd = m.nm + m.nM - 1;
+    double *d = nullptr;
+    GF_TRY(dev_alloc(&d, 2 * (size_t)npix + nd + 4));
+    double *pix32 = d, *pix64 = d + npix, *hist = d + 2 * (size_t)npix, *acc = hist + nd;
+    GF_CUDA(cudaMemsetAsync(d, 0, 8 * (2 * (size_t)npix + nd + 4), st));
+    cudaError_t e = gfk::launch_precision(m, s->geom, ms.d_Dtab, pix32, pix64, hist, (unsigned long long *)acc, acc + 1,
+                                          (unsigned long long *)(acc + 2), st);
+    if (e != cudaSuccess) { dev_free(d); return fail(GF_E_CUDA, cudaGetErrorString(e)); }
+    std::vector<double> h(2 * (size_t)npix + nd + 4);
+    GF_CUDA(cudaMemcpyAsync(h.data(), d, 8 * h.size(), cudaMemcpyDeviceToHost, st));
+    GF_CUDA(cudaStreamSynchronize(st));
+    dev_free(d);
+    double e32 = 0, e64 = 0, pmax = 0, psum = 0;
+    int64_t pn = 0;
+    for (int i = 0; i < npix; i++) {
+        const double a = h[i], b = h[npix + i];
+        e32 += a;
+        e64 += b;
+        if (b != 0.0) {
+            const double r = fabs(a - b) / fabs(b);
+            pmax = std::max(pmax, r);
+            psum += r;
+            pn++;
+        }
+    }
+    const double *hacc = h.data() + 2 * (size_t)npix + nd;
+    uint64_t mbits;
+    memcpy(&mbits, hacc, 8);
+    double bmax;
+    memcpy(&bmax, &mbits, 8);
+    uint64_t nb;
+    memcpy(&nb, hacc + 2, 8);
+    rep->expected32 = e32;
+    rep->expected64 = e64;
+    rep->total_rel_err = e64 != 0 ? fabs(e32 - e64) / fabs(e64) : 0.0;
+    rep->bin_max_rel_err = bmax;
+    rep->bin_mean_rel_err = nb ? hacc[1] / (double)nb : 0.0;
+    rep->pixel_max_rel_err = pmax;
+    rep->pixel_mean_rel_err = pn ? psum / (double)pn : 0.0;
+    rep->bins = (int64_t)nb;
+    if (per_pixel32) memcpy(per_pixel32, h.data(), 8 * (size_t)npix);
+    if (per_pixel64) memcpy(per_pixel64, h.data() + npix, 8 * (size_t)npix);
+    if (dm_hist64) memcpy(dm_hist64, h.data() + 2 * (size_t)npix, 8 * (size_t)nd);
     return GF_OK;
 }
 

@@ -129,6 +129,10 @@ cudaError_t launch_photoerrors(const PerrTables &c, int64_t row_offset, gf_table
 cudaError_t launch_vel2pm(const gf_vel2pm_config &c, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
 cudaError_t launch_gal2other(int32_t coordsys, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
 
+cudaError_t launch_precision(const SkyModel &m, const SkyGeom &g, const float *Dtab, double *pix32, double *pix64,
+                             double *hist64, unsigned long long *max_rel, double *sum_rel, unsigned long long *nbins,
+                             cudaStream_t s);
+
 /* module kernels over the rows of many requests (row_slot: the request slot of each row) */
 struct MultiRows {
     const int32_t *row_slot;       /* [rows] */

@@ -376,6 +376,26 @@ typedef int (*gf_batch_callback)(void *user, int32_t model, const gf_table *dev_
 
 gf_status gf_catalog_run(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, void *user, gf_catalog_stats *stats);
 
+/* ---- precision form ---- */
+
+typedef struct gf_precision_report {
+    double expected32;          /* FP32 bin counts (as generated), Kahan-summed per pixel in FP32 */
+    double expected64;          /* FP64 evaluation of the same bins (same LF texels and anchors) */
+    double total_rel_err;       /* |expected32 - expected64| / expected64 */
+    double bin_max_rel_err;     /* over bins with an expected count */
+    double bin_mean_rel_err;
+    double pixel_max_rel_err;   /* per-pixel sums, over pixels with a nonzero FP64 count */
+    double pixel_mean_rel_err;
+    int64_t bins;
+} gf_precision_report;
+
+/* The expected counts of one model in both precisions (see gf_precision_report).
+ * per_pixel32/per_pixel64: npixels entries or NULL; dm_hist64: FP64 counts per
+ * distance-modulus row d = im + iM (nm + nM - 1 entries, DM = m0 - M1 + d dm) or
+ * NULL.  Needs nm*nM to be a multiple of 10 (the crawl's anchors per pixel). */
+gf_status gf_skygen_precision(gf_skygen *s, int32_t model, gf_precision_report *rep, double *per_pixel32,
+                              double *per_pixel64, double *dm_hist64);
+
 /* ---- many requests per pass ---- */
 
 /* Called once per model with the device table holding that model's rows of

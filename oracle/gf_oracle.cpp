@@ -982,6 +982,66 @@ int or_skygen_integrate(void *h, int32_t mi, double *expected, double *expected_
     return 0;
 }
 
+/* The precision form's FP64 oracle for one pixel: every bin in the crawl's order
+ * with its anchor at the block starts (every 10th bin, nm*nM a multiple of 10)
+ * and the diagonal starts, the reference's float expected count (skygen.cu.h:
+ * 541-565, summed in double) and the same bin evaluated in double throughout
+ * (D = 10^(0.2 DM + 1), model density, D^3 dA POGSON dm dM; the LF texel and the
+ * float model parameters as given). */
+int or_expected_fp64(void *h, int32_t mi, int32_t px, double *sum32, double *sum64)
+{
+    Sky *s = (Sky *)h;
+    const Model &m = s->models[mi];
+    const int nm = m.nm, nM = m.nM, kmax = nm * nM;
+    if (px < 0 || px >= (int)s->pixels.size() || kmax % BLOCK) return 1;
+    Launch L = {};
+    L.sky = s; L.m = &m; L.npixels = (int)s->pixels.size(); L.pixels = s->pixels.data();
+    const gf_pencil_beam pix = s->pixels[px];
+    double a32 = 0, a64 = 0;
+    float D = 0, Am = 0, ms = 0;
+    double ms64 = 0, D364 = 0, K64 = 0;
+    for (int k = 0; k < kmax; k++) {
+        int ilb = 0, im, iM, kk = k;
+        diagIndexToIJ(ilb, im, iM, kk, nm, nM);
+        const bool anchor = (k % BLOCK == 0) || im == 0 || iM == nM - 1;
+        const float M = m.M1 - iM * m.dM;
+        if (anchor) {
+            F3 pos = compute_pos(L, D, Am, M, im, pix);
+            ms = m.rho(pos.x, pos.y, pos.z);
+            const double Md = (double)m.M1 - (double)iM * (double)m.dM;
+            const double mm = (double)m.m0 + (double)im * (double)m.dm;
+            const double Dd = pow(10.0, 0.2 * (mm - Md) + 1.0);
+            const double x = Dd * (double)pix.cl * (double)pix.cb, y = Dd * (double)pix.sl * (double)pix.cb, z = Dd * (double)pix.sb;
+            const double vx = x + m.T[0], vy = y + m.T[1], vz = z + m.T[2];
+            const double wx = m.M[0][0] * vx + m.M[0][1] * vy + m.M[0][2] * vz;
+            const double wy = m.M[1][0] * vx + m.M[1][1] * vy + m.M[1][2] * vz;
+            const double wz = m.M[2][0] * vx + m.M[2][1] * vy + m.M[2][2] * vz;
+            if (m.type == GF_MODEL_EXP_DISK) {
+                const double r2 = wx * wx + wy * wy;
+                ms64 = (m.r_cut2 && r2 + wz * wz > m.r_cut2) ? 0.0 : m.f * exp(-sqrt(r2) / m.l - fabs(wz) / m.h);
+            } else {
+                const double DSq = wx * wx + wy * wy + wz * wz;
+                const double ty = wy / m.ba, tz = wz / m.ca;
+                ms64 = (m.rmaxSq && (DSq < m.rminSq || DSq >= m.rmaxSq)) ? 0.0 : m.f * pow(wx * wx + ty * ty + tz * tz, 0.5 * m.n);
+            }
+            D364 = Dd * Dd * Dd;
+            K64 = (double)pix.dA * 0.46051701859880913680 * (double)m.dm * (double)m.dM;
+        }
+        if ((m.dmin || m.dmax) && (m.dmin > D || m.dmax <= D)) continue;
+        if (m.m0 + m.dm * im + Am > m.m1) continue;
+        const float lfv = m.lf_sample(M);
+        float rho = lfv * ms;
+        rho *= m.norm;
+        rho *= D * D * D;
+        rho *= pix.dA * POGSON * m.dm * m.dM;
+        a32 += rho;
+        a64 += (double)lfv * ms64 * (double)m.norm * D364 * K64;
+    }
+    *sum32 = a32;
+    *sum64 = a64;
+    return 0;
+}
+
 /* setDensityNorm (skyconfig_impl.h:308-320) */
 int or_skygen_set_norm(void *h, int32_t mi, float norm)
 {

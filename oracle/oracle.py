@@ -39,6 +39,7 @@ def load(flavour="p"):
         L.or_skygen_model_info.argtypes = [vp, C.c_int32, vp]
         L.or_skygen_model_lf.argtypes = [vp, C.c_int32, vp]
         L.or_skygen_integrate.argtypes = [vp, C.c_int32, vp, vp, vp]
+        L.or_expected_fp64.argtypes = [vp, C.c_int32, C.c_int32, vp, vp]
         L.or_skygen_set_norm.argtypes = [vp, C.c_int32, C.c_float]
         L.or_skygen_draw.argtypes = [vp, C.c_int32, vp, C.c_int32, vp, vp, vp]
         L.or_module_clipper.argtypes = [vp, vp, vp, C.c_int64, C.c_int64]
@@ -110,6 +111,14 @@ class OracleSkygen:
         self.L.or_skygen_integrate(self.h, model, C.addressof(e), C.addressof(ec), pp.ctypes.data if pp is not None else None)
         return e.value, ec.value, pp
 
+
+    def expected_fp64(self, model, pixel):
+        """(reference float sum, FP64 sum) of the expected counts of one pixel."""
+        a = C.c_double()
+        b = C.c_double()
+        if self.L.or_expected_fp64(self.h, model, pixel, C.addressof(a), C.addressof(b)) != 0:
+            raise ValueError("pixel out of range or nm*nM not a multiple of 10")
+        return a.value, b.value
     def set_density_norm(self, model, norm):
         self.L.or_skygen_set_norm(self.h, model, norm)
 
