@@ -3,7 +3,8 @@
  * (pixel, m, M) bin evaluated twice, as the catalog path evaluates them (FP32,
  * the reference's float expressions) and in FP64, over the same
  * discretisation (the same LF texels, the same anchor bins: block starts and
- * diagonal starts of the crawl, skygen.cu.h:216-229, 541-565).
+ * diagonal starts of the crawl, skygen.cu.h:216-229, 541-565).  The per-bin
+ * statistics cover the bins whose FP64 count is at least FLT_MIN.
  *
  * One warp per pixel; lane l takes the pixel's blocks l, l + 32, ...  Per pixel
  * the FP32 values are summed with Kahan compensation in FP32 and the FP64
@@ -96,12 +97,14 @@ __global__ void __launch_bounds__(128) precision_kernel(SkyModel m, SkyGeom g, c
                 c32 = (tk - s32) - yk;
                 s32 = tk;
                 s64 += mu64;
-                if (mu64 != 0.0) {
+                /* relative error over bins whose count is a normal float; below FLT_MIN a
+                 * float keeps fewer significant bits (those bins add < 1e-30 stars) */
+                if (fabs(mu64) >= 1.17549435082228750797e-38) {
                     const double r = fabs((double)mu - mu64) / fabs(mu64);
                     rel_max = r > rel_max ? r : rel_max;
                     rel_sum += r;
+                    count++;
                 }
-                count++;
                 atomicAdd(&s_hist[ci + cj], mu64);
             }
         }
