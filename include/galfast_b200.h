@@ -382,7 +382,8 @@ typedef struct gf_precision_report {
     double expected32;          /* FP32 bin counts (as generated), Kahan-summed per pixel in FP32 */
     double expected64;          /* FP64 evaluation of the same bins (same LF texels and anchors) */
     double total_rel_err;       /* |expected32 - expected64| / expected64 */
-    double bin_max_rel_err;     /* over bins whose FP64 count is a normal float (>= FLT_MIN) */
+    double bin_max_rel_err;     /* over bins with >= 1e-30 expected stars (smaller counts pass through
+                                   subnormal floats in the reference's expressions) */
     double bin_mean_rel_err;
     double pixel_max_rel_err;   /* per-pixel sums, over pixels with a nonzero FP64 count */
     double pixel_mean_rel_err;
