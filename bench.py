@@ -292,7 +292,8 @@ def reduce_max_sum(dist, tmax, tsum):
     if dist is None:
         return tmax, tsum
     import torch
-    t = torch.tensor([tmax, tsum], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([tmax, tsum], dtype=torch.float64, device=dev)
     a, b = t[:1].clone(), t[1:].clone()
     dist.all_reduce(a, op=dist.ReduceOp.MAX)
     dist.all_reduce(b, op=dist.ReduceOp.SUM)
