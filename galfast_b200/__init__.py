@@ -98,6 +98,8 @@ def lib():
         L.gf_catalog_run.argtypes = [vp, C.POINTER(Job), BatchCallback, vp, C.POINTER(CatalogStats)]
         L.gf_catalog_run_multi.argtypes = [vp, C.POINTER(Job), C.c_int32, MultiCallback, vp, C.POINTER(CatalogStats)]
         L.gf_multi_set_memory_budget.argtypes = [vp, C.c_int64]
+        L.gf_tuning_get.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32)]
+        L.gf_tuning_set.argtypes = [vp, C.c_int32, C.c_int32]
         L.gf_table_download_rows.argtypes = [vp, C.POINTER(Table), C.c_int64, C.c_int64, C.POINTER(Table)]
         L.gf_server_create.argtypes = [C.c_int32, C.c_int32, C.c_int64, C.c_int32, C.POINTER(vp)]
         L.gf_server_submit.argtypes = [vp, C.POINTER(Job), ServerRows, ServerDone, vp, C.POINTER(C.c_int64)]
@@ -224,6 +226,18 @@ class Context:
         ms = C.c_float()
         check(lib().gf_ctx_elapsed(self.h, a, b, C.byref(ms)))
         return ms.value
+
+    def tuning(self):
+        """{model kind: warps per stream of the batched draw} (0 = not tuned yet)."""
+        out = {}
+        for k in (A.GF_MODEL_EXP_DISK, A.GF_MODEL_POWER_LAW_ELLIPSOID):
+            w = C.c_int32()
+            check(lib().gf_tuning_get(self.h, k, C.byref(w)))
+            out[k] = w.value
+        return out
+
+    def set_tuning(self, model_kind, warps):
+        check(lib().gf_tuning_set(self.h, model_kind, warps))
 
     def set_multi_budget(self, nbytes):
         """Device bytes per chunk of gf_catalog_run_multi (0 = 60% of free memory)."""

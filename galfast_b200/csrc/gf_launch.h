@@ -28,6 +28,7 @@ struct LaunchCrawl {
     Checkpoint *ck;                /* draw: checkpoints at the first bin with stars and every ck_every stars */
     uint32_t *ck_count;
     int32_t ck_capacity, ck_every;
+    int32_t cw;                    /* draw: warps per stream (1, 2 or 4; 0 = 4) */
 };
 
 struct LaunchPlace {
@@ -68,6 +69,7 @@ struct LaunchCrawlMulti {
     StarRecord *rec;
     int64_t rec_capacity;
     unsigned long long *rec_count, *err;
+    int32_t cw;                    /* draw: warps per stream (1, 2 or 4; 0 = 4) */
 };
 
 struct LaunchPlaceMulti {

@@ -575,6 +575,41 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
             for (int j : batched) want += S[j].expected[i] + 8.0 * sqrt(S[j].expected[i]) + 1024.0;
             int64_t cap = (int64_t)want;
             GF_CUDA(cudaMemcpyAsync(d_rng_snap, d_rng, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
+            const int mtype = R[batched[0]].hm[i].m.type;
+            GF_TRY(rec.need((size_t)cap));
+            if (ctx->draw_cw[mtype] == 0) {
+                /* autotuner: time 4, 2 and 1 warps per stream on the head of the work queue
+                 * (the largest requests), from the same stream states, and keep the fastest */
+                const int32_t trial = std::min<int32_t>(nitems, std::max<int32_t>(nitems / 16, 148 * 32));
+                float best_ms = 0.f;
+                int best = 4;
+                cudaEvent_t e0, e1;
+                GF_CUDA(cudaEventCreate(&e0));
+                GF_CUDA(cudaEventCreate(&e1));
+                for (int cw : {4, 2, 1}) {
+                    GF_CUDA(cudaMemcpyAsync(d_rng, d_rng_snap, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
+                    GF_CUDA(cudaMemsetAsync(cs_base, 0, cs_bytes, st));
+                    GF_CUDA(cudaMemsetAsync(ctx->d_counters, 0, 24, st));
+                    gfk::LaunchCrawlMulti T;
+                    memset(&T, 0, sizeof(T));
+                    T.jobs = d_jobs; T.items = d_items; T.nitems = trial; T.counter = d_counter;
+                    T.model_type = mtype; T.max_tab = max_tab(i, batched); T.jt = ctx->jt;
+                    T.rec = rec.p; T.rec_capacity = (int64_t)rec.n;
+                    T.rec_count = ctx->d_counters; T.err = ctx->d_counters + 2;
+                    T.cw = cw;
+                    GF_CUDA(cudaEventRecord(e0, st));
+                    GF_CUDA(gfk::launch_crawl_multi(T, 1, st));
+                    GF_CUDA(cudaEventRecord(e1, st));
+                    GF_CUDA(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    GF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    if (cw == 4 || ms < best_ms) { best_ms = ms; best = cw; }
+                }
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                ctx->draw_cw[mtype] = best;
+                GF_CUDA(cudaMemcpyAsync(d_rng, d_rng_snap, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
+            }
             int64_t nrec = 0;
             for (;;) {
                 GF_TRY(rec.need((size_t)cap));
@@ -588,6 +623,7 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
                 L.jt = ctx->jt;
                 L.rec = rec.p; L.rec_capacity = (int64_t)rec.n;
                 L.rec_count = ctx->d_counters; L.err = ctx->d_counters + 2;
+                L.cw = ctx->draw_cw[mtype];
                 {
                     ProfScope ps(ctx, GF_PROF_DRAW_WINDOW);
                     GF_CUDA(gfk::launch_crawl_multi(L, 1, st));
@@ -717,5 +753,23 @@ extern "C" gf_status gf_multi_set_memory_budget(gf_ctx *ctx, int64_t bytes)
     GF_TRY(gfa::check_ctx(ctx));
     if (bytes < 0) return fail(GF_E_INVALID, "negative memory budget");
     ctx->multi_budget = bytes;
+    return GF_OK;
+}
+
+extern "C" gf_status gf_tuning_get(gf_ctx *ctx, int32_t model_kind, int32_t *warps_per_stream)
+{
+    GF_TRY(gfa::check_ctx(ctx));
+    if (model_kind < 1 || model_kind > 2 || !warps_per_stream) return fail(GF_E_INVALID, "invalid arguments");
+    *warps_per_stream = ctx->draw_cw[model_kind];
+    return GF_OK;
+}
+
+extern "C" gf_status gf_tuning_set(gf_ctx *ctx, int32_t model_kind, int32_t warps_per_stream)
+{
+    GF_TRY(gfa::check_ctx(ctx));
+    if (model_kind < 1 || model_kind > 2) return fail(GF_E_INVALID, "invalid model kind");
+    if (warps_per_stream != 0 && warps_per_stream != 1 && warps_per_stream != 2 && warps_per_stream != 4)
+        return fail(GF_E_INVALID, "warps per stream must be 1, 2, 4 or 0 (tune again)");
+    ctx->draw_cw[model_kind] = warps_per_stream;
     return GF_OK;
 }

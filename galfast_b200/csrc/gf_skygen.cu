@@ -50,8 +50,8 @@ struct CrawlParams {
     uint32_t *next_item;           /* persistent launch: work-queue counter (items taken in order), or null */
 };
 
-#define GF_CW 4                    /* warps per stream */
-#define GF_WIN (GF_CW * 32)        /* blocks of a stream evaluated together (one per thread) */
+/* CW (a template parameter of the crawl): warps per stream; a window holds CW * 32
+ * blocks of the stream, one per thread.  1, 2 or 4, picked by the autotuner. */
 #define FULLMASK 0xffffffffu
 
 __device__ __forceinline__ uint64_t shfl64(uint64_t v, int src)
@@ -130,17 +130,17 @@ struct Cursor {
 
 #define GF_RECBUF 64               /* star records staged in shared memory per stream */
 
-template <int DRAW>
+template <int DRAW, int CW>
 struct CrawlSmem {
     CrawlJob job;
-    float4 slot[GF_WIN * GF_BLOCK];           /* anchor inputs (pixel, i<<16|j), then AnchorX; thread L owns [10L, 10L+10) */
-    uint16_t dense[GF_WIN * GF_BLOCK];        /* compacted list of the window's anchor slots */
-    float mu[DRAW ? GF_CW : 1][GF_BLOCK][32]; /* mu of bin s of each thread's block */
+    float4 slot[(CW * 32) * GF_BLOCK];           /* anchor inputs (pixel, i<<16|j), then AnchorX; thread L owns [10L, 10L+10) */
+    uint16_t dense[(CW * 32) * GF_BLOCK];        /* compacted list of the window's anchor slots */
+    float mu[DRAW ? CW : 1][GF_BLOCK][32]; /* mu of bin s of each thread's block */
     StarRecord recbuf[DRAW ? GF_RECBUF : 1];
     int nrec;
-    int wtot[GF_CW];
-    int wev[GF_CW];
-    int scan[GF_CW];
+    int wtot[CW];
+    int wev[CW];
+    int scan[CW];
     unsigned long long v_end;
     /* stream state shared by the CTA; written by one thread between barriers */
     Cursor cur;
@@ -148,12 +148,12 @@ struct CrawlSmem {
     unsigned long long mult;       /* scaled a^(k-1) after a bin with stars that drew k uniforms */
     long long nstars, limit;
     int next_ck, flag, fL, es;
-    double red[2][GF_CW];
+    double red[2][CW];
 };
 
 /* Write the staged star records to the global buffer (one warp, all lanes). */
-template <int DRAW>
-__device__ void flush_records(const CrawlParams &P, CrawlSmem<DRAW> &S, int lane)
+template <int DRAW, int CW>
+__device__ void flush_records(const CrawlParams &P, CrawlSmem<DRAW, CW> &S, int lane)
 {
     __syncwarp();
     const int n = S.nrec;
@@ -174,8 +174,8 @@ __device__ void flush_records(const CrawlParams &P, CrawlSmem<DRAW> &S, int lane
  * limit (draw_stars, skygen.cu.h:366-457); the uniforms are staged as star
  * records for the placement kernel.  Executed identically by all lanes of one
  * warp; lane 0 writes. */
-template <int DRAW>
-__device__ void draw_stars(const CrawlParams &P, CrawlSmem<DRAW> &S, int sid, int lane, gfr::Mwc &r, int &ndraw,
+template <int DRAW, int CW>
+__device__ void draw_stars(const CrawlParams &P, CrawlSmem<DRAW, CW> &S, int sid, int lane, gfr::Mwc &r, int &ndraw,
                            long long &nstars, long long limit, int ilb, int im, int iM)
 {
     if (!ndraw) return;
@@ -234,8 +234,8 @@ __device__ __noinline__ bool has_stars(float u, float mu)
  * reached its limit and pauses after the bin, 2: stop on an infinite expected
  * count).  For a block inside one pixel the bin and its anchor are found by
  * stepping from the block start and reading the window's anchor slots. */
-template <int DRAW, int MODEL>
-__device__ __noinline__ void handle_event(const CrawlParams &P, CrawlSmem<DRAW> &S, int sid, int lane, int fL, int es,
+template <int DRAW, int MODEL, int CW>
+__device__ __noinline__ void handle_event(const CrawlParams &P, CrawlSmem<DRAW, CW> &S, int sid, int lane, int fL, int es,
                                           uint64_t vb, float emu, int f_ilb, int f_k, int f_i0, int f_j0, bool f_fast,
                                           uint32_t a, const uint64_t *jlo, const uint64_t *jhi)
 {
@@ -287,7 +287,7 @@ __device__ __noinline__ void handle_event(const CrawlParams &P, CrawlSmem<DRAW> 
         r.set_v(vb);
         r.used = 0;
         nd = (int)r.poisson(emu);
-        draw_stars<DRAW>(P, S, sid, lane, r, nd, ns, S.limit, e_ilb, e_im, e_iM);
+        draw_stars<DRAW, CW>(P, S, sid, lane, r, nd, ns, S.limit, e_ilb, e_im, e_iM);
         vnew = r.v();
         if (nd) flag = 1;             /* the stream reached its limit: pause right after the bin */
         /* The walk assumed one uniform for this bin; it drew r.used >= 1.  Every later
@@ -316,15 +316,15 @@ __device__ __noinline__ void handle_event(const CrawlParams &P, CrawlSmem<DRAW> 
 
 /* Finish the draw that did not complete before the previous batch filled
  * (skygen.cu.h:497-502); warp 0. */
-template <int DRAW>
-__device__ __noinline__ void finish_pending(const CrawlParams &P, CrawlSmem<DRAW> &S, int sid, int lane, uint32_t a)
+template <int DRAW, int CW>
+__device__ __noinline__ void finish_pending(const CrawlParams &P, CrawlSmem<DRAW, CW> &S, int sid, int lane, uint32_t a)
 {
     gfr::Mwc r;
     r.a = a;
     r.set_v(S.v);
     int nd = S.cur.ndraw;
     long long ns = S.nstars;
-    draw_stars<DRAW>(P, S, sid, lane, r, nd, ns, S.limit, S.cur.cur_ilb, S.cur.cur_im, S.cur.cur_iM);
+    draw_stars<DRAW, CW>(P, S, sid, lane, r, nd, ns, S.limit, S.cur.cur_ilb, S.cur.cur_im, S.cur.cur_iM);
     __syncwarp();
     if (lane == 0) { S.v = r.v(); S.nstars = ns; S.cur.ndraw = nd; S.next_ck = (int)ns; }
     __syncwarp();
@@ -333,8 +333,8 @@ __device__ __noinline__ void finish_pending(const CrawlParams &P, CrawlSmem<DRAW
 /* A block that runs past the end of its pixel (possible only when nm*nM is not
  * a multiple of 10): follow advance() bin by bin with the anchors inline.
  * Returns whether the crawl left the last pixel inside the block. */
-template <int DRAW, int MODEL>
-__device__ __noinline__ bool slow_block(CrawlSmem<DRAW> &S, const float *LFM, const float *MMr, int L, int i0, int j0,
+template <int DRAW, int MODEL, int CW>
+__device__ __noinline__ bool slow_block(CrawlSmem<DRAW, CW> &S, const float *LFM, const float *MMr, int L, int i0, int j0,
                                         int my_ilb, int s_begin, uint32_t &live, double &cnt_sum, double &cov_sum)
 {
     const CrawlJob &J = S.job;
@@ -380,8 +380,8 @@ __device__ __noinline__ bool slow_block(CrawlSmem<DRAW> &S, const float *LFM, co
 
 /* Crawl of one stream by one CTA (integrate when DRAW = 0, Poisson draw when
  * DRAW = 1).  Thread L of the CTA owns block j+L of the stream's window. */
-template <int DRAW, int MODEL>
-__device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float *LFM, const float *MMr, int tid)
+template <int DRAW, int MODEL, int CW>
+__device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW, CW> &S, const float *LFM, const float *MMr, int tid)
 {
     const CrawlJob &J = S.job;
     const SkyModel &m = J.m;
@@ -393,7 +393,7 @@ __device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float
     const long long step = (long long)GF_BLOCK * m.nthreads;
     const long long offL = (long long)L * step;
     const int qL = (int)(offL / kmax), rL = (int)(offL % kmax);
-    const long long offW = (long long)GF_WIN * step;
+    const long long offW = (long long)(CW * 32) * step;
     const int QW = (int)(offW / kmax), RW = (int)(offW % kmax);
     const int sid = (J.job_id << 16) | tid;
 
@@ -434,7 +434,7 @@ __device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float
         jlo = P.jt.lo + (size_t)tid * 32;
         jhi = P.jt.hi + (size_t)tid * GF_JUMP_HI;
         if (S.cur.ndraw) {
-            if (warp == 0) finish_pending<DRAW>(P, S, sid, lane, a);
+            if (warp == 0) finish_pending<DRAW, CW>(P, S, sid, lane, a);
             __syncthreads();
         }
         v = S.v;
@@ -456,7 +456,7 @@ __device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float
             if (lane == 31) S.scan[warp] = inc;
             __syncthreads();
             int woff = 0;
-            for (int q = 0; q < GF_CW; q++) {
+            for (int q = 0; q < CW; q++) {
                 const int t = S.scan[q];
                 woff += (q < warp) ? t : 0;
                 dtot += t;
@@ -499,7 +499,7 @@ __device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float
             if (lane == 31) S.scan[warp] = inc;
             __syncthreads();
             int woff = 0, T = 0;
-            for (int q = 0; q < GF_CW; q++) {
+            for (int q = 0; q < CW; q++) {
                 const int t = S.scan[q];
                 woff += (q < warp) ? t : 0;
                 T += t;
@@ -507,7 +507,7 @@ __device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float
             const int excl = woff + inc - na;
             for (int n = 0; n < na; n++) S.dense[excl + n] = (uint16_t)(base + n);
             __syncthreads();
-            for (int d = L; d < T; d += GF_WIN) {
+            for (int d = L; d < T; d += (CW * 32)) {
                 const int sl = S.dense[d];
                 const float4 in = S.slot[sl];
                 const int ij = __float_as_int(in.y);
@@ -545,7 +545,7 @@ __device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float
             }
             if (!DRAW && J.per_pixel) atomicAdd(&J.per_pixel[my_ilb + J.pix_base], bcov);
         } else if (!dead0) {
-            if (slow_block<DRAW, MODEL>(S, LFM, MMr, L, i0, j0, my_ilb, s_begin, live, cnt_sum, cov_sum)) lane_end = true;
+            if (slow_block<DRAW, MODEL, CW>(S, LFM, MMr, L, i0, j0, my_ilb, s_begin, live, cnt_sum, cov_sum)) lane_end = true;
         }
         const int any_end = __syncthreads_or(lane_end);
 
@@ -561,7 +561,7 @@ __device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float
                 if (lane == 31) S.wtot[warp] = inc;
                 __syncthreads();
                 int woff = 0;
-                for (int q = 0; q < GF_CW; q++) woff += (q < warp) ? S.wtot[q] : 0;
+                for (int q = 0; q < CW; q++) woff += (q < warp) ? S.wtot[q] : 0;
                 wst = jump(v, woff + inc - cnt, jlo, jhi, a);
             }
             const uint64_t pmod = ((uint64_t)a << 32) - 1;
@@ -586,10 +586,10 @@ __device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float
                 }
                 const unsigned evm = __ballot_sync(FULLMASK, ev_s >= 0);
                 if (lane == 0) S.wev[warp] = evm ? (__ffs(evm) - 1) : -1;
-                if (L == GF_WIN - 1) S.v_end = w;
+                if (L == (CW * 32) - 1) S.v_end = w;
                 __syncthreads();
                 int fw = -1, fl = 0;
-                for (int q = 0; q < GF_CW; q++) {
+                for (int q = 0; q < CW; q++) {
                     const int e = S.wev[q];
                     if (fw < 0 && e >= 0) { fw = q; fl = e; }
                 }
@@ -606,7 +606,7 @@ __device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float
                     const int f_i0 = __shfl_sync(FULLMASK, i0, fl);
                     const int f_j0 = __shfl_sync(FULLMASK, j0, fl);
                     const bool f_fast = __shfl_sync(FULLMASK, fast ? 1 : 0, fl) != 0;
-                    handle_event<DRAW, MODEL>(P, S, sid, lane, fw * 32 + fl, es, vb, emu, f_ilb, f_k, f_i0, f_j0, f_fast,
+                    handle_event<DRAW, MODEL, CW>(P, S, sid, lane, fw * 32 + fl, es, vb, emu, f_ilb, f_k, f_i0, f_j0, f_fast,
                                               a, jlo, jhi);
                 }
                 __syncthreads();
@@ -651,7 +651,7 @@ __device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float
         __syncthreads();
         if (L == 0) {
             double e = 0.0, ec = 0.0;
-            for (int q = 0; q < GF_CW; q++) { e += S.red[0][q]; ec += S.red[1][q]; }
+            for (int q = 0; q < CW; q++) { e += S.red[0][q]; ec += S.red[1][q]; }
             J.counts[tid] += e;
             J.countsCovered[tid] += ec;
         }
@@ -659,7 +659,7 @@ __device__ void crawl_item(const CrawlParams &P, CrawlSmem<DRAW> &S, const float
     }
 
     __syncthreads();
-    if (warp == 0) flush_records<DRAW>(P, S, lane);
+    if (warp == 0) flush_records<DRAW, CW>(P, S, lane);
     if (L == 0) {
         const Cursor &c = S.cur;
         const bool paused = c.ndraw != 0;
@@ -695,11 +695,11 @@ __device__ __forceinline__ int next_work_item(const CrawlParams &P, int *slot, i
     return *slot;
 }
 
-template <int DRAW, int MODEL>
-__global__ void __launch_bounds__(GF_WIN, DRAW ? 4 : 6) crawl_kernel(CrawlParams P)
+template <int DRAW, int MODEL, int CW>
+__global__ void __launch_bounds__(CW * 32, DRAW ? 16 / CW : 24 / CW) crawl_kernel(CrawlParams P)
 {
     extern __shared__ float s_tab[];
-    __shared__ CrawlSmem<DRAW> S;
+    __shared__ CrawlSmem<DRAW, CW> S;
     __shared__ int s_item;
     int loaded = -1;
     int it = P.next_item ? next_work_item(P, &s_item, 0) : (int)blockIdx.x;
@@ -721,7 +721,7 @@ __global__ void __launch_bounds__(GF_WIN, DRAW ? 4 : 6) crawl_kernel(CrawlParams
             loaded = job;
         }
         __syncthreads();
-        crawl_item<DRAW, MODEL>(P, S, s_tab, s_tab + S.job.m.nM, tid);
+        crawl_item<DRAW, MODEL, CW>(P, S, s_tab, s_tab + S.job.m.nM, tid);
     }
 }
 
@@ -944,18 +944,23 @@ static void fill_job(CrawlJob &J, const LaunchCrawl &L)
 }
 
 /* one launch of crawl_kernel: one CTA per stream (the hardware scheduler balances them) */
-template <int DRAW, int MODEL>
+template <int DRAW, int MODEL, int CW>
 static cudaError_t start_crawl(const CrawlParams &P, size_t smem, cudaStream_t s)
 {
     static bool attr_set = false;       /* the per-model tables may exceed the 48 KB default */
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(crawl_kernel<DRAW, MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        cudaError_t e = cudaFuncSetAttribute(crawl_kernel<DRAW, MODEL, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    crawl_kernel<DRAW, MODEL><<<P.nitems, GF_WIN, smem, s>>>(P);
+    crawl_kernel<DRAW, MODEL, CW><<<P.nitems, (CW * 32), smem, s>>>(P);
     return cudaSuccess;
 }
+
+cudaError_t dispatch_crawl(int draw, int model_type, int cw, bool persistent, const CrawlParams &P, size_t smem,
+                           cudaStream_t s);
+template <int DRAW, int MODEL, int CW>
+static cudaError_t start_crawl_persistent(const CrawlParams &P, size_t smem, cudaStream_t s);
 
 cudaError_t launch_crawl(const LaunchCrawl &L, int draw, cudaStream_t s)
 {
@@ -976,10 +981,7 @@ cudaError_t launch_crawl(const LaunchCrawl &L, int draw, cudaStream_t s)
     if (P.nitems <= 0) return cudaSuccess;
     const size_t smem = (size_t)(L.m.nm + L.m.nM) * sizeof(float);
     if (smem > 64 * 1024) return cudaErrorInvalidValue;
-    const bool disk = L.m.type == GF_MODEL_EXP_DISK;
-    cudaError_t e;
-    if (draw) e = disk ? start_crawl<1, GF_MODEL_EXP_DISK>(P, smem, s) : start_crawl<1, GF_MODEL_POWER_LAW_ELLIPSOID>(P, smem, s);
-    else e = disk ? start_crawl<0, GF_MODEL_EXP_DISK>(P, smem, s) : start_crawl<0, GF_MODEL_POWER_LAW_ELLIPSOID>(P, smem, s);
+    cudaError_t e = dispatch_crawl(draw, L.m.type, L.cw, false, P, smem, s);
     if (e != cudaSuccess) return e;
     count_launches(1);
     return cudaGetLastError();
@@ -1120,23 +1122,45 @@ cudaError_t launch_seed_streams(const uint32_t *seeds, int njobs, const uint32_t
     return cudaGetLastError();
 }
 
-template <int DRAW, int MODEL>
+template <int DRAW, int MODEL, int CW>
 static cudaError_t start_crawl_persistent(const CrawlParams &P, size_t smem, cudaStream_t s)
 {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(crawl_kernel<DRAW, MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        cudaError_t e = cudaFuncSetAttribute(crawl_kernel<DRAW, MODEL, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, crawl_kernel<DRAW, MODEL>, GF_WIN, smem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, crawl_kernel<DRAW, MODEL, CW>, (CW * 32), smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     int grid = sm_count() * per_sm;
     if (grid > P.nitems) grid = P.nitems;
-    crawl_kernel<DRAW, MODEL><<<grid, GF_WIN, smem, s>>>(P);
+    crawl_kernel<DRAW, MODEL, CW><<<grid, (CW * 32), smem, s>>>(P);
     return cudaSuccess;
+}
+
+/* the crawl instance for (pass, model kind, warps per stream); the integrate pass
+ * always runs 4 warps per stream (it has no sequential phase to shorten) */
+cudaError_t dispatch_crawl(int draw, int model_type, int cw, bool persistent, const CrawlParams &P, size_t smem,
+                           cudaStream_t s)
+{
+#define GF_GO(D, M, W) return persistent ? start_crawl_persistent<D, M, W>(P, smem, s) : start_crawl<D, M, W>(P, smem, s)
+    const bool disk = model_type == GF_MODEL_EXP_DISK;
+    if (!draw) {
+        if (disk) GF_GO(0, GF_MODEL_EXP_DISK, 4);
+        GF_GO(0, GF_MODEL_POWER_LAW_ELLIPSOID, 4);
+    }
+    if (disk) {
+        if (cw == 1) GF_GO(1, GF_MODEL_EXP_DISK, 1);
+        if (cw == 2) GF_GO(1, GF_MODEL_EXP_DISK, 2);
+        GF_GO(1, GF_MODEL_EXP_DISK, 4);
+    }
+    if (cw == 1) GF_GO(1, GF_MODEL_POWER_LAW_ELLIPSOID, 1);
+    if (cw == 2) GF_GO(1, GF_MODEL_POWER_LAW_ELLIPSOID, 2);
+    GF_GO(1, GF_MODEL_POWER_LAW_ELLIPSOID, 4);
+#undef GF_GO
 }
 
 cudaError_t launch_crawl_multi(const LaunchCrawlMulti &L, int draw, cudaStream_t s)
@@ -1158,9 +1182,7 @@ cudaError_t launch_crawl_multi(const LaunchCrawlMulti &L, int draw, cudaStream_t
     if (smem > 64 * 1024) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(L.counter, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
-    const bool disk = L.model_type == GF_MODEL_EXP_DISK;
-    if (draw) e = disk ? start_crawl_persistent<1, GF_MODEL_EXP_DISK>(P, smem, s) : start_crawl_persistent<1, GF_MODEL_POWER_LAW_ELLIPSOID>(P, smem, s);
-    else e = disk ? start_crawl_persistent<0, GF_MODEL_EXP_DISK>(P, smem, s) : start_crawl_persistent<0, GF_MODEL_POWER_LAW_ELLIPSOID>(P, smem, s);
+    e = dispatch_crawl(draw, L.model_type, L.cw, true, P, smem, s);
     if (e != cudaSuccess) return e;
     count_launches(1);
     return cudaGetLastError();

@@ -99,3 +99,32 @@ def test_multi_request_is_repeatable_and_chunking_is_transparent(lib):
         for k in runs[0]:
             np.testing.assert_array_equal(np.concatenate(runs[0][k], axis=-1), np.concatenate(other[k], axis=-1))
     ctx.close()
+
+
+def test_warps_per_stream_choice_does_not_change_rows(lib):
+    """The tuner picks 1, 2 or 4 warps per crawl stream for the batched draw; every
+    forced choice gives the same rows (the stars of a stream do not depend on how
+    many warps crawl it)."""
+    ws = requests(lib, n=4)
+    ctx = G.Context(0)
+    assert set(ctx.tuning().values()) == {0}
+    runs = []
+    for cw in (None, 1, 2, 4):
+        if cw is not None:
+            for kind in ctx.tuning():
+                ctx.set_tuning(kind, cw)
+        got = {}
+
+        def sink(j, model, rows):
+            got.setdefault((j, model), []).append(np.concatenate([rows["lb"].ravel(), rows["DM"].ravel(), rows["absmag"].ravel()]))
+        G.run_catalog_multi(ctx, ws, sink=sink)
+        if cw is None:
+            assert all(v in (1, 2, 4) for v in ctx.tuning().values())
+        runs.append(got)
+    for other in runs[1:]:
+        assert runs[0].keys() == other.keys()
+        for k in runs[0]:
+            np.testing.assert_array_equal(np.concatenate(runs[0][k]), np.concatenate(other[k]))
+    with pytest.raises(G.GalfastError):
+        ctx.set_tuning(1, 3)
+    ctx.close()
