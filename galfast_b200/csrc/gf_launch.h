@@ -135,6 +135,32 @@ cudaError_t launch_precision(const SkyModel &m, const SkyGeom &g, const float *D
                              double *hist64, unsigned long long *max_rel, double *sum_rel, unsigned long long *nbins,
                              cudaStream_t s);
 
+/* expected counts pixel by pixel (gf_integrate.cu) */
+struct IntegPlanHdr {
+    int32_t nd, nanchors, nslots, ok;      /* ok = 0: the plan did not fit its buffer */
+    int32_t off_slot, off_anc;             /* byte offsets of the slot distances and anchor slots */
+    int32_t max_anchors, max_slots;
+};
+struct IntegPlanDesc {
+    const float *Dtab;             /* D[im][iM], rows of nM_tab */
+    int32_t nm, nM, nM_tab;
+    int32_t max_anchors, max_slots;
+    unsigned char *plan;           /* integ_plan_bytes(nm, nM) bytes */
+};
+struct IntegPixParams {
+    const CrawlJob *jobs;          /* per request: model, geometry (pixels, extinction) */
+    const unsigned char *const *plans;   /* per request: plan of its grid, or null (request skipped) */
+    const int32_t *pix_off;        /* [njobs + 1] first flat pixel of each request */
+    int32_t njobs, total_pix;
+    double2 *pix_sum;              /* [total_pix] (expected, expected covered) */
+    int32_t off_lf, off_mr, off_q, warp_bytes;   /* per-warp shared-memory layout (integ_warp_bytes) */
+};
+size_t integ_plan_bytes(int nm, int nM, int *max_anchors, int *max_slots);
+cudaError_t launch_integ_plans(const IntegPlanDesc *desc_dev, int nplans, cudaStream_t s);
+size_t integ_warp_bytes(int nm_max, int nM_max, int slots_max, IntegPixParams *P);
+/* per-pixel sums into P.pix_sum, then per-request totals into tot[njobs] */
+cudaError_t launch_integrate_pixels(const IntegPixParams &P, int model_type, double2 *tot, cudaStream_t s);
+
 /* module kernels over the rows of many requests (row_slot: the request slot of each row) */
 struct MultiRows {
     const int32_t *row_slot;       /* [rows] */

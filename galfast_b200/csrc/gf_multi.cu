@@ -173,6 +173,10 @@ struct MultiWS {
     Grow<uint64_t> key, key_b;
     Grow<uint32_t> idx_a, idx_b, slot_a, slot_b;
     Grow<char> temp;
+    Grow<double2> pixsum, tot;              /* pixel-by-pixel integrate: per pixel, per request */
+    Grow<const unsigned char *> plans;
+    Grow<int32_t> pixoff;
+    Grow<gfk::IntegPlanDesc> pdesc;
     gf_table out;
     HostGrow<char> h_stage;              /* page-locked staging of uploads and downloads */
     MultiWS() { memset(&out, 0, sizeof(out)); }
@@ -433,33 +437,121 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
         if (!R[j].plain) integ.push_back(j);
     int32_t nitems = 0;
     if (!integ.empty()) GF_TRY(upload_items(integ, &nitems));
+    /* pixel-by-pixel integrate: anchor plans per magnitude grid (nm * nM is a
+     * multiple of 10 for every batched request) */
+    std::map<std::tuple<float, float, float, float, int, int>, unsigned char *> plans;
+    std::vector<double2> htot(njobs);
+    const bool pixel_integrate = pix_total < (int64_t)INT32_MAX;
+    if (pixel_integrate && !integ.empty()) {
+        std::vector<int32_t> off(njobs + 1);
+        for (int j = 0; j < njobs; j++) off[j] = (int32_t)R[j].pix_off;
+        off[njobs] = (int32_t)pix_total;
+        GF_TRY(ws.pixoff.need((size_t)njobs + 1));
+        GF_CUDA(cudaMemcpyAsync(ws.pixoff.p, off.data(), 4 * ((size_t)njobs + 1), cudaMemcpyHostToDevice, st));
+        GF_TRY(ws.pixsum.need((size_t)std::max<int64_t>(pix_total, 1)));
+        GF_TRY(ws.tot.need((size_t)njobs));
+        GF_TRY(ws.plans.need((size_t)njobs));
+    }
     for (int i = 0; i < nmod && !integ.empty(); i++) {
         for (int j = 0; j < njobs; j++) hj[j] = crawl_job(j, i);
         GF_CUDA(cudaMemcpyAsync(d_jobs, hj.data(), sizeof(CrawlJob) * (size_t)njobs, cudaMemcpyHostToDevice, st));
-        GF_CUDA(cudaMemsetAsync(d_counts, 0, 16 * nall, st));
-        gfk::LaunchCrawlMulti L;
-        memset(&L, 0, sizeof(L));
-        L.jobs = d_jobs; L.items = d_items; L.nitems = nitems; L.counter = d_counter;
-        L.model_type = R[integ[0]].hm[i].m.type;
-        L.max_tab = max_tab(i, integ);
-        L.jt = ctx->jt;
-        {
-            ProfScope ps(ctx, GF_PROF_INTEGRATE);
-            GF_CUDA(gfk::launch_crawl_multi(L, 0, st));
-        }
-        GF_TRY(ws.h_stage.need(16 * nall));
-        GF_CUDA(cudaMemcpyAsync(ws.h_stage.p, d_counts, 16 * nall, cudaMemcpyDeviceToHost, st));
-        GF_CUDA(cudaStreamSynchronize(st));
-        memcpy(hc.data(), ws.h_stage.p, 16 * nall);
-        for (int j : integ) {
-            double e = 0, ec = 0;
-            for (int t = 0; t < N; t++) {
-                e += hc[(size_t)j * N + t];
-                ec += hc[nall + (size_t)j * N + t];
+        bool done = false;
+        if (pixel_integrate) {
+            /* plans of the grids not seen yet */
+            std::vector<gfk::IntegPlanDesc> nd;
+            std::vector<unsigned char *> job_plan(njobs, nullptr);
+            for (int j : integ) {
+                const SkyModel &m = R[j].hm[i].m;
+                auto key = std::make_tuple(m.m0, m.dm, m.M1, m.dM, m.nM, m.nm);
+                auto it = plans.find(key);
+                if (it == plans.end()) {
+                    gfk::IntegPlanDesc d;
+                    memset(&d, 0, sizeof(d));
+                    const size_t bytes = gfk::integ_plan_bytes(m.nm, m.nM, &d.max_anchors, &d.max_slots);
+                    GF_TRY(pool.alloc(&d.plan, bytes));
+                    d.Dtab = hj[j].Dtab;
+                    d.nm = m.nm; d.nM = m.nM; d.nM_tab = m.nM;
+                    nd.push_back(d);
+                    it = plans.insert({key, d.plan}).first;
+                }
+                job_plan[j] = it->second;
             }
-            S[j].expected[i] = e;
-            S[j].expected_covered[i] = ec;
+            if (!nd.empty()) {
+                GF_TRY(ws.pdesc.need(nd.size()));
+                GF_CUDA(cudaMemcpyAsync(ws.pdesc.p, nd.data(), sizeof(gfk::IntegPlanDesc) * nd.size(), cudaMemcpyHostToDevice, st));
+                GF_CUDA(gfk::launch_integ_plans(ws.pdesc.p, (int)nd.size(), st));
+            }
+            /* every plan's header: slot count, and whether it fitted */
+            std::vector<unsigned char *> uniq;
+            for (auto &kv : plans) uniq.push_back(kv.second);
+            GF_TRY(ws.h_stage.need(sizeof(gfk::IntegPlanHdr) * uniq.size()));
+            gfk::IntegPlanHdr *hh = (gfk::IntegPlanHdr *)ws.h_stage.p;
+            for (size_t q = 0; q < uniq.size(); q++)
+                GF_CUDA(cudaMemcpyAsync(hh + q, uniq[q], sizeof(gfk::IntegPlanHdr), cudaMemcpyDeviceToHost, st));
+            GF_CUDA(cudaStreamSynchronize(st));
+            bool ok = true;
+            int slots_max = 1, nm_max = 1, nM_max = 1;
+            for (size_t q = 0; q < uniq.size(); q++) {
+                ok = ok && hh[q].ok;
+                slots_max = std::max(slots_max, hh[q].nslots);
+            }
+            for (int j : integ) {
+                nm_max = std::max(nm_max, R[j].hm[i].m.nm);
+                nM_max = std::max(nM_max, R[j].hm[i].m.nM);
+            }
+            gfk::IntegPixParams P;
+            memset(&P, 0, sizeof(P));
+            if (ok && gfk::integ_warp_bytes(nm_max, nM_max, slots_max, &P) <= 200 * 1024) {
+                GF_CUDA(cudaMemcpyAsync(ws.plans.p, job_plan.data(), sizeof(unsigned char *) * (size_t)njobs, cudaMemcpyHostToDevice, st));
+                P.jobs = d_jobs;
+                P.plans = ws.plans.p;
+                P.pix_off = ws.pixoff.p;
+                P.njobs = njobs;
+                P.total_pix = (int32_t)pix_total;
+                P.pix_sum = ws.pixsum.p;
+                {
+                    ProfScope ps(ctx, GF_PROF_INTEGRATE);
+                    GF_CUDA(gfk::launch_integrate_pixels(P, R[integ[0]].hm[i].m.type, ws.tot.p, st));
+                }
+                GF_CUDA(cudaMemcpyAsync(htot.data(), ws.tot.p, sizeof(double2) * (size_t)njobs, cudaMemcpyDeviceToHost, st));
+                GF_CUDA(cudaStreamSynchronize(st));
+                for (int j : integ) {
+                    S[j].expected[i] = htot[j].x;
+                    S[j].expected_covered[i] = htot[j].y;
+                }
+                done = true;
+            }
+        }
+        if (!done) {
+            /* the stream crawl (a grid whose plan does not fit) */
+            GF_CUDA(cudaMemsetAsync(d_counts, 0, 16 * nall, st));
+            gfk::LaunchCrawlMulti L;
+            memset(&L, 0, sizeof(L));
+            L.jobs = d_jobs; L.items = d_items; L.nitems = nitems; L.counter = d_counter;
+            L.model_type = R[integ[0]].hm[i].m.type;
+            L.max_tab = max_tab(i, integ);
+            L.jt = ctx->jt;
+            {
+                ProfScope ps(ctx, GF_PROF_INTEGRATE);
+                GF_CUDA(gfk::launch_crawl_multi(L, 0, st));
+            }
+            GF_TRY(ws.h_stage.need(16 * nall));
+            GF_CUDA(cudaMemcpyAsync(ws.h_stage.p, d_counts, 16 * nall, cudaMemcpyDeviceToHost, st));
+            GF_CUDA(cudaStreamSynchronize(st));
+            memcpy(hc.data(), ws.h_stage.p, 16 * nall);
+            for (int j : integ) {
+                double e = 0, ec = 0;
+                for (int t = 0; t < N; t++) {
+                    e += hc[(size_t)j * N + t];
+                    ec += hc[nall + (size_t)j * N + t];
+                }
+                S[j].expected[i] = e;
+                S[j].expected_covered[i] = ec;
+            }
+        }
+        for (int j : integ) {
             /* room for the Poisson spread of the model's stars in one batch */
+            const double e = S[j].expected[i];
             if (e + 8.0 * sqrt(e) + 1024.0 >= (double)jobs[j].capacity) R[j].plain = true;
         }
     }
