@@ -228,7 +228,7 @@ class Context:
         return ms.value
 
     def tuning(self):
-        """{model kind: warps per stream of the batched draw} (0 = not tuned yet)."""
+        """{model kind: warps per CTA of the batched draw} (0 = not tuned yet)."""
         out = {}
         for k in (A.GF_MODEL_EXP_DISK, A.GF_MODEL_POWER_LAW_ELLIPSOID):
             w = C.c_int32()

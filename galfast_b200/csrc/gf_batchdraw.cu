@@ -1,0 +1,529 @@
+/*
+ * gf_batchdraw.cu -- the Poisson draw pass of many requests (the batched form).
+ *
+ * The bins, uniforms and star draws are exactly those of the reference's
+ * draw pass (skygenGPU<T>::kernel with draw = 1, skygen.cu.h:469-618, and
+ * draw_stars, :366-457): stream t of a request crawls blocks t, t + N, t + 2N, ...
+ * of 10 consecutive bins (N streams), takes one uniform per uncut bin, and a
+ * bin with stars consumes the Poisson sampler's uniforms and 2 or 4 per star.
+ * The arrangement is this library's, for requests whose nm * nM is a multiple
+ * of 10 (so every pixel's blocks start at local indices 0, 10, 20, ...):
+ *
+ *   slot densities  (warp per pixel) the model density at each slot distance of
+ *                   the request's anchor plan along the pixel's direction: the
+ *                   anchor quantity that depends on the pixel.  The anchor of any
+ *                   bin is then a table lookup: block-start anchors through the
+ *                   plan's per-block slot, diagonal starts through its
+ *                   per-diagonal slot.
+ *   draw            one warp per stream, lane L on block r + L of the stream's
+ *                   window of 32 blocks.  Each lane computes mu of its 10 bins in
+ *                   registers, jumps to the stream state of its first uncut bin
+ *                   (the MWC stream is a Lehmer generator modulo its safe prime;
+ *                   assuming no earlier bin of the window has stars) and walks its
+ *                   bins with plain MWC steps.  The first lane whose bin has stars
+ *                   runs the reference's Poisson sampler and the star uniforms by
+ *                   itself, records the bin (an event: its k and the stream state
+ *                   at its first star), and the lanes after it move their start
+ *                   states by a^(used - 1) and walk again.  Nothing else waits.
+ *   expand          (thread per event) the star records of each event, regenerated
+ *                   from its stream state, at offsets from a scan over k.
+ * The stream states left behind are the reference's, for the modules that
+ * continue the streams (Bond2010).
+ */
+#include "gf_crawl.cuh"
+#include "gf_launch.h"
+#include "gf_rng.h"
+#include <cub/cub.cuh>
+
+namespace gfk {
+
+namespace {
+
+#define BD_FULL 0xffffffffu
+#define GF_EVBUF 32                /* events staged in shared memory per warp */
+
+__device__ __forceinline__ uint64_t bd_shfl64(uint64_t v, int src)
+{
+    const uint32_t lo = __shfl_sync(BD_FULL, (uint32_t)v, src);
+    const uint32_t hi = __shfl_sync(BD_FULL, (uint32_t)(v >> 32), src);
+    return ((uint64_t)hi << 32) | lo;
+}
+
+__device__ __forceinline__ int bd_incl_scan(int v, int lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(BD_FULL, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+__device__ __forceinline__ float bd_mwc_step(uint64_t &v, uint32_t a)
+{
+    const uint64_t t = (uint64_t)a * (uint32_t)v + (v >> 32);
+    v = t;
+    return GF_MWC_SCALE * (float)(uint32_t)t;
+}
+
+/* v * a^n mod p for 0 <= n < 2048 from the stream's scaled powers */
+__device__ __forceinline__ uint64_t bd_jump(uint64_t v, int n, const uint64_t *lo, const uint64_t *hi, uint32_t a, uint64_t p)
+{
+    const uint64_t w = gfr::mwc_mulmod_scaled(__ldg(lo + (n & 31)), v, a, p);
+    return gfr::mwc_mulmod_scaled(__ldg(hi + (n >> 5)), w, a, p);
+}
+
+/* scaled a^n for any n >= 0 */
+__device__ uint64_t bd_power(uint32_t n, const uint64_t *lo, const uint64_t *hi, uint32_t a, uint64_t p)
+{
+    uint64_t ms = __ldg(lo);                                  /* scaled a^0 */
+    if (n >= 2048) {
+        const uint64_t m2047 = gfr::mwc_mulmod_scaled(__ldg(lo + 31), __ldg(hi + 63), a, p);
+        while (n >= 2047) { ms = gfr::mwc_mulmod_scaled(ms, m2047, a, p); n -= 2047; }
+    }
+    return gfr::mwc_mulmod_scaled(ms, gfr::mwc_mulmod_scaled(__ldg(lo + (n & 31)), __ldg(hi + (n >> 5)), a, p), a, p);
+}
+
+/* exp(-mu) >= 1 - mu: bins that surely draw no star, without exp */
+__device__ __forceinline__ bool bd_surely_empty(float u, float mu)
+{
+    return u <= (1.0f - mu) - 3.0e-7f;
+}
+
+/* the sampler's exact test (mu > 10 takes the branch that never compares with exp(-mu)) */
+__device__ __forceinline__ bool bd_has_stars(float u, float mu)
+{
+    return mu > 10.f || u > gfm::expf_(-mu);
+}
+
+template <class T>
+__device__ __forceinline__ const T *plan_at(const unsigned char *plan, int off)
+{
+    return (const T *)(plan + off);
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(256) slot_density_kernel(SlotDensityParams P)
+{
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < P.total_pix; p += nwarps) {
+        int lo = 0, hi = P.njobs;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (P.pix_off[mid] <= p) lo = mid; else hi = mid;
+        }
+        const int job = P.job_list[lo];
+        const int ilb = p - P.pix_off[lo];
+        const CrawlJob &J = P.jobs[job];
+        const unsigned char *plan = P.plans[job];
+        const IntegPlanHdr *h = (const IntegPlanHdr *)plan;
+        const int nslots = h->nslots;
+        const float *slotD = plan_at<float>(plan, h->off_slot);
+        const gf_pencil_beam pix = J.g.pixels[ilb];
+        float *row = P.ms[job] + (size_t)ilb * nslots;
+        for (int s = lane; s < nslots; s += 32) {
+            const float D = slotD[s];
+            const float px = D * pix.cl * pix.cb;
+            const float py = D * pix.sl * pix.cb;
+            const float pz = D * pix.sb;
+            row[s] = gfc::model_rho<MODEL>(J.m, px, py, pz);
+        }
+    }
+}
+
+/* A bin with stars, on the lane that found it: the reference's Poisson sampler
+ * from the bin's stream state wb, then the stars' uniforms (draw_stars: x, y,
+ * and M, m unless x^2 + y^2 > 2), counted to move the stream on; the event is
+ * staged for the expansion.  Returns 1 (and sets the error flag) for an
+ * infinite expected count. */
+__device__ __noinline__ int draw_event(const BatchDrawParams &P, EventRecord *evb, int *nev, uint32_t a, const uint64_t *jlo,
+                                       const uint64_t *jhi, uint64_t pmod, uint64_t wb, float mu, int sid, int pix, int i0,
+                                       int j0, int es, int x, int y, const gf_pencil_beam *pixels, int &nst, uint64_t &vnew,
+                                       uint64_t &mult)
+{
+    int i = i0, j = j0;
+    for (int s = 1; s <= es; s++) gfc::step_in_pixel(i, j, x, y);
+    if (!(mu < 3.0e38f)) {
+        /* an infinite expected count would never leave the sampler's gamma loop */
+        atomicOr(P.err, 1ull);
+        return 1;
+    }
+    gfr::Mwc r;
+    r.a = a;
+    r.set_v(wb);
+    r.used = 0;
+    const int k = (int)r.poisson(mu);
+    const uint64_t v_star = r.v();
+    if (k > 0) {
+        const gf_pencil_beam pp = pixels[pix];
+        for (int n = 0; n < k; n++) {
+            const float u0 = r.uniform();
+            const float u1 = r.uniform();
+            float xx = pp.X, yy = pp.Y;
+            xx += pp.dx * (u0 - 0.5f);
+            yy += pp.dx * (u1 - 0.5f);
+            if (!(xx * xx + yy * yy > 2.f)) {
+                r.uniform();
+                r.uniform();
+            }
+        }
+        EventRecord e;
+        e.stream = sid;
+        e.ilb = pix;
+        e.im = (int16_t)i;
+        e.iM = (int16_t)j;
+        e.k = k;
+        e.nstars = nst;
+        e.pad = 0;
+        e.v_star = v_star;
+        const int q = *nev;
+        if (q < GF_EVBUF) {
+            evb[q] = e;
+            *nev = q + 1;
+        } else {
+            const unsigned long long sl = atomicAdd(P.ev_count, 1ull);
+            if (sl < (unsigned long long)P.ev_capacity) P.ev[sl] = e;
+        }
+        nst += k;
+    }
+    vnew = r.v();
+    mult = bd_power(r.used - 1, jlo, jhi, a, pmod);
+    return 0;
+}
+
+/* write the warp's staged events to the global list (all lanes) */
+__device__ __forceinline__ void flush_events(const BatchDrawParams &P, EventRecord *evb, int *nev, int lane)
+{
+    __syncwarp();
+    const int n = *nev;
+    if (n == 0) return;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(P.ev_count, (unsigned long long)n);
+    base = __shfl_sync(BD_FULL, base, 0);
+    for (int q = lane; q < n; q += 32)
+        if (base + q < (unsigned long long)P.ev_capacity) P.ev[base + q] = evb[q];
+    __syncwarp();
+    if (lane == 0) *nev = 0;
+    __syncwarp();
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(256) batch_draw_kernel(BatchDrawParams P)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    unsigned char *mine = smem + (size_t)wib * P.warp_bytes;
+    SkyModel &m = *(SkyModel *)mine;
+    float *LFM = (float *)(mine + P.off_tab);
+    EventRecord *evb = (EventRecord *)(mine + P.off_ev);
+    int *nev = (int *)(evb + GF_EVBUF);
+    if (lane == 0) *nev = 0;
+    __syncwarp();
+
+    int loaded = -1;
+    const float *MMr = nullptr;
+    const uint32_t *blk = nullptr;
+    const uint16_t *bslot = nullptr, *dslot = nullptr;
+    const float *slotD = nullptr, *msbase = nullptr;
+    const gf_pencil_beam *pixels = nullptr;
+    const float *ammin = nullptr;
+    int nslots = 0, Bp = 1, npix = 0, x = 1, y = 1, N = 1;
+    float norm = 0.f, m1 = 0.f, kdm = 0.f, dmin = 0.f, dmax = 0.f;
+    bool dlim = false;
+    const float INF = __int_as_float(0x7f800000);
+
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = (int)atomicAdd(P.next_item, 1u);
+        it = __shfl_sync(BD_FULL, it, 0);
+        if (it >= P.nitems) break;
+        const uint32_t wi = P.items[it];
+        const int job = (int)(wi >> 16), t = (int)(wi & 0xffffu);
+        const CrawlJob &J = P.jobs[job];
+        if (job != loaded) {
+            __syncwarp();
+            const uint32_t *src = (const uint32_t *)&J.m;
+            for (int w = lane; w < (int)(sizeof(SkyModel) / 4); w += 32) ((uint32_t *)&m)[w] = src[w];
+            __syncwarp();
+            x = m.nm; y = m.nM; N = m.nthreads;
+            MMr = LFM + y;
+            for (int q = lane; q < y; q += 32) LFM[q] = gfc::lf_sample(m, m.lf, m.M1 - (float)q * m.dM);
+            for (int q = lane; q < x; q += 32) ((float *)MMr)[q] = m.m0 + m.dm * (float)q;
+            const unsigned char *plan = P.plans[job];
+            const IntegPlanHdr *h = (const IntegPlanHdr *)plan;
+            nslots = h->nslots;
+            Bp = h->nblocks;
+            slotD = plan_at<float>(plan, h->off_slot);
+            blk = plan_at<uint32_t>(plan, h->off_blk);
+            bslot = plan_at<uint16_t>(plan, h->off_bslot);
+            dslot = plan_at<uint16_t>(plan, h->off_dslot);
+            msbase = P.ms[job];
+            pixels = J.g.pixels;
+            npix = J.g.npixels;
+            ammin = (J.g.ext_kind != GF_EXT_NONE) ? J.g.ammin : nullptr;
+            norm = m.norm;
+            m1 = m.m1;
+            kdm = m.dm;                      /* K = ((dA * POGSON) * dm) * dM */
+            dmin = m.dmin;
+            dmax = m.dmax;
+            dlim = m.dmin != 0.f || m.dmax != 0.f;
+            __syncwarp();
+            loaded = job;
+        }
+        const float dM = m.dM;
+        const int NS = J.rng_nstreams;
+        uint32_t *rng = J.rng;
+        const uint32_t a = rng[t];
+        uint64_t v = ((uint64_t)rng[NS + t] << 32) | rng[2 * NS + t];
+        const uint64_t *jlo = P.jt.lo + (size_t)t * 32, *jhi = P.jt.hi + (size_t)t * GF_JUMP_HI;
+        const uint64_t pmod = ((uint64_t)a << 32) - 1;
+        const int sid = (job << 16) | t;
+        /* block r of the stream is the stream's (t + r N)-th global block */
+        const long long g0 = (long long)t + (long long)N * lane;
+        int pix = (int)(g0 / Bp), lb = (int)(g0 - (long long)pix * Bp);
+        const long long stepw = 32ll * N;
+        const int QW = (int)(stepw / Bp), RW = (int)(stepw - (long long)QW * Bp);
+        int nst = 0;
+        bool stop = false;
+        for (;;) {
+            const bool valid = pix < npix;
+            if (!__any_sync(BD_FULL, valid)) break;
+            float mu[GF_BLOCK];
+            uint32_t live = 0;
+            int i0 = 0, j0 = 0;
+            if (valid) {
+                const uint32_t bij = __ldg(blk + lb);
+                i0 = (int)(bij & 0xffffu);
+                j0 = (int)(bij >> 16);
+                int slot = __ldg(bslot + lb);
+                const gf_pencil_beam *pp = pixels + pix;
+                const float Am = ammin ? __ldg(ammin + pp->extIdx) : 0.f;
+                const float K = pp->dA * GF_POGSON * kdm * dM;
+                const float *msr = msbase + (size_t)pix * nslots;
+                float ms = msr[slot], D = __ldg(slotD + slot);
+                float D3 = D * D * D;
+                float Ae = (dlim && (dmin > D || dmax <= D)) ? INF : Am;
+                int i = i0, j = j0;
+#pragma unroll
+                for (int s = 0; s < GF_BLOCK; s++) {
+                    if (s > 0 && gfc::step_in_pixel(i, j, x, y)) {
+                        slot = __ldg(dslot + i + j);
+                        ms = msr[slot];
+                        D = __ldg(slotD + slot);
+                        D3 = D * D * D;
+                        Ae = (dlim && (dmin > D || dmax <= D)) ? INF : Am;
+                    }
+                    float r = LFM[j] * ms;
+                    r *= norm;
+                    r *= D3;
+                    r *= K;
+                    mu[s] = r;
+                    live |= (MMr[i] + Ae > m1) ? 0u : (1u << s);
+                }
+            } else {
+#pragma unroll
+                for (int s = 0; s < GF_BLOCK; s++) mu[s] = 0.f;
+            }
+            /* each lane's start state if no earlier bin of the window has stars */
+            const int cnt = __popc(live);
+            const int inc = bd_incl_scan(cnt, lane);
+            uint64_t wst = bd_jump(v, inc - cnt, jlo, jhi, a, pmod);
+            uint32_t act = live;
+            for (;;) {
+                int ev_s = -1;
+                uint64_t w = wst, wb_ev = 0;
+                float mu_ev = 0.f;
+                uint32_t todo = act;
+                for (;;) {
+                    /* the next bin that is not surely empty, then the exact test once */
+                    int c = -1;
+                    uint64_t cwb = 0;
+                    float cu = 0.f, cmu = 0.f;
+#pragma unroll
+                    for (int s = 0; s < GF_BLOCK; s++) {
+                        if (c < 0 && ((todo >> s) & 1u)) {
+                            const uint64_t wb = w;
+                            const float u = bd_mwc_step(w, a);
+                            if (!bd_surely_empty(u, mu[s])) { c = s; cwb = wb; cu = u; cmu = mu[s]; }
+                        }
+                    }
+                    if (c < 0) break;
+                    if (bd_has_stars(cu, cmu)) {
+                        ev_s = c;
+                        wb_ev = cwb;
+                        mu_ev = cmu;
+                        break;
+                    }
+                    todo &= ~((2u << c) - 1u);
+                }
+                const unsigned evm = __ballot_sync(BD_FULL, ev_s >= 0);
+                if (!evm) {
+                    v = bd_shfl64(w, 31);
+                    break;
+                }
+                const int fl = __ffs(evm) - 1;
+                uint64_t vnew = 0, mult = 0;
+                int flag = 0;
+                if (lane == fl)
+                    flag = draw_event(P, evb, nev, a, jlo, jhi, pmod, wb_ev, mu_ev, sid, pix, i0, j0, ev_s, x, y,
+                                      pixels, nst, vnew, mult);
+                flag = __shfl_sync(BD_FULL, flag, fl);
+                if (flag) {
+                    stop = true;
+                    break;
+                }
+                vnew = bd_shfl64(vnew, fl);
+                mult = bd_shfl64(mult, fl);
+                nst = __shfl_sync(BD_FULL, nst, fl);
+                /* continue after the bin with stars */
+                if (lane < fl) {
+                    act = 0u;
+                } else if (lane == fl) {
+                    const int lo = ev_s + 1;
+                    act = lo >= GF_BLOCK ? 0u : ((act >> lo) << lo);
+                    wst = vnew;
+                } else {
+                    wst = gfr::mwc_mulmod_scaled(mult, wst, a, pmod);
+                }
+            }
+            if (stop) break;
+            __syncwarp();
+            if (*nev >= GF_EVBUF / 2) flush_events(P, evb, nev, lane);
+            pix += QW;
+            lb += RW;
+            if (lb >= Bp) { lb -= Bp; pix++; }
+        }
+        if (!stop && lane == 0) {
+            rng[NS + t] = (uint32_t)(v >> 32);
+            rng[2 * NS + t] = (uint32_t)v;
+        }
+    }
+    flush_events(P, evb, nev, lane);
+}
+
+__global__ void event_k_kernel(const EventRecord *ev, int64_t n, int64_t *k64)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        k64[e] = ev[e].k;
+}
+
+/* the star records of each event (draw_stars' uniforms, skygen.cu.h:366-457) */
+__global__ void __launch_bounds__(256) expand_kernel(const EventRecord *ev, int64_t n, const int64_t *off, const int64_t *k64,
+                                                     const CrawlJob *jobs, StarRecord *rec, int64_t cap, int64_t *total)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const EventRecord E = ev[e];
+        const int job = E.stream >> 16, t = E.stream & 0xffff;
+        const CrawlJob &J = jobs[job];
+        const gf_pencil_beam pix = J.g.pixels[E.ilb];
+        gfr::Mwc r;
+        r.a = J.rng[t];
+        r.set_v(E.v_star);
+        r.used = 0;
+        const int64_t o = off[e];
+        for (int q = 0; q < E.k; q++) {
+            StarRecord s;
+            s.stream = E.stream;
+            s.ilb = E.ilb + J.pix_base;
+            s.im = E.im;
+            s.iM = E.iM;
+            s.seq = E.nstars + q;
+            s.u[0] = r.uniform();
+            s.u[1] = r.uniform();
+            float xx = pix.X, yy = pix.Y;
+            xx += pix.dx * (s.u[0] - 0.5f);
+            yy += pix.dx * (s.u[1] - 0.5f);
+            if (xx * xx + yy * yy > 2.f) {
+                s.u[2] = s.u[3] = 0.f;
+            } else {
+                s.u[2] = r.uniform();
+                s.u[3] = r.uniform();
+            }
+            if (o + q < cap) rec[o + q] = s;
+        }
+        if (e == n - 1) *total = o + k64[e];
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_slot_density(const SlotDensityParams &P, int model_type, cudaStream_t s)
+{
+    if (P.total_pix <= 0) return cudaSuccess;
+    const long long need = ((long long)P.total_pix + 7) / 8;
+    const int blocks = (int)std::min<long long>(need, (long long)sm_count() * 8);
+    if (model_type == GF_MODEL_EXP_DISK)
+        slot_density_kernel<GF_MODEL_EXP_DISK><<<blocks, 256, 0, s>>>(P);
+    else
+        slot_density_kernel<GF_MODEL_POWER_LAW_ELLIPSOID><<<blocks, 256, 0, s>>>(P);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+size_t batch_draw_warp_bytes(int max_tab, BatchDrawParams *P)
+{
+    size_t off = (sizeof(SkyModel) + 15) & ~(size_t)15;
+    P->off_tab = (int32_t)off;
+    off += ((size_t)4 * max_tab + 15) & ~(size_t)15;
+    P->off_ev = (int32_t)off;
+    off += sizeof(EventRecord) * GF_EVBUF + 16;
+    off = (off + 15) & ~(size_t)15;
+    P->warp_bytes = (int32_t)off;
+    return off;
+}
+
+cudaError_t launch_batch_draw(const BatchDrawParams &P, int model_type, int warps_per_cta, cudaStream_t s)
+{
+    if (P.nitems <= 0) return cudaSuccess;
+    if (warps_per_cta < 1 || warps_per_cta > 8) warps_per_cta = 4;
+    const size_t smem = (size_t)warps_per_cta * P.warp_bytes;
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    const int threads = 32 * warps_per_cta;
+    cudaError_t e = cudaMemsetAsync(P.next_item, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    if (model_type == GF_MODEL_EXP_DISK) {
+        e = cudaFuncSetAttribute(batch_draw_kernel<GF_MODEL_EXP_DISK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_draw_kernel<GF_MODEL_EXP_DISK>, threads, smem);
+    } else {
+        e = cudaFuncSetAttribute(batch_draw_kernel<GF_MODEL_POWER_LAW_ELLIPSOID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_draw_kernel<GF_MODEL_POWER_LAW_ELLIPSOID>, threads, smem);
+    }
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    const long long want = ((long long)P.nitems + warps_per_cta - 1) / warps_per_cta;
+    const int blocks = (int)std::min<long long>(want, (long long)sm_count() * per_sm);
+    if (model_type == GF_MODEL_EXP_DISK)
+        batch_draw_kernel<GF_MODEL_EXP_DISK><<<blocks, threads, smem, s>>>(P);
+    else
+        batch_draw_kernel<GF_MODEL_POWER_LAW_ELLIPSOID><<<blocks, threads, smem, s>>>(P);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t expand_temp_bytes(int64_t nev, size_t *bytes)
+{
+    *bytes = 0;
+    if (nev <= 0) return cudaSuccess;
+    return cub::DeviceScan::ExclusiveSum(nullptr, *bytes, (const int64_t *)nullptr, (int64_t *)nullptr, (int)nev);
+}
+
+cudaError_t launch_expand_events(const EventRecord *ev, int64_t nev, const CrawlJob *jobs, int64_t *k64, int64_t *off64,
+                                 void *temp, size_t temp_bytes, StarRecord *rec, int64_t rec_capacity, int64_t *total,
+                                 cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(total, 0, sizeof(int64_t), s);
+    if (e != cudaSuccess || nev <= 0) return e;
+    const int blocks = (int)std::min<long long>((nev + 255) / 256, (long long)sm_count() * 16);
+    event_k_kernel<<<blocks, 256, 0, s>>>(ev, nev, k64);
+    size_t tb = temp_bytes;
+    e = cub::DeviceScan::ExclusiveSum(temp, tb, k64, off64, (int)nev, s);
+    if (e != cudaSuccess) return e;
+    expand_kernel<<<blocks, 256, 0, s>>>(ev, nev, off64, k64, jobs, rec, rec_capacity, total);
+    count_launches(3);
+    return cudaGetLastError();
+}
+
+}  // namespace gfk

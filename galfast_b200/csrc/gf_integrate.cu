@@ -61,7 +61,7 @@ __device__ __forceinline__ int first_block_start(long long k0)
 #define GF_PLAN_REMEMBER 8          /* distinct distances remembered per diagonal */
 
 /* distinct anchor distances of diagonal d, in order of first appearance; calls
- * emit(anchor ordinal, slot ordinal on the diagonal, D) for every anchor */
+ * emit(anchor ordinal, slot ordinal on the diagonal, D, local index, i, j) for every anchor */
 template <class F>
 __device__ __forceinline__ int diag_anchors(const float *Dtab, int nM_tab, int d, int x, int y, F emit)
 {
@@ -81,7 +81,7 @@ __device__ __forceinline__ int diag_anchors(const float *Dtab, int nM_tab, int d
             s = nslot++;
             if (nseen < GF_PLAN_REMEMBER) seen[nseen++] = b;
         }
-        emit(q, s, D);
+        emit(q, s, D, k0 + t, i, j);
     }
     return nslot;
 }
@@ -108,32 +108,68 @@ __device__ __forceinline__ void scan2(int &a, int &b, int *sa, int *sb, int &tot
     __syncthreads();
 }
 
+/* byte layout of a plan (the header's offsets) */
+__host__ __device__ inline void plan_layout(int nm, int nM, int max_anchors, int max_slots, IntegPlanHdr &h)
+{
+    const long long nd = (long long)nm + nM - 1, nb = (long long)nm * nM / GF_BLOCK;
+    long long off = (sizeof(IntegPlanHdr) + 15) & ~15ll;
+    off += (8 * nd + 15) & ~15ll;
+    h.off_slot = (int32_t)off;
+    off += (4 * (long long)max_slots + 15) & ~15ll;
+    h.off_anc = (int32_t)off;
+    off += (2 * (long long)max_anchors + 15) & ~15ll;
+    h.off_blk = (int32_t)off;
+    off += (4 * nb + 15) & ~15ll;
+    h.off_bslot = (int32_t)off;
+    off += (2 * nb + 15) & ~15ll;
+    h.off_dslot = (int32_t)off;
+    off += (2 * nd + 15) & ~15ll;
+    h.nd = (int32_t)nd;
+    h.nblocks = (int32_t)nb;
+    h.max_anchors = max_anchors;
+    h.max_slots = max_slots;
+    h.bytes = (int32_t)off;
+    h.nanchors = 0;
+    h.nslots = 0;
+    h.ok = 0;
+    h.pad[0] = h.pad[1] = h.pad[2] = 0;
+}
+
 __global__ void __launch_bounds__(1024) plan_kernel(const IntegPlanDesc *desc)
 {
     __shared__ int sa[1024], sb[1024];
     const IntegPlanDesc P = desc[blockIdx.x];
     const int x = P.nm, y = P.nM, nd = x + y - 1;
     unsigned char *plan = P.plan;
-    const int off_slot = 32 + ((8 * nd + 15) & ~15);
-    const int off_anc = off_slot + ((4 * P.max_slots + 15) & ~15);
-    int2 *diag = (int2 *)(plan + 32);
-    float *slotD = (float *)(plan + off_slot);
-    uint16_t *anc = (uint16_t *)(plan + off_anc);
+    IntegPlanHdr h;
+    plan_layout(x, y, P.max_anchors, P.max_slots, h);
+    int2 *diag = (int2 *)(plan + ((sizeof(IntegPlanHdr) + 15) & ~15));
+    float *slotD = (float *)(plan + h.off_slot);
+    uint16_t *anc = (uint16_t *)(plan + h.off_anc);
+    uint32_t *blk = (uint32_t *)(plan + h.off_blk);
+    uint16_t *bslot = (uint16_t *)(plan + h.off_bslot);
+    uint16_t *dslot = (uint16_t *)(plan + h.off_dslot);
     int base_a = 0, base_s = 0;
     bool overflow = false;
     for (int c0 = 0; c0 < nd; c0 += blockDim.x) {
         const int d = c0 + threadIdx.x;
         int na = 0, ns = 0;
-        if (d < nd) ns = diag_anchors(P.Dtab, P.nM_tab, d, x, y, [&](int q, int, float) { na = q + 1; });
+        if (d < nd) ns = diag_anchors(P.Dtab, P.nM_tab, d, x, y, [&](int q, int, float, long long, int, int) { na = q + 1; });
         int ea = na, es = ns, ta = 0, ts = 0;
         scan2(ea, es, sa, sb, ta, ts);
         const int abase = base_a + ea, sbase = base_s + es;
         if (d < nd) {
             diag[d] = make_int2(abase, first_block_start(diag_start(d, x, y)));
             if (abase + na <= P.max_anchors && sbase + ns <= P.max_slots && sbase + ns <= 65536)
-                diag_anchors(P.Dtab, P.nM_tab, d, x, y, [&](int q, int s, float D) {
-                    anc[abase + q] = (uint16_t)(sbase + s);
-                    slotD[sbase + s] = D;
+                diag_anchors(P.Dtab, P.nM_tab, d, x, y, [&](int q, int s, float D, long long k, int i, int j) {
+                    const int slot = sbase + s;
+                    anc[abase + q] = (uint16_t)slot;
+                    slotD[slot] = D;
+                    if (q == 0) dslot[d] = (uint16_t)slot;
+                    if (k % GF_BLOCK == 0) {
+                        blk[k / GF_BLOCK] = (uint32_t)i | ((uint32_t)j << 16);
+                        bslot[k / GF_BLOCK] = (uint16_t)slot;
+                    }
                 });
             else
                 overflow = true;
@@ -143,15 +179,9 @@ __global__ void __launch_bounds__(1024) plan_kernel(const IntegPlanDesc *desc)
     }
     overflow = __syncthreads_or(overflow);
     if (threadIdx.x == 0) {
-        IntegPlanHdr h;
-        h.nd = nd;
         h.nanchors = base_a;
         h.nslots = base_s;
         h.ok = overflow ? 0 : 1;
-        h.off_slot = off_slot;
-        h.off_anc = off_anc;
-        h.max_anchors = P.max_anchors;
-        h.max_slots = P.max_slots;
         *(IntegPlanHdr *)plan = h;
     }
 }
@@ -199,7 +229,7 @@ __global__ void __launch_bounds__(256) integrate_pixels_kernel(IntegPixParams P)
                 for (int q = lane; q < m.nm; q += 32) MMr[q] = m.m0 + m.dm * (float)q;
                 const IntegPlanHdr *h = (const IntegPlanHdr *)plan;
                 nslots = h->nslots;
-                diag = (const int2 *)(plan + 32);
+                diag = (const int2 *)(plan + ((sizeof(IntegPlanHdr) + 15) & ~15));
                 slotD = (const float *)(plan + h->off_slot);
                 anc = (const uint16_t *)(plan + h->off_anc);
                 pixels = P.jobs[job].g.pixels;
@@ -308,8 +338,9 @@ size_t integ_plan_bytes(int nm, int nM, int *max_anchors, int *max_slots)
     const long long na = (long long)nm * nM / GF_BLOCK + nd;
     *max_anchors = (int)std::min<long long>(na, 1ll << 30);
     *max_slots = (int)std::min<long long>(na, 65536);
-    return 32 + (size_t)(((8 * nd) + 15) & ~15ll) + (size_t)((4 * (long long)*max_slots + 15) & ~15ll) +
-           (size_t)((2 * na + 15) & ~15ll);
+    IntegPlanHdr h;
+    plan_layout(nm, nM, *max_anchors, *max_slots, h);
+    return (size_t)h.bytes;
 }
 
 cudaError_t launch_integ_plans(const IntegPlanDesc *desc_dev, int nplans, cudaStream_t s)

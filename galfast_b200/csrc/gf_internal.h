@@ -45,6 +45,19 @@ struct StarRecord {
     float u[4];                    /* uniforms x, y, M, m (u[2..3] = 0 if hidden by x^2+y^2>2) */
 };
 
+/* A bin with stars found by the batched draw: its stars' uniforms start at the
+ * stream state v_star (after the Poisson sampler's uniforms), and the stream
+ * had drawn nstars stars before it.  Expanded into k StarRecords. */
+struct EventRecord {
+    int32_t stream;                /* (request << 16) | stream */
+    int32_t ilb;                   /* pixel */
+    int16_t im, iM;                /* bin */
+    int32_t k;                     /* stars in the bin */
+    int32_t nstars;                /* the stream's stars before this bin */
+    int32_t pad;
+    uint64_t v_star;               /* stream state c*2^32 + x before the first star's first uniform */
+};
+
 /* Anchor quantities of a bin in the form the per-bin loop consumes:
  *   Am  beam extinction, or +inf when the anchor's distance is outside [dmin, dmax)
  *   ms  model density at the anchor position

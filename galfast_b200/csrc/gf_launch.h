@@ -136,10 +136,20 @@ cudaError_t launch_precision(const SkyModel &m, const SkyGeom &g, const float *D
                              cudaStream_t s);
 
 /* expected counts pixel by pixel (gf_integrate.cu) */
+/* Anchor plan of one magnitude grid (nm x nM, nm * nM a multiple of 10), one
+ * device buffer: this header, then
+ *   int2     diag[nd]        per diagonal: first anchor ordinal, first block start after its first bin
+ *   float    slotD[]         distance of every slot (distinct anchor distance of a diagonal)
+ *   uint16_t anc[]           slot of every anchor, diagonal by diagonal
+ *   uint32_t blk[nblocks]    per block of 10 bins (local index 10 b): i | j << 16 of its first bin
+ *   uint16_t bslot[nblocks]  slot of the block-start anchor
+ *   uint16_t dslot[nd]       slot of each diagonal's first bin */
 struct IntegPlanHdr {
     int32_t nd, nanchors, nslots, ok;      /* ok = 0: the plan did not fit its buffer */
-    int32_t off_slot, off_anc;             /* byte offsets of the slot distances and anchor slots */
+    int32_t off_slot, off_anc;             /* byte offsets of the tables */
     int32_t max_anchors, max_slots;
+    int32_t off_blk, off_bslot, off_dslot, nblocks;
+    int32_t bytes, pad[3];                 /* size of the plan buffer */
 };
 struct IntegPlanDesc {
     const float *Dtab;             /* D[im][iM], rows of nM_tab */
@@ -160,6 +170,38 @@ cudaError_t launch_integ_plans(const IntegPlanDesc *desc_dev, int nplans, cudaSt
 size_t integ_warp_bytes(int nm_max, int nM_max, int slots_max, IntegPixParams *P);
 /* per-pixel sums into P.pix_sum, then per-request totals into tot[njobs] */
 cudaError_t launch_integrate_pixels(const IntegPixParams &P, int model_type, double2 *tot, cudaStream_t s);
+
+/* the batched draw (gf_batchdraw.cu) */
+struct SlotDensityParams {
+    const CrawlJob *jobs;
+    const unsigned char *const *plans;   /* per request */
+    float *const *ms;              /* per request: model density [npixels][nslots] */
+    const int32_t *job_list;       /* requests of the launch */
+    const int32_t *pix_off;        /* [njobs + 1] first flat pixel of each listed request */
+    int32_t njobs, total_pix;
+};
+struct BatchDrawParams {
+    const CrawlJob *jobs;
+    const unsigned char *const *plans;   /* per request */
+    float *const *ms;              /* per request: slot densities */
+    const uint32_t *items;         /* (request << 16) | stream */
+    int32_t nitems;
+    uint32_t *next_item;           /* work-queue counter */
+    JumpTables jt;
+    EventRecord *ev;
+    int64_t ev_capacity;
+    unsigned long long *ev_count;  /* events found (may exceed the capacity) */
+    unsigned long long *err;       /* set when a bin's expected count is infinite */
+    int32_t off_tab, off_ev, warp_bytes;   /* per-warp shared-memory layout (batch_draw_warp_bytes) */
+};
+cudaError_t launch_slot_density(const SlotDensityParams &P, int model_type, cudaStream_t s);
+size_t batch_draw_warp_bytes(int max_tab, BatchDrawParams *P);
+cudaError_t launch_batch_draw(const BatchDrawParams &P, int model_type, int warps_per_cta, cudaStream_t s);
+cudaError_t expand_temp_bytes(int64_t nev, size_t *bytes);
+/* star records of the events at offsets from a scan over k; *total = the stars of all events */
+cudaError_t launch_expand_events(const EventRecord *ev, int64_t nev, const CrawlJob *jobs, int64_t *k64, int64_t *off64,
+                                 void *temp, size_t temp_bytes, StarRecord *rec, int64_t rec_capacity, int64_t *total,
+                                 cudaStream_t s);
 
 /* module kernels over the rows of many requests (row_slot: the request slot of each row) */
 struct MultiRows {

@@ -177,6 +177,11 @@ struct MultiWS {
     Grow<const unsigned char *> plans;
     Grow<int32_t> pixoff;
     Grow<gfk::IntegPlanDesc> pdesc;
+    Grow<float> msbuf;                      /* batched draw: slot densities of the chunk's pixels */
+    Grow<float *> msptr;
+    Grow<int32_t> joblist, chunkoff;
+    Grow<EventRecord> ev;
+    Grow<int64_t> k64, off64;
     gf_table out;
     HostGrow<char> h_stage;              /* page-locked staging of uploads and downloads */
     MultiWS() { memset(&out, 0, sizeof(out)); }
@@ -440,6 +445,13 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
     /* pixel-by-pixel integrate: anchor plans per magnitude grid (nm * nM is a
      * multiple of 10 for every batched request) */
     std::map<std::tuple<float, float, float, float, int, int>, unsigned char *> plans;
+    std::map<const unsigned char *, int> plan_nslots;
+    std::vector<char> plan_used(nmod, 0);
+    auto plan_of = [&](int j, int i) -> unsigned char * {
+        const SkyModel &m = R[j].hm[i].m;
+        auto it = plans.find(std::make_tuple(m.m0, m.dm, m.M1, m.dM, m.nM, m.nm));
+        return it == plans.end() ? nullptr : it->second;
+    };
     std::vector<double2> htot(njobs);
     const bool pixel_integrate = pix_total < (int64_t)INT32_MAX;
     if (pixel_integrate && !integ.empty()) {
@@ -494,6 +506,7 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
             for (size_t q = 0; q < uniq.size(); q++) {
                 ok = ok && hh[q].ok;
                 slots_max = std::max(slots_max, hh[q].nslots);
+                plan_nslots[uniq[q]] = hh[q].nslots;
             }
             for (int j : integ) {
                 nm_max = std::max(nm_max, R[j].hm[i].m.nm);
@@ -520,6 +533,7 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
                     S[j].expected_covered[i] = htot[j].y;
                 }
                 done = true;
+                plan_used[i] = 1;
             }
         }
         if (!done) {
@@ -575,7 +589,11 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
         for (int j : batched_all) {
             double mx = 0;
             for (int i = 0; i < nmod; i++) mx = std::max(mx, S[j].expected[i] + 8.0 * sqrt(S[j].expected[i]) + 1024.0);
-            const double need = mx * kStarBytes;
+            /* + events (48 bytes per star at most) and the slot densities of the request's pixels */
+            int ns = 0;
+            for (int i = 0; i < nmod; i++)
+                if (plan_used[i] && plan_of(j, i)) ns = std::max(ns, plan_nslots[plan_of(j, i)]);
+            const double need = mx * (kStarBytes + 48.0) + 4.0 * (double)jobs[j].npixels * ns;
             if (chunks.empty() || (used + need > (double)budget && !chunks.back().empty())) {
                 chunks.emplace_back();
                 used = 0;
@@ -669,65 +687,139 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
             GF_CUDA(cudaMemcpyAsync(d_rng_snap, d_rng, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
             const int mtype = R[batched[0]].hm[i].m.type;
             GF_TRY(rec.need((size_t)cap));
-            if (ctx->draw_cw[mtype] == 0) {
-                /* autotuner: time 4, 2 and 1 warps per stream on the head of the work queue
-                 * (the largest requests), from the same stream states, and keep the fastest */
-                const int32_t trial = std::min<int32_t>(nitems, std::max<int32_t>(nitems / 16, 148 * 32));
-                float best_ms = 0.f;
-                int best = 4;
-                cudaEvent_t e0, e1;
-                GF_CUDA(cudaEventCreate(&e0));
-                GF_CUDA(cudaEventCreate(&e1));
-                for (int cw : {4, 2, 1}) {
-                    GF_CUDA(cudaMemcpyAsync(d_rng, d_rng_snap, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
-                    GF_CUDA(cudaMemsetAsync(cs_base, 0, cs_bytes, st));
-                    GF_CUDA(cudaMemsetAsync(ctx->d_counters, 0, 24, st));
-                    gfk::LaunchCrawlMulti T;
-                    memset(&T, 0, sizeof(T));
-                    T.jobs = d_jobs; T.items = d_items; T.nitems = trial; T.counter = d_counter;
-                    T.model_type = mtype; T.max_tab = max_tab(i, batched); T.jt = ctx->jt;
-                    T.rec = rec.p; T.rec_capacity = (int64_t)rec.n;
-                    T.rec_count = ctx->d_counters; T.err = ctx->d_counters + 2;
-                    T.cw = cw;
-                    GF_CUDA(cudaEventRecord(e0, st));
-                    GF_CUDA(gfk::launch_crawl_multi(T, 1, st));
-                    GF_CUDA(cudaEventRecord(e1, st));
-                    GF_CUDA(cudaEventSynchronize(e1));
-                    float ms = 0.f;
-                    GF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-                    if (cw == 4 || ms < best_ms) { best_ms = ms; best = cw; }
-                }
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-                ctx->draw_cw[mtype] = best;
-                GF_CUDA(cudaMemcpyAsync(d_rng, d_rng_snap, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
-            }
             int64_t nrec = 0;
-            for (;;) {
-                GF_TRY(rec.need((size_t)cap));
-                GF_CUDA(cudaMemsetAsync(cs_base, 0, cs_bytes, st));
-                GF_CUDA(cudaMemsetAsync(ctx->d_counters, 0, 24, st));
-                gfk::LaunchCrawlMulti L;
-                memset(&L, 0, sizeof(L));
-                L.jobs = d_jobs; L.items = d_items; L.nitems = nitems; L.counter = d_counter;
-                L.model_type = R[batched[0]].hm[i].m.type;
-                L.max_tab = max_tab(i, batched);
-                L.jt = ctx->jt;
-                L.rec = rec.p; L.rec_capacity = (int64_t)rec.n;
-                L.rec_count = ctx->d_counters; L.err = ctx->d_counters + 2;
-                L.cw = ctx->draw_cw[mtype];
+            if (plan_used[i]) {
+                /* slot densities of the chunk's pixels */
+                std::vector<const unsigned char *> jp(njobs, nullptr);
+                std::vector<float *> jm(njobs, nullptr);
+                std::vector<int32_t> jl, poff;
+                std::vector<int64_t> moff(njobs, 0);
+                int64_t ms_total = 0;
+                int32_t tp = 0;
+                for (int j : batched) {
+                    jp[j] = plan_of(j, i);
+                    moff[j] = ms_total;
+                    ms_total += (int64_t)jobs[j].npixels * plan_nslots[jp[j]];
+                    jl.push_back(j);
+                    poff.push_back(tp);
+                    tp += jobs[j].npixels;
+                }
+                poff.push_back(tp);
+                GF_TRY(ws.msbuf.need((size_t)std::max<int64_t>(ms_total, 1)));
+                for (int j : batched) jm[j] = ws.msbuf.p + moff[j];
+                GF_TRY(ws.msptr.need((size_t)njobs));
+                GF_TRY(ws.joblist.need(jl.size()));
+                GF_TRY(ws.chunkoff.need(poff.size()));
+                GF_CUDA(cudaMemcpyAsync(ws.plans.p, jp.data(), sizeof(void *) * (size_t)njobs, cudaMemcpyHostToDevice, st));
+                GF_CUDA(cudaMemcpyAsync(ws.msptr.p, jm.data(), sizeof(void *) * (size_t)njobs, cudaMemcpyHostToDevice, st));
+                GF_CUDA(cudaMemcpyAsync(ws.joblist.p, jl.data(), 4 * jl.size(), cudaMemcpyHostToDevice, st));
+                GF_CUDA(cudaMemcpyAsync(ws.chunkoff.p, poff.data(), 4 * poff.size(), cudaMemcpyHostToDevice, st));
+                gfk::SlotDensityParams SD;
+                SD.jobs = d_jobs; SD.plans = ws.plans.p; SD.ms = ws.msptr.p;
+                SD.job_list = ws.joblist.p; SD.pix_off = ws.chunkoff.p;
+                SD.njobs = (int32_t)jl.size(); SD.total_pix = tp;
                 {
                     ProfScope ps(ctx, GF_PROF_DRAW_WINDOW);
-                    GF_CUDA(gfk::launch_crawl_multi(L, 1, st));
+                    GF_CUDA(gfk::launch_slot_density(SD, mtype, st));
                 }
-                GF_CUDA(cudaMemcpyAsync(ctx->h_counters, ctx->d_counters, 24, cudaMemcpyDeviceToHost, st));
-                GF_CUDA(cudaStreamSynchronize(st));
-                nrec = (int64_t)ctx->h_counters[0];
-                if (ctx->h_counters[2]) return fail(GF_E_INVALID, "a bin has an infinite expected star count");
-                if (nrec <= (int64_t)rec.n) break;
-                /* more stars than the buffer holds: restore the streams and draw again */
-                GF_CUDA(cudaMemcpyAsync(d_rng, d_rng_snap, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
-                cap = nrec + nrec / 8 + 65536;
+                gfk::BatchDrawParams B;
+                memset(&B, 0, sizeof(B));
+                if (gfk::batch_draw_warp_bytes(max_tab(i, batched), &B) > 200 * 1024)
+                    return fail(GF_E_UNSUPPORTED, "magnitude grid too large for the batched draw");
+                B.jobs = d_jobs; B.plans = ws.plans.p; B.ms = ws.msptr.p;
+                B.items = d_items; B.nitems = nitems; B.next_item = d_counter; B.jt = ctx->jt;
+                B.ev_count = ctx->d_counters; B.err = ctx->d_counters + 2;
+                GF_TRY(ws.ev.need((size_t)cap));
+                B.ev = ws.ev.p; B.ev_capacity = (int64_t)ws.ev.n;
+                if (ctx->draw_cw[mtype] == 0) {
+                    /* autotuner: time 8, 4, 2 and 1 warps per CTA on the head of the work queue
+                     * (the largest requests), from the same stream states, and keep the fastest */
+                    gfk::BatchDrawParams T = B;
+                    T.nitems = std::min<int32_t>(nitems, std::max<int32_t>(nitems / 16, 148 * 64));
+                    float best_ms = 0.f;
+                    int best = 4;
+                    cudaEvent_t e0, e1;
+                    GF_CUDA(cudaEventCreate(&e0));
+                    GF_CUDA(cudaEventCreate(&e1));
+                    for (int wpc : {8, 4, 2, 1}) {
+                        GF_CUDA(cudaMemcpyAsync(d_rng, d_rng_snap, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
+                        GF_CUDA(cudaMemsetAsync(ctx->d_counters, 0, 24, st));
+                        GF_CUDA(cudaEventRecord(e0, st));
+                        GF_CUDA(gfk::launch_batch_draw(T, mtype, wpc, st));
+                        GF_CUDA(cudaEventRecord(e1, st));
+                        GF_CUDA(cudaEventSynchronize(e1));
+                        float ms = 0.f;
+                        GF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                        if (wpc == 8 || ms < best_ms) { best_ms = ms; best = wpc; }
+                    }
+                    cudaEventDestroy(e0);
+                    cudaEventDestroy(e1);
+                    ctx->draw_cw[mtype] = best;
+                    GF_CUDA(cudaMemcpyAsync(d_rng, d_rng_snap, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
+                }
+                int64_t nev = 0;
+                for (;;) {
+                    GF_CUDA(cudaMemsetAsync(ctx->d_counters, 0, 24, st));
+                    {
+                        ProfScope ps(ctx, GF_PROF_DRAW_WINDOW);
+                        GF_CUDA(gfk::launch_batch_draw(B, mtype, ctx->draw_cw[mtype], st));
+                    }
+                    GF_CUDA(cudaMemcpyAsync(ctx->h_counters, ctx->d_counters, 24, cudaMemcpyDeviceToHost, st));
+                    GF_CUDA(cudaStreamSynchronize(st));
+                    nev = (int64_t)ctx->h_counters[0];
+                    if (ctx->h_counters[2]) return fail(GF_E_INVALID, "a bin has an infinite expected star count");
+                    if (nev <= B.ev_capacity) break;
+                    /* more bins with stars than the event list holds: restore the streams and draw again */
+                    GF_CUDA(cudaMemcpyAsync(d_rng, d_rng_snap, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
+                    GF_TRY(ws.ev.need((size_t)(nev + nev / 8 + 65536)));
+                    B.ev = ws.ev.p; B.ev_capacity = (int64_t)ws.ev.n;
+                }
+                /* the star records of the events */
+                GF_TRY(ws.k64.need((size_t)std::max<int64_t>(nev, 1)));
+                GF_TRY(ws.off64.need((size_t)std::max<int64_t>(nev, 1)));
+                size_t tb = 0;
+                GF_CUDA(gfk::expand_temp_bytes(nev, &tb));
+                GF_TRY(temp.need(tb + 256));
+                int64_t *d_total = (int64_t *)(ctx->d_counters + 1);
+                for (;;) {
+                    {
+                        ProfScope ps(ctx, GF_PROF_PLACE);
+                        GF_CUDA(gfk::launch_expand_events(ws.ev.p, nev, d_jobs, ws.k64.p, ws.off64.p, temp.p, temp.n, rec.p,
+                                                          (int64_t)rec.n, d_total, st));
+                    }
+                    GF_CUDA(cudaMemcpyAsync(ctx->h_counters + 1, ctx->d_counters + 1, 8, cudaMemcpyDeviceToHost, st));
+                    GF_CUDA(cudaStreamSynchronize(st));
+                    nrec = (int64_t)ctx->h_counters[1];
+                    if (nrec <= (int64_t)rec.n) break;
+                    GF_TRY(rec.need((size_t)(nrec + nrec / 8 + 65536)));
+                }
+            } else {
+                for (;;) {
+                    GF_TRY(rec.need((size_t)cap));
+                    GF_CUDA(cudaMemsetAsync(cs_base, 0, cs_bytes, st));
+                    GF_CUDA(cudaMemsetAsync(ctx->d_counters, 0, 24, st));
+                    gfk::LaunchCrawlMulti L;
+                    memset(&L, 0, sizeof(L));
+                    L.jobs = d_jobs; L.items = d_items; L.nitems = nitems; L.counter = d_counter;
+                    L.model_type = mtype;
+                    L.max_tab = max_tab(i, batched);
+                    L.jt = ctx->jt;
+                    L.rec = rec.p; L.rec_capacity = (int64_t)rec.n;
+                    L.rec_count = ctx->d_counters; L.err = ctx->d_counters + 2;
+                    L.cw = 1;
+                    {
+                        ProfScope ps(ctx, GF_PROF_DRAW_WINDOW);
+                        GF_CUDA(gfk::launch_crawl_multi(L, 1, st));
+                    }
+                    GF_CUDA(cudaMemcpyAsync(ctx->h_counters, ctx->d_counters, 24, cudaMemcpyDeviceToHost, st));
+                    GF_CUDA(cudaStreamSynchronize(st));
+                    nrec = (int64_t)ctx->h_counters[0];
+                    if (ctx->h_counters[2]) return fail(GF_E_INVALID, "a bin has an infinite expected star count");
+                    if (nrec <= (int64_t)rec.n) break;
+                    /* more stars than the buffer holds: restore the streams and draw again */
+                    GF_CUDA(cudaMemcpyAsync(d_rng, d_rng_snap, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
+                    cap = nrec + nrec / 8 + 65536;
+                }
             }
             /* placement and the (request, star_comp) sort */
             const size_t n = (size_t)std::max<int64_t>(nrec, 1);
@@ -848,20 +940,20 @@ extern "C" gf_status gf_multi_set_memory_budget(gf_ctx *ctx, int64_t bytes)
     return GF_OK;
 }
 
-extern "C" gf_status gf_tuning_get(gf_ctx *ctx, int32_t model_kind, int32_t *warps_per_stream)
+extern "C" gf_status gf_tuning_get(gf_ctx *ctx, int32_t model_kind, int32_t *warps_per_cta)
 {
     GF_TRY(gfa::check_ctx(ctx));
-    if (model_kind < 1 || model_kind > 2 || !warps_per_stream) return fail(GF_E_INVALID, "invalid arguments");
-    *warps_per_stream = ctx->draw_cw[model_kind];
+    if (model_kind < 1 || model_kind > 2 || !warps_per_cta) return fail(GF_E_INVALID, "invalid arguments");
+    *warps_per_cta = ctx->draw_cw[model_kind];
     return GF_OK;
 }
 
-extern "C" gf_status gf_tuning_set(gf_ctx *ctx, int32_t model_kind, int32_t warps_per_stream)
+extern "C" gf_status gf_tuning_set(gf_ctx *ctx, int32_t model_kind, int32_t warps_per_cta)
 {
     GF_TRY(gfa::check_ctx(ctx));
     if (model_kind < 1 || model_kind > 2) return fail(GF_E_INVALID, "invalid model kind");
-    if (warps_per_stream != 0 && warps_per_stream != 1 && warps_per_stream != 2 && warps_per_stream != 4)
-        return fail(GF_E_INVALID, "warps per stream must be 1, 2, 4 or 0 (tune again)");
-    ctx->draw_cw[model_kind] = warps_per_stream;
+    if (warps_per_cta != 0 && warps_per_cta != 1 && warps_per_cta != 2 && warps_per_cta != 4 && warps_per_cta != 8)
+        return fail(GF_E_INVALID, "warps per CTA must be 1, 2, 4, 8 or 0 (tune again)");
+    ctx->draw_cw[model_kind] = warps_per_cta;
     return GF_OK;
 }

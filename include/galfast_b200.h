@@ -428,12 +428,13 @@ gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, g
  * 0 (the default) = 60% of the free device memory at the start of the run. */
 gf_status gf_multi_set_memory_budget(gf_ctx *ctx, int64_t bytes);
 
-/* Warps per crawl stream in the batched draw, by model kind (GF_MODEL_*): 1, 2 or 4.
- * The first gf_catalog_run_multi pass of each kind times the three on the head of
- * its work queue and keeps the fastest for the context (0 = not tuned yet);
- * gf_tuning_set fixes the choice, or with 0 asks for a new trial. */
-gf_status gf_tuning_get(gf_ctx *ctx, int32_t model_kind, int32_t *warps_per_stream);
-gf_status gf_tuning_set(gf_ctx *ctx, int32_t model_kind, int32_t warps_per_stream);
+/* Warps per CTA of the batched draw kernel (one warp per stream), by model kind
+ * (GF_MODEL_*): 1, 2, 4 or 8.  The first gf_catalog_run_multi pass of each kind
+ * times the four on the head of its work queue and keeps the fastest for the
+ * context (0 = not tuned yet); gf_tuning_set fixes the choice, or with 0 asks
+ * for a new trial. */
+gf_status gf_tuning_get(gf_ctx *ctx, int32_t model_kind, int32_t *warps_per_cta);
+gf_status gf_tuning_set(gf_ctx *ctx, int32_t model_kind, int32_t warps_per_cta);
 
 /* ---- serving: continuous batching of requests ---- */
 

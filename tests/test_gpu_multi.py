@@ -108,15 +108,14 @@ def test_multi_request_is_repeatable_and_chunking_is_transparent(lib):
     ctx.close()
 
 
-def test_warps_per_stream_choice_does_not_change_rows(lib):
-    """The tuner picks 1, 2 or 4 warps per crawl stream for the batched draw; every
-    forced choice gives the same rows (the stars of a stream do not depend on how
-    many warps crawl it)."""
+def test_draw_block_size_choice_does_not_change_rows(lib):
+    """The tuner picks 1, 2, 4 or 8 warps per CTA for the batched draw; every forced
+    choice gives the same rows."""
     ws = requests(lib, n=4)
     ctx = G.Context(0)
     assert set(ctx.tuning().values()) == {0}
     runs = []
-    for cw in (None, 1, 2, 4):
+    for cw in (None, 1, 2, 4, 8):
         if cw is not None:
             for kind in ctx.tuning():
                 ctx.set_tuning(kind, cw)
@@ -126,7 +125,7 @@ def test_warps_per_stream_choice_does_not_change_rows(lib):
             got.setdefault((j, model), []).append(np.concatenate([rows["lb"].ravel(), rows["DM"].ravel(), rows["absmag"].ravel()]))
         G.run_catalog_multi(ctx, ws, sink=sink)
         if cw is None:
-            assert all(v in (1, 2, 4) for v in ctx.tuning().values())
+            assert all(v in (1, 2, 4, 8) for v in ctx.tuning().values())
         runs.append(got)
     for other in runs[1:]:
         assert runs[0].keys() == other.keys()
