@@ -117,7 +117,7 @@ def workload(G, W, name, rank=0):
 
 
 C4_NREQ = 4096
-C4_CAPACITY = 1 << 23          # rows per output batch of each request
+C4_CAPACITY = 1 << 24          # rows per output batch of each request: 16M, the full-sky chunk size and the most one batch holds (256 rows x 65536 streams)
 C4_PLAIN_STRIDE = 16           # the plain path is timed on every 16th request
 
 

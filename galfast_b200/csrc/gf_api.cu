@@ -337,6 +337,7 @@ gf_status gf_ctx_destroy(gf_ctx *ctx)
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     gfa::free_multi_ws(ctx);
+    gf_table_free(ctx, &ctx->plain_table);
     dev_free(ctx->d_rng);
     dev_free(ctx->d_mult);
     dev_free(ctx->jt.lo);
@@ -868,6 +869,22 @@ gf_status gf_skygen_draw(gf_skygen *s, int32_t model, gf_table *out, int64_t *n_
 
 /* ---------------- tables ---------------- */
 
+/* module columns start at zero so that rows a module skips are defined */
+static gf_status zero_module_columns(gf_ctx *ctx, gf_table *t)
+{
+    const size_t n = (size_t)t->capacity, nb = (size_t)t->nbands;
+    GF_CUDA(cudaMemsetAsync(t->FeH, 0, 4 * n, ctx->stream));
+    GF_CUDA(cudaMemsetAsync(t->vcyl, 0, 12 * n, ctx->stream));
+    if (nb) {
+        GF_CUDA(cudaMemsetAsync(t->mags, 0, 4 * nb * n, ctx->stream));
+        GF_CUDA(cudaMemsetAsync(t->obsmags, 0, 4 * nb * n, ctx->stream));
+    }
+    GF_CUDA(cudaMemsetAsync(t->photoflags, 0, 4 * n, ctx->stream));
+    GF_CUDA(cudaMemsetAsync(t->pm, 0, 12 * n, ctx->stream));
+    GF_CUDA(cudaMemsetAsync(t->radec, 0, 16 * n, ctx->stream));
+    return GF_OK;
+}
+
 gf_status gf_table_alloc(gf_ctx *ctx, int64_t capacity, int32_t nbands, gf_table *t)
 {
     GF_TRY(check_ctx(ctx));
@@ -895,16 +912,7 @@ gf_status gf_table_alloc(gf_ctx *ctx, int64_t capacity, int32_t nbands, gf_table
     GF_TRY(dev_alloc(&t->photoflags, n));
     GF_TRY(dev_alloc(&t->pm, 3 * n));
     GF_TRY(dev_alloc(&t->radec, 2 * n));
-    /* module columns start at zero so that rows a module skips are defined */
-    GF_CUDA(cudaMemsetAsync(t->FeH, 0, 4 * n, ctx->stream));
-    GF_CUDA(cudaMemsetAsync(t->vcyl, 0, 12 * n, ctx->stream));
-    if (nbands) {
-        GF_CUDA(cudaMemsetAsync(t->mags, 0, 4 * (size_t)nbands * n, ctx->stream));
-        GF_CUDA(cudaMemsetAsync(t->obsmags, 0, 4 * (size_t)nbands * n, ctx->stream));
-    }
-    GF_CUDA(cudaMemsetAsync(t->photoflags, 0, 4 * n, ctx->stream));
-    GF_CUDA(cudaMemsetAsync(t->pm, 0, 12 * n, ctx->stream));
-    GF_CUDA(cudaMemsetAsync(t->radec, 0, 16 * n, ctx->stream));
+    GF_TRY(zero_module_columns(ctx, t));
     GF_CUDA(cudaStreamSynchronize(ctx->stream));
     return GF_OK;
 }
@@ -1128,7 +1136,13 @@ gf_status gf_catalog_run(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, v
                             (int32_t)models.size(), &sky));
     struct Guard {
         gf_ctx *ctx; gf_skygen *sky; gf_table t; gf_photometry *ph; gf_photoerr *pe;
-        ~Guard() { gf_table_free(ctx, &t); gf_photometry_destroy(ph); gf_photoerr_destroy(pe); gf_skygen_destroy(sky); }
+        ~Guard()
+        {
+            /* the output table stays with the context for the next request of the same shape */
+            gf_table_free(ctx, &ctx->plain_table);
+            ctx->plain_table = t;
+            gf_photometry_destroy(ph); gf_photoerr_destroy(pe); gf_skygen_destroy(sky);
+        }
     } g{ctx, sky, gf_table(), nullptr, nullptr};
     memset(&g.t, 0, sizeof(g.t));
     /* integrate every model first (os_skygen.cpp:875-880) */
@@ -1143,7 +1157,14 @@ gf_status gf_catalog_run(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, v
         S.norm = (float)norm;
         for (int i = 0; i < (int)models.size(); i++) GF_TRY(gf_skygen_set_norm(sky, i, (float)norm));
     }
-    GF_TRY(gf_table_alloc(ctx, job->capacity, job->nbands, &g.t));
+    if (ctx->plain_table.capacity == job->capacity && ctx->plain_table.nbands == job->nbands) {
+        g.t = ctx->plain_table;
+        memset(&ctx->plain_table, 0, sizeof(gf_table));
+        g.t.size = 0;
+        GF_TRY(zero_module_columns(ctx, &g.t));
+    } else {
+        GF_TRY(gf_table_alloc(ctx, job->capacity, job->nbands, &g.t));
+    }
     if (job->phot) GF_TRY(gf_photometry_create(ctx, job->phot, &g.ph));
     if (job->perr) GF_TRY(gf_photoerr_create(ctx, job->perr, &g.pe));
     int64_t row_offset = 0;

@@ -121,13 +121,29 @@ __global__ void __launch_bounds__(256) slot_density_kernel(SlotDensityParams P)
         const int nslots = h->nslots;
         const float *slotD = plan_at<float>(plan, h->off_slot);
         const gf_pencil_beam pix = J.g.pixels[ilb];
-        float *row = P.ms[job] + (size_t)ilb * nslots;
+        float *row = P.ms[job] + (size_t)ilb * (nslots + 2);
         for (int s = lane; s < nslots; s += 32) {
             const float D = slotD[s];
             const float px = D * pix.cl * pix.cb;
             const float py = D * pix.sl * pix.cb;
             const float pz = D * pix.sb;
             row[s] = gfc::model_rho<MODEL>(J.m, px, py, pz);
+        }
+        /* the pixel's first cut apparent-magnitude row (m0 + dm im + Am > m1; increasing in im)
+         * and its volume factor K = dA * POGSON * dm * dM */
+        const SkyModel &m = J.m;
+        const float Am = gfc::beam_extinction(J.g, pix);
+        int icut = m.nm;
+        for (int i = lane; i < m.nm; i += 32)
+            if (m.m0 + m.dm * (float)i + Am > m.m1) { icut = i; break; }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const int t = __shfl_xor_sync(0xffffffffu, icut, o);
+            icut = t < icut ? t : icut;
+        }
+        if (lane == 0) {
+            row[nslots] = __int_as_float(icut);
+            row[nslots + 1] = pix.dA * GF_POGSON * m.dm * m.dM;
         }
     }
 }
@@ -209,7 +225,7 @@ __device__ __forceinline__ void flush_events(const BatchDrawParams &P, EventReco
 }
 
 template <int MODEL>
-__global__ void __launch_bounds__(256) batch_draw_kernel(BatchDrawParams P)
+__global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -222,16 +238,13 @@ __global__ void __launch_bounds__(256) batch_draw_kernel(BatchDrawParams P)
     __syncwarp();
 
     int loaded = -1;
-    const float *MMr = nullptr;
     const uint32_t *blk = nullptr;
     const uint16_t *bslot = nullptr, *dslot = nullptr;
     const float *slotD = nullptr, *msbase = nullptr;
     const gf_pencil_beam *pixels = nullptr;
-    const float *ammin = nullptr;
     int nslots = 0, Bp = 1, npix = 0, x = 1, y = 1, N = 1;
-    float norm = 0.f, m1 = 0.f, kdm = 0.f, dmin = 0.f, dmax = 0.f;
+    float norm = 0.f, dmin = 0.f, dmax = 0.f;
     bool dlim = false;
-    const float INF = __int_as_float(0x7f800000);
 
     for (;;) {
         int it = 0;
@@ -247,9 +260,7 @@ __global__ void __launch_bounds__(256) batch_draw_kernel(BatchDrawParams P)
             for (int w = lane; w < (int)(sizeof(SkyModel) / 4); w += 32) ((uint32_t *)&m)[w] = src[w];
             __syncwarp();
             x = m.nm; y = m.nM; N = m.nthreads;
-            MMr = LFM + y;
             for (int q = lane; q < y; q += 32) LFM[q] = gfc::lf_sample(m, m.lf, m.M1 - (float)q * m.dM);
-            for (int q = lane; q < x; q += 32) ((float *)MMr)[q] = m.m0 + m.dm * (float)q;
             const unsigned char *plan = P.plans[job];
             const IntegPlanHdr *h = (const IntegPlanHdr *)plan;
             nslots = h->nslots;
@@ -261,17 +272,13 @@ __global__ void __launch_bounds__(256) batch_draw_kernel(BatchDrawParams P)
             msbase = P.ms[job];
             pixels = J.g.pixels;
             npix = J.g.npixels;
-            ammin = (J.g.ext_kind != GF_EXT_NONE) ? J.g.ammin : nullptr;
             norm = m.norm;
-            m1 = m.m1;
-            kdm = m.dm;                      /* K = ((dA * POGSON) * dm) * dM */
             dmin = m.dmin;
             dmax = m.dmax;
             dlim = m.dmin != 0.f || m.dmax != 0.f;
             __syncwarp();
             loaded = job;
         }
-        const float dM = m.dM;
         const int NS = J.rng_nstreams;
         uint32_t *rng = J.rng;
         const uint32_t a = rng[t];
@@ -297,13 +304,12 @@ __global__ void __launch_bounds__(256) batch_draw_kernel(BatchDrawParams P)
                 i0 = (int)(bij & 0xffffu);
                 j0 = (int)(bij >> 16);
                 int slot = __ldg(bslot + lb);
-                const gf_pencil_beam *pp = pixels + pix;
-                const float Am = ammin ? __ldg(ammin + pp->extIdx) : 0.f;
-                const float K = pp->dA * GF_POGSON * kdm * dM;
-                const float *msr = msbase + (size_t)pix * nslots;
+                const float *msr = msbase + (size_t)pix * (nslots + 2);
+                const int icut = __float_as_int(msr[nslots]);
+                const float K = msr[nslots + 1];
                 float ms = msr[slot], D = __ldg(slotD + slot);
                 float D3 = D * D * D;
-                float Ae = (dlim && (dmin > D || dmax <= D)) ? INF : Am;
+                bool dc = dlim && (dmin > D || dmax <= D);      /* anchor outside [dmin, dmax): Am = inf */
                 int i = i0, j = j0;
 #pragma unroll
                 for (int s = 0; s < GF_BLOCK; s++) {
@@ -312,14 +318,14 @@ __global__ void __launch_bounds__(256) batch_draw_kernel(BatchDrawParams P)
                         ms = msr[slot];
                         D = __ldg(slotD + slot);
                         D3 = D * D * D;
-                        Ae = (dlim && (dmin > D || dmax <= D)) ? INF : Am;
+                        dc = dlim && (dmin > D || dmax <= D);
                     }
                     float r = LFM[j] * ms;
                     r *= norm;
                     r *= D3;
                     r *= K;
                     mu[s] = r;
-                    live |= (MMr[i] + Ae > m1) ? 0u : (1u << s);
+                    live |= (i < icut && !dc) ? (1u << s) : 0u;
                 }
             } else {
 #pragma unroll

@@ -175,7 +175,8 @@ cudaError_t launch_integrate_pixels(const IntegPixParams &P, int model_type, dou
 struct SlotDensityParams {
     const CrawlJob *jobs;
     const unsigned char *const *plans;   /* per request */
-    float *const *ms;              /* per request: model density [npixels][nslots] */
+    float *const *ms;              /* per request, per pixel: model density of each slot, then the first
+                                    * cut apparent-magnitude row (int bits) and K = dA POGSON dm dM */
     const int32_t *job_list;       /* requests of the launch */
     const int32_t *pix_off;        /* [njobs + 1] first flat pixel of each listed request */
     int32_t njobs, total_pix;

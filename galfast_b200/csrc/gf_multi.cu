@@ -593,7 +593,7 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
             int ns = 0;
             for (int i = 0; i < nmod; i++)
                 if (plan_used[i] && plan_of(j, i)) ns = std::max(ns, plan_nslots[plan_of(j, i)]);
-            const double need = mx * (kStarBytes + 48.0) + 4.0 * (double)jobs[j].npixels * ns;
+            const double need = mx * (kStarBytes + 48.0) + 4.0 * (double)jobs[j].npixels * (ns + 2);
             if (chunks.empty() || (used + need > (double)budget && !chunks.back().empty())) {
                 chunks.emplace_back();
                 used = 0;
@@ -699,7 +699,7 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
                 for (int j : batched) {
                     jp[j] = plan_of(j, i);
                     moff[j] = ms_total;
-                    ms_total += (int64_t)jobs[j].npixels * plan_nslots[jp[j]];
+                    ms_total += (int64_t)jobs[j].npixels * (plan_nslots[jp[j]] + 2);
                     jl.push_back(j);
                     poff.push_back(tp);
                     tp += jobs[j].npixels;
