@@ -45,6 +45,7 @@ BatchCallback = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.POINTER(Table), C.
 ServerRows = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.POINTER(Table), C.c_int64, C.c_int64)
 ServerDone = C.CFUNCTYPE(None, C.c_void_p, C.c_int64, C.c_int32, C.POINTER(CatalogStats))
 MultiCallback = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.POINTER(Table), C.POINTER(C.c_int64), C.POINTER(C.c_int64))
+MultiHostCallback = MultiCallback      # the same signature; the table is in host memory
 
 _lib = None
 
@@ -97,6 +98,8 @@ def lib():
         L.gf_module_gal2other.argtypes = [vp, C.c_int32, C.POINTER(Table), C.c_int64, C.c_int64]
         L.gf_catalog_run.argtypes = [vp, C.POINTER(Job), BatchCallback, vp, C.POINTER(CatalogStats)]
         L.gf_catalog_run_multi.argtypes = [vp, C.POINTER(Job), C.c_int32, MultiCallback, vp, C.POINTER(CatalogStats)]
+        L.gf_catalog_run_multi_host.argtypes = [vp, C.POINTER(Job), C.c_int32, C.c_int64, MultiHostCallback, vp,
+                                                C.POINTER(CatalogStats)]
         L.gf_multi_set_memory_budget.argtypes = [vp, C.c_int64]
         L.gf_tuning_get.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32)]
         L.gf_tuning_set.argtypes = [vp, C.c_int32, C.c_int32]
@@ -400,6 +403,50 @@ def run_catalog_multi(ctx, workloads, sink=None, device_sink=None):
 
     ccb = MultiCallback(cb)
     check(lib().gf_catalog_run_multi(ctx.h, jobs, n, ccb, None, stats))
+    return list(stats)
+
+
+def table_rows(t, a, b, names=None):
+    """Copies of rows [a, b) of a gf_table in host memory (vector columns (ncomp, rows))."""
+    out = {}
+    cap = int(t.capacity)
+    for name, dt, ncomp in COLUMNS:
+        if names is not None and name not in names:
+            continue
+        k = int(t.nbands) if ncomp == "bands" else ncomp
+        ptr = getattr(t, name)
+        if not ptr or k == 0:
+            continue
+        arr = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(np.ctypeslib.as_ctypes_type(dt))), shape=(k * cap,))
+        arr = arr.reshape(k, cap)[:, a:b].copy()
+        out[name] = arr[0] if ncomp == 1 else arr
+    return out
+
+
+def run_catalog_multi_host(ctx, workloads, sink, piece_rows=0):
+    """gf_catalog_run_multi_host: the catalogs of many requests generated together,
+    their rows copied to page-locked host memory while the device works on.
+
+    sink(job, model, rows) receives copies of a request's rows in one delivered
+    piece (a dict of column arrays); a request's rows of a model may come in
+    several pieces, in order.  Called from a CUDA driver thread.  Returns the
+    per-request CatalogStats."""
+    n = len(workloads)
+    jobs = (Job * n)(*[w.job(Job) for w in workloads])
+    stats = (CatalogStats * n)()
+
+    def cb(user, model, tptr, rb, rc):
+        try:
+            t = tptr.contents
+            for j in range(n):
+                if rc[j] > 0 and sink(j, model, table_rows(t, rb[j], rb[j] + rc[j])):
+                    return 1
+            return 0
+        except Exception:
+            return 1
+
+    ccb = MultiHostCallback(cb)
+    check(lib().gf_catalog_run_multi_host(ctx.h, jobs, n, int(piece_rows), ccb, None, stats))
     return list(stats)
 
 

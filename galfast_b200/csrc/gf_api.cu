@@ -24,6 +24,26 @@ gf_status fail(gf_status s, const std::string &msg)
     return s;
 }
 
+gf_status zero_module_rows(gf_ctx *ctx, const gf_table *t, int64_t n)
+{
+    if (n <= 0) return GF_OK;
+    const size_t P = (size_t)t->capacity, m = (size_t)n;
+    cudaStream_t st = ctx->stream;
+    auto z = [&](void *p, size_t elem, size_t ncomp) -> gf_status {
+        if (!p || ncomp == 0) return GF_OK;
+        GF_CUDA(cudaMemset2DAsync(p, P * elem, 0, m * elem, ncomp, st));
+        return GF_OK;
+    };
+    GF_TRY(z(t->FeH, 4, 1));
+    GF_TRY(z(t->vcyl, 4, 3));
+    GF_TRY(z(t->mags, 4, (size_t)t->nbands));
+    GF_TRY(z(t->photoflags, 4, 1));
+    GF_TRY(z(t->obsmags, 4, (size_t)t->nbands));
+    GF_TRY(z(t->pm, 4, 3));
+    GF_TRY(z(t->radec, 8, 2));
+    return GF_OK;
+}
+
 gf_status check_ctx(gf_ctx *ctx)
 {
     if (!ctx) return fail(GF_E_INVALID, "null context");
@@ -872,17 +892,7 @@ gf_status gf_skygen_draw(gf_skygen *s, int32_t model, gf_table *out, int64_t *n_
 /* module columns start at zero so that rows a module skips are defined */
 static gf_status zero_module_columns(gf_ctx *ctx, gf_table *t)
 {
-    const size_t n = (size_t)t->capacity, nb = (size_t)t->nbands;
-    GF_CUDA(cudaMemsetAsync(t->FeH, 0, 4 * n, ctx->stream));
-    GF_CUDA(cudaMemsetAsync(t->vcyl, 0, 12 * n, ctx->stream));
-    if (nb) {
-        GF_CUDA(cudaMemsetAsync(t->mags, 0, 4 * nb * n, ctx->stream));
-        GF_CUDA(cudaMemsetAsync(t->obsmags, 0, 4 * nb * n, ctx->stream));
-    }
-    GF_CUDA(cudaMemsetAsync(t->photoflags, 0, 4 * n, ctx->stream));
-    GF_CUDA(cudaMemsetAsync(t->pm, 0, 12 * n, ctx->stream));
-    GF_CUDA(cudaMemsetAsync(t->radec, 0, 16 * n, ctx->stream));
-    return GF_OK;
+    return gfa::zero_module_rows(ctx, t, t->capacity);
 }
 
 gf_status gf_table_alloc(gf_ctx *ctx, int64_t capacity, int32_t nbands, gf_table *t)
@@ -1177,6 +1187,7 @@ gf_status gf_catalog_run(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, v
             const int64_t n = g.t.size;
             if (n == 0) continue;
             S.batches++;
+            GF_TRY(gfa::zero_module_rows(ctx, &g.t, n));
             /* the module chain in pipeline order (pipeline.h:75-88) */
             if (job->foot) GF_TRY(gf_module_clipper(ctx, job->foot, job->sky.proj, &g.t, 0, n));
             if (job->feh) GF_TRY(gf_module_fixedfeh(ctx, job->feh, &g.t, 0, n));

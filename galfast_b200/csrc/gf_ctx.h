@@ -87,6 +87,9 @@ struct gf_photoerr {
 namespace gfa {
 
 gf_status check_ctx(gf_ctx *ctx);
+/* zero the module columns (FeH, vcyl, mags, photoflags, obsmags, pm, radec) of rows
+ * [0, n): rows a module skips (hidden stars) read zero whatever the table held before */
+gf_status zero_module_rows(gf_ctx *ctx, const gf_table *t, int64_t n);
 void free_multi_ws(gf_ctx *ctx);
 /* multipliers and jump tables of all 65536 streams on the context's device */
 gf_status ensure_multipliers(gf_ctx *ctx);

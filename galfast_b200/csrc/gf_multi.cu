@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <tuple>
 #include <vector>
@@ -183,8 +184,27 @@ struct MultiWS {
     Grow<EventRecord> ev;
     Grow<int64_t> k64, off64;
     gf_table out;
+    gf_table out2;                          /* host delivery: passes alternate between out and out2 */
     HostGrow<char> h_stage;              /* page-locked staging of uploads and downloads */
-    MultiWS() { memset(&out, 0, sizeof(out)); }
+    /* host delivery: copy stream, per-table events, page-locked ring of host tables */
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_pass[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+    bool free_recorded[2] = {false, false};
+    HostGrow<char> ring;
+    MultiWS()
+    {
+        memset(&out, 0, sizeof(out));
+        memset(&out2, 0, sizeof(out2));
+    }
+    ~MultiWS()
+    {
+        if (copy_stream) cudaStreamSynchronize(copy_stream);
+        for (int b = 0; b < 2; b++) {
+            if (ev_pass[b]) cudaEventDestroy(ev_pass[b]);
+            if (ev_free[b]) cudaEventDestroy(ev_free[b]);
+        }
+        if (copy_stream) cudaStreamDestroy(copy_stream);
+    }
 };
 
 namespace gfa {
@@ -192,6 +212,7 @@ void free_multi_ws(gf_ctx *ctx)
 {
     if (!ctx->multi_ws) return;
     gf_table_free(ctx, &ctx->multi_ws->out);
+    gf_table_free(ctx, &ctx->multi_ws->out2);
     delete ctx->multi_ws;
     ctx->multi_ws = nullptr;
 }
@@ -218,8 +239,147 @@ int forward_plain_batch(void *u, int32_t model, const gf_table *dev, int64_t row
 
 }  // namespace
 
-extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, void *user,
-                                          gf_catalog_stats *stats)
+namespace {
+
+/* ---- host delivery: rows copied to a page-locked ring while the device works on ---- */
+#define GF_RING 3
+
+/* bytes of one row of a table with nb bands */
+size_t row_bytes(int nb)
+{
+    return 16 + 4 + 8 + 4 + 4 + 12 + 4 + 4 + 4 + 4 + 4 + 12 + 4 * (size_t)nb + 4 + 4 * (size_t)nb + 12 + 16;
+}
+
+/* host table of `cap` rows and nb bands over page-locked memory at p (column by column) */
+gf_table carve_table(char *p, int64_t cap, int nb)
+{
+    gf_table t;
+    memset(&t, 0, sizeof(t));
+    t.capacity = cap;
+    t.nbands = nb;
+    const size_t n = (size_t)cap;
+    auto take = [&](size_t bytes) { char *r = p; p += (bytes + 255) & ~(size_t)255; return (void *)r; };
+    t.lb = (double *)take(16 * n); t.projIdx = (int32_t *)take(4 * n); t.projXY = (float *)take(8 * n);
+    t.DM = (float *)take(4 * n); t.absmag = (float *)take(4 * n); t.XYZ = (float *)take(12 * n);
+    t.comp = (int32_t *)take(4 * n); t.Am = (float *)take(4 * n); t.AmInf = (float *)take(4 * n);
+    t.hidden = (int32_t *)take(4 * n); t.FeH = (float *)take(4 * n); t.vcyl = (float *)take(12 * n);
+    if (nb) { t.mags = (float *)take(4 * n * nb); t.obsmags = (float *)take(4 * n * nb); }
+    t.photoflags = (int32_t *)take(4 * n); t.pm = (float *)take(12 * n); t.radec = (double *)take(16 * n);
+    return t;
+}
+
+size_t carved_bytes(int64_t cap, int nb) { return row_bytes(nb) * (size_t)cap + 20 * 256; }
+
+/* rows [r0, r1) of the device table d into the host table h, on stream cs */
+gf_status copy_rows_async(const gf_table &d, int64_t r0, int64_t r1, gf_table &h, cudaStream_t cs)
+{
+    const size_t n = (size_t)(r1 - r0), P = (size_t)d.capacity, H = (size_t)h.capacity;
+    auto cp = [&](void *hp, const void *dp, size_t elem, int ncomp) -> gf_status {
+        if (!hp || !dp || n == 0 || ncomp <= 0) return GF_OK;
+        GF_CUDA(cudaMemcpy2DAsync(hp, H * elem, (const char *)dp + (size_t)r0 * elem, P * elem, n * elem, (size_t)ncomp,
+                                  cudaMemcpyDeviceToHost, cs));
+        return GF_OK;
+    };
+    GF_TRY(cp(h.lb, d.lb, 8, 2)); GF_TRY(cp(h.projIdx, d.projIdx, 4, 1)); GF_TRY(cp(h.projXY, d.projXY, 4, 2));
+    GF_TRY(cp(h.DM, d.DM, 4, 1)); GF_TRY(cp(h.absmag, d.absmag, 4, 1)); GF_TRY(cp(h.XYZ, d.XYZ, 4, 3));
+    GF_TRY(cp(h.comp, d.comp, 4, 1)); GF_TRY(cp(h.Am, d.Am, 4, 1)); GF_TRY(cp(h.AmInf, d.AmInf, 4, 1));
+    GF_TRY(cp(h.hidden, d.hidden, 4, 1)); GF_TRY(cp(h.FeH, d.FeH, 4, 1)); GF_TRY(cp(h.vcyl, d.vcyl, 4, 3));
+    GF_TRY(cp(h.mags, d.mags, 4, d.nbands)); GF_TRY(cp(h.photoflags, d.photoflags, 4, 1));
+    GF_TRY(cp(h.obsmags, d.obsmags, 4, d.nbands)); GF_TRY(cp(h.pm, d.pm, 4, 3)); GF_TRY(cp(h.radec, d.radec, 8, 2));
+    return GF_OK;
+}
+
+/* one delivered piece: run by the copy stream after its rows have arrived */
+struct Piece {
+    gf_multi_host_callback cb;
+    void *user;
+    int32_t model;
+    gf_table host;
+    std::vector<int64_t> begin, count;
+    int *stop;
+};
+
+void CUDART_CB deliver_piece(void *arg)
+{
+    Piece *p = (Piece *)arg;
+    if (*p->stop || !p->cb) return;
+    if (p->cb(p->user, p->model, &p->host, p->begin.data(), p->count.data()) != 0) *p->stop = 1;
+}
+
+struct HostDelivery {
+    gf_multi_host_callback cb = nullptr;
+    void *user = nullptr;
+    int64_t piece_rows = 0;
+    int nbands = 0;
+    int64_t next = 0;                    /* pieces enqueued */
+    std::deque<Piece> pieces;
+    int stop = 0;
+    gf_table ring[GF_RING];
+};
+
+/* Enqueue the delivery of rows [0, total) of the device table d, whose slot s holds
+ * request slot_job[s] at rows [row_begin[s], row_begin[s] + rows[s]). */
+gf_status deliver_pass(MultiWS &ws, HostDelivery &hd, int b, cudaStream_t st, const gf_table &d, int32_t model,
+                       const std::vector<int> &slot_job, const std::vector<int64_t> &row_begin,
+                       const std::vector<int64_t> &rows, int njobs)
+{
+    cudaStream_t cs = ws.copy_stream;
+    GF_CUDA(cudaEventRecord(ws.ev_pass[b], st));
+    GF_CUDA(cudaStreamWaitEvent(cs, ws.ev_pass[b], 0));
+    const int64_t total = row_begin[slot_job.size()];
+    for (int64_t r0 = 0; r0 < total; r0 += hd.piece_rows) {
+        const int64_t r1 = std::min(total, r0 + hd.piece_rows);
+        gf_table &h = hd.ring[hd.next % GF_RING];
+        hd.next++;
+        GF_TRY(copy_rows_async(d, r0, r1, h, cs));
+        hd.pieces.emplace_back();
+        Piece &p = hd.pieces.back();
+        p.cb = hd.cb; p.user = hd.user; p.model = model; p.stop = &hd.stop;
+        p.host = h;
+        p.host.size = r1 - r0;
+        p.host.nbands = d.nbands;
+        p.begin.assign(njobs, 0);
+        p.count.assign(njobs, 0);
+        for (size_t q = 0; q < slot_job.size(); q++) {
+            const int64_t a = std::max(r0, row_begin[q]), e = std::min(r1, row_begin[q] + rows[q]);
+            if (e > a) { p.begin[slot_job[q]] = a - r0; p.count[slot_job[q]] = e - a; }
+        }
+        GF_CUDA(cudaLaunchHostFunc(cs, deliver_piece, &p));
+    }
+    GF_CUDA(cudaEventRecord(ws.ev_free[b], cs));
+    ws.free_recorded[b] = true;
+    return GF_OK;
+}
+
+struct PlainHostForward {
+    HostDelivery *hd;
+    gf_ctx *ctx;
+    int32_t njobs, job;
+};
+
+/* a plain-path batch of a request run inside the multi call, delivered to the host
+ * through the ring on the calling thread */
+int forward_plain_host(void *u, int32_t model, const gf_table *dev, int64_t row_offset)
+{
+    (void)row_offset;
+    PlainHostForward *f = (PlainHostForward *)u;
+    HostDelivery &hd = *f->hd;
+    for (int64_t r0 = 0; r0 < dev->size; r0 += hd.piece_rows) {
+        const int64_t r1 = std::min(dev->size, r0 + hd.piece_rows);
+        gf_table h = hd.ring[0];
+        if (copy_rows_async(*dev, r0, r1, h, f->ctx->stream) != GF_OK) return 1;
+        if (cudaStreamSynchronize(f->ctx->stream) != cudaSuccess) return 1;
+        h.size = r1 - r0;
+        h.nbands = dev->nbands;
+        std::vector<int64_t> b(f->njobs, 0), c(f->njobs, 0);
+        c[f->job] = r1 - r0;
+        if (hd.cb && hd.cb(hd.user, model, &h, b.data(), c.data()) != 0) return 1;
+    }
+    return 0;
+}
+
+gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, gf_multi_host_callback hcb,
+                    int64_t piece_rows, void *user, gf_catalog_stats *stats)
 {
     GF_TRY(gfa::check_ctx(ctx));
     if (!jobs || njobs <= 0 || njobs > 32767) return fail(GF_E_INVALID, "njobs must be in [1, 32767]");
@@ -663,8 +823,34 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
     auto &key = ws.key, &key_b = ws.key_b;
     auto &idx_a = ws.idx_a, &idx_b = ws.idx_b, &slot_a = ws.slot_a, &slot_b = ws.slot_b;
     auto &temp = ws.temp;
-    gf_table &out = ws.out;
     std::vector<int64_t> catoff(njobs, 0);
+    /* host delivery: copy stream, events and the page-locked ring */
+    HostDelivery hd;
+    const bool to_host = hcb != nullptr;
+    if (to_host) {
+        if (!ws.copy_stream) {
+            GF_CUDA(cudaStreamCreateWithFlags(&ws.copy_stream, cudaStreamNonBlocking));
+            for (int b = 0; b < 2; b++) {
+                GF_CUDA(cudaEventCreateWithFlags(&ws.ev_pass[b], cudaEventDisableTiming));
+                GF_CUDA(cudaEventCreateWithFlags(&ws.ev_free[b], cudaEventDisableTiming));
+            }
+        }
+        ws.free_recorded[0] = ws.free_recorded[1] = false;
+        hd.cb = hcb;
+        hd.user = user;
+        hd.piece_rows = piece_rows > 0 ? piece_rows : (int64_t)4 << 20;
+        hd.nbands = nbands;
+        const size_t slot_bytes = carved_bytes(hd.piece_rows, nbands);
+        GF_TRY(ws.ring.need(slot_bytes * GF_RING));
+        for (int r = 0; r < GF_RING; r++) hd.ring[r] = carve_table(ws.ring.p + (size_t)r * slot_bytes, hd.piece_rows, nbands);
+    }
+    /* the copy stream finishes (and stops calling back) before this function returns */
+    struct CopyDrain {
+        MultiWS *ws;
+        bool on;
+        ~CopyDrain() { if (on && ws->copy_stream) cudaStreamSynchronize(ws->copy_stream); }
+    } copy_drain{&ws, to_host};
+    int pass = 0;
 
     for (const std::vector<int> &batched : chunks) {
         /* output order of the chunk: by module group, then request */
@@ -865,7 +1051,12 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
                 slot_comp[s] = R[j].hm[i].m.comp;
             }
             const int64_t total = row_begin[nslots];
+            /* host delivery: this pass's table must have been copied out by its previous user */
+            const int ob = to_host ? (pass & 1) : 0;
+            gf_table &out = ob ? ws.out2 : ws.out;
+            if (to_host && ws.free_recorded[ob]) GF_CUDA(cudaStreamWaitEvent(st, ws.ev_free[ob], 0));
             if (out.capacity < std::max<int64_t>(total, 1) || out.nbands < nbands) {
+                if (to_host) GF_CUDA(cudaStreamSynchronize(ws.copy_stream));
                 gf_table_free(ctx, &out);
                 GF_TRY(gf_table_alloc(ctx, std::max<int64_t>(total + total / 8, 1024), nbands, &out));
             }
@@ -880,6 +1071,7 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
                 GF_CUDA(gfk::launch_tie_gather_multi(PL, d_row_begin, d_slot_comp, out, row_slot.p, st));
             }
             out.size = total;
+            GF_TRY(gfa::zero_module_rows(ctx, &out, total));
             /* the module chain in pipeline order (pipeline.h:75-88) over every request's rows */
             gfk::MultiRows MR;
             MR.row_slot = row_slot.p; MR.slot_row_begin = d_row_begin; MR.slot_job = d_slot_job;
@@ -909,27 +1101,60 @@ extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32
                 if (J0.v2pm) GF_TRY(gf_module_vel2pm(ctx, J0.v2pm, &out, 0, total));
                 if (J0.gal2other) GF_TRY(gf_module_gal2other(ctx, J0.gal2other, &out, 0, total));
             }
-            GF_CUDA(cudaStreamSynchronize(st));
-            if (cb) {
-                std::vector<int64_t> rb(njobs, 0), rc(njobs, 0);
-                for (int s = 0; s < nslots; s++) { rb[slot_job[s]] = row_begin[s]; rc[slot_job[s]] = slot_rows[s]; }
-                if (cb(user, R[batched[0]].hm[i].m.comp, &out, rb.data(), rc.data()) != 0)
-                    return fail(GF_E_STATE, "stopped by the batch callback");
+            if (to_host) {
+                GF_TRY(deliver_pass(ws, hd, ob, st, out, R[batched[0]].hm[i].m.comp, slot_job, row_begin, slot_rows, njobs));
+                if (hd.stop) return fail(GF_E_STATE, "stopped by the host callback");
+            } else {
+                GF_CUDA(cudaStreamSynchronize(st));
+                if (cb) {
+                    std::vector<int64_t> rb(njobs, 0), rc(njobs, 0);
+                    for (int s = 0; s < nslots; s++) { rb[slot_job[s]] = row_begin[s]; rc[slot_job[s]] = slot_rows[s]; }
+                    if (cb(user, R[batched[0]].hm[i].m.comp, &out, rb.data(), rc.data()) != 0)
+                        return fail(GF_E_STATE, "stopped by the batch callback");
+                }
             }
+            pass++;
             for (int s = 0; s < nslots; s++) catoff[slot_job[s]] += slot_rows[s];
         }
     }
 
     /* ---- requests that need the batch rules of the plain path ---- */
+    if (to_host) {
+        /* deliveries stay in order: the batched passes first */
+        GF_CUDA(cudaStreamSynchronize(ws.copy_stream));
+        if (hd.stop) return fail(GF_E_STATE, "stopped by the host callback");
+    }
     for (int j = 0; j < njobs; j++) {
         if (!R[j].plain) continue;
-        PlainForward f;
-        f.cb = cb; f.user = user; f.njobs = njobs; f.job = j;
-        f.begin.assign(njobs, 0);
-        f.count.assign(njobs, 0);
-        GF_TRY(gf_catalog_run(ctx, &jobs[j], forward_plain_batch, &f, &S[j]));
+        if (to_host) {
+            PlainHostForward f;
+            f.hd = &hd; f.ctx = ctx; f.njobs = njobs; f.job = j;
+            GF_TRY(gf_catalog_run(ctx, &jobs[j], forward_plain_host, &f, &S[j]));
+        } else {
+            PlainForward f;
+            f.cb = cb; f.user = user; f.njobs = njobs; f.job = j;
+            f.begin.assign(njobs, 0);
+            f.count.assign(njobs, 0);
+            GF_TRY(gf_catalog_run(ctx, &jobs[j], forward_plain_batch, &f, &S[j]));
+        }
     }
     return GF_OK;
+}
+
+}  // namespace
+
+extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, void *user,
+                                          gf_catalog_stats *stats)
+{
+    return run_multi(ctx, jobs, njobs, cb, nullptr, 0, user, stats);
+}
+
+extern "C" gf_status gf_catalog_run_multi_host(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, int64_t piece_rows,
+                                               gf_multi_host_callback cb, void *user, gf_catalog_stats *stats)
+{
+    if (!cb) return fail(GF_E_INVALID, "host delivery needs a callback");
+    if (piece_rows < 0) return fail(GF_E_INVALID, "negative piece size");
+    return run_multi(ctx, jobs, njobs, nullptr, cb, piece_rows, user, stats);
 }
 
 extern "C" gf_status gf_multi_set_memory_budget(gf_ctx *ctx, int64_t bytes)

@@ -428,6 +428,21 @@ gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, g
  * 0 (the default) = 60% of the free device memory at the start of the run. */
 gf_status gf_multi_set_memory_budget(gf_ctx *ctx, int64_t bytes);
 
+/* gf_catalog_run_multi with the rows delivered in host memory.  After each model
+ * pass the library copies the pass's rows to a ring of page-locked host tables on
+ * a second stream while the device generates the next pass, in pieces of at most
+ * piece_rows rows (0: 4M).  cb sees one piece: request j's rows are
+ * host rows row_begin[j] .. row_begin[j] + row_count[j] - 1 (count 0: none in
+ * this piece); a request's rows of a model arrive in order, possibly over several
+ * pieces.  The host table is valid until cb returns.  cb runs on a CUDA driver
+ * thread (or, for requests that need several output batches, on the calling
+ * thread) and must not call CUDA or this library; a nonzero return stops the run
+ * (GF_E_STATE).  All callbacks have returned when this function returns. */
+typedef int (*gf_multi_host_callback)(void *user, int32_t model, const gf_table *host, const int64_t *row_begin,
+                                      const int64_t *row_count);
+gf_status gf_catalog_run_multi_host(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, int64_t piece_rows,
+                                    gf_multi_host_callback cb, void *user, gf_catalog_stats *stats);
+
 /* Warps per CTA of the batched draw kernel (one warp per stream), by model kind
  * (GF_MODEL_*): 1, 2, 4 or 8.  The first gf_catalog_run_multi pass of each kind
  * times the four on the head of its work queue and keeps the fastest for the

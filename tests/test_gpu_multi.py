@@ -134,3 +134,36 @@ def test_draw_block_size_choice_does_not_change_rows(lib):
     with pytest.raises(G.GalfastError):
         ctx.set_tuning(1, 3)
     ctx.close()
+
+
+def test_host_delivery_equals_device_rows(lib):
+    """gf_catalog_run_multi_host: rows copied to page-locked host memory while the
+    device works on, in pieces small enough to split requests, equal the rows of
+    gf_catalog_run_multi (including a request that needs the plain batch rules)."""
+    ws = requests(lib, n=5)
+    ctx = G.Context(0)
+    ref = {}
+
+    def sink(j, model, rows):
+        ref.setdefault((j, model), []).append(rows)
+    st_ref = G.run_catalog_multi(ctx, ws, sink=sink)
+    for piece in (0, 1000):
+        got = {}
+
+        def hsink(j, model, rows):
+            got.setdefault((j, model), []).append(rows)
+        st = G.run_catalog_multi_host(ctx, ws, hsink, piece_rows=piece)
+        assert sorted(got) == sorted(ref)
+        if piece:
+            assert max(len(v) for v in got.values()) > 1          # requests split over pieces
+        for k in ref:
+            a = {c: np.concatenate([p[c] for p in ref[k]], axis=-1) for c in ref[k][0]}
+            b = {c: np.concatenate([p[c] for p in got[k]], axis=-1) for c in got[k][0]}
+            for c in a:
+                x, y = a[c], b[c]
+                if c in ("mags", "obsmags"):
+                    y = y[: x.shape[0]]
+                np.testing.assert_array_equal(x, y, err_msg="%s %s" % (c, k))
+        for j in range(len(ws)):
+            assert st[j].generated[:3] == st_ref[j].generated[:3]
+    ctx.close()
