@@ -294,12 +294,12 @@ def draw_rooflines(pk, pk_kind, bins, diags, stars_step, npix_models, draw_ms, d
     pf32, psfu, pf64 = B200_SMS * FP32_PER_SM * clk, B200_SMS * SFU_PER_SM * clk, B200_SMS * FP64_PER_SM * clk
     t_roof = max(fp32 / pf32, sfu / psfu, fp64 / pf64, bytes_alg / (pk["hbm_gbs"] * 1e9))
     achieved = bytes_alg / t_draw / 1e9 if t_draw == t_draw else None
-    roofline = {"bound": "hbm", "kernel": "crawl_kernel<1> (draw pass)", "achieved": achieved,
+    roofline = {"bound": "hbm", "kernel": "batch_draw_kernel (draw pass)", "achieved": achieved,
                 "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": (achieved / pk["hbm_gbs"]) if achieved else None,
                 "traffic": None, "peak_source": pk_kind,
                 "algorithmic_bytes_per_launch": bytes_alg * nsteps / max(draw_launches, 1),
                 "avg_launch_ms": draw_ms / max(draw_launches, 1)}
-    compute = {"bound": "sfu/fp32 issue (nominal)", "kernel": "crawl_kernel<1> (draw pass)",
+    compute = {"bound": "sfu/fp32 issue (nominal)", "kernel": "batch_draw_kernel (draw pass)",
                "t_bound_s": t_roof, "t_measured_s": t_draw, "frac": t_roof / t_draw if t_draw == t_draw else None,
                "fp32_ops": fp32, "sfu_ops": sfu, "fp64_ops": fp64,
                "peaks": {"fp32_ops_per_s": pf32, "sfu_ops_per_s": psfu, "fp64_ops_per_s": pf64, "clock_mhz": clk / 1e6}}

@@ -142,7 +142,7 @@ COLUMNS = [  # name, dtype, components (or "bands")
     ("pm", np.float32, 3), ("radec", np.float64, 2),
 ]
 PROFILE_PHASES = ["integrate", "draw_window", "draw_rerun", "place", "sort", "clipper", "fixedfeh", "bond2010",
-                  "photometry", "photoerrors", "vel2pm", "gal2other"]
+                  "photometry", "photoerrors", "vel2pm", "gal2other", "slot_density", "expand"]
 SKYGEN_COLUMNS = ["lb", "projIdx", "projXY", "DM", "absmag", "XYZ", "comp", "Am", "AmInf", "hidden"]
 
 
@@ -220,10 +220,10 @@ class Context:
 
     def profile_read(self):
         """{phase: (milliseconds, launches)} accumulated since the last read."""
-        ms = (C.c_double * 12)()
-        n = (C.c_int64 * 12)()
+        ms = (C.c_double * len(PROFILE_PHASES))()
+        n = (C.c_int64 * len(PROFILE_PHASES))()
         check(lib().gf_profile_read(self.h, ms, n))
-        return {PROFILE_PHASES[i]: (ms[i], n[i]) for i in range(12) if n[i]}
+        return {PROFILE_PHASES[i]: (ms[i], n[i]) for i in range(len(PROFILE_PHASES)) if n[i]}
 
     def elapsed_ms(self, a, b):
         ms = C.c_float()

@@ -15,16 +15,15 @@
  *                   bin is then a table lookup: block-start anchors through the
  *                   plan's per-block slot, diagonal starts through its
  *                   per-diagonal slot.
- *   draw            one warp per stream, lane L on block r + L of the stream's
- *                   window of 32 blocks.  Each lane computes mu of its 10 bins in
- *                   registers, jumps to the stream state of its first uncut bin
- *                   (the MWC stream is a Lehmer generator modulo its safe prime;
- *                   assuming no earlier bin of the window has stars) and walks its
- *                   bins with plain MWC steps.  The first lane whose bin has stars
- *                   runs the reference's Poisson sampler and the star uniforms by
- *                   itself, records the bin (an event: its k and the stream state
- *                   at its first star), and the lanes after it move their start
- *                   states by a^(used - 1) and walk again.  Nothing else waits.
+ *   draw            one warp per 32 consecutive streams, one lane per stream.
+ *                   The lanes' blocks at the same step are consecutive blocks of
+ *                   one pixel (stream t + L takes block t + L + r N at step r), so
+ *                   the plan and slot-density loads coalesce.  Each lane computes
+ *                   mu of its block's 10 bins in registers and walks them with
+ *                   plain MWC steps; the lanes whose bin has stars run the
+ *                   reference's Poisson sampler and the star uniforms together,
+ *                   record the bin (an event: its k and the stream state at its
+ *                   first star) and walk on from the state after the stars.
  *   expand          (thread per event) the star records of each event, regenerated
  *                   from its stream state, at offsets from a scan over k.
  * The stream states left behind are the reference's, for the modules that
@@ -42,46 +41,11 @@ namespace {
 #define BD_FULL 0xffffffffu
 #define GF_EVBUF 32                /* events staged in shared memory per warp */
 
-__device__ __forceinline__ uint64_t bd_shfl64(uint64_t v, int src)
-{
-    const uint32_t lo = __shfl_sync(BD_FULL, (uint32_t)v, src);
-    const uint32_t hi = __shfl_sync(BD_FULL, (uint32_t)(v >> 32), src);
-    return ((uint64_t)hi << 32) | lo;
-}
-
-__device__ __forceinline__ int bd_incl_scan(int v, int lane)
-{
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(BD_FULL, v, o);
-        if (lane >= o) v += t;
-    }
-    return v;
-}
-
 __device__ __forceinline__ float bd_mwc_step(uint64_t &v, uint32_t a)
 {
     const uint64_t t = (uint64_t)a * (uint32_t)v + (v >> 32);
     v = t;
     return GF_MWC_SCALE * (float)(uint32_t)t;
-}
-
-/* v * a^n mod p for 0 <= n < 2048 from the stream's scaled powers */
-__device__ __forceinline__ uint64_t bd_jump(uint64_t v, int n, const uint64_t *lo, const uint64_t *hi, uint32_t a, uint64_t p)
-{
-    const uint64_t w = gfr::mwc_mulmod_scaled(__ldg(lo + (n & 31)), v, a, p);
-    return gfr::mwc_mulmod_scaled(__ldg(hi + (n >> 5)), w, a, p);
-}
-
-/* scaled a^n for any n >= 0 */
-__device__ uint64_t bd_power(uint32_t n, const uint64_t *lo, const uint64_t *hi, uint32_t a, uint64_t p)
-{
-    uint64_t ms = __ldg(lo);                                  /* scaled a^0 */
-    if (n >= 2048) {
-        const uint64_t m2047 = gfr::mwc_mulmod_scaled(__ldg(lo + 31), __ldg(hi + 63), a, p);
-        while (n >= 2047) { ms = gfr::mwc_mulmod_scaled(ms, m2047, a, p); n -= 2047; }
-    }
-    return gfr::mwc_mulmod_scaled(ms, gfr::mwc_mulmod_scaled(__ldg(lo + (n & 31)), __ldg(hi + (n >> 5)), a, p), a, p);
 }
 
 /* exp(-mu) >= 1 - mu: bins that surely draw no star, without exp */
@@ -148,64 +112,35 @@ __global__ void __launch_bounds__(256) slot_density_kernel(SlotDensityParams P)
     }
 }
 
-/* A bin with stars, on the lane that found it: the reference's Poisson sampler
- * from the bin's stream state wb, then the stars' uniforms (draw_stars: x, y,
- * and M, m unless x^2 + y^2 > 2), counted to move the stream on; the event is
- * staged for the expansion.  Returns 1 (and sets the error flag) for an
- * infinite expected count. */
-__device__ __noinline__ int draw_event(const BatchDrawParams &P, EventRecord *evb, int *nev, uint32_t a, const uint64_t *jlo,
-                                       const uint64_t *jhi, uint64_t pmod, uint64_t wb, float mu, int sid, int pix, int i0,
-                                       int j0, int es, int x, int y, const gf_pencil_beam *pixels, int &nst, uint64_t &vnew,
-                                       uint64_t &mult)
+/* A bin with stars, on the lane (stream) that found it: the reference's Poisson
+ * sampler from the bin's stream state wb, then the stars' uniforms (draw_stars:
+ * x, y, and M, m unless x^2 + y^2 > 2).  Returns the number of stars and the
+ * stream state after them; fills the event record when there are stars. */
+__device__ __noinline__ int draw_event(uint32_t a, uint64_t wb, float mu, const gf_pencil_beam *pp, uint64_t &vnew,
+                                       uint64_t &v_star)
 {
-    int i = i0, j = j0;
-    for (int s = 1; s <= es; s++) gfc::step_in_pixel(i, j, x, y);
-    if (!(mu < 3.0e38f)) {
-        /* an infinite expected count would never leave the sampler's gamma loop */
-        atomicOr(P.err, 1ull);
-        return 1;
-    }
     gfr::Mwc r;
     r.a = a;
     r.set_v(wb);
     r.used = 0;
     const int k = (int)r.poisson(mu);
-    const uint64_t v_star = r.v();
+    v_star = r.v();
     if (k > 0) {
-        const gf_pencil_beam pp = pixels[pix];
+        const float X = pp->X, Y = pp->Y, dx = pp->dx;
         for (int n = 0; n < k; n++) {
             const float u0 = r.uniform();
             const float u1 = r.uniform();
-            float xx = pp.X, yy = pp.Y;
-            xx += pp.dx * (u0 - 0.5f);
-            yy += pp.dx * (u1 - 0.5f);
+            float xx = X, yy = Y;
+            xx += dx * (u0 - 0.5f);
+            yy += dx * (u1 - 0.5f);
             if (!(xx * xx + yy * yy > 2.f)) {
                 r.uniform();
                 r.uniform();
             }
         }
-        EventRecord e;
-        e.stream = sid;
-        e.ilb = pix;
-        e.im = (int16_t)i;
-        e.iM = (int16_t)j;
-        e.k = k;
-        e.nstars = nst;
-        e.pad = 0;
-        e.v_star = v_star;
-        const int q = *nev;
-        if (q < GF_EVBUF) {
-            evb[q] = e;
-            *nev = q + 1;
-        } else {
-            const unsigned long long sl = atomicAdd(P.ev_count, 1ull);
-            if (sl < (unsigned long long)P.ev_capacity) P.ev[sl] = e;
-        }
-        nst += k;
     }
     vnew = r.v();
-    mult = bd_power(r.used - 1, jlo, jhi, a, pmod);
-    return 0;
+    return k;
 }
 
 /* write the warp's staged events to the global list (all lanes) */
@@ -224,6 +159,11 @@ __device__ __forceinline__ void flush_events(const BatchDrawParams &P, EventReco
     __syncwarp();
 }
 
+/* One warp per 32 consecutive streams of a request, one lane per stream.  Lane L
+ * walks its stream block by block: the blocks of the 32 streams at the same step
+ * are 32 consecutive blocks of (mostly) one pixel, so the table loads coalesce.
+ * Lanes whose bin has stars run the sampler together and go on from the state
+ * after the stars. */
 template <int MODEL>
 __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
 {
@@ -252,7 +192,7 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
         it = __shfl_sync(BD_FULL, it, 0);
         if (it >= P.nitems) break;
         const uint32_t wi = P.items[it];
-        const int job = (int)(wi >> 16), t = (int)(wi & 0xffffu);
+        const int job = (int)(wi >> 16), t = (int)(wi & 0xffffu) + lane;
         const CrawlJob &J = P.jobs[job];
         if (job != loaded) {
             __syncwarp();
@@ -281,20 +221,17 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
         }
         const int NS = J.rng_nstreams;
         uint32_t *rng = J.rng;
-        const uint32_t a = rng[t];
-        uint64_t v = ((uint64_t)rng[NS + t] << 32) | rng[2 * NS + t];
-        const uint64_t *jlo = P.jt.lo + (size_t)t * 32, *jhi = P.jt.hi + (size_t)t * GF_JUMP_HI;
-        const uint64_t pmod = ((uint64_t)a << 32) - 1;
+        const bool stream_ok = t < N;
+        const uint32_t a = stream_ok ? rng[t] : 0u;
+        uint64_t w = stream_ok ? (((uint64_t)rng[NS + t] << 32) | rng[2 * NS + t]) : 0ull;
         const int sid = (job << 16) | t;
-        /* block r of the stream is the stream's (t + r N)-th global block */
-        const long long g0 = (long long)t + (long long)N * lane;
-        int pix = (int)(g0 / Bp), lb = (int)(g0 - (long long)pix * Bp);
-        const long long stepw = 32ll * N;
-        const int QW = (int)(stepw / Bp), RW = (int)(stepw - (long long)QW * Bp);
+        /* block r of stream t is the (t + r N)-th block of the request */
+        int pix = stream_ok ? t / Bp : npix, lb = stream_ok ? t - (t / Bp) * Bp : 0;
+        const int QN = N / Bp, RN = N - QN * Bp;
         int nst = 0;
-        bool stop = false;
+        bool stop = !stream_ok;
         for (;;) {
-            const bool valid = pix < npix;
+            const bool valid = !stop && pix < npix;
             if (!__any_sync(BD_FULL, valid)) break;
             float mu[GF_BLOCK];
             uint32_t live = 0;
@@ -331,18 +268,13 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
 #pragma unroll
                 for (int s = 0; s < GF_BLOCK; s++) mu[s] = 0.f;
             }
-            /* each lane's start state if no earlier bin of the window has stars */
-            const int cnt = __popc(live);
-            const int inc = bd_incl_scan(cnt, lane);
-            uint64_t wst = bd_jump(v, inc - cnt, jlo, jhi, a, pmod);
-            uint32_t act = live;
+            uint32_t todo = live;
             for (;;) {
+                /* walk the lane's remaining bins up to the first with stars */
                 int ev_s = -1;
-                uint64_t w = wst, wb_ev = 0;
+                uint64_t wb_ev = 0;
                 float mu_ev = 0.f;
-                uint32_t todo = act;
                 for (;;) {
-                    /* the next bin that is not surely empty, then the exact test once */
                     int c = -1;
                     uint64_t cwb = 0;
                     float cu = 0.f, cmu = 0.f;
@@ -354,55 +286,64 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                             if (!bd_surely_empty(u, mu[s])) { c = s; cwb = wb; cu = u; cmu = mu[s]; }
                         }
                     }
-                    if (c < 0) break;
+                    if (c < 0) { todo = 0; break; }
+                    todo &= ~((2u << c) - 1u);
                     if (bd_has_stars(cu, cmu)) {
                         ev_s = c;
                         wb_ev = cwb;
                         mu_ev = cmu;
                         break;
                     }
-                    todo &= ~((2u << c) - 1u);
                 }
-                const unsigned evm = __ballot_sync(BD_FULL, ev_s >= 0);
-                if (!evm) {
-                    v = bd_shfl64(w, 31);
-                    break;
+                const bool ev = ev_s >= 0;
+                if (!__any_sync(BD_FULL, ev)) break;
+                int k = 0;
+                uint64_t v_star = 0;
+                int ei = 0, ej = 0;
+                if (ev) {
+                    if (!(mu_ev < 3.0e38f)) {
+                        /* an infinite expected count would never leave the sampler's gamma loop */
+                        atomicOr(P.err, 1ull);
+                        stop = true;
+                        todo = 0;
+                    } else {
+                        k = draw_event(a, wb_ev, mu_ev, pixels + pix, w, v_star);
+                        ei = i0; ej = j0;
+                        for (int s = 1; s <= ev_s; s++) gfc::step_in_pixel(ei, ej, x, y);
+                    }
                 }
-                const int fl = __ffs(evm) - 1;
-                uint64_t vnew = 0, mult = 0;
-                int flag = 0;
-                if (lane == fl)
-                    flag = draw_event(P, evb, nev, a, jlo, jhi, pmod, wb_ev, mu_ev, sid, pix, i0, j0, ev_s, x, y,
-                                      pixels, nst, vnew, mult);
-                flag = __shfl_sync(BD_FULL, flag, fl);
-                if (flag) {
-                    stop = true;
-                    break;
-                }
-                vnew = bd_shfl64(vnew, fl);
-                mult = bd_shfl64(mult, fl);
-                nst = __shfl_sync(BD_FULL, nst, fl);
-                /* continue after the bin with stars */
-                if (lane < fl) {
-                    act = 0u;
-                } else if (lane == fl) {
-                    const int lo = ev_s + 1;
-                    act = lo >= GF_BLOCK ? 0u : ((act >> lo) << lo);
-                    wst = vnew;
-                } else {
-                    wst = gfr::mwc_mulmod_scaled(mult, wst, a, pmod);
+                /* stage the bins with stars (all lanes converged) */
+                const bool rec = ev && k > 0;
+                const unsigned rm = __ballot_sync(BD_FULL, rec);
+                if (rm) {
+                    if (*nev + __popc(rm) > GF_EVBUF) flush_events(P, evb, nev, lane);
+                    if (rec) {
+                        EventRecord e;
+                        e.stream = sid;
+                        e.ilb = pix;
+                        e.im = (int16_t)ei;
+                        e.iM = (int16_t)ej;
+                        e.k = k;
+                        e.nstars = nst;
+                        e.pad = 0;
+                        e.v_star = v_star;
+                        evb[*nev + __popc(rm & ((1u << lane) - 1u))] = e;
+                        nst += k;
+                    }
+                    __syncwarp();
+                    if (lane == 0) *nev += __popc(rm);
+                    __syncwarp();
                 }
             }
-            if (stop) break;
-            __syncwarp();
             if (*nev >= GF_EVBUF / 2) flush_events(P, evb, nev, lane);
-            pix += QW;
-            lb += RW;
+            /* the stream's next block: N blocks further */
+            pix += QN;
+            lb += RN;
             if (lb >= Bp) { lb -= Bp; pix++; }
         }
-        if (!stop && lane == 0) {
-            rng[NS + t] = (uint32_t)(v >> 32);
-            rng[2 * NS + t] = (uint32_t)v;
+        if (stream_ok && !stop) {
+            rng[NS + t] = (uint32_t)(w >> 32);
+            rng[2 * NS + t] = (uint32_t)w;
         }
     }
     flush_events(P, evb, nev, lane);

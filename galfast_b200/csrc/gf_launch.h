@@ -185,10 +185,9 @@ struct BatchDrawParams {
     const CrawlJob *jobs;
     const unsigned char *const *plans;   /* per request */
     float *const *ms;              /* per request: slot densities */
-    const uint32_t *items;         /* (request << 16) | stream */
+    const uint32_t *items;         /* (request << 16) | first of 32 consecutive streams */
     int32_t nitems;
     uint32_t *next_item;           /* work-queue counter */
-    JumpTables jt;
     EventRecord *ev;
     int64_t ev_capacity;
     unsigned long long *ev_count;  /* events found (may exceed the capacity) */

@@ -183,6 +183,7 @@ struct MultiWS {
     Grow<int32_t> joblist, chunkoff;
     Grow<EventRecord> ev;
     Grow<int64_t> k64, off64;
+    Grow<uint32_t> gitems;                  /* batched draw: (request << 16) | first of 32 streams */
     gf_table out;
     gf_table out2;                          /* host delivery: passes alternate between out and out2 */
     HostGrow<char> h_stage;              /* page-locked staging of uploads and downloads */
@@ -905,7 +906,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                 SD.job_list = ws.joblist.p; SD.pix_off = ws.chunkoff.p;
                 SD.njobs = (int32_t)jl.size(); SD.total_pix = tp;
                 {
-                    ProfScope ps(ctx, GF_PROF_DRAW_WINDOW);
+                    ProfScope ps(ctx, GF_PROF_SLOTS);
                     GF_CUDA(gfk::launch_slot_density(SD, mtype, st));
                 }
                 gfk::BatchDrawParams B;
@@ -913,7 +914,20 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                 if (gfk::batch_draw_warp_bytes(max_tab(i, batched), &B) > 200 * 1024)
                     return fail(GF_E_UNSUPPORTED, "magnitude grid too large for the batched draw");
                 B.jobs = d_jobs; B.plans = ws.plans.p; B.ms = ws.msptr.p;
-                B.items = d_items; B.nitems = nitems; B.next_item = d_counter; B.jt = ctx->jt;
+                /* work items: 32 consecutive streams of a request, requests in decreasing size */
+                const int ngroups = (N + 31) / 32;
+                GF_TRY(ws.gitems.need((size_t)batched.size() * ngroups));
+                {
+                    GF_TRY(ws.h_stage.need(4 * batched.size() * (size_t)ngroups));
+                    uint32_t *gi = (uint32_t *)ws.h_stage.p;
+                    size_t q = 0;
+                    for (int j : batched)
+                        for (int g = 0; g < ngroups; g++) gi[q++] = ((uint32_t)j << 16) | (uint32_t)(32 * g);
+                    GF_CUDA(cudaMemcpyAsync(ws.gitems.p, gi, 4 * q, cudaMemcpyHostToDevice, st));
+                    GF_CUDA(cudaStreamSynchronize(st));
+                }
+                const int32_t ngitems = (int32_t)(batched.size() * (size_t)ngroups);
+                B.items = ws.gitems.p; B.nitems = ngitems; B.next_item = d_counter;
                 B.ev_count = ctx->d_counters; B.err = ctx->d_counters + 2;
                 GF_TRY(ws.ev.need((size_t)cap));
                 B.ev = ws.ev.p; B.ev_capacity = (int64_t)ws.ev.n;
@@ -921,7 +935,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                     /* autotuner: time 8, 4, 2 and 1 warps per CTA on the head of the work queue
                      * (the largest requests), from the same stream states, and keep the fastest */
                     gfk::BatchDrawParams T = B;
-                    T.nitems = std::min<int32_t>(nitems, std::max<int32_t>(nitems / 16, 148 * 64));
+                    T.nitems = std::min<int32_t>(ngitems, std::max<int32_t>(ngitems / 16, 148 * 8));
                     float best_ms = 0.f;
                     int best = 4;
                     cudaEvent_t e0, e1;
@@ -969,7 +983,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                 int64_t *d_total = (int64_t *)(ctx->d_counters + 1);
                 for (;;) {
                     {
-                        ProfScope ps(ctx, GF_PROF_PLACE);
+                        ProfScope ps(ctx, GF_PROF_EXPAND);
                         GF_CUDA(gfk::launch_expand_events(ws.ev.p, nev, d_jobs, ws.k64.p, ws.off64.p, temp.p, temp.n, rec.p,
                                                           (int64_t)rec.n, d_total, st));
                     }

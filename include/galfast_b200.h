@@ -249,7 +249,10 @@ int64_t gf_launch_count(void);
 enum {
     GF_PROF_INTEGRATE = 0, GF_PROF_DRAW_WINDOW = 1, GF_PROF_DRAW_RERUN = 2, GF_PROF_PLACE = 3,
     GF_PROF_SORT = 4, GF_PROF_CLIPPER = 5, GF_PROF_FEH = 6, GF_PROF_BOND2010 = 7, GF_PROF_PHOTOMETRY = 8,
-    GF_PROF_PHOTOERR = 9, GF_PROF_VEL2PM = 10, GF_PROF_GAL2OTHER = 11, GF_PROF_NPHASES = 12
+    GF_PROF_PHOTOERR = 9, GF_PROF_VEL2PM = 10, GF_PROF_GAL2OTHER = 11,
+    GF_PROF_SLOTS = 12,          /* batched draw: model density at the slot distances of each pixel */
+    GF_PROF_EXPAND = 13,         /* batched draw: star records of the bins with stars */
+    GF_PROF_NPHASES = 14
 };
 gf_status gf_profile_enable(gf_ctx *ctx, int32_t on);
 gf_status gf_profile_read(gf_ctx *ctx, double *ms, int64_t *launches);
