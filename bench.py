@@ -281,8 +281,14 @@ def reduce_max_sum(dist, tmax, tsum):
     return float(a[0]), float(b[0])
 
 
+# DRAM bytes per bin of batch_draw_kernel: (325.05 + 220.28) MB over 4.34e9 bins in the ncu
+# capture of profiles/batch_draw_kernel_config4_64req.md; traffic grows with the bins (the
+# per-pixel slot rows and plan tables are read once per block, the events once per star)
+DRAW_TRAFFIC_PER_BIN = 545.33e6 / 4.3396e9
+
+
 def draw_rooflines(pk, pk_kind, bins, diags, stars_step, npix_models, draw_ms, draw_launches, nsteps):
-    """HBM roofline of the draw crawl (algorithmic bytes: star records written and
+    """HBM roofline of the batched draw (algorithmic bytes: star records written and
     beams read) and its issue roofline (per-bin / per-diagonal / per-star work of
     the reference kernel against nominal B200 FP32, SFU and FP64 rates)."""
     fp32 = 6.0 * bins + 60.0 * diags + 250.0 * stars_step
@@ -296,7 +302,9 @@ def draw_rooflines(pk, pk_kind, bins, diags, stars_step, npix_models, draw_ms, d
     achieved = bytes_alg / t_draw / 1e9 if t_draw == t_draw else None
     roofline = {"bound": "hbm", "kernel": "batch_draw_kernel (draw pass)", "achieved": achieved,
                 "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": (achieved / pk["hbm_gbs"]) if achieved else None,
-                "traffic": None, "peak_source": pk_kind,
+                "traffic": DRAW_TRAFFIC_PER_BIN * bins * nsteps / max(draw_launches, 1),
+                "traffic_note": "scaled from the 64-request ncu capture by bins per launch",
+                "peak_source": pk_kind,
                 "algorithmic_bytes_per_launch": bytes_alg * nsteps / max(draw_launches, 1),
                 "avg_launch_ms": draw_ms / max(draw_launches, 1)}
     compute = {"bound": "sfu/fp32 issue (nominal)", "kernel": "batch_draw_kernel (draw pass)",
@@ -399,10 +407,18 @@ def bench_multi(args, G, W, ctx, rank, world, dist):
 
     pk, pk_kind = peaks()
     bins, diags = set_bins(ws)
-    draw_ms = prof.get("draw_window", (0, 0))[0]
-    draw_launches = prof.get("draw_window", (0, 0))[1]
-    roofline, compute = draw_rooflines(pk, pk_kind, bins, diags, generated, nmod * sum(w.npixels for w in ws),
+    # the batched draw's share: requests whose stars fit one batch (the others take the plain path)
+    capd = float(C4_CAPACITY)
+    batched = [j for j in range(n)
+               if max(st_e + 8.0 * np.sqrt(max(st_e, 0.0)) + 1024.0 for st_e in list(stats[j].expected)[:nmod]) < capd]
+    bb = sum(model_bins(ws[j])[0] for j in batched)
+    bd = sum(model_bins(ws[j])[1] for j in batched)
+    bstars = sum(stats[j].generated[i] for j in batched for i in range(nmod))
+    draw_ms = prof.get("batch_draw", (0, 0))[0]
+    draw_launches = prof.get("batch_draw", (0, 0))[1]
+    roofline, compute = draw_rooflines(pk, pk_kind, bb, bd, bstars, nmod * sum(ws[j].npixels for j in batched),
                                        draw_ms, draw_launches, args.steps)
+    roofline["batched_requests"] = len(batched)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:

@@ -142,7 +142,7 @@ COLUMNS = [  # name, dtype, components (or "bands")
     ("pm", np.float32, 3), ("radec", np.float64, 2),
 ]
 PROFILE_PHASES = ["integrate", "draw_window", "draw_rerun", "place", "sort", "clipper", "fixedfeh", "bond2010",
-                  "photometry", "photoerrors", "vel2pm", "gal2other", "slot_density", "expand"]
+                  "photometry", "photoerrors", "vel2pm", "gal2other", "slot_density", "expand", "batch_draw"]
 SKYGEN_COLUMNS = ["lb", "projIdx", "projXY", "DM", "absmag", "XYZ", "comp", "Am", "AmInf", "hidden"]
 
 

@@ -29,8 +29,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <atomic>
 #include <cstring>
 #include <deque>
+#include <thread>
 #include <map>
 #include <tuple>
 #include <vector>
@@ -57,6 +59,24 @@ struct Pool {
         for (void *p : ptrs) cudaFree(p);
     }
 };
+
+/* fn(0) .. fn(n - 1) on up to 32 host threads (items taken in order from a shared counter) */
+template <class F>
+void parallel_for(int n, F fn)
+{
+    const int nt = std::max(1, std::min<int>({n / 16 + 1, (int)std::thread::hardware_concurrency(), 32}));
+    if (nt <= 1) {
+        for (int i = 0; i < n; i++) fn(i);
+        return;
+    }
+    std::atomic<int> next(0);
+    std::vector<std::thread> th;
+    for (int k = 0; k < nt; k++)
+        th.emplace_back([&] {
+            for (int i = next++; i < n; i = next++) fn(i);
+        });
+    for (auto &t : th) t.join();
+}
 
 /* a buffer that only grows */
 template <typename T>
@@ -421,18 +441,24 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         S[j].norm = 1.f;
     }
 
-    /* ---- host set-up of every request ---- */
+    /* ---- host set-up of every request (models and module signatures on host threads) ---- */
     std::vector<ReqInfo> R(njobs);
     int64_t pix_total = 0;
     std::map<std::string, int> groups;          /* module-table signature -> group */
     std::vector<int> group_rep;                 /* a request of each group */
-    for (int j = 0; j < njobs; j++) {
+    std::vector<std::string> errs(njobs), sigs(njobs);
+    parallel_for(njobs, [&](int j) {
         const gf_job &J = jobs[j];
         ReqInfo &q = R[j];
         q.mc.assign(J.models, J.models + nmod);
         std::stable_sort(q.mc.begin(), q.mc.end(), [](const gf_model_config &a, const gf_model_config &b) { return a.comp < b.comp; });
-        std::string err;
-        if (!gfh::setup_models(J.sky, J.npixels, q.mc.data(), nmod, q.hm, err)) return fail(GF_E_INVALID, err);
+        if (!gfh::setup_models(J.sky, J.npixels, q.mc.data(), nmod, q.hm, errs[j]) && errs[j].empty()) errs[j] = "invalid model";
+        sigs[j] = module_signature(J);
+    });
+    for (int j = 0; j < njobs; j++) {
+        const gf_job &J = jobs[j];
+        ReqInfo &q = R[j];
+        if (!errs[j].empty()) return fail(GF_E_INVALID, errs[j]);
         for (int i = 0; i < nmod; i++) {
             if (q.hm[i].m.type != R[0].hm[i].m.type)
                 return fail(GF_E_INVALID, "model kinds must agree across requests (in component order)");
@@ -443,7 +469,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         q.pix_off = pix_total;
         pix_total += J.npixels;
         q.cost = (double)J.npixels * q.hm[0].m.nm;
-        const std::string key = module_signature(J);
+        const std::string &key = sigs[j];
         auto it = groups.find(key);
         if (it == groups.end()) {
             it = groups.insert({key, (int)groups.size()}).first;
@@ -472,13 +498,13 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         gf_pencil_beam *hp = (gf_pencil_beam *)h;
         float *ha = (float *)(h + pb), *hl = (float *)(h + pb + ab);
         memset(hl, 0, lb_);
-        for (int j = 0; j < njobs; j++) {
+        parallel_for(njobs, [&](int j) {
             memcpy(hp + R[j].pix_off, jobs[j].pixels, sizeof(gf_pencil_beam) * (size_t)jobs[j].npixels);
             if (jobs[j].beam_ammin) memcpy(ha + R[j].pix_off, jobs[j].beam_ammin, 4 * (size_t)jobs[j].npixels);
             else memset(ha + R[j].pix_off, 0, 4 * (size_t)jobs[j].npixels);
             for (int i = 0; i < nmod; i++)
                 std::copy(R[j].hm[i].lf.begin(), R[j].hm[i].lf.end(), hl + ((size_t)j * nmod + i) * 1024);
-        }
+        });
         GF_CUDA(cudaMemcpyAsync(d_pix, hp, pb, cudaMemcpyHostToDevice, st));
         GF_CUDA(cudaMemcpyAsync(d_ammin, ha, ab, cudaMemcpyHostToDevice, st));
         GF_CUDA(cudaMemcpyAsync(d_lf, hl, lb_, cudaMemcpyHostToDevice, st));
@@ -961,7 +987,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                 for (;;) {
                     GF_CUDA(cudaMemsetAsync(ctx->d_counters, 0, 24, st));
                     {
-                        ProfScope ps(ctx, GF_PROF_DRAW_WINDOW);
+                        ProfScope ps(ctx, GF_PROF_BATCH_DRAW);
                         GF_CUDA(gfk::launch_batch_draw(B, mtype, ctx->draw_cw[mtype], st));
                     }
                     GF_CUDA(cudaMemcpyAsync(ctx->h_counters, ctx->d_counters, 24, cudaMemcpyDeviceToHost, st));

@@ -252,7 +252,8 @@ enum {
     GF_PROF_PHOTOERR = 9, GF_PROF_VEL2PM = 10, GF_PROF_GAL2OTHER = 11,
     GF_PROF_SLOTS = 12,          /* batched draw: model density at the slot distances of each pixel */
     GF_PROF_EXPAND = 13,         /* batched draw: star records of the bins with stars */
-    GF_PROF_NPHASES = 14
+    GF_PROF_BATCH_DRAW = 14,     /* batched draw: the Poisson draw of every stream (one launch per model pass) */
+    GF_PROF_NPHASES = 15
 };
 gf_status gf_profile_enable(gf_ctx *ctx, int32_t on);
 gf_status gf_profile_read(gf_ctx *ctx, double *ms, int64_t *launches);
