@@ -143,12 +143,28 @@ __device__ __noinline__ int draw_event(uint32_t a, uint64_t wb, float mu, const 
     return k;
 }
 
+/* stage one event from divergent code (any lanes of the warp) */
+__device__ __forceinline__ void stage_event(const BatchDrawParams &P, EventRecord *evb, int *nev, const EventRecord &e)
+{
+    const int q = atomicAdd(nev, 1);
+    if (q < GF_EVBUF) {
+        evb[q] = e;
+    } else {
+        const unsigned long long sl = atomicAdd(P.ev_count, 1ull);
+        if (sl < (unsigned long long)P.ev_capacity) P.ev[sl] = e;
+    }
+}
+
 /* write the warp's staged events to the global list (all lanes) */
 __device__ __forceinline__ void flush_events(const BatchDrawParams &P, EventRecord *evb, int *nev, int lane)
 {
     __syncwarp();
-    const int n = *nev;
-    if (n == 0) return;
+    const int n = *nev < GF_EVBUF ? *nev : GF_EVBUF;     /* events past the buffer went straight to the list */
+    if (n == 0) {
+        if (lane == 0) *nev = 0;
+        __syncwarp();
+        return;
+    }
     unsigned long long base = 0;
     if (lane == 0) base = atomicAdd(P.ev_count, (unsigned long long)n);
     base = __shfl_sync(BD_FULL, base, 0);
@@ -157,6 +173,32 @@ __device__ __forceinline__ void flush_events(const BatchDrawParams &P, EventReco
     __syncwarp();
     if (lane == 0) *nev = 0;
     __syncwarp();
+}
+
+/* Per request of a chunk and block of its grid: the largest LF value over the
+ * block's 10 bins (the same LF(M) samples the draw's shared table holds). */
+__global__ void __launch_bounds__(256) block_lfmax_kernel(BlockLfParams P)
+{
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < P.total; f += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = P.njobs;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (P.blk_off[mid] <= f) lo = mid; else hi = mid;
+        }
+        const int job = P.job_list[lo];
+        const int b = (int)(f - P.blk_off[lo]);
+        const SkyModel &m = P.jobs[job].m;
+        const unsigned char *plan = P.plans[job];
+        const IntegPlanHdr *h = (const IntegPlanHdr *)plan;
+        const uint32_t bij = plan_at<uint32_t>(plan, h->off_blk)[b];
+        int i = (int)(bij & 0xffffu), j = (int)(bij >> 16);
+        float mx = gfc::lf_sample(m, m.lf, m.M1 - (float)j * m.dM);
+        for (int s = 1; s < GF_BLOCK; s++) {
+            gfc::step_in_pixel(i, j, m.nm, m.nM);
+            mx = fmaxf(mx, gfc::lf_sample(m, m.lf, m.M1 - (float)j * m.dM));
+        }
+        P.lfmax[job][b] = mx;
+    }
 }
 
 /* One warp per 32 consecutive streams of a request, one lane per stream.  Lane L
@@ -180,11 +222,12 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
     int loaded = -1;
     const uint32_t *blk = nullptr;
     const uint16_t *bslot = nullptr, *dslot = nullptr;
-    const float *slotD = nullptr, *msbase = nullptr;
+    const float *slotD = nullptr, *msbase = nullptr, *lfmx = nullptr;
+    const uint32_t *binfo = nullptr;
     const gf_pencil_beam *pixels = nullptr;
     int nslots = 0, Bp = 1, npix = 0, x = 1, y = 1, N = 1;
     float norm = 0.f, dmin = 0.f, dmax = 0.f;
-    bool dlim = false;
+    bool dlim = false, bound = false;
 
     for (;;) {
         int it = 0;
@@ -216,6 +259,10 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
             dmin = m.dmin;
             dmax = m.dmax;
             dlim = m.dmin != 0.f || m.dmax != 0.f;
+            binfo = plan_at<uint32_t>(plan, h->off_binfo);
+            lfmx = P.lfmax ? P.lfmax[job] : nullptr;
+            /* the block bound needs non-negative densities (f >= 0) and normalisation */
+            bound = lfmx && !dlim && m.f >= 0.f && m.norm >= 0.f;
             __syncwarp();
             loaded = job;
         }
@@ -233,6 +280,115 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
         for (;;) {
             const bool valid = !stop && pix < npix;
             if (!__any_sync(BD_FULL, valid)) break;
+            if (bound) {
+                /* Upper bound of the block's expected counts: the reference's float product
+                 * with each factor at its largest over the block (correctly rounded products of
+                 * non-negative factors are monotone).  u <= 1 - bound - 3e-7 proves a bin
+                 * empty; only the bins whose uniform exceeds it need their exact mu. */
+                uint32_t live = 0, cand = 0;
+                int i0 = 0, j0 = 0, sl0 = 0;
+                float K = 0.f, thr = 0.f;
+                const float *msr = msbase;
+                const uint64_t w0 = w;
+                if (valid) {
+                    const uint32_t bij = __ldg(blk + lb);
+                    i0 = (int)(bij & 0xffffu);
+                    j0 = (int)(bij >> 16);
+                    const uint32_t bi = __ldg(binfo + lb);
+                    const int imax = (int)(bi & 0xffffu);
+                    const uint32_t wm = (bi >> 16) & 0x3ffu;
+                    sl0 = __ldg(bslot + lb);
+                    msr = msbase + (size_t)pix * (nslots + 2);
+                    const int icut = __float_as_int(msr[nslots]);
+                    K = msr[nslots + 1];
+                    float msmax = msr[sl0], Dmax = __ldg(slotD + sl0);
+                    int d = i0 + j0;
+                    for (uint32_t mm = wm; mm; mm &= mm - 1u) {
+                        d++;
+                        const int sl = __ldg(dslot + d);
+                        msmax = fmaxf(msmax, msr[sl]);
+                        Dmax = fmaxf(Dmax, __ldg(slotD + sl));
+                    }
+                    float mub = fmaxf(__ldg(lfmx + lb), 0.f) * msmax;
+                    mub *= norm;
+                    mub *= Dmax * Dmax * Dmax;
+                    mub *= K;
+                    thr = (1.0f - mub) - 3.0e-7f;
+                    if (imax < icut) {
+                        live = (1u << GF_BLOCK) - 1u;
+                    } else {
+                        int ii = i0, dd = i0 + j0;
+                        live = ii < icut ? 1u : 0u;
+                        for (int s = 1; s < GF_BLOCK; s++) {
+                            if ((wm >> s) & 1u) {
+                                dd++;
+                                ii = dd - (y - 1) > 0 ? dd - (y - 1) : 0;
+                            } else {
+                                ii++;
+                            }
+                            live |= ii < icut ? (1u << s) : 0u;
+                        }
+                    }
+#pragma unroll
+                    for (int s = 0; s < GF_BLOCK; s++) {
+                        if ((live >> s) & 1u) {
+                            const float u = bd_mwc_step(w, a);
+                            if (!(u <= thr)) cand |= 1u << s;
+                        }
+                    }
+                }
+                if (cand) {
+                    /* the block again in order from its first state, exact where the bound fails */
+                    w = w0;
+                    int i = i0, j = j0, slot = sl0;
+                    float ms = msr[slot], D = __ldg(slotD + slot);
+                    float D3 = D * D * D;
+                    for (int s = 0; s < GF_BLOCK; s++) {
+                        if (s > 0 && gfc::step_in_pixel(i, j, x, y)) {
+                            slot = __ldg(dslot + i + j);
+                            ms = msr[slot];
+                            D = __ldg(slotD + slot);
+                            D3 = D * D * D;
+                        }
+                        if (!((live >> s) & 1u)) continue;
+                        const uint64_t wb = w;
+                        const float u = bd_mwc_step(w, a);
+                        if (u <= thr) continue;
+                        float r = LFM[j] * ms;
+                        r *= norm;
+                        r *= D3;
+                        r *= K;
+                        if (bd_surely_empty(u, r) || !bd_has_stars(u, r)) continue;
+                        if (!(r < 3.0e38f)) {
+                            /* an infinite expected count would never leave the sampler's gamma loop */
+                            atomicOr(P.err, 1ull);
+                            stop = true;
+                            break;
+                        }
+                        uint64_t v_star = 0;
+                        const int k = draw_event(a, wb, r, pixels + pix, w, v_star);
+                        if (k > 0) {
+                            EventRecord e;
+                            e.stream = sid;
+                            e.ilb = pix;
+                            e.im = (int16_t)i;
+                            e.iM = (int16_t)j;
+                            e.k = k;
+                            e.nstars = nst;
+                            e.pad = 0;
+                            e.v_star = v_star;
+                            stage_event(P, evb, nev, e);
+                            nst += k;
+                        }
+                    }
+                }
+                __syncwarp();
+                if (*nev >= GF_EVBUF / 2) flush_events(P, evb, nev, lane);
+                pix += QN;
+                lb += RN;
+                if (lb >= Bp) { lb -= Bp; pix++; }
+                continue;
+            }
             float mu[GF_BLOCK];
             uint32_t live = 0;
             int i0 = 0, j0 = 0;
@@ -316,7 +472,7 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                 const bool rec = ev && k > 0;
                 const unsigned rm = __ballot_sync(BD_FULL, rec);
                 if (rm) {
-                    if (*nev + __popc(rm) > GF_EVBUF) flush_events(P, evb, nev, lane);
+                    if (*nev + __popc(rm) > GF_EVBUF) flush_events(P, evb, nev, lane);      /* leaves *nev = 0 */
                     if (rec) {
                         EventRecord e;
                         e.stream = sid;
@@ -404,6 +560,15 @@ cudaError_t launch_slot_density(const SlotDensityParams &P, int model_type, cuda
         slot_density_kernel<GF_MODEL_EXP_DISK><<<blocks, 256, 0, s>>>(P);
     else
         slot_density_kernel<GF_MODEL_POWER_LAW_ELLIPSOID><<<blocks, 256, 0, s>>>(P);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_block_lfmax(const BlockLfParams &P, cudaStream_t s)
+{
+    if (P.total <= 0) return cudaSuccess;
+    const int blocks = (int)std::min<long long>((P.total + 255) / 256, (long long)sm_count() * 16);
+    block_lfmax_kernel<<<blocks, 256, 0, s>>>(P);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -124,6 +124,8 @@ __host__ __device__ inline void plan_layout(int nm, int nM, int max_anchors, int
     off += (2 * nb + 15) & ~15ll;
     h.off_dslot = (int32_t)off;
     off += (2 * nd + 15) & ~15ll;
+    h.off_binfo = (int32_t)off;
+    off += (4 * nb + 15) & ~15ll;
     h.nd = (int32_t)nd;
     h.nblocks = (int32_t)nb;
     h.max_anchors = max_anchors;
@@ -132,7 +134,7 @@ __host__ __device__ inline void plan_layout(int nm, int nM, int max_anchors, int
     h.nanchors = 0;
     h.nslots = 0;
     h.ok = 0;
-    h.pad[0] = h.pad[1] = h.pad[2] = 0;
+    h.pad[0] = h.pad[1] = 0;
 }
 
 __global__ void __launch_bounds__(1024) plan_kernel(const IntegPlanDesc *desc)
@@ -178,11 +180,62 @@ __global__ void __launch_bounds__(1024) plan_kernel(const IntegPlanDesc *desc)
         base_s += ts;
     }
     overflow = __syncthreads_or(overflow);
+    /* per block: its largest m row and its diagonal starts, from the block-start bins above */
+    if (!overflow) {
+        uint32_t *binfo = (uint32_t *)(plan + h.off_binfo);
+        for (int b = threadIdx.x; b < h.nblocks; b += blockDim.x) {
+            const uint32_t bij = blk[b];
+            int i = (int)(bij & 0xffffu), j = (int)(bij >> 16);
+            int imax = i;
+            uint32_t wm = 0;
+            for (int s = 1; s < GF_BLOCK; s++) {
+                if (gfc::step_in_pixel(i, j, x, y)) wm |= 1u << s;
+                imax = i > imax ? i : imax;
+            }
+            binfo[b] = (uint32_t)imax | (wm << 16);
+        }
+    }
     if (threadIdx.x == 0) {
         h.nanchors = base_a;
         h.nslots = base_s;
         h.ok = overflow ? 0 : 1;
         *(IntegPlanHdr *)plan = h;
+    }
+}
+
+/* The lane's diagonals d = lane, lane + 32, ... of one pixel: every uncut bin's mu
+ * from its anchor slot, summed in FP64 (and, when COV, mu * cf as well). */
+template <bool COV>
+__device__ __forceinline__ void walk_diagonals(int lane, int nd, int x, int y, int icut, const int2 *diag,
+                                               const uint16_t *anc, const float *LFM, const float2 *Q, float norm,
+                                               float K, float cf, double &cnt, double &cov)
+{
+    for (int d = lane; d < nd; d += 32) {
+        const int i0 = d - (y - 1) > 0 ? d - (y - 1) : 0;
+        int i1 = d < x - 1 ? d : x - 1;
+        i1 = i1 < icut - 1 ? i1 : icut - 1;
+        if (i1 < i0) continue;
+        const int2 dg = diag[d];
+        const uint16_t *ap = anc + dg.x;
+        const float *lf = LFM + (d - i0);           /* LF of bin t of the diagonal: lf[-t] */
+        const int tl = i1 - i0 + 1;
+        int t = 0, seg_end = dg.y < tl ? dg.y : tl;
+        for (;;) {
+            const float2 q = Q[*ap++];
+            if (q.y >= 0.f) {
+                for (; t < seg_end; t++) {
+                    float mu = lf[-t] * q.x;
+                    mu *= norm;
+                    mu *= q.y;
+                    mu *= K;
+                    cnt += (double)mu;
+                    if (COV) cov += (double)(mu * cf);
+                }
+            }
+            t = seg_end;
+            if (t >= tl) break;
+            seg_end = t + GF_BLOCK < tl ? t + GF_BLOCK : tl;
+        }
     }
 }
 
@@ -268,32 +321,12 @@ __global__ void __launch_bounds__(256) integrate_pixels_kernel(IntegPixParams P)
         }
         __syncwarp();
         double cnt = 0.0, cov = 0.0;
-        for (int d = lane; d < nd; d += 32) {
-            const int i0 = d - (y - 1) > 0 ? d - (y - 1) : 0;
-            int i1 = d < x - 1 ? d : x - 1;
-            i1 = i1 < icut - 1 ? i1 : icut - 1;
-            if (i1 < i0) continue;
-            const int2 dg = diag[d];
-            const uint16_t *ap = anc + dg.x;
-            const float *lf = LFM + (d - i0);           /* LF of bin t of the diagonal: lf[-t] */
-            const int tl = i1 - i0 + 1;
-            int t = 0, seg_end = dg.y < tl ? dg.y : tl;
-            for (;;) {
-                const float2 q = Q[*ap++];
-                if (q.y >= 0.f) {
-                    for (; t < seg_end; t++) {
-                        float mu = lf[-t] * q.x;
-                        mu *= norm;
-                        mu *= q.y;
-                        mu *= K;
-                        cnt += (double)mu;
-                        cov += (double)(mu * cf);
-                    }
-                }
-                t = seg_end;
-                if (t >= tl) break;
-                seg_end = t + GF_BLOCK < tl ? t + GF_BLOCK : tl;
-            }
+        if (cf == 1.0f) {
+            /* fully covered pixel: mu * cf == mu, so the covered sum is the sum */
+            walk_diagonals<false>(lane, nd, x, y, icut, diag, anc, LFM, Q, norm, K, cf, cnt, cov);
+            cov = cnt;
+        } else {
+            walk_diagonals<true>(lane, nd, x, y, icut, diag, anc, LFM, Q, norm, K, cf, cnt, cov);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {

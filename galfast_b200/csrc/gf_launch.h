@@ -143,13 +143,17 @@ cudaError_t launch_precision(const SkyModel &m, const SkyGeom &g, const float *D
  *   uint16_t anc[]           slot of every anchor, diagonal by diagonal
  *   uint32_t blk[nblocks]    per block of 10 bins (local index 10 b): i | j << 16 of its first bin
  *   uint16_t bslot[nblocks]  slot of the block-start anchor
- *   uint16_t dslot[nd]       slot of each diagonal's first bin */
+ *   uint16_t dslot[nd]       slot of each diagonal's first bin
+ *   uint32_t binfo[nblocks]  per block: largest apparent-magnitude row im of its bins (bits 0-15)
+ *                            and which of its bins 1..9 start a diagonal (bits 16-25) */
 struct IntegPlanHdr {
     int32_t nd, nanchors, nslots, ok;      /* ok = 0: the plan did not fit its buffer */
     int32_t off_slot, off_anc;             /* byte offsets of the tables */
     int32_t max_anchors, max_slots;
     int32_t off_blk, off_bslot, off_dslot, nblocks;
-    int32_t bytes, pad[3];                 /* size of the plan buffer */
+    int32_t bytes;                         /* size of the plan buffer */
+    int32_t off_binfo;                     /* uint32_t binfo[nblocks]: largest m row of the block | diagonal starts << 16 */
+    int32_t pad[2];
 };
 struct IntegPlanDesc {
     const float *Dtab;             /* D[im][iM], rows of nM_tab */
@@ -181,10 +185,20 @@ struct SlotDensityParams {
     const int32_t *pix_off;        /* [njobs + 1] first flat pixel of each listed request */
     int32_t njobs, total_pix;
 };
+struct BlockLfParams {
+    const CrawlJob *jobs;
+    const unsigned char *const *plans;   /* per request */
+    float *const *lfmax;           /* per request: [nblocks] largest LF value of each block */
+    const int32_t *job_list;       /* requests of the launch */
+    const int64_t *blk_off;        /* [njobs + 1] first flat block of each listed request */
+    int32_t njobs;
+    int64_t total;
+};
 struct BatchDrawParams {
     const CrawlJob *jobs;
     const unsigned char *const *plans;   /* per request */
     float *const *ms;              /* per request: slot densities */
+    float *const *lfmax;           /* per request: per-block LF maxima (null: exact test for every bin) */
     const uint32_t *items;         /* (request << 16) | first of 32 consecutive streams */
     int32_t nitems;
     uint32_t *next_item;           /* work-queue counter */
@@ -195,6 +209,7 @@ struct BatchDrawParams {
     int32_t off_tab, off_ev, warp_bytes;   /* per-warp shared-memory layout (batch_draw_warp_bytes) */
 };
 cudaError_t launch_slot_density(const SlotDensityParams &P, int model_type, cudaStream_t s);
+cudaError_t launch_block_lfmax(const BlockLfParams &P, cudaStream_t s);
 size_t batch_draw_warp_bytes(int max_tab, BatchDrawParams *P);
 cudaError_t launch_batch_draw(const BatchDrawParams &P, int model_type, int warps_per_cta, cudaStream_t s);
 cudaError_t expand_temp_bytes(int64_t nev, size_t *bytes);

@@ -204,6 +204,9 @@ struct MultiWS {
     Grow<EventRecord> ev;
     Grow<int64_t> k64, off64;
     Grow<uint32_t> gitems;                  /* batched draw: (request << 16) | first of 32 streams */
+    Grow<float> lfmax;                      /* batched draw: per request and block, the largest LF value */
+    Grow<float *> lfmptr;
+    Grow<int64_t> blkoff;
     gf_table out;
     gf_table out2;                          /* host delivery: passes alternate between out and out2 */
     HostGrow<char> h_stage;              /* page-locked staging of uploads and downloads */
@@ -628,7 +631,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
     for (int j : order_all)
         if (!R[j].plain) integ.push_back(j);
     int32_t nitems = 0;
-    if (!integ.empty()) GF_TRY(upload_items(integ, &nitems));
+    bool items_integ = false;          /* per-stream items of the crawl integrate, uploaded when needed */
     /* pixel-by-pixel integrate: anchor plans per magnitude grid (nm * nM is a
      * multiple of 10 for every batched request) */
     std::map<std::tuple<float, float, float, float, int, int>, unsigned char *> plans;
@@ -725,6 +728,10 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         }
         if (!done) {
             /* the stream crawl (a grid whose plan does not fit) */
+            if (!items_integ) {
+                GF_TRY(upload_items(integ, &nitems));
+                items_integ = true;
+            }
             GF_CUDA(cudaMemsetAsync(d_counts, 0, 16 * nall, st));
             gfk::LaunchCrawlMulti L;
             memset(&L, 0, sizeof(L));
@@ -887,7 +894,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         for (int sl = 0; sl < nslots; sl++) job_slot[slot_job[sl]] = sl;
         GF_CUDA(cudaMemcpyAsync(d_job_slot, job_slot.data(), 4 * (size_t)njobs, cudaMemcpyHostToDevice, st));
         GF_CUDA(cudaMemcpyAsync(d_slot_job, slot_job.data(), 4 * (size_t)nslots, cudaMemcpyHostToDevice, st));
-        GF_TRY(upload_items(batched, &nitems));
+        bool items_chunk = false;      /* per-stream items of the crawl draw, uploaded when needed */
         int slot_bits = 1;
         while ((1 << slot_bits) < nslots) slot_bits++;
 
@@ -935,8 +942,34 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                     ProfScope ps(ctx, GF_PROF_SLOTS);
                     GF_CUDA(gfk::launch_slot_density(SD, mtype, st));
                 }
+                /* the largest LF value of every block of every request (bounds of the draw's test) */
+                {
+                    std::vector<float *> lp(njobs, nullptr);
+                    std::vector<int64_t> boff;
+                    int64_t nb_total = 0;
+                    for (int j : batched) {
+                        boff.push_back(nb_total);
+                        nb_total += (int64_t)R[j].hm[i].m.nm * R[j].hm[i].m.nM / GF_BLOCK;
+                    }
+                    boff.push_back(nb_total);
+                    GF_TRY(ws.lfmax.need((size_t)std::max<int64_t>(nb_total, 1)));
+                    for (size_t q = 0; q < batched.size(); q++) lp[batched[q]] = ws.lfmax.p + boff[q];
+                    GF_TRY(ws.lfmptr.need((size_t)njobs));
+                    GF_TRY(ws.blkoff.need(boff.size()));
+                    GF_CUDA(cudaMemcpyAsync(ws.lfmptr.p, lp.data(), sizeof(void *) * (size_t)njobs, cudaMemcpyHostToDevice, st));
+                    GF_CUDA(cudaMemcpyAsync(ws.blkoff.p, boff.data(), 8 * boff.size(), cudaMemcpyHostToDevice, st));
+                    gfk::BlockLfParams BL;
+                    BL.jobs = d_jobs; BL.plans = ws.plans.p; BL.lfmax = ws.lfmptr.p;
+                    BL.job_list = ws.joblist.p; BL.blk_off = ws.blkoff.p;
+                    BL.njobs = (int32_t)batched.size(); BL.total = nb_total;
+                    ProfScope ps(ctx, GF_PROF_SLOTS);
+                    GF_CUDA(gfk::launch_block_lfmax(BL, st));
+                    /* the host vectors are read by the copies above before they go out of scope */
+                    GF_CUDA(cudaStreamSynchronize(st));
+                }
                 gfk::BatchDrawParams B;
                 memset(&B, 0, sizeof(B));
+                B.lfmax = ws.lfmptr.p;
                 if (gfk::batch_draw_warp_bytes(max_tab(i, batched), &B) > 200 * 1024)
                     return fail(GF_E_UNSUPPORTED, "magnitude grid too large for the batched draw");
                 B.jobs = d_jobs; B.plans = ws.plans.p; B.ms = ws.msptr.p;
@@ -1020,6 +1053,10 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                     GF_TRY(rec.need((size_t)(nrec + nrec / 8 + 65536)));
                 }
             } else {
+                if (!items_chunk) {
+                    GF_TRY(upload_items(batched, &nitems));
+                    items_chunk = true;
+                }
                 for (;;) {
                     GF_TRY(rec.need((size_t)cap));
                     GF_CUDA(cudaMemsetAsync(cs_base, 0, cs_bytes, st));
