@@ -281,10 +281,10 @@ def reduce_max_sum(dist, tmax, tsum):
     return float(a[0]), float(b[0])
 
 
-# DRAM bytes per bin of batch_draw_kernel: (325.05 + 220.28) MB over 4.34e9 bins in the ncu
+# DRAM bytes per bin of batch_draw_kernel: (332.69 + 228.86) MB over 4.34e9 bins in the ncu
 # capture of profiles/batch_draw_kernel_config4_64req.md; traffic grows with the bins (the
 # per-pixel slot rows and plan tables are read once per block, the events once per star)
-DRAW_TRAFFIC_PER_BIN = 545.33e6 / 4.3396e9
+DRAW_TRAFFIC_PER_BIN = 561.55e6 / 4.3396e9
 
 
 def draw_rooflines(pk, pk_kind, bins, diags, stars_step, npix_models, draw_ms, draw_launches, nsteps):
