@@ -29,6 +29,7 @@ import math
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -198,8 +199,11 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=32, help="config5: requests per rate")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--clock-log", default=None, help="CSV of the SM clock samples taken during the timed region")
     ap.add_argument("--requests", type=int, default=C4_NREQ, help="config4: requests per step (a prefix of the set)")
     args = ap.parse_args()
+    global CLOCK_LOG
+    CLOCK_LOG = args.clock_log
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -263,9 +267,13 @@ def main():
     ctx.close()
 
 
+CLOCK_LOG = None                 # --clock-log: where the nvidia-smi samples of the timed region go
+
+
 def clock_sampler(rank):
-    d = os.path.join(ROOT, "gpurun_out")
-    return ClockSampler(os.path.join(d, "bench_clocks_rank%d.csv" % rank) if os.path.isdir(d) else "/tmp/bench_clocks.csv")
+    path = CLOCK_LOG or os.path.join(tempfile.gettempdir(), "bench_clocks.csv")
+    root, ext = os.path.splitext(path)
+    return ClockSampler("%s_rank%d%s" % (root, rank, ext or ".csv"))
 
 
 def reduce_max_sum(dist, tmax, tsum):
