@@ -210,6 +210,9 @@ __device__ __forceinline__ void walk_diagonals(int lane, int nd, int x, int y, i
                                                const uint16_t *anc, const float *LFM, const float2 *Q, float norm,
                                                float K, float cf, double &cnt, double &cov)
 {
+    /* two partial sums per quantity (even and odd bins of each run) halve the chain of
+     * dependent FP64 additions; they are added at the end, in a fixed order */
+    double c0 = 0.0, c1 = 0.0, v0 = 0.0, v1 = 0.0;
     for (int d = lane; d < nd; d += 32) {
         const int i0 = d - (y - 1) > 0 ? d - (y - 1) : 0;
         int i1 = d < x - 1 ? d : x - 1;
@@ -223,13 +226,28 @@ __device__ __forceinline__ void walk_diagonals(int lane, int nd, int x, int y, i
         for (;;) {
             const float2 q = Q[*ap++];
             if (q.y >= 0.f) {
-                for (; t < seg_end; t++) {
-                    float mu = lf[-t] * q.x;
-                    mu *= norm;
-                    mu *= q.y;
-                    mu *= K;
-                    cnt += (double)mu;
-                    if (COV) cov += (double)(mu * cf);
+                for (; t + 1 < seg_end; t += 2) {
+                    float m0 = lf[-t] * q.x, m1 = lf[-(t + 1)] * q.x;
+                    m0 *= norm;
+                    m1 *= norm;
+                    m0 *= q.y;
+                    m1 *= q.y;
+                    m0 *= K;
+                    m1 *= K;
+                    c0 += (double)m0;
+                    c1 += (double)m1;
+                    if (COV) {
+                        v0 += (double)(m0 * cf);
+                        v1 += (double)(m1 * cf);
+                    }
+                }
+                if (t < seg_end) {
+                    float m0 = lf[-t] * q.x;
+                    m0 *= norm;
+                    m0 *= q.y;
+                    m0 *= K;
+                    c0 += (double)m0;
+                    if (COV) v0 += (double)(m0 * cf);
                 }
             }
             t = seg_end;
@@ -237,6 +255,8 @@ __device__ __forceinline__ void walk_diagonals(int lane, int nd, int x, int y, i
             seg_end = t + GF_BLOCK < tl ? t + GF_BLOCK : tl;
         }
     }
+    cnt += c0 + c1;
+    if (COV) cov += v0 + v1;
 }
 
 /* One warp per pixel.  Per-warp shared tables: the request's model, LF at every
