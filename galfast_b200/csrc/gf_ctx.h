@@ -70,7 +70,7 @@ struct gf_ctx {
     int64_t multi_budget = 0;            /* device bytes per multi-request chunk (0: 60% of free memory) */
     MultiWS *multi_ws = nullptr;         /* buffers of gf_catalog_run_multi kept between calls */
     gf_table plain_table = {};           /* output table of gf_catalog_run, kept for the next call of the same shape */
-    int32_t draw_cw[3] = {0, 0, 0};      /* warps per CTA of the batched draw, by model kind (0: not tuned yet) */
+    int32_t draw_wpc[3] = {0, 0, 0};      /* warps per CTA of the batched draw, by model kind (0: not tuned yet) */
 };
 
 struct gf_photometry {

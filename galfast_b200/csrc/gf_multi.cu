@@ -990,7 +990,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                 B.ev_count = ctx->d_counters; B.err = ctx->d_counters + 2;
                 GF_TRY(ws.ev.need((size_t)cap));
                 B.ev = ws.ev.p; B.ev_capacity = (int64_t)ws.ev.n;
-                if (ctx->draw_cw[mtype] == 0) {
+                if (ctx->draw_wpc[mtype] == 0) {
                     /* autotuner: time 8, 4, 2 and 1 warps per CTA on the head of the work queue
                      * (the largest requests), from the same stream states, and keep the fastest */
                     gfk::BatchDrawParams T = B;
@@ -1013,7 +1013,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                     }
                     cudaEventDestroy(e0);
                     cudaEventDestroy(e1);
-                    ctx->draw_cw[mtype] = best;
+                    ctx->draw_wpc[mtype] = best;
                     GF_CUDA(cudaMemcpyAsync(d_rng, d_rng_snap, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
                 }
                 int64_t nev = 0;
@@ -1021,7 +1021,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                     GF_CUDA(cudaMemsetAsync(ctx->d_counters, 0, 24, st));
                     {
                         ProfScope ps(ctx, GF_PROF_BATCH_DRAW);
-                        GF_CUDA(gfk::launch_batch_draw(B, mtype, ctx->draw_cw[mtype], st));
+                        GF_CUDA(gfk::launch_batch_draw(B, mtype, ctx->draw_wpc[mtype], st));
                     }
                     GF_CUDA(cudaMemcpyAsync(ctx->h_counters, ctx->d_counters, 24, cudaMemcpyDeviceToHost, st));
                     GF_CUDA(cudaStreamSynchronize(st));
@@ -1246,7 +1246,7 @@ extern "C" gf_status gf_tuning_get(gf_ctx *ctx, int32_t model_kind, int32_t *war
 {
     GF_TRY(gfa::check_ctx(ctx));
     if (model_kind < 1 || model_kind > 2 || !warps_per_cta) return fail(GF_E_INVALID, "invalid arguments");
-    *warps_per_cta = ctx->draw_cw[model_kind];
+    *warps_per_cta = ctx->draw_wpc[model_kind];
     return GF_OK;
 }
 
@@ -1256,6 +1256,6 @@ extern "C" gf_status gf_tuning_set(gf_ctx *ctx, int32_t model_kind, int32_t warp
     if (model_kind < 1 || model_kind > 2) return fail(GF_E_INVALID, "invalid model kind");
     if (warps_per_cta != 0 && warps_per_cta != 1 && warps_per_cta != 2 && warps_per_cta != 4 && warps_per_cta != 8)
         return fail(GF_E_INVALID, "warps per CTA must be 1, 2, 4, 8 or 0 (tune again)");
-    ctx->draw_cw[model_kind] = warps_per_cta;
+    ctx->draw_wpc[model_kind] = warps_per_cta;
     return GF_OK;
 }

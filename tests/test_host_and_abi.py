@@ -188,3 +188,24 @@ def test_crawl_bin_order_is_a_bijection():
                 assert (ii.value, jj.value) == (i2.value, j2.value), (x, y, k)
                 assert i2.value + j2.value >= i.value + j.value
         assert len(seen) == x * y
+
+
+def test_table_rows_reads_a_row_range_of_a_host_table():
+    """table_rows (the host-delivery callback's view of a piece) copies rows [a, b) of
+    every column of a gf_table in host memory, vector columns as (components, rows)."""
+    h = G.HostTable(16, 5)
+    for name, dt, nc in G.COLUMNS:
+        k = 5 if nc == "bands" else nc
+        arr = h.arrays[name]
+        arr[...] = (np.arange(k * 16, dtype=np.float64).reshape(arr.shape) + 0.5).astype(dt)
+    rows = G.table_rows(h.t, 3, 9)
+    assert set(rows) == {name for name, _, _ in G.COLUMNS}
+    for name, dt, nc in G.COLUMNS:
+        full = h.arrays[name].reshape(-1, 16)
+        want = full[:, 3:9]
+        got = rows[name] if rows[name].ndim == 2 else rows[name][None, :]
+        np.testing.assert_array_equal(got, want, err_msg=name)
+        assert rows[name].dtype == np.dtype(dt)
+    # copies, not views: the ring slot behind a delivered piece is reused after the callback
+    rows["DM"][0] = -1.0
+    assert h.arrays["DM"].reshape(-1)[3] != -1.0
