@@ -122,12 +122,15 @@ C4_CAPACITY = 1 << 24          # rows per output batch of each request: 16M, the
 C4_PLAIN_STRIDE = 16           # the plain path is timed on every 16th request
 
 
+def config4_desc(nreq):
+    return ("config4: %d pencil beams, centres uniform at |b|>5 deg, radius log-uniform 0.5-5 deg, 0.1 deg pixels, "
+            "14<r<U(19,24), thin-disk h U(250,350), halo q U(0.55,0.75), own seed each, ugriz, full module chain" % nreq)
+
+
 def config4_set(G, W, rank=0, nreq=C4_NREQ):
     reqs = W.config4_requests(nreq, seed=1234567 + C4_NREQ * rank)
     ws = W.config4_workloads(G.lib(), reqs, capacity=C4_CAPACITY)
-    desc = ("config4: %d pencil beams, centres uniform at |b|>5 deg, radius log-uniform 0.5-5 deg, 0.1 deg pixels, "
-            "14<r<U(19,24), thin-disk h U(250,350), halo q U(0.55,0.75), own seed each, ugriz, full module chain" % nreq)
-    return ws, desc
+    return ws, config4_desc(nreq)
 
 
 def set_bins(ws):
@@ -143,21 +146,6 @@ def row_bytes(G, nbands):
     return sum((nbands if nc == "bands" else nc) * np.dtype(dt).itemsize for _, dt, nc in G.COLUMNS)
 
 
-def cpu_baseline_set(G, O, ws, threads=1, budget_s=12.0):
-    """The reference CPU path (oracle, libm) on the set's first requests, in order,
-    until budget_s of CPU work (at least one request)."""
-    mult = np.zeros(65536, dtype=np.uint32)
-    G.lib().gf_multipliers(mult.ctypes.data_as(C.POINTER(C.c_uint32)), 65536)
-    stars, t_all, k = 0, 0.0, 0
-    while k < len(ws) and (k == 0 or t_all < budget_s):
-        t0 = time.perf_counter()
-        st, _ = O.run_catalog(ws[k], mult, flavour="l", threads=threads)
-        t_all += time.perf_counter() - t0
-        stars += sum(st["stored"].values())
-        k += 1
-    return stars / t_all, stars, t_all, k
-
-
 def model_bins(w):
     """bins and diagonals of the three models (same binning for each)."""
     nm = int(round((w.sky.m1 - w.sky.m0) / w.sky.dm))
@@ -165,15 +153,11 @@ def model_bins(w):
     return len(w.models) * w.npixels * nm * nM, len(w.models) * w.npixels * (nm + nM - 1)
 
 
-def cpu_baseline(G, W, O, w_full, flavour="l", threads=1):
-    """The reference CPU path (oracle, libm) on every 1000th pixel of the workload."""
+def subsample_pixels(G, w_full, idx):
+    """The workload restricted to the pixels idx (per-beam extinction rows renumbered)."""
     import copy
-    mult = np.zeros(65536, dtype=np.uint32)
-    G.lib().gf_multipliers(mult.ctypes.data_as(C.POINTER(C.c_uint32)), 65536)
     sub = copy.copy(w_full)
-    idx = np.arange(0, w_full.npixels, 1000)
     pix = np.frombuffer(w_full.pixels, dtype=np.uint8).reshape(w_full.npixels, -1)[idx].copy()
-    # renumber the per-beam extinction rows
     pb = (G.PencilBeam * len(idx)).from_buffer(pix)
     for k in range(len(idx)):
         pb[k].extIdx = k
@@ -181,11 +165,57 @@ def cpu_baseline(G, W, O, w_full, flavour="l", threads=1):
     sub.npixels = len(idx)
     sub.ammin = np.ascontiguousarray(w_full.ammin[idx])
     sub.keep = list(w_full.keep)
+    return sub
+
+
+def cpu_baseline(G, W, O, w_full, flavour="l", threads=1):
+    """The reference CPU path (oracle, libm) on every 1000th pixel of the workload."""
+    mult = np.zeros(65536, dtype=np.uint32)
+    G.lib().gf_multipliers(mult.ctypes.data_as(C.POINTER(C.c_uint32)), 65536)
+    idx = np.arange(0, w_full.npixels, 1000)
+    sub = subsample_pixels(G, w_full, idx)
     t0 = time.perf_counter()
     stats, _ = O.run_catalog(sub, mult, flavour=flavour, threads=threads)
     dt = time.perf_counter() - t0
     stars = sum(stats["stored"].values())
     return stars / dt, stars, dt, len(idx)
+
+
+C4_CPU_REQ_STRIDE = 64           # CPU sample of the config-4 set: every 64th request ...
+C4_CPU_BINS = 3.0e8              # ... and one pixel stride over their pixels for about this many bins
+
+
+def config4_cpu_sample(G, ws_sampled):
+    """A stratified sample of the config-4 set for the CPU reference path: the given
+    requests (every C4_CPU_REQ_STRIDE-th of the set) and, with one stride over all their
+    pixels, about C4_CPU_BINS bins, so that the sample's mix of bright and faint bins is
+    the set's (a few leading requests can hold 10x more or fewer stars per bin than the
+    set).  Returns the sub-workloads and a description."""
+    total = sum(model_bins(w)[0] for w in ws_sampled)
+    p = max(1, int(round(total / C4_CPU_BINS)))
+    subs, g, npx = [], 0, 0
+    for w in ws_sampled:
+        idx = np.arange((-g) % p, w.npixels, p)
+        g += w.npixels
+        if len(idx):
+            subs.append(subsample_pixels(G, w, idx))
+            npx += len(idx)
+    desc = ("every %dth request of the 4096 (%d requests), every %dth of their pixels (%d pixels, %.2g bins)"
+            % (C4_CPU_REQ_STRIDE, len(ws_sampled), p, npx, total / p))
+    return subs, desc
+
+
+def run_cpu_sample(G, O, subs, threads):
+    """The reference CPU path (oracle, libm flavour, full module chain) over the sample."""
+    mult = np.zeros(65536, dtype=np.uint32)
+    G.lib().gf_multipliers(mult.ctypes.data_as(C.POINTER(C.c_uint32)), 65536)
+    stars, dt = 0, 0.0
+    for w in subs:
+        t0 = time.perf_counter()
+        st, _ = O.run_catalog(w, mult, flavour="l", threads=threads)
+        dt += time.perf_counter() - t0
+        stars += sum(st["stored"].values())
+    return stars / dt, stars, dt, len(subs)
 
 
 def main():
@@ -227,9 +257,12 @@ def main():
             return
         threads = os.cpu_count() or 1
         if args.config == "config4":
-            ws, desc = config4_set(G, W, 0, nreq=8)
-            sample_fn = lambda: cpu_baseline_set(G, O, ws[:2], threads=threads, budget_s=0.0)
-            sample_desc = "the first 2 requests of the config-4 set, all modules, %d threads" % threads
+            reqs = W.config4_requests(C4_NREQ, seed=1234567)[::C4_CPU_REQ_STRIDE]
+            ws = W.config4_workloads(G.lib(), reqs, capacity=C4_CAPACITY)
+            desc = config4_desc(C4_NREQ)
+            subs, sdesc = config4_cpu_sample(G, ws)
+            sample_fn = lambda: run_cpu_sample(G, O, subs, threads)
+            sample_desc = "%s, all modules, %d threads" % (sdesc, threads)
         else:
             w, desc = workload(G, W, args.config)
             sample_fn = lambda: cpu_baseline(G, W, O, w, threads=threads)
@@ -431,9 +464,10 @@ def bench_multi(args, G, W, ctx, rank, world, dist):
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         from oracle import oracle as O
-        v, s_, dt, k = cpu_baseline_set(G, O, ws, threads=1)
+        subs, sdesc = config4_cpu_sample(G, ws[::C4_CPU_REQ_STRIDE])
+        v, s_, dt, k = run_cpu_sample(G, O, subs, threads=1)
         cpu = {"value": v, "unit": "stars/s", "cores": 1, "kind": "port",
-               "sample": "the first %d requests of the set, full module chain, single-threaded restatement (libm), %.1f s" % (k, dt)}
+               "sample": "%s; full module chain, single-threaded restatement (libm), %.1f s" % (sdesc, dt)}
 
     if rank == 0:
         lat = np.array(times) / 1e3
