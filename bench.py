@@ -200,7 +200,7 @@ def config4_cpu_sample(G, ws_sampled):
         if len(idx):
             subs.append(subsample_pixels(G, w, idx))
             npx += len(idx)
-    desc = ("every %dth request of the 4096 (%d requests), every %dth of their pixels (%d pixels, %.2g bins)"
+    desc = ("every %dth request of the set (%d requests), every %dth of their pixels (%d pixels, %.2g bins)"
             % (C4_CPU_REQ_STRIDE, len(ws_sampled), p, npx, total / p))
     return subs, desc
 
