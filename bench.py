@@ -142,10 +142,6 @@ def set_bins(ws):
     return b, d
 
 
-def row_bytes(G, nbands):
-    return sum((nbands if nc == "bands" else nc) * np.dtype(dt).itemsize for _, dt, nc in G.COLUMNS)
-
-
 def model_bins(w):
     """bins and diagonals of the three models (same binning for each)."""
     nm = int(round((w.sky.m1 - w.sky.m0) / w.sky.dm))
@@ -153,27 +149,12 @@ def model_bins(w):
     return len(w.models) * w.npixels * nm * nM, len(w.models) * w.npixels * (nm + nM - 1)
 
 
-def subsample_pixels(G, w_full, idx):
-    """The workload restricted to the pixels idx (per-beam extinction rows renumbered)."""
-    import copy
-    sub = copy.copy(w_full)
-    pix = np.frombuffer(w_full.pixels, dtype=np.uint8).reshape(w_full.npixels, -1)[idx].copy()
-    pb = (G.PencilBeam * len(idx)).from_buffer(pix)
-    for k in range(len(idx)):
-        pb[k].extIdx = k
-    sub.pixels = bytearray(pix.tobytes())
-    sub.npixels = len(idx)
-    sub.ammin = np.ascontiguousarray(w_full.ammin[idx])
-    sub.keep = list(w_full.keep)
-    return sub
-
-
 def cpu_baseline(G, W, O, w_full, flavour="l", threads=1):
     """The reference CPU path (oracle, libm) on every 1000th pixel of the workload."""
     mult = np.zeros(65536, dtype=np.uint32)
     G.lib().gf_multipliers(mult.ctypes.data_as(C.POINTER(C.c_uint32)), 65536)
     idx = np.arange(0, w_full.npixels, 1000)
-    sub = subsample_pixels(G, w_full, idx)
+    sub = W.restrict_pixels(w_full, idx)
     t0 = time.perf_counter()
     stats, _ = O.run_catalog(sub, mult, flavour=flavour, threads=threads)
     dt = time.perf_counter() - t0
@@ -181,7 +162,7 @@ def cpu_baseline(G, W, O, w_full, flavour="l", threads=1):
     return stars / dt, stars, dt, len(idx)
 
 
-C4_CPU_REQ_STRIDE = 64           # CPU sample of the config-4 set: every 64th request ...
+C4_CPU_REQ_STRIDE = 8            # CPU sample of the config-4 set: every 8th request ...
 C4_CPU_BINS = 3.0e8              # ... and one pixel stride over their pixels for about this many bins
 
 
@@ -191,6 +172,7 @@ def config4_cpu_sample(G, ws_sampled):
     pixels, about C4_CPU_BINS bins, so that the sample's mix of bright and faint bins is
     the set's (a few leading requests can hold 10x more or fewer stars per bin than the
     set).  Returns the sub-workloads and a description."""
+    from galfast_b200 import workloads as W
     total = sum(model_bins(w)[0] for w in ws_sampled)
     p = max(1, int(round(total / C4_CPU_BINS)))
     subs, g, npx = [], 0, 0
@@ -198,7 +180,7 @@ def config4_cpu_sample(G, ws_sampled):
         idx = np.arange((-g) % p, w.npixels, p)
         g += w.npixels
         if len(idx):
-            subs.append(subsample_pixels(G, w, idx))
+            subs.append(W.restrict_pixels(w, idx))
             npx += len(idx)
     desc = ("every %dth request of the set (%d requests), every %dth of their pixels (%d pixels, %.2g bins)"
             % (C4_CPU_REQ_STRIDE, len(ws_sampled), p, npx, total / p))
@@ -210,9 +192,13 @@ def run_cpu_sample(G, O, subs, threads):
     mult = np.zeros(65536, dtype=np.uint32)
     G.lib().gf_multipliers(mult.ctypes.data_as(C.POINTER(C.c_uint32)), 65536)
     stars, dt = 0, 0.0
+    tables = {}
     for w in subs:
+        key = (w.capacity, w.nbands)
+        if key not in tables:
+            tables[key] = G.HostTable(*key)
         t0 = time.perf_counter()
-        st, _ = O.run_catalog(w, mult, flavour="l", threads=threads)
+        st, _ = O.run_catalog(w, mult, flavour="l", threads=threads, table=tables[key])
         dt += time.perf_counter() - t0
         stars += sum(st["stored"].values())
     return stars / dt, stars, dt, len(subs)
@@ -231,6 +217,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--clock-log", default=None, help="CSV of the SM clock samples taken during the timed region")
     ap.add_argument("--requests", type=int, default=C4_NREQ, help="config4: requests per step (a prefix of the set)")
+    ap.add_argument("--parity", type=int, default=16, help="config4: timed requests re-run alone and compared (0: none)")
+    ap.add_argument("--serve-rates", default="100,1000", help="config4: arrival rates of the serving sub-measurement ('' = none)")
     args = ap.parse_args()
     global CLOCK_LOG
     CLOCK_LOG = args.clock_log
@@ -273,11 +261,14 @@ def main():
             if i >= args.warmup:
                 vals.append((v, dt))
         value = float(np.mean([v for v, _ in vals]))
+        sbins = sum(model_bins(x)[0] for x in subs) if args.config == "config4" else None
         line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "stars/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean([d for _, d in vals])),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": desc, "sample": sample_desc},
-                "cpu_baseline": {"value": value, "unit": "stars/s", "cores": threads, "kind": "port", "sample": sample_desc},
+                "cpu_baseline": {"value": value, "unit": "stars/s", "cores": threads, "kind": "port", "sample": sample_desc,
+                                 "bins_per_s": (sbins / float(np.mean([d for _, d in vals]))) if sbins else None,
+                                 "stars_per_bin_sample": (stars / sbins) if sbins else None},
                 "e2e": {"value": value, "unit": "stars/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         if dist is not None:
@@ -322,37 +313,40 @@ def reduce_max_sum(dist, tmax, tsum):
     return float(a[0]), float(b[0])
 
 
-# DRAM bytes per bin of batch_draw_kernel: (332.69 + 228.86) MB over 4.34e9 bins in the ncu
-# capture of profiles/batch_draw_kernel_config4_64req.md; traffic grows with the bins (the
-# per-pixel slot rows and plan tables are read once per block, the events once per star)
+# DRAM bytes per bin of batch_draw_kernel, from the one-launch ncu capture of a
+# 64-request case of the batched workload (DRAM read + write over its bins);
+# traffic grows with the bins (each block reads its plan entries and slot row,
+# each star its event), so a full launch's traffic is this times its bins.
 DRAW_TRAFFIC_PER_BIN = 561.55e6 / 4.3396e9
+DRAW_TRAFFIC_SOURCE = "ncu capture of batch_draw_kernel on 64 requests of the set, scaled by bins per launch"
 
 
-def draw_rooflines(pk, pk_kind, bins, diags, stars_step, npix_models, draw_ms, draw_launches, nsteps):
-    """HBM roofline of the batched draw (algorithmic bytes: star records written and
-    beams read) and its issue roofline (per-bin / per-diagonal / per-star work of
-    the reference kernel against nominal B200 FP32, SFU and FP64 rates)."""
-    fp32 = 6.0 * bins + 60.0 * diags + 250.0 * stars_step
-    sfu = 1.0 * bins + 6.0 * diags + 40.0 * stars_step
-    fp64 = 150.0 * stars_step
-    bytes_alg = 32.0 * stars_step + 48.0 * npix_models
-    t_draw = draw_ms / 1e3 / nsteps if draw_ms else float("nan")
-    clk = (pk.get("sm_max_mhz") or 1965.0) * 1e6
-    pf32, psfu, pf64 = B200_SMS * FP32_PER_SM * clk, B200_SMS * SFU_PER_SM * clk, B200_SMS * FP64_PER_SM * clk
-    t_roof = max(fp32 / pf32, sfu / psfu, fp64 / pf64, bytes_alg / (pk["hbm_gbs"] * 1e9))
-    achieved = bytes_alg / t_draw / 1e9 if t_draw == t_draw else None
-    roofline = {"bound": "hbm", "kernel": "batch_draw_kernel (draw pass)", "achieved": achieved,
-                "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": (achieved / pk["hbm_gbs"]) if achieved else None,
-                "traffic": DRAW_TRAFFIC_PER_BIN * bins * nsteps / max(draw_launches, 1),
-                "traffic_note": "scaled from the 64-request ncu capture by bins per launch",
-                "peak_source": pk_kind,
-                "algorithmic_bytes_per_launch": bytes_alg * nsteps / max(draw_launches, 1),
-                "avg_launch_ms": draw_ms / max(draw_launches, 1)}
-    compute = {"bound": "sfu/fp32 issue (nominal)", "kernel": "batch_draw_kernel (draw pass)",
-               "t_bound_s": t_roof, "t_measured_s": t_draw, "frac": t_roof / t_draw if t_draw == t_draw else None,
-               "fp32_ops": fp32, "sfu_ops": sfu, "fp64_ops": fp64,
-               "peaks": {"fp32_ops_per_s": pf32, "sfu_ops_per_s": psfu, "fp64_ops_per_s": pf64, "clock_mhz": clk / 1e6}}
-    return roofline, compute
+def issue_peaks(clock_mhz):
+    """Nominal B200 issue rates (operations/s) at the given SM clock: 148 SMs x 128
+    FP32 lanes, x 16 special-function units, x 64 FP64 lanes."""
+    clk = (clock_mhz or 1965.0) * 1e6
+    return {"fp32": B200_SMS * FP32_PER_SM * clk, "sfu": B200_SMS * SFU_PER_SM * clk,
+            "fp64": B200_SMS * FP64_PER_SM * clk, "clock_mhz": clk / 1e6}
+
+
+def issue_roofline(kernel, work, ms, launches, nsteps, peaks_, note):
+    """Roofline of an issue-bound kernel.  work: algorithmic operations per step by
+    unit ("fp32", "sfu", "fp64"); the binding unit is the one whose operations take
+    longest at its peak rate.  achieved = that unit's operations per launch / the
+    launch's average device time (CUDA events on the launching stream)."""
+    if not ms or not launches:
+        return None
+    t_unit = {u: work[u] / peaks_[u] for u in work if work[u] > 0}
+    bound = max(t_unit, key=t_unit.get)
+    per_launch = work[bound] * nsteps / launches
+    avg_s = ms / launches / 1e3
+    achieved = per_launch / avg_s
+    return {"bound": bound + " issue", "kernel": kernel, "achieved": achieved / 1e9, "peak": peaks_[bound] / 1e9,
+            "unit": "Gop/s", "frac": achieved / peaks_[bound],
+            "ops_per_launch": {u: work[u] * nsteps / launches for u in work}, "avg_launch_ms": ms / launches,
+            "launches": launches, "work_model": note,
+            "peak_source": "nominal B200 issue rate at the sampled SM clock (%.0f MHz); MEASURED_PEAKS.json holds "
+                           "only HBM and bf16 figures" % peaks_["clock_mhz"]}
 
 
 def bench_multi(args, G, W, ctx, rank, world, dist):
@@ -416,18 +410,21 @@ def bench_multi(args, G, W, ctx, rank, world, dist):
     pm, pr = reduce_max_sum(dist, float(np.sum(plain_ms)), float(np.sum(plain_rows)))
     plain_value = pr / (pm / 1e3)
 
-    # ---- e2e: every request's rows copied to page-locked host memory inside the timed region ----
+    # ---- e2e: every request's output columns copied to page-locked host memory inside the timed region ----
     # gf_catalog_run_multi_host copies each model pass's rows on a second stream while the
-    # device generates the next pass; the callback sees every piece in host memory.
+    # device generates the next pass; the callback sees every piece in host memory.  The
+    # copied columns are the output catalog's (ra, dec, DM, Mr, true and observed
+    # magnitudes, velocities, proper motions), as a catalog writer selects them.
     e2e = None
     if args.e2e_steps > 0:
         d2h = [0]
 
         def hcb(user, model, tptr, rb, rc):
             t = tptr.contents
-            d2h[0] += int(t.size) * row_bytes(G, t.nbands)
+            d2h[0] += int(t.size) * host_row_bytes(G, t)
             return 0
         chcb = G.MultiHostCallback(hcb)
+        ctx.set_host_columns(G.COL_CATALOG)
 
         def host_step():
             ctx.mark(2)
@@ -441,33 +438,73 @@ def bench_multi(args, G, W, ctx, rank, world, dist):
             ms, r = host_step()
             e_ms.append(ms)
             e_rows.append(r)
+        ctx.set_host_columns(G.COL_ALL)
         em, er = reduce_max_sum(dist, float(np.sum(e_ms)), float(np.sum(e_rows)))
         h2d = sum(w.npixels * (C.sizeof(G.PencilBeam) + 4) + nmod * 1024 * 4 for w in ws)
         e2e = {"value": er / (em / 1e3), "unit": "stars/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h[0]),
+               "columns": "radec, DM, absmag, mags, obsmags, vcyl, pm (gf_multi_set_host_columns(GF_COL_CATALOG))",
                "path": "gf_catalog_run_multi_host: rows of each pass copied to page-locked host memory on a second stream"}
 
-    pk, pk_kind = peaks()
+    # ---- parity of the timed catalogs: requests of the plain sample, batched against alone ----
+    parity = None
+    if args.parity > 0:
+        check_ids = sample[:args.parity]
+        got = batched_rows(G, L, ctx, jobs, n, check_ids)
+        equal = 0
+        nrows = 0
+        for j in check_ids:
+            ref = standalone_rows(G, ctx, ws[j])
+            ok = same_catalog(ref, got.get(j, {}))
+            equal += int(ok)
+            nrows += sum(len(v["DM"]) for v in ref.values())
+        parity = {"checked": len(check_ids), "equal": equal, "rows": nrows,
+                  "against": "the same requests through gf_catalog_run alone (plain path), every column compared bit for bit",
+                  "requests": "every %dth request of the timed set" % C4_PLAIN_STRIDE}
+
+    # ---- rooflines: the batched draw (dominant kernel) and the pixel integrate ----
+    clk_summary = clock.summary()
+    ipk = issue_peaks(clk_summary.get("sm_mhz") or 1965.0)
     bins, diags = set_bins(ws)
-    # the batched draw's share: requests whose stars fit one batch (the others take the plain path)
+    # the batched engine's share: requests whose stars fit one batch (the others take the plain path)
     capd = float(C4_CAPACITY)
     batched = [j for j in range(n)
                if max(st_e + 8.0 * np.sqrt(max(st_e, 0.0)) + 1024.0 for st_e in list(stats[j].expected)[:nmod]) < capd]
     bb = sum(model_bins(ws[j])[0] for j in batched)
     bd = sum(model_bins(ws[j])[1] for j in batched)
-    bstars = sum(stats[j].generated[i] for j in batched for i in range(nmod))
-    draw_ms = prof.get("batch_draw", (0, 0))[0]
-    draw_launches = prof.get("batch_draw", (0, 0))[1]
-    roofline, compute = draw_rooflines(pk, pk_kind, bb, bd, bstars, nmod * sum(ws[j].npixels for j in batched),
-                                       draw_ms, draw_launches, args.steps)
-    roofline["batched_requests"] = len(batched)
+    draw_ms, draw_launches = prof.get("batch_draw", (0, 0))
+    roofline = issue_roofline("batch_draw_kernel", {"fp32": 6.0 * bb, "sfu": 1.0 * bb}, draw_ms, draw_launches,
+                              args.steps, ipk, "per bin 6 FP32 + 1 SFU (exp(-mu)) + 1 MWC step; %d batched requests, "
+                              "%.4g bins per step" % (len(batched), bb))
+    if roofline is not None:
+        roofline["traffic"] = DRAW_TRAFFIC_PER_BIN * bb * args.steps / draw_launches
+        roofline["traffic_source"] = DRAW_TRAFFIC_SOURCE
+    integ_ms, integ_launches = prof.get("integrate", (0, 0))
+    integ_roof = issue_roofline("integrate_pixels_kernel", {"fp32": 8.0 * bb + 60.0 * bd, "sfu": 6.0 * bd},
+                                integ_ms, integ_launches, args.steps, ipk,
+                                "per bin 8 FP32 (4 products, 2 cuts, 2 sums); per diagonal 60 FP32 + 6 SFU")
+    pk, pk_kind = peaks()
+    draw_bytes = 48.0 * nmod * sum(ws[j].npixels for j in batched) + 32.0 * sum(
+        stats[j].generated[i] for j in batched for i in range(nmod))
+    roofline_hbm = None
+    if draw_ms:
+        ach = draw_bytes / (draw_ms / args.steps / 1e3) / 1e9
+        roofline_hbm = {"bound": "hbm", "kernel": "batch_draw_kernel", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                        "frac": ach / pk["hbm_gbs"], "peak_source": pk_kind,
+                        "work_model": "48 B per beam read + 32 B per star event written"}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         from oracle import oracle as O
         subs, sdesc = config4_cpu_sample(G, ws[::C4_CPU_REQ_STRIDE])
         v, s_, dt, k = run_cpu_sample(G, O, subs, threads=1)
+        sbins = sum(model_bins(w)[0] for w in subs)
         cpu = {"value": v, "unit": "stars/s", "cores": 1, "kind": "port",
+               "bins_per_s": sbins / dt, "stars_per_bin_sample": s_ / sbins, "stars_per_bin_set": generated / bins,
                "sample": "%s; full module chain, single-threaded restatement (libm), %.1f s" % (sdesc, dt)}
+
+    serve = None
+    if args.serve_rates and world == 1:
+        serve = serve_summary(G, W, L, ctx, [float(x) for x in args.serve_rates.split(",")], args.serve_requests)
 
     if rank == 0:
         lat = np.array(times) / 1e3
@@ -487,10 +524,116 @@ def bench_multi(args, G, W, ctx, rank, world, dist):
                           "gf_catalog_run, one at a time" % (C4_PLAIN_STRIDE, len(sample)),
                           "latency_p50_s": float(np.percentile(plat, 50)), "latency_p99_s": float(np.percentile(plat, 99))},
                 "batched_over_plain": value / plain_value if plain_value else None,
-                "e2e": e2e, "roofline": roofline, "compute_roofline": compute, "cpu_baseline": cpu,
-                "gpu_launches": int(launches), "clocks": clock.summary(),
+                "parity": parity, "serve": serve,
+                "e2e": e2e, "roofline": roofline, "integrate_roofline": integ_roof, "roofline_hbm": roofline_hbm,
+                "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk_summary,
                 "phases_ms_per_step": {k: v[0] / args.steps for k, v in prof.items()}}
         print(json.dumps(line))
+
+
+def host_row_bytes(G, t):
+    """Bytes per row of the columns a host table carries (NULL columns excluded)."""
+    b = 0
+    for name, dt, nc in G.COLUMNS:
+        k = int(t.nbands) if nc == "bands" else nc
+        if getattr(t, name):
+            b += k * np.dtype(dt).itemsize
+    return b
+
+
+def batched_rows(G, L, ctx, jobs, n, wanted):
+    """The rows of the requests `wanted` from one gf_catalog_run_multi call, downloaded
+    request by request: {request: {model: [column dicts]}}."""
+    got = {}
+    wanted = list(wanted)
+    stats = (G.CatalogStats * n)()
+
+    def cb(user, model, tptr, rb, rc):
+        t = tptr.contents
+        for j in wanted:
+            c = int(rc[j])
+            if c <= 0:
+                continue
+            h = G.HostTable(c, t.nbands)
+            if L.gf_table_download_rows(ctx.h, tptr, rb[j], rb[j] + c, C.byref(h.t)) != 0:
+                return 1
+            h.t.size = c
+            got.setdefault(j, {}).setdefault(model, []).append(h.as_dict())
+        return 0
+    ccb = G.MultiCallback(cb)
+    G.check(L.gf_catalog_run_multi(ctx.h, jobs, n, ccb, None, stats))
+    return got
+
+
+def standalone_rows(G, ctx, w):
+    """One request's rows through gf_catalog_run: {model: [column dicts]}."""
+    out = {}
+    G.run_catalog(ctx, w, sink=lambda m, t, off: out.setdefault(m, []).append(t.as_dict()))
+    return out
+
+
+def same_catalog(a, b):
+    """Every column of every model equal, bit for bit (NaN equal to NaN)."""
+    if sorted(a) != sorted(b):
+        return False
+    for m in a:
+        x = {k: np.concatenate([p[k] for p in a[m]], axis=-1) for k in a[m][0]}
+        y = {k: np.concatenate([p[k] for p in b[m]], axis=-1) for k in b[m][0]}
+        for k in x:
+            u, v = x[k], y.get(k)
+            if v is None or u.shape[-1] != v.shape[-1]:
+                return False
+            if k in ("mags", "obsmags"):
+                v = v[: u.shape[0]]
+            if u.shape != v.shape:
+                return False
+            eq = (u == v) | (np.isnan(u) & np.isnan(v)) if u.dtype.kind == "f" else (u == v)
+            if not eq.all():
+                return False
+    return True
+
+
+def serve_summary(G, W, L, ctx, rates, nreq, nchecks=4):
+    """Served requests (gf_server, continuous batching) at the given Poisson arrival
+    rates: latency percentiles and throughput, and the smallest `nchecks` requests of
+    each rate compared bit for bit with their standalone gf_catalog_run."""
+    base = W.config5_requests(nreq, 1.0, seed=99)
+    ws = W.config5_workloads(L, base)
+    size = [r["area"] * 10 ** (0.6 * (r["rmax"] - 20.0)) for r in base]
+    small = set(int(k) for k in np.argsort(size)[:nchecks])
+    srv = G.Server(0, workers=2, memory_budget=150 * 2 ** 30, max_batch=512)
+    for w in ws[: min(4, nreq)]:
+        srv.submit(w)
+    srv.drain()
+    srv.close()
+    out = []
+    for rate in rates:
+        order = {}
+        srv = G.Server(0, workers=2, memory_budget=150 * 2 ** 30, max_batch=512,
+                       keep_rows=lambda rid: order.get(rid) in small)
+        t0 = time.perf_counter()
+        for k, (r, w) in enumerate(zip(base, ws)):
+            t_arr = r["t"] / rate
+            while time.perf_counter() - t0 < t_arr:
+                time.sleep(0.0005)
+            rid = srv.submit(w)
+            order[rid] = k
+        srv.drain()
+        lat = np.array([srv.finished[i] - srv.submitted[i] for i in srv.submitted])
+        rows = sum(st.stored[i] for st in srv.stats.values() for i in range(len(ws[0].models)))
+        span = max(srv.finished.values()) - min(srv.submitted.values())
+        failed = sum(1 for s_ in srv.status.values() if s_ != 0)
+        equal = 0
+        for rid, k in order.items():
+            if k in small and srv.status.get(rid) == 0:
+                equal += int(same_catalog(standalone_rows(G, ctx, ws[k]), srv.rows.get(rid, {})))
+        srv.close()
+        out.append({"rate_per_s": rate, "requests": nreq, "failed": failed, "rows": int(rows), "stars_per_s": rows / span,
+                    "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+                    "makespan_s": span, "bit_exact_checked": len(small), "bit_exact_equal": equal})
+    return {"workload": "Poisson arrivals of caps and lon/lat rectangles of log-uniform 1-1000 deg^2 at |b|>10 deg, "
+                        "14<r<U(20,25), half ugriz / half ugrizy; gf_server with 2 workers, 150 GiB budget",
+            "latency": "submit to completion, host wall clock", "rates": out}
 
 
 def bench_precision(args, G, W, ctx, rank, world, dist):
@@ -632,8 +775,7 @@ def bench_single(args, G, W, ctx, rank, world, dist):
     ctx.sync()
     n0 = L.gf_launch_count()
     times, stars = [], []
-    clock = ClockSampler(os.path.join(ROOT, "gpurun_out", "bench_clocks_rank%d.csv" % rank)) if os.path.isdir(
-        os.path.join(ROOT, "gpurun_out")) else ClockSampler("/tmp/bench_clocks.csv")
+    clock = clock_sampler(rank)
     with clock:
         for _ in range(args.steps):
             ms, st = step()
@@ -713,34 +855,14 @@ def bench_single(args, G, W, ctx, rank, world, dist):
                "unit": "stars/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h[0])}
 
     # ---- roofline of the dominant kernel (the draw crawl) ----
-    pk, pk_kind = peaks()
     bins, diags = model_bins(w)
     nsteps = args.steps
     draw_ms = prof.get("draw_window", (0, 0))[0] + prof.get("draw_rerun", (0, 0))[0]
     draw_launches = prof.get("draw_window", (0, 0))[1] + prof.get("draw_rerun", (0, 0))[1]
-    stars_step = float(np.mean(stars))
-    gen_stars = stars_step
-    # algorithmic work of the draw pass per step (per-bin / per-diagonal / per-star counts of the reference kernel)
-    fp32 = 6.0 * bins + 60.0 * diags + 250.0 * gen_stars
-    sfu = 1.0 * bins + 6.0 * diags + 40.0 * gen_stars
-    fp64 = 150.0 * gen_stars
-    bytes_alg = 32.0 * gen_stars + 48.0 * w.npixels * len(w.models)       # star records written + beams read
-    t_draw = draw_ms / 1e3 / nsteps if draw_ms else float("nan")
-    clk = (pk.get("sm_max_mhz") or 1965.0) * 1e6
-    pf32, psfu, pf64 = B200_SMS * FP32_PER_SM * clk, B200_SMS * SFU_PER_SM * clk, B200_SMS * FP64_PER_SM * clk
-    t_roof = max(fp32 / pf32, sfu / psfu, fp64 / pf64, bytes_alg / (pk["hbm_gbs"] * 1e9))
-    achieved_gbs = bytes_alg / t_draw / 1e9 if t_draw == t_draw else None
-    roofline = {"bound": "hbm", "kernel": "crawl_kernel<1> (draw pass)", "achieved": achieved_gbs,
-                "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": (achieved_gbs / pk["hbm_gbs"]) if achieved_gbs else None,
-                "traffic": None, "peak_source": pk_kind,
-                "algorithmic_bytes_per_launch": bytes_alg * nsteps / max(draw_launches, 1),
-                "avg_launch_ms": draw_ms / max(draw_launches, 1)}
-    compute_roofline = {"bound": "sfu/fp32 issue (nominal)", "kernel": "crawl_kernel<1> (draw pass)",
-                        "t_bound_s": t_roof, "t_measured_s": t_draw, "frac": t_roof / t_draw if t_draw == t_draw else None,
-                        "fp32_ops": fp32, "sfu_ops": sfu, "fp64_ops": fp64,
-                        "peaks": {"fp32_ops_per_s": pf32, "sfu_ops_per_s": psfu, "fp64_ops_per_s": pf64,
-                                  "clock_mhz": clk / 1e6}}
-
+    clk_summary = clock.summary()
+    roofline = issue_roofline("crawl_kernel<1> (draw pass)", {"fp32": 6.0 * bins + 60.0 * diags, "sfu": 1.0 * bins + 6.0 * diags},
+                              draw_ms, draw_launches, nsteps, issue_peaks(clk_summary.get("sm_mhz") or 1965.0),
+                              "per bin 6 FP32 + 1 SFU + 1 MWC step; per diagonal 60 FP32 + 6 SFU")
     cpu = None
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         from oracle import oracle as O
@@ -758,8 +880,8 @@ def bench_single(args, G, W, ctx, rank, world, dist):
                            "parallelism": "replicas" if world > 1 else "single request",
                            "l2": "inputs larger than L2 (164 MB pixel list, 10+ GB catalog per step)",
                            "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99))},
-                "e2e": e2e, "roofline": roofline, "compute_roofline": compute_roofline, "cpu_baseline": cpu,
-                "gpu_launches": int(launches), "clocks": clock.summary(),
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+                "gpu_launches": int(launches), "clocks": clk_summary,
                 "phases_ms_per_step": {k: v[0] / nsteps for k, v in prof.items()}}
         print(json.dumps(line))
 

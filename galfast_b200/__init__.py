@@ -72,6 +72,7 @@ def lib():
         L.gf_rng_seed48_from_cli_seed.restype = C.c_uint32
         L.gf_rng_get_state.argtypes = [vp, vp, C.c_int32]
         L.gf_rng_set_state.argtypes = [vp, vp, C.c_int32]
+        L.gf_rng_poisson.argtypes = [vp, vp, vp, C.c_int32, vp]
         L.gf_skygen_create.argtypes = [vp, C.POINTER(SkygenConfig), C.POINTER(PencilBeam), C.c_int32,
                                        C.POINTER(C.c_float), C.POINTER(Extinction), C.POINTER(ModelConfig),
                                        C.c_int32, C.POINTER(vp)]
@@ -101,6 +102,9 @@ def lib():
         L.gf_catalog_run_multi_host.argtypes = [vp, C.POINTER(Job), C.c_int32, C.c_int64, MultiHostCallback, vp,
                                                 C.POINTER(CatalogStats)]
         L.gf_multi_set_memory_budget.argtypes = [vp, C.c_int64]
+        L.gf_multi_set_host_columns.argtypes = [vp, C.c_uint32]
+        L.gf_multi_set_admission.argtypes = [vp, C.c_double]
+        L.gf_debug_fail_allocations.argtypes = [C.c_int64, C.c_int64]
         L.gf_tuning_get.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32)]
         L.gf_tuning_set.argtypes = [vp, C.c_int32, C.c_int32]
         L.gf_table_download_rows.argtypes = [vp, C.POINTER(Table), C.c_int64, C.c_int64, C.POINTER(Table)]
@@ -144,6 +148,10 @@ COLUMNS = [  # name, dtype, components (or "bands")
 PROFILE_PHASES = ["integrate", "draw_window", "draw_rerun", "place", "sort", "clipper", "fixedfeh", "bond2010",
                   "photometry", "photoerrors", "vel2pm", "gal2other", "slot_density", "expand", "batch_draw"]
 SKYGEN_COLUMNS = ["lb", "projIdx", "projXY", "DM", "absmag", "XYZ", "comp", "Am", "AmInf", "hidden"]
+# column bits of gf_multi_set_host_columns (GF_COL_*): bit i is COLUMNS[i]
+COL = {name: 1 << i for i, (name, _, _) in enumerate(COLUMNS)}
+COL_ALL = (1 << len(COLUMNS)) - 1
+COL_CATALOG = sum(COL[n] for n in ("radec", "DM", "absmag", "mags", "obsmags", "vcyl", "pm"))
 
 
 class HostTable:
@@ -241,6 +249,14 @@ class Context:
 
     def set_tuning(self, model_kind, warps):
         check(lib().gf_tuning_set(self.h, model_kind, warps))
+
+    def set_host_columns(self, mask):
+        """Columns gf_catalog_run_multi_host copies to host memory (COL bits)."""
+        check(lib().gf_multi_set_host_columns(self.h, int(mask)))
+
+    def set_admission(self, sigmas):
+        """gf_multi_set_admission: batched if expected + sigmas sqrt(expected) + 1024 < capacity."""
+        check(lib().gf_multi_set_admission(self.h, float(sigmas)))
 
     def set_multi_budget(self, nbytes):
         """Device bytes per chunk of gf_catalog_run_multi (0 = 60% of free memory)."""
@@ -454,7 +470,8 @@ class Server:
     """gf_server: continuous batching of catalog requests on one device.
 
     submit(w) queues a workload; keep_rows=True keeps each request's rows in host
-    memory (a dict per model of column arrays).  Completion wall-clock times are
+    memory (a dict per model of column arrays), a callable keep_rows(request id)
+    those of the requests it accepts.  Completion wall-clock times are
     recorded for latency.  Callbacks run on the server's worker threads."""
 
     def __init__(self, device=0, workers=2, memory_budget=150 * 2 ** 30, max_batch=512, keep_rows=False):
@@ -470,7 +487,7 @@ class Server:
         self._stage = {}
 
         def on_rows(user, rid, model, wctx, tptr, begin, count):
-            if not self.keep_rows:
+            if not (self.keep_rows(rid) if callable(self.keep_rows) else self.keep_rows):
                 return 0
             t = tptr.contents
             h = HostTable(max(int(count), 1), t.nbands)

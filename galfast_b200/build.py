@@ -2,8 +2,8 @@
 
     python -m galfast_b200.build          # or galfast_b200.build.build()
 
-compiles every CUDA and C++ source under galfast_b200/csrc into
-galfast_b200/_lib/libgalfast_b200.so and writes the stream-multiplier table
+compiles every CUDA and C++ source under galfast_b200/csrc (one nvcc process
+per source file, in parallel) into galfast_b200/_lib/libgalfast_b200.so and writes the stream-multiplier table
 (safeprimes_65536.bin) next to it.  Device code is compiled with -fmad=false
 and host code with -ffp-contract=off: the catalog's Poisson draws depend on the
 exact float results of the reference's expressions, so no multiply-add may be
@@ -31,21 +31,43 @@ def nvcc_path():
     return cand
 
 
-def build(verbose=False, extra=None):
+def _flags(extra):
+    return [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "--expt-relaxed-constexpr",
+            "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math", *(extra or [])]
+
+
+def build(verbose=False, extra=None, jobs=None):
+    """Compile every source to an object file (in parallel), then link the shared
+    library.  No device symbol crosses a source file, so no device link is needed."""
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIBDIR, exist_ok=True)
+    objdir = os.path.join(LIBDIR, "obj")
+    os.makedirs(objdir, exist_ok=True)
     out = os.path.join(LIBDIR, LIBNAME)
-    srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    cmd = [nvcc_path(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
-           "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
-           "-shared", "-o", out, *srcs, "-ldl", "-lpthread"]
-    if extra:
-        cmd[1:1] = list(extra)
+    nvcc = nvcc_path()
+
+    def compile_one(src):
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        cmd = [nvcc, *_flags(extra), "-c", "-o", obj, os.path.join(CSRC, src)]
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return obj, r
+
+    n = jobs or min(len(SOURCES), os.cpu_count() or 1)
+    with ThreadPoolExecutor(max_workers=n) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    for (obj, r), src in zip(results, SOURCES):
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("nvcc build of %s failed (%s)" % (LIBNAME, src))
+    cmd = [nvcc, *ARCH, "-shared", "-o", out, *[o for o, _ in results], "-ldl", "-lpthread"]
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc build of %s failed" % LIBNAME)
+        raise RuntimeError("link of %s failed" % LIBNAME)
     write_multiplier_table(out)
     return out
 

@@ -13,10 +13,44 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <atomic>
 
 namespace gfa {
 
 thread_local std::string g_err;
+
+/* allocation failures arranged by gf_debug_fail_allocations: the allocations
+ * after the next g_fail_after ones fail, g_fail_count of them (0: all) */
+static std::atomic<long long> g_fail_after(-1), g_fail_count(0), g_alloc_seen(0);
+
+void set_alloc_failures(long long after, long long count)
+{
+    g_fail_after.store(-1);
+    g_alloc_seen.store(0);
+    g_fail_count.store(count);
+    g_fail_after.store(after < 0 ? -1 : after);
+}
+
+void release_caches(gf_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    gf_table_free(ctx, &ctx->plain_table);
+    free_multi_ws(ctx);
+}
+
+cudaError_t device_malloc(void **p, size_t bytes)
+{
+    *p = nullptr;
+    const long long after = g_fail_after.load();
+    if (after >= 0) {
+        const long long k = g_alloc_seen.fetch_add(1);
+        const long long cnt = g_fail_count.load();
+        if (k >= after && (cnt == 0 || k < after + cnt)) return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(p, bytes);
+}
 
 gf_status fail(gf_status s, const std::string &msg)
 {
@@ -128,7 +162,7 @@ size_t crawl_state_bytes(int n) { return (size_t)n * (8 * 4 + 16 + 8) + 256; }
 
 gf_status alloc_crawl_state(int n, CrawlState &st, void **mem)
 {
-    GF_CUDA(cudaMalloc(mem, crawl_state_bytes(n)));
+    GF_CUDA(gfa::device_malloc(mem, crawl_state_bytes(n)));
     char *p = (char *)*mem;
     auto take = [&](size_t bytes) { char *r = p; p += (bytes + 15) & ~(size_t)15; return r; };
     st.anc = (AnchorX *)take(16 * (size_t)n);
@@ -186,7 +220,7 @@ gf_status ensure_rec_capacity(gf_skygen *s, int64_t need, int64_t keep)
     GF_TRY(dev_alloc(&s->d_idx2, cap));
     size_t tb = 0;
     GF_CUDA(gfk::sort_temp_bytes(cap, &tb));
-    GF_CUDA(cudaMalloc(&s->d_sort_temp, tb + 256));
+    GF_CUDA(gfa::device_malloc(&s->d_sort_temp, tb + 256));
     s->sort_temp_bytes = tb + 256;
     s->rec_cap = cap;
     return GF_OK;
@@ -341,7 +375,7 @@ gf_status gf_ctx_create(int device, gf_ctx **out)
     gf_ctx *c = new gf_ctx();
     c->device = device;
     cudaError_t ce = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-    if (ce == cudaSuccess) ce = cudaMalloc(&c->d_counters, 64);
+    if (ce == cudaSuccess) ce = gfa::device_malloc((void **)&c->d_counters, 64);
     if (ce == cudaSuccess) ce = cudaMallocHost(&c->h_counters, 64);
     if (ce != cudaSuccess) {
         delete c;
@@ -464,6 +498,34 @@ gf_status gf_rng_set_state(gf_ctx *ctx, const uint32_t *host_state, int32_t nstr
     GF_CUDA(cudaMemcpyAsync(ctx->d_rng, host_state, 12 * (size_t)nstreams, cudaMemcpyHostToDevice, ctx->stream));
     GF_CUDA(cudaStreamSynchronize(ctx->stream));
     return GF_OK;
+}
+
+gf_status gf_rng_poisson(gf_ctx *ctx, uint32_t state[3], const float *mu, int32_t n, uint32_t *out)
+{
+    GF_TRY(check_ctx(ctx));
+    if (!state || n < 0 || (n > 0 && (!mu || !out))) return fail(GF_E_INVALID, "invalid gf_rng_poisson arguments");
+    if (state[0] == 0) return fail(GF_E_INVALID, "stream multiplier must be nonzero");
+    for (int32_t i = 0; i < n; i++)
+        if (!(mu[i] >= 0.f && mu[i] < 1e7f)) return fail(GF_E_INVALID, "Poisson means must be in [0, 1e7)");
+    uint32_t *d_st = nullptr, *d_out = nullptr;
+    float *d_mu = nullptr;
+    gf_status st = dev_alloc(&d_st, 3);
+    if (st == GF_OK) st = dev_alloc(&d_mu, (size_t)n + 1);
+    if (st == GF_OK) st = dev_alloc(&d_out, (size_t)n + 1);
+    if (st == GF_OK) {
+        cudaError_t e = cudaMemcpyAsync(d_st, state, 12, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess && n) e = cudaMemcpyAsync(d_mu, mu, 4 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) e = gfk::launch_poisson_stream(d_st, d_mu, n, d_out, ctx->stream);
+        if (e == cudaSuccess && n) e = cudaMemcpyAsync(out, d_out, 4 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(state, d_st, 12, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) st = fail(GF_E_CUDA, std::string("gf_rng_poisson: ") + cudaGetErrorString(e));
+    }
+    cudaStreamSynchronize(ctx->stream);
+    dev_free(d_st);
+    dev_free(d_mu);
+    dev_free(d_out);
+    return st;
 }
 
 gf_status gf_skygen_destroy(gf_skygen *s);
@@ -895,14 +957,9 @@ static gf_status zero_module_columns(gf_ctx *ctx, gf_table *t)
     return gfa::zero_module_rows(ctx, t, t->capacity);
 }
 
-gf_status gf_table_alloc(gf_ctx *ctx, int64_t capacity, int32_t nbands, gf_table *t)
+/* the columns of a table of n rows (any that fail leave the others allocated) */
+static gf_status table_alloc_columns(gf_table *t, size_t n, int32_t nbands)
 {
-    GF_TRY(check_ctx(ctx));
-    if (!t || capacity <= 0 || nbands < 0 || nbands > GF_MAX_BANDS) return fail(GF_E_INVALID, "invalid table arguments");
-    memset(t, 0, sizeof(*t));
-    t->capacity = capacity;
-    t->nbands = nbands;
-    size_t n = (size_t)capacity;
     GF_TRY(dev_alloc(&t->lb, 2 * n));
     GF_TRY(dev_alloc(&t->projIdx, n));
     GF_TRY(dev_alloc(&t->projXY, 2 * n));
@@ -922,6 +979,22 @@ gf_status gf_table_alloc(gf_ctx *ctx, int64_t capacity, int32_t nbands, gf_table
     GF_TRY(dev_alloc(&t->photoflags, n));
     GF_TRY(dev_alloc(&t->pm, 3 * n));
     GF_TRY(dev_alloc(&t->radec, 2 * n));
+    return GF_OK;
+}
+
+gf_status gf_table_alloc(gf_ctx *ctx, int64_t capacity, int32_t nbands, gf_table *t)
+{
+    GF_TRY(check_ctx(ctx));
+    if (!t || capacity <= 0 || nbands < 0 || nbands > GF_MAX_BANDS) return fail(GF_E_INVALID, "invalid table arguments");
+    memset(t, 0, sizeof(*t));
+    t->capacity = capacity;
+    t->nbands = nbands;
+    gf_status st = table_alloc_columns(t, (size_t)capacity, nbands);
+    if (st != GF_OK) {
+        const std::string msg = gfa::g_err;
+        gf_table_free(ctx, t);         /* no partial table is left behind */
+        return fail(st, msg);
+    }
     GF_TRY(zero_module_columns(ctx, t));
     GF_CUDA(cudaStreamSynchronize(ctx->stream));
     return GF_OK;
@@ -1127,7 +1200,7 @@ gf_status gf_module_gal2other(gf_ctx *ctx, int32_t coordsys, gf_table *t, int64_
 
 /* ---------------- the catalog path ---------------- */
 
-gf_status gf_catalog_run(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, void *user, gf_catalog_stats *stats)
+static gf_status catalog_run_once(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, void *user, gf_catalog_stats *stats)
 {
     GF_TRY(check_ctx(ctx));
     if (!job || job->nmodels <= 0 || job->nmodels > GF_MAX_MODELS || job->capacity <= 0) return fail(GF_E_INVALID, "invalid job");
@@ -1202,6 +1275,42 @@ gf_status gf_catalog_run(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, v
             row_offset += n;
         }
     }
+    return GF_OK;
+}
+
+namespace {
+struct CountingBatch {
+    gf_batch_callback cb;
+    void *user;
+    long long calls;
+};
+int counting_batch(void *u, int32_t model, const gf_table *t, int64_t off)
+{
+    CountingBatch *c = (CountingBatch *)u;
+    c->calls++;
+    return c->cb ? c->cb(c->user, model, t, off) : 0;
+}
+}  // namespace
+
+/* os_skygen::run + the module chain.  An out-of-memory failure before any batch
+ * was delivered frees the context's cached buffers and runs the request once
+ * more, as the reference collects garbage and retries a failed allocation
+ * (cux.cpp:189-198); the streams are seeded again, so the retry is the same run. */
+gf_status gf_catalog_run(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, void *user, gf_catalog_stats *stats)
+{
+    CountingBatch c = {cb, user, 0};
+    gf_status st = catalog_run_once(ctx, job, counting_batch, &c, stats);
+    if (st == GF_E_OOM && c.calls == 0 && job && job->nstreams > 0) {
+        gfa::release_caches(ctx);
+        st = catalog_run_once(ctx, job, counting_batch, &c, stats);
+    }
+    return st;
+}
+
+gf_status gf_debug_fail_allocations(int64_t after, int64_t count)
+{
+    if (count < 0) return fail(GF_E_INVALID, "negative failure count");
+    gfa::set_alloc_failures(after, count);
     return GF_OK;
 }
 

@@ -48,6 +48,14 @@ __device__ __forceinline__ float bd_mwc_step(uint64_t &v, uint32_t a)
     return GF_MWC_SCALE * (float)(uint32_t)t;
 }
 
+/* one MWC step; returns the new x (the uniform is 2^-32 x) */
+__device__ __forceinline__ uint32_t bd_mwc_x(uint64_t &v, uint32_t a)
+{
+    const uint64_t t = (uint64_t)a * (uint32_t)v + (v >> 32);
+    v = t;
+    return (uint32_t)t;
+}
+
 /* exp(-mu) >= 1 - mu: bins that surely draw no star, without exp */
 __device__ __forceinline__ bool bd_surely_empty(float u, float mu)
 {
@@ -205,8 +213,10 @@ __global__ void __launch_bounds__(256) block_lfmax_kernel(BlockLfParams P)
  * walks its stream block by block: the blocks of the 32 streams at the same step
  * are 32 consecutive blocks of (mostly) one pixel, so the table loads coalesce.
  * Lanes whose bin has stars run the sampler together and go on from the state
- * after the stars. */
-template <int MODEL>
+ * after the stars.  BOUND: every request of the launch takes the block bound
+ * (non-negative densities, no distance limits, per-block LF maxima present);
+ * otherwise every bin's expected count is formed and tested exactly. */
+template <int MODEL, bool BOUND>
 __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -266,6 +276,11 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
             __syncwarp();
             loaded = job;
         }
+        if (BOUND && !bound) {
+            /* the host put a request that needs the exact test into the bound launch */
+            if (lane == 0) atomicOr(P.err, 2ull);
+            continue;
+        }
         const int NS = J.rng_nstreams;
         uint32_t *rng = J.rng;
         const bool stream_ok = t < N;
@@ -280,7 +295,7 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
         for (;;) {
             const bool valid = !stop && pix < npix;
             if (!__any_sync(BD_FULL, valid)) break;
-            if (bound) {
+            if constexpr (BOUND) {
                 /* Upper bound of the block's expected counts: the reference's float product
                  * with each factor at its largest over the block (correctly rounded products of
                  * non-negative factors are monotone).  u <= 1 - bound - 3e-7 proves a bin
@@ -288,6 +303,7 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                 uint32_t live = 0, cand = 0;
                 int i0 = 0, j0 = 0, sl0 = 0;
                 float K = 0.f, thr = 0.f;
+                int64_t xthr = -1;             /* uniform u = 2^-32 x passes the bound iff x <= xthr */
                 const float *msr = msbase;
                 const uint64_t w0 = w;
                 if (valid) {
@@ -314,6 +330,7 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                     mub *= Dmax * Dmax * Dmax;
                     mub *= K;
                     thr = (1.0f - mub) - 3.0e-7f;
+                    xthr = gfr::uniform_threshold(thr);
                     if (imax < icut) {
                         live = (1u << GF_BLOCK) - 1u;
                     } else {
@@ -329,11 +346,15 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                             live |= ii < icut ? (1u << s) : 0u;
                         }
                     }
+                    if (xthr < 0) {
+                        cand = live;                   /* the bound proves nothing: exact test throughout */
+                    } else {
+                        const uint32_t X = (uint32_t)xthr;
 #pragma unroll
-                    for (int s = 0; s < GF_BLOCK; s++) {
-                        if ((live >> s) & 1u) {
-                            const float u = bd_mwc_step(w, a);
-                            if (!(u <= thr)) cand |= 1u << s;
+                        for (int s = 0; s < GF_BLOCK; s++) {
+                            if ((live >> s) & 1u) {
+                                if (bd_mwc_x(w, a) > X) cand |= 1u << s;
+                            }
                         }
                     }
                 }
@@ -352,8 +373,9 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                         }
                         if (!((live >> s) & 1u)) continue;
                         const uint64_t wb = w;
-                        const float u = bd_mwc_step(w, a);
-                        if (u <= thr) continue;
+                        const uint32_t xs = bd_mwc_x(w, a);
+                        if ((int64_t)xs <= xthr) continue;
+                        const float u = GF_MWC_SCALE * (float)xs;
                         float r = LFM[j] * ms;
                         r *= norm;
                         r *= D3;
@@ -388,7 +410,7 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                 lb += RN;
                 if (lb >= Bp) { lb -= Bp; pix++; }
                 continue;
-            }
+            } else {
             float mu[GF_BLOCK];
             uint32_t live = 0;
             int i0 = 0, j0 = 0;
@@ -496,6 +518,7 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
             pix += QN;
             lb += RN;
             if (lb >= Bp) { lb -= Bp; pix++; }
+            }
         }
         if (stream_ok && !stop) {
             rng[NS + t] = (uint32_t)(w >> 32);
@@ -585,34 +608,35 @@ size_t batch_draw_warp_bytes(int max_tab, BatchDrawParams *P)
     return off;
 }
 
-cudaError_t launch_batch_draw(const BatchDrawParams &P, int model_type, int warps_per_cta, cudaStream_t s)
+template <int MODEL, bool BOUND>
+cudaError_t launch_batch_draw_t(const BatchDrawParams &P, int warps_per_cta, size_t smem, cudaStream_t s)
+{
+    const int threads = 32 * warps_per_cta;
+    cudaError_t e = cudaFuncSetAttribute(batch_draw_kernel<MODEL, BOUND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_draw_kernel<MODEL, BOUND>, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    const long long want = ((long long)P.nitems + warps_per_cta - 1) / warps_per_cta;
+    const int blocks = (int)std::min<long long>(want, (long long)sm_count() * per_sm);
+    batch_draw_kernel<MODEL, BOUND><<<blocks, threads, smem, s>>>(P);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_draw(const BatchDrawParams &P, int model_type, int warps_per_cta, bool bound, cudaStream_t s)
 {
     if (P.nitems <= 0) return cudaSuccess;
     if (warps_per_cta < 1 || warps_per_cta > 8) warps_per_cta = 4;
     const size_t smem = (size_t)warps_per_cta * P.warp_bytes;
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
-    const int threads = 32 * warps_per_cta;
     cudaError_t e = cudaMemsetAsync(P.next_item, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    if (model_type == GF_MODEL_EXP_DISK) {
-        e = cudaFuncSetAttribute(batch_draw_kernel<GF_MODEL_EXP_DISK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_draw_kernel<GF_MODEL_EXP_DISK>, threads, smem);
-    } else {
-        e = cudaFuncSetAttribute(batch_draw_kernel<GF_MODEL_POWER_LAW_ELLIPSOID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_draw_kernel<GF_MODEL_POWER_LAW_ELLIPSOID>, threads, smem);
-    }
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
-    const long long want = ((long long)P.nitems + warps_per_cta - 1) / warps_per_cta;
-    const int blocks = (int)std::min<long long>(want, (long long)sm_count() * per_sm);
     if (model_type == GF_MODEL_EXP_DISK)
-        batch_draw_kernel<GF_MODEL_EXP_DISK><<<blocks, threads, smem, s>>>(P);
-    else
-        batch_draw_kernel<GF_MODEL_POWER_LAW_ELLIPSOID><<<blocks, threads, smem, s>>>(P);
-    count_launches(1);
-    return cudaGetLastError();
+        return bound ? launch_batch_draw_t<GF_MODEL_EXP_DISK, true>(P, warps_per_cta, smem, s)
+                     : launch_batch_draw_t<GF_MODEL_EXP_DISK, false>(P, warps_per_cta, smem, s);
+    return bound ? launch_batch_draw_t<GF_MODEL_POWER_LAW_ELLIPSOID, true>(P, warps_per_cta, smem, s)
+                 : launch_batch_draw_t<GF_MODEL_POWER_LAW_ELLIPSOID, false>(P, warps_per_cta, smem, s);
 }
 
 cudaError_t expand_temp_bytes(int64_t nev, size_t *bytes)

@@ -41,12 +41,18 @@ void dev_free(T *&p)
     } while (0)
 
 namespace gfa {
+/* Every device allocation of the library goes through here: cudaMalloc, or the
+ * out-of-memory error that gf_debug_fail_allocations arranges, without calling it. */
+cudaError_t device_malloc(void **p, size_t bytes);
+/* gf_debug_fail_allocations */
+void set_alloc_failures(long long after, long long count);
+
 template <typename T>
 gf_status dev_alloc(T **p, size_t n)
 {
     *p = nullptr;
     if (n == 0) return GF_OK;
-    GF_CUDA(cudaMalloc((void **)p, n * sizeof(T)));
+    GF_CUDA(device_malloc((void **)p, n * sizeof(T)));
     return GF_OK;
 }
 }  // namespace gfa
@@ -71,6 +77,8 @@ struct gf_ctx {
     MultiWS *multi_ws = nullptr;         /* buffers of gf_catalog_run_multi kept between calls */
     gf_table plain_table = {};           /* output table of gf_catalog_run, kept for the next call of the same shape */
     int32_t draw_wpc[3] = {0, 0, 0};      /* warps per CTA of the batched draw, by model kind (0: not tuned yet) */
+    uint32_t host_cols = GF_COL_ALL;     /* columns gf_catalog_run_multi_host copies to host memory */
+    double admit_sigma = 8.0;            /* batched if expected + admit_sigma sqrt(expected) + 1024 < capacity */
 };
 
 struct gf_photometry {
@@ -91,6 +99,8 @@ gf_status check_ctx(gf_ctx *ctx);
  * [0, n): rows a module skips (hidden stars) read zero whatever the table held before */
 gf_status zero_module_rows(gf_ctx *ctx, const gf_table *t, int64_t n);
 void free_multi_ws(gf_ctx *ctx);
+/* free the buffers a context keeps between calls (output table, multi-request workspace) */
+void release_caches(gf_ctx *ctx);
 /* multipliers and jump tables of all 65536 streams on the context's device */
 gf_status ensure_multipliers(gf_ctx *ctx);
 

@@ -110,6 +110,7 @@ cudaError_t launch_tie_gather_multi(const LaunchPlaceMulti &L, const int64_t *ro
 
 /* modules (gf_modules.cu) */
 cudaError_t launch_clipper(const gf_footprint &foot, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
+cudaError_t launch_poisson_stream(uint32_t *st, const float *mu, int32_t n, uint32_t *out, cudaStream_t s);
 cudaError_t launch_fixedfeh(const gf_fixedfeh_config &c, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
 cudaError_t launch_bond2010(const gf_bond2010_config &c, uint32_t *rng, int32_t rng_nstreams, gf_table t,
                             int64_t begin, int64_t end, cudaStream_t s);
@@ -211,7 +212,9 @@ struct BatchDrawParams {
 cudaError_t launch_slot_density(const SlotDensityParams &P, int model_type, cudaStream_t s);
 cudaError_t launch_block_lfmax(const BlockLfParams &P, cudaStream_t s);
 size_t batch_draw_warp_bytes(int max_tab, BatchDrawParams *P);
-cudaError_t launch_batch_draw(const BatchDrawParams &P, int model_type, int warps_per_cta, cudaStream_t s);
+/* bound: every request of P takes the block bound of its expected counts (see
+ * batch_draw_kernel); otherwise every bin is tested exactly */
+cudaError_t launch_batch_draw(const BatchDrawParams &P, int model_type, int warps_per_cta, bool bound, cudaStream_t s);
 cudaError_t expand_temp_bytes(int64_t nev, size_t *bytes);
 /* star records of the events at offsets from a scan over k; *total = the stars of all events */
 cudaError_t launch_expand_events(const EventRecord *ev, int64_t nev, const CrawlJob *jobs, int64_t *k64, int64_t *off64,

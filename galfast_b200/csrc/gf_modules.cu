@@ -29,6 +29,26 @@ static int grid_for(int64_t n, int threads)
     return (int)b;
 }
 
+/* ---------------- sampler check: Poisson deviates of one stream ---------------- */
+/* rng_t::poisson (cuda_rng.h:344-376) applied to mu[0..n) one after another on a
+ * single stream: the device form of the sampler, including the gamma_int /
+ * binomial reduction for mu > 10 that catalog bins rarely reach. */
+__global__ void poisson_stream_kernel(uint32_t *st, const float *mu, int32_t n, uint32_t *out)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    gfr::Mwc r;
+    r.a = st[0]; r.c = st[1]; r.x = st[2]; r.used = 0;
+    for (int32_t i = 0; i < n; i++) out[i] = r.poisson(mu[i]);
+    st[0] = r.a; st[1] = r.c; st[2] = r.x;
+}
+
+cudaError_t launch_poisson_stream(uint32_t *st, const float *mu, int32_t n, uint32_t *out, cudaStream_t s)
+{
+    poisson_stream_kernel<<<1, 32, 0, s>>>(st, mu, n, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 /* ---------------- clipper ---------------- */
 __device__ __forceinline__ void clip_row(const gf_footprint &foot, gf_table &t, int64_t row)
 {

@@ -146,6 +146,11 @@ struct ReqInfo {
     std::vector<gf_model_config> mc;
     int64_t pix_off = 0;
     bool plain = false;
+    /* batched, but one model's stars filled a whole output batch: its rows of that
+     * pass on are withheld and the request runs alone at the end, delivering only
+     * the components it had not delivered yet */
+    bool overflow = false;
+    std::vector<int32_t> delivered;    /* components delivered by batched passes */
     int group = 0;
     int slot = -1;
     double cost = 0;
@@ -248,13 +253,19 @@ struct PlainForward {
     void *user;
     int32_t njobs, job;
     std::vector<int64_t> begin, count;
+    std::vector<int32_t> skip;         /* components already delivered by batched passes */
 };
+
+bool skipped(const std::vector<int32_t> &skip, int32_t comp)
+{
+    return std::find(skip.begin(), skip.end(), comp) != skip.end();
+}
 
 int forward_plain_batch(void *u, int32_t model, const gf_table *dev, int64_t row_offset)
 {
     (void)row_offset;
     PlainForward *f = (PlainForward *)u;
-    if (!f->cb) return 0;
+    if (!f->cb || skipped(f->skip, model)) return 0;
     std::fill(f->begin.begin(), f->begin.end(), 0);
     std::fill(f->count.begin(), f->count.end(), 0);
     f->count[f->job] = dev->size;
@@ -268,31 +279,44 @@ namespace {
 /* ---- host delivery: rows copied to a page-locked ring while the device works on ---- */
 #define GF_RING 3
 
-/* bytes of one row of a table with nb bands */
-size_t row_bytes(int nb)
+/* bytes of one row of a table with nb bands, counting the columns in mask (GF_COL_*) */
+size_t row_bytes(int nb, uint32_t mask)
 {
-    return 16 + 4 + 8 + 4 + 4 + 12 + 4 + 4 + 4 + 4 + 4 + 12 + 4 * (size_t)nb + 4 + 4 * (size_t)nb + 12 + 16;
+    const size_t w[17] = {16, 4, 8, 4, 4, 12, 4, 4, 4, 4, 4, 12, 4 * (size_t)nb, 4, 4 * (size_t)nb, 12, 16};
+    size_t b = 0;
+    for (int i = 0; i < 17; i++)
+        if (mask & (1u << i)) b += w[i];
+    return b;
 }
 
-/* host table of `cap` rows and nb bands over page-locked memory at p (column by column) */
-gf_table carve_table(char *p, int64_t cap, int nb)
+/* host table of `cap` rows and nb bands over page-locked memory at p (column by
+ * column; the columns outside mask stay NULL and are not copied) */
+gf_table carve_table(char *p, int64_t cap, int nb, uint32_t mask)
 {
     gf_table t;
     memset(&t, 0, sizeof(t));
     t.capacity = cap;
     t.nbands = nb;
     const size_t n = (size_t)cap;
-    auto take = [&](size_t bytes) { char *r = p; p += (bytes + 255) & ~(size_t)255; return (void *)r; };
-    t.lb = (double *)take(16 * n); t.projIdx = (int32_t *)take(4 * n); t.projXY = (float *)take(8 * n);
-    t.DM = (float *)take(4 * n); t.absmag = (float *)take(4 * n); t.XYZ = (float *)take(12 * n);
-    t.comp = (int32_t *)take(4 * n); t.Am = (float *)take(4 * n); t.AmInf = (float *)take(4 * n);
-    t.hidden = (int32_t *)take(4 * n); t.FeH = (float *)take(4 * n); t.vcyl = (float *)take(12 * n);
-    if (nb) { t.mags = (float *)take(4 * n * nb); t.obsmags = (float *)take(4 * n * nb); }
-    t.photoflags = (int32_t *)take(4 * n); t.pm = (float *)take(12 * n); t.radec = (double *)take(16 * n);
+    auto take = [&](uint32_t col, size_t bytes) -> void * {
+        if (!(mask & col) || bytes == 0) return nullptr;
+        char *r = p;
+        p += (bytes + 255) & ~(size_t)255;
+        return (void *)r;
+    };
+    t.lb = (double *)take(GF_COL_LB, 16 * n); t.projIdx = (int32_t *)take(GF_COL_PROJIDX, 4 * n);
+    t.projXY = (float *)take(GF_COL_PROJXY, 8 * n); t.DM = (float *)take(GF_COL_DM, 4 * n);
+    t.absmag = (float *)take(GF_COL_ABSMAG, 4 * n); t.XYZ = (float *)take(GF_COL_XYZ, 12 * n);
+    t.comp = (int32_t *)take(GF_COL_COMP, 4 * n); t.Am = (float *)take(GF_COL_AM, 4 * n);
+    t.AmInf = (float *)take(GF_COL_AMINF, 4 * n); t.hidden = (int32_t *)take(GF_COL_HIDDEN, 4 * n);
+    t.FeH = (float *)take(GF_COL_FEH, 4 * n); t.vcyl = (float *)take(GF_COL_VCYL, 12 * n);
+    t.mags = (float *)take(GF_COL_MAGS, 4 * n * nb); t.photoflags = (int32_t *)take(GF_COL_PHOTOFLAGS, 4 * n);
+    t.obsmags = (float *)take(GF_COL_OBSMAGS, 4 * n * nb); t.pm = (float *)take(GF_COL_PM, 12 * n);
+    t.radec = (double *)take(GF_COL_RADEC, 16 * n);
     return t;
 }
 
-size_t carved_bytes(int64_t cap, int nb) { return row_bytes(nb) * (size_t)cap + 20 * 256; }
+size_t carved_bytes(int64_t cap, int nb, uint32_t mask) { return row_bytes(nb, mask) * (size_t)cap + 20 * 256; }
 
 /* rows [r0, r1) of the device table d into the host table h, on stream cs */
 gf_status copy_rows_async(const gf_table &d, int64_t r0, int64_t r1, gf_table &h, cudaStream_t cs)
@@ -379,6 +403,7 @@ struct PlainHostForward {
     HostDelivery *hd;
     gf_ctx *ctx;
     int32_t njobs, job;
+    std::vector<int32_t> skip;         /* components already delivered by batched passes */
 };
 
 /* a plain-path batch of a request run inside the multi call, delivered to the host
@@ -388,6 +413,7 @@ int forward_plain_host(void *u, int32_t model, const gf_table *dev, int64_t row_
     (void)row_offset;
     PlainHostForward *f = (PlainHostForward *)u;
     HostDelivery &hd = *f->hd;
+    if (skipped(f->skip, model)) return 0;
     for (int64_t r0 = 0; r0 < dev->size; r0 += hd.piece_rows) {
         const int64_t r1 = std::min(dev->size, r0 + hd.piece_rows);
         gf_table h = hd.ring[0];
@@ -760,7 +786,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         for (int j : integ) {
             /* room for the Poisson spread of the model's stars in one batch */
             const double e = S[j].expected[i];
-            if (e + 8.0 * sqrt(e) + 1024.0 >= (double)jobs[j].capacity) R[j].plain = true;
+            if (e + ctx->admit_sigma * sqrt(e) + 1024.0 >= (double)jobs[j].capacity) R[j].plain = true;
         }
     }
 
@@ -874,9 +900,10 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         hd.user = user;
         hd.piece_rows = piece_rows > 0 ? piece_rows : (int64_t)4 << 20;
         hd.nbands = nbands;
-        const size_t slot_bytes = carved_bytes(hd.piece_rows, nbands);
+        const size_t slot_bytes = carved_bytes(hd.piece_rows, nbands, ctx->host_cols);
         GF_TRY(ws.ring.need(slot_bytes * GF_RING));
-        for (int r = 0; r < GF_RING; r++) hd.ring[r] = carve_table(ws.ring.p + (size_t)r * slot_bytes, hd.piece_rows, nbands);
+        for (int r = 0; r < GF_RING; r++)
+            hd.ring[r] = carve_table(ws.ring.p + (size_t)r * slot_bytes, hd.piece_rows, nbands, ctx->host_cols);
     }
     /* the copy stream finishes (and stops calling back) before this function returns */
     struct CopyDrain {
@@ -973,15 +1000,25 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                 if (gfk::batch_draw_warp_bytes(max_tab(i, batched), &B) > 200 * 1024)
                     return fail(GF_E_UNSUPPORTED, "magnitude grid too large for the batched draw");
                 B.jobs = d_jobs; B.plans = ws.plans.p; B.ms = ws.msptr.p;
-                /* work items: 32 consecutive streams of a request, requests in decreasing size */
+                /* work items: 32 consecutive streams of a request, requests in decreasing size;
+                 * first the requests that take the block bound of their expected counts
+                 * (non-negative densities, no distance limits), then the others */
                 const int ngroups = (N + 31) / 32;
                 GF_TRY(ws.gitems.need((size_t)batched.size() * ngroups));
+                int32_t nbound = 0;
                 {
                     GF_TRY(ws.h_stage.need(4 * batched.size() * (size_t)ngroups));
                     uint32_t *gi = (uint32_t *)ws.h_stage.p;
                     size_t q = 0;
-                    for (int j : batched)
-                        for (int g = 0; g < ngroups; g++) gi[q++] = ((uint32_t)j << 16) | (uint32_t)(32 * g);
+                    for (int pass_bound = 1; pass_bound >= 0; pass_bound--) {
+                        for (int j : batched) {
+                            const SkyModel &mj = R[j].hm[i].m;
+                            const bool bj = mj.dmin == 0.f && mj.dmax == 0.f && mj.f >= 0.f && mj.norm >= 0.f;
+                            if (bj != (pass_bound == 1)) continue;
+                            for (int g = 0; g < ngroups; g++) gi[q++] = ((uint32_t)j << 16) | (uint32_t)(32 * g);
+                        }
+                        if (pass_bound == 1) nbound = (int32_t)q;
+                    }
                     GF_CUDA(cudaMemcpyAsync(ws.gitems.p, gi, 4 * q, cudaMemcpyHostToDevice, st));
                     GF_CUDA(cudaStreamSynchronize(st));
                 }
@@ -990,11 +1027,24 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                 B.ev_count = ctx->d_counters; B.err = ctx->d_counters + 2;
                 GF_TRY(ws.ev.need((size_t)cap));
                 B.ev = ws.ev.p; B.ev_capacity = (int64_t)ws.ev.n;
+                /* the two launches of a draw pass: bound requests, then exact ones */
+                auto draw_all = [&](const gfk::BatchDrawParams &BB, int wpc) -> gf_status {
+                    gfk::BatchDrawParams X = BB;
+                    X.nitems = nbound;
+                    GF_CUDA(gfk::launch_batch_draw(X, mtype, wpc, true, st));
+                    X.items = BB.items + nbound;
+                    X.nitems = ngitems - nbound;
+                    GF_CUDA(gfk::launch_batch_draw(X, mtype, wpc, false, st));
+                    return GF_OK;
+                };
                 if (ctx->draw_wpc[mtype] == 0) {
                     /* autotuner: time 8, 4, 2 and 1 warps per CTA on the head of the work queue
                      * (the largest requests), from the same stream states, and keep the fastest */
+                    const bool tb = nbound > 0;
                     gfk::BatchDrawParams T = B;
-                    T.nitems = std::min<int32_t>(ngitems, std::max<int32_t>(ngitems / 16, 148 * 8));
+                    const int32_t avail = tb ? nbound : ngitems;
+                    T.items = B.items + (tb ? 0 : nbound);
+                    T.nitems = std::min<int32_t>(avail, std::max<int32_t>(avail / 16, 148 * 8));
                     float best_ms = 0.f;
                     int best = 4;
                     cudaEvent_t e0, e1;
@@ -1004,7 +1054,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                         GF_CUDA(cudaMemcpyAsync(d_rng, d_rng_snap, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
                         GF_CUDA(cudaMemsetAsync(ctx->d_counters, 0, 24, st));
                         GF_CUDA(cudaEventRecord(e0, st));
-                        GF_CUDA(gfk::launch_batch_draw(T, mtype, wpc, st));
+                        GF_CUDA(gfk::launch_batch_draw(T, mtype, wpc, tb, st));
                         GF_CUDA(cudaEventRecord(e1, st));
                         GF_CUDA(cudaEventSynchronize(e1));
                         float ms = 0.f;
@@ -1021,11 +1071,12 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                     GF_CUDA(cudaMemsetAsync(ctx->d_counters, 0, 24, st));
                     {
                         ProfScope ps(ctx, GF_PROF_BATCH_DRAW);
-                        GF_CUDA(gfk::launch_batch_draw(B, mtype, ctx->draw_wpc[mtype], st));
+                        GF_TRY(draw_all(B, ctx->draw_wpc[mtype]));
                     }
                     GF_CUDA(cudaMemcpyAsync(ctx->h_counters, ctx->d_counters, 24, cudaMemcpyDeviceToHost, st));
                     GF_CUDA(cudaStreamSynchronize(st));
                     nev = (int64_t)ctx->h_counters[0];
+                    if (ctx->h_counters[2] & 2ull) return fail(GF_E_STATE, "internal: a request without the block bound in the bound draw");
                     if (ctx->h_counters[2]) return fail(GF_E_INVALID, "a bin has an infinite expected star count");
                     if (nev <= B.ev_capacity) break;
                     /* more bins with stars than the event list holds: restore the streams and draw again */
@@ -1116,8 +1167,23 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                 const int j = slot_job[s];
                 const int64_t gen = seg[2 * nslots + s] - seg[s];
                 const int64_t vis = gen > 0 ? seg[nslots + s] - seg[s] : 0;
-                if (gen >= jobs[j].capacity)
-                    return fail(GF_E_STATE, "a request drew a full output batch in the multi-request run; run it with gf_catalog_run");
+                if (gen >= jobs[j].capacity && !R[j].overflow) {
+                    /* the batch rules of the plain path apply: withhold this request's rows
+                     * from here on and run it alone after the batched passes */
+                    R[j].overflow = true;
+                    R[j].plain = true;
+                }
+                if (R[j].overflow) {
+                    /* no rows of this slot in the output: its visible range ends where it begins */
+                    seg[nslots + s] = seg[s];
+                    GF_CUDA(cudaMemcpyAsync(d_seg + nslots + s, &seg[nslots + s], 8, cudaMemcpyHostToDevice, st));
+                    slot_rows[s] = 0;
+                    row_begin[s + 1] = row_begin[s];
+                    chunk_begin[s] = nchunks;
+                    slot_comp[s] = R[j].hm[i].m.comp;
+                    continue;
+                }
+                R[j].delivered.push_back(R[j].hm[i].m.comp);
                 S[j].generated[i] = gen;
                 S[j].stored[i] = vis;
                 if (vis > 0) S[j].batches++;
@@ -1206,10 +1272,12 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         if (to_host) {
             PlainHostForward f;
             f.hd = &hd; f.ctx = ctx; f.njobs = njobs; f.job = j;
+            f.skip = R[j].delivered;
             GF_TRY(gf_catalog_run(ctx, &jobs[j], forward_plain_host, &f, &S[j]));
         } else {
             PlainForward f;
             f.cb = cb; f.user = user; f.njobs = njobs; f.job = j;
+            f.skip = R[j].delivered;
             f.begin.assign(njobs, 0);
             f.count.assign(njobs, 0);
             GF_TRY(gf_catalog_run(ctx, &jobs[j], forward_plain_batch, &f, &S[j]));
@@ -1220,10 +1288,44 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
 
 }  // namespace
 
+namespace {
+struct CountingMulti {
+    gf_multi_callback cb;
+    void *user;
+    std::atomic<long long> calls{0};
+};
+int counting_multi(void *u, int32_t model, const gf_table *t, const int64_t *rb, const int64_t *rc)
+{
+    CountingMulti *c = (CountingMulti *)u;
+    c->calls++;
+    return c->cb ? c->cb(c->user, model, t, rb, rc) : 0;
+}
+
+/* An out-of-memory failure before any rows were delivered frees the context's
+ * cached buffers and runs the call once more, as the reference collects garbage
+ * and retries a failed allocation (cux.cpp:189-198).  Every request's streams
+ * are seeded again, so the retry is the same run. */
+gf_status run_multi_retry(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, gf_multi_host_callback hcb,
+                          int64_t piece_rows, void *user, gf_catalog_stats *stats)
+{
+    CountingMulti c;
+    c.cb = cb ? cb : hcb;
+    c.user = user;
+    gf_multi_callback d = cb ? counting_multi : nullptr;
+    gf_multi_host_callback h = hcb ? counting_multi : nullptr;
+    gf_status st = run_multi(ctx, jobs, njobs, d, h, piece_rows, &c, stats);
+    if (st == GF_E_OOM && c.calls.load() == 0) {
+        gfa::release_caches(ctx);
+        st = run_multi(ctx, jobs, njobs, d, h, piece_rows, &c, stats);
+    }
+    return st;
+}
+}  // namespace
+
 extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, void *user,
                                           gf_catalog_stats *stats)
 {
-    return run_multi(ctx, jobs, njobs, cb, nullptr, 0, user, stats);
+    return run_multi_retry(ctx, jobs, njobs, cb, nullptr, 0, user, stats);
 }
 
 extern "C" gf_status gf_catalog_run_multi_host(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, int64_t piece_rows,
@@ -1231,7 +1333,23 @@ extern "C" gf_status gf_catalog_run_multi_host(gf_ctx *ctx, const gf_job *jobs, 
 {
     if (!cb) return fail(GF_E_INVALID, "host delivery needs a callback");
     if (piece_rows < 0) return fail(GF_E_INVALID, "negative piece size");
-    return run_multi(ctx, jobs, njobs, nullptr, cb, piece_rows, user, stats);
+    return run_multi_retry(ctx, jobs, njobs, nullptr, cb, piece_rows, user, stats);
+}
+
+extern "C" gf_status gf_multi_set_admission(gf_ctx *ctx, double sigmas)
+{
+    GF_TRY(gfa::check_ctx(ctx));
+    if (!(sigmas >= -1000.0 && sigmas <= 1000.0)) return fail(GF_E_INVALID, "admission margin out of range");
+    ctx->admit_sigma = sigmas;
+    return GF_OK;
+}
+
+extern "C" gf_status gf_multi_set_host_columns(gf_ctx *ctx, uint32_t columns)
+{
+    GF_TRY(gfa::check_ctx(ctx));
+    if (columns & ~(uint32_t)GF_COL_ALL) return fail(GF_E_INVALID, "unknown column bits");
+    ctx->host_cols = columns;
+    return GF_OK;
 }
 
 extern "C" gf_status gf_multi_set_memory_budget(gf_ctx *ctx, int64_t bytes)

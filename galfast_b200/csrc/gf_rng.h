@@ -184,6 +184,25 @@ struct Mwc {
     }
 };
 
+/* The largest x in [0, 2^32) whose uniform 2^-32 * (float)x (x rounded to float,
+ * to nearest even, then scaled exactly) is <= thr, or -1 when none is: a test
+ * u <= thr on the next uniform becomes x <= threshold on the integer state,
+ * without the conversion. */
+GFR_HD int64_t uniform_threshold(float thr)
+{
+    if (!(thr >= 0.f)) return -1;
+    const float T = thr * 4294967296.0f;               /* exact: scaling by 2^32 */
+    if (T >= 4294967296.0f) return 0xffffffffll;
+    if (T < 16777216.0f) return (int64_t)T;             /* below 2^24 every integer is a float */
+    union { float f; uint32_t u; } cv;
+    cv.f = T;
+    const uint32_t bits = cv.u;
+    const int e = (int)(bits >> 23) - 127;              /* 24 <= e <= 31 */
+    const int64_t half = (int64_t)1 << (e - 24);        /* half the spacing of floats above T */
+    /* x in (T, T + half) rounds down to T; x = T + half is a tie, kept by an even mantissa */
+    return (int64_t)T + half - 1 + ((bits & 1u) ? 0 : 1);
+}
+
 /* (a * b) mod p for the stream prime p = A*2^32 - 1, a, b < p.
  * The 128-bit product N is folded with N -> A*(N mod 2^32) + (N >> 32), which
  * multiplies the residue by 2^-32 (mod p); the caller pre-scales one operand

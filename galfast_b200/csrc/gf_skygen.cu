@@ -912,16 +912,21 @@ static std::atomic<long long> g_launches(0);
 void count_launches(int n) { g_launches += n; }
 long long launches() { return g_launches.load(); }
 
-static int sm_count_cached = 0;
+/* SM count of the current device, cached per device (any host thread) */
+static std::atomic<int> g_sm_count[64];
 int sm_count()
 {
-    if (!sm_count_cached) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sm_count_cached, cudaDevAttrMultiProcessorCount, dev);
-        if (sm_count_cached <= 0) sm_count_cached = 148;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64) {
+        const int c = g_sm_count[dev].load(std::memory_order_relaxed);
+        if (c > 0) return c;
     }
-    return sm_count_cached;
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+    if (dev >= 0 && dev < 64) g_sm_count[dev].store(n, std::memory_order_relaxed);
+    return n;
 }
 
 static void fill_job(CrawlJob &J, const LaunchCrawl &L)
@@ -947,12 +952,10 @@ static void fill_job(CrawlJob &J, const LaunchCrawl &L)
 template <int DRAW, int MODEL, int CW>
 static cudaError_t start_crawl(const CrawlParams &P, size_t smem, cudaStream_t s)
 {
-    static bool attr_set = false;       /* the per-model tables may exceed the 48 KB default */
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(crawl_kernel<DRAW, MODEL, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    /* the per-model tables may exceed the 48 KB default; the opt-in is a property of
+     * the current device's context, so it is set before every launch (it is cheap) */
+    cudaError_t e = cudaFuncSetAttribute(crawl_kernel<DRAW, MODEL, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    if (e != cudaSuccess) return e;
     crawl_kernel<DRAW, MODEL, CW><<<P.nitems, (CW * 32), smem, s>>>(P);
     return cudaSuccess;
 }
@@ -1125,14 +1128,10 @@ cudaError_t launch_seed_streams(const uint32_t *seeds, int njobs, const uint32_t
 template <int DRAW, int MODEL, int CW>
 static cudaError_t start_crawl_persistent(const CrawlParams &P, size_t smem, cudaStream_t s)
 {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(crawl_kernel<DRAW, MODEL, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    cudaError_t e = cudaFuncSetAttribute(crawl_kernel<DRAW, MODEL, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, crawl_kernel<DRAW, MODEL, CW>, (CW * 32), smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, crawl_kernel<DRAW, MODEL, CW>, (CW * 32), smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     int grid = sm_count() * per_sm;

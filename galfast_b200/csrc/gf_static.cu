@@ -13,13 +13,14 @@
  *
  * The array is a file-scope __device__ object: every GPU that loads this
  * library holds its 1.3 MB until the process exits.  Its device address is
- * looked up once per device, on the first call made with that device current,
- * with cudaGetSymbolAddress; make that first call before any stream capture.
- * All calls share the array and it keeps the last call's contents (the
- * partial sums are cleared at the start of every call), so calls that overlap
- * on the GPU -- from two host threads, or on two streams -- race; the entry
- * point synchronises its stream before returning, so calls made one after
- * another from one thread do not overlap.
+ * looked up once per device (devices 0-63), on the first call made with that
+ * device current, with cudaGetSymbolAddress.  Every call copies the LF from
+ * host memory and synchronises its stream before it returns, also when it
+ * fails, so it must not be called while its stream is being captured.  All
+ * calls share the array and it keeps the last call's contents (the partial
+ * sums are cleared at the start of every call), so calls that overlap on the
+ * GPU -- from two host threads, or on two streams -- race; calls made one
+ * after another from one thread do not overlap.
  */
 #include "gf_launch.h"
 #include "gf_host.h"
@@ -81,7 +82,8 @@ extern "C" gf_status gf_skygen_integrate_static(const gf_skygen_config *cfg, con
         return sfail(GF_E_INVALID, "nm*nM above the static scratch limit of 65536 bins per pixel");
 
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return sfail(GF_E_CUDA, "no current CUDA device");
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return sfail(GF_E_CUDA, "no current CUDA device");
+    if (dev >= 64) return sfail(GF_E_UNSUPPORTED, "device index above the static entry point's limit of 64 devices");
     StaticScratch *S = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_addr_mutex);
@@ -98,7 +100,10 @@ extern "C" gf_status gf_skygen_integrate_static(const gf_skygen_config *cfg, con
     if (e == cudaSuccess) e = cudaMemsetAsync(S->counts, 0, sizeof(double) * (size_t)cfg->nthreads, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(S->covered, 0, sizeof(double) * (size_t)cfg->nthreads, st);
     if (e == cudaSuccess) e = gfk::launch_dtab(hm, S->dtab, st);
-    if (e != cudaSuccess) return sfail(GF_E_CUDA, std::string("setup: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+        cudaStreamSynchronize(st);     /* nothing of this call stays in flight on the shared array */
+        return sfail(GF_E_CUDA, std::string("setup: ") + cudaGetErrorString(e));
+    }
 
     gfk::LaunchCrawl L;
     memset(&L, 0, sizeof(L));
@@ -135,6 +140,9 @@ extern "C" gf_status gf_skygen_integrate_static(const gf_skygen_config *cfg, con
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return sfail(GF_E_CUDA, std::string("integrate: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+        cudaStreamSynchronize(st);
+        return sfail(GF_E_CUDA, std::string("integrate: ") + cudaGetErrorString(e));
+    }
     return GF_OK;
 }

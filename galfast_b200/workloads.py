@@ -309,6 +309,22 @@ def build_workload(lib, *, foot, dx_deg, m0, m1, nthreads=7680, seed48=42, capac
     return w
 
 
+def restrict_pixels(w, idx):
+    """The workload `w` restricted to the pixels `idx` (per-beam extinction rows
+    renumbered); the grid, models, seeds and module chain are unchanged."""
+    import copy
+    sub = copy.copy(w)
+    pix = np.frombuffer(w.pixels, dtype=np.uint8).reshape(w.npixels, -1)[idx].copy()
+    pb = (A.PencilBeam * len(idx)).from_buffer(pix)
+    for k in range(len(idx)):
+        pb[k].extIdx = k
+    sub.pixels = bytearray(pix.tobytes())
+    sub.npixels = len(idx)
+    sub.ammin = np.ascontiguousarray(w.ammin[idx])
+    sub.keep = list(w.keep)
+    return sub
+
+
 def config1(lib, **kw):
     """10x10 deg patch centred on the north galactic pole, 0.25 deg pixels, 15 < r < 21."""
     half = 5.0 * D2R

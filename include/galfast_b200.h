@@ -271,6 +271,13 @@ uint32_t gf_rng_seed48_from_cli_seed(uint64_t seed);
 gf_status gf_rng_get_state(gf_ctx *ctx, uint32_t *host_state, int32_t nstreams);
 gf_status gf_rng_set_state(gf_ctx *ctx, const uint32_t *host_state, int32_t nstreams);
 
+/* n Poisson deviates drawn one after another from ONE stream on the device:
+ * out[i] = poisson(mu[i]) with rng_t::poisson (src/common/cuda_rng.h:344-376),
+ * including its gamma / binomial reduction for mu > 10.  state[3] = (a, c, x),
+ * host memory, updated to the stream's state after the draws.  A direct check
+ * of the sampler the draw kernels use; means must lie in [0, 1e7). */
+gf_status gf_rng_poisson(gf_ctx *ctx, uint32_t state[3], const float *mu, int32_t n, uint32_t *out);
+
 /* ---- skygen ---- */
 
 /* Build the generator for a footprint pixelisation and a list of models
@@ -415,15 +422,24 @@ typedef int (*gf_multi_callback)(void *user, int32_t model, const gf_table *dev_
  * chain of each, as gf_catalog_run), generated together: every crawl, sort
  * and module pass covers all requests at once.  Each request's rows are those
  * gf_catalog_run produces for it alone, bit for bit.  A request whose expected
- * stars of some model reach its batch capacity (within 8 sigma), or whose grid
- * has nm*nM not a multiple of 10, runs alone through gf_catalog_run after the
- * others.  All requests need the same nthreads, model kinds (in component
+ * stars of some model reach its batch capacity (within 8 sigma, see
+ * gf_multi_set_admission), or whose grid has nm*nM not a multiple of 10, runs
+ * alone through gf_catalog_run after the others.  All requests need the same nthreads, model kinds (in component
  * order) and fixedFeH/Bond2010/vel2pm/gal2other settings, nstreams > 0 and
  * nstars = 0; footprints, models, grids, seeds, capacities and photometry may
  * differ.  stats: njobs entries or NULL.  No counterpart in the reference,
  * which generates one catalog per process (os_skygen.cpp:866-932). */
 gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, void *user,
                                gf_catalog_stats *stats);
+
+/* The admission rule of gf_catalog_run_multi: a request is generated with the
+ * others when every model's expected stars e satisfy e + sigmas sqrt(e) + 1024 <
+ * its batch capacity (default sigmas = 8); otherwise it runs alone through
+ * gf_catalog_run.  A batched request whose stars fill a whole batch anyway has
+ * its rows of that model on withheld and runs alone at the end of the call,
+ * delivering only the components not delivered yet, so its catalog is still the
+ * one gf_catalog_run gives it. */
+gf_status gf_multi_set_admission(gf_ctx *ctx, double sigmas);
 
 /* Device memory that one chunk of a multi-request run may use for its draw
  * passes (records, placement, sort and output columns, about 320 bytes per
@@ -446,6 +462,25 @@ typedef int (*gf_multi_host_callback)(void *user, int32_t model, const gf_table 
                                       const int64_t *row_count);
 gf_status gf_catalog_run_multi_host(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, int64_t piece_rows,
                                     gf_multi_host_callback cb, void *user, gf_catalog_stats *stats);
+
+/* Columns of a gf_table (bits for gf_multi_set_host_columns). */
+enum {
+    GF_COL_LB = 1u << 0, GF_COL_PROJIDX = 1u << 1, GF_COL_PROJXY = 1u << 2, GF_COL_DM = 1u << 3,
+    GF_COL_ABSMAG = 1u << 4, GF_COL_XYZ = 1u << 5, GF_COL_COMP = 1u << 6, GF_COL_AM = 1u << 7,
+    GF_COL_AMINF = 1u << 8, GF_COL_HIDDEN = 1u << 9, GF_COL_FEH = 1u << 10, GF_COL_VCYL = 1u << 11,
+    GF_COL_MAGS = 1u << 12, GF_COL_PHOTOFLAGS = 1u << 13, GF_COL_OBSMAGS = 1u << 14, GF_COL_PM = 1u << 15,
+    GF_COL_RADEC = 1u << 16,
+    GF_COL_ALL = (1u << 17) - 1,
+    /* the output catalog of the full-sky form: ra, dec, DM, Mr, true and observed
+     * magnitudes, vR/vPhi/vZ, proper motions (and radial velocity) */
+    GF_COL_CATALOG = GF_COL_RADEC | GF_COL_DM | GF_COL_ABSMAG | GF_COL_MAGS | GF_COL_OBSMAGS | GF_COL_VCYL | GF_COL_PM
+};
+
+/* The columns gf_catalog_run_multi_host copies to host memory (default
+ * GF_COL_ALL); the others are NULL in the host tables the callback sees.  The
+ * column selection of galfast's text output (the output module's column list,
+ * src/pipeline.cpp:199-289), applied before the copy instead of when writing. */
+gf_status gf_multi_set_host_columns(gf_ctx *ctx, uint32_t columns);
 
 /* Warps per CTA of the batched draw kernel (one warp per stream), by model kind
  * (GF_MODEL_*): 1, 2, 4 or 8.  The first gf_catalog_run_multi pass of each kind
@@ -495,11 +530,25 @@ gf_status gf_server_destroy(gf_server *s);
  * The scratch (per-stream partial sums, LF, distance table) is a fixed 1.3 MB
  * __device__ array of the library: at most 65536 streams, 1024 LF samples and
  * 65536 (m, M) bins per pixel; larger requests are rejected with GF_E_INVALID.
- * The first call on each device looks up the array's address (make it before any
- * stream capture); calls share the array, so calls that overlap on the GPU race. */
+ * Devices 0-63 (GF_E_UNSUPPORTED above).  The first call on each device looks up
+ * the array's address.  Every call synchronises its stream before returning,
+ * also on failure, so it must not be called while its stream is being captured.
+ * Calls share the array, so calls that overlap on the GPU race. */
 gf_status gf_skygen_integrate_static(const gf_skygen_config *cfg, const gf_pencil_beam *d_pixels, int32_t npixels,
                                      const float *d_beam_ammin, const gf_extinction *ext,
                                      const gf_model_config *model, double *d_result, void *cuda_stream);
+
+/* ---- failure injection (tests) ---- */
+
+/* Make the library's device allocations fail as if the device were out of
+ * memory, without calling cudaMalloc for them: the allocations after the next
+ * `after` ones fail, `count` of them (0: every one), then allocations succeed
+ * again; after < 0 turns it off.  Process-wide.  gf_catalog_run and
+ * gf_catalog_run_multi answer an out-of-memory failure before their first
+ * delivered rows by freeing the context's cached buffers and running once more
+ * (as src/common/cux.cpp:189-198 collects garbage and retries an allocation);
+ * a second failure returns GF_E_OOM and leaves the context usable. */
+gf_status gf_debug_fail_allocations(int64_t after, int64_t count);
 
 /* ---- host-side setup helpers (no GPU needed) ---- */
 

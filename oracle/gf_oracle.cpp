@@ -24,6 +24,11 @@
 #include <string>
 #include <vector>
 #include <thread>
+#include <atomic>
+#include <condition_variable>
+#include <functional>
+#include <memory>
+#include <mutex>
 
 #ifdef OR_PORTABLE
 #define OR_EXPF gfm::expf_
@@ -378,6 +383,14 @@ struct Sky {
     std::vector<char> ks_alloc;
 };
 
+/* One star row of the skygen columns (os_skygen.cpp:838-858), as draw_stars
+ * fills it; rows hidden by the projection edge carry only hidden = 1. */
+struct StarRow {
+    double l, b;
+    float x, y, absmag, DM, X, Y, Z, Am, AmInf;
+    int32_t projIdx, comp, hidden;
+};
+
 /* The constant part of one kernel launch (skygenGPU<T> in __constant__ memory). */
 struct Launch {
     const Sky *sky;
@@ -387,13 +400,16 @@ struct Launch {
     int stopstars;
     /* draw */
     int *nstars;
-    gf_table *out;
+    gf_table *out;                 /* rows at their atomicAdd index ... */
+    std::vector<StarRow> *rows;    /* ... or appended here (the parallel draw's private runs) */
     KState *ks;
     RngState rng;
     /* integrate */
     double *counts, *countsCovered;
     float *countsCoveredPerBeam;   /* [nthreads][npixels] */
     float *maxCount;
+    int64_t *nabove;               /* diagnostics (nullable): bins with rho > above, per thread */
+    float above;
 };
 
 /* skygen.cu.h:257-300 */
@@ -494,25 +510,49 @@ void deproject(const gf_lambert &p, double &l, double &b, const float x, const f
     l = p.l0 + OR_ATAN2(x * sc, p.cb * cc / ir - y * p.sb * sc);
 }
 
+/* Store one row at index idx of the launch's output. */
+void put_row(const Launch &L, int idx, const StarRow &r)
+{
+    if (L.rows) { L.rows->push_back(r); return; }
+    gf_table &s = *L.out;
+    const int64_t P = s.capacity;
+    s.hidden[idx] = r.hidden;
+    if (r.hidden && r.projIdx < 0) return;          /* beyond the projection edge: only the flag */
+    s.projIdx[idx] = r.projIdx;
+    s.projXY[idx] = r.x;
+    s.projXY[P + idx] = r.y;
+    s.lb[idx] = r.l;
+    s.lb[P + idx] = r.b;
+    s.absmag[idx] = r.absmag;
+    s.DM[idx] = r.DM;
+    s.XYZ[idx] = r.X;
+    s.XYZ[P + idx] = r.Y;
+    s.XYZ[2 * P + idx] = r.Z;
+    s.comp[idx] = r.comp;
+    s.Am[idx] = r.Am;
+    s.AmInf[idx] = r.AmInf;
+}
+
 /* skygen.cu.h:366-457 */
 void draw_stars(const Launch &L, Rng &rng, int &ndraw, const float &M, const int &im, const gf_pencil_beam &pix, float AmMin)
 {
     if (!ndraw) return;
     const Model &m = *L.m;
-    gf_table &s = *L.out;
-    const int64_t P = s.capacity;
     int idx = *L.nstars; *L.nstars += ndraw;          /* CPU atomicAdd, skygen.cu.h:153 */
     for (; ndraw && idx < L.stopstars; idx++, ndraw--) {
+        StarRow r = StarRow();
         float x = pix.X, y = pix.Y;
         x += pix.dx * (rng.uniform() - 0.5f);
         y += pix.dx * (rng.uniform() - 0.5f);
         if (x * x + y * y > 2.f) {
-            s.hidden[idx] = 1;
+            r.hidden = 1;
+            r.projIdx = -1;
+            put_row(L, idx, r);
             continue;
         }
-        s.projIdx[idx] = pix.projIdx;
-        s.projXY[idx] = x;
-        s.projXY[P + idx] = y;
+        r.projIdx = pix.projIdx;
+        r.x = x;
+        r.y = y;
         double l, b;
         deproject(L.sky->cfg.proj[pix.projIdx], l, b, x, y);
         Dir dir2 = make_dir(l, b);
@@ -520,24 +560,25 @@ void draw_stars(const Launch &L, Rng &rng, int &ndraw, const float &M, const int
         if (l < 0.) l += 360.;
         if (l > 360.) l -= 360.;
         b *= dbl_r2d;
-        s.lb[idx] = l;
-        s.lb[P + idx] = b;
+        r.l = l;
+        r.b = b;
         float Mtmp, mtmp, DM;
-        s.absmag[idx] = Mtmp = M + m.dM * (rng.uniform() - 0.5f);
+        r.absmag = Mtmp = M + m.dM * (rng.uniform() - 0.5f);
         mtmp = m.m0 + m.dm * (im + rng.uniform() - 0.5f);
         DM = mtmp - Mtmp;
-        s.DM[idx] = DM;
+        r.DM = DM;
         float D = OR_POWF(10, 0.2f * DM + 1.f);
-        s.XYZ[idx] = D * dir2.cl * dir2.cb;
-        s.XYZ[P + idx] = D * dir2.sl * dir2.cb;
-        s.XYZ[2 * P + idx] = D * dir2.sb;
-        s.comp[idx] = m.comp;
+        r.X = D * dir2.cl * dir2.cb;
+        r.Y = D * dir2.sl * dir2.cb;
+        r.Z = D * dir2.sb;
+        r.comp = m.comp;
         float Am0, Am1;
-        s.Am[idx] = Am0 = star_extinction(L, dir2);
+        r.Am = Am0 = star_extinction(L, dir2);
         Am1 = star_extinction(L, dir2);
-        s.AmInf[idx] = Am1 > Am0 ? Am1 : Am0;
-        s.hidden[idx] = (mtmp + Am0 > m.m1) ? 1 : 0;
-        if (AmMin > Am0) s.AmInf[idx] = -AmMin;
+        r.AmInf = Am1 > Am0 ? Am1 : Am0;
+        r.hidden = (mtmp + Am0 > m.m1) ? 1 : 0;
+        if (AmMin > Am0) r.AmInf = -AmMin;
+        put_row(L, idx, r);
     }
 }
 
@@ -620,6 +661,7 @@ void kernel(const Launch &L, int draw, int tid)
             countCovered += rho * pix.coveredFraction;
             rhoBeam += rho * pix.coveredFraction;
             if (maxCount1 < rho) maxCount1 = rho;
+            if (L.nabove && rho > L.above) L.nabove[tid]++;
         }
     }
 
@@ -642,16 +684,174 @@ thread_local std::string g_err;
 
 int g_nthreads_cpu = 1;     /* host threads used by the parallel loops (or_set_threads) */
 
-/* Run f(i) for i in [0, n) on g_nthreads_cpu host threads (interleaved assignment). */
-template <typename F>
-void parallel_for(int n, F f)
+/* A persistent pool of host threads for the loops over independent streams,
+ * rows and columns.  run(n, f) calls f(i) for every i in [0, n) once, handing
+ * out indices in small chunks from a counter of that run; the calling thread
+ * takes part and returns when every index is done, without waiting for workers
+ * that woke too late to find work.  Idle workers spin briefly before they sleep,
+ * since loops follow one another closely.  Results never depend on which thread
+ * ran an index. */
+class Pool {
+public:
+    ~Pool() { resize(0); }
+    void resize(int nworkers)
+    {
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            stop_ = true;
+            gen_.fetch_add(1);
+        }
+        cv_.notify_all();
+        for (auto &t : th_) t.join();
+        th_.clear();
+        stop_ = false;
+        const uint64_t g0 = gen_.load();      /* workers wait for the first run after this generation */
+        for (int i = 0; i < nworkers; i++) th_.emplace_back([this, g0]() { worker(g0); });
+    }
+    int workers() const { return (int)th_.size(); }
+    void run(int n, int chunk, const std::function<void(int)> &f)
+    {
+        if (th_.empty() || n <= chunk) { for (int i = 0; i < n; i++) f(i); return; }
+        auto job = std::make_shared<Job>();
+        job->f = &f; job->n = n; job->chunk = chunk;
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            cur_ = job;
+            gen_.fetch_add(1);
+        }
+        cv_.notify_all();
+        work(*job);
+        while (job->done.load() < n) std::this_thread::yield();
+    }
+
+private:
+    struct Job {
+        const std::function<void(int)> *f = nullptr;
+        int n = 0, chunk = 1;
+        std::atomic<int> next{0}, done{0};
+    };
+    static void work(Job &j)
+    {
+        for (;;) {
+            int b = j.next.fetch_add(j.chunk);
+            if (b >= j.n) break;
+            int e = std::min(b + j.chunk, j.n);
+            for (int i = b; i < e; i++) (*j.f)(i);
+            j.done.fetch_add(e - b);
+        }
+    }
+    void worker(uint64_t seen)
+    {
+        for (;;) {
+            for (int spin = 0; spin < 20000 && gen_.load() == seen; spin++) std::this_thread::yield();
+            std::shared_ptr<Job> job;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&]() { return gen_.load() != seen; });
+                seen = gen_.load();
+                if (stop_) return;
+                job = cur_;
+            }
+            if (job) work(*job);
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::shared_ptr<Job> cur_;
+    std::atomic<uint64_t> gen_{0};
+    bool stop_ = false;
+};
+
+Pool &pool()
 {
-    int nt = std::max(1, std::min(g_nthreads_cpu, n));
-    if (nt == 1) { for (int i = 0; i < n; i++) f(i); return; }
-    std::vector<std::thread> th;
-    for (int t = 0; t < nt; t++)
-        th.emplace_back([&, t]() { for (int i = t; i < n; i += nt) f(i); });
-    for (auto &x : th) x.join();
+    static Pool p;
+    if (p.workers() != g_nthreads_cpu - 1) p.resize(g_nthreads_cpu - 1);
+    return p;
+}
+
+/* Run f(i) for i in [0, n) on g_nthreads_cpu host threads. */
+template <typename F>
+void parallel_for(int n, F f, int chunk = 16)
+{
+    if (g_nthreads_cpu <= 1 || n <= 1) { for (int i = 0; i < n; i++) f(i); return; }
+    std::function<void(int)> fn = f;
+    pool().run(n, chunk, fn);
+}
+
+/* f(begin, end) over [0, n) in contiguous pieces of at least `grain` rows. */
+template <typename F>
+void parallel_rows(int64_t n, F f, int64_t grain = 128)
+{
+    if (g_nthreads_cpu <= 1 || n <= grain) { if (n > 0) f((int64_t)0, n); return; }
+    int64_t pieces = std::min<int64_t>((n + grain - 1) / grain, 64 * (int64_t)g_nthreads_cpu);
+    int64_t step = (n + pieces - 1) / pieces;
+    parallel_for((int)pieces, [&](int i) {
+        int64_t b = i * step, e = std::min(n, b + step);
+        if (b < e) f(b, e);
+    }, 1);
+}
+
+/* Copy stream tid's crawl state from one runtime_state to another. */
+void copy_state(KState &d, const KState &s, int tid)
+{
+    d.cont[tid] = s.cont[tid]; d.ilb[tid] = s.ilb[tid]; d.im[tid] = s.im[tid]; d.iM[tid] = s.iM[tid];
+    d.k[tid] = s.k[tid]; d.bc[tid] = s.bc[tid]; d.ndraw[tid] = s.ndraw[tid]; d.pos[tid] = s.pos[tid];
+    d.D[tid] = s.D[tid]; d.Am[tid] = s.Am[tid]; d.ms[tid] = s.ms[tid]; d.pix[tid] = s.pix[tid];
+}
+
+/* One draw batch with the emulated threads run on several host threads, with
+ * the result of running them one after another (skygen.cu.h:119-151; batch
+ * rules skyconfig_impl.h:445-534).  First every stream runs alone from its
+ * state, on a private counter and with the whole capacity as its room.  The
+ * streams' counts, summed in stream order, give each stream's first output
+ * index in the sequential run (its atomicAdd base).  Streams whose stars all fit
+ * keep that run.  The stream whose stars cross the capacity and every later one
+ * run again from their saved state with the room the sequential run leaves them:
+ * what remains of the capacity for the crossing stream, none for the later ones
+ * (they stop at their first bin with stars).  *nstars receives the sequential
+ * run's final counter, or any value >= stopstars when a stream crossed. */
+void draw_parallel(const Sky *s, const Model &m, KState &ks, RngState rs, gf_table *t, int stopstars, int64_t *nstars)
+{
+    const int N = m.nthreads;
+    KState snap = ks;
+    std::vector<Rng> rng0(N);
+    for (int tid = 0; tid < N; tid++) rng0[tid] = rs.load(tid);
+    std::vector<std::vector<StarRow>> rows(N);
+    std::vector<int64_t> cnt(N, 0);
+    auto run = [&](int tid, int room) {
+        int c = 0;
+        Launch L = {};
+        L.sky = s; L.m = &m; L.npixels = m.npixels; L.pixels = s->pixels.data();
+        L.stopstars = room; L.nstars = &c; L.rows = &rows[tid]; L.ks = &ks; L.rng = rs;
+        rows[tid].clear();
+        kernel(L, 1, tid);
+        cnt[tid] = c;
+    };
+    parallel_for(N, [&](int tid) { run(tid, stopstars); }, 64);
+    std::vector<int64_t> base(N, 0);
+    int64_t G = 0;
+    int T = -1;
+    for (int tid = 0; tid < N; tid++) {
+        base[tid] = G;
+        if (G + cnt[tid] > stopstars) { T = tid; break; }
+        G += cnt[tid];
+    }
+    int placed = N;
+    if (T >= 0) {
+        for (int tid = T; tid < N; tid++) { copy_state(ks, snap, tid); rs.store(tid, rng0[tid]); }
+        parallel_for(N - T, [&](int i) {
+            const int tid = T + i;
+            run(tid, tid == T ? (int)(stopstars - base[T]) : 0);
+        }, 64);
+        placed = T + 1;
+    }
+    Launch P = {};
+    P.out = t;
+    parallel_for(placed, [&](int tid) {
+        for (size_t k = 0; k < rows[tid].size(); k++) put_row(P, (int)(base[tid] + (int64_t)k), rows[tid][k]);
+    }, 16);
+    *nstars = T >= 0 ? (int64_t)stopstars + 1 : G;
 }
 
 /* star_comp (skyconfig_impl.h:34-68) */
@@ -670,6 +870,29 @@ struct StarComp {
         return t->Am[a] < t->Am[b];
     }
 };
+
+/* The order of star_comp over row indices: std::sort on one thread; on several,
+ * sorted pieces merged pairwise.  star_comp orders rows by (hidden, l, b, DM, M,
+ * Am); rows equal in all six never occur in practice, so both give one order. */
+void sort_rows(std::vector<size_t> &idx, const StarComp &sc)
+{
+    const size_t n = idx.size();
+    if (g_nthreads_cpu <= 1 || n < 65536) { std::sort(idx.begin(), idx.end(), sc); return; }
+    int pieces = 1;
+    while (pieces < 2 * g_nthreads_cpu && pieces < 64) pieces *= 2;
+    std::vector<size_t> bnd(pieces + 1);
+    for (int i = 0; i <= pieces; i++) bnd[i] = n * i / pieces;
+    parallel_for(pieces, [&](int i) { std::sort(idx.begin() + bnd[i], idx.begin() + bnd[i + 1], sc); }, 1);
+    std::vector<size_t> tmp(n);
+    for (int w = 1; w < pieces; w *= 2) {
+        const int pairs = pieces / (2 * w);
+        parallel_for(pairs, [&](int p) {
+            size_t a = bnd[2 * w * p], b = bnd[2 * w * p + w], e = bnd[2 * w * (p + 1)];
+            std::merge(idx.begin() + a, idx.begin() + b, idx.begin() + b, idx.begin() + e, tmp.begin() + a, sc);
+        }, 1);
+        idx.swap(tmp);
+    }
+}
 
 template <typename T>
 void permute(T *col, const std::vector<size_t> &s, int64_t n)
@@ -814,11 +1037,42 @@ int or_math_portable(void)
 }
 
 /* Seeding of the persistent streams (cux.cpp:404-414, cuda_rng.h:466-497) with
- * glibc's srand48/drand48/lrand48.  `primes` holds the stream multipliers.
+ * glibc's srand48/drand48/lrand48 (on several host threads: the same recurrence
+ * with jump-ahead).  `primes` holds the stream multipliers.
  * (int)(drand48()*prime) uses the x86 conversion: out-of-range values become INT_MIN. */
 int or_rng_seed(uint32_t seed, int32_t nstreams, const uint32_t *primes, uint32_t *state)
 {
     if (nstreams % 64) nstreams += 64 - nstreams % 64;
+    if (g_nthreads_cpu > 1) {
+        /* the same draws from the drand48 recurrence x' = (0x5DEECE66D x + 11) mod 2^48
+         * (POSIX), with each block of streams jumping ahead to its first draw */
+        const uint64_t A = 0x5DEECE66DULL, Cc = 0xB, M48 = (1ULL << 48) - 1;
+        const uint64_t x0 = (((uint64_t)seed << 16) | 0x330E) & M48;
+        const int per = 256;
+        parallel_for((nstreams + per - 1) / per, [&](int blk) {
+            /* x after 2 * blk * per steps: x_n = A^n x0 + C (A^n - 1) / (A - 1), by squaring */
+            uint64_t n = 2ULL * blk * per, ma = 1, mc = 0, pa = A, pc = Cc;
+            while (n) {
+                if (n & 1) { ma = (ma * pa) & M48; mc = (mc * pa + pc) & M48; }
+                pc = (pc * (pa + 1)) & M48;
+                pa = (pa * pa) & M48;
+                n >>= 1;
+            }
+            uint64_t x = (ma * x0 + mc) & M48;
+            const int i1 = std::min(nstreams, (blk + 1) * per);
+            for (int i = blk * per; i < i1; i++) {
+                uint32_t prime = primes[i];
+                state[i] = prime;
+                x = (A * x + Cc) & M48;
+                double t = ldexp((double)x, -48) * prime;
+                int32_t cv = (t >= 2147483648.0) ? INT32_MIN : (int32_t)t;
+                state[nstreams + i] = (uint32_t)cv;
+                x = (A * x + Cc) & M48;
+                state[2 * nstreams + i] = (uint32_t)(x >> 17);
+            }
+        }, 1);
+        return nstreams;
+    }
     srand48(seed);
     for (int i = 0; i != nstreams; i++) {
         uint32_t prime = primes[i];
@@ -964,7 +1218,7 @@ int or_skygen_integrate(void *h, int32_t mi, double *expected, double *expected_
         L.countsCoveredPerBeam = ccpb.data(); L.maxCount = maxCount.data();
         std::fill(counts.begin(), counts.end(), 0.);
         std::fill(countsCovered.begin(), countsCovered.end(), 0.);
-        parallel_for(N, [&](int tid) { kernel(L, 0, tid); });
+        parallel_for(N, [&](int tid) { kernel(L, 0, tid); }, 64);
         for (int i = 0; i != N; i++) { nE += counts[i]; nEC += countsCovered[i]; }
         if (per_pixel) {
             for (int px = 0; px < npix; px++) {
@@ -979,6 +1233,36 @@ int or_skygen_integrate(void *h, int32_t mi, double *expected, double *expected_
     m.nstarsExpected = nEC;
     if (expected) *expected = nE;
     if (expected_covered) *expected_covered = nEC;
+    return 0;
+}
+
+/* Diagnostics for the tests: the number of bins of one model whose expected
+ * count exceeds `above` (e.g. 10, where rng::poisson switches to the gamma /
+ * binomial reduction, cuda_rng.h:344-376), by the integrate crawl of
+ * or_skygen_integrate. */
+int or_count_bins_above(void *h, int32_t mi, float above, int64_t *count)
+{
+    Sky *s = (Sky *)h;
+    Model &m = s->models[mi];
+    const int N = m.nthreads;
+    const int lastpix = m.npixels;
+    const int PIXBLOCK = 1024 * 1024 * 2 / N;
+    std::vector<double> counts(N), countsCovered(N);
+    std::vector<float> maxCount(N);
+    std::vector<int64_t> nab(N, 0);
+    for (int startpix = 0; startpix < lastpix; startpix += PIXBLOCK) {
+        int npix = std::min(startpix + PIXBLOCK, lastpix) - startpix;
+        std::vector<float> ccpb((size_t)N * npix, 0.f);
+        Launch L = {};
+        L.sky = s; L.m = &m; L.npixels = npix; L.pixels = s->pixels.data() + startpix;
+        L.counts = counts.data(); L.countsCovered = countsCovered.data();
+        L.countsCoveredPerBeam = ccpb.data(); L.maxCount = maxCount.data();
+        L.nabove = nab.data(); L.above = above;
+        parallel_for(N, [&](int tid) { kernel(L, 0, tid); }, 64);
+    }
+    int64_t t = 0;
+    for (int i = 0; i < N; i++) t += nab[i];
+    *count = t;
     return 0;
 }
 
@@ -1062,34 +1346,53 @@ int or_skygen_draw(void *h, int32_t mi, uint32_t *rng_state, int32_t nstreams, g
     Sky *s = (Sky *)h;
     Model &m = s->models[mi];
     if (!s->ks_alloc[mi]) { s->ks[mi].alloc(m.nthreads); s->ks_alloc[mi] = 1; }
-    int nstars = 0;
-    Launch L = {};
-    L.sky = s; L.m = &m; L.npixels = m.npixels; L.pixels = s->pixels.data();
-    L.stopstars = (int)t->capacity;
-    L.nstars = &nstars;
-    L.out = t;
-    L.ks = &s->ks[mi];
-    L.rng.g = rng_state; L.rng.nstreams = nstreams;
-    for (int tid = 0; tid < m.nthreads; tid++) kernel(L, 1, tid);
-    int stars_generated = std::min(nstars, L.stopstars);
-    int generated_all = stars_generated < L.stopstars;
+    const int stopstars = (int)t->capacity;
+    RngState rs = {rng_state, nstreams};
+    int64_t nstars = 0;
+    if (g_nthreads_cpu <= 1) {
+        /* the reference CPU build: emulated threads one after another */
+        int n = 0;
+        Launch L = {};
+        L.sky = s; L.m = &m; L.npixels = m.npixels; L.pixels = s->pixels.data();
+        L.stopstars = stopstars;
+        L.nstars = &n;
+        L.out = t;
+        L.ks = &s->ks[mi];
+        L.rng = rs;
+        for (int tid = 0; tid < m.nthreads; tid++) kernel(L, 1, tid);
+        nstars = n;
+    } else {
+        draw_parallel(s, m, s->ks[mi], rs, t, stopstars, &nstars);
+    }
+    int stars_generated = (int)std::min<int64_t>(nstars, stopstars);
+    int generated_all = stars_generated < stopstars;
 
     /* sort by (hidden, l, b, DM, M, Am) and truncate at the first hidden row */
     std::vector<size_t> idx(stars_generated);
     for (int i = 0; i < stars_generated; i++) idx[i] = i;
     t->size = stars_generated;
     StarComp sc = {t};
-    std::sort(idx.begin(), idx.end(), sc);
+    sort_rows(idx, sc);
     const int64_t P = t->capacity;
-    permute(t->lb, idx, stars_generated); permute(t->lb + P, idx, stars_generated);
-    permute(t->projIdx, idx, stars_generated);
-    permute(t->projXY, idx, stars_generated); permute(t->projXY + P, idx, stars_generated);
-    permute(t->Am, idx, stars_generated); permute(t->AmInf, idx, stars_generated);
-    permute(t->XYZ, idx, stars_generated); permute(t->XYZ + P, idx, stars_generated); permute(t->XYZ + 2 * P, idx, stars_generated);
-    permute(t->comp, idx, stars_generated);
-    permute(t->absmag, idx, stars_generated);
-    permute(t->DM, idx, stars_generated);
-    permute(t->hidden, idx, stars_generated);
+    const int n = stars_generated;
+    parallel_for(14, [&](int c) {
+        switch (c) {
+        case 0: permute(t->lb, idx, n); break;
+        case 1: permute(t->lb + P, idx, n); break;
+        case 2: permute(t->projIdx, idx, n); break;
+        case 3: permute(t->projXY, idx, n); break;
+        case 4: permute(t->projXY + P, idx, n); break;
+        case 5: permute(t->Am, idx, n); break;
+        case 6: permute(t->AmInf, idx, n); break;
+        case 7: permute(t->XYZ, idx, n); break;
+        case 8: permute(t->XYZ + P, idx, n); break;
+        case 9: permute(t->XYZ + 2 * P, idx, n); break;
+        case 10: permute(t->comp, idx, n); break;
+        case 11: permute(t->absmag, idx, n); break;
+        case 12: permute(t->DM, idx, n); break;
+        case 13: permute(t->hidden, idx, n); break;
+        }
+    }, 1);
     int32_t *h0 = std::upper_bound(t->hidden, t->hidden + stars_generated, 0);
     t->size = h0 - t->hidden;
     *n_generated = stars_generated;
@@ -1107,34 +1410,38 @@ int or_module_clipper(const gf_footprint *foot, const gf_lambert *proj, gf_table
 {
     (void)proj;
     const int64_t P = t->capacity;
-    for (int64_t row = begin; row < end; row++) {
-        if (t->hidden[row]) continue;
-        bool in = true;
-        if (foot->kind == GF_FOOT_LAMBERT_RECT) {
-            float x = t->projXY[row], y = t->projXY[P + row];
-            in = t->projIdx[row] == foot->proj && x >= foot->a && x < foot->b && y >= foot->c && y < foot->d;
-        } else if (foot->kind == GF_FOOT_CAP) {
-            double l = t->lb[row] * dbl_d2r, b = t->lb[P + row] * dbl_d2r;
-            double l0 = foot->a * dbl_d2r, b0 = foot->b * dbl_d2r;
-            double cosd = OR_SIN(b) * OR_SIN(b0) + OR_COS(b) * OR_COS(b0) * OR_COS(l - l0);
-            in = cosd >= OR_COS(foot->c * dbl_d2r);
-        } else if (foot->kind == GF_FOOT_LATCUT) {
-            in = fabs(t->lb[P + row]) > foot->a;
+    parallel_rows(end - begin, [&](int64_t rb_, int64_t re_) {
+        for (int64_t row = begin + rb_; row < begin + re_; row++) {
+            if (t->hidden[row]) continue;
+            bool in = true;
+            if (foot->kind == GF_FOOT_LAMBERT_RECT) {
+                float x = t->projXY[row], y = t->projXY[P + row];
+                in = t->projIdx[row] == foot->proj && x >= foot->a && x < foot->b && y >= foot->c && y < foot->d;
+            } else if (foot->kind == GF_FOOT_CAP) {
+                double l = t->lb[row] * dbl_d2r, b = t->lb[P + row] * dbl_d2r;
+                double l0 = foot->a * dbl_d2r, b0 = foot->b * dbl_d2r;
+                double cosd = OR_SIN(b) * OR_SIN(b0) + OR_COS(b) * OR_COS(b0) * OR_COS(l - l0);
+                in = cosd >= OR_COS(foot->c * dbl_d2r);
+            } else if (foot->kind == GF_FOOT_LATCUT) {
+                in = fabs(t->lb[P + row]) > foot->a;
+            }
+            if (!in) t->hidden[row] = 1;
         }
-        if (!in) t->hidden[row] = 1;
-    }
+    });
     return 0;
 }
 
 /* os_fixedFeH_kernel (fixedFeH_gpu.cu.h:34-50) */
 int or_module_fixedfeh(const gf_fixedfeh_config *c, gf_table *t, int64_t begin, int64_t end)
 {
-    for (int64_t row = begin; row < end; row++) {
-        if (t->hidden[row]) continue;
-        int cmp = t->comp[row];
-        if (!((c->comp_mask >> cmp) & 1u)) continue;
-        t->FeH[row] = c->FeH;
-    }
+    parallel_rows(end - begin, [&](int64_t rb_, int64_t re_) {
+        for (int64_t row = begin + rb_; row < begin + re_; row++) {
+            if (t->hidden[row]) continue;
+            int cmp = t->comp[row];
+            if (!((c->comp_mask >> cmp) & 1u)) continue;
+            t->FeH[row] = c->FeH;
+        }
+    });
     return 0;
 }
 
@@ -1183,7 +1490,7 @@ int or_module_bond2010(const gf_bond2010_config *par, uint32_t *rng_state, int32
     int64_t n = end - begin;
     int64_t nth = n / 256 + (n % 256 ? 1 : 0);
     if (nth > nstreams) { g_err = "Bond2010: more than 256*nstreams rows"; return -1; }
-    for (int64_t th = 0; th < nth; th++) {
+    parallel_for((int)nth, [&](int th) {
         Rng rng = rs.load((int)th);
         int64_t rb = begin + 256 * th, re = std::min(begin + 256 * (th + 1), end);
         for (int64_t row = rb; row < re; row++) {
@@ -1221,7 +1528,7 @@ int or_module_bond2010(const gf_bond2010_config *par, uint32_t *rng_state, int32
             t->vcyl[2 * P + row] = tmp[2];
         }
         rs.store((int)th, rng);
-    }
+    }, 16);
     return 0;
 }
 
@@ -1231,53 +1538,55 @@ int or_module_photometry(const gf_photometry_config *lt, gf_table *t, int64_t be
     const int64_t P = t->capacity;
     const int ncolors = lt->nbands - 1;
     Phot ph = {lt};
-    float c[GF_MAX_BANDS];
-    for (int64_t row = begin; row < end; row++) {
-        if (t->hidden[row]) continue;
-        int cmp = t->comp[row];
-        if (!((lt->comp_mask >> cmp) & 1u)) continue;
-        float fFeH = t->FeH[row];
-        uint32_t flag = 0;
-        float fMr = t->absmag[row];
-        if (!(fMr >= 99.999f)) {
-            for (int ic = 0; ic < ncolors; ic++) {
-                bool fl;
-                c[ic] = ph.tex(ic, fFeH, fMr, fl);
-                flag |= ((uint32_t)fl) << ic;
+    parallel_rows(end - begin, [&](int64_t rb_, int64_t re_) {
+        for (int64_t row = begin + rb_; row < begin + re_; row++) {
+            float c[GF_MAX_BANDS];
+            if (t->hidden[row]) continue;
+            int cmp = t->comp[row];
+            if (!((lt->comp_mask >> cmp) & 1u)) continue;
+            float fFeH = t->FeH[row];
+            uint32_t flag = 0;
+            float fMr = t->absmag[row];
+            if (!(fMr >= 99.999f)) {
+                for (int ic = 0; ic < ncolors; ic++) {
+                    bool fl;
+                    c[ic] = ph.tex(ic, fFeH, fMr, fl);
+                    flag |= ((uint32_t)fl) << ic;
+                }
+                for (int b = 0; b <= ncolors; b++) {
+                    float M = fMr;
+                    if (b < lt->bidx) { for (int i = b; i != lt->bidx; i++) M += c[i]; }
+                    if (b > lt->bidx) { for (int i = lt->bidx; i != b; i++) M -= c[i]; }
+                    float L = OR_EXP10F(-0.4f * M);
+                    t->mags[b * P + row] = L;
+                }
             }
+            bool fl = false;
+            for (int i = lt->bidx - 1; i >= 0; i--) {
+                uint32_t mask = 1u << i;
+                fl = fl || (flag & mask);
+                flag |= ((uint32_t)fl) << i;
+            }
+            fl = false;
+            for (int i = lt->bidx; i < ncolors; i++) {
+                uint32_t mask = 1u << i;
+                fl = fl || (flag & mask);
+                flag |= ((uint32_t)fl) << i << 1;
+            }
+            flag &= ~(1u << lt->bidx);
+            flag = brev32(flag);
+            flag >>= (8 * sizeof(flag) - ncolors - 1);
+            t->photoflags[row] = (int32_t)flag;
+            float dm = t->DM[row];
+            float Am0 = t->Am[row];
             for (int b = 0; b <= ncolors; b++) {
-                float M = fMr;
-                if (b < lt->bidx) { for (int i = b; i != lt->bidx; i++) M += c[i]; }
-                if (b > lt->bidx) { for (int i = lt->bidx; i != b; i++) M -= c[i]; }
-                float L = OR_EXP10F(-0.4f * M);
-                t->mags[b * P + row] = L;
+                float Msys = -2.5f * OR_LOG10F(t->mags[b * P + row]);
+                float msys = dm + Msys;
+                float Am = Am0 * lt->reddening[b];
+                t->mags[b * P + row] = msys + Am;
             }
         }
-        bool fl = false;
-        for (int i = lt->bidx - 1; i >= 0; i--) {
-            uint32_t mask = 1u << i;
-            fl = fl || (flag & mask);
-            flag |= ((uint32_t)fl) << i;
-        }
-        fl = false;
-        for (int i = lt->bidx; i < ncolors; i++) {
-            uint32_t mask = 1u << i;
-            fl = fl || (flag & mask);
-            flag |= ((uint32_t)fl) << i << 1;
-        }
-        flag &= ~(1u << lt->bidx);
-        flag = brev32(flag);
-        flag >>= (8 * sizeof(flag) - ncolors - 1);
-        t->photoflags[row] = (int32_t)flag;
-        float dm = t->DM[row];
-        float Am0 = t->Am[row];
-        for (int b = 0; b <= ncolors; b++) {
-            float Msys = -2.5f * OR_LOG10F(t->mags[b * P + row]);
-            float msys = dm + Msys;
-            float Am = Am0 * lt->reddening[b];
-            t->mags[b * P + row] = msys + Am;
-        }
-    }
+    });
     return 0;
 }
 
@@ -1286,16 +1595,18 @@ int or_module_photometry(const gf_photometry_config *lt, gf_table *t, int64_t be
 int or_module_photoerrors(const gf_photoerr_config *c, int64_t row_offset, gf_table *t, int64_t begin, int64_t end)
 {
     const int64_t P = t->capacity;
-    for (int b = 0; b < c->nbands; b++) {
-        const double *mk = c->mag + (size_t)b * c->nknots, *sk = c->sigma + (size_t)b * c->nknots;
-        for (int64_t row = begin; row < end; row++) {
-            if (t->hidden[row]) continue;
-            float mag = t->mags[b * P + row];
-            float sigma = (float)linear_eval(mk, sk, c->nknots, mag);
-            double z = error_normal(c->seed, (uint64_t)(row_offset + row), (uint32_t)b);
-            t->obsmags[b * P + row] = mag + (float)(sigma * z);
+    parallel_rows(end - begin, [&](int64_t rb_, int64_t re_) {
+        for (int b = 0; b < c->nbands; b++) {
+            const double *mk = c->mag + (size_t)b * c->nknots, *sk = c->sigma + (size_t)b * c->nknots;
+            for (int64_t row = begin + rb_; row < begin + re_; row++) {
+                if (t->hidden[row]) continue;
+                float mag = t->mags[b * P + row];
+                float sigma = (float)linear_eval(mk, sk, c->nknots, mag);
+                double z = error_normal(c->seed, (uint64_t)(row_offset + row), (uint32_t)b);
+                t->obsmags[b * P + row] = mag + (float)(sigma * z);
+            }
         }
-    }
+    });
     return 0;
 }
 
@@ -1303,32 +1614,34 @@ int or_module_photoerrors(const gf_photoerr_config *c, int64_t row_offset, gf_ta
 int or_module_vel2pm(const gf_vel2pm_config *par, gf_table *t, int64_t begin, int64_t end)
 {
     const int64_t P = t->capacity;
-    for (int64_t row = begin; row < end; row++) {
-        if (t->hidden[row]) continue;
-        float l = 0.017453292519943295769f * (float)t->lb[row];
-        float b = 0.017453292519943295769f * (float)t->lb[P + row];
-        float X = par->Rg - t->XYZ[row];
-        float Y = -t->XYZ[P + row];
-        float Z = t->XYZ[2 * P + row];
-        float vx = t->vcyl[row], vy = t->vcyl[P + row], vz = t->vcyl[2 * P + row];
-        float px, py, pz;
-        vel_cyl2xyz(px, py, pz, vx, vy, vz, X, Y);
-        px -= par->u0;
-        py -= par->v0 + par->vLSR;
-        pz -= par->w0;
-        vel_xyz2lbr(px, py, pz, -px, -py, pz, l, b);
-        float D = sqrtf((8000.f - X) * (8000.f - X) + Y * Y + Z * Z);
-        px = (float)(px / (4.74 * D * 1e-3));
-        py = (float)(py / (4.74 * D * 1e-3));
-        if (par->coordsys == 1) {
-            transform_pm(px, py, l, b, px, py, GE_ce, GE_se, GE_l0);
-        } else if (par->coordsys != 0) {
-            px = py = pz = -9.99f;
+    parallel_rows(end - begin, [&](int64_t rb_, int64_t re_) {
+        for (int64_t row = begin + rb_; row < begin + re_; row++) {
+            if (t->hidden[row]) continue;
+            float l = 0.017453292519943295769f * (float)t->lb[row];
+            float b = 0.017453292519943295769f * (float)t->lb[P + row];
+            float X = par->Rg - t->XYZ[row];
+            float Y = -t->XYZ[P + row];
+            float Z = t->XYZ[2 * P + row];
+            float vx = t->vcyl[row], vy = t->vcyl[P + row], vz = t->vcyl[2 * P + row];
+            float px, py, pz;
+            vel_cyl2xyz(px, py, pz, vx, vy, vz, X, Y);
+            px -= par->u0;
+            py -= par->v0 + par->vLSR;
+            pz -= par->w0;
+            vel_xyz2lbr(px, py, pz, -px, -py, pz, l, b);
+            float D = sqrtf((8000.f - X) * (8000.f - X) + Y * Y + Z * Z);
+            px = (float)(px / (4.74 * D * 1e-3));
+            py = (float)(py / (4.74 * D * 1e-3));
+            if (par->coordsys == 1) {
+                transform_pm(px, py, l, b, px, py, GE_ce, GE_se, GE_l0);
+            } else if (par->coordsys != 0) {
+                px = py = pz = -9.99f;
+            }
+            t->pm[row] = px;
+            t->pm[P + row] = py;
+            t->pm[2 * P + row] = pz;
         }
-        t->pm[row] = px;
-        t->pm[P + row] = py;
-        t->pm[2 * P + row] = pz;
-    }
+    });
     return 0;
 }
 
@@ -1337,25 +1650,27 @@ int or_module_gal2other(int32_t coordsys, gf_table *t, int64_t begin, int64_t en
 {
     const int64_t P = t->capacity;
     const double pi2 = 2 * dbl_pi;
-    for (int64_t row = begin; row < end; row++) {
-        if (t->hidden[row]) continue;
-        double lx = t->lb[row] * dbl_d2r, ly = t->lb[P + row] * dbl_d2r;
-        double rx, ry;
-        if (coordsys == 1) {
-            const double cb = OR_COS(ly);
-            const double sb = OR_SIN(ly);
-            const double cl = OR_COS(lx - GE_l0);
-            const double sl = OR_SIN(lx - GE_l0);
-            rx = OR_ATAN2(cb * cl, sb * GE_ce - cb * GE_se * sl) + GE_angp;
-            ry = OR_ASIN(cb * GE_ce * sl + sb * GE_se);
-            while (rx < 0.) rx += pi2;
-            while (rx >= pi2) rx -= pi2;
-        } else {
-            rx = ry = -9999.;
+    parallel_rows(end - begin, [&](int64_t rb_, int64_t re_) {
+        for (int64_t row = begin + rb_; row < begin + re_; row++) {
+            if (t->hidden[row]) continue;
+            double lx = t->lb[row] * dbl_d2r, ly = t->lb[P + row] * dbl_d2r;
+            double rx, ry;
+            if (coordsys == 1) {
+                const double cb = OR_COS(ly);
+                const double sb = OR_SIN(ly);
+                const double cl = OR_COS(lx - GE_l0);
+                const double sl = OR_SIN(lx - GE_l0);
+                rx = OR_ATAN2(cb * cl, sb * GE_ce - cb * GE_se * sl) + GE_angp;
+                ry = OR_ASIN(cb * GE_ce * sl + sb * GE_se);
+                while (rx < 0.) rx += pi2;
+                while (rx >= pi2) rx -= pi2;
+            } else {
+                rx = ry = -9999.;
+            }
+            t->radec[row] = rx / dbl_d2r;
+            t->radec[P + row] = ry / dbl_d2r;
         }
-        t->radec[row] = rx / dbl_d2r;
-        t->radec[P + row] = ry / dbl_d2r;
-    }
+    });
     return 0;
 }
 

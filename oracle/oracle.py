@@ -40,6 +40,7 @@ def load(flavour="p"):
         L.or_skygen_model_lf.argtypes = [vp, C.c_int32, vp]
         L.or_skygen_integrate.argtypes = [vp, C.c_int32, vp, vp, vp]
         L.or_expected_fp64.argtypes = [vp, C.c_int32, C.c_int32, vp, vp]
+        L.or_count_bins_above.argtypes = [vp, C.c_int32, C.c_float, vp]
         L.or_skygen_set_norm.argtypes = [vp, C.c_int32, C.c_float]
         L.or_skygen_draw.argtypes = [vp, C.c_int32, vp, C.c_int32, vp, vp, vp]
         L.or_module_clipper.argtypes = [vp, vp, vp, C.c_int64, C.c_int64]
@@ -111,7 +112,6 @@ class OracleSkygen:
         self.L.or_skygen_integrate(self.h, model, C.addressof(e), C.addressof(ec), pp.ctypes.data if pp is not None else None)
         return e.value, ec.value, pp
 
-
     def expected_fp64(self, model, pixel):
         """(reference float sum, FP64 sum) of the expected counts of one pixel."""
         a = C.c_double()
@@ -119,6 +119,13 @@ class OracleSkygen:
         if self.L.or_expected_fp64(self.h, model, pixel, C.addressof(a), C.addressof(b)) != 0:
             raise ValueError("pixel out of range or nm*nM not a multiple of 10")
         return a.value, b.value
+
+    def count_bins_above(self, model, above):
+        """Bins of `model` whose expected count exceeds `above` (diagnostics)."""
+        n = C.c_int64()
+        self.L.or_count_bins_above(self.h, model, above, C.addressof(n))
+        return n.value
+
     def set_density_norm(self, model, norm):
         self.L.or_skygen_set_norm(self.h, model, norm)
 
@@ -130,9 +137,11 @@ class OracleSkygen:
         return n.value, bool(d.value)
 
 
-def run_catalog(w, multipliers, flavour="p", sink=None, threads=1):
+def run_catalog(w, multipliers, flavour="p", sink=None, threads=1, table=None):
     """The reference catalog path on the CPU: integrate all models, then draw
-    every model's batches and run the module chain (os_skygen.cpp:866-932)."""
+    every model's batches and run the module chain (os_skygen.cpp:866-932).
+    table: a HostTable of w.capacity rows and w.nbands bands to reuse (the
+    otable of the reference is reused from batch to batch the same way)."""
     import galfast_b200 as G
     L = load(flavour)
     L.or_set_threads(threads)
@@ -149,7 +158,7 @@ def run_catalog(w, multipliers, flavour="p", sink=None, threads=1):
         norm = float(np.float32(w.sky.nstars / total))
         for i in range(len(w.models)):
             sky.set_density_norm(i, norm)
-    t = G.HostTable(w.capacity, w.nbands)
+    t = table if table is not None else G.HostTable(w.capacity, w.nbands)
     row_offset = 0
     stats = {"expected": expected, "generated": {}, "stored": {}, "batches": 0}
     NS = len(state) // 3

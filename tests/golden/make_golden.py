@@ -1,6 +1,6 @@
 """Regenerate the golden fixtures from the reference's own test data.
 
-    python tests/golden/make_golden.py /path/to/galfast
+    python tests/golden/make_golden.py /path/to/galfast      (or GALFAST_REFERENCE=/path/to/galfast)
 
 reads tests/os_vel2pm/result/sky.obs.txt of the reference (the output of its
 postprocessing test, tests/os_vel2pm/go.sh) and writes os_vel2pm_sky_obs.npz
@@ -24,4 +24,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GALFAST_REFERENCE")
+    if not src:
+        sys.exit("usage: make_golden.py <galfast source tree> (or set GALFAST_REFERENCE)")
+    main(src)

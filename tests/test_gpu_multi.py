@@ -167,3 +167,36 @@ def test_host_delivery_equals_device_rows(lib):
         for j in range(len(ws)):
             assert st[j].generated[:3] == st_ref[j].generated[:3]
     ctx.close()
+
+
+def test_request_that_fills_a_batch_runs_alone(lib):
+    """Admission lets every request into the batched passes (margin -1000 sigma);
+    the first request's halo stars (about 2850) then fill its 2000-row batch while
+    its thin and thick disks (about 1000 and 1600 stars) fit.  The call does not
+    fail: the request's halo rows are withheld and it runs alone afterwards,
+    delivering only the halo, so every request still gets exactly the catalog
+    gf_catalog_run gives it alone (two halo batches for the first)."""
+    ws = [W.build_workload(lib, foot=W.cap_footprint(60.0, 70.0, 1.0), dx_deg=0.1, m0=14.0, m1=21.5,
+                           capacity=2000, seed48=4242)]
+    ws += requests(lib, n=3)[::2]
+    ctx = G.Context(0)
+    ctx.set_admission(-1000.0)
+    got = {}
+
+    def sink(j, model, rows):
+        got.setdefault(j, {}).setdefault(model, []).append(rows)
+    stats = G.run_catalog_multi(ctx, ws, sink=sink)
+    for j, w in enumerate(ws):
+        ref, st = catalog_alone(ctx, w)
+        assert sorted(ref) == sorted(got[j]), j
+        for m in ref:
+            b = {k: np.concatenate([p[k] for p in got[j][m]], axis=-1) for k in got[j][m][0]}
+            for c in ref[m]:
+                x, y = ref[m][c], b[c]
+                if c in ("mags", "obsmags"):
+                    y = y[: x.shape[0]]
+                np.testing.assert_array_equal(x, y, err_msg="%s request %d model %d" % (c, j, m))
+        assert list(stats[j].generated[:3]) == list(st.generated[:3]), j
+    assert stats[0].generated[0] < 2000 <= stats[0].generated[2]
+    assert len(got[0][2]) >= 2 and len(got[0][0]) == 1
+    ctx.close()

@@ -1,0 +1,158 @@
+"""The batched engine (gf_catalog_run_multi: anchor plans, integrate_pixels_kernel,
+batch_draw_kernel, event expansion, joint sort and module chain) against the CPU
+oracle -- the reference CPU path restated -- on requests of the batched workload
+itself (4096 pencil beams, |b| > 5 deg, radii 0.5-5 deg, 14 < r < U(19, 24)),
+and the Poisson sampler's large-mean branch on the device.
+
+Every skygen column must be bit-exact against the oracle (the reference kernel
+skygen.cu.h:469-618 and its batch rules skyconfig_impl.h:435-545); the module
+columns agree within 1e-5 relative on the rows the modules process.
+"""
+import numpy as np
+import pytest
+
+import galfast_b200 as G
+from galfast_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SKY = ["lb", "projIdx", "projXY", "DM", "absmag", "XYZ", "comp", "Am", "AmInf", "hidden"]
+MODULE = ["FeH", "vcyl", "mags", "photoflags", "obsmags", "pm", "radec"]
+RTOL = 1e-5
+
+# Requests of the batched workload's own set (W.config4_requests(4096), the
+# benchmark's seeds): 34 has the largest cap (4.999 deg), 1361 the deepest r_max
+# (23.996), 3792 the lowest latitude (|b| = 5.007 deg); 1819, 3264 and 1915 are
+# the richest (5 deg caps at |b| < 14 deg with r_max > 23.7); the rest are the
+# first, last and a few ordinary requests.
+CONFIG4_PICK = [34, 1361, 3792, 1819, 3264, 1915, 0, 1, 2, 100, 2000, 4095]
+PIXELS_PER_REQUEST = 96
+
+
+def concat(parts):
+    return {k: np.concatenate([p[k] for p in parts], axis=-1) for k in parts[0]}
+
+
+def oracle_catalog(w, multipliers):
+    per_model = {}
+    st, state = O.run_catalog(w, multipliers, sink=lambda m, t, off: per_model.setdefault(m, []).append(t.as_dict()),
+                              threads=8)
+    return {m: concat(p) for m, p in per_model.items()}, st, state
+
+
+def compare(ref, got, tag):
+    assert sorted(ref) == sorted(got), tag
+    for m in ref:
+        a, b = ref[m], got[m]
+        assert a["DM"].shape == b["DM"].shape, (tag, m)
+        for c in SKY:
+            x, y = a[c], b[c]
+            same = (x == y) | (np.isnan(x) & np.isnan(y)) if x.dtype.kind == "f" else (x == y)
+            assert same.all(), "%s: %s model %d differs in %d of %d values" % (tag, c, m, (~same).sum(), same.size)
+        vis = a["hidden"] == 0
+        for c in MODULE:
+            if c not in a or a[c].size == 0:
+                continue
+            x, y = a[c], b[c]
+            if c in ("mags", "obsmags"):
+                y = y[: x.shape[0]]
+            if x.dtype.kind == "f":
+                np.testing.assert_allclose(y[..., vis], x[..., vis], rtol=RTOL, atol=1e-6,
+                                           err_msg="%s: %s model %d" % (tag, c, m))
+            else:
+                np.testing.assert_array_equal(y[..., vis], x[..., vis], err_msg="%s: %s model %d" % (tag, c, m))
+
+
+def batched_catalogs(ctx, ws):
+    got = {}
+    stats = G.run_catalog_multi(ctx, ws, sink=lambda j, m, rows: got.setdefault(j, {}).setdefault(m, []).append(rows))
+    return {j: {m: concat(p) for m, p in got[j].items()} for j in got}, stats
+
+
+def config4_sample(lib):
+    reqs = W.config4_requests(4096)
+    ws = []
+    for i in CONFIG4_PICK:
+        w = W.config4_workload(lib, reqs[i], capacity=1 << 24)
+        stride = max(1, w.npixels // PIXELS_PER_REQUEST)
+        ws.append(W.restrict_pixels(w, np.arange(stride // 2, w.npixels, stride)))
+    return ws
+
+
+def test_config4_requests_batched_equal_oracle(lib, multipliers):
+    """Twelve requests of the benchmark's set, each on a stride of its pixels,
+    generated together by the batched engine and one by one by the oracle."""
+    ws = config4_sample(lib)
+    ctx = G.Context(0)
+    got, stats = batched_catalogs(ctx, ws)
+    ctx.close()
+    total = 0
+    for j, w in enumerate(ws):
+        ref, st, _ = oracle_catalog(w, multipliers)
+        compare(ref, got.get(j, {}), "request %d" % CONFIG4_PICK[j])
+        for i in range(3):
+            assert stats[j].generated[i] == st["generated"][i], (CONFIG4_PICK[j], i)
+            assert stats[j].expected[i] == pytest.approx(st["expected"][i][0], rel=1e-12)
+        total += sum(st["stored"].values())
+    assert total > 5e5
+
+
+def large_mu_workload(lib, capacity=1 << 20):
+    """3-deg pixels near the plane: thousands of bins with 10 < mu < 200, where
+    rng::poisson reduces mu through gamma_int and binomial (cuda_rng.h:344-376)."""
+    return W.build_workload(lib, foot=W.cap_footprint(20.0, 8.0, 3.0), dx_deg=3.0, m0=14.0, m1=17.0,
+                            capacity=capacity)
+
+
+def test_poisson_large_mu_plain_and_batched_equal_oracle(lib, multipliers):
+    w = large_mu_workload(lib)
+    osk = O.OracleSkygen(w)
+    above10 = sum(osk.count_bins_above(m, 10.0) for m in range(3))
+    above100 = sum(osk.count_bins_above(m, 100.0) for m in range(3))
+    osk.close()
+    assert above10 >= 100 and above100 >= 10, (above10, above100)
+    ref, st, ostate = oracle_catalog(w, multipliers)
+
+    ctx = G.Context(0)
+    # plain path: the crawl kernels, one output batch per model
+    plain = {}
+    gst = G.run_catalog(ctx, w, sink=lambda m, t, off: plain.setdefault(m, []).append(t.as_dict()))
+    compare(ref, {m: concat(p) for m, p in plain.items()}, "plain")
+    for i in range(3):
+        assert gst.generated[i] == st["generated"][i]
+    # the streams after the whole catalog (skygen and Bond2010 consume them)
+    gstate = ctx.rng_state()
+    assert np.array_equal(gstate, ostate), "stream states differ after the catalog"
+
+    # batched path: the request twice in one call, with another seed's copy between them
+    w2 = large_mu_workload(lib)
+    w2.seed48 = w.seed48 + 1
+    ref2, st2, _ = oracle_catalog(w2, multipliers)
+    got, stats = batched_catalogs(ctx, [w, w2, w])
+    ctx.close()
+    compare(ref, got[0], "batched 0")
+    compare(ref2, got[1], "batched 1")
+    compare(ref, got[2], "batched 2")
+    for i in range(3):
+        assert stats[0].generated[i] == st["generated"][i]
+        assert stats[1].generated[i] == st2["generated"][i]
+
+
+def test_poisson_sampler_on_device_equals_oracle(ctx):
+    """rng::poisson for means from 1e-3 to 3e3 drawn one after another from one
+    stream (gf_rng_poisson): the gamma_int / gamma_large / binomial reduction above
+    mu = 10 included, draw for draw and with the same final stream state."""
+    mu = np.exp(np.linspace(np.log(1e-3), np.log(3e3), 6000)).astype(np.float32)
+    ctx.rng_init(7, 64)
+    a, c, x = (int(v[0]) for v in ctx.rng_state().reshape(3, -1))
+    lo = O.load("p")
+    out_o = np.zeros(mu.size, dtype=np.uint32)
+    oa, oc, ox = (np.array([v], dtype=np.uint32) for v in (a, c, x))
+    lo.or_mwc_poisson(oa.ctypes.data, oc.ctypes.data, ox.ctypes.data, mu.ctypes.data, mu.size, out_o.ctypes.data)
+    assert out_o.max() > 2000 and (mu > 10).sum() > 2000
+    st = np.array([a, c, x], dtype=np.uint32)
+    out_g = np.zeros(mu.size, dtype=np.uint32)
+    G.check(G.lib().gf_rng_poisson(ctx.h, st.ctypes.data, mu.ctypes.data, mu.size, out_g.ctypes.data))
+    np.testing.assert_array_equal(out_g, out_o)
+    assert (st[1], st[2]) == (oc[0], ox[0])

@@ -162,6 +162,57 @@ def test_catalog_parity(ctx, lib, multipliers, capacity):
         assert gs.generated[m] == os_["generated"][m]
 
 
+def test_catalog_parity_lsst_ugrizy(ctx, lib, multipliers):
+    """The six-band LSST-like system (five colours: two colour textures in the
+    reference, photometry_host.cpp:233-344) with depths one magnitude deeper."""
+    w = small_patch(lib, capacity=1 << 18, nbands=6, m5=W.LSST_M5)
+    gs, os_, gb, ob = run_both(ctx, w, multipliers)
+    assert len(gb) == len(ob) > 0
+    for (gm, go, g), (om, oo, o) in zip(gb, ob):
+        assert (gm, go) == (om, oo)
+        assert g["mags"].shape[0] == 6 and g["obsmags"].shape[0] == 6
+        assert_same(g, o, SKY_COLS)
+        assert_same(g, o, MODULE_COLS, exact=False)
+
+
+@pytest.mark.parametrize("nbands,m5", [(5, W.SDSS_M5), (6, W.LSST_M5)])
+def test_photometric_error_statistics(ctx, lib, nbands, m5):
+    """os_photometricErrors draws obs = true + sigma(true) * N(0, 1) with
+    sigma(m) = 0.005 + 0.04 * 10^(0.4 (m - m5)) (photometricErrors_host.cpp:112-131,
+    the configurations' error model).  Over more than 1e6 rows per band: the
+    normalised deviations have mean 0 (within 5 / sqrt(n)) and standard deviation 1
+    (within 1 %), and in every 0.5-mag bin of true magnitude the spread of
+    obs - true equals the formula's sigma within 3 %."""
+    w = W.build_workload(lib, foot=W.cap_footprint(60.0, 40.0, 7.0), dx_deg=0.1, m0=14.0, m1=22.0,
+                         capacity=1 << 22, nbands=nbands, m5=m5)
+    true, obs = [], []
+
+    def sink(model, t, off):
+        d = t.as_dict(["mags", "obsmags", "hidden"])
+        vis = d["hidden"] == 0
+        true.append(d["mags"][:, vis].astype(np.float64))
+        obs.append(d["obsmags"][:, vis].astype(np.float64))
+    G.run_catalog(ctx, w, sink)
+    true = np.concatenate(true, axis=1)
+    obs = np.concatenate(obs, axis=1)
+    n = true.shape[1]
+    assert n > 1e6
+    for b in range(nbands):
+        m = true[b]
+        sig = 0.005 + 0.04 * 10.0 ** (0.4 * (m - m5[b]))
+        z = (obs[b] - m) / sig
+        assert abs(z.mean()) < 5.0 / np.sqrt(n), (b, z.mean())
+        assert abs(z.std() - 1.0) < 0.01, (b, z.std())
+        edges = np.arange(np.floor(m.min()), np.ceil(m.max()) + 0.5, 0.5)
+        which = np.digitize(m, edges)
+        for k in np.unique(which):
+            sel = which == k
+            if sel.sum() < 20000:
+                continue
+            ratio = (obs[b][sel] - m[sel]).std() / np.sqrt(np.mean(sig[sel] ** 2))
+            assert abs(ratio - 1.0) < 0.03, (b, edges[k - 1], ratio)
+
+
 def test_config1_catalog(ctx, lib, multipliers):
     """Configuration 1 in full (about 1e5 stars)."""
     w = W.config1(lib)

@@ -74,9 +74,13 @@ def test_safeprime_multipliers_are_safe(multipliers):
     assert np.all(np.diff(multipliers[54735:].astype(np.int64)) < 0) and multipliers[54735] > 2 ** 31
 
 
-@pytest.mark.skipif(not os.path.exists("/root/reference/data/safeprimes32.txt"), reason="reference tree not present")
+REFERENCE = os.environ.get("GALFAST_REFERENCE", "")
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REFERENCE, "data", "safeprimes32.txt")),
+                    reason="set GALFAST_REFERENCE to a galfast source tree")
 def test_safeprime_multipliers_equal_reference_table(multipliers):
-    ref = np.loadtxt("/root/reference/data/safeprimes32.txt", dtype=np.uint64, max_rows=65536)
+    ref = np.loadtxt(os.path.join(REFERENCE, "data", "safeprimes32.txt"), dtype=np.uint64, max_rows=65536)
     assert np.array_equal(ref[:, 0].astype(np.uint32), multipliers)
     assert np.array_equal(ref[:, 1], ref[:, 0] * 2 ** 32 - 1)
 
@@ -209,3 +213,23 @@ def test_table_rows_reads_a_row_range_of_a_host_table():
     # copies, not views: the ring slot behind a delivered piece is reused after the callback
     rows["DM"][0] = -1.0
     assert h.arrays["DM"].reshape(-1)[3] != -1.0
+
+
+def test_uniform_threshold_integer_test_equals_float_test(tmp_path):
+    """The batched draw compares the MWC state x with an integer threshold instead
+    of converting x to the uniform 2^-32 * (float)x: for 2.2e6 thresholds (random,
+    tiny, and around every power of two) the threshold passes u <= thr and the next
+    integer does not (tests/cpp/uniform_threshold_check.cu, run on the host)."""
+    import shutil
+    import subprocess
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not available")
+    here = os.path.dirname(os.path.abspath(__file__))
+    exe = str(tmp_path / "utc")
+    subprocess.run([nvcc, "-O2", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler",
+                    "-ffp-contract=off", "-I", os.path.join(ROOT, "galfast_b200", "csrc"), "-o", exe,
+                    os.path.join(here, "cpp", "uniform_threshold_check.cu")], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True)
+    n, bad = (int(x) for x in r.stdout.split())
+    assert r.returncode == 0 and bad == 0 and n > 2000000, r.stdout

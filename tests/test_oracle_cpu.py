@@ -98,3 +98,42 @@ def test_draw_count_is_consistent_with_expectation(lib, multipliers):
     st, _ = O.run_catalog(w, multipliers)
     gen = sum(st["generated"].values())
     assert abs(gen - exp) < 5 * math.sqrt(exp)
+
+
+@pytest.mark.parametrize("nthreads,capacity", [(7680, 1 << 18), (7680, 1500), (97, 700), (3, 400)])
+def test_parallel_oracle_equals_sequential(lib, multipliers, nthreads, capacity):
+    """The oracle on several host threads (streams crawled in parallel, then the
+    stream that crosses a batch boundary and the later ones run again; parallel
+    sort, permutation and modules) gives the catalog, batch boundaries and stream
+    states of the reference's one-thread-after-another order, including batches
+    that stop part-way through a stream while Bond2010 shares the streams."""
+    w = patch(lib, half_deg=1.5, nthreads=nthreads, capacity=capacity)
+    runs = []
+    for threads in (1, 4):
+        rows = []
+        st, state = O.run_catalog(w, multipliers, threads=threads,
+                                  sink=lambda m, t, off: rows.append((m, off, t.as_dict())))
+        runs.append((rows, st, state))
+    (r1, s1, st1), (r4, s4, st4) = runs
+    assert len(r1) == len(r4) and (capacity > 1 << 17 or len(r1) > 3)
+    for (m1, o1, a), (m4, o4, b) in zip(r1, r4):
+        assert (m1, o1) == (m4, o4)
+        for c in a:
+            np.testing.assert_array_equal(a[c], b[c], err_msg=c)
+    assert s1["generated"] == s4["generated"] and s1["stored"] == s4["stored"]
+    assert np.array_equal(st1, st4)
+
+
+def test_parallel_seeding_equals_glibc(multipliers):
+    """Stream seeding on several host threads (the drand48 recurrence with
+    jump-ahead) equals glibc's srand48/drand48/lrand48 sequence."""
+    L = O.load("p")
+    try:
+        for seed in (0, 42, 0xFFFFFFFF):
+            L.or_set_threads(1)
+            a = O.seed_streams(seed, multipliers)
+            L.or_set_threads(5)
+            b = O.seed_streams(seed, multipliers)
+            assert np.array_equal(a, b), seed
+    finally:
+        L.or_set_threads(1)
