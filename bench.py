@@ -218,6 +218,7 @@ def main():
     ap.add_argument("--clock-log", default=None, help="CSV of the SM clock samples taken during the timed region")
     ap.add_argument("--requests", type=int, default=C4_NREQ, help="config4: requests per step (a prefix of the set)")
     ap.add_argument("--parity", type=int, default=16, help="config4: timed requests re-run alone and compared (0: none)")
+    ap.add_argument("--text-requests", type=int, default=32, help="config4: requests written as text catalogs (0: none)")
     ap.add_argument("--serve-rates", default="100,1000", help="config4: arrival rates of the serving sub-measurement ('' = none)")
     args = ap.parse_args()
     global CLOCK_LOG
@@ -456,10 +457,15 @@ def bench_multi(args, G, W, ctx, rank, world, dist):
             ref = standalone_rows(G, ctx, ws[j])
             ok = same_catalog(ref, got.get(j, {}))
             equal += int(ok)
-            nrows += sum(len(v["DM"]) for v in ref.values())
+            nrows += sum(len(p["DM"]) for parts in ref.values() for p in parts)
         parity = {"checked": len(check_ids), "equal": equal, "rows": nrows,
                   "against": "the same requests through gf_catalog_run alone (plain path), every column compared bit for bit",
                   "requests": "every %dth request of the timed set" % C4_PLAIN_STRIDE}
+
+    # ---- the catalog written as text files (gf_textout, the reference's os_textout) ----
+    textout = None
+    if args.text_requests > 0 and rank == 0:
+        textout = text_output(G, L, ctx, ws[:args.text_requests])
 
     # ---- rooflines: the batched draw (dominant kernel) and the pixel integrate ----
     clk_summary = clock.summary()
@@ -524,11 +530,43 @@ def bench_multi(args, G, W, ctx, rank, world, dist):
                           "gf_catalog_run, one at a time" % (C4_PLAIN_STRIDE, len(sample)),
                           "latency_p50_s": float(np.percentile(plat, 50)), "latency_p99_s": float(np.percentile(plat, 99))},
                 "batched_over_plain": value / plain_value if plain_value else None,
-                "parity": parity, "serve": serve,
+                "parity": parity, "serve": serve, "text_output": textout,
                 "e2e": e2e, "roofline": roofline, "integrate_roofline": integ_roof, "roofline_hbm": roofline_hbm,
                 "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk_summary,
                 "phases_ms_per_step": {k: v[0] / args.steps for k, v in prof.items()}}
         print(json.dumps(line))
+
+
+def text_output(G, L, ctx, ws):
+    """The requests' catalogs written to text files in the reference's format while
+    the device generates (gf_catalog_run_multi_host + gf_textout_multi_sink, one
+    file per request, formatting on all host threads); host wall clock from the
+    call to the last byte written, files removed afterwards."""
+    import shutil
+    n = len(ws)
+    d = tempfile.mkdtemp(prefix="gf_text_")
+    try:
+        writers = [G.TextWriter(os.path.join(d, "sky%04d.obs.txt" % j), G.textout_config(w)) for j, w in enumerate(ws)]
+        arr = (C.c_void_p * n)(*[wr.h.value for wr in writers])
+        tset = G.TextoutSet(n, C.cast(arr, C.POINTER(C.c_void_p)))
+        sink = G.MultiHostCallback(C.cast(L.gf_textout_multi_sink, C.c_void_p).value)
+        jobs = (G.Job * n)(*[w.job(G.Job) for w in ws])
+        stats = (G.CatalogStats * n)()
+        ctx.set_host_columns(G.COL_ALL & ~(G.COL["projIdx"] | G.COL["projXY"]))
+        t0 = time.perf_counter()
+        G.check(L.gf_catalog_run_multi_host(ctx.h, jobs, n, 0, sink, C.byref(tset), stats))
+        rows = nbytes = 0
+        for wr in writers:
+            r, b = wr.close()
+            rows += r
+            nbytes += b
+        dt = time.perf_counter() - t0
+        ctx.set_host_columns(G.COL_ALL)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    return {"requests": n, "rows": int(rows), "bytes": int(nbytes), "seconds": dt, "stars_per_s": rows / dt,
+            "MB_per_s": nbytes / dt / 1e6, "threads": os.cpu_count(),
+            "path": "gf_catalog_run_multi_host + gf_textout_multi_sink: one text file per request, the first requests of the set"}
 
 
 def host_row_bytes(G, t):

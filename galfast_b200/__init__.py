@@ -105,6 +105,10 @@ def lib():
         L.gf_multi_set_host_columns.argtypes = [vp, C.c_uint32]
         L.gf_multi_set_admission.argtypes = [vp, C.c_double]
         L.gf_debug_fail_allocations.argtypes = [C.c_int64, C.c_int64]
+        L.gf_textout_open.argtypes = [C.c_char_p, vp, C.POINTER(vp)]
+        L.gf_textout_write.argtypes = [vp, vp, C.c_int64, C.c_int64]
+        L.gf_textout_close.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.gf_textout_multi_sink.argtypes = [vp, C.c_int32, vp, vp, vp]
         L.gf_tuning_get.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32)]
         L.gf_tuning_set.argtypes = [vp, C.c_int32, C.c_int32]
         L.gf_table_download_rows.argtypes = [vp, C.POINTER(Table), C.c_int64, C.c_int64, C.POINTER(Table)]
@@ -266,9 +270,12 @@ class Context:
         check(lib().gf_rng_init(self.h, seed48, nstreams))
         self.nstreams = nstreams + (-nstreams) % 64
 
-    def rng_state(self):
-        s = np.zeros(3 * self.nstreams, dtype=np.uint32)
-        check(lib().gf_rng_get_state(self.h, s.ctypes.data, self.nstreams))
+    def rng_state(self, nstreams=None):
+        """The [3][nstreams] stream states (nstreams: as seeded by rng_init, or given
+        for streams a catalog run seeded)."""
+        n = self.nstreams if nstreams is None else int(nstreams)
+        s = np.zeros(3 * n, dtype=np.uint32)
+        check(lib().gf_rng_get_state(self.h, s.ctypes.data, n))
         return s
 
     def set_rng_state(self, s):
@@ -532,3 +539,66 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# catalog text output (gf_textout, the reference's os_textout)
+# ---------------------------------------------------------------------------
+class TextoutConfig(C.Structure):
+    _fields_ = [("bandset", C.c_char_p), ("bands", C.POINTER(C.c_char_p)), ("nbands", C.c_int32),
+                ("band", C.c_char_p), ("absband", C.c_char_p), ("radec", C.c_int32), ("feh", C.c_int32),
+                ("vcyl", C.c_int32), ("pm_coordsys", C.c_int32), ("photoerrors", C.c_int32),
+                ("comp_ids", C.POINTER(C.c_int32)), ("ncomp", C.c_int32), ("version", C.c_char_p),
+                ("threads", C.c_int32)]
+
+
+class TextoutSet(C.Structure):
+    _fields_ = [("njobs", C.c_int32), ("writers", C.POINTER(C.c_void_p))]
+
+
+def textout_config(w, version=None, threads=0):
+    """The text-output columns of a workload's module chain: SDSS-like ugriz
+    (bandset SDSSugriz) or LSST-like ugrizy (LSSTugrizy) by the band count,
+    bootstrap band r."""
+    cfg = TextoutConfig()
+    nb = int(w.nbands)
+    keep = []
+    if nb:
+        pre, bs = ("SDSS", "SDSSugriz") if nb == 5 else ("LSST", "LSSTugrizy")
+        bands = [pre + ch for ch in "ugrizy"[:nb]]
+        arr = (C.c_char_p * nb)(*[b.encode() for b in bands])
+        keep.append(arr)
+        cfg.bandset = bs.encode()
+        cfg.bands = arr
+        cfg.nbands = nb
+        cfg.band = bands[2].encode()
+    else:
+        cfg.band = b"SDSSr"
+    cfg.radec = 1 if w.gal2other else 0
+    cfg.feh = 1 if w.feh is not None else 0
+    cfg.vcyl = 1 if w.kin is not None else 0
+    cfg.pm_coordsys = int(w.v2pm.coordsys) if w.v2pm is not None else -1
+    cfg.photoerrors = 1 if w.perr is not None else 0
+    cfg.version = version.encode() if version else None
+    cfg.threads = int(threads)
+    cfg._keep = keep
+    return cfg
+
+
+class TextWriter:
+    """gf_textout: a catalog text file in the reference's format."""
+
+    def __init__(self, path, cfg):
+        self.h = C.c_void_p()
+        self.cfg = cfg
+        check(lib().gf_textout_open(str(path).encode(), C.byref(cfg), C.byref(self.h)))
+
+    def write(self, table, begin, end):
+        check(lib().gf_textout_write(self.h, C.byref(table), int(begin), int(end)))
+
+    def close(self):
+        rows, nbytes = C.c_int64(), C.c_int64()
+        if self.h:
+            check(lib().gf_textout_close(self.h, C.byref(rows), C.byref(nbytes)))
+            self.h = C.c_void_p()
+        return rows.value, nbytes.value

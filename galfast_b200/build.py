@@ -21,7 +21,7 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIBNAME = "libgalfast_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-SOURCES = ["gf_skygen.cu", "gf_modules.cu", "gf_api.cu", "gf_static.cu", "gf_multi.cu", "gf_integrate.cu", "gf_batchdraw.cu", "gf_precision.cu", "gf_server.cpp", "gf_host.cpp", "gf_safeprimes.cpp"]
+SOURCES = ["gf_skygen.cu", "gf_modules.cu", "gf_api.cu", "gf_static.cu", "gf_multi.cu", "gf_integrate.cu", "gf_batchdraw.cu", "gf_precision.cu", "gf_server.cpp", "gf_host.cpp", "gf_safeprimes.cpp", "gf_textout.cpp"]
 
 
 def nvcc_path():

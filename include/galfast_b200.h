@@ -538,6 +538,51 @@ gf_status gf_skygen_integrate_static(const gf_skygen_config *cfg, const gf_penci
                                      const float *d_beam_ammin, const gf_extinction *ext,
                                      const gf_model_config *model, double *d_result, void *cuda_stream);
 
+/* ---- catalog text output (os_textout, src/pipeline.cpp:199-289) ---- */
+
+/* The columns of the text catalog and their names.  The file is the
+ * reference's: a "# " header line with every output column's definition
+ * (otable::serialize_header, src/common/otable.cpp:542-558), an optional
+ * "# generated with galfast version ..." line, then one line per row that is
+ * not hidden, each column component printed with the column's printf format
+ * (otable.cpp:719-745) and separated by single spaces.  Columns come in the
+ * reference's output order: lb, radec, XYZ, DM, the absolute magnitude, comp,
+ * FeH, vcyl, pmlb/pmradec, Am, AmInf, then the photometry columns by name. */
+typedef struct gf_textout_config {
+    const char *bandset;             /* photometric system, e.g. "SDSSugriz" (NULL: no photometry columns) */
+    const char *const *bands;        /* nbands band names, e.g. "SDSSu" ... */
+    int32_t nbands;
+    const char *band;                /* bootstrap band of the absolute magnitude, e.g. "SDSSr" */
+    const char *absband;             /* its column name (NULL: "abs" + band) */
+    int32_t radec;                   /* gal2other equatorial coordinates present */
+    int32_t feh;                     /* FeH present */
+    int32_t vcyl;                    /* Bond2010 velocities present */
+    int32_t pm_coordsys;             /* vel2pm: -1 absent, 0 pmlb, 1 pmradec */
+    int32_t photoerrors;             /* observed magnitudes present */
+    const int32_t *comp_ids;         /* comp column value -> component id written (NULL: as stored) */
+    int32_t ncomp;
+    const char *version;             /* galfast version for the second header line (NULL: none) */
+    int32_t threads;                 /* formatting threads (0: all hardware threads) */
+} gf_textout_config;
+
+typedef struct gf_textout gf_textout;
+gf_status gf_textout_open(const char *path, const gf_textout_config *cfg, gf_textout **out);
+/* Append the rows [begin, end) of a HOST table that are not hidden (formatted on
+ * the writer's threads, written in order).  One write at a time per writer. */
+gf_status gf_textout_write(gf_textout *w, const gf_table *host, int64_t begin, int64_t end);
+/* Close the file; rows and bytes written (nullable). */
+gf_status gf_textout_close(gf_textout *w, int64_t *rows, int64_t *bytes);
+
+/* One writer per request of a multi-request run: pass gf_textout_multi_sink and
+ * a gf_textout_set to gf_catalog_run_multi_host to write every request's
+ * catalog while the device generates the next pass (writers[j] NULL: request
+ * j is not written). */
+typedef struct gf_textout_set {
+    int32_t njobs;
+    gf_textout *const *writers;
+} gf_textout_set;
+int gf_textout_multi_sink(void *set, int32_t model, const gf_table *host, const int64_t *row_begin, const int64_t *row_count);
+
 /* ---- failure injection (tests) ---- */
 
 /* Make the library's device allocations fail as if the device were out of

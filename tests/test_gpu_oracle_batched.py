@@ -122,7 +122,7 @@ def test_poisson_large_mu_plain_and_batched_equal_oracle(lib, multipliers):
     for i in range(3):
         assert gst.generated[i] == st["generated"][i]
     # the streams after the whole catalog (skygen and Bond2010 consume them)
-    gstate = ctx.rng_state()
+    gstate = ctx.rng_state(w.nstreams)
     assert np.array_equal(gstate, ostate), "stream states differ after the catalog"
 
     # batched path: the request twice in one call, with another seed's copy between them

@@ -183,7 +183,7 @@ def test_photometric_error_statistics(ctx, lib, nbands, m5):
     normalised deviations have mean 0 (within 5 / sqrt(n)) and standard deviation 1
     (within 1 %), and in every 0.5-mag bin of true magnitude the spread of
     obs - true equals the formula's sigma within 3 %."""
-    w = W.build_workload(lib, foot=W.cap_footprint(60.0, 40.0, 7.0), dx_deg=0.1, m0=14.0, m1=22.0,
+    w = W.build_workload(lib, foot=W.cap_footprint(60.0, 40.0, 10.0), dx_deg=0.1, m0=14.0, m1=22.0,
                          capacity=1 << 22, nbands=nbands, m5=m5)
     true, obs = [], []
 
