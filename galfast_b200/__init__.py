@@ -32,7 +32,8 @@ class Job(C.Structure):
                 ("seed48", C.c_uint32), ("nstreams", C.c_int32), ("capacity", C.c_int64), ("nbands", C.c_int32),
                 ("foot", C.POINTER(Footprint)), ("feh", C.POINTER(FixedFeHConfig)),
                 ("kin", C.POINTER(Bond2010Config)), ("phot", C.POINTER(PhotometryConfig)),
-                ("perr", C.POINTER(PhotoerrConfig)), ("v2pm", C.POINTER(Vel2pmConfig)), ("gal2other", C.c_int32)]
+                ("perr", C.POINTER(PhotoerrConfig)), ("v2pm", C.POINTER(Vel2pmConfig)), ("gal2other", C.c_int32),
+                ("feh_ivezic", C.POINTER(A.FehConfig)), ("feh_gauss", C.POINTER(A.GaussFehConfig))]
 
 
 class CatalogStats(C.Structure):
@@ -89,6 +90,8 @@ def lib():
         L.gf_module_clipper.argtypes = [vp, C.POINTER(Footprint), C.POINTER(Lambert), C.POINTER(Table), C.c_int64, C.c_int64]
         L.gf_module_fixedfeh.argtypes = [vp, C.POINTER(FixedFeHConfig), C.POINTER(Table), C.c_int64, C.c_int64]
         L.gf_module_bond2010.argtypes = [vp, C.POINTER(Bond2010Config), C.POINTER(Table), C.c_int64, C.c_int64]
+        L.gf_module_feh.argtypes = [vp, C.POINTER(A.FehConfig), C.POINTER(Table), C.c_int64, C.c_int64]
+        L.gf_module_gaussfeh.argtypes = [vp, C.POINTER(A.GaussFehConfig), C.POINTER(Table), C.c_int64, C.c_int64]
         L.gf_photometry_create.argtypes = [vp, C.POINTER(PhotometryConfig), C.POINTER(vp)]
         L.gf_photometry_destroy.argtypes = [vp]
         L.gf_module_photometry.argtypes = [vp, vp, C.POINTER(Table), C.c_int64, C.c_int64]
@@ -147,7 +150,7 @@ COLUMNS = [  # name, dtype, components (or "bands")
     ("absmag", np.float32, 1), ("XYZ", np.float32, 3), ("comp", np.int32, 1), ("Am", np.float32, 1),
     ("AmInf", np.float32, 1), ("hidden", np.int32, 1), ("FeH", np.float32, 1), ("vcyl", np.float32, 3),
     ("mags", np.float32, "bands"), ("photoflags", np.int32, 1), ("obsmags", np.float32, "bands"),
-    ("pm", np.float32, 3), ("radec", np.float64, 2),
+    ("pm", np.float32, 3), ("radec", np.float64, 2), ("FeH_comp", np.int32, 1),
 ]
 PROFILE_PHASES = ["integrate", "draw_window", "draw_rerun", "place", "sort", "clipper", "fixedfeh", "bond2010",
                   "photometry", "photoerrors", "vel2pm", "gal2other", "slot_density", "expand", "batch_draw"]
@@ -547,7 +550,7 @@ class Server:
 class TextoutConfig(C.Structure):
     _fields_ = [("bandset", C.c_char_p), ("bands", C.POINTER(C.c_char_p)), ("nbands", C.c_int32),
                 ("band", C.c_char_p), ("absband", C.c_char_p), ("radec", C.c_int32), ("feh", C.c_int32),
-                ("vcyl", C.c_int32), ("pm_coordsys", C.c_int32), ("photoerrors", C.c_int32),
+                ("feh_comp", C.c_int32), ("vcyl", C.c_int32), ("pm_coordsys", C.c_int32), ("photoerrors", C.c_int32),
                 ("comp_ids", C.POINTER(C.c_int32)), ("ncomp", C.c_int32), ("version", C.c_char_p),
                 ("threads", C.c_int32)]
 
@@ -575,7 +578,8 @@ def textout_config(w, version=None, threads=0):
     else:
         cfg.band = b"SDSSr"
     cfg.radec = 1 if w.gal2other else 0
-    cfg.feh = 1 if w.feh is not None else 0
+    cfg.feh = 1 if (w.feh is not None or w.feh_ivezic is not None or w.feh_gauss is not None) else 0
+    cfg.feh_comp = 1 if w.feh_gauss is not None else 0
     cfg.vcyl = 1 if w.kin is not None else 0
     cfg.pm_coordsys = int(w.v2pm.coordsys) if w.v2pm is not None else -1
     cfg.photoerrors = 1 if w.perr is not None else 0

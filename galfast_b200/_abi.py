@@ -63,11 +63,26 @@ class Table(C.Structure):
                 ("comp", C.c_void_p), ("Am", C.c_void_p), ("AmInf", C.c_void_p),
                 ("hidden", C.c_void_p), ("FeH", C.c_void_p), ("vcyl", C.c_void_p),
                 ("mags", C.c_void_p), ("photoflags", C.c_void_p), ("obsmags", C.c_void_p),
-                ("pm", C.c_void_p), ("radec", C.c_void_p)]
+                ("pm", C.c_void_p), ("radec", C.c_void_p), ("FeH_comp", C.c_void_p)]
 
 
 class FixedFeHConfig(C.Structure):
     _fields_ = [("FeH", C.c_float), ("comp_mask", C.c_uint32)]
+
+
+class FehConfig(C.Structure):            # gf_feh_config (os_FeH, Ivezic et al. 2008)
+    _fields_ = [("A", C.c_float * 2), ("sigma", C.c_float * 3), ("offs", C.c_float * 3), ("Hmu", C.c_float),
+                ("muInf", C.c_float), ("DeltaMu", C.c_float), ("comp_thin", C.c_uint32), ("comp_thick", C.c_uint32),
+                ("comp_halo", C.c_uint32), ("M", C.c_float * 9), ("T", C.c_float * 3)]
+
+
+GF_GAUSSFEH_MAXCOMP = 10
+
+
+class GaussFehConfig(C.Structure):       # gf_gaussfeh_config (os_GaussianFeH)
+    _fields_ = [("ncomp", C.c_int32), ("mean", C.c_float * GF_GAUSSFEH_MAXCOMP),
+                ("sigma", C.c_float * GF_GAUSSFEH_MAXCOMP), ("pcum", C.c_float * GF_GAUSSFEH_MAXCOMP),
+                ("comp_mask", C.c_uint32)]
 
 
 class VMoments(C.Structure):

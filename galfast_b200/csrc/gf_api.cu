@@ -75,6 +75,7 @@ gf_status zero_module_rows(gf_ctx *ctx, const gf_table *t, int64_t n)
     GF_TRY(z(t->obsmags, 4, (size_t)t->nbands));
     GF_TRY(z(t->pm, 4, 3));
     GF_TRY(z(t->radec, 8, 2));
+    GF_TRY(z(t->FeH_comp, 4, 1));
     return GF_OK;
 }
 
@@ -979,6 +980,7 @@ static gf_status table_alloc_columns(gf_table *t, size_t n, int32_t nbands)
     GF_TRY(dev_alloc(&t->photoflags, n));
     GF_TRY(dev_alloc(&t->pm, 3 * n));
     GF_TRY(dev_alloc(&t->radec, 2 * n));
+    GF_TRY(dev_alloc(&t->FeH_comp, n));
     return GF_OK;
 }
 
@@ -1008,7 +1010,7 @@ gf_status gf_table_free(gf_ctx *ctx, gf_table *t)
     dev_free(t->lb); dev_free(t->projIdx); dev_free(t->projXY); dev_free(t->DM); dev_free(t->absmag);
     dev_free(t->XYZ); dev_free(t->comp); dev_free(t->Am); dev_free(t->AmInf); dev_free(t->hidden);
     dev_free(t->FeH); dev_free(t->vcyl); dev_free(t->mags); dev_free(t->photoflags); dev_free(t->obsmags);
-    dev_free(t->pm); dev_free(t->radec);
+    dev_free(t->pm); dev_free(t->radec); dev_free(t->FeH_comp);
     memset(t, 0, sizeof(*t));
     return GF_OK;
 }
@@ -1046,6 +1048,7 @@ gf_status gf_table_download_rows(gf_ctx *ctx, const gf_table *dev, int64_t begin
     GF_TRY(cp(host->obsmags, dev->obsmags, 4, dev->nbands));
     GF_TRY(cp(host->pm, dev->pm, 4, 3));
     GF_TRY(cp(host->radec, dev->radec, 8, 2));
+    GF_TRY(cp(host->FeH_comp, dev->FeH_comp, 4, 1));
     GF_CUDA(cudaStreamSynchronize(st));
     host->size = end - begin;
     return GF_OK;
@@ -1084,6 +1087,35 @@ gf_status gf_module_fixedfeh(gf_ctx *ctx, const gf_fixedfeh_config *cfg, gf_tabl
     ProfScope ps(ctx, GF_PROF_FEH);
     GF_CUDA(gfk::launch_fixedfeh(*cfg, *t, begin, end, ctx->stream));
     return GF_OK;
+}
+
+static gf_status module_feh(gf_ctx *ctx, const gf_feh_config *fp, const gf_gaussfeh_config *gp, gf_table *t,
+                            int64_t begin, int64_t end)
+{
+    GF_TRY(check_ctx(ctx));
+    GF_TRY(row_range(t, begin, end));
+    if (!fp && !gp) return fail(GF_E_INVALID, "null config");
+    if (gp && (gp->ncomp < 1 || gp->ncomp >= GF_GAUSSFEH_MAXCOMP || !(gp->pcum[gp->ncomp - 1] > 0.f)))
+        return fail(GF_E_INVALID, "GaussianFeH needs 1 <= ncomp < 10 and positive cumulative weights");
+    if (gp && !t->FeH_comp) return fail(GF_E_INVALID, "table without the FeH_comp column");
+    if (!ctx->d_rng) return fail(GF_E_STATE, "gf_rng_init must precede the metallicity modules");
+    const int64_t n = end - begin;
+    if ((n + 255) / 256 > ctx->rng_nstreams) return fail(GF_E_INVALID, "more than 256 rows per stream");
+    ProfScope ps(ctx, GF_PROF_FEH);
+    GF_CUDA(gfk::launch_feh(fp, gp, ctx->d_rng, ctx->rng_nstreams, *t, begin, end, ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_module_feh(gf_ctx *ctx, const gf_feh_config *cfg, gf_table *t, int64_t begin, int64_t end)
+{
+    if (!cfg) return fail(GF_E_INVALID, "null config");
+    return module_feh(ctx, cfg, nullptr, t, begin, end);
+}
+
+gf_status gf_module_gaussfeh(gf_ctx *ctx, const gf_gaussfeh_config *cfg, gf_table *t, int64_t begin, int64_t end)
+{
+    if (!cfg) return fail(GF_E_INVALID, "null config");
+    return module_feh(ctx, nullptr, cfg, t, begin, end);
 }
 
 gf_status gf_module_bond2010(gf_ctx *ctx, const gf_bond2010_config *cfg, gf_table *t, int64_t begin, int64_t end)
@@ -1264,6 +1296,8 @@ static gf_status catalog_run_once(gf_ctx *ctx, const gf_job *job, gf_batch_callb
             /* the module chain in pipeline order (pipeline.h:75-88) */
             if (job->foot) GF_TRY(gf_module_clipper(ctx, job->foot, job->sky.proj, &g.t, 0, n));
             if (job->feh) GF_TRY(gf_module_fixedfeh(ctx, job->feh, &g.t, 0, n));
+            if (job->feh_ivezic) GF_TRY(gf_module_feh(ctx, job->feh_ivezic, &g.t, 0, n));
+            if (job->feh_gauss) GF_TRY(gf_module_gaussfeh(ctx, job->feh_gauss, &g.t, 0, n));
             if (job->kin) GF_TRY(gf_module_bond2010(ctx, job->kin, &g.t, 0, n));
             if (g.ph) GF_TRY(gf_module_photometry(ctx, g.ph, &g.t, 0, n));
             if (g.pe) GF_TRY(gf_module_photoerrors(ctx, g.pe, row_offset, &g.t, 0, n));

@@ -68,6 +68,18 @@ __device__ __forceinline__ bool bd_has_stars(float u, float mu)
     return mu > 10.f || u > gfm::expf_(-mu);
 }
 
+/* a request's view for the draw walk (per warp, in shared memory) */
+struct DrawJobView {
+    const uint32_t *blk, *binfo;
+    const uint16_t *bslot, *dslot;
+    const float *slotD, *msbase, *lfmx;
+    const gf_pencil_beam *pixels;
+    int nslots, Bp, npix, x, y, N;
+    int QN, RN;                    /* N = QN Bp + RN: a stream's step in (pixel, block) */
+    float norm, dmin, dmax;
+    bool dlim, bound;
+};
+
 template <class T>
 __device__ __forceinline__ const T *plan_at(const unsigned char *plan, int off)
 {
@@ -124,7 +136,7 @@ __global__ void __launch_bounds__(256) slot_density_kernel(SlotDensityParams P)
  * sampler from the bin's stream state wb, then the stars' uniforms (draw_stars:
  * x, y, and M, m unless x^2 + y^2 > 2).  Returns the number of stars and the
  * stream state after them; fills the event record when there are stars. */
-__device__ __noinline__ int draw_event(uint32_t a, uint64_t wb, float mu, const gf_pencil_beam *pp, uint64_t &vnew,
+__device__ __forceinline__ int draw_event(uint32_t a, uint64_t wb, float mu, const gf_pencil_beam *pp, uint64_t &vnew,
                                        uint64_t &v_star)
 {
     gfr::Mwc r;
@@ -229,15 +241,10 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
     if (lane == 0) *nev = 0;
     __syncwarp();
 
+    /* the request's tables and scalars live in the warp's shared memory, not in
+     * registers: the walk keeps its registers for the stream state and the block */
+    DrawJobView &V = *(DrawJobView *)(mine + P.off_view);
     int loaded = -1;
-    const uint32_t *blk = nullptr;
-    const uint16_t *bslot = nullptr, *dslot = nullptr;
-    const float *slotD = nullptr, *msbase = nullptr, *lfmx = nullptr;
-    const uint32_t *binfo = nullptr;
-    const gf_pencil_beam *pixels = nullptr;
-    int nslots = 0, Bp = 1, npix = 0, x = 1, y = 1, N = 1;
-    float norm = 0.f, dmin = 0.f, dmax = 0.f;
-    bool dlim = false, bound = false;
 
     for (;;) {
         int it = 0;
@@ -252,48 +259,51 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
             const uint32_t *src = (const uint32_t *)&J.m;
             for (int w = lane; w < (int)(sizeof(SkyModel) / 4); w += 32) ((uint32_t *)&m)[w] = src[w];
             __syncwarp();
-            x = m.nm; y = m.nM; N = m.nthreads;
-            for (int q = lane; q < y; q += 32) LFM[q] = gfc::lf_sample(m, m.lf, m.M1 - (float)q * m.dM);
-            const unsigned char *plan = P.plans[job];
-            const IntegPlanHdr *h = (const IntegPlanHdr *)plan;
-            nslots = h->nslots;
-            Bp = h->nblocks;
-            slotD = plan_at<float>(plan, h->off_slot);
-            blk = plan_at<uint32_t>(plan, h->off_blk);
-            bslot = plan_at<uint16_t>(plan, h->off_bslot);
-            dslot = plan_at<uint16_t>(plan, h->off_dslot);
-            msbase = P.ms[job];
-            pixels = J.g.pixels;
-            npix = J.g.npixels;
-            norm = m.norm;
-            dmin = m.dmin;
-            dmax = m.dmax;
-            dlim = m.dmin != 0.f || m.dmax != 0.f;
-            binfo = plan_at<uint32_t>(plan, h->off_binfo);
-            lfmx = P.lfmax ? P.lfmax[job] : nullptr;
-            /* the block bound needs non-negative densities (f >= 0) and normalisation */
-            bound = lfmx && !dlim && m.f >= 0.f && m.norm >= 0.f;
+            for (int q = lane; q < m.nM; q += 32) LFM[q] = gfc::lf_sample(m, m.lf, m.M1 - (float)q * m.dM);
+            if (lane == 0) {
+                const unsigned char *plan = P.plans[job];
+                const IntegPlanHdr *h = (const IntegPlanHdr *)plan;
+                V.x = m.nm; V.y = m.nM; V.N = m.nthreads;
+                V.nslots = h->nslots;
+                V.Bp = h->nblocks;
+                V.QN = V.N / V.Bp;
+                V.RN = V.N - V.QN * V.Bp;
+                V.slotD = plan_at<float>(plan, h->off_slot);
+                V.blk = plan_at<uint32_t>(plan, h->off_blk);
+                V.bslot = plan_at<uint16_t>(plan, h->off_bslot);
+                V.dslot = plan_at<uint16_t>(plan, h->off_dslot);
+                V.binfo = plan_at<uint32_t>(plan, h->off_binfo);
+                V.msbase = P.ms[job];
+                V.pixels = J.g.pixels;
+                V.npix = J.g.npixels;
+                V.norm = m.norm;
+                V.dmin = m.dmin;
+                V.dmax = m.dmax;
+                V.dlim = m.dmin != 0.f || m.dmax != 0.f;
+                V.lfmx = P.lfmax ? P.lfmax[job] : nullptr;
+                /* the block bound needs non-negative densities (f >= 0) and normalisation */
+                V.bound = V.lfmx && !V.dlim && m.f >= 0.f && m.norm >= 0.f;
+            }
             __syncwarp();
             loaded = job;
         }
-        if (BOUND && !bound) {
+        if (BOUND && !V.bound) {
             /* the host put a request that needs the exact test into the bound launch */
             if (lane == 0) atomicOr(P.err, 2ull);
             continue;
         }
         const int NS = J.rng_nstreams;
         uint32_t *rng = J.rng;
-        const bool stream_ok = t < N;
+        const bool stream_ok = t < V.N;
         const uint32_t a = stream_ok ? rng[t] : 0u;
         uint64_t w = stream_ok ? (((uint64_t)rng[NS + t] << 32) | rng[2 * NS + t]) : 0ull;
         const int sid = (job << 16) | t;
         /* block r of stream t is the (t + r N)-th block of the request */
-        int pix = stream_ok ? t / Bp : npix, lb = stream_ok ? t - (t / Bp) * Bp : 0;
-        const int QN = N / Bp, RN = N - QN * Bp;
+        int pix = stream_ok ? t / V.Bp : V.npix, lb = stream_ok ? t - (t / V.Bp) * V.Bp : 0;
         int nst = 0;
         bool stop = !stream_ok;
         for (;;) {
-            const bool valid = !stop && pix < npix;
+            const bool valid = !stop && pix < V.npix;
             if (!__any_sync(BD_FULL, valid)) break;
             if constexpr (BOUND) {
                 /* Upper bound of the block's expected counts: the reference's float product
@@ -304,29 +314,29 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                 int i0 = 0, j0 = 0, sl0 = 0;
                 float K = 0.f, thr = 0.f;
                 int64_t xthr = -1;             /* uniform u = 2^-32 x passes the bound iff x <= xthr */
-                const float *msr = msbase;
+                const float *msr = V.msbase;
                 const uint64_t w0 = w;
                 if (valid) {
-                    const uint32_t bij = __ldg(blk + lb);
+                    const uint32_t bij = __ldg(V.blk + lb);
                     i0 = (int)(bij & 0xffffu);
                     j0 = (int)(bij >> 16);
-                    const uint32_t bi = __ldg(binfo + lb);
+                    const uint32_t bi = __ldg(V.binfo + lb);
                     const int imax = (int)(bi & 0xffffu);
                     const uint32_t wm = (bi >> 16) & 0x3ffu;
-                    sl0 = __ldg(bslot + lb);
-                    msr = msbase + (size_t)pix * (nslots + 2);
-                    const int icut = __float_as_int(msr[nslots]);
-                    K = msr[nslots + 1];
-                    float msmax = msr[sl0], Dmax = __ldg(slotD + sl0);
+                    sl0 = __ldg(V.bslot + lb);
+                    msr = V.msbase + (size_t)pix * (V.nslots + 2);
+                    const int icut = __float_as_int(msr[V.nslots]);
+                    K = msr[V.nslots + 1];
+                    float msmax = msr[sl0], Dmax = __ldg(V.slotD + sl0);
                     int d = i0 + j0;
                     for (uint32_t mm = wm; mm; mm &= mm - 1u) {
                         d++;
-                        const int sl = __ldg(dslot + d);
+                        const int sl = __ldg(V.dslot + d);
                         msmax = fmaxf(msmax, msr[sl]);
-                        Dmax = fmaxf(Dmax, __ldg(slotD + sl));
+                        Dmax = fmaxf(Dmax, __ldg(V.slotD + sl));
                     }
-                    float mub = fmaxf(__ldg(lfmx + lb), 0.f) * msmax;
-                    mub *= norm;
+                    float mub = fmaxf(__ldg(V.lfmx + lb), 0.f) * msmax;
+                    mub *= V.norm;
                     mub *= Dmax * Dmax * Dmax;
                     mub *= K;
                     thr = (1.0f - mub) - 3.0e-7f;
@@ -339,7 +349,7 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                         for (int s = 1; s < GF_BLOCK; s++) {
                             if ((wm >> s) & 1u) {
                                 dd++;
-                                ii = dd - (y - 1) > 0 ? dd - (y - 1) : 0;
+                                ii = dd - (V.y - 1) > 0 ? dd - (V.y - 1) : 0;
                             } else {
                                 ii++;
                             }
@@ -359,25 +369,58 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                     }
                 }
                 if (cand) {
-                    /* the block again in order from its first state, exact where the bound fails */
+                    /* Exact tests from the first candidate bin on.  The state before bin
+                     * s is w0 advanced over the live bins before s; the bin's position
+                     * follows from the block's diagonal starts (wm), as step_in_pixel
+                     * walks it.  While no star is drawn the uniforms are the bound
+                     * walk's, so once no candidate is left the walk's end state stands. */
+                    const uint64_t w_end = w;
+                    const bool walked = xthr >= 0;
+                    const uint32_t bi = __ldg(V.binfo + lb);
+                    const uint32_t wm = (bi >> 16) & 0x3ffu;
+                    int s = __ffs(cand) - 1;
                     w = w0;
-                    int i = i0, j = j0, slot = sl0;
-                    float ms = msr[slot], D = __ldg(slotD + slot);
+                    for (uint32_t q = live & ((1u << s) - 1u); q; q &= q - 1u) bd_mwc_x(w, a);
+                    /* position and anchor of bin s */
+                    const uint32_t starts = wm & ((2u << s) - 2u);         /* diagonal starts in bins 1..s */
+                    int d = i0 + j0 + __popc(starts), i, j, slot;
+                    if (starts) {
+                        const int s1 = 31 - __clz(starts);
+                        i = d - (V.y - 1) > 0 ? d - (V.y - 1) : 0;
+                        i += s - s1;
+                        j = d - i;
+                        slot = __ldg(V.dslot + d);
+                    } else {
+                        i = i0 + s;
+                        j = j0 - s;
+                        slot = sl0;
+                    }
+                    float ms = msr[slot], D = __ldg(V.slotD + slot);
                     float D3 = D * D * D;
-                    for (int s = 0; s < GF_BLOCK; s++) {
-                        if (s > 0 && gfc::step_in_pixel(i, j, x, y)) {
-                            slot = __ldg(dslot + i + j);
-                            ms = msr[slot];
-                            D = __ldg(slotD + slot);
-                            D3 = D * D * D;
+                    bool star = false;
+                    for (const int s0 = s; s < GF_BLOCK; s++) {
+                        if (s > s0) {
+                            if ((wm >> s) & 1u) {
+                                d++;
+                                i = d - (V.y - 1) > 0 ? d - (V.y - 1) : 0;
+                                j = d - i;
+                                slot = __ldg(V.dslot + d);
+                                ms = msr[slot];
+                                D = __ldg(V.slotD + slot);
+                                D3 = D * D * D;
+                            } else {
+                                i++;
+                                j--;
+                            }
                         }
                         if (!((live >> s) & 1u)) continue;
+                        if (walked && !star && !(cand >> s)) { w = w_end; break; }
                         const uint64_t wb = w;
                         const uint32_t xs = bd_mwc_x(w, a);
                         if ((int64_t)xs <= xthr) continue;
                         const float u = GF_MWC_SCALE * (float)xs;
                         float r = LFM[j] * ms;
-                        r *= norm;
+                        r *= V.norm;
                         r *= D3;
                         r *= K;
                         if (bd_surely_empty(u, r) || !bd_has_stars(u, r)) continue;
@@ -388,7 +431,8 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                             break;
                         }
                         uint64_t v_star = 0;
-                        const int k = draw_event(a, wb, r, pixels + pix, w, v_star);
+                        const int k = draw_event(a, wb, r, V.pixels + pix, w, v_star);
+                        star = true;
                         if (k > 0) {
                             EventRecord e;
                             e.stream = sid;
@@ -406,37 +450,37 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                 }
                 __syncwarp();
                 if (*nev >= GF_EVBUF / 2) flush_events(P, evb, nev, lane);
-                pix += QN;
-                lb += RN;
-                if (lb >= Bp) { lb -= Bp; pix++; }
+                pix += V.QN;
+                lb += V.RN;
+                if (lb >= V.Bp) { lb -= V.Bp; pix++; }
                 continue;
             } else {
             float mu[GF_BLOCK];
             uint32_t live = 0;
             int i0 = 0, j0 = 0;
             if (valid) {
-                const uint32_t bij = __ldg(blk + lb);
+                const uint32_t bij = __ldg(V.blk + lb);
                 i0 = (int)(bij & 0xffffu);
                 j0 = (int)(bij >> 16);
-                int slot = __ldg(bslot + lb);
-                const float *msr = msbase + (size_t)pix * (nslots + 2);
-                const int icut = __float_as_int(msr[nslots]);
-                const float K = msr[nslots + 1];
-                float ms = msr[slot], D = __ldg(slotD + slot);
+                int slot = __ldg(V.bslot + lb);
+                const float *msr = V.msbase + (size_t)pix * (V.nslots + 2);
+                const int icut = __float_as_int(msr[V.nslots]);
+                const float K = msr[V.nslots + 1];
+                float ms = msr[slot], D = __ldg(V.slotD + slot);
                 float D3 = D * D * D;
-                bool dc = dlim && (dmin > D || dmax <= D);      /* anchor outside [dmin, dmax): Am = inf */
+                bool dc = V.dlim && (V.dmin > D || V.dmax <= D);      /* anchor outside [V.dmin, V.dmax): Am = inf */
                 int i = i0, j = j0;
 #pragma unroll
                 for (int s = 0; s < GF_BLOCK; s++) {
-                    if (s > 0 && gfc::step_in_pixel(i, j, x, y)) {
-                        slot = __ldg(dslot + i + j);
+                    if (s > 0 && gfc::step_in_pixel(i, j, V.x, V.y)) {
+                        slot = __ldg(V.dslot + i + j);
                         ms = msr[slot];
-                        D = __ldg(slotD + slot);
+                        D = __ldg(V.slotD + slot);
                         D3 = D * D * D;
-                        dc = dlim && (dmin > D || dmax <= D);
+                        dc = V.dlim && (V.dmin > D || V.dmax <= D);
                     }
                     float r = LFM[j] * ms;
-                    r *= norm;
+                    r *= V.norm;
                     r *= D3;
                     r *= K;
                     mu[s] = r;
@@ -485,9 +529,9 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                         stop = true;
                         todo = 0;
                     } else {
-                        k = draw_event(a, wb_ev, mu_ev, pixels + pix, w, v_star);
+                        k = draw_event(a, wb_ev, mu_ev, V.pixels + pix, w, v_star);
                         ei = i0; ej = j0;
-                        for (int s = 1; s <= ev_s; s++) gfc::step_in_pixel(ei, ej, x, y);
+                        for (int s = 1; s <= ev_s; s++) gfc::step_in_pixel(ei, ej, V.x, V.y);
                     }
                 }
                 /* stage the bins with stars (all lanes converged) */
@@ -515,9 +559,9 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
             }
             if (*nev >= GF_EVBUF / 2) flush_events(P, evb, nev, lane);
             /* the stream's next block: N blocks further */
-            pix += QN;
-            lb += RN;
-            if (lb >= Bp) { lb -= Bp; pix++; }
+            pix += V.QN;
+            lb += V.RN;
+            if (lb >= V.Bp) { lb -= V.Bp; pix++; }
             }
         }
         if (stream_ok && !stop) {
@@ -599,6 +643,8 @@ cudaError_t launch_block_lfmax(const BlockLfParams &P, cudaStream_t s)
 size_t batch_draw_warp_bytes(int max_tab, BatchDrawParams *P)
 {
     size_t off = (sizeof(SkyModel) + 15) & ~(size_t)15;
+    P->off_view = (int32_t)off;
+    off += (sizeof(DrawJobView) + 15) & ~(size_t)15;
     P->off_tab = (int32_t)off;
     off += ((size_t)4 * max_tab + 15) & ~(size_t)15;
     P->off_ev = (int32_t)off;

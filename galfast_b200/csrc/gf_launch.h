@@ -82,8 +82,8 @@ struct LaunchPlaceMulti {
     float *projXY, *DM, *absmag, *XYZ, *Am, *AmInf;
     int32_t *hidden;
     uint64_t *key, *key_b;
-    uint32_t *idx_a, *idx_b, *slot_a, *slot_b;
-    int slot_bits;
+    uint32_t *idx_a, *idx_b, *slot_a;
+    int slot_bits;             /* bits of the output slot at the top of the sort key */
     void *temp;
     size_t temp_bytes;
     int64_t *seg_begin, *vis_end, *seg_end;     /* per slot, preset to zero by the caller */
@@ -111,6 +111,9 @@ cudaError_t launch_tie_gather_multi(const LaunchPlaceMulti &L, const int64_t *ro
 /* modules (gf_modules.cu) */
 cudaError_t launch_clipper(const gf_footprint &foot, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
 cudaError_t launch_poisson_stream(uint32_t *st, const float *mu, int32_t n, uint32_t *out, cudaStream_t s);
+/* os_FeH (fp) or os_GaussianFeH (gp): the one that is not NULL */
+cudaError_t launch_feh(const gf_feh_config *fp, const gf_gaussfeh_config *gp, uint32_t *rng, int32_t NS, gf_table t,
+                       int64_t begin, int64_t end, cudaStream_t s);
 cudaError_t launch_fixedfeh(const gf_fixedfeh_config &c, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
 cudaError_t launch_bond2010(const gf_bond2010_config &c, uint32_t *rng, int32_t rng_nstreams, gf_table t,
                             int64_t begin, int64_t end, cudaStream_t s);
@@ -207,7 +210,7 @@ struct BatchDrawParams {
     int64_t ev_capacity;
     unsigned long long *ev_count;  /* events found (may exceed the capacity) */
     unsigned long long *err;       /* set when a bin's expected count is infinite */
-    int32_t off_tab, off_ev, warp_bytes;   /* per-warp shared-memory layout (batch_draw_warp_bytes) */
+    int32_t off_view, off_tab, off_ev, warp_bytes;   /* per-warp shared-memory layout (batch_draw_warp_bytes) */
 };
 cudaError_t launch_slot_density(const SlotDensityParams &P, int model_type, cudaStream_t s);
 cudaError_t launch_block_lfmax(const BlockLfParams &P, cudaStream_t s);
@@ -232,6 +235,9 @@ cudaError_t launch_clipper_multi(const gf_footprint *foot_by_job, MultiRows R, g
 cudaError_t launch_bond2010_multi(const gf_bond2010_config &c, uint32_t *rng_all, int32_t NS, MultiRows R,
                                   const int64_t *slot_chunk_begin, int32_t nslots, int64_t nchunks,
                                   const int64_t *slot_rows, gf_table t, cudaStream_t s);
+cudaError_t launch_feh_multi(const gf_feh_config *fp, const gf_gaussfeh_config *gp, uint32_t *rng_all, int32_t NS,
+                             MultiRows R, const int64_t *slot_chunk_begin, int32_t nslots, int64_t nchunks,
+                             const int64_t *slot_rows, gf_table t, cudaStream_t s);
 cudaError_t launch_photoerrors_multi(const PerrTables &c, const uint64_t *seed_by_job, const int64_t *catalog_offset_by_job,
                                      MultiRows R, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
 

@@ -6,6 +6,8 @@
  *
  *   clipper_kernel     os_clipper::process (src/skygen/os_skygen.cpp:999-1044), analytic footprints
  *   fixedfeh_kernel    os_fixedFeH_kernel (src/modules/fixedFeH_gpu.cu.h:34-50)
+ *   feh_kernel<0>      os_FeH_kernel (src/modules/FeH_gpu.cu.h:43-87)
+ *   feh_kernel<1>      os_GaussianFeH_kernel (src/modules/GaussianFeH_gpu.cu.h:42-73)
  *   bond2010_kernel    os_Bond2010_kernel (src/modules/Bond2010_gpu.cu.h:81-218)
  *   photometry_kernel  os_photometry_kernel (src/modules/photometry_gpu.cu.h:87-174)
  *   photoerr_kernel    os_photometricErrors::process (photometricErrors_host.cpp:112-131)
@@ -246,6 +248,127 @@ cudaError_t launch_bond2010(const gf_bond2010_config &c, uint32_t *rng, int32_t 
     int64_t nchunks = n / 256 + (n % 256 ? 1 : 0);
     if (nchunks > NS) return cudaErrorInvalidValue;
     bond2010_kernel<<<(int)((nchunks + 127) / 128), 128, 0, s>>>(c, rng, NS, t, begin, end, nchunks);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+/* ---------------- FeH (Ivezic et al. 2008) and GaussianFeH ---------------- */
+
+/* os_FeH_kernel (FeH_gpu.cu.h:43-87) on rows [begin + 256 th, ...) with stream th */
+__device__ __forceinline__ void feh_chunk(const gf_feh_config &par, uint32_t *rng, int32_t NS, gf_table &t, int64_t begin,
+                                          int64_t end, int64_t th)
+{
+    const int64_t P = t.capacity;
+    gfr::Mwc r;
+    r.a = rng[th]; r.c = rng[NS + th]; r.x = rng[2 * NS + th]; r.used = 0;
+    int64_t rb = begin + 256 * th, re = begin + 256 * (th + 1);
+    if (re > end) re = end;
+    for (int64_t row = rb; row < re; row++) {
+        if (t.hidden[row]) continue;
+        const int cmp = t.comp[row];
+        if (((par.comp_thin | par.comp_thick) >> cmp) & 1u) {
+            /* the Gaussian to draw from */
+            const float p = r.uniform() * (par.A[0] + par.A[1]);
+            const int i = p < par.A[0] ? 0 : 1;
+            /* the star's place in the disk */
+            const float vx = t.XYZ[row] + par.T[0], vy = t.XYZ[P + row] + par.T[1], vz = t.XYZ[2 * P + row] + par.T[2];
+            const float wz = par.M[6] * vx + par.M[7] * vy + par.M[8] * vz;
+            /* Bond et al. A2; exp in single precision through the portable expf */
+            const float muD = par.muInf + par.DeltaMu * gfm::expf_(-fabsf(wz) / par.Hmu);
+            const float aZ = muD - 0.067f;
+            const float feh = r.gaussian(par.sigma[i]) + aZ + par.offs[i];
+            t.FeH[row] = feh;
+        } else if ((par.comp_halo >> cmp) & 1u) {
+            const float feh = par.offs[2] + r.gaussian(par.sigma[2]);
+            t.FeH[row] = feh;
+        }
+    }
+    rng[NS + th] = r.c;
+    rng[2 * NS + th] = r.x;
+}
+
+/* os_GaussianFeH_kernel (GaussianFeH_gpu.cu.h:42-73) on rows [begin + 256 th, ...) with stream th */
+__device__ __forceinline__ void gaussfeh_chunk(const gf_gaussfeh_config &par, uint32_t *rng, int32_t NS, gf_table &t,
+                                               int64_t begin, int64_t end, int64_t th)
+{
+    gfr::Mwc r;
+    r.a = rng[th]; r.c = rng[NS + th]; r.x = rng[2 * NS + th]; r.used = 0;
+    int64_t rb = begin + 256 * th, re = begin + 256 * (th + 1);
+    if (re > end) re = end;
+    for (int64_t row = rb; row < re; row++) {
+        if (t.hidden[row]) continue;
+        const int cmp = t.comp[row];
+        if (!((par.comp_mask >> cmp) & 1u)) continue;
+        int at = 0;
+        if (par.ncomp != 1) {
+            const float u = r.uniform();
+            while (par.pcum[at] < u) ++at;
+        }
+        t.FeH[row] = par.mean[at] + r.gaussian(par.sigma[at]);
+        t.FeH_comp[row] = at;
+    }
+    rng[NS + th] = r.c;
+    rng[2 * NS + th] = r.x;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(128) feh_kernel(const gf_feh_config fp, const gf_gaussfeh_config gp, uint32_t *rng,
+                                                  int32_t NS, gf_table t, int64_t begin, int64_t end, int64_t nchunks)
+{
+    const int64_t th = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (th >= nchunks) return;
+    if (KIND == 0) feh_chunk(fp, rng, NS, t, begin, end, th);
+    else gaussfeh_chunk(gp, rng, NS, t, begin, end, th);
+}
+
+/* the 256-row chunks of every request of a multi-request pass, each with its request's streams */
+template <int KIND>
+__global__ void __launch_bounds__(128) feh_multi_kernel(const gf_feh_config fp, const gf_gaussfeh_config gp,
+                                                        uint32_t *rng_all, int32_t NS, MultiRows R,
+                                                        const int64_t *slot_chunk_begin, int32_t nslots, int64_t nchunks,
+                                                        const int64_t *slot_rows, gf_table t)
+{
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nchunks) return;
+    int lo = 0, hi = nslots - 1;          /* last slot whose first chunk is <= c */
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (slot_chunk_begin[mid] <= c) lo = mid; else hi = mid - 1;
+    }
+    const int64_t b = R.slot_row_begin[lo];
+    uint32_t *rng = rng_all + (size_t)R.slot_job[lo] * 3 * NS;
+    if (KIND == 0) feh_chunk(fp, rng, NS, t, b, b + slot_rows[lo], c - slot_chunk_begin[lo]);
+    else gaussfeh_chunk(gp, rng, NS, t, b, b + slot_rows[lo], c - slot_chunk_begin[lo]);
+}
+
+cudaError_t launch_feh(const gf_feh_config *fp, const gf_gaussfeh_config *gp, uint32_t *rng, int32_t NS, gf_table t,
+                       int64_t begin, int64_t end, cudaStream_t s)
+{
+    if (end <= begin) return cudaSuccess;
+    const int64_t n = end - begin, nchunks = n / 256 + (n % 256 ? 1 : 0);
+    if (nchunks > NS) return cudaErrorInvalidValue;
+    gf_feh_config f = {};
+    gf_gaussfeh_config g = {};
+    if (fp) f = *fp;
+    if (gp) g = *gp;
+    if (fp) feh_kernel<0><<<(int)((nchunks + 127) / 128), 128, 0, s>>>(f, g, rng, NS, t, begin, end, nchunks);
+    else feh_kernel<1><<<(int)((nchunks + 127) / 128), 128, 0, s>>>(f, g, rng, NS, t, begin, end, nchunks);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_feh_multi(const gf_feh_config *fp, const gf_gaussfeh_config *gp, uint32_t *rng_all, int32_t NS,
+                             MultiRows R, const int64_t *slot_chunk_begin, int32_t nslots, int64_t nchunks,
+                             const int64_t *slot_rows, gf_table t, cudaStream_t s)
+{
+    if (nchunks <= 0) return cudaSuccess;
+    gf_feh_config f = {};
+    gf_gaussfeh_config g = {};
+    if (fp) f = *fp;
+    if (gp) g = *gp;
+    const unsigned blocks = (unsigned)((nchunks + 127) / 128);
+    if (fp) feh_multi_kernel<0><<<blocks, 128, 0, s>>>(f, g, rng_all, NS, R, slot_chunk_begin, nslots, nchunks, slot_rows, t);
+    else feh_multi_kernel<1><<<blocks, 128, 0, s>>>(f, g, rng_all, NS, R, slot_chunk_begin, nslots, nchunks, slot_rows, t);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -197,7 +197,7 @@ struct MultiWS {
     Grow<int32_t> projIdx, hidden, row_slot;
     Grow<float> projXY, DMc, absmag, XYZ, Am, AmInf;
     Grow<uint64_t> key, key_b;
-    Grow<uint32_t> idx_a, idx_b, slot_a, slot_b;
+    Grow<uint32_t> idx_a, idx_b, slot_a;
     Grow<char> temp;
     Grow<double2> pixsum, tot;              /* pixel-by-pixel integrate: per pixel, per request */
     Grow<const unsigned char *> plans;
@@ -282,9 +282,9 @@ namespace {
 /* bytes of one row of a table with nb bands, counting the columns in mask (GF_COL_*) */
 size_t row_bytes(int nb, uint32_t mask)
 {
-    const size_t w[17] = {16, 4, 8, 4, 4, 12, 4, 4, 4, 4, 4, 12, 4 * (size_t)nb, 4, 4 * (size_t)nb, 12, 16};
+    const size_t w[18] = {16, 4, 8, 4, 4, 12, 4, 4, 4, 4, 4, 12, 4 * (size_t)nb, 4, 4 * (size_t)nb, 12, 16, 4};
     size_t b = 0;
-    for (int i = 0; i < 17; i++)
+    for (int i = 0; i < 18; i++)
         if (mask & (1u << i)) b += w[i];
     return b;
 }
@@ -313,10 +313,11 @@ gf_table carve_table(char *p, int64_t cap, int nb, uint32_t mask)
     t.mags = (float *)take(GF_COL_MAGS, 4 * n * nb); t.photoflags = (int32_t *)take(GF_COL_PHOTOFLAGS, 4 * n);
     t.obsmags = (float *)take(GF_COL_OBSMAGS, 4 * n * nb); t.pm = (float *)take(GF_COL_PM, 12 * n);
     t.radec = (double *)take(GF_COL_RADEC, 16 * n);
+    t.FeH_comp = (int32_t *)take(GF_COL_FEHCOMP, 4 * n);
     return t;
 }
 
-size_t carved_bytes(int64_t cap, int nb, uint32_t mask) { return row_bytes(nb, mask) * (size_t)cap + 20 * 256; }
+size_t carved_bytes(int64_t cap, int nb, uint32_t mask) { return row_bytes(nb, mask) * (size_t)cap + 21 * 256; }
 
 /* rows [r0, r1) of the device table d into the host table h, on stream cs */
 gf_status copy_rows_async(const gf_table &d, int64_t r0, int64_t r1, gf_table &h, cudaStream_t cs)
@@ -334,6 +335,7 @@ gf_status copy_rows_async(const gf_table &d, int64_t r0, int64_t r1, gf_table &h
     GF_TRY(cp(h.hidden, d.hidden, 4, 1)); GF_TRY(cp(h.FeH, d.FeH, 4, 1)); GF_TRY(cp(h.vcyl, d.vcyl, 4, 3));
     GF_TRY(cp(h.mags, d.mags, 4, d.nbands)); GF_TRY(cp(h.photoflags, d.photoflags, 4, 1));
     GF_TRY(cp(h.obsmags, d.obsmags, 4, d.nbands)); GF_TRY(cp(h.pm, d.pm, 4, 3)); GF_TRY(cp(h.radec, d.radec, 8, 2));
+    GF_TRY(cp(h.FeH_comp, d.FeH_comp, 4, 1));
     return GF_OK;
 }
 
@@ -454,11 +456,16 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         NS = std::max(NS, ns);
         nbands = std::max(nbands, (int)J.nbands);
         if (!!J.feh != !!J0.feh || !!J.kin != !!J0.kin || !!J.v2pm != !!J0.v2pm || J.gal2other != J0.gal2other ||
-            !!J.phot != !!J0.phot || !!J.perr != !!J0.perr)
+            !!J.phot != !!J0.phot || !!J.perr != !!J0.perr || !!J.feh_ivezic != !!J0.feh_ivezic ||
+            !!J.feh_gauss != !!J0.feh_gauss)
             return fail(GF_E_INVALID, "all requests of a multi-request run need the same modules");
         if (!same_cfg(J.feh, J0.feh, sizeof(gf_fixedfeh_config)) || !same_cfg(J.kin, J0.kin, sizeof(gf_bond2010_config)) ||
-            !same_cfg(J.v2pm, J0.v2pm, sizeof(gf_vel2pm_config)))
-            return fail(GF_E_INVALID, "fixedFeH, Bond2010 and vel2pm configurations must agree across requests");
+            !same_cfg(J.v2pm, J0.v2pm, sizeof(gf_vel2pm_config)) ||
+            !same_cfg(J.feh_ivezic, J0.feh_ivezic, sizeof(gf_feh_config)) ||
+            !same_cfg(J.feh_gauss, J0.feh_gauss, sizeof(gf_gaussfeh_config)))
+            return fail(GF_E_INVALID, "the metallicity, Bond2010 and vel2pm configurations must agree across requests");
+        if (J.feh_gauss && (J.feh_gauss->ncomp < 1 || J.feh_gauss->ncomp >= GF_GAUSSFEH_MAXCOMP))
+            return fail(GF_E_INVALID, "GaussianFeH needs 1 <= ncomp < 10");
     }
     GF_TRY(gfa::ensure_multipliers(ctx));
     cudaStream_t st = ctx->stream;
@@ -881,7 +888,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
     auto &projIdx = ws.projIdx, &hidden = ws.hidden, &row_slot = ws.row_slot;
     auto &projXY = ws.projXY, &DMc = ws.DMc, &absmag = ws.absmag, &XYZ = ws.XYZ, &Am = ws.Am, &AmInf = ws.AmInf;
     auto &key = ws.key, &key_b = ws.key_b;
-    auto &idx_a = ws.idx_a, &idx_b = ws.idx_b, &slot_a = ws.slot_a, &slot_b = ws.slot_b;
+    auto &idx_a = ws.idx_a, &idx_b = ws.idx_b, &slot_a = ws.slot_a;
     auto &temp = ws.temp;
     std::vector<int64_t> catoff(njobs, 0);
     /* host delivery: copy stream, events and the page-locked ring */
@@ -1140,7 +1147,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
             GF_TRY(lb.need(2 * n)); GF_TRY(projIdx.need(n)); GF_TRY(hidden.need(n)); GF_TRY(projXY.need(2 * n));
             GF_TRY(DMc.need(n)); GF_TRY(absmag.need(n)); GF_TRY(XYZ.need(3 * n)); GF_TRY(Am.need(n)); GF_TRY(AmInf.need(n));
             GF_TRY(key.need(n)); GF_TRY(key_b.need(n)); GF_TRY(idx_a.need(n)); GF_TRY(idx_b.need(n));
-            GF_TRY(slot_a.need(n)); GF_TRY(slot_b.need(n));
+            GF_TRY(slot_a.need(n));
             size_t tb = 0;
             GF_CUDA(gfk::sort_temp_bytes_multi((int64_t)n, &tb));
             GF_TRY(temp.need(tb + 256));
@@ -1150,7 +1157,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
             PL.jobs = d_jobs; PL.job_slot = d_job_slot; PL.rec = rec.p; PL.n = nrec;
             PL.lb = lb.p; PL.projIdx = projIdx.p; PL.projXY = projXY.p; PL.DM = DMc.p; PL.absmag = absmag.p;
             PL.XYZ = XYZ.p; PL.Am = Am.p; PL.AmInf = AmInf.p; PL.hidden = hidden.p; PL.key = key.p; PL.key_b = key_b.p;
-            PL.idx_a = idx_a.p; PL.idx_b = idx_b.p; PL.slot_a = slot_a.p; PL.slot_b = slot_b.p; PL.slot_bits = slot_bits;
+            PL.idx_a = idx_a.p; PL.idx_b = idx_b.p; PL.slot_a = slot_a.p; PL.slot_bits = slot_bits;
             PL.temp = temp.p; PL.temp_bytes = temp.n;
             PL.seg_begin = d_seg; PL.vis_end = d_seg + nslots; PL.seg_end = d_seg + 2 * nslots;
             {
@@ -1224,6 +1231,15 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                     GF_CUDA(gfk::launch_clipper_multi(d_foot, MR, out, 0, total, st));
                 }
                 if (J0.feh) GF_TRY(gf_module_fixedfeh(ctx, J0.feh, &out, 0, total));
+                if (J0.feh_ivezic || J0.feh_gauss) {
+                    ProfScope ps(ctx, GF_PROF_FEH);
+                    if (J0.feh_ivezic)
+                        GF_CUDA(gfk::launch_feh_multi(J0.feh_ivezic, nullptr, d_rng, NS, MR, d_chunk_begin, nslots, nchunks,
+                                                      d_slot_rows, out, st));
+                    if (J0.feh_gauss)
+                        GF_CUDA(gfk::launch_feh_multi(nullptr, J0.feh_gauss, d_rng, NS, MR, d_chunk_begin, nslots, nchunks,
+                                                      d_slot_rows, out, st));
+                }
                 if (J0.kin) {
                     ProfScope ps(ctx, GF_PROF_BOND2010);
                     GF_CUDA(gfk::launch_bond2010_multi(*J0.kin, d_rng, NS, MR, d_chunk_begin, nslots, nchunks, d_slot_rows, out, st));

@@ -58,7 +58,8 @@ bool compatible(const gf_job &a, const gf_job &b)
     if (a.sky.nstars != 0.f || b.sky.nstars != 0.f || a.nstreams <= 0 || b.nstreams <= 0) return false;
     if (!!a.phot != !!b.phot || !!a.perr != !!b.perr) return false;
     if (!same_bytes(a.feh, b.feh, sizeof(gf_fixedfeh_config)) || !same_bytes(a.kin, b.kin, sizeof(gf_bond2010_config)) ||
-        !same_bytes(a.v2pm, b.v2pm, sizeof(gf_vel2pm_config)))
+        !same_bytes(a.v2pm, b.v2pm, sizeof(gf_vel2pm_config)) || !same_bytes(a.feh_ivezic, b.feh_ivezic, sizeof(gf_feh_config)) ||
+        !same_bytes(a.feh_gauss, b.feh_gauss, sizeof(gf_gaussfeh_config)))
         return false;
     /* same model kinds in component order */
     return model_kinds(a) == model_kinds(b);

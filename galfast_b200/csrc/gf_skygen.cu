@@ -1187,65 +1187,79 @@ cudaError_t launch_crawl_multi(const LaunchCrawlMulti &L, int draw, cudaStream_t
     return cudaGetLastError();
 }
 
-/* placement of the records of many requests; slotkey = output position of the record's request */
+/* The sort key of a record of a many-request pass: its request's output slot in
+ * the top sb bits, below them the IEEE bits 62..sb-1 of l (l >= 0, so the sign
+ * bit is 0 and the order of the bits is the order of l), all ones for hidden
+ * rows (after every visible row of the slot: l <= 360 never has all those bits
+ * set).  The sort uses the bits from GF_SORT_LOW_BIT up; records equal there --
+ * within about 2^-24 of l of each other -- are ordered by the tie pass on the
+ * full (l, b, DM, M, Am), star_comp's order (skyconfig_impl.h:34-68). */
+__device__ __forceinline__ uint64_t multi_key(uint32_t slot, int sb, uint64_t lkey)
+{
+    const uint64_t low = (lkey == ~0ull) ? (~0ull >> sb) : (lkey >> (sb - 1));
+    return ((uint64_t)slot << (64 - sb)) | low;
+}
+
+/* placement of the records of many requests, with their combined sort keys */
 __global__ void __launch_bounds__(256) place_multi_kernel(PlaceParams P, const CrawlJob *jobs, const int32_t *job_slot,
-                                                          uint32_t *slotkey)
+                                                          int sb)
 {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += (int64_t)gridDim.x * blockDim.x) {
         const StarRecord rec = P.rec[i];
         const int job = rec.stream >> 16;
         const CrawlJob &J = jobs[job];
         place_one(J.m, J.g, rec, i, P.n, P);
-        slotkey[i] = (uint32_t)job_slot[job];
+        P.key[i] = multi_key((uint32_t)job_slot[job], sb, P.key[i]);
     }
 }
 
-__global__ void gather_u32_kernel(const uint32_t *src, const uint32_t *idx, uint32_t *dst, int64_t n)
+/* the slot of every sorted record (the top sb bits of its key) */
+__global__ void key_slot_kernel(const uint64_t *key, int sb, uint32_t *slot, int64_t n)
 {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        dst[i] = src[idx[i]];
-}
-
-__global__ void gather_u64_kernel(const uint64_t *src, const uint32_t *idx, uint64_t *dst, int64_t n)
-{
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        dst[i] = src[idx[i]];
+        slot[i] = (uint32_t)(key[i] >> (64 - sb));
 }
 
 /* per output slot: first sorted position, end of its visible rows (hidden rows
- * carry the largest key and sort last within the slot) and end of the slot */
-__global__ void segment_bounds_kernel(const uint32_t *slot, const uint64_t *key, int64_t n, int64_t *seg_begin,
+ * carry all ones below the slot bits and sort last within the slot) and end of
+ * the slot */
+__global__ void segment_bounds_kernel(const uint32_t *slot, const uint64_t *key, int sb, int64_t n, int64_t *seg_begin,
                                       int64_t *vis_end, int64_t *seg_end)
 {
+    const uint64_t lmask = ~0ull >> sb;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t sl = slot[i];
         const bool first = (i == 0) || slot[i - 1] != sl;
         const bool last = (i + 1 == n) || slot[i + 1] != sl;
         if (first) seg_begin[sl] = i;
         if (last) seg_end[sl] = i + 1;
-        const bool hid = key[i] == ~0ull;
-        if (hid && (first || key[i - 1] != ~0ull)) vis_end[sl] = i;
+        const bool hid = (key[i] & lmask) == lmask;
+        if (hid && (first || (key[i - 1] & lmask) != lmask)) vis_end[sl] = i;
         if (!hid && last) vis_end[sl] = i + 1;
     }
 }
 
-/* runs of equal (slot, l) ordered by (b, DM, M, Am) (star_comp, skyconfig_impl.h:58-67) */
-__global__ void tie_multi_kernel(const uint64_t *key, const uint32_t *slot, uint32_t *idx, int64_t n, const double *lb,
+/* Runs of visible records equal in the sorted key bits (one slot, l within the
+ * key's resolution) ordered by (l, b, DM, M, Am) (star_comp, skyconfig_impl.h:34-68). */
+__global__ void tie_multi_kernel(const uint64_t *key, int sb, int low_bit, uint32_t *idx, int64_t n, const double *lb,
                                  const float *DM, const float *absmag, const float *Am, int64_t pitch)
 {
+    const uint64_t lmask = ~0ull >> sb;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        if (key[i] == ~0ull) continue;
-        if (i + 1 >= n || key[i] != key[i + 1] || slot[i] != slot[i + 1]) continue;
-        if (i > 0 && key[i - 1] == key[i] && slot[i - 1] == slot[i]) continue;
+        if ((key[i] & lmask) == lmask) continue;
+        const uint64_t k = key[i] >> low_bit;
+        if (i + 1 >= n || (key[i + 1] >> low_bit) != k) continue;
+        if (i > 0 && (key[i - 1] >> low_bit) == k) continue;     /* not a run start */
         int64_t e = i + 1;
-        while (e + 1 < n && key[e + 1] == key[i] && slot[e + 1] == slot[i]) e++;
+        while (e + 1 < n && (key[e + 1] >> low_bit) == k) e++;
         for (int64_t q = i + 1; q <= e; q++) {
             uint32_t cur = idx[q];
             int64_t r = q - 1;
             while (r >= i) {
                 uint32_t o = idx[r];
                 bool less;
-                if (lb[pitch + cur] != lb[pitch + o]) less = lb[pitch + cur] < lb[pitch + o];
+                if (lb[cur] != lb[o]) less = lb[cur] < lb[o];
+                else if (lb[pitch + cur] != lb[pitch + o]) less = lb[pitch + cur] < lb[pitch + o];
                 else if (DM[cur] != DM[o]) less = DM[cur] < DM[o];
                 else if (absmag[cur] != absmag[o]) less = absmag[cur] < absmag[o];
                 else less = Am[cur] < Am[o];
@@ -1287,28 +1301,34 @@ __global__ void __launch_bounds__(256) gather_multi_kernel(GatherParams G, const
     }
 }
 
+/* lowest key bit the multi-request sort looks at: keeps the slot and l to 24
+ * mantissa bits (2^-24 relative); the tie pass orders what the sort leaves equal */
+static int sort_low_bit(int sb)
+{
+    const int b = 53 - sb - 24;
+    return b > 0 ? b : 0;
+}
+
 cudaError_t launch_place_sort_multi(const LaunchPlaceMulti &L, cudaStream_t s)
 {
     if (L.n <= 0) return cudaSuccess;
     const int blocks = (int)std::min<int64_t>((L.n + 255) / 256, (int64_t)sm_count() * 16);
+    const int sb = L.slot_bits;
     PlaceParams P;
     memset(&P, 0, sizeof(P));
     P.rec = L.rec; P.n = L.n;
     P.lb = L.lb; P.projIdx = L.projIdx; P.projXY = L.projXY; P.DM = L.DM; P.absmag = L.absmag;
     P.XYZ = L.XYZ; P.Am = L.Am; P.AmInf = L.AmInf; P.hidden = L.hidden; P.key = L.key;
-    place_multi_kernel<<<blocks, 256, 0, s>>>(P, L.jobs, L.job_slot, L.slot_a);
-    iota_kernel<<<blocks, 256, 0, s>>>(L.idx_a, L.n);
-    /* by l, then (stable) by slot: the records of each request in star_comp order */
+    place_multi_kernel<<<blocks, 256, 0, s>>>(P, L.jobs, L.job_slot, sb);
+    iota_kernel<<<blocks, 256, 0, s>>>(L.idx_b, L.n);
+    /* one radix sort by (slot, l): the records of each request in star_comp order up to ties */
     size_t tb = L.temp_bytes;
-    cudaError_t e = cub::DeviceRadixSort::SortPairs(L.temp, tb, L.key, L.key_b, L.idx_a, L.idx_b, (int)L.n, 0, 64, s);
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(L.temp, tb, L.key, L.key_b, L.idx_b, L.idx_a, (int)L.n,
+                                                    sort_low_bit(sb), 64, s);
     if (e != cudaSuccess) return e;
-    gather_u32_kernel<<<blocks, 256, 0, s>>>(L.slot_a, L.idx_b, L.slot_b, L.n);
-    tb = L.temp_bytes;
-    e = cub::DeviceRadixSort::SortPairs(L.temp, tb, L.slot_b, L.slot_a, L.idx_b, L.idx_a, (int)L.n, 0, L.slot_bits, s);
-    if (e != cudaSuccess) return e;
-    gather_u64_kernel<<<blocks, 256, 0, s>>>(L.key, L.idx_a, L.key_b, L.n);
-    segment_bounds_kernel<<<blocks, 256, 0, s>>>(L.slot_a, L.key_b, L.n, L.seg_begin, L.vis_end, L.seg_end);
-    count_launches(6);
+    key_slot_kernel<<<blocks, 256, 0, s>>>(L.key_b, sb, L.slot_a, L.n);
+    segment_bounds_kernel<<<blocks, 256, 0, s>>>(L.slot_a, L.key_b, sb, L.n, L.seg_begin, L.vis_end, L.seg_end);
+    count_launches(4);
     return cudaGetLastError();
 }
 
@@ -1317,7 +1337,8 @@ cudaError_t launch_tie_gather_multi(const LaunchPlaceMulti &L, const int64_t *ro
 {
     if (L.n <= 0) return cudaSuccess;
     const int blocks = (int)std::min<int64_t>((L.n + 255) / 256, (int64_t)sm_count() * 16);
-    tie_multi_kernel<<<blocks, 256, 0, s>>>(L.key_b, L.slot_a, L.idx_a, L.n, L.lb, L.DM, L.absmag, L.Am, L.n);
+    tie_multi_kernel<<<blocks, 256, 0, s>>>(L.key_b, L.slot_bits, sort_low_bit(L.slot_bits), L.idx_a, L.n, L.lb, L.DM,
+                                            L.absmag, L.Am, L.n);
     GatherParams G;
     G.idx = L.idx_a; G.n = L.n; G.src_pitch = L.n;
     G.lb = L.lb; G.projIdx = L.projIdx; G.projXY = L.projXY; G.DM = L.DM; G.absmag = L.absmag;
@@ -1333,9 +1354,8 @@ cudaError_t sort_temp_bytes_multi(int64_t n, size_t *bytes)
     cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, a, (const uint64_t *)nullptr, (uint64_t *)nullptr,
                                                     (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)n);
     if (e != cudaSuccess) return e;
-    e = cub::DeviceRadixSort::SortPairs(nullptr, b, (const uint32_t *)nullptr, (uint32_t *)nullptr,
-                                        (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)n);
-    *bytes = a > b ? a : b;
+    *bytes = a;
+    (void)b;
     return e;
 }
 

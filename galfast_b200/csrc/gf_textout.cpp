@@ -271,6 +271,8 @@ std::vector<ColumnDef> output_columns(const gf_textout_config &c)
     }
     ranked.push_back({"comp", Field{I32, GF_OFF(comp), 1, 0, 3, false, true}});
     if (c.feh) ranked.push_back({"FeH", Field{F32, GF_OFF(FeH), 1, 3, 6, true, false}});
+    /* provided as "FeH_comp{type=int; fmt=%3d;}" (GaussianFeH_host.cpp:46-47) */
+    if (c.feh_comp) ranked.push_back({"FeH_comp{type=int;fmt=%3d;}", Field{I32, GF_OFF(FeH_comp), 1, 0, 3, false, false}});
     if (c.vcyl) ranked.push_back({"vcyl[3]", Field{F32, GF_OFF(vcyl), 3, 1, 7, true, false}});
     if (c.pm_coordsys == 0) ranked.push_back({"pmlb[3]", Field{F32, GF_OFF(pm), 3, 2, 8, true, false}});
     if (c.pm_coordsys == 1) ranked.push_back({"pmradec[3]", Field{F32, GF_OFF(pm), 3, 2, 8, true, false}});

@@ -82,6 +82,44 @@ def galplane_frame(Rg=8000.0, z0=25.0):
     return M, T
 
 
+def feh_config(Rg=8000.0, z0=25.0, thin=1, thick=2, halo=4):
+    """os_FeH with the reference's default parameters (FeH_host.cpp:88-108): disk
+    Gaussians A = (0.63, 0.37) (normalised), sigma 0.20, offsets 0 and 0.14, median
+    -0.82 + 0.55 exp(-|Z| / 500 pc); halo N(-1.46, 0.30); galplane frame."""
+    c = A.FehConfig()
+    a0, a1 = 0.63, 0.37
+    s_ = a0 + a1
+    c.A[0], c.A[1] = a0 / s_, a1 / s_
+    c.sigma[0], c.sigma[1], c.sigma[2] = 0.20, 0.20, 0.30
+    c.offs[0], c.offs[1], c.offs[2] = 0.00, 0.14, -1.46
+    c.Hmu, c.muInf, c.DeltaMu = 500.0, -0.82, 0.55
+    c.comp_thin, c.comp_thick, c.comp_halo = thin, thick, halo
+    M, T = galplane_frame(Rg, z0)
+    for i in range(9):
+        c.M[i] = float(M[i])
+    for i in range(3):
+        c.T[i] = float(T[i])
+    return c
+
+
+def gaussfeh_config(mean=(-0.6, -1.5), sigma=(0.2, 0.3), wt=(3.0, 1.0), comp_mask=0xFFFFFFFF):
+    """os_GaussianFeH (GaussianFeH_host.cpp:78-104): a mixture of Gaussians with
+    cumulative weights normalised to 1, in float as the reference stores them."""
+    c = A.GaussFehConfig()
+    c.ncomp = len(mean)
+    acc = 0.0
+    pc = []
+    for w_ in wt:
+        acc += w_
+        pc.append(np.float32(acc))
+    for i in range(c.ncomp):
+        c.mean[i] = mean[i]
+        c.sigma[i] = sigma[i]
+        c.pcum[i] = float(np.float32(pc[i]) / np.float32(pc[-1]))
+    c.comp_mask = comp_mask
+    return c
+
+
 def bond2010_config(disk_sigma=(35.0, 25.0, 20.0), halo_sigma=(140.0, 100.0, 95.0), Rg=8000.0, z0=25.0):
     """Bond et al. (2010) kinematics with constant dispersions (Bond2010_host.cpp:142-227 layout)."""
     cfg = A.Bond2010Config()
@@ -143,6 +181,8 @@ class Workload:
     perr: Optional[A.PhotoerrConfig] = None
     v2pm: Optional[A.Vel2pmConfig] = None
     gal2other: int = 0
+    feh_ivezic: Optional[A.FehConfig] = None
+    feh_gauss: Optional[A.GaussFehConfig] = None
     keep: list = field(default_factory=list)   # keeps ctypes buffers alive
 
     def pixel_array(self):
@@ -164,7 +204,7 @@ class Workload:
         j.nstreams = self.nstreams
         j.capacity = self.capacity
         j.nbands = self.nbands
-        for name in ("foot", "feh", "kin", "phot", "perr", "v2pm"):
+        for name in ("foot", "feh", "kin", "phot", "perr", "v2pm", "feh_ivezic", "feh_gauss"):
             v = getattr(self, name)
             if v is not None:
                 setattr(j, name, C.pointer(v))

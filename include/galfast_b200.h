@@ -170,6 +170,7 @@ typedef struct gf_table {
     float   *obsmags;          /* [nbands] magnitudes with photometric errors */
     float   *pm;               /* [3] mu_l/mu_ra, mu_b/mu_dec (mas/yr), v_r (km/s) */
     double  *radec;            /* [2] (degrees) */
+    int32_t *FeH_comp;         /* Gaussian of the multi-Gaussian metallicity draw (GaussianFeH) */
 } gf_table;
 
 /* ------------------------------------------------------------------ */
@@ -212,6 +213,25 @@ typedef struct gf_photoerr_config {        /* os_photometricErrors: sigma(m) per
     const double *sigma;                   /* [nbands][nknots] */
     uint64_t seed;                         /* key of the counter-based Gaussian draws */
 } gf_photoerr_config;
+
+typedef struct gf_feh_config {             /* os_FeH_data, src/modules/FeH_gpu.cu.h:26-36 (Ivezic et al. 2008) */
+    float A[2];                            /* disk Gaussian amplitudes (normalised to sum 1, FeH_host.cpp:100-102) */
+    float sigma[3];                        /* disk 1, disk 2, halo widths */
+    float offs[3];                         /* disk 1, disk 2 offsets; halo mean */
+    float Hmu, muInf, DeltaMu;             /* disk median: muInf + DeltaMu exp(-|Z| / Hmu) */
+    uint32_t comp_thin, comp_thick, comp_halo;   /* component bit masks */
+    float M[9];                            /* galactic -> model frame rotation (row major) */
+    float T[3];
+} gf_feh_config;
+
+#define GF_GAUSSFEH_MAXCOMP 10
+typedef struct gf_gaussfeh_config {        /* os_GaussianFeH_data, src/modules/GaussianFeH_gpu.cu.h:26-34 */
+    int32_t ncomp;                         /* 1 .. GF_GAUSSFEH_MAXCOMP - 1 */
+    float mean[GF_GAUSSFEH_MAXCOMP];
+    float sigma[GF_GAUSSFEH_MAXCOMP];
+    float pcum[GF_GAUSSFEH_MAXCOMP];       /* cumulative weights, pcum[ncomp - 1] = 1 */
+    uint32_t comp_mask;                    /* components it applies to */
+} gf_gaussfeh_config;
 
 typedef struct gf_vel2pm_config {          /* os_vel2pm_data, vel2pm_gpu.cu.h:26-34 */
     int32_t coordsys;                      /* 0 = GAL (pmlb), 1 = EQU (pmradec) */
@@ -333,6 +353,12 @@ gf_status gf_table_download_rows(gf_ctx *ctx, const gf_table *dev, int64_t begin
 gf_status gf_module_clipper(gf_ctx *ctx, const gf_footprint *foot, const gf_lambert proj[2],
                             gf_table *t, int64_t begin, int64_t end);
 gf_status gf_module_fixedfeh(gf_ctx *ctx, const gf_fixedfeh_config *cfg, gf_table *t, int64_t begin, int64_t end);
+/* os_FeH (FeH_host.cpp:60-78, kernel FeH_gpu.cu.h:43-87) and os_GaussianFeH
+ * (GaussianFeH_host.cpp:56-76, kernel GaussianFeH_gpu.cu.h:42-73): metallicities
+ * drawn from the context's streams, 256 rows per stream as the reference's
+ * kernels take them (row r of [begin, end) uses stream (r - begin) / 256). */
+gf_status gf_module_feh(gf_ctx *ctx, const gf_feh_config *cfg, gf_table *t, int64_t begin, int64_t end);
+gf_status gf_module_gaussfeh(gf_ctx *ctx, const gf_gaussfeh_config *cfg, gf_table *t, int64_t begin, int64_t end);
 gf_status gf_module_bond2010(gf_ctx *ctx, const gf_bond2010_config *cfg, gf_table *t, int64_t begin, int64_t end);
 /* Photometry: upload the colour grids once (os_photometry::construct), then process batches. */
 gf_status gf_photometry_create(gf_ctx *ctx, const gf_photometry_config *cfg, gf_photometry **out);
@@ -368,6 +394,8 @@ typedef struct gf_job {
     const gf_photoerr_config *perr;
     const gf_vel2pm_config *v2pm;
     int32_t gal2other;                         /* 0 = absent, 1 = equatorial (radec) */
+    const gf_feh_config *feh_ivezic;           /* os_FeH (after fixedFeH), NULL = absent */
+    const gf_gaussfeh_config *feh_gauss;       /* os_GaussianFeH (after os_FeH), NULL = absent */
 } gf_job;
 
 #define GF_MAX_MODELS 32
@@ -469,8 +497,8 @@ enum {
     GF_COL_ABSMAG = 1u << 4, GF_COL_XYZ = 1u << 5, GF_COL_COMP = 1u << 6, GF_COL_AM = 1u << 7,
     GF_COL_AMINF = 1u << 8, GF_COL_HIDDEN = 1u << 9, GF_COL_FEH = 1u << 10, GF_COL_VCYL = 1u << 11,
     GF_COL_MAGS = 1u << 12, GF_COL_PHOTOFLAGS = 1u << 13, GF_COL_OBSMAGS = 1u << 14, GF_COL_PM = 1u << 15,
-    GF_COL_RADEC = 1u << 16,
-    GF_COL_ALL = (1u << 17) - 1,
+    GF_COL_RADEC = 1u << 16, GF_COL_FEHCOMP = 1u << 17,
+    GF_COL_ALL = (1u << 18) - 1,
     /* the output catalog of the full-sky form: ra, dec, DM, Mr, true and observed
      * magnitudes, vR/vPhi/vZ, proper motions (and radial velocity) */
     GF_COL_CATALOG = GF_COL_RADEC | GF_COL_DM | GF_COL_ABSMAG | GF_COL_MAGS | GF_COL_OBSMAGS | GF_COL_VCYL | GF_COL_PM
@@ -556,6 +584,7 @@ typedef struct gf_textout_config {
     const char *absband;             /* its column name (NULL: "abs" + band) */
     int32_t radec;                   /* gal2other equatorial coordinates present */
     int32_t feh;                     /* FeH present */
+    int32_t feh_comp;                /* FeH_comp present (GaussianFeH) */
     int32_t vcyl;                    /* Bond2010 velocities present */
     int32_t pm_coordsys;             /* vel2pm: -1 absent, 0 pmlb, 1 pmradec */
     int32_t photoerrors;             /* observed magnitudes present */

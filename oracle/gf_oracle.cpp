@@ -1532,6 +1532,67 @@ int or_module_bond2010(const gf_bond2010_config *par, uint32_t *rng_state, int32
     return 0;
 }
 
+/* os_FeH_kernel (FeH_gpu.cu.h:43-87) and os_GaussianFeH_kernel
+ * (GaussianFeH_gpu.cu.h:42-73): thread t owns rows [begin + 256 t, ...) and
+ * stream t.  exp(-|Z|/Hmu) is evaluated in single precision (the GPU build's
+ * float overload) with this flavour's expf. */
+int or_module_feh(const gf_feh_config *par, uint32_t *rng_state, int32_t nstreams, gf_table *t, int64_t begin, int64_t end)
+{
+    const int64_t P = t->capacity;
+    RngState rs = {rng_state, nstreams};
+    const int64_t n = end - begin, nth = n / 256 + (n % 256 ? 1 : 0);
+    if (nth > nstreams) { g_err = "FeH: more than 256*nstreams rows"; return -1; }
+    parallel_for((int)nth, [&](int th) {
+        Rng rng = rs.load(th);
+        const int64_t rb = begin + 256 * (int64_t)th, re = std::min(begin + 256 * ((int64_t)th + 1), end);
+        for (int64_t row = rb; row < re; row++) {
+            if (t->hidden[row]) continue;
+            const int cmp = t->comp[row];
+            if (((par->comp_thin | par->comp_thick) >> cmp) & 1u) {
+                float p = rng.uniform() * (par->A[0] + par->A[1]);
+                int i = p < par->A[0] ? 0 : 1;
+                float vx = t->XYZ[row] + par->T[0], vy = t->XYZ[P + row] + par->T[1], vz = t->XYZ[2 * P + row] + par->T[2];
+                float z = par->M[6] * vx + par->M[7] * vy + par->M[8] * vz;
+                float muD = par->muInf + par->DeltaMu * OR_EXPF(-fabsf(z) / par->Hmu);
+                float aZ = muD - 0.067f;
+                float feh = rng.gaussian(par->sigma[i]) + aZ + par->offs[i];
+                t->FeH[row] = feh;
+            } else if ((par->comp_halo >> cmp) & 1u) {
+                float feh = par->offs[2] + rng.gaussian(par->sigma[2]);
+                t->FeH[row] = feh;
+            }
+        }
+        rs.store(th, rng);
+    }, 4);
+    return 0;
+}
+
+int or_module_gaussfeh(const gf_gaussfeh_config *par, uint32_t *rng_state, int32_t nstreams, gf_table *t, int64_t begin,
+                       int64_t end)
+{
+    RngState rs = {rng_state, nstreams};
+    const int64_t n = end - begin, nth = n / 256 + (n % 256 ? 1 : 0);
+    if (nth > nstreams) { g_err = "GaussianFeH: more than 256*nstreams rows"; return -1; }
+    parallel_for((int)nth, [&](int th) {
+        Rng rng = rs.load(th);
+        const int64_t rb = begin + 256 * (int64_t)th, re = std::min(begin + 256 * ((int64_t)th + 1), end);
+        for (int64_t row = rb; row < re; row++) {
+            if (t->hidden[row]) continue;
+            int cmp = t->comp[row];
+            if (!((par->comp_mask >> cmp) & 1u)) continue;
+            int at = 0;
+            if (par->ncomp != 1) {
+                float u = rng.uniform();
+                while (par->pcum[at] < u) ++at;
+            }
+            t->FeH[row] = par->mean[at] + rng.gaussian(par->sigma[at]);
+            t->FeH_comp[row] = at;
+        }
+        rs.store(th, rng);
+    }, 4);
+    return 0;
+}
+
 /* os_photometry_kernel (photometry_gpu.cu.h:87-174) for single stars (nabsmag = 1) */
 int or_module_photometry(const gf_photometry_config *lt, gf_table *t, int64_t begin, int64_t end)
 {

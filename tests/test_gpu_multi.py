@@ -200,3 +200,25 @@ def test_request_that_fills_a_batch_runs_alone(lib):
     assert stats[0].generated[0] < 2000 <= stats[0].generated[2]
     assert len(got[0][2]) >= 2 and len(got[0][0]) == 1
     ctx.close()
+
+
+def test_metallicity_modules_in_the_batched_passes(lib):
+    """os_FeH and os_GaussianFeH over the rows of many requests, each request's
+    256-row chunks drawing from its own streams: rows equal the standalone run's."""
+    ws = requests(lib, n=4)
+    for w in ws:
+        w.feh_ivezic = W.feh_config()
+        w.feh_gauss = W.gaussfeh_config(comp_mask=0b100)
+    ctx = G.Context(0)
+    got = {}
+    G.run_catalog_multi(ctx, ws, sink=lambda j, m, rows: got.setdefault(j, {}).setdefault(m, []).append(rows))
+    for j, w in enumerate(ws):
+        ref, st = catalog_alone(ctx, w)
+        for m in ref:
+            b = {k: np.concatenate([p[k] for p in got[j][m]], axis=-1) for k in got[j][m][0]}
+            for c in ref[m]:
+                x, y = ref[m][c], b[c]
+                if c in ("mags", "obsmags"):
+                    y = y[: x.shape[0]]
+                np.testing.assert_array_equal(x, y, err_msg="%s request %d model %d" % (c, j, m))
+    ctx.close()

@@ -222,3 +222,22 @@ def test_config1_catalog(ctx, lib, multipliers):
     for (gm, go, g), (om, oo, o) in zip(gb, ob):
         assert_same(g, o, SKY_COLS)
         assert_same(g, o, MODULE_COLS, exact=False)
+
+
+def test_metallicity_modules_parity(ctx, lib, multipliers):
+    """os_FeH (Ivezic et al. 2008) and os_GaussianFeH (halo only, two Gaussians)
+    draw from the shared streams between the clipper and Bond2010; a 4000-row
+    batch capacity makes the streams carry over between batches."""
+    w = small_patch(lib, capacity=4000)
+    w.feh = None
+    w.feh_ivezic = W.feh_config()
+    w.feh_gauss = W.gaussfeh_config(comp_mask=0b100)
+    gs, os_, gb, ob = run_both(ctx, w, multipliers)
+    assert len(gb) == len(ob) > 3
+    nonzero = 0
+    for (gm, go, g), (om, oo, o) in zip(gb, ob):
+        assert (gm, go) == (om, oo)
+        assert_same(g, o, SKY_COLS)
+        assert_same(g, o, MODULE_COLS + ["FeH_comp"], exact=False)
+        nonzero += int((g["FeH_comp"] == 1).sum())
+    assert nonzero > 0

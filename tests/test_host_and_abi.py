@@ -36,10 +36,42 @@ def test_library_exports_every_declared_function(lib):
         assert n in exported, n
 
 
-def test_struct_layouts():
+def test_struct_layouts(tmp_path):
+    """Every ctypes mirror has the size and field offsets of its struct in
+    include/galfast_b200.h (a C program compiled against the header prints them)."""
+    import shutil
+    import subprocess
     assert C.sizeof(A.PencilBeam) == 48
     assert C.sizeof(A.Lambert) == 32
     assert C.sizeof(A.Bond2010Config) == 4 * (4 + 3 * 45 + 12)
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    exe = str(tmp_path / "abi_layout")
+    here = os.path.dirname(os.path.abspath(__file__))
+    subprocess.run([cc, "-std=c99", "-I", os.path.join(ROOT, "include"), "-o", exe,
+                    os.path.join(here, "cpp", "abi_layout.c")], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout
+    mirror = {"gf_pencil_beam": A.PencilBeam, "gf_lambert": A.Lambert, "gf_skygen_config": A.SkygenConfig,
+              "gf_model_config": A.ModelConfig, "gf_extinction": A.Extinction, "gf_footprint": A.Footprint,
+              "gf_table": A.Table, "gf_fixedfeh_config": A.FixedFeHConfig, "gf_vmoments": A.VMoments,
+              "gf_bond2010_config": A.Bond2010Config, "gf_feh_config": A.FehConfig, "gf_gaussfeh_config": A.GaussFehConfig,
+              "gf_photometry_config": A.PhotometryConfig, "gf_photoerr_config": A.PhotoerrConfig,
+              "gf_vel2pm_config": A.Vel2pmConfig, "gf_skygen_model_info": A.ModelInfo, "gf_job": G.Job,
+              "gf_catalog_stats": G.CatalogStats, "gf_precision_report": A.PrecisionReport,
+              "gf_textout_config": G.TextoutConfig, "gf_textout_set": G.TextoutSet}
+    checked = 0
+    for line in out.split("\n"):
+        if not line.strip():
+            continue
+        name, field, value = line.split()
+        T = mirror[name]
+        if field == "-":
+            assert C.sizeof(T) == int(value), (name, C.sizeof(T), value)
+        else:
+            assert getattr(T, field).offset == int(value), (name, field, getattr(T, field).offset, value)
+        checked += 1
+    assert checked > 60
 
 
 def test_safeprime_multipliers_are_safe(multipliers):
