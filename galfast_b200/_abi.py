@@ -4,6 +4,8 @@ import ctypes as C
 GF_OK = 0
 GF_MODEL_EXP_DISK = 1
 GF_MODEL_POWER_LAW_ELLIPSOID = 2
+GF_MODEL_BROKEN_POWER_LAW = 3
+GF_MODEL_LCBULGE = 4
 GF_FRAME_GALPLANE = 0
 GF_FRAME_EXPLICIT = 1
 GF_EXT_NONE = 0
@@ -44,7 +46,8 @@ class ModelConfig(C.Structure):
                 ("frame", C.c_int32), ("Rg", C.c_double), ("z0", C.c_double),
                 ("T", C.c_double * 3), ("M", C.c_double * 9),
                 ("lf_l", C.c_double), ("lf_b", C.c_double), ("lf_D", C.c_double),
-                ("lf_M", C.POINTER(C.c_double)), ("lf_phi", C.POINTER(C.c_double)), ("lf_n", C.c_int32)]
+                ("lf_M", C.POINTER(C.c_double)), ("lf_phi", C.POINTER(C.c_double)), ("lf_n", C.c_int32),
+                ("nbreaks", C.c_int32), ("n_brk", C.c_double * 10), ("rbreak", C.c_double * 9)]
 
 
 class Extinction(C.Structure):

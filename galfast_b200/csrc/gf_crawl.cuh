@@ -152,12 +152,21 @@ __device__ __forceinline__ float model_rho(const SkyModel &m, float x, float y, 
         if (m.r_cut2 != 0.f && r2 + wz * wz > m.r_cut2) return 0.f;
         float r = sqrtf(r2);
         return m.f * gfm::expf_(-r / m.l - fabsf(wz) / m.h);
+    } else if (m.type == GF_MODEL_LCBULGE) {
+        /* LCBulge::rho (model_LCBulge.h:79-92): no density factor (the LF carries f) */
+        const float t = gfm::powf_(gfm::powf_(wx, m.n) + gfm::powf_(wy / m.ba, m.n) + gfm::powf_(wz / m.ca, m.n),
+                                   (float)(1. / m.n));
+        return gfm::expf_(-t / m.l);
     } else {
+        /* powerLawEllipsoid::rho (model_powerLawEllipsoid.h:60-92) and brokenPowerLaw::rho
+         * (model_brokenPowerLaw.h:55-82): f fArr[k] rSq^(nArr[k] / 2) beyond k breaks */
         float DSq = wx * wx + wy * wy + wz * wz;
         if (m.rmaxSq != 0.f && (DSq < m.rminSq || DSq >= m.rmaxSq)) return 0.f;
         float ty = wy / m.ba, tz = wz / m.ca;
         float rSq = wx * wx + ty * ty + tz * tz;
-        return m.f * gfm::powf_(rSq, 0.5f * m.n);
+        int k = 0;
+        while (k != m.nbreaks && rSq > m.rbreakSq[k]) k++;
+        return m.f * m.fArr[k] * gfm::powf_(rSq, 0.5f * m.nArr[k]);
     }
 }
 

@@ -132,11 +132,18 @@ float rho_host(const SkyModel &m, float x, float y, float z)
         if (m.r_cut2 != 0.f && r2 + wz * wz > m.r_cut2) return 0.f;
         return m.f * gfm::expf_(-sqrtf(r2) / m.l - fabsf(wz) / m.h);
     }
+    if (m.type == GF_MODEL_LCBULGE) {
+        const float t = gfm::powf_(gfm::powf_(wx, m.n) + gfm::powf_(wy / m.ba, m.n) + gfm::powf_(wz / m.ca, m.n),
+                                   (float)(1. / m.n));
+        return gfm::expf_(-t / m.l);
+    }
     float DSq = wx * wx + wy * wy + wz * wz;
     if (m.rmaxSq != 0.f && (DSq < m.rminSq || DSq >= m.rmaxSq)) return 0.f;
     float ty = wy / m.ba, tz = wz / m.ca;
     float rSq = wx * wx + ty * ty + tz * tz;
-    return m.f * gfm::powf_(rSq, 0.5f * m.n);
+    int k = 0;
+    while (k != m.nbreaks && rSq > m.rbreakSq[k]) k++;
+    return m.f * m.fArr[k] * gfm::powf_(rSq, 0.5f * m.nArr[k]);
 }
 
 }  // namespace
@@ -166,7 +173,7 @@ bool setup_models(const gf_skygen_config &cfg, int npixels, const gf_model_confi
         HostModel hm;
         SkyModel &m = hm.m;
         m = base;
-        if (c.type != GF_MODEL_EXP_DISK && c.type != GF_MODEL_POWER_LAW_ELLIPSOID) { err = "unknown model type"; return false; }
+        if (c.type < GF_MODEL_EXP_DISK || c.type > GF_MODEL_LCBULGE) { err = "unknown model type"; return false; }
         if (c.comp < 0 || c.comp > 31) { err = "component id must be in [0, 31]"; return false; }
         m.type = c.type;
         m.comp = c.comp;
@@ -192,6 +199,28 @@ bool setup_models(const gf_skygen_config &cfg, int npixels, const gf_model_confi
             m.n = (float)c.n;
             m.ba = (float)c.ba;
             m.ca = (float)c.ca;
+            m.nbreaks = 0;
+            m.nArr[0] = m.n;
+            m.fArr[0] = 1.f;
+            if (c.type == GF_MODEL_LCBULGE) {
+                if (!(c.l > 0) || !(c.n != 0)) { err = "LC bulge needs l > 0 and n != 0"; return false; }
+                m.l = (float)c.l;
+            }
+            if (c.type == GF_MODEL_BROKEN_POWER_LAW) {
+                /* brokenPowerLaw::load (model_brokenPowerLaw.cpp:31-62): indices, squared break
+                 * radii, and the piece-wise factors that keep the profile continuous */
+                if (c.nbreaks < 0 || c.nbreaks > 9) { err = "a broken power law has 0 to 9 breaks"; return false; }
+                m.nbreaks = c.nbreaks;
+                for (int k = 0; k <= c.nbreaks; k++) m.nArr[k] = (float)c.n_brk[k];
+                for (int k = 0; k < c.nbreaks; k++) {
+                    const float rb = (float)c.rbreak[k];
+                    m.rbreakSq[k] = rb * rb;
+                }
+                m.fArr[0] = 1.f;
+                for (int k = 0; k < c.nbreaks; k++)
+                    m.fArr[k + 1] = m.fArr[k] * gfm::powf_(m.rbreakSq[k], 0.5f * (m.nArr[k] - m.nArr[k + 1]));
+                m.n = m.nArr[0];
+            }
         }
         m.r_cut2 = 0.f;
         m.rminSq = m.rmaxSq = 0.f;
@@ -218,21 +247,29 @@ bool setup_models(const gf_skygen_config &cfg, int npixels, const gf_model_confi
             m.lf_inv_dx = (float)(1. / dX);
         }
         m.lf_n = (int)hm.lf.size();
+        if (c.type == GF_MODEL_LCBULGE) {
+            /* the LF scaled by f, no normalisation at a point (model_LCBulge.cpp:50-56) */
+            const float f0 = (float)c.f;
+            for (auto &v : hm.lf) v *= f0;
+            m.f = 1.f;
+        }
         /* normalisation at the LF sampling point (model_lib.h:68-95) */
         const double d2r = 0.01745329251994329576923691;
         float lfl = (float)c.lf_l, lfb = (float)c.lf_b, lfD = (float)c.lf_D;
         double rl = lfl * d2r, rb = lfb * d2r;
         float cl = (float)gfm::cos_d(rl), cb = (float)gfm::cos_d(rb), sl = (float)gfm::sin_d(rl), sb = (float)gfm::sin_d(rb);
         float px = lfD * cl * cb, py = lfD * sl * cb, pz = lfD * sb;
-        m.f = 1.f;
-        float norm = rho_host(m, px, py, pz);
-        if (!(norm != 0.f && std::isnormal(norm))) { err = "density is zero at the LF sampling point"; return false; }
-        float f0 = (float)c.f;
-        m.f = f0 / norm;
+        if (c.type != GF_MODEL_LCBULGE) {
+            m.f = 1.f;
+            float norm = rho_host(m, px, py, pz);
+            if (!(norm != 0.f && std::isnormal(norm))) { err = "density is zero at the LF sampling point"; return false; }
+            float f0 = (float)c.f;
+            m.f = f0 / norm;
+        }
         if (c.type == GF_MODEL_EXP_DISK) {
             float rc = (float)c.rcut;
             m.r_cut2 = rc * rc;
-        } else {
+        } else if (c.type != GF_MODEL_LCBULGE) {
             float rmin = (float)c.rmin, rmax = (float)c.rmax;
             m.rminSq = rmin * rmin;
             m.rmaxSq = rmax * rmax;

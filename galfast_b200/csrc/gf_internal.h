@@ -24,6 +24,10 @@ struct SkyModel {
     float lf_x0, lf_inv_dx;
     int32_t lf_n;
     const float *lf;               /* device pointer, lf_n samples */
+    /* power-law ellipsoids: index nArr[k] and scale fArr[k] between break radii
+     * rbreakSq[k - 1] and rbreakSq[k] (a plain power law: nbreaks = 0, nArr[0] = n, fArr[0] = 1) */
+    int32_t nbreaks;
+    float nArr[10], fArr[10], rbreakSq[9];
 };
 
 /* Sky geometry shared by all models of a generator. */

@@ -141,6 +141,9 @@ bool same_cfg(const void *a, const void *b, size_t n)
     return memcmp(a, b, n) == 0;
 }
 
+/* the kernel template a model type runs in: GF_MODEL_EXP_DISK or GF_MODEL_POWER_LAW_ELLIPSOID */
+int model_kind(int type) { return type == GF_MODEL_EXP_DISK ? GF_MODEL_EXP_DISK : GF_MODEL_POWER_LAW_ELLIPSOID; }
+
 struct ReqInfo {
     std::vector<gfh::HostModel> hm;    /* models in component order */
     std::vector<gf_model_config> mc;
@@ -496,7 +499,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         ReqInfo &q = R[j];
         if (!errs[j].empty()) return fail(GF_E_INVALID, errs[j]);
         for (int i = 0; i < nmod; i++) {
-            if (q.hm[i].m.type != R[0].hm[i].m.type)
+            if (model_kind(q.hm[i].m.type) != model_kind(R[0].hm[i].m.type))
                 return fail(GF_E_INVALID, "model kinds must agree across requests (in component order)");
             const long long kmax = (long long)q.hm[i].m.nm * q.hm[i].m.nM;
             if (kmax % GF_BLOCK) q.plain = true;
@@ -747,7 +750,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                 P.pix_sum = ws.pixsum.p;
                 {
                     ProfScope ps(ctx, GF_PROF_INTEGRATE);
-                    GF_CUDA(gfk::launch_integrate_pixels(P, R[integ[0]].hm[i].m.type, ws.tot.p, st));
+                    GF_CUDA(gfk::launch_integrate_pixels(P, model_kind(R[integ[0]].hm[i].m.type), ws.tot.p, st));
                 }
                 GF_CUDA(cudaMemcpyAsync(htot.data(), ws.tot.p, sizeof(double2) * (size_t)njobs, cudaMemcpyDeviceToHost, st));
                 GF_CUDA(cudaStreamSynchronize(st));
@@ -769,7 +772,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
             gfk::LaunchCrawlMulti L;
             memset(&L, 0, sizeof(L));
             L.jobs = d_jobs; L.items = d_items; L.nitems = nitems; L.counter = d_counter;
-            L.model_type = R[integ[0]].hm[i].m.type;
+            L.model_type = model_kind(R[integ[0]].hm[i].m.type);
             L.max_tab = max_tab(i, integ);
             L.jt = ctx->jt;
             {
@@ -939,7 +942,9 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
             for (int j : batched) want += S[j].expected[i] + 8.0 * sqrt(S[j].expected[i]) + 1024.0;
             int64_t cap = (int64_t)want;
             GF_CUDA(cudaMemcpyAsync(d_rng_snap, d_rng, 12 * (size_t)njobs * NS, cudaMemcpyDeviceToDevice, st));
-            const int mtype = R[batched[0]].hm[i].m.type;
+            /* the kernels' model kind: exponential disks, or the ellipsoids (power laws,
+             * broken power laws, LC bulges: their density is chosen per request) */
+            const int mtype = model_kind(R[batched[0]].hm[i].m.type);
             GF_TRY(rec.need((size_t)cap));
             int64_t nrec = 0;
             if (plan_used[i]) {

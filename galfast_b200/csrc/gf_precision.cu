@@ -19,6 +19,16 @@ namespace gfk {
 
 namespace {
 
+/* x^y in double, with pow's result for a negative x and an integer y */
+__device__ __forceinline__ double pow_fp64(double x, double y)
+{
+    if (x == 0.0) return y > 0.0 ? 0.0 : __longlong_as_double(0x7ff0000000000000ll);
+    if (x > 0.0) return gfm::exp_d(y * gfm::log_d(x));
+    if (y != rint(y)) return __longlong_as_double(0x7ff8000000000000ll);
+    const double r = gfm::exp_d(y * gfm::log_d(-x));
+    return fmod(fabs(y), 2.0) == 1.0 ? -r : r;
+}
+
 /* the anchor quantities of the bin (ilb, im, iM) in FP64 */
 template <int MODEL>
 __device__ void anchor_fp64(const SkyModel &m, const SkyGeom &g, int ilb, int im, int iM, double &ms, double &D3, double &K)
@@ -36,6 +46,10 @@ __device__ void anchor_fp64(const SkyModel &m, const SkyGeom &g, int ilb, int im
         const double r2 = wx * wx + wy * wy;
         if (m.r_cut2 != 0.f && r2 + wz * wz > (double)m.r_cut2) ms = 0.0;
         else ms = (double)m.f * gfm::exp_d(-sqrt(r2) / (double)m.l - fabs(wz) / (double)m.h);
+    } else if (m.type == GF_MODEL_LCBULGE) {
+        const double n = (double)m.n;
+        const double t = pow_fp64(pow_fp64(wx, n) + pow_fp64(wy / (double)m.ba, n) + pow_fp64(wz / (double)m.ca, n), 1.0 / n);
+        ms = gfm::exp_d(-t / (double)m.l);
     } else {
         const double DSq = wx * wx + wy * wy + wz * wz;
         if (m.rmaxSq != 0.f && (DSq < (double)m.rminSq || DSq >= (double)m.rmaxSq)) {
@@ -43,7 +57,9 @@ __device__ void anchor_fp64(const SkyModel &m, const SkyGeom &g, int ilb, int im
         } else {
             const double ty = wy / (double)m.ba, tz = wz / (double)m.ca;
             const double rSq = wx * wx + ty * ty + tz * tz;
-            ms = (double)m.f * gfm::exp_d(0.5 * (double)m.n * gfm::log_d(rSq));
+            int k = 0;
+            while (k != m.nbreaks && rSq > (double)m.rbreakSq[k]) k++;
+            ms = (double)m.f * (double)m.fArr[k] * gfm::exp_d(0.5 * (double)m.nArr[k] * gfm::log_d(rSq));
         }
     }
     D3 = D * D * D;

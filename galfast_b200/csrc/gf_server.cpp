@@ -47,7 +47,7 @@ std::vector<int32_t> model_kinds(const gf_job &j)
     for (int i = 0; i < j.nmodels; i++) m.push_back(&j.models[i]);
     std::stable_sort(m.begin(), m.end(), [](const gf_model_config *x, const gf_model_config *y) { return x->comp < y->comp; });
     std::vector<int32_t> k;
-    for (auto *p : m) k.push_back(p->type);
+    for (auto *p : m) k.push_back(p->type == GF_MODEL_EXP_DISK ? GF_MODEL_EXP_DISK : GF_MODEL_POWER_LAW_ELLIPSOID);
     return k;
 }
 

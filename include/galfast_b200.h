@@ -90,7 +90,9 @@ typedef struct gf_skygen_config {
 
 typedef enum {
     GF_MODEL_EXP_DISK = 1,                 /* src/skygen/model_expDisk.h */
-    GF_MODEL_POWER_LAW_ELLIPSOID = 2       /* src/skygen/model_powerLawEllipsoid.h */
+    GF_MODEL_POWER_LAW_ELLIPSOID = 2,      /* src/skygen/model_powerLawEllipsoid.h */
+    GF_MODEL_BROKEN_POWER_LAW = 3,         /* src/skygen/model_brokenPowerLaw.h: power-law ellipsoid with breaks */
+    GF_MODEL_LCBULGE = 4                   /* src/skygen/model_LCBulge.h: exp(-t/l), t = (x^n + (y/ba)^n + (z/ca)^n)^(1/n) */
 } gf_model_type;
 
 typedef enum {
@@ -114,6 +116,13 @@ typedef struct gf_model_config {
     const double *lf_M;        /* LF knots (absolute magnitude); NULL = constant LF of 1 */
     const double *lf_phi;      /* LF values */
     int32_t lf_n;              /* number of knots */
+    /* broken power law (keys n, rbreak; model_brokenPowerLaw.cpp:31-62): indices n_brk[0..nbreaks]
+     * inside and beyond the ellipsoidal break radii rbreak[0..nbreaks-1] (pc), nbreaks <= 9 */
+    int32_t nbreaks;
+    double n_brk[10];
+    double rbreak[9];
+    /* The LC bulge (model_LCBulge.cpp:33-60) uses n, l, ba, ca and the frame, and scales the
+     * LF by f instead of normalising the density at (lf_l, lf_b, lf_D). */
 } gf_model_config;
 
 typedef enum {

@@ -252,6 +252,8 @@ struct Model {
     int type, comp;
     float f, l, h, r_cut2;
     float n, ba, ca, rminSq, rmaxSq;
+    int nbreaks;                       /* brokenPowerLaw (model_brokenPowerLaw.h:41-45) */
+    float nArr[10], fArr[10], rbreakSq[9];
     float T[3];
     float M[3][3];
     std::vector<float> lf;
@@ -275,7 +277,22 @@ struct Model {
             float r = sqrtf(r2);
             float rho = f * OR_EXPF(-r / l - fabsf(wz) / h);
             return rho;
+        } else if (type == GF_MODEL_BROKEN_POWER_LAW) {
+            /* brokenPowerLaw::rho (model_brokenPowerLaw.h:55-82) */
+            float DSq = wx * wx + wy * wy + wz * wz;
+            if (rmaxSq && (DSq < rminSq || DSq >= rmaxSq)) return 0.f;
+            int k = 0;
+            float rSq = wx * wx + (wy / ba) * (wy / ba) + (wz / ca) * (wz / ca);
+            while (k != nbreaks && rSq > rbreakSq[k]) k++;
+            float rho = f * fArr[k] * OR_POWF(rSq, 0.5f * nArr[k]);
+            return rho;
+        } else if (type == GF_MODEL_LCBULGE) {
+            /* LCBulge::rho (model_LCBulge.h:79-92) */
+            float t = OR_POWF(OR_POWF(wx, n) + OR_POWF(wy / ba, n) + OR_POWF(wz / ca, n), (float)(1. / n));
+            float rho = OR_EXPF(-t / l);
+            return rho;
         } else {
+            /* powerLawEllipsoid::rho (model_powerLawEllipsoid.h:60-92) */
             float DSq = wx * wx + wy * wy + wz * wz;
             if (rmaxSq && (DSq < rminSq || DSq >= rmaxSq)) return 0.f;
             float ty = wy / ba, tz = wz / ca;
@@ -1138,24 +1155,40 @@ void *or_skygen_create(const gf_skygen_config *cfg, const gf_pencil_beam *pixels
         m.l = (float)c.l; m.h = (float)c.h; m.r_cut2 = 0.f;
         m.n = (float)c.n; m.ba = (float)c.ba; m.ca = (float)c.ca;
         m.rminSq = m.rmaxSq = 0.f;
-        /* load_lf (model_lib.h:68-95) */
-        load_lf(m, c);
-        float lfx = (float)c.lf_l, lfy = (float)c.lf_b, lfz = (float)c.lf_D;
-        Dir d = make_dir(lfx * dbl_d2r, lfy * dbl_d2r);
-        F3 lfc = {lfz * d.cl * d.cb, lfz * d.sl * d.cb, lfz * d.sb};
-        m.f = 1.f;
-        float norm = m.rho(lfc.x, lfc.y, lfc.z);
-        if (!(norm != 0.f && std::isnormal(norm))) {
-            g_err = "LF normalisation point has zero density";
-            delete s;
-            return nullptr;
+        m.nbreaks = 0;
+        if (c.type == GF_MODEL_BROKEN_POWER_LAW) {
+            /* brokenPowerLaw::load (model_brokenPowerLaw.cpp:31-62) */
+            m.nbreaks = c.nbreaks;
+            for (int k = 0; k <= c.nbreaks; k++) m.nArr[k] = (float)c.n_brk[k];
+            for (int k = 0; k < c.nbreaks; k++) { float rb = (float)c.rbreak[k]; m.rbreakSq[k] = rb * rb; }
+            m.fArr[0] = m.f = 1.f;
+            for (int k = 0; k < m.nbreaks; k++)
+                m.fArr[k + 1] = m.fArr[k] * OR_POWF(m.rbreakSq[k], 0.5f * (m.nArr[k] - m.nArr[k + 1]));
         }
-        float f0 = (float)c.f;
-        m.f = f0 / norm;
+        /* load_lf (model_lib.h:68-95); the LC bulge: load_lf_raw times f (model_LCBulge.cpp:50-56) */
+        load_lf(m, c);
+        if (c.type == GF_MODEL_LCBULGE) {
+            float f0 = (float)c.f;
+            for (auto &v : m.lf) v *= f0;
+            m.f = 1.f;
+        } else {
+            float lfx = (float)c.lf_l, lfy = (float)c.lf_b, lfz = (float)c.lf_D;
+            Dir d = make_dir(lfx * dbl_d2r, lfy * dbl_d2r);
+            F3 lfc = {lfz * d.cl * d.cb, lfz * d.sl * d.cb, lfz * d.sb};
+            m.f = 1.f;
+            float norm = m.rho(lfc.x, lfc.y, lfc.z);
+            if (!(norm != 0.f && std::isnormal(norm))) {
+                g_err = "LF normalisation point has zero density";
+                delete s;
+                return nullptr;
+            }
+            float f0 = (float)c.f;
+            m.f = f0 / norm;
+        }
         if (c.type == GF_MODEL_EXP_DISK) {
             float rc = (float)c.rcut;
             m.r_cut2 = rc * rc;
-        } else {
+        } else if (c.type != GF_MODEL_LCBULGE) {
             float rmin = (float)c.rmin, rmax = (float)c.rmax;
             m.rminSq = rmin * rmin;
             m.rmaxSq = rmax * rmax;
@@ -1303,10 +1336,18 @@ int or_expected_fp64(void *h, int32_t mi, int32_t px, double *sum32, double *sum
             if (m.type == GF_MODEL_EXP_DISK) {
                 const double r2 = wx * wx + wy * wy;
                 ms64 = (m.r_cut2 && r2 + wz * wz > m.r_cut2) ? 0.0 : m.f * exp(-sqrt(r2) / m.l - fabs(wz) / m.h);
+            } else if (m.type == GF_MODEL_LCBULGE) {
+                const double t = pow(pow(wx, (double)m.n) + pow(wy / m.ba, (double)m.n) + pow(wz / m.ca, (double)m.n), 1.0 / m.n);
+                ms64 = exp(-t / m.l);
             } else {
                 const double DSq = wx * wx + wy * wy + wz * wz;
                 const double ty = wy / m.ba, tz = wz / m.ca;
-                ms64 = (m.rmaxSq && (DSq < m.rminSq || DSq >= m.rmaxSq)) ? 0.0 : m.f * pow(wx * wx + ty * ty + tz * tz, 0.5 * m.n);
+                const double rSq = wx * wx + ty * ty + tz * tz;
+                int k = 0;
+                while (k != m.nbreaks && rSq > m.rbreakSq[k]) k++;
+                const double nk = m.type == GF_MODEL_BROKEN_POWER_LAW ? m.nArr[k] : m.n;
+                const double fk = m.type == GF_MODEL_BROKEN_POWER_LAW ? m.fArr[k] : 1.0;
+                ms64 = (m.rmaxSq && (DSq < m.rminSq || DSq >= m.rmaxSq)) ? 0.0 : m.f * fk * pow(rSq, 0.5 * nk);
             }
             D364 = Dd * Dd * Dd;
             K64 = (double)pix.dA * 0.46051701859880913680 * (double)m.dm * (double)m.dM;

@@ -55,6 +55,10 @@ def load(flavour="p"):
         L.or_vcyl2pm.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp]
         L.or_error_normal.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32]
         L.or_error_normal.restype = C.c_double
+        L.or_math_f.argtypes = [C.c_int, C.c_int, vp, vp, vp]
+        L.or_math_d.argtypes = [C.c_int, C.c_int, vp, vp, vp]
+        L.or_diag.argtypes = [C.c_int, C.c_int, C.c_int, vp, vp]
+        L.or_advance.argtypes = [vp, vp, C.c_int, C.c_int]
         _libs[flavour] = L
     return _libs[flavour]
 

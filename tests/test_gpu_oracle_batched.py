@@ -156,3 +156,42 @@ def test_poisson_sampler_on_device_equals_oracle(ctx):
     G.check(G.lib().gf_rng_poisson(ctx.h, st.ctypes.data, mu.ctypes.data, mu.size, out_g.ctypes.data))
     np.testing.assert_array_equal(out_g, out_o)
     assert (st[1], st[2]) == (oc[0], ox[0])
+
+
+def model_types_workload(lib, seed48=42):
+    """An exponential disk, an LC bulge (exp(-t / l), t the ellipsoidal radius with
+    n = 2, LF scaled by f = 10) and a broken power-law halo (n = -2.5 inside
+    25 kpc, -3.5 beyond), towards the bulge at (l, b) = (5, 8) deg."""
+    from galfast_b200 import _abi as A
+    w = W.build_workload(lib, foot=W.cap_footprint(5.0, 8.0, 1.5), dx_deg=0.25, m0=15.0, m1=19.0, capacity=1 << 20,
+                         seed48=seed48)
+    b = w.models[1]
+    b.type = A.GF_MODEL_LCBULGE
+    b.f, b.l, b.n, b.ba, b.ca = 10.0, 700.0, 2.0, 0.6, 0.4
+    h = w.models[2]
+    h.type = A.GF_MODEL_BROKEN_POWER_LAW
+    h.nbreaks = 1
+    h.n_brk[0], h.n_brk[1] = -2.5, -3.5
+    h.rbreak[0] = 25000.0
+    return w
+
+
+def test_bulge_and_broken_power_law_equal_oracle(lib, multipliers):
+    """model_LCBulge and model_brokenPowerLaw (src/skygen/) on the plain path and
+    in the batched passes, against the oracle's restatement of each model."""
+    w = model_types_workload(lib)
+    ref, st, _ = oracle_catalog(w, multipliers)
+    assert st["generated"][1] > 1000 and st["generated"][2] > 1000
+    ctx = G.Context(0)
+    plain = {}
+    gst = G.run_catalog(ctx, w, sink=lambda m, t, off: plain.setdefault(m, []).append(t.as_dict()))
+    compare(ref, {m: concat(p) for m, p in plain.items()}, "plain")
+    for i in range(3):
+        assert gst.generated[i] == st["generated"][i]
+        assert gst.expected[i] == pytest.approx(st["expected"][i][0], rel=1e-12)
+    w2 = model_types_workload(lib, seed48=43)
+    ref2, st2, _ = oracle_catalog(w2, multipliers)
+    got, stats = batched_catalogs(ctx, [w, w2])
+    ctx.close()
+    compare(ref, got[0], "batched 0")
+    compare(ref2, got[1], "batched 1")

