@@ -220,6 +220,8 @@ def main():
     ap.add_argument("--parity", type=int, default=16, help="config4: timed requests re-run alone and compared (0: none)")
     ap.add_argument("--text-requests", type=int, default=32, help="config4: requests written as text catalogs (0: none)")
     ap.add_argument("--serve-rates", default="100,1000", help="config4: arrival rates of the serving sub-measurement ('' = none)")
+    ap.add_argument("--no-fullsky", dest="fullsky", action="store_false",
+                    help="config4: skip the full-sky plain run and the precision form")
     args = ap.parse_args()
     global CLOCK_LOG
     CLOCK_LOG = args.clock_log
@@ -508,6 +510,9 @@ def bench_multi(args, G, W, ctx, rank, world, dist):
                "bins_per_s": sbins / dt, "stars_per_bin_sample": s_ / sbins, "stars_per_bin_set": generated / bins,
                "sample": "%s; full module chain, single-threaded restatement (libm), %.1f s" % (sdesc, dt)}
 
+    fullsky = None
+    if args.fullsky and rank == 0:
+        fullsky = fullsky_summary(G, W, L, ctx)
     serve = None
     if args.serve_rates and world == 1:
         serve = serve_summary(G, W, L, ctx, [float(x) for x in args.serve_rates.split(",")], args.serve_requests)
@@ -530,7 +535,7 @@ def bench_multi(args, G, W, ctx, rank, world, dist):
                           "gf_catalog_run, one at a time" % (C4_PLAIN_STRIDE, len(sample)),
                           "latency_p50_s": float(np.percentile(plat, 50)), "latency_p99_s": float(np.percentile(plat, 99))},
                 "batched_over_plain": value / plain_value if plain_value else None,
-                "parity": parity, "serve": serve, "text_output": textout,
+                "parity": parity, "serve": serve, "text_output": textout, "fullsky": fullsky,
                 "e2e": e2e, "roofline": roofline, "integrate_roofline": integ_roof, "roofline_hbm": roofline_hbm,
                 "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk_summary,
                 "phases_ms_per_step": {k: v[0] / args.steps for k, v in prof.items()}}
@@ -631,6 +636,35 @@ def same_catalog(a, b):
     return True
 
 
+def fullsky_summary(G, W, L, ctx):
+    """The plain full-sky workload (one request through gf_catalog_run, rows kept on
+    the device) and the precision form on the same footprint (FP32 expected counts
+    as generated against FP64, per model)."""
+    w, desc = workload(G, W, "config2", 0)
+    job = w.job(G.Job)
+    stats = G.CatalogStats()
+    ctx.mark(0)
+    G.check(L.gf_catalog_run(ctx.h, C.byref(job), G.BatchCallback(), None, C.byref(stats)))
+    ctx.mark(1)
+    ms = ctx.elapsed_ms(0, 1)
+    stored = sum(stats.stored[i] for i in range(len(w.models)))
+    sk = G.Skygen(ctx, w)
+    reps = []
+    t0 = time.perf_counter()
+    for m in range(len(w.models)):
+        rep = sk.precision(m)[0]
+        reps.append({"model": m, "total_rel_err": rep.total_rel_err, "pixel_max_rel_err": rep.pixel_max_rel_err,
+                     "bin_max_rel_err": rep.bin_max_rel_err, "bin_mean_rel_err": rep.bin_mean_rel_err, "bins": int(rep.bins)})
+    t_prec = time.perf_counter() - t0
+    sk.close()
+    return {"plain_fullsky": {"workload": "config2: " + desc, "pixels": w.npixels, "stars": int(stored),
+                              "batches": int(stats.batches), "seconds": ms / 1e3, "stars_per_s": stored / (ms / 1e3),
+                              "timing": "CUDA events on the library's stream, one request after the batched steps"},
+            "precision": {"workload": "config3: the same footprint, every (pixel, m, M) bin in FP32 and FP64",
+                          "max_total_rel_err": max(r["total_rel_err"] for r in reps), "target": 1e-6,
+                          "models": reps, "seconds": t_prec}}
+
+
 def serve_summary(G, W, L, ctx, rates, nreq, nchecks=4):
     """Served requests (gf_server, continuous batching) at the given Poisson arrival
     rates: latency percentiles and throughput, and the smallest `nchecks` requests of
@@ -665,10 +699,13 @@ def serve_summary(G, W, L, ctx, rates, nreq, nchecks=4):
         for rid, k in order.items():
             if k in small and srv.status.get(rid) == 0:
                 equal += int(same_catalog(standalone_rows(G, ctx, ws[k]), srv.rows.get(rid, {})))
+        info = srv.info()
         srv.close()
         out.append({"rate_per_s": rate, "requests": nreq, "failed": failed, "rows": int(rows), "stars_per_s": rows / span,
                     "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
-                    "makespan_s": span, "bit_exact_checked": len(small), "bit_exact_equal": equal})
+                    "makespan_s": span, "bit_exact_checked": len(small), "bit_exact_equal": equal,
+                    "batches": info["runs"], "deferred_at_admission": info["deferred"],
+                    "peak_batches_running": info["peak_running"], "peak_reserved_bytes": info["peak_reserved"]})
     return {"workload": "Poisson arrivals of caps and lon/lat rectangles of log-uniform 1-1000 deg^2 at |b|>10 deg, "
                         "14<r<U(20,25), half ugriz / half ugrizy; gf_server with 2 workers, 150 GiB budget",
             "latency": "submit to completion, host wall clock", "rates": out}

@@ -42,6 +42,11 @@ class CatalogStats(C.Structure):
                 ("norm", C.c_float)]
 
 
+class ServerInfo(C.Structure):
+    _fields_ = [("runs", C.c_int64), ("completed", C.c_int64), ("deferred", C.c_int64), ("peak_reserved", C.c_int64),
+                ("peak_running", C.c_int32), ("queued", C.c_int32), ("active", C.c_int32), ("pad", C.c_int32)]
+
+
 BatchCallback = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int32, C.POINTER(Table), C.c_int64)
 ServerRows = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.POINTER(Table), C.c_int64, C.c_int64)
 ServerDone = C.CFUNCTYPE(None, C.c_void_p, C.c_int64, C.c_int32, C.POINTER(CatalogStats))
@@ -109,6 +114,7 @@ def lib():
         L.gf_multi_set_admission.argtypes = [vp, C.c_double]
         L.gf_debug_fail_allocations.argtypes = [C.c_int64, C.c_int64]
         L.gf_textout_open.argtypes = [C.c_char_p, vp, C.POINTER(vp)]
+        L.gf_fitsout_open.argtypes = [C.c_char_p, vp, C.POINTER(vp)]
         L.gf_textout_write.argtypes = [vp, vp, C.c_int64, C.c_int64]
         L.gf_textout_close.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         L.gf_textout_multi_sink.argtypes = [vp, C.c_int32, vp, vp, vp]
@@ -118,6 +124,8 @@ def lib():
         L.gf_server_create.argtypes = [C.c_int32, C.c_int32, C.c_int64, C.c_int32, C.POINTER(vp)]
         L.gf_server_submit.argtypes = [vp, C.POINTER(Job), ServerRows, ServerDone, vp, C.POINTER(C.c_int64)]
         L.gf_server_drain.argtypes = [vp]
+        L.gf_server_get_info.argtypes = [vp, C.POINTER(ServerInfo)]
+        L.gf_server_pause.argtypes = [vp, C.c_int32]
         L.gf_server_destroy.argtypes = [vp]
         L.gf_skygen_precision.argtypes = [vp, C.c_int32, C.POINTER(A.PrecisionReport), C.POINTER(C.c_double),
                                           C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -479,7 +487,8 @@ def run_catalog_multi_host(ctx, workloads, sink, piece_rows=0):
 class Server:
     """gf_server: continuous batching of catalog requests on one device.
 
-    submit(w) queues a workload; keep_rows=True keeps each request's rows in host
+    submit(w) queues a workload (the server copies the job, so nothing of it has
+    to be kept here); keep_rows=True keeps each request's rows in host
     memory (a dict per model of column arrays), a callable keep_rows(request id)
     those of the requests it accepts.  Completion wall-clock times are
     recorded for latency.  Callbacks run on the server's worker threads."""
@@ -492,7 +501,6 @@ class Server:
         check(lib().gf_server_create(device, workers, int(memory_budget), max_batch, C.byref(self.h)))
         self.keep_rows = keep_rows
         self.lock = threading.Lock()
-        self.jobs = {}
         self.submitted, self.finished, self.status, self.stats, self.rows = {}, {}, {}, {}, {}
         self._stage = {}
 
@@ -525,12 +533,22 @@ class Server:
         t = self._time.perf_counter()
         check(lib().gf_server_submit(self.h, C.byref(job), self._rows_cb, self._done_cb, None, C.byref(rid)))
         with self.lock:
-            self.jobs[rid.value] = (job, w)
             self.submitted[rid.value] = t
         return rid.value
 
     def drain(self):
         check(lib().gf_server_drain(self.h))
+
+    def pause(self, paused=True):
+        """gf_server_pause: hold (or release) the queue; running batches finish."""
+        check(lib().gf_server_pause(self.h, 1 if paused else 0))
+
+    def info(self):
+        """gf_server_get_info: batches run, requests completed and deferred at
+        admission, the largest memory reservation and most batches at once."""
+        i = ServerInfo()
+        check(lib().gf_server_get_info(self.h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in ServerInfo._fields_ if k != "pad"}
 
     def close(self):
         if self.h:
@@ -592,10 +610,12 @@ def textout_config(w, version=None, threads=0):
 class TextWriter:
     """gf_textout: a catalog text file in the reference's format."""
 
+    _open = "gf_textout_open"
+
     def __init__(self, path, cfg):
         self.h = C.c_void_p()
         self.cfg = cfg
-        check(lib().gf_textout_open(str(path).encode(), C.byref(cfg), C.byref(self.h)))
+        check(getattr(lib(), self._open)(str(path).encode(), C.byref(cfg), C.byref(self.h)))
 
     def write(self, table, begin, end):
         check(lib().gf_textout_write(self.h, C.byref(table), int(begin), int(end)))
@@ -606,3 +626,9 @@ class TextWriter:
             check(lib().gf_textout_close(self.h, C.byref(rows), C.byref(nbytes)))
             self.h = C.c_void_p()
         return rows.value, nbytes.value
+
+
+class FitsWriter(TextWriter):
+    """gf_fitsout_open: the same catalog as a FITS file (the reference's os_fitsout)."""
+
+    _open = "gf_fitsout_open"

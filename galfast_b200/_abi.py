@@ -124,7 +124,7 @@ class ModelInfo(C.Structure):
 # exported symbols of libgalfast_b200.so declared in include/galfast_b200.h
 EXPORTS = [
     "gf_last_error", "gf_ctx_create", "gf_ctx_destroy", "gf_ctx_sync", "gf_ctx_mark", "gf_ctx_elapsed",
-    "gf_launch_count", "gf_catalog_run", "gf_catalog_run_multi", "gf_multi_set_memory_budget", "gf_table_download_rows", "gf_server_create", "gf_server_submit", "gf_server_drain", "gf_server_destroy", "gf_skygen_precision", "gf_tuning_get", "gf_tuning_set", "gf_catalog_run_multi_host", "gf_profile_enable", "gf_profile_read",
+    "gf_launch_count", "gf_catalog_run", "gf_catalog_run_multi", "gf_multi_set_memory_budget", "gf_table_download_rows", "gf_server_create", "gf_server_submit", "gf_server_drain", "gf_server_get_info", "gf_server_pause", "gf_server_destroy", "gf_skygen_precision", "gf_tuning_get", "gf_tuning_set", "gf_catalog_run_multi_host", "gf_profile_enable", "gf_profile_read",
     "gf_rng_init", "gf_rng_seed48_from_cli_seed", "gf_rng_get_state", "gf_rng_set_state",
     "gf_skygen_create", "gf_skygen_destroy", "gf_skygen_model_info_get", "gf_skygen_model_lf_get",
     "gf_skygen_integrate", "gf_skygen_set_norm", "gf_skygen_draw",

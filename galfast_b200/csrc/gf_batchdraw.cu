@@ -65,14 +65,16 @@ __device__ __forceinline__ bool bd_surely_empty(float u, float mu)
 /* the sampler's exact test (mu > 10 takes the branch that never compares with exp(-mu)) */
 __device__ __forceinline__ bool bd_has_stars(float u, float mu)
 {
-    return mu > 10.f || u > gfm::expf_(-mu);
+    return mu > 10.f || gfr::exceeds_exp_neg(u, mu);
 }
 
 /* a request's view for the draw walk (per warp, in shared memory) */
 struct DrawJobView {
     const uint32_t *blk, *binfo;
     const uint16_t *bslot, *dslot;
-    const float *slotD, *msbase, *lfmx;
+    const float *slotD;
+    const float2 *ms2;             /* per pixel: (density, D^3) of each slot, then (first cut row, K) */
+    const uint4 *brec;             /* per block: blk, binfo, bslot | first diagonal-start slot << 16, LF max */
     const gf_pencil_beam *pixels;
     int nslots, Bp, npix, x, y, N;
     int QN, RN;                    /* N = QN Bp + RN: a stream's step in (pixel, block) */
@@ -105,13 +107,14 @@ __global__ void __launch_bounds__(256) slot_density_kernel(SlotDensityParams P)
         const int nslots = h->nslots;
         const float *slotD = plan_at<float>(plan, h->off_slot);
         const gf_pencil_beam pix = J.g.pixels[ilb];
-        float *row = P.ms[job] + (size_t)ilb * (nslots + 2);
+        float2 *row = P.ms[job] + (size_t)ilb * (nslots + 1);
         for (int s = lane; s < nslots; s += 32) {
             const float D = slotD[s];
             const float px = D * pix.cl * pix.cb;
             const float py = D * pix.sl * pix.cb;
             const float pz = D * pix.sb;
-            row[s] = gfc::model_rho<MODEL>(J.m, px, py, pz);
+            /* D^3 with the reference's float product (skygen.cu.h:554) */
+            row[s] = make_float2(gfc::model_rho<MODEL>(J.m, px, py, pz), D * D * D);
         }
         /* the pixel's first cut apparent-magnitude row (m0 + dm im + Am > m1; increasing in im)
          * and its volume factor K = dA * POGSON * dm * dM */
@@ -125,10 +128,7 @@ __global__ void __launch_bounds__(256) slot_density_kernel(SlotDensityParams P)
             const int t = __shfl_xor_sync(0xffffffffu, icut, o);
             icut = t < icut ? t : icut;
         }
-        if (lane == 0) {
-            row[nslots] = __int_as_float(icut);
-            row[nslots + 1] = pix.dA * GF_POGSON * m.dm * m.dM;
-        }
+        if (lane == 0) row[nslots] = make_float2(__int_as_float(icut), pix.dA * GF_POGSON * m.dm * m.dM);
     }
 }
 
@@ -195,9 +195,12 @@ __device__ __forceinline__ void flush_events(const BatchDrawParams &P, EventReco
     __syncwarp();
 }
 
-/* Per request of a chunk and block of its grid: the largest LF value over the
- * block's 10 bins (the same LF(M) samples the draw's shared table holds). */
-__global__ void __launch_bounds__(256) block_lfmax_kernel(BlockLfParams P)
+/* Per request of a chunk and block of its grid, the record the bound walk loads
+ * in one piece: the block's first bin (i | j << 16), its binfo word, its
+ * block-start slot | the slot of its first diagonal start << 16, and the largest
+ * LF value over its 10 bins (the same LF(M) samples the draw's shared table
+ * holds; negative values count as 0). */
+__global__ void __launch_bounds__(256) block_records_kernel(BlockLfParams P)
 {
     for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < P.total; f += (long long)gridDim.x * blockDim.x) {
         int lo = 0, hi = P.njobs;
@@ -212,12 +215,16 @@ __global__ void __launch_bounds__(256) block_lfmax_kernel(BlockLfParams P)
         const IntegPlanHdr *h = (const IntegPlanHdr *)plan;
         const uint32_t bij = plan_at<uint32_t>(plan, h->off_blk)[b];
         int i = (int)(bij & 0xffffu), j = (int)(bij >> 16);
+        const uint32_t bi = plan_at<uint32_t>(plan, h->off_binfo)[b];
+        const uint32_t wm = (bi >> 16) & 0x3ffu;
+        const uint32_t s0 = plan_at<uint16_t>(plan, h->off_bslot)[b];
+        const uint32_t s1 = wm ? plan_at<uint16_t>(plan, h->off_dslot)[i + j + 1] : 0u;
         float mx = gfc::lf_sample(m, m.lf, m.M1 - (float)j * m.dM);
         for (int s = 1; s < GF_BLOCK; s++) {
             gfc::step_in_pixel(i, j, m.nm, m.nM);
             mx = fmaxf(mx, gfc::lf_sample(m, m.lf, m.M1 - (float)j * m.dM));
         }
-        P.lfmax[job][b] = mx;
+        P.brec[job][b] = make_uint4(bij, bi, s0 | (s1 << 16), __float_as_uint(fmaxf(mx, 0.f)));
     }
 }
 
@@ -273,16 +280,16 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                 V.bslot = plan_at<uint16_t>(plan, h->off_bslot);
                 V.dslot = plan_at<uint16_t>(plan, h->off_dslot);
                 V.binfo = plan_at<uint32_t>(plan, h->off_binfo);
-                V.msbase = P.ms[job];
+                V.ms2 = P.ms[job];
                 V.pixels = J.g.pixels;
                 V.npix = J.g.npixels;
                 V.norm = m.norm;
                 V.dmin = m.dmin;
                 V.dmax = m.dmax;
                 V.dlim = m.dmin != 0.f || m.dmax != 0.f;
-                V.lfmx = P.lfmax ? P.lfmax[job] : nullptr;
+                V.brec = P.brec ? P.brec[job] : nullptr;
                 /* the block bound needs non-negative densities (f >= 0) and normalisation */
-                V.bound = V.lfmx && !V.dlim && m.f >= 0.f && m.norm >= 0.f;
+                V.bound = V.brec && !V.dlim && m.f >= 0.f && m.norm >= 0.f;
             }
             __syncwarp();
             loaded = job;
@@ -309,38 +316,45 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                 /* Upper bound of the block's expected counts: the reference's float product
                  * with each factor at its largest over the block (correctly rounded products of
                  * non-negative factors are monotone).  u <= 1 - bound - 3e-7 proves a bin
-                 * empty; only the bins whose uniform exceeds it need their exact mu. */
-                uint32_t live = 0, cand = 0;
-                int i0 = 0, j0 = 0, sl0 = 0;
-                float K = 0.f, thr = 0.f;
+                 * empty, so the walk only steps the stream over the block's live bins and
+                 * compares the largest uniform with the threshold; a block whose largest
+                 * uniform exceeds it is walked again with the exact expected counts. */
+                uint32_t live = 0;
+                bool any = false;
                 int64_t xthr = -1;             /* uniform u = 2^-32 x passes the bound iff x <= xthr */
-                const float *msr = V.msbase;
+                uint4 br = make_uint4(0u, 0u, 0u, 0u);
+                const float2 *row = V.ms2;
+                float K = 0.f;
                 const uint64_t w0 = w;
                 if (valid) {
-                    const uint32_t bij = __ldg(V.blk + lb);
-                    i0 = (int)(bij & 0xffffu);
-                    j0 = (int)(bij >> 16);
-                    const uint32_t bi = __ldg(V.binfo + lb);
-                    const int imax = (int)(bi & 0xffffu);
-                    const uint32_t wm = (bi >> 16) & 0x3ffu;
-                    sl0 = __ldg(V.bslot + lb);
-                    msr = V.msbase + (size_t)pix * (V.nslots + 2);
-                    const int icut = __float_as_int(msr[V.nslots]);
-                    K = msr[V.nslots + 1];
-                    float msmax = msr[sl0], Dmax = __ldg(V.slotD + sl0);
-                    int d = i0 + j0;
-                    for (uint32_t mm = wm; mm; mm &= mm - 1u) {
-                        d++;
-                        const int sl = __ldg(V.dslot + d);
-                        msmax = fmaxf(msmax, msr[sl]);
-                        Dmax = fmaxf(Dmax, __ldg(V.slotD + sl));
+                    br = __ldg(V.brec + lb);
+                    const int i0 = (int)(br.x & 0xffffu), j0 = (int)(br.x >> 16);
+                    const int imax = (int)(br.y & 0xffffu);
+                    const uint32_t wm = (br.y >> 16) & 0x3ffu;
+                    row = V.ms2 + (size_t)pix * (V.nslots + 1);
+                    const float2 ik = row[V.nslots];
+                    const int icut = __float_as_int(ik.x);
+                    K = ik.y;
+                    const float2 q0 = row[br.z & 0xffffu];
+                    float msmax = q0.x, D3max = q0.y;
+                    if (wm) {
+                        const float2 q1 = row[br.z >> 16];
+                        msmax = fmaxf(msmax, q1.x);
+                        D3max = fmaxf(D3max, q1.y);
+                        /* further diagonal starts in the block (short diagonals only) */
+                        int d = i0 + j0 + 1;
+                        for (uint32_t mm = wm & (wm - 1u); mm; mm &= mm - 1u) {
+                            d++;
+                            const float2 q2 = row[__ldg(V.dslot + d)];
+                            msmax = fmaxf(msmax, q2.x);
+                            D3max = fmaxf(D3max, q2.y);
+                        }
                     }
-                    float mub = fmaxf(__ldg(V.lfmx + lb), 0.f) * msmax;
+                    float mub = __uint_as_float(br.w) * msmax;
                     mub *= V.norm;
-                    mub *= Dmax * Dmax * Dmax;
+                    mub *= D3max;
                     mub *= K;
-                    thr = (1.0f - mub) - 3.0e-7f;
-                    xthr = gfr::uniform_threshold(thr);
+                    xthr = gfr::uniform_threshold((1.0f - mub) - 3.0e-7f);
                     if (imax < icut) {
                         live = (1u << GF_BLOCK) - 1u;
                     } else {
@@ -357,31 +371,48 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                         }
                     }
                     if (xthr < 0) {
-                        cand = live;                   /* the bound proves nothing: exact test throughout */
-                    } else {
-                        const uint32_t X = (uint32_t)xthr;
+                        any = live != 0;               /* the bound proves nothing: exact test throughout */
+                    } else if (live == (1u << GF_BLOCK) - 1u) {
+                        uint32_t mx = 0;
 #pragma unroll
-                        for (int s = 0; s < GF_BLOCK; s++) {
-                            if ((live >> s) & 1u) {
-                                if (bd_mwc_x(w, a) > X) cand |= 1u << s;
-                            }
-                        }
+                        for (int s = 0; s < GF_BLOCK; s++) mx = max(mx, bd_mwc_x(w, a));
+                        any = mx > (uint32_t)xthr;
+                    } else {
+                        uint32_t mx = 0;
+#pragma unroll
+                        for (int s = 0; s < GF_BLOCK; s++)
+                            if ((live >> s) & 1u) mx = max(mx, bd_mwc_x(w, a));
+                        any = mx > (uint32_t)xthr;
                     }
                 }
-                if (cand) {
-                    /* Exact tests from the first candidate bin on.  The state before bin
-                     * s is w0 advanced over the live bins before s; the bin's position
-                     * follows from the block's diagonal starts (wm), as step_in_pixel
-                     * walks it.  While no star is drawn the uniforms are the bound
+                if (any) {
+                    /* The candidate bins (uniform above the threshold), the first of them and the
+                     * stream state before it.  While no star is drawn the uniforms are the bound
                      * walk's, so once no candidate is left the walk's end state stands. */
                     const uint64_t w_end = w;
                     const bool walked = xthr >= 0;
-                    const uint32_t bi = __ldg(V.binfo + lb);
-                    const uint32_t wm = (bi >> 16) & 0x3ffu;
-                    int s = __ffs(cand) - 1;
-                    w = w0;
-                    for (uint32_t q = live & ((1u << s) - 1u); q; q &= q - 1u) bd_mwc_x(w, a);
-                    /* position and anchor of bin s */
+                    uint32_t cand = 0;
+                    int s = -1;
+                    {
+                        uint64_t ww = w0, wf = w0;
+#pragma unroll
+                        for (int q = 0; q < GF_BLOCK; q++) {
+                            if ((live >> q) & 1u) {
+                                const uint64_t wb = ww;
+                                const uint32_t x = bd_mwc_x(ww, a);
+                                if (!walked || (int64_t)x > xthr) {
+                                    cand |= 1u << q;
+                                    if (s < 0) { s = q; wf = wb; }
+                                }
+                            }
+                        }
+                        w = wf;
+                    }
+                    const int i0 = (int)(br.x & 0xffffu), j0 = (int)(br.x >> 16);
+                    const uint32_t wm = (br.y >> 16) & 0x3ffu;
+                    const int sl0 = (int)(br.z & 0xffffu);
+                    /* exact tests from the first candidate bin s on; the bin's position
+                     * follows from the block's diagonal starts (wm), as step_in_pixel walks it */
                     const uint32_t starts = wm & ((2u << s) - 2u);         /* diagonal starts in bins 1..s */
                     int d = i0 + j0 + __popc(starts), i, j, slot;
                     if (starts) {
@@ -395,8 +426,8 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                         j = j0 - s;
                         slot = sl0;
                     }
-                    float ms = msr[slot], D = __ldg(V.slotD + slot);
-                    float D3 = D * D * D;
+                    float2 q = row[slot];
+                    float ms = q.x, D3 = q.y;
                     bool star = false;
                     for (const int s0 = s; s < GF_BLOCK; s++) {
                         if (s > s0) {
@@ -405,9 +436,9 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                                 i = d - (V.y - 1) > 0 ? d - (V.y - 1) : 0;
                                 j = d - i;
                                 slot = __ldg(V.dslot + d);
-                                ms = msr[slot];
-                                D = __ldg(V.slotD + slot);
-                                D3 = D * D * D;
+                                q = row[slot];
+                                ms = q.x;
+                                D3 = q.y;
                             } else {
                                 i++;
                                 j--;
@@ -463,20 +494,23 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                 i0 = (int)(bij & 0xffffu);
                 j0 = (int)(bij >> 16);
                 int slot = __ldg(V.bslot + lb);
-                const float *msr = V.msbase + (size_t)pix * (V.nslots + 2);
-                const int icut = __float_as_int(msr[V.nslots]);
-                const float K = msr[V.nslots + 1];
-                float ms = msr[slot], D = __ldg(V.slotD + slot);
-                float D3 = D * D * D;
+                const float2 *row = V.ms2 + (size_t)pix * (V.nslots + 1);
+                const float2 ik = row[V.nslots];
+                const int icut = __float_as_int(ik.x);
+                const float K = ik.y;
+                float2 q = row[slot];
+                float ms = q.x, D3 = q.y;
+                float D = V.dlim ? __ldg(V.slotD + slot) : 0.f;
                 bool dc = V.dlim && (V.dmin > D || V.dmax <= D);      /* anchor outside [V.dmin, V.dmax): Am = inf */
                 int i = i0, j = j0;
 #pragma unroll
                 for (int s = 0; s < GF_BLOCK; s++) {
                     if (s > 0 && gfc::step_in_pixel(i, j, V.x, V.y)) {
                         slot = __ldg(V.dslot + i + j);
-                        ms = msr[slot];
-                        D = __ldg(V.slotD + slot);
-                        D3 = D * D * D;
+                        q = row[slot];
+                        ms = q.x;
+                        D3 = q.y;
+                        D = V.dlim ? __ldg(V.slotD + slot) : 0.f;
                         dc = V.dlim && (V.dmin > D || V.dmax <= D);
                     }
                     float r = LFM[j] * ms;
@@ -631,11 +665,11 @@ cudaError_t launch_slot_density(const SlotDensityParams &P, int model_type, cuda
     return cudaGetLastError();
 }
 
-cudaError_t launch_block_lfmax(const BlockLfParams &P, cudaStream_t s)
+cudaError_t launch_block_records(const BlockLfParams &P, cudaStream_t s)
 {
     if (P.total <= 0) return cudaSuccess;
     const int blocks = (int)std::min<long long>((P.total + 255) / 256, (long long)sm_count() * 16);
-    block_lfmax_kernel<<<blocks, 256, 0, s>>>(P);
+    block_records_kernel<<<blocks, 256, 0, s>>>(P);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -94,6 +94,21 @@ struct gf_photoerr {
 
 namespace gfa {
 
+/* Admission of a multi-request call (the serving workers' hook).  After the
+ * integrate pass, admit() receives need[k], the device memory (bytes) of the
+ * k-th batched request in submission order, returns how many of them, from the
+ * first, to generate in this call (at least one) and sets *budget, the memory the
+ * call's chunks may use.  The requests after them are not generated
+ * (deferred[j] = 1) and receive no rows; requests that take the plain path are
+ * always generated. */
+struct Admission {
+    int32_t (*admit)(void *user, const double *need, int32_t n, int64_t *budget) = nullptr;
+    void *user = nullptr;
+    std::vector<char> deferred;
+};
+gf_status catalog_run_multi_admitted(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, void *user,
+                                     gf_catalog_stats *stats, Admission *adm);
+
 gf_status check_ctx(gf_ctx *ctx);
 /* zero the module columns (FeH, vcyl, mags, photoflags, obsmags, pm, radec) of rows
  * [0, n): rows a module skips (hidden stars) read zero whatever the table held before */

@@ -183,8 +183,8 @@ cudaError_t launch_integrate_pixels(const IntegPixParams &P, int model_type, dou
 struct SlotDensityParams {
     const CrawlJob *jobs;
     const unsigned char *const *plans;   /* per request */
-    float *const *ms;              /* per request, per pixel: model density of each slot, then the first
-                                    * cut apparent-magnitude row (int bits) and K = dA POGSON dm dM */
+    float2 *const *ms;             /* per request, per pixel, nslots + 1 pairs: (model density, D^3) of each
+                                    * slot, then (first cut apparent-magnitude row as int bits, K = dA POGSON dm dM) */
     const int32_t *job_list;       /* requests of the launch */
     const int32_t *pix_off;        /* [njobs + 1] first flat pixel of each listed request */
     int32_t njobs, total_pix;
@@ -192,7 +192,8 @@ struct SlotDensityParams {
 struct BlockLfParams {
     const CrawlJob *jobs;
     const unsigned char *const *plans;   /* per request */
-    float *const *lfmax;           /* per request: [nblocks] largest LF value of each block */
+    uint4 *const *brec;            /* per request, per block: blk, binfo, bslot | first diagonal-start slot << 16,
+                                    * largest LF value of its bins (float bits, at least 0) */
     const int32_t *job_list;       /* requests of the launch */
     const int64_t *blk_off;        /* [njobs + 1] first flat block of each listed request */
     int32_t njobs;
@@ -201,8 +202,8 @@ struct BlockLfParams {
 struct BatchDrawParams {
     const CrawlJob *jobs;
     const unsigned char *const *plans;   /* per request */
-    float *const *ms;              /* per request: slot densities */
-    float *const *lfmax;           /* per request: per-block LF maxima (null: exact test for every bin) */
+    const float2 *const *ms;       /* per request: slot densities (SlotDensityParams::ms) */
+    const uint4 *const *brec;      /* per request: block records (null: exact test for every bin) */
     const uint32_t *items;         /* (request << 16) | first of 32 consecutive streams */
     int32_t nitems;
     uint32_t *next_item;           /* work-queue counter */
@@ -213,7 +214,7 @@ struct BatchDrawParams {
     int32_t off_view, off_tab, off_ev, warp_bytes;   /* per-warp shared-memory layout (batch_draw_warp_bytes) */
 };
 cudaError_t launch_slot_density(const SlotDensityParams &P, int model_type, cudaStream_t s);
-cudaError_t launch_block_lfmax(const BlockLfParams &P, cudaStream_t s);
+cudaError_t launch_block_records(const BlockLfParams &P, cudaStream_t s);
 size_t batch_draw_warp_bytes(int max_tab, BatchDrawParams *P);
 /* bound: every request of P takes the block bound of its expected counts (see
  * batch_draw_kernel); otherwise every bin is tested exactly */

@@ -154,6 +154,7 @@ struct ReqInfo {
      * the components it had not delivered yet */
     bool overflow = false;
     std::vector<int32_t> delivered;    /* components delivered by batched passes */
+    bool deferred = false;             /* left for a later call by the admission hook */
     int group = 0;
     int slot = -1;
     double cost = 0;
@@ -206,14 +207,14 @@ struct MultiWS {
     Grow<const unsigned char *> plans;
     Grow<int32_t> pixoff;
     Grow<gfk::IntegPlanDesc> pdesc;
-    Grow<float> msbuf;                      /* batched draw: slot densities of the chunk's pixels */
-    Grow<float *> msptr;
+    Grow<float2> msbuf;                     /* batched draw: slot densities of the chunk's pixels */
+    Grow<float2 *> msptr;
     Grow<int32_t> joblist, chunkoff;
     Grow<EventRecord> ev;
     Grow<int64_t> k64, off64;
     Grow<uint32_t> gitems;                  /* batched draw: (request << 16) | first of 32 streams */
-    Grow<float> lfmax;                      /* batched draw: per request and block, the largest LF value */
-    Grow<float *> lfmptr;
+    Grow<uint4> brec;                       /* batched draw: per request and block, the bound walk's record */
+    Grow<uint4 *> brecptr;
     Grow<int64_t> blkoff;
     gf_table out;
     gf_table out2;                          /* host delivery: passes alternate between out and out2 */
@@ -434,7 +435,7 @@ int forward_plain_host(void *u, int32_t model, const gf_table *dev, int64_t row_
 }
 
 gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, gf_multi_host_callback hcb,
-                    int64_t piece_rows, void *user, gf_catalog_stats *stats)
+                    int64_t piece_rows, void *user, gf_catalog_stats *stats, gfa::Admission *adm)
 {
     GF_TRY(gfa::check_ctx(ctx));
     if (!jobs || njobs <= 0 || njobs > 32767) return fail(GF_E_INVALID, "njobs must be in [1, 32767]");
@@ -801,29 +802,54 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
     }
 
     /* ---- requests generated together ---- */
+    /* device memory of a batched request's draw passes: records, placement, sort and
+     * output columns take about kStarBytes per star of its largest model, events 48
+     * bytes per star at most, and the slot densities of its pixels */
+    const double kStarBytes = 320.0;
+    auto need_of = [&](int j) {
+        double mx = 0;
+        for (int i = 0; i < nmod; i++) mx = std::max(mx, S[j].expected[i] + 8.0 * sqrt(S[j].expected[i]) + 1024.0);
+        int ns = 0;
+        for (int i = 0; i < nmod; i++)
+            if (plan_used[i] && plan_of(j, i)) ns = std::max(ns, plan_nslots[plan_of(j, i)]);
+        return mx * (kStarBytes + 48.0) + 8.0 * (double)jobs[j].npixels * (ns + 1) +
+               16.0 * (double)R[j].hm[0].m.nm * R[j].hm[0].m.nM / GF_BLOCK;
+    };
+    int64_t budget = ctx->multi_budget;
+    if (adm && adm->admit) {
+        /* the caller admits the leading batched requests (in submission order) whose
+         * memory it can grant now; the others are left for a later call */
+        adm->deferred.assign(njobs, 0);
+        std::vector<int> cand;
+        for (int j = 0; j < njobs; j++)
+            if (!R[j].plain) cand.push_back(j);
+        if (!cand.empty()) {
+            std::vector<double> need(cand.size());
+            for (size_t k = 0; k < cand.size(); k++) need[k] = need_of(cand[k]);
+            int64_t granted = 0;
+            int32_t take = adm->admit(adm->user, need.data(), (int32_t)cand.size(), &granted);
+            take = std::max<int32_t>(1, std::min<int32_t>(take, (int32_t)cand.size()));
+            for (size_t k = (size_t)take; k < cand.size(); k++) {
+                R[cand[k]].deferred = true;
+                adm->deferred[cand[k]] = 1;
+            }
+            if (granted > 0) budget = granted;
+        }
+    }
     std::vector<int> batched_all;
     for (int j : order_all)
-        if (!R[j].plain) batched_all.push_back(j);
-    /* chunks of requests whose draw passes fit the memory budget: records, placement,
-     * sort and output columns take about kStarBytes per star of the largest model */
-    const double kStarBytes = 320.0;
-    int64_t budget = ctx->multi_budget;
+        if (!R[j].plain && !R[j].deferred) batched_all.push_back(j);
     if (budget <= 0) {
         size_t fr = 0, tot = 0;
         GF_CUDA(cudaMemGetInfo(&fr, &tot));
         budget = (int64_t)(0.6 * (double)fr);
     }
+    /* chunks of requests whose draw passes fit the memory budget */
     std::vector<std::vector<int>> chunks;
     {
         double used = 0;
         for (int j : batched_all) {
-            double mx = 0;
-            for (int i = 0; i < nmod; i++) mx = std::max(mx, S[j].expected[i] + 8.0 * sqrt(S[j].expected[i]) + 1024.0);
-            /* + events (48 bytes per star at most) and the slot densities of the request's pixels */
-            int ns = 0;
-            for (int i = 0; i < nmod; i++)
-                if (plan_used[i] && plan_of(j, i)) ns = std::max(ns, plan_nslots[plan_of(j, i)]);
-            const double need = mx * (kStarBytes + 48.0) + 4.0 * (double)jobs[j].npixels * (ns + 2);
+            const double need = need_of(j);
             if (chunks.empty() || (used + need > (double)budget && !chunks.back().empty())) {
                 chunks.emplace_back();
                 used = 0;
@@ -950,7 +976,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
             if (plan_used[i]) {
                 /* slot densities of the chunk's pixels */
                 std::vector<const unsigned char *> jp(njobs, nullptr);
-                std::vector<float *> jm(njobs, nullptr);
+                std::vector<float2 *> jm(njobs, nullptr);
                 std::vector<int32_t> jl, poff;
                 std::vector<int64_t> moff(njobs, 0);
                 int64_t ms_total = 0;
@@ -958,7 +984,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                 for (int j : batched) {
                     jp[j] = plan_of(j, i);
                     moff[j] = ms_total;
-                    ms_total += (int64_t)jobs[j].npixels * (plan_nslots[jp[j]] + 2);
+                    ms_total += (int64_t)jobs[j].npixels * (plan_nslots[jp[j]] + 1);
                     jl.push_back(j);
                     poff.push_back(tp);
                     tp += jobs[j].npixels;
@@ -981,9 +1007,9 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                     ProfScope ps(ctx, GF_PROF_SLOTS);
                     GF_CUDA(gfk::launch_slot_density(SD, mtype, st));
                 }
-                /* the largest LF value of every block of every request (bounds of the draw's test) */
+                /* the record of every block of every request (the draw's bound walk) */
                 {
-                    std::vector<float *> lp(njobs, nullptr);
+                    std::vector<uint4 *> lp(njobs, nullptr);
                     std::vector<int64_t> boff;
                     int64_t nb_total = 0;
                     for (int j : batched) {
@@ -991,24 +1017,24 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                         nb_total += (int64_t)R[j].hm[i].m.nm * R[j].hm[i].m.nM / GF_BLOCK;
                     }
                     boff.push_back(nb_total);
-                    GF_TRY(ws.lfmax.need((size_t)std::max<int64_t>(nb_total, 1)));
-                    for (size_t q = 0; q < batched.size(); q++) lp[batched[q]] = ws.lfmax.p + boff[q];
-                    GF_TRY(ws.lfmptr.need((size_t)njobs));
+                    GF_TRY(ws.brec.need((size_t)std::max<int64_t>(nb_total, 1)));
+                    for (size_t q = 0; q < batched.size(); q++) lp[batched[q]] = ws.brec.p + boff[q];
+                    GF_TRY(ws.brecptr.need((size_t)njobs));
                     GF_TRY(ws.blkoff.need(boff.size()));
-                    GF_CUDA(cudaMemcpyAsync(ws.lfmptr.p, lp.data(), sizeof(void *) * (size_t)njobs, cudaMemcpyHostToDevice, st));
+                    GF_CUDA(cudaMemcpyAsync(ws.brecptr.p, lp.data(), sizeof(void *) * (size_t)njobs, cudaMemcpyHostToDevice, st));
                     GF_CUDA(cudaMemcpyAsync(ws.blkoff.p, boff.data(), 8 * boff.size(), cudaMemcpyHostToDevice, st));
                     gfk::BlockLfParams BL;
-                    BL.jobs = d_jobs; BL.plans = ws.plans.p; BL.lfmax = ws.lfmptr.p;
+                    BL.jobs = d_jobs; BL.plans = ws.plans.p; BL.brec = ws.brecptr.p;
                     BL.job_list = ws.joblist.p; BL.blk_off = ws.blkoff.p;
                     BL.njobs = (int32_t)batched.size(); BL.total = nb_total;
                     ProfScope ps(ctx, GF_PROF_SLOTS);
-                    GF_CUDA(gfk::launch_block_lfmax(BL, st));
+                    GF_CUDA(gfk::launch_block_records(BL, st));
                     /* the host vectors are read by the copies above before they go out of scope */
                     GF_CUDA(cudaStreamSynchronize(st));
                 }
                 gfk::BatchDrawParams B;
                 memset(&B, 0, sizeof(B));
-                B.lfmax = ws.lfmptr.p;
+                B.brec = ws.brecptr.p;
                 if (gfk::batch_draw_warp_bytes(max_tab(i, batched), &B) > 200 * 1024)
                     return fail(GF_E_UNSUPPORTED, "magnitude grid too large for the batched draw");
                 B.jobs = d_jobs; B.plans = ws.plans.p; B.ms = ws.msptr.p;
@@ -1289,7 +1315,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         if (hd.stop) return fail(GF_E_STATE, "stopped by the host callback");
     }
     for (int j = 0; j < njobs; j++) {
-        if (!R[j].plain) continue;
+        if (!R[j].plain || R[j].deferred) continue;
         if (to_host) {
             PlainHostForward f;
             f.hd = &hd; f.ctx = ctx; f.njobs = njobs; f.job = j;
@@ -1327,21 +1353,29 @@ int counting_multi(void *u, int32_t model, const gf_table *t, const int64_t *rb,
  * and retries a failed allocation (cux.cpp:189-198).  Every request's streams
  * are seeded again, so the retry is the same run. */
 gf_status run_multi_retry(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, gf_multi_host_callback hcb,
-                          int64_t piece_rows, void *user, gf_catalog_stats *stats)
+                          int64_t piece_rows, void *user, gf_catalog_stats *stats, gfa::Admission *adm = nullptr)
 {
     CountingMulti c;
     c.cb = cb ? cb : hcb;
     c.user = user;
     gf_multi_callback d = cb ? counting_multi : nullptr;
     gf_multi_host_callback h = hcb ? counting_multi : nullptr;
-    gf_status st = run_multi(ctx, jobs, njobs, d, h, piece_rows, &c, stats);
+    gf_status st = run_multi(ctx, jobs, njobs, d, h, piece_rows, &c, stats, adm);
     if (st == GF_E_OOM && c.calls.load() == 0) {
         gfa::release_caches(ctx);
-        st = run_multi(ctx, jobs, njobs, d, h, piece_rows, &c, stats);
+        st = run_multi(ctx, jobs, njobs, d, h, piece_rows, &c, stats, adm);
     }
     return st;
 }
 }  // namespace
+
+namespace gfa {
+gf_status catalog_run_multi_admitted(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, void *user,
+                                     gf_catalog_stats *stats, Admission *adm)
+{
+    return run_multi_retry(ctx, jobs, njobs, cb, nullptr, 0, user, stats, adm);
+}
+}  // namespace gfa
 
 extern "C" gf_status gf_catalog_run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_callback cb, void *user,
                                           gf_catalog_stats *stats)

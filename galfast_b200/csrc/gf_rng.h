@@ -27,6 +27,12 @@
 
 namespace gfr {
 
+/* The range of mu (and relative margin) within which the hardware __expf(-mu)
+ * brackets the correctly rounded exp(-mu) (see poisson_small). */
+#define GF_FASTEXP_MIN_MU (-0.01f)
+#define GF_FASTEXP_MAX_MU 10.5f
+#define GF_FASTEXP_MARGIN 1.0e-5f
+
 /* 2.32830643708e-10f == 2^-32 exactly */
 #define GF_MWC_SCALE 2.32830643708e-10f
 
@@ -162,8 +168,6 @@ struct Mwc {
     /* poisson: cuda_rng.h:344-376 */
     GFR_HD unsigned int poisson(float mu)
     {
-        float emu;
-        float prod = 1.0f;
         unsigned int k = 0;
         while (mu > 10) {
             unsigned int m = (unsigned int)(mu * (7.0 / 8.0));
@@ -175,7 +179,38 @@ struct Mwc {
                 mu -= X;
             }
         }
-        emu = gfm::expf_(-mu);
+        return k + poisson_small(mu);
+    }
+
+    /* the sampler's last stage (mu <= 10): multiply uniforms until the product
+     * falls to exp(-mu) or below (cuda_rng.h:370-375) */
+    GFR_HD unsigned int poisson_small(float mu)
+    {
+#ifdef __CUDA_ARCH__
+        if (mu >= GF_FASTEXP_MIN_MU && mu <= GF_FASTEXP_MAX_MU) {
+            /* exp(-mu) lies within GF_FASTEXP_MARGIN (relative) of the hardware
+             * __expf(-mu) for every float mu in this range (checked exhaustively by
+             * tests/cpp/expf_margin_check.cu), so a product outside the bracket is
+             * decided without it; the correctly rounded value is formed only for a
+             * product inside the bracket */
+            const float ea = __expf(-mu);
+            const float lo = ea * (1.0f - GF_FASTEXP_MARGIN), hi = ea * (1.0f + GF_FASTEXP_MARGIN);
+            float prod = 1.0f, emu = -1.0f;
+            unsigned int k = 0;
+            for (;;) {
+                prod *= uniform();
+                k++;
+                if (prod > hi) continue;
+                if (prod <= lo) break;
+                if (emu < 0.0f) emu = gfm::expf_(-mu);
+                if (!(prod > emu)) break;
+            }
+            return k - 1;
+        }
+#endif
+        const float emu = gfm::expf_(-mu);
+        float prod = 1.0f;
+        unsigned int k = 0;
         do {
             prod *= uniform();
             k++;
@@ -183,6 +218,20 @@ struct Mwc {
         return k - 1;
     }
 };
+
+#ifdef __CUDACC__
+/* u > exp(-mu), the sampler's first test (a bin has stars), decided with the
+ * bracket of poisson_small when mu is in its range */
+__device__ __forceinline__ bool exceeds_exp_neg(float u, float mu)
+{
+    if (mu >= GF_FASTEXP_MIN_MU && mu <= GF_FASTEXP_MAX_MU) {
+        const float ea = __expf(-mu);
+        if (u > ea * (1.0f + GF_FASTEXP_MARGIN)) return true;
+        if (u <= ea * (1.0f - GF_FASTEXP_MARGIN)) return false;
+    }
+    return u > gfm::expf_(-mu);
+}
+#endif
 
 /* The largest x in [0, 2^32) whose uniform 2^-32 * (float)x (x rounded to float,
  * to nearest even, then scaled exactly) is <= thr, or -1 when none is: a test

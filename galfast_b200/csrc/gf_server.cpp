@@ -1,34 +1,119 @@
 /*
  * gf_server.cpp -- the serving form: continuous batching of catalog requests.
  *
- * Requests are submitted at any time from any thread.  Each worker thread owns
- * a context (its own CUDA stream, streams, workspace) and repeatedly takes the
- * compatible requests waiting at the head of the queue, reserves its share of
- * the device-memory budget and generates them together with
- * gf_catalog_run_multi, whose chunking admits requests by their output-memory
- * estimate (expected stars from the integrate pass).  A request that arrives
- * while a batch is on the GPU is taken by the next worker that frees up, so
- * with two or more workers its work overlaps with the running batch on the
- * device.  Each request's rows are exactly those gf_catalog_run gives it alone,
- * whatever it was batched with.
+ * Requests are submitted at any time from any thread; submit copies the job and
+ * everything it points to, so the caller's memory may be reused at once.  Each
+ * worker thread owns a context (its own CUDA stream, streams, workspace) and
+ * repeatedly takes the compatible requests waiting at the head of the queue and
+ * generates them together (gf_catalog_run_multi).  Admission happens after the
+ * call's integrate pass, when each request's device-memory need is known from
+ * its expected star counts: the worker reserves, from the server's memory
+ * budget, the needs of the leading requests that fit what is free and generates
+ * those; the others go back to the head of the queue, where they join the
+ * requests that arrived meanwhile in the next call of whichever worker is free.
+ * A batch thus holds one memory-budget pass, a request waits at most for the
+ * passes ahead of it, and batches of several workers run side by side on the
+ * device when their reservations fit together.  Each request's rows are exactly
+ * those gf_catalog_run gives it alone, whatever it was batched with.
  *
  * No counterpart in the reference, which generates one catalog per process.
  */
-#include "../../include/galfast_b200.h"
+#include "gf_ctx.h"
 
 #include <algorithm>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
 
 namespace {
 
+/* a job with its own copies of the arrays and configurations it points to */
+struct OwnedJob {
+    gf_job job;
+    std::vector<gf_pencil_beam> pixels;
+    std::vector<float> ammin;
+    std::vector<gf_model_config> models;
+    std::vector<std::vector<double>> lf_M, lf_phi;
+    gf_footprint foot;
+    gf_fixedfeh_config feh;
+    gf_bond2010_config kin;
+    gf_photometry_config phot;
+    std::vector<float> colors;
+    std::vector<uint8_t> eflags;
+    gf_photoerr_config perr;
+    std::vector<double> perr_mag, perr_sigma;
+    gf_vel2pm_config v2pm;
+    gf_feh_config feh_ivezic;
+    gf_gaussfeh_config feh_gauss;
+};
+
+template <class T>
+const T *copy_one(const T *src, T &dst)
+{
+    if (!src) return nullptr;
+    dst = *src;
+    return &dst;
+}
+
+/* nullptr when the job's arrays cannot be copied (negative or absurd sizes) */
+std::shared_ptr<OwnedJob> own(const gf_job &j)
+{
+    auto o = std::make_shared<OwnedJob>();
+    o->job = j;
+    if (j.npixels < 0 || j.nmodels < 0 || j.nmodels > GF_MAX_MODELS) return nullptr;
+    if (j.pixels) {
+        o->pixels.assign(j.pixels, j.pixels + j.npixels);
+        o->job.pixels = o->pixels.data();
+    }
+    if (j.beam_ammin) {
+        o->ammin.assign(j.beam_ammin, j.beam_ammin + j.npixels);
+        o->job.beam_ammin = o->ammin.data();
+    }
+    if (j.models) {
+        o->models.assign(j.models, j.models + j.nmodels);
+        o->lf_M.resize(j.nmodels);
+        o->lf_phi.resize(j.nmodels);
+        for (int i = 0; i < j.nmodels; i++) {
+            gf_model_config &m = o->models[i];
+            if (m.lf_n < 0) return nullptr;
+            if (m.lf_M) { o->lf_M[i].assign(m.lf_M, m.lf_M + m.lf_n); m.lf_M = o->lf_M[i].data(); }
+            if (m.lf_phi) { o->lf_phi[i].assign(m.lf_phi, m.lf_phi + m.lf_n); m.lf_phi = o->lf_phi[i].data(); }
+        }
+        o->job.models = o->models.data();
+    }
+    o->job.foot = copy_one(j.foot, o->foot);
+    o->job.feh = copy_one(j.feh, o->feh);
+    o->job.kin = copy_one(j.kin, o->kin);
+    o->job.v2pm = copy_one(j.v2pm, o->v2pm);
+    o->job.feh_ivezic = copy_one(j.feh_ivezic, o->feh_ivezic);
+    o->job.feh_gauss = copy_one(j.feh_gauss, o->feh_gauss);
+    if (j.phot) {
+        o->phot = *j.phot;
+        if (o->phot.nbands < 1 || o->phot.nMr < 0 || o->phot.nFeH < 0) return nullptr;
+        const size_t n = (size_t)(o->phot.nbands - 1) * (size_t)o->phot.nMr * (size_t)o->phot.nFeH;
+        if (o->phot.colors) { o->colors.assign(o->phot.colors, o->phot.colors + n); o->phot.colors = o->colors.data(); }
+        if (o->phot.eflags) { o->eflags.assign(o->phot.eflags, o->phot.eflags + n); o->phot.eflags = o->eflags.data(); }
+        o->job.phot = &o->phot;
+    }
+    if (j.perr) {
+        o->perr = *j.perr;
+        if (o->perr.nbands < 0 || o->perr.nknots < 0) return nullptr;
+        const size_t n = (size_t)o->perr.nbands * (size_t)o->perr.nknots;
+        if (o->perr.mag) { o->perr_mag.assign(o->perr.mag, o->perr.mag + n); o->perr.mag = o->perr_mag.data(); }
+        if (o->perr.sigma) { o->perr_sigma.assign(o->perr.sigma, o->perr.sigma + n); o->perr.sigma = o->perr_sigma.data(); }
+        o->job.perr = &o->perr;
+    }
+    return o;
+}
+
 struct Request {
     int64_t id;
-    gf_job job;
+    std::shared_ptr<OwnedJob> owned;
     gf_server_rows rows;
     gf_server_done done;
     void *user;
@@ -65,7 +150,6 @@ bool compatible(const gf_job &a, const gf_job &b)
     return model_kinds(a) == model_kinds(b);
 }
 
-
 }  // namespace
 
 struct gf_server {
@@ -73,13 +157,17 @@ struct gf_server {
     int64_t budget = 0;
     int32_t max_batch = 0;
     std::mutex mu;
-    std::condition_variable cv_work, cv_idle;
+    std::condition_variable cv_work, cv_idle, cv_budget;
     std::deque<Request> queue;
     int64_t next_id = 0;
     int64_t inflight = 0;                /* submitted and not yet done */
-    int64_t free_budget = 0;             /* budget not reserved by a running batch */
+    int64_t reserved = 0;                /* device memory reserved by the running batches */
+    int32_t running = 0;                 /* batches holding a reservation */
+    int32_t active = 0;                  /* batches taken from the queue and not finished */
+    bool paused = false;                 /* gf_server_pause: workers take no new batch */
     bool stop = false;
     gf_status first_error = GF_OK;
+    gf_server_info info = {};
     std::vector<std::thread> workers;
 };
 
@@ -101,7 +189,51 @@ int forward_rows(void *u, int32_t model, const gf_table *dev, const int64_t *row
     return 0;
 }
 
-void worker_main(gf_server *s, int64_t share)
+struct Reservation {
+    gf_server *s;
+    int64_t bytes = 0;
+    bool held = false;
+};
+
+void release(Reservation &r)
+{
+    if (!r.held) return;
+    {
+        std::lock_guard<std::mutex> g(r.s->mu);
+        r.s->reserved -= r.bytes;
+        r.s->running--;
+    }
+    r.held = false;
+    r.bytes = 0;
+    r.s->cv_budget.notify_all();
+}
+
+/* the admission hook: wait until the first request's need fits what the running
+ * batches leave free (or nothing else runs: a request larger than the whole budget
+ * then runs alone), reserve the needs of the leading requests that fit */
+int32_t admit(void *u, const double *need, int32_t n, int64_t *budget)
+{
+    Reservation &r = *(Reservation *)u;
+    release(r);                       /* a retried call reserves afresh */
+    gf_server *s = r.s;
+    std::unique_lock<std::mutex> g(s->mu);
+    s->cv_budget.wait(g, [&] { return (double)(s->budget - s->reserved) >= need[0] || s->running == 0; });
+    const double avail = std::max((double)(s->budget - s->reserved), need[0]);
+    double sum = 0;
+    int32_t k = 0;
+    while (k < n && sum + need[k] <= avail) sum += need[k++];
+    if (k == 0) { k = 1; sum = need[0]; }
+    r.bytes = (int64_t)std::ceil(sum);
+    r.held = true;
+    s->reserved += r.bytes;
+    s->running++;
+    s->info.peak_reserved = std::max(s->info.peak_reserved, s->reserved);
+    s->info.peak_running = std::max(s->info.peak_running, s->running);
+    *budget = std::max<int64_t>(r.bytes, 1);
+    return k;
+}
+
+void worker_main(gf_server *s)
 {
     gf_ctx *ctx = nullptr;
     gf_status st = gf_ctx_create(s->device, &ctx);
@@ -113,40 +245,60 @@ void worker_main(gf_server *s, int64_t share)
     }
     for (;;) {
         std::vector<Request> batch;
-        int64_t reserved = 0;
         {
             std::unique_lock<std::mutex> g(s->mu);
-            s->cv_work.wait(g, [&] { return s->stop || (!s->queue.empty() && s->free_budget > 0); });
+            s->cv_work.wait(g, [&] { return s->stop || (!s->queue.empty() && !s->paused); });
             if (s->queue.empty() && s->stop) break;
-            if (s->queue.empty()) continue;
+            if (s->queue.empty() || (s->paused && !s->stop)) continue;
             /* the compatible requests at the head of the queue, in arrival order */
             batch.push_back(s->queue.front());
             s->queue.pop_front();
-            while (!s->queue.empty() && (int32_t)batch.size() < s->max_batch && compatible(batch[0].job, s->queue.front().job)) {
+            while (!s->queue.empty() && (int32_t)batch.size() < s->max_batch &&
+                   compatible(batch[0].owned->job, s->queue.front().owned->job)) {
                 batch.push_back(s->queue.front());
                 s->queue.pop_front();
             }
-            reserved = std::min(share, s->free_budget);
-            s->free_budget -= reserved;
+            s->active++;
         }
         std::vector<gf_job> jobs;
-        for (auto &r : batch) jobs.push_back(r.job);
+        for (auto &r : batch) jobs.push_back(r.owned->job);
         std::vector<gf_catalog_stats> stats(batch.size());
         BatchForward f;
         f.reqs = &batch;
         f.ctx = ctx;
-        if (ctx) gf_multi_set_memory_budget(ctx, reserved);
-        st = gf_catalog_run_multi(ctx, jobs.data(), (int32_t)jobs.size(), forward_rows, &f, stats.data());
+        Reservation res;
+        res.s = s;
+        gfa::Admission adm;
+        adm.admit = admit;
+        adm.user = &res;
+        st = ctx ? gfa::catalog_run_multi_admitted(ctx, jobs.data(), (int32_t)jobs.size(), forward_rows, &f, stats.data(), &adm)
+                 : GF_E_STATE;
+        release(res);
+        /* deferred requests go back to the head of the queue in arrival order, unless the call failed */
+        std::vector<size_t> finished;
+        int64_t ndeferred = 0;
         {
             std::lock_guard<std::mutex> g(s->mu);
-            s->free_budget += reserved;
+            for (size_t j = batch.size(); j-- > 0;) {
+                if (st == GF_OK && j < adm.deferred.size() && adm.deferred[j]) {
+                    s->queue.push_front(batch[j]);
+                    ndeferred++;
+                }
+            }
+            s->info.runs++;
+            s->info.deferred += ndeferred;
+            s->active--;
         }
-        s->cv_work.notify_all();
-        for (size_t j = 0; j < batch.size(); j++)
+        if (ndeferred) s->cv_work.notify_all();
+        for (size_t j = 0; j < batch.size(); j++) {
+            if (st == GF_OK && j < adm.deferred.size() && adm.deferred[j]) continue;
             if (batch[j].done) batch[j].done(batch[j].user, batch[j].id, st, &stats[j]);
+            finished.push_back(j);
+        }
         {
             std::lock_guard<std::mutex> g(s->mu);
-            s->inflight -= (int64_t)batch.size();
+            s->inflight -= (int64_t)finished.size();
+            s->info.completed += (int64_t)finished.size();
             if (st != GF_OK && s->first_error == GF_OK) s->first_error = st;
         }
         s->cv_idle.notify_all();
@@ -164,10 +316,8 @@ gf_status gf_server_create(int32_t device, int32_t nworkers, int64_t memory_budg
     gf_server *s = new gf_server();
     s->device = device;
     s->budget = memory_budget;
-    s->free_budget = memory_budget;
     s->max_batch = max_batch;
-    const int64_t share = memory_budget / nworkers;
-    for (int w = 0; w < nworkers; w++) s->workers.emplace_back(worker_main, s, share);
+    for (int w = 0; w < nworkers; w++) s->workers.emplace_back(worker_main, s);
     *out = s;
     return GF_OK;
 }
@@ -176,12 +326,14 @@ gf_status gf_server_submit(gf_server *s, const gf_job *job, gf_server_rows rows,
                            int64_t *request)
 {
     if (!s || !job) return GF_E_INVALID;
+    std::shared_ptr<OwnedJob> o = own(*job);
+    if (!o) return GF_E_INVALID;
     {
         std::lock_guard<std::mutex> g(s->mu);
         if (s->stop) return GF_E_STATE;
         Request r;
         r.id = s->next_id++;
-        r.job = *job;
+        r.owned = std::move(o);
         r.rows = rows;
         r.done = done;
         r.user = user;
@@ -199,6 +351,27 @@ gf_status gf_server_drain(gf_server *s)
     std::unique_lock<std::mutex> g(s->mu);
     s->cv_idle.wait(g, [&] { return s->inflight == 0; });
     return s->first_error;
+}
+
+gf_status gf_server_get_info(gf_server *s, gf_server_info *out)
+{
+    if (!s || !out) return GF_E_INVALID;
+    std::lock_guard<std::mutex> g(s->mu);
+    *out = s->info;
+    out->queued = (int32_t)s->queue.size();
+    out->active = s->active;
+    return GF_OK;
+}
+
+gf_status gf_server_pause(gf_server *s, int32_t paused)
+{
+    if (!s) return GF_E_INVALID;
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        s->paused = paused != 0;
+    }
+    s->cv_work.notify_all();
+    return GF_OK;
 }
 
 gf_status gf_server_destroy(gf_server *s)

@@ -224,7 +224,7 @@ __device__ __noinline__ AnchorX anchor_cold(const SkyModel &m, const SkyGeom &g,
  * or mu > 10 (the branch that does not compare with exp(-mu) at all). */
 __device__ __noinline__ bool has_stars(float u, float mu)
 {
-    return mu > 10.f || u > gfm::expf_(-mu);
+    return mu > 10.f || gfr::exceeds_exp_neg(u, mu);
 }
 
 /* A bin with stars found by phase B: thread fL = 32 fw + fl of the CTA, bin es of

@@ -1,6 +1,7 @@
 /*
- * gf_textout.cpp -- the catalog text writer: galfast's os_textout output module
- * (src/pipeline.cpp:199-289) over host tables of this library.
+ * gf_textout.cpp -- the catalog writers: galfast's os_textout output module
+ * (src/pipeline.cpp:199-289) and os_fitsout (pipeline.cpp:767-1035) over host
+ * tables of this library.
  *
  * The file is the reference's: a header line "# " followed by the definition of
  * every output column and a space (otable::serialize_header,
@@ -19,6 +20,13 @@
  * fixed-point routine (the correctly rounded decimal of the binary value,
  * ties to even, as glibc's printf), rows are formatted in parallel pieces on
  * host threads and written in order.
+ *
+ * The FITS catalog has os_fitsout's layout, written from the FITS standard (no
+ * CFITSIO): an empty primary HDU, a binary table CATALOG with one column per
+ * output column (TTYPE its primary name, TFORM its width and type code: D
+ * double, E float, J int) and one big-endian row per visible row, then a binary
+ * table METADATA with one row whose string column HEADER holds the column
+ * definitions of the text header.
  */
 #include "../../include/galfast_b200.h"
 #include "gf_launch.h"
@@ -241,6 +249,12 @@ struct gf_textout {
     int64_t bytes = 0;
     bool failed = false;
     std::mutex mu;          /* one write at a time */
+    /* FITS catalogs (gf_fitsout_open) */
+    bool fits = false;
+    int64_t row_bytes = 0;          /* NAXIS1 of the CATALOG table */
+    long naxis2_at = 0;             /* file offset of its NAXIS2 card */
+    int64_t data_bytes = 0;         /* bytes of table rows written */
+    std::string header_def;         /* the column definitions (METADATA extension) */
 };
 
 namespace {
@@ -351,9 +365,186 @@ gf_status tfail(gf_status s, const std::string &m)
     return s;
 }
 
+/* ---------------- FITS (os_fitsout, src/pipeline.cpp:767-1035) ---------------- */
+
+/* One 80-character header card (FITS standard 4.0, section 4.1): the keyword in
+ * columns 1-8, "= " in 9-10, then a fixed-format value: integers and logicals
+ * right-justified to column 30, strings quoted from column 11 and padded to at
+ * least 8 characters inside the quotes. */
+std::string fits_card(const std::string &key, const std::string &value, bool quoted)
+{
+    std::string c = key;
+    c.resize(8, ' ');
+    if (key != "END") {
+        c += "= ";
+        if (quoted) {
+            std::string v;
+            for (char ch : value) { v += ch; if (ch == '\'') v += '\''; }
+            if (v.size() < 8) v.resize(8, ' ');
+            c += "'" + v + "'";
+        } else {
+            std::string v = value;
+            if (v.size() < 20) v = std::string(20 - v.size(), ' ') + v;
+            c += v;
+        }
+    }
+    c.resize(80, ' ');
+    return c;
+}
+
+std::string fits_pad(std::string h)
+{
+    h.resize((h.size() + 2879) / 2880 * 2880, ' ');
+    return h;
+}
+
+char fits_code(Kind k) { return k == F64 ? 'D' : k == F32 ? 'E' : 'J'; }
+size_t kind_bytes(Kind k) { return k == F64 ? 8 : 4; }
+
+/* the primary name of a column (its definition up to "[" or "{") */
+std::string primary_name(const std::string &def) { return def.substr(0, def.find_first_of("[{")); }
+
+inline void put_be32(unsigned char *d, uint32_t v)
+{
+    d[0] = (unsigned char)(v >> 24); d[1] = (unsigned char)(v >> 16); d[2] = (unsigned char)(v >> 8); d[3] = (unsigned char)v;
+}
+inline void put_be64(unsigned char *d, uint64_t v)
+{
+    put_be32(d, (uint32_t)(v >> 32));
+    put_be32(d + 4, (uint32_t)v);
+}
+
+/* the rows [r0, r1) of t that are not hidden, as big-endian FITS table rows */
+void pack_rows(const gf_textout &w, const gf_table &t, int64_t r0, int64_t r1, std::string &out, int64_t &nrows)
+{
+    const size_t P = (size_t)t.capacity;
+    const int32_t *hidden = t.hidden;
+    std::vector<unsigned char> row((size_t)w.row_bytes);
+    nrows = 0;
+    for (int64_t r = r0; r < r1; r++) {
+        if (hidden && hidden[r]) continue;
+        unsigned char *d = row.data();
+        for (const Field &f : w.fields) {
+            for (int k = 0; k < f.ncomp; k++) {
+                const size_t idx = (size_t)k * P + (size_t)r;
+                if (f.kind == F64) {
+                    uint64_t b;
+                    memcpy(&b, &col_ptr<double>(t, f.col_off)[idx], 8);
+                    put_be64(d, b);
+                    d += 8;
+                } else if (f.kind == F32) {
+                    uint32_t b;
+                    memcpy(&b, &col_ptr<float>(t, f.col_off)[idx], 4);
+                    put_be32(d, b);
+                    d += 4;
+                } else {
+                    int32_t v = col_ptr<int32_t>(t, f.col_off)[idx];
+                    if (f.comp_map && v >= 0 && v < (int32_t)w.comp_ids.size()) v = w.comp_ids[v];
+                    put_be32(d, (uint32_t)v);
+                    d += 4;
+                }
+            }
+        }
+        out.append((const char *)row.data(), row.size());
+        nrows++;
+    }
+}
+
+/* the header of a binary-table extension; *naxis2_at receives the offset of the
+ * NAXIS2 card within it */
+std::string bintable_header(int64_t naxis1, int64_t naxis2, const std::vector<std::pair<std::string, std::string>> &cols,
+                            const std::string &extname, size_t *naxis2_at)
+{
+    std::string h;
+    h += fits_card("XTENSION", "BINTABLE", true);
+    h += fits_card("BITPIX", "8", false);
+    h += fits_card("NAXIS", "2", false);
+    h += fits_card("NAXIS1", std::to_string(naxis1), false);
+    if (naxis2_at) *naxis2_at = h.size();
+    h += fits_card("NAXIS2", std::to_string(naxis2), false);
+    h += fits_card("PCOUNT", "0", false);
+    h += fits_card("GCOUNT", "1", false);
+    h += fits_card("TFIELDS", std::to_string(cols.size()), false);
+    for (size_t i = 0; i < cols.size(); i++) {
+        h += fits_card("TTYPE" + std::to_string(i + 1), cols[i].first, true);
+        h += fits_card("TFORM" + std::to_string(i + 1), cols[i].second, true);
+    }
+    h += fits_card("EXTNAME", extname, true);
+    h += fits_card("END", "", false);
+    return fits_pad(h);
+}
+
+bool put(gf_textout *w, const std::string &b)
+{
+    if (fwrite(b.data(), 1, b.size(), w->fp) != b.size()) return false;
+    w->bytes += (int64_t)b.size();
+    return true;
+}
+
+/* close a FITS catalog: pad the CATALOG rows to a whole record, write the row
+ * count into its header, and append the METADATA extension (one row, one
+ * string column HEADER holding the column definitions, as os_fitsout's
+ * destructor writes it) */
+bool fits_finish(gf_textout *w)
+{
+    const int64_t pad = (2880 - w->data_bytes % 2880) % 2880;
+    if (!put(w, std::string((size_t)pad, '\0'))) return false;
+    const long end = ftell(w->fp);
+    if (fseek(w->fp, w->naxis2_at, SEEK_SET) != 0) return false;
+    const std::string c = fits_card("NAXIS2", std::to_string(w->rows), false);
+    if (fwrite(c.data(), 1, c.size(), w->fp) != c.size()) return false;
+    if (fseek(w->fp, end, SEEK_SET) != 0) return false;
+    const std::string &hd = w->header_def;
+    const int64_t len = std::max<int64_t>((int64_t)hd.size(), 1);
+    if (!put(w, bintable_header(len, 1, {{"HEADER", std::to_string(len) + "A"}}, "METADATA", nullptr))) return false;
+    std::string data = hd;
+    data.resize((size_t)len, '\0');
+    data.resize(((size_t)len + 2879) / 2880 * 2880, '\0');
+    return put(w, data);
+}
+
 }  // namespace
 
 extern "C" {
+
+gf_status gf_fitsout_open(const char *path, const gf_textout_config *cfg, gf_textout **out)
+{
+    if (!path || !cfg || !out) return tfail(GF_E_INVALID, "invalid FITS output arguments");
+    if (cfg->nbands < 0 || cfg->nbands > GF_MAX_BANDS) return tfail(GF_E_INVALID, "band count out of range");
+    if (cfg->pm_coordsys < -1 || cfg->pm_coordsys > 1) return tfail(GF_E_INVALID, "pm_coordsys must be -1, 0 or 1");
+    gf_textout *w = new gf_textout();
+    w->fits = true;
+    w->fp = fopen(path, "w+b");
+    if (!w->fp) {
+        delete w;
+        return tfail(GF_E_INVALID, std::string("cannot open ") + path);
+    }
+    setvbuf(w->fp, nullptr, _IOFBF, (size_t)8 << 20);
+    std::vector<std::pair<std::string, std::string>> cols;
+    for (auto &c : output_columns(*cfg)) {
+        w->header_def += c.def + " ";
+        w->fields.push_back(c.f);
+        cols.push_back({primary_name(c.def), std::to_string(c.f.ncomp) + fits_code(c.f.kind)});
+        w->row_bytes += (int64_t)c.f.ncomp * (int64_t)kind_bytes(c.f.kind);
+    }
+    if (cfg->version && cfg->version[0]) w->header_def += std::string("\n# generated with galfast version ") + cfg->version;
+    if (cfg->comp_ids && cfg->ncomp > 0) w->comp_ids.assign(cfg->comp_ids, cfg->comp_ids + cfg->ncomp);
+    w->threads = cfg->threads > 0 ? cfg->threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    /* an empty primary HDU, then the CATALOG table (its row count written at close) */
+    std::string primary = fits_card("SIMPLE", "T", false) + fits_card("BITPIX", "8", false) + fits_card("NAXIS", "0", false) +
+                          fits_card("EXTEND", "T", false) + fits_card("END", "", false);
+    size_t at = 0;
+    const std::string cat = bintable_header(w->row_bytes, 0, cols, "CATALOG", &at);
+    primary = fits_pad(primary);
+    w->naxis2_at = (long)(primary.size() + at);
+    if (!put(w, primary) || !put(w, cat)) {
+        fclose(w->fp);
+        delete w;
+        return tfail(GF_E_INVALID, "cannot write the FITS headers");
+    }
+    *out = w;
+    return GF_OK;
+}
 
 gf_status gf_textout_open(const char *path, const gf_textout_config *cfg, gf_textout **out)
 {
@@ -406,8 +597,13 @@ gf_status gf_textout_write(gf_textout *w, const gf_table *host, int64_t begin, i
     std::vector<int64_t> cnt(npieces, 0);
     FmtPool::get().run(npieces, w->threads, [&](int i) {
         const int64_t a = begin + (int64_t)i * piece, b = std::min(end, a + piece);
-        buf[i].reserve((size_t)(b - a) * 256);
-        format_rows(*w, *host, a, b, buf[i], cnt[i]);
+        if (w->fits) {
+            buf[i].reserve((size_t)(b - a) * (size_t)w->row_bytes);
+            pack_rows(*w, *host, a, b, buf[i], cnt[i]);
+        } else {
+            buf[i].reserve((size_t)(b - a) * 256);
+            format_rows(*w, *host, a, b, buf[i], cnt[i]);
+        }
     });
     for (int i = 0; i < npieces; i++) {
         if (fwrite(buf[i].data(), 1, buf[i].size(), w->fp) != buf[i].size()) {
@@ -416,6 +612,7 @@ gf_status gf_textout_write(gf_textout *w, const gf_table *host, int64_t begin, i
         }
         w->rows += cnt[i];
         w->bytes += (int64_t)buf[i].size();
+        w->data_bytes += (int64_t)buf[i].size();
     }
     return GF_OK;
 }
@@ -436,6 +633,7 @@ gf_status gf_textout_close(gf_textout *w, int64_t *rows, int64_t *bytes)
 {
     if (!w) return GF_OK;
     gf_status st = w->failed ? GF_E_INVALID : GF_OK;
+    if (w->fits && w->fp && st == GF_OK && !fits_finish(w)) st = tfail(GF_E_INVALID, "cannot finish the FITS file");
     if (w->fp && fclose(w->fp) != 0) st = tfail(GF_E_INVALID, "close error");
     if (rows) *rows = w->rows;
     if (bytes) *bytes = w->bytes;

@@ -540,17 +540,35 @@ typedef void (*gf_server_done)(void *user, int64_t request, gf_status status, co
 
 /* A request server on one device: nworkers worker threads, each with its own
  * context and CUDA stream, take the compatible requests waiting at the head of
- * the queue and generate them together (gf_catalog_run_multi) within their
- * share of memory_budget bytes of device memory; requests that arrive while
- * others run are taken by the next free worker, so batches overlap on the GPU.
- * max_batch caps the requests of one batch.  No counterpart in the reference. */
+ * the queue (at most max_batch) and generate them together.  After a batch's
+ * integrate pass each request's device-memory need is known from its expected
+ * star counts; the worker reserves, from memory_budget bytes shared by all
+ * workers, the needs of the leading requests that fit what the running batches
+ * leave free, generates those, and returns the others to the head of the queue,
+ * where they join the requests that arrived meanwhile in the next batch.  Batches
+ * of several workers run side by side on the device when their reservations fit
+ * together.  No counterpart in the reference. */
 gf_status gf_server_create(int32_t device, int32_t nworkers, int64_t memory_budget, int32_t max_batch, gf_server **out);
-/* Queue one request; the job and everything it points to must stay valid until
- * its done callback.  *request receives its id. */
+/* Queue one request.  The job and the arrays and configurations it points to are
+ * copied: the caller's memory may be reused when this returns.  *request
+ * receives its id. */
 gf_status gf_server_submit(gf_server *s, const gf_job *job, gf_server_rows rows, gf_server_done done, void *user,
                            int64_t *request);
 /* Wait until every submitted request is done; returns the first error seen. */
 gf_status gf_server_drain(gf_server *s);
+typedef struct gf_server_info {
+    int64_t runs;              /* batches generated */
+    int64_t completed;         /* requests done (successfully or not) */
+    int64_t deferred;          /* times a request went back to the queue at admission */
+    int64_t peak_reserved;     /* most device memory reserved at once by running batches (bytes) */
+    int32_t peak_running;      /* most batches generating at once */
+    int32_t queued;            /* requests waiting now */
+    int32_t active;            /* batches taken from the queue and not finished, now */
+    int32_t pad;
+} gf_server_info;
+gf_status gf_server_get_info(gf_server *s, gf_server_info *out);
+/* paused != 0: the workers take no new batch (running batches finish); 0 resumes */
+gf_status gf_server_pause(gf_server *s, int32_t paused);
 gf_status gf_server_destroy(gf_server *s);
 
 /* ---- expected counts without device allocation ---- */
@@ -610,6 +628,15 @@ gf_status gf_textout_open(const char *path, const gf_textout_config *cfg, gf_tex
 gf_status gf_textout_write(gf_textout *w, const gf_table *host, int64_t begin, int64_t end);
 /* Close the file; rows and bytes written (nullable). */
 gf_status gf_textout_close(gf_textout *w, int64_t *rows, int64_t *bytes);
+
+/* A FITS catalog (os_fitsout, src/pipeline.cpp:767-1035) with the same columns:
+ * an empty primary HDU, a binary table CATALOG (one column per output column,
+ * TTYPE its name, TFORM its width and D/E/J type, big-endian rows of the
+ * visible rows), then a binary table METADATA whose single row holds the
+ * column definitions (and version line) of the text header.  The handle is a
+ * catalog writer like gf_textout_open's: write with gf_textout_write, finish
+ * with gf_textout_close (which writes the row count into the CATALOG header). */
+gf_status gf_fitsout_open(const char *path, const gf_textout_config *cfg, gf_textout **out);
 
 /* One writer per request of a multi-request run: pass gf_textout_multi_sink and
  * a gf_textout_set to gf_catalog_run_multi_host to write every request's

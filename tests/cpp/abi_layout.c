@@ -33,5 +33,6 @@ int main(void)
     SZ(gf_textout_config); OF(gf_textout_config, nbands); OF(gf_textout_config, feh_comp); OF(gf_textout_config, comp_ids);
     OF(gf_textout_config, version); OF(gf_textout_config, threads);
     SZ(gf_textout_set); OF(gf_textout_set, writers);
+    SZ(gf_server_info); OF(gf_server_info, deferred); OF(gf_server_info, peak_running); OF(gf_server_info, active);
     return 0;
 }

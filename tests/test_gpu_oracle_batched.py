@@ -195,3 +195,25 @@ def test_bulge_and_broken_power_law_equal_oracle(lib, multipliers):
     ctx.close()
     compare(ref, got[0], "batched 0")
     compare(ref2, got[1], "batched 1")
+
+
+def test_hardware_exp_brackets_the_exact_exp_for_every_float(tmp_path):
+    """The samplers decide u > exp(-mu) and the Poisson product test with the
+    hardware __expf(-mu) and a relative bracket of 1e-5, forming the correctly
+    rounded exp(-mu) only inside the bracket.  For every float mu in
+    [-0.01, 10.5] the exact value lies inside the bracket
+    (tests/cpp/expf_margin_check.cu, run on the device)."""
+    import os
+    import shutil
+    import subprocess
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    exe = str(tmp_path / "expf_margin")
+    subprocess.run([nvcc, "-O2", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-fmad=false",
+                    "-I", os.path.join(root, "galfast_b200", "csrc"), "-o", exe,
+                    os.path.join(here, "cpp", "expf_margin_check.cu")], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    n, bad, worst = r.stdout.split()
+    assert r.returncode == 0 and int(bad) == 0 and int(n) > 2000000000, r.stdout
+    assert float(worst) < 0.5e-5

@@ -59,7 +59,8 @@ def test_struct_layouts(tmp_path):
               "gf_photometry_config": A.PhotometryConfig, "gf_photoerr_config": A.PhotoerrConfig,
               "gf_vel2pm_config": A.Vel2pmConfig, "gf_skygen_model_info": A.ModelInfo, "gf_job": G.Job,
               "gf_catalog_stats": G.CatalogStats, "gf_precision_report": A.PrecisionReport,
-              "gf_textout_config": G.TextoutConfig, "gf_textout_set": G.TextoutSet}
+              "gf_textout_config": G.TextoutConfig, "gf_textout_set": G.TextoutSet,
+              "gf_server_info": G.ServerInfo}
     checked = 0
     for line in out.split("\n"):
         if not line.strip():

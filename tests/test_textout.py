@@ -213,3 +213,99 @@ def test_multi_request_catalogs_through_the_text_sink(tmp_path, lib):
         wr.close()
         assert_same_text((tmp_path / ("multi%d.txt" % j)).read_text(), p.read_text())
     ctx.close()
+
+
+# ---------------- FITS catalogs (os_fitsout) ----------------
+
+def read_fits(path):
+    """A minimal reader of this writer's files (FITS standard 4.0): the HDUs as
+    (header cards {keyword: value}, raw data bytes)."""
+    raw = open(path, "rb").read()
+    assert len(raw) % 2880 == 0
+    hdus, pos = [], 0
+    while pos < len(raw):
+        cards, order = {}, []
+        while True:
+            blk = raw[pos:pos + 2880]
+            pos += 2880
+            done = False
+            for k in range(36):
+                c = blk[80 * k:80 * k + 80].decode("ascii")
+                key = c[:8].strip()
+                if key == "END":
+                    done = True
+                    break
+                if c[8:10] == "= ":
+                    v = c[10:].strip()
+                    if v.startswith("'"):
+                        v = v[1:v.rindex("'")].replace("''", "'").rstrip()
+                    elif v in ("T", "F"):
+                        v = v == "T"
+                    else:
+                        v = int(v)
+                    cards[key] = v
+                    order.append(key)
+            if done:
+                break
+        nbytes = cards.get("NAXIS1", 0) * cards.get("NAXIS2", 0) if cards.get("NAXIS", 0) == 2 else 0
+        data = raw[pos:pos + nbytes]
+        pos += (nbytes + 2879) // 2880 * 2880
+        hdus.append((cards, order, data))
+    return hdus
+
+
+def fits_columns(cards, data):
+    """{TTYPE: array (nrows, width)} of a binary table with D/E/J columns."""
+    codes = {"D": ">f8", "E": ">f4", "J": ">i4"}
+    fields = []
+    for i in range(cards["TFIELDS"]):
+        form = cards["TFORM%d" % (i + 1)]
+        fields.append((cards["TTYPE%d" % (i + 1)], codes[form[-1]], (int(form[:-1]),)))
+    rec = np.frombuffer(data, dtype=np.dtype(fields), count=cards["NAXIS2"])
+    return {name: rec[name] for name, _, _ in fields}
+
+
+def test_fits_catalog_structure_and_rows(tmp_path, lib):
+    """The FITS catalog: an empty primary HDU, CATALOG with one column per output
+    column in the text file's order and every visible row, big-endian; METADATA
+    with the text header's column definitions."""
+    n = 40000
+    t = random_table(n)
+    cfg = G.textout_config(workload(lib), threads=4, version="0.0.0-test")
+    ids = (G.C.c_int32 * 3)(7, 8, 9)
+    cfg.comp_ids = ids
+    cfg.ncomp = 3
+    path = tmp_path / "sky.fits"
+    wr = G.FitsWriter(path, cfg)
+    wr.write(t.t, 0, 15000)
+    wr.write(t.t, 15000, n)
+    rows, nbytes = wr.close()
+    assert nbytes == os.path.getsize(path)
+    hdus = read_fits(path)
+    assert len(hdus) == 3
+    prim, cat, meta = hdus
+    assert prim[0]["SIMPLE"] is True and prim[0]["NAXIS"] == 0 and prim[0]["BITPIX"] == 8
+    assert cat[0]["XTENSION"] == "BINTABLE" and cat[0]["EXTNAME"] == "CATALOG"
+    assert cat[1][:8] == ["XTENSION", "BITPIX", "NAXIS", "NAXIS1", "NAXIS2", "PCOUNT", "GCOUNT", "TFIELDS"]
+    vis = t.arrays["hidden"][0, :n] == 0
+    assert cat[0]["NAXIS2"] == rows == int(vis.sum())
+    names = [cat[0]["TTYPE%d" % (i + 1)] for i in range(cat[0]["TFIELDS"])]
+    order = RANKED + [(c, f) for _, c, f in photometry_columns(5)[0]]
+    want_names = ["lb", "radec", "XYZ", "DM", "absSDSSr", "comp", "FeH", "vcyl", "pmradec", "Am", "AmInf"]
+    want_names += [d.split("[")[0].split("{")[0] for d, _, _ in photometry_columns(5)[0]]
+    assert names == want_names
+    cols = fits_columns(cat[0], cat[2])
+    for (name, fmt), fname in zip(order, want_names):
+        a = t.arrays[name][:, :n][:, vis]
+        got = cols[fname].T
+        if name == "comp":
+            a = np.array([7, 8, 9])[a]
+        if fmt.endswith("d"):
+            np.testing.assert_array_equal(got, a.astype(np.int32), err_msg=fname)
+        else:
+            g = got.astype(got.dtype.newbyteorder("="))
+            u = np.uint32 if g.itemsize == 4 else np.uint64
+            np.testing.assert_array_equal(g.view(u), a.astype(g.dtype).view(u), err_msg=fname)
+    assert meta[0]["EXTNAME"] == "METADATA" and meta[0]["NAXIS2"] == 1 and meta[0]["TTYPE1"] == "HEADER"
+    text_header = header(version="0.0.0-test")[2:-1]
+    assert meta[2].rstrip(b"\0").decode() == text_header
