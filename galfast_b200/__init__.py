@@ -33,7 +33,8 @@ class Job(C.Structure):
                 ("foot", C.POINTER(Footprint)), ("feh", C.POINTER(FixedFeHConfig)),
                 ("kin", C.POINTER(Bond2010Config)), ("phot", C.POINTER(PhotometryConfig)),
                 ("perr", C.POINTER(PhotoerrConfig)), ("v2pm", C.POINTER(Vel2pmConfig)), ("gal2other", C.c_int32),
-                ("feh_ivezic", C.POINTER(A.FehConfig)), ("feh_gauss", C.POINTER(A.GaussFehConfig))]
+                ("feh_ivezic", C.POINTER(A.FehConfig)), ("feh_gauss", C.POINTER(A.GaussFehConfig)),
+                ("multiples", C.POINTER(A.MultiplesConfig))]
 
 
 class CatalogStats(C.Structure):
@@ -97,6 +98,10 @@ def lib():
         L.gf_module_bond2010.argtypes = [vp, C.POINTER(Bond2010Config), C.POINTER(Table), C.c_int64, C.c_int64]
         L.gf_module_feh.argtypes = [vp, C.POINTER(A.FehConfig), C.POINTER(Table), C.c_int64, C.c_int64]
         L.gf_module_gaussfeh.argtypes = [vp, C.POINTER(A.GaussFehConfig), C.POINTER(Table), C.c_int64, C.c_int64]
+        L.gf_module_multiples.argtypes = [vp, C.POINTER(A.MultiplesConfig), C.POINTER(Table), C.c_int64, C.c_int64]
+        dp = C.POINTER(C.c_double)
+        L.gf_multiples_build.argtypes = [dp, dp, C.c_int32, dp, dp, C.c_int32, C.c_int32, C.c_uint32,
+                                         C.POINTER(A.MultiplesConfig)]
         L.gf_photometry_create.argtypes = [vp, C.POINTER(PhotometryConfig), C.POINTER(vp)]
         L.gf_photometry_destroy.argtypes = [vp]
         L.gf_module_photometry.argtypes = [vp, vp, C.POINTER(Table), C.c_int64, C.c_int64]
@@ -159,6 +164,7 @@ COLUMNS = [  # name, dtype, components (or "bands")
     ("AmInf", np.float32, 1), ("hidden", np.int32, 1), ("FeH", np.float32, 1), ("vcyl", np.float32, 3),
     ("mags", np.float32, "bands"), ("photoflags", np.int32, 1), ("obsmags", np.float32, "bands"),
     ("pm", np.float32, 3), ("radec", np.float64, 2), ("FeH_comp", np.int32, 1),
+    ("absmagSys", np.float32, 2), ("absmagSysNcomp", np.int32, 1),
 ]
 PROFILE_PHASES = ["integrate", "draw_window", "draw_rerun", "place", "sort", "clipper", "fixedfeh", "bond2010",
                   "photometry", "photoerrors", "vel2pm", "gal2other", "slot_density", "expand", "batch_draw"]
@@ -570,7 +576,7 @@ class TextoutConfig(C.Structure):
                 ("band", C.c_char_p), ("absband", C.c_char_p), ("radec", C.c_int32), ("feh", C.c_int32),
                 ("feh_comp", C.c_int32), ("vcyl", C.c_int32), ("pm_coordsys", C.c_int32), ("photoerrors", C.c_int32),
                 ("comp_ids", C.POINTER(C.c_int32)), ("ncomp", C.c_int32), ("version", C.c_char_p),
-                ("threads", C.c_int32)]
+                ("threads", C.c_int32), ("multiples", C.c_int32)]
 
 
 class TextoutSet(C.Structure):
@@ -603,6 +609,7 @@ def textout_config(w, version=None, threads=0):
     cfg.photoerrors = 1 if w.perr is not None else 0
     cfg.version = version.encode() if version else None
     cfg.threads = int(threads)
+    cfg.multiples = 1 if getattr(w, "multiples", None) is not None else 0
     cfg._keep = keep
     return cfg
 

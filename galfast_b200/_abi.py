@@ -66,7 +66,18 @@ class Table(C.Structure):
                 ("comp", C.c_void_p), ("Am", C.c_void_p), ("AmInf", C.c_void_p),
                 ("hidden", C.c_void_p), ("FeH", C.c_void_p), ("vcyl", C.c_void_p),
                 ("mags", C.c_void_p), ("photoflags", C.c_void_p), ("obsmags", C.c_void_p),
-                ("pm", C.c_void_p), ("radec", C.c_void_p), ("FeH_comp", C.c_void_p)]
+                ("pm", C.c_void_p), ("radec", C.c_void_p), ("FeH_comp", C.c_void_p),
+                ("absmagSys", C.c_void_p), ("absmagSysNcomp", C.c_void_p), ("systems", C.c_int32)]
+
+
+GF_MULT_LF_M2_GT_M1, GF_MULT_LF, GF_MULT_EQUAL_MASS = 1, 2, 3
+
+
+class MultiplesConfig(C.Structure):     # gf_multiples_config (os_unresolvedMultiples)
+    _fields_ = [("algo", C.c_int32), ("comp_mask", C.c_uint32),
+                ("sec_x0", C.c_float), ("sec_inv_dx", C.c_float), ("nsec", C.c_int32), ("secprob", C.c_float * 64),
+                ("cum_x0", C.c_float), ("cum_inv_dx", C.c_float), ("ncum", C.c_int32), ("cumlf", C.c_float * 256),
+                ("inv_x0", C.c_float), ("inv_inv_dx", C.c_float), ("ninv", C.c_int32), ("invcumlf", C.c_float * 256)]
 
 
 class FixedFeHConfig(C.Structure):
@@ -129,7 +140,7 @@ EXPORTS = [
     "gf_skygen_create", "gf_skygen_destroy", "gf_skygen_model_info_get", "gf_skygen_model_lf_get",
     "gf_skygen_integrate", "gf_skygen_set_norm", "gf_skygen_draw",
     "gf_table_alloc", "gf_table_free", "gf_table_download",
-    "gf_module_clipper", "gf_module_fixedfeh", "gf_module_bond2010",
+    "gf_module_clipper", "gf_module_fixedfeh", "gf_module_bond2010", "gf_module_multiples", "gf_multiples_build",
     "gf_photometry_create", "gf_photometry_destroy", "gf_module_photometry",
     "gf_photoerr_create", "gf_photoerr_destroy", "gf_module_photoerrors",
     "gf_module_vel2pm", "gf_module_gal2other",

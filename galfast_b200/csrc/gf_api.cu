@@ -76,6 +76,8 @@ gf_status zero_module_rows(gf_ctx *ctx, const gf_table *t, int64_t n)
     GF_TRY(z(t->pm, 4, 3));
     GF_TRY(z(t->radec, 8, 2));
     GF_TRY(z(t->FeH_comp, 4, 1));
+    GF_TRY(z(t->absmagSys, 4, 2));
+    GF_TRY(z(t->absmagSysNcomp, 4, 1));
     return GF_OK;
 }
 
@@ -981,6 +983,8 @@ static gf_status table_alloc_columns(gf_table *t, size_t n, int32_t nbands)
     GF_TRY(dev_alloc(&t->pm, 3 * n));
     GF_TRY(dev_alloc(&t->radec, 2 * n));
     GF_TRY(dev_alloc(&t->FeH_comp, n));
+    GF_TRY(dev_alloc(&t->absmagSys, 2 * n));
+    GF_TRY(dev_alloc(&t->absmagSysNcomp, n));
     return GF_OK;
 }
 
@@ -1010,7 +1014,7 @@ gf_status gf_table_free(gf_ctx *ctx, gf_table *t)
     dev_free(t->lb); dev_free(t->projIdx); dev_free(t->projXY); dev_free(t->DM); dev_free(t->absmag);
     dev_free(t->XYZ); dev_free(t->comp); dev_free(t->Am); dev_free(t->AmInf); dev_free(t->hidden);
     dev_free(t->FeH); dev_free(t->vcyl); dev_free(t->mags); dev_free(t->photoflags); dev_free(t->obsmags);
-    dev_free(t->pm); dev_free(t->radec); dev_free(t->FeH_comp);
+    dev_free(t->pm); dev_free(t->radec); dev_free(t->FeH_comp); dev_free(t->absmagSys); dev_free(t->absmagSysNcomp);
     memset(t, 0, sizeof(*t));
     return GF_OK;
 }
@@ -1049,8 +1053,11 @@ gf_status gf_table_download_rows(gf_ctx *ctx, const gf_table *dev, int64_t begin
     GF_TRY(cp(host->pm, dev->pm, 4, 3));
     GF_TRY(cp(host->radec, dev->radec, 8, 2));
     GF_TRY(cp(host->FeH_comp, dev->FeH_comp, 4, 1));
+    GF_TRY(cp(host->absmagSys, dev->absmagSys, 4, 2));
+    GF_TRY(cp(host->absmagSysNcomp, dev->absmagSysNcomp, 4, 1));
     GF_CUDA(cudaStreamSynchronize(st));
     host->size = end - begin;
+    host->systems = dev->systems;
     return GF_OK;
 }
 
@@ -1103,6 +1110,24 @@ static gf_status module_feh(gf_ctx *ctx, const gf_feh_config *fp, const gf_gauss
     if ((n + 255) / 256 > ctx->rng_nstreams) return fail(GF_E_INVALID, "more than 256 rows per stream");
     ProfScope ps(ctx, GF_PROF_FEH);
     GF_CUDA(gfk::launch_feh(fp, gp, ctx->d_rng, ctx->rng_nstreams, *t, begin, end, ctx->stream));
+    return GF_OK;
+}
+
+gf_status gf_module_multiples(gf_ctx *ctx, const gf_multiples_config *cfg, gf_table *t, int64_t begin, int64_t end)
+{
+    GF_TRY(check_ctx(ctx));
+    GF_TRY(row_range(t, begin, end));
+    if (!cfg) return fail(GF_E_INVALID, "null config");
+    if (cfg->algo < GF_MULT_LF_M2_GT_M1 || cfg->algo > GF_MULT_EQUAL_MASS || cfg->nsec < 1 || cfg->nsec > 64 ||
+        cfg->ncum < 1 || cfg->ncum > GF_MULT_TEX || cfg->ninv < 1 || cfg->ninv > GF_MULT_TEX)
+        return fail(GF_E_INVALID, "invalid unresolved-multiples configuration");
+    if (!t->absmagSys || !t->absmagSysNcomp) return fail(GF_E_INVALID, "table without the absmagSys columns");
+    if (!ctx->d_rng) return fail(GF_E_STATE, "gf_rng_init must precede gf_module_multiples");
+    const int64_t n = end - begin;
+    if ((n + 255) / 256 > ctx->rng_nstreams) return fail(GF_E_INVALID, "more than 256 rows per stream");
+    ProfScope ps(ctx, GF_PROF_FEH);
+    GF_CUDA(gfk::launch_multiples(*cfg, ctx->d_rng, ctx->rng_nstreams, *t, begin, end, ctx->stream));
+    t->systems = 1;
     return GF_OK;
 }
 
@@ -1293,11 +1318,13 @@ static gf_status catalog_run_once(gf_ctx *ctx, const gf_job *job, gf_batch_callb
             if (n == 0) continue;
             S.batches++;
             GF_TRY(gfa::zero_module_rows(ctx, &g.t, n));
+            g.t.systems = 0;
             /* the module chain in pipeline order (pipeline.h:75-88) */
             if (job->foot) GF_TRY(gf_module_clipper(ctx, job->foot, job->sky.proj, &g.t, 0, n));
             if (job->feh) GF_TRY(gf_module_fixedfeh(ctx, job->feh, &g.t, 0, n));
             if (job->feh_ivezic) GF_TRY(gf_module_feh(ctx, job->feh_ivezic, &g.t, 0, n));
             if (job->feh_gauss) GF_TRY(gf_module_gaussfeh(ctx, job->feh_gauss, &g.t, 0, n));
+            if (job->multiples) GF_TRY(gf_module_multiples(ctx, job->multiples, &g.t, 0, n));
             if (job->kin) GF_TRY(gf_module_bond2010(ctx, job->kin, &g.t, 0, n));
             if (g.ph) GF_TRY(gf_module_photometry(ctx, g.ph, &g.t, 0, n));
             if (g.pe) GF_TRY(gf_module_photoerrors(ctx, g.pe, row_offset, &g.t, 0, n));

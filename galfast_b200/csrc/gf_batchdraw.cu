@@ -354,10 +354,23 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                     mub *= V.norm;
                     mub *= D3max;
                     mub *= K;
-                    xthr = gfr::uniform_threshold((1.0f - mub) - 3.0e-7f);
+                    xthr = gfr::uniform_threshold_lower((1.0f - mub) - 3.0e-7f);
                     if (imax < icut) {
                         live = (1u << GF_BLOCK) - 1u;
+                    } else if (!(wm & (wm - 1u))) {
+                        /* At most one diagonal start (bin p): bins before it continue the
+                         * first diagonal (im = i0 + s), bins from it on the next one from
+                         * im = max(0, d + 1 - (y - 1)); a bin is live while im < icut, so
+                         * each run's live bins are a prefix of it. */
+                        const int p = wm ? __ffs(wm) - 1 : GF_BLOCK;
+                        live = (1u << min(p, max(0, icut - i0))) - 1u;
+                        if (wm) {
+                            const int dB = i0 + j0 + 1;
+                            const int iB = dB - (V.y - 1) > 0 ? dB - (V.y - 1) : 0;
+                            live |= ((1u << min(GF_BLOCK - p, max(0, icut - iB))) - 1u) << p;
+                        }
                     } else {
+                        /* several diagonal starts (short diagonals at the grid's corners) */
                         int ii = i0, dd = i0 + j0;
                         live = ii < icut ? 1u : 0u;
                         for (int s = 1; s < GF_BLOCK; s++) {
@@ -372,12 +385,8 @@ __global__ void __launch_bounds__(256, 4) batch_draw_kernel(BatchDrawParams P)
                     }
                     if (xthr < 0) {
                         any = live != 0;               /* the bound proves nothing: exact test throughout */
-                    } else if (live == (1u << GF_BLOCK) - 1u) {
-                        uint32_t mx = 0;
-#pragma unroll
-                        for (int s = 0; s < GF_BLOCK; s++) mx = max(mx, bd_mwc_x(w, a));
-                        any = mx > (uint32_t)xthr;
                     } else {
+                        /* one predicated walk for full and partial blocks alike (no divergence) */
                         uint32_t mx = 0;
 #pragma unroll
                         for (int s = 0; s < GF_BLOCK; s++)

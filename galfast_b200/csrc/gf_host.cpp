@@ -652,4 +652,76 @@ gf_status gf_photometry_build(const double *rows, int32_t nrows, int32_t ncolors
     return GF_OK;
 }
 
+/* os_unresolvedMultiples::construct (unresolvedMultiples_host.cpp:96-189): the
+ * binary-fraction table (resampled to 64 texels, or the constant 1 over
+ * [-100, 100]), and the cumulative luminosity function of the secondaries (the
+ * trapezoid integral of the linearly interpolated LF at 256 points, normalised)
+ * with its inverse, both resampled to 256 texels (cux.cpp:310-350). */
+static void resample_1d(const std::vector<double> &X, const std::vector<double> &Y, int nsamp, float *tab, float *x0,
+                        float *inv_dx)
+{
+    const double X0 = X[0], X1 = X.back(), dX = (X1 - X0) / (nsamp - 1);
+    for (int i = 0; i != nsamp; i++) tab[i] = (float)gfh::interp_linear(X, Y, X0 + i * dX);
+    *x0 = (float)X0;
+    *inv_dx = (float)(1. / dX);
+}
+
+gf_status gf_multiples_build(const double *frac_M, const double *frac_p, int32_t nfrac, const double *lf_M,
+                             const double *lf_phi, int32_t nlf, int32_t algo, uint32_t comp_mask, gf_multiples_config *out)
+{
+    if (!out || algo < GF_MULT_LF_M2_GT_M1 || algo > GF_MULT_EQUAL_MASS || nfrac < 0 || nlf < 0 || nfrac == 1 || nlf == 1 ||
+        (nfrac && (!frac_M || !frac_p)) || (nlf && (!lf_M || !lf_phi)))
+        return GF_E_INVALID;
+    for (int i = 1; i < nfrac; i++)
+        if (!(frac_M[i] > frac_M[i - 1])) return GF_E_INVALID;
+    for (int i = 1; i < nlf; i++)
+        if (!(lf_M[i] > lf_M[i - 1])) return GF_E_INVALID;
+    memset(out, 0, sizeof(*out));
+    out->algo = algo;
+    out->comp_mask = comp_mask;
+    if (nfrac) {
+        const std::vector<double> X(frac_M, frac_M + nfrac), Y(frac_p, frac_p + nfrac);
+        out->nsec = 64;
+        resample_1d(X, Y, 64, out->secprob, &out->sec_x0, &out->sec_inv_dx);
+    } else {
+        /* load_constant_texture_1D(1, -100, 100) */
+        out->nsec = 2;
+        out->secprob[0] = out->secprob[1] = 1.f;
+        out->sec_x0 = -100.f;
+        out->sec_inv_dx = (float)(1. / (100. - -100.));
+    }
+    std::vector<double> x, y;
+    if (nlf) {
+        x.assign(lf_M, lf_M + nlf);
+        y.assign(lf_phi, lf_phi + nlf);
+    } else {
+        x = {-100., 100.};
+        y = {1., 1.};
+    }
+    const int NPIX = GF_MULT_TEX;
+    const double dx = (x.back() - x.front()) / (NPIX - 1);
+    std::vector<double> ycum(NPIX), xcum(NPIX);
+    xcum[0] = x.front();
+    ycum[0] = 0;
+    double yprev = gfh::interp_linear(x, y, x.front());
+    for (int i = 1; i < NPIX; i++) {
+        const double xx = x.front() + i * dx;
+        const double yy = gfh::interp_linear(x, y, xx);
+        const double dy = yy - yprev;
+        const double dA = (yprev + 0.5 * dy) * dx;
+        xcum[i] = xx;
+        ycum[i] = ycum[i - 1] + dA;
+        yprev = yy;
+    }
+    const double norm = ycum.back();
+    if (!(norm > 0)) return GF_E_INVALID;
+    for (auto &v : ycum) v /= norm;
+    for (int i = 1; i < NPIX; i++)
+        if (!(ycum[i] > ycum[i - 1])) return GF_E_INVALID;     /* the inverse needs a strictly increasing integral */
+    out->ncum = out->ninv = NPIX;
+    resample_1d(xcum, ycum, NPIX, out->cumlf, &out->cum_x0, &out->cum_inv_dx);
+    resample_1d(ycum, xcum, NPIX, out->invcumlf, &out->inv_x0, &out->inv_inv_dx);
+    return GF_OK;
+}
+
 }  /* extern "C" */

@@ -126,6 +126,8 @@ struct PhotTables {
     uint32_t comp_mask;
 };
 cudaError_t launch_photometry(const PhotTables &c, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
+cudaError_t launch_multiples(const gf_multiples_config &c, uint32_t *rng, int32_t NS, gf_table t, int64_t begin, int64_t end,
+                             cudaStream_t s);
 struct PerrTables {
     int32_t nbands, nknots;
     const double *mag, *sigma;    /* device */
@@ -239,6 +241,9 @@ cudaError_t launch_bond2010_multi(const gf_bond2010_config &c, uint32_t *rng_all
 cudaError_t launch_feh_multi(const gf_feh_config *fp, const gf_gaussfeh_config *gp, uint32_t *rng_all, int32_t NS,
                              MultiRows R, const int64_t *slot_chunk_begin, int32_t nslots, int64_t nchunks,
                              const int64_t *slot_rows, gf_table t, cudaStream_t s);
+cudaError_t launch_multiples_multi(const gf_multiples_config &c, uint32_t *rng_all, int32_t NS, MultiRows R,
+                                   const int64_t *slot_chunk_begin, int32_t nslots, int64_t nchunks, const int64_t *slot_rows,
+                                   gf_table t, cudaStream_t s);
 cudaError_t launch_photoerrors_multi(const PerrTables &c, const uint64_t *seed_by_job, const int64_t *catalog_offset_by_job,
                                      MultiRows R, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
 

@@ -373,6 +373,117 @@ cudaError_t launch_feh_multi(const gf_feh_config *fp, const gf_gaussfeh_config *
     return cudaGetLastError();
 }
 
+/* ---------------- unresolved multiple systems ---------------- */
+
+/* nearest-texel lookup of a 1-D table (cux.h:786-792, 849-855) */
+__device__ __forceinline__ float mult_tex(const float *tab, int n, float x0, float inv_dx, float x)
+{
+    float xi = (x - x0) * inv_dx + 0.5f;
+    if (xi < 0.f) xi = 0.f;
+    else if (xi >= (float)n) xi = (float)n - 1;
+    return tab[(uint32_t)xi];
+}
+
+/* draw_companion (unresolvedMultiples_gpu.cu.h:46-77) */
+__device__ __forceinline__ bool mult_companion(const gf_multiples_config &c, float M1, gfr::Mwc &r, float &M2)
+{
+    const float psec = mult_tex(c.secprob, c.nsec, c.sec_x0, c.sec_inv_dx, M1);
+    float u = r.uniform();
+    if (u > psec) return false;
+    if (c.algo == GF_MULT_EQUAL_MASS) { M2 = M1; return true; }
+    const float pprim = mult_tex(c.cumlf, c.ncum, c.cum_x0, c.cum_inv_dx, M1);
+    u = r.uniform();
+    /* fainter than the primary: u rescaled into [pprim, 1] in double, as written */
+    if (c.algo == GF_MULT_LF_M2_GT_M1) u = (float)((double)pprim + (double)u * (1. - (double)pprim));
+    M2 = mult_tex(c.invcumlf, c.ninv, c.inv_x0, c.inv_inv_dx, u);
+    if (c.algo == GF_MULT_LF_M2_GT_M1 && M2 < M1) M2 = M1;
+    return true;
+}
+
+/* os_unresolvedMultiples_kernel (unresolvedMultiples_gpu.cu.h:80-123) on rows
+ * [begin + 256 th, ...) with stream th; two system components (absmagSys[2]) */
+__device__ __forceinline__ void multiples_chunk(const gf_multiples_config &c, uint32_t *rng, int32_t NS, gf_table &t,
+                                                int64_t begin, int64_t end, int64_t th)
+{
+    const int64_t P = t.capacity;
+    gfr::Mwc r;
+    r.a = rng[th]; r.c = rng[NS + th]; r.x = rng[2 * NS + th]; r.used = 0;
+    int64_t rb = begin + 256 * th, re = begin + 256 * (th + 1);
+    if (re > end) re = end;
+    for (int64_t row = rb; row < re; row++) {
+        const float M1 = t.absmag[row];
+        if (t.hidden[row] || !((c.comp_mask >> t.comp[row]) & 1u)) {
+            /* a single star */
+            t.absmagSys[row] = M1;
+            t.absmagSys[P + row] = 99.999f;
+            t.absmagSysNcomp[row] = 1;
+            continue;
+        }
+        t.absmagSys[row] = M1;
+        float Ltot = gfm::exp10f_(-0.4f * M1);
+        int ncomps = 1;
+        float M2 = 0.f;
+        if (mult_companion(c, M1, r, M2)) {
+            t.absmagSys[P + row] = M2;
+            Ltot += gfm::exp10f_(-0.4f * M2);
+            ncomps++;
+        } else {
+            t.absmagSys[P + row] = 99.999f;
+        }
+        /* -2.5 is a double: the product is formed in double and stored as float */
+        t.absmag[row] = (float)(-2.5 * (double)gfm::log10f_(Ltot));
+        t.absmagSysNcomp[row] = ncomps;
+    }
+    rng[NS + th] = r.c;
+    rng[2 * NS + th] = r.x;
+}
+
+__global__ void __launch_bounds__(128) multiples_kernel(const gf_multiples_config c, uint32_t *rng, int32_t NS, gf_table t,
+                                                        int64_t begin, int64_t end, int64_t nchunks)
+{
+    const int64_t th = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (th >= nchunks) return;
+    multiples_chunk(c, rng, NS, t, begin, end, th);
+}
+
+__global__ void __launch_bounds__(128) multiples_multi_kernel(const gf_multiples_config c, uint32_t *rng_all, int32_t NS,
+                                                              MultiRows R, const int64_t *slot_chunk_begin, int32_t nslots,
+                                                              int64_t nchunks, const int64_t *slot_rows, gf_table t)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nchunks) return;
+    int lo = 0, hi = nslots - 1;          /* last slot whose first chunk is <= k */
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (slot_chunk_begin[mid] <= k) lo = mid; else hi = mid - 1;
+    }
+    const int64_t b = R.slot_row_begin[lo];
+    uint32_t *rng = rng_all + (size_t)R.slot_job[lo] * 3 * NS;
+    multiples_chunk(c, rng, NS, t, b, b + slot_rows[lo], k - slot_chunk_begin[lo]);
+}
+
+cudaError_t launch_multiples(const gf_multiples_config &c, uint32_t *rng, int32_t NS, gf_table t, int64_t begin, int64_t end,
+                             cudaStream_t s)
+{
+    if (end <= begin) return cudaSuccess;
+    const int64_t n = end - begin, nchunks = n / 256 + (n % 256 ? 1 : 0);
+    if (nchunks > NS) return cudaErrorInvalidValue;
+    multiples_kernel<<<(int)((nchunks + 127) / 128), 128, 0, s>>>(c, rng, NS, t, begin, end, nchunks);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_multiples_multi(const gf_multiples_config &c, uint32_t *rng_all, int32_t NS, MultiRows R,
+                                   const int64_t *slot_chunk_begin, int32_t nslots, int64_t nchunks, const int64_t *slot_rows,
+                                   gf_table t, cudaStream_t s)
+{
+    if (nchunks <= 0) return cudaSuccess;
+    multiples_multi_kernel<<<(unsigned)((nchunks + 127) / 128), 128, 0, s>>>(c, rng_all, NS, R, slot_chunk_begin, nslots,
+                                                                             nchunks, slot_rows, t);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 /* ---------------- photometry ---------------- */
 __device__ __forceinline__ uint32_t brev(uint32_t a) { return __brev(a); }
 
@@ -380,15 +491,21 @@ __global__ void __launch_bounds__(256) photometry_kernel(PhotTables lt, gf_table
 {
     const int64_t P = t.capacity;
     const int ncolors = lt.nbands - 1;
+    const bool sys = t.systems && t.absmagSys;
+    const float *Mr = sys ? t.absmagSys : t.absmag;
+    const int nabsmag = sys ? 2 : 1;
     for (int64_t row = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < end; row += (int64_t)gridDim.x * blockDim.x) {
         if (t.hidden[row]) continue;
         int cmp = t.comp[row];
         if (!((lt.comp_mask >> cmp) & 1u)) continue;
         float fFeH = t.FeH[row];
-        float fMr = t.absmag[row];
         uint32_t flag = 0;
         float c[GF_MAX_BANDS];
-        if (!(fMr >= 99.999f)) {
+        /* the system's components (absmagSys when unresolved multiples ran, else the
+         * single absmag): their luminosities are summed band by band */
+        for (int syscomp = 0; syscomp < nabsmag; syscomp++) {
+            const float fMr = Mr[(size_t)syscomp * P + row];
+            if (fMr >= 99.999f) break;
             float xi = (fFeH - lt.tcFeH[0]) * lt.tcFeH[1] + 0.5f;
             float yi = (fMr - lt.tcMr[0]) * lt.tcMr[1] + 0.5f;
             if (xi < 0.f) xi = 0.f; else if (xi >= (float)lt.nFeH) xi = (float)lt.nFeH - 1;
@@ -403,7 +520,9 @@ __global__ void __launch_bounds__(256) photometry_kernel(PhotTables lt, gf_table
                 float M = fMr;
                 if (b < lt.bidx) { for (int q = b; q != lt.bidx; q++) M += c[q]; }
                 if (b > lt.bidx) { for (int q = lt.bidx; q != b; q++) M -= c[q]; }
-                t.mags[b * P + row] = gfm::exp10f_(-0.4f * M);
+                float L = gfm::exp10f_(-0.4f * M);
+                if (syscomp) L += t.mags[b * P + row];
+                t.mags[b * P + row] = L;
             }
         }
         bool fl = false;

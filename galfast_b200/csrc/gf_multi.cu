@@ -286,9 +286,9 @@ namespace {
 /* bytes of one row of a table with nb bands, counting the columns in mask (GF_COL_*) */
 size_t row_bytes(int nb, uint32_t mask)
 {
-    const size_t w[18] = {16, 4, 8, 4, 4, 12, 4, 4, 4, 4, 4, 12, 4 * (size_t)nb, 4, 4 * (size_t)nb, 12, 16, 4};
+    const size_t w[20] = {16, 4, 8, 4, 4, 12, 4, 4, 4, 4, 4, 12, 4 * (size_t)nb, 4, 4 * (size_t)nb, 12, 16, 4, 8, 4};
     size_t b = 0;
-    for (int i = 0; i < 18; i++)
+    for (int i = 0; i < 20; i++)
         if (mask & (1u << i)) b += w[i];
     return b;
 }
@@ -318,10 +318,12 @@ gf_table carve_table(char *p, int64_t cap, int nb, uint32_t mask)
     t.obsmags = (float *)take(GF_COL_OBSMAGS, 4 * n * nb); t.pm = (float *)take(GF_COL_PM, 12 * n);
     t.radec = (double *)take(GF_COL_RADEC, 16 * n);
     t.FeH_comp = (int32_t *)take(GF_COL_FEHCOMP, 4 * n);
+    t.absmagSys = (float *)take(GF_COL_ABSMAGSYS, 8 * n);
+    t.absmagSysNcomp = (int32_t *)take(GF_COL_SYSNCOMP, 4 * n);
     return t;
 }
 
-size_t carved_bytes(int64_t cap, int nb, uint32_t mask) { return row_bytes(nb, mask) * (size_t)cap + 21 * 256; }
+size_t carved_bytes(int64_t cap, int nb, uint32_t mask) { return row_bytes(nb, mask) * (size_t)cap + 23 * 256; }
 
 /* rows [r0, r1) of the device table d into the host table h, on stream cs */
 gf_status copy_rows_async(const gf_table &d, int64_t r0, int64_t r1, gf_table &h, cudaStream_t cs)
@@ -340,6 +342,8 @@ gf_status copy_rows_async(const gf_table &d, int64_t r0, int64_t r1, gf_table &h
     GF_TRY(cp(h.mags, d.mags, 4, d.nbands)); GF_TRY(cp(h.photoflags, d.photoflags, 4, 1));
     GF_TRY(cp(h.obsmags, d.obsmags, 4, d.nbands)); GF_TRY(cp(h.pm, d.pm, 4, 3)); GF_TRY(cp(h.radec, d.radec, 8, 2));
     GF_TRY(cp(h.FeH_comp, d.FeH_comp, 4, 1));
+    GF_TRY(cp(h.absmagSys, d.absmagSys, 4, 2)); GF_TRY(cp(h.absmagSysNcomp, d.absmagSysNcomp, 4, 1));
+    h.systems = d.systems;
     return GF_OK;
 }
 
@@ -456,18 +460,20 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         int ns = J.nstreams > GF_MAX_STREAMS ? GF_MAX_STREAMS : J.nstreams;
         if (ns % 64) ns += 64 - ns % 64;
         if (ns < N) return fail(GF_E_INVALID, "nstreams below nthreads");
-        if (J.kin && (J.capacity + 255) / 256 > ns) return fail(GF_E_INVALID, "capacity above 256 rows per stream (Bond2010)");
+        if ((J.kin || J.feh_ivezic || J.feh_gauss || J.multiples) && (J.capacity + 255) / 256 > ns)
+            return fail(GF_E_INVALID, "capacity above 256 rows per stream (the stream-drawing modules)");
         NS = std::max(NS, ns);
         nbands = std::max(nbands, (int)J.nbands);
         if (!!J.feh != !!J0.feh || !!J.kin != !!J0.kin || !!J.v2pm != !!J0.v2pm || J.gal2other != J0.gal2other ||
             !!J.phot != !!J0.phot || !!J.perr != !!J0.perr || !!J.feh_ivezic != !!J0.feh_ivezic ||
-            !!J.feh_gauss != !!J0.feh_gauss)
+            !!J.feh_gauss != !!J0.feh_gauss || !!J.multiples != !!J0.multiples)
             return fail(GF_E_INVALID, "all requests of a multi-request run need the same modules");
         if (!same_cfg(J.feh, J0.feh, sizeof(gf_fixedfeh_config)) || !same_cfg(J.kin, J0.kin, sizeof(gf_bond2010_config)) ||
             !same_cfg(J.v2pm, J0.v2pm, sizeof(gf_vel2pm_config)) ||
             !same_cfg(J.feh_ivezic, J0.feh_ivezic, sizeof(gf_feh_config)) ||
-            !same_cfg(J.feh_gauss, J0.feh_gauss, sizeof(gf_gaussfeh_config)))
-            return fail(GF_E_INVALID, "the metallicity, Bond2010 and vel2pm configurations must agree across requests");
+            !same_cfg(J.feh_gauss, J0.feh_gauss, sizeof(gf_gaussfeh_config)) ||
+            !same_cfg(J.multiples, J0.multiples, sizeof(gf_multiples_config)))
+            return fail(GF_E_INVALID, "the metallicity, multiples, Bond2010 and vel2pm configurations must agree across requests");
         if (J.feh_gauss && (J.feh_gauss->ncomp < 1 || J.feh_gauss->ncomp >= GF_GAUSSFEH_MAXCOMP))
             return fail(GF_E_INVALID, "GaussianFeH needs 1 <= ncomp < 10");
     }
@@ -1253,6 +1259,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
             }
             out.size = total;
             GF_TRY(gfa::zero_module_rows(ctx, &out, total));
+            out.systems = J0.multiples ? 1 : 0;
             /* the module chain in pipeline order (pipeline.h:75-88) over every request's rows */
             gfk::MultiRows MR;
             MR.row_slot = row_slot.p; MR.slot_row_begin = d_row_begin; MR.slot_job = d_slot_job;
@@ -1270,6 +1277,11 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                     if (J0.feh_gauss)
                         GF_CUDA(gfk::launch_feh_multi(nullptr, J0.feh_gauss, d_rng, NS, MR, d_chunk_begin, nslots, nchunks,
                                                       d_slot_rows, out, st));
+                }
+                if (J0.multiples) {
+                    ProfScope ps(ctx, GF_PROF_FEH);
+                    GF_CUDA(gfk::launch_multiples_multi(*J0.multiples, d_rng, NS, MR, d_chunk_begin, nslots, nchunks, d_slot_rows,
+                                                        out, st));
                 }
                 if (J0.kin) {
                     ProfScope ps(ctx, GF_PROF_BOND2010);

@@ -252,6 +252,18 @@ GFR_HD int64_t uniform_threshold(float thr)
     return (int64_t)T + half - 1 + ((bits & 1u) ? 0 : 1);
 }
 
+/* A cheaper threshold for tests that only need to be safe: x <= X implies
+ * 2^-32 * (float)x <= thr (X at most 3.6e-7 relative below uniform_threshold's);
+ * -1 when thr <= 0.  For 0 < thr < 1: the scaling by 2^32 is exact, the factor
+ * 1 - 2^-22 (rounded product within 2^-24) keeps X * (1 + 2^-24), the largest
+ * float x rounds to, below thr * 2^32. */
+GFR_HD int64_t uniform_threshold_lower(float thr)
+{
+    if (!(thr > 0.f)) return -1;
+    if (thr >= 1.f) return 0xffffffffll;
+    return (int64_t)(uint32_t)(thr * 4294967296.0f * 0.99999976f);
+}
+
 /* (a * b) mod p for the stream prime p = A*2^32 - 1, a, b < p.
  * The 128-bit product N is folded with N -> A*(N mod 2^32) + (N >> 32), which
  * multiplies the residue by 2^-32 (mod p); the caller pre-scales one operand

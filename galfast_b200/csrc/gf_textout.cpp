@@ -275,13 +275,22 @@ std::vector<ColumnDef> output_columns(const gf_textout_config &c)
          * (byte-wise) name order, then the properties */
         const std::string band = c.band ? c.band : "";
         const std::string name = c.absband ? c.absband : ("abs" + band);
-        std::vector<std::string> alias = {"M1", "absmag"};
+        /* unresolved multiples drop the M1 alias (it names the primary of absmag + "Sys",
+         * unresolvedMultiples_host.cpp:56-80) */
+        std::vector<std::string> alias = {"absmag"};
+        if (!c.multiples) alias.push_back("M1");
         std::sort(alias.begin(), alias.end());
         std::string d = name + "{";
         for (auto &a : alias) d += "alias=" + a + ";";
         if (!band.empty()) d += "band=" + band + ";";
         d += "}";
         ranked.push_back({d, Field{F32, GF_OFF(absmag), 1, 3, 7, true, false}});
+        if (c.multiples) {
+            const std::string bp = band.empty() ? "" : "band=" + band + ";";
+            others.push_back({name + "Sys[2]{class=magnitude;fieldNames=0:M1,1:M2;alias=absmagSys;" + bp + "}",
+                              Field{F32, GF_OFF(absmagSys), 2, 3, 7, true, false}});
+            others.push_back({name + "SysNcomp{type=int;fmt=%1d;}", Field{I32, GF_OFF(absmagSysNcomp), 1, 0, 1, false, false}});
+        }
     }
     ranked.push_back({"comp", Field{I32, GF_OFF(comp), 1, 0, 3, false, true}});
     if (c.feh) ranked.push_back({"FeH", Field{F32, GF_OFF(FeH), 1, 3, 6, true, false}});

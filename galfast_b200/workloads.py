@@ -120,6 +120,39 @@ def gaussfeh_config(mean=(-0.6, -1.5), sigma=(0.2, 0.3), wt=(3.0, 1.0), comp_mas
     return c
 
 
+def multiples_config(lib, algo=A.GF_MULT_LF_M2_GT_M1, comp_mask=0xFFFFFFFF, fraction=None, lf=None):
+    """os_unresolvedMultiples through gf_multiples_build.  fraction: (M, p) knots of
+    the binary fraction (None: 1 everywhere); lf: (M, phi) knots of the secondaries'
+    luminosity function (None: flat).  The default synthetic choices: a binary
+    fraction falling from 0.6 at M = 0 to 0.3 at M = 14, and a secondary LF rising
+    towards faint magnitudes."""
+    c = A.MultiplesConfig()
+    dp = C.POINTER(C.c_double)
+
+    def arr(v):
+        a = np.ascontiguousarray(np.asarray(v, dtype=np.float64))
+        return a, a.ctypes.data_as(dp)
+    fm = fp = lm = lp = None
+    nf = nl = 0
+    keep = []
+    if fraction is not None:
+        (a, fm), (b, fp) = arr(fraction[0]), arr(fraction[1])
+        keep += [a, b]
+        nf = len(a)
+    if lf is not None:
+        (a, lm), (b, lp) = arr(lf[0]), arr(lf[1])
+        keep += [a, b]
+        nl = len(a)
+    st = lib.gf_multiples_build(fm, fp, nf, lm, lp, nl, algo, comp_mask, C.byref(c))
+    if st != 0:
+        raise RuntimeError("gf_multiples_build failed (%d)" % st)
+    return c
+
+
+MULT_FRACTION = ([-2.0, 0.0, 6.0, 14.0, 20.0], [0.6, 0.6, 0.45, 0.3, 0.3])
+MULT_LF = ([-2.0, 2.0, 6.0, 10.0, 14.0, 18.0], [0.2, 0.5, 1.0, 2.0, 3.0, 3.2])
+
+
 def bond2010_config(disk_sigma=(35.0, 25.0, 20.0), halo_sigma=(140.0, 100.0, 95.0), Rg=8000.0, z0=25.0):
     """Bond et al. (2010) kinematics with constant dispersions (Bond2010_host.cpp:142-227 layout)."""
     cfg = A.Bond2010Config()
@@ -183,6 +216,7 @@ class Workload:
     gal2other: int = 0
     feh_ivezic: Optional[A.FehConfig] = None
     feh_gauss: Optional[A.GaussFehConfig] = None
+    multiples: Optional[A.MultiplesConfig] = None
     keep: list = field(default_factory=list)   # keeps ctypes buffers alive
 
     def pixel_array(self):
@@ -204,7 +238,7 @@ class Workload:
         j.nstreams = self.nstreams
         j.capacity = self.capacity
         j.nbands = self.nbands
-        for name in ("foot", "feh", "kin", "phot", "perr", "v2pm", "feh_ivezic", "feh_gauss"):
+        for name in ("foot", "feh", "kin", "phot", "perr", "v2pm", "feh_ivezic", "feh_gauss", "multiples"):
             v = getattr(self, name)
             if v is not None:
                 setattr(j, name, C.pointer(v))

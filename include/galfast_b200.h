@@ -180,6 +180,13 @@ typedef struct gf_table {
     float   *pm;               /* [3] mu_l/mu_ra, mu_b/mu_dec (mas/yr), v_r (km/s) */
     double  *radec;            /* [2] (degrees) */
     int32_t *FeH_comp;         /* Gaussian of the multi-Gaussian metallicity draw (GaussianFeH) */
+    /* unresolved multiple systems (unresolvedMultiples_host.cpp:56-80): absmag + "Sys"[2] holds
+     * the absolute magnitudes of the system's components (99.999 = absent), absmag + "SysNcomp"
+     * their number; absmag then holds the system's total absolute magnitude */
+    float   *absmagSys;        /* [2] */
+    int32_t *absmagSysNcomp;
+    int32_t systems;           /* 1: absmagSys is in use (set by gf_module_multiples); photometry then
+                                * sums the luminosities of the system's components */
 } gf_table;
 
 /* ------------------------------------------------------------------ */
@@ -241,6 +248,33 @@ typedef struct gf_gaussfeh_config {        /* os_GaussianFeH_data, src/modules/G
     float pcum[GF_GAUSSFEH_MAXCOMP];       /* cumulative weights, pcum[ncomp - 1] = 1 */
     uint32_t comp_mask;                    /* components it applies to */
 } gf_gaussfeh_config;
+
+/* os_unresolvedMultiples (unresolvedMultiples_host.cpp:96-189, kernel
+ * unresolvedMultiples_gpu.cu.h:36-123): each star of the selected components may
+ * get a secondary with probability secprob(M1); its absolute magnitude is M1
+ * (equal mass) or drawn from the inverse cumulative LF, above the primary's
+ * cumulative LF value for GF_MULT_LF_M2_GT_M1.  The three tables are sampled at
+ * the nearest texel, as the reference's host build samples its textures:
+ * value(x) = tab[clamp(trunc((x - x0) * inv_dx + 0.5), 0, n - 1)]. */
+typedef enum {
+    GF_MULT_LF_M2_GT_M1 = 1,
+    GF_MULT_LF = 2,
+    GF_MULT_EQUAL_MASS = 3
+} gf_multiples_algo;
+#define GF_MULT_TEX 256
+typedef struct gf_multiples_config {
+    int32_t algo;                          /* gf_multiples_algo */
+    uint32_t comp_mask;                    /* components it applies to */
+    float sec_x0, sec_inv_dx;              /* probability of a secondary, against M1 */
+    int32_t nsec;
+    float secprob[64];
+    float cum_x0, cum_inv_dx;              /* cumulative LF, against M */
+    int32_t ncum;
+    float cumlf[GF_MULT_TEX];
+    float inv_x0, inv_inv_dx;              /* its inverse, against the cumulative value */
+    int32_t ninv;
+    float invcumlf[GF_MULT_TEX];
+} gf_multiples_config;
 
 typedef struct gf_vel2pm_config {          /* os_vel2pm_data, vel2pm_gpu.cu.h:26-34 */
     int32_t coordsys;                      /* 0 = GAL (pmlb), 1 = EQU (pmradec) */
@@ -369,6 +403,15 @@ gf_status gf_module_fixedfeh(gf_ctx *ctx, const gf_fixedfeh_config *cfg, gf_tabl
 gf_status gf_module_feh(gf_ctx *ctx, const gf_feh_config *cfg, gf_table *t, int64_t begin, int64_t end);
 gf_status gf_module_gaussfeh(gf_ctx *ctx, const gf_gaussfeh_config *cfg, gf_table *t, int64_t begin, int64_t end);
 gf_status gf_module_bond2010(gf_ctx *ctx, const gf_bond2010_config *cfg, gf_table *t, int64_t begin, int64_t end);
+/* os_unresolvedMultiples: the tables from the binary fraction (knots frac_M, frac_p;
+ * nfrac = 0: 1 everywhere) and the luminosity function of the secondaries (knots
+ * lf_M, lf_phi; nlf = 0: flat over [-100, 100]) as os_unresolvedMultiples::construct
+ * builds them; then the module on rows [begin, end), drawing from the context's
+ * streams 256 rows per stream like the other modules.  Rows it skips (hidden,
+ * other components) hold a single-star system: (absmag, 99.999) and 1. */
+gf_status gf_multiples_build(const double *frac_M, const double *frac_p, int32_t nfrac, const double *lf_M,
+                             const double *lf_phi, int32_t nlf, int32_t algo, uint32_t comp_mask, gf_multiples_config *out);
+gf_status gf_module_multiples(gf_ctx *ctx, const gf_multiples_config *cfg, gf_table *t, int64_t begin, int64_t end);
 /* Photometry: upload the colour grids once (os_photometry::construct), then process batches. */
 gf_status gf_photometry_create(gf_ctx *ctx, const gf_photometry_config *cfg, gf_photometry **out);
 gf_status gf_photometry_destroy(gf_photometry *p);
@@ -405,6 +448,7 @@ typedef struct gf_job {
     int32_t gal2other;                         /* 0 = absent, 1 = equatorial (radec) */
     const gf_feh_config *feh_ivezic;           /* os_FeH (after fixedFeH), NULL = absent */
     const gf_gaussfeh_config *feh_gauss;       /* os_GaussianFeH (after os_FeH), NULL = absent */
+    const gf_multiples_config *multiples;      /* os_unresolvedMultiples (after the metallicities), NULL = absent */
 } gf_job;
 
 #define GF_MAX_MODELS 32
@@ -506,8 +550,8 @@ enum {
     GF_COL_ABSMAG = 1u << 4, GF_COL_XYZ = 1u << 5, GF_COL_COMP = 1u << 6, GF_COL_AM = 1u << 7,
     GF_COL_AMINF = 1u << 8, GF_COL_HIDDEN = 1u << 9, GF_COL_FEH = 1u << 10, GF_COL_VCYL = 1u << 11,
     GF_COL_MAGS = 1u << 12, GF_COL_PHOTOFLAGS = 1u << 13, GF_COL_OBSMAGS = 1u << 14, GF_COL_PM = 1u << 15,
-    GF_COL_RADEC = 1u << 16, GF_COL_FEHCOMP = 1u << 17,
-    GF_COL_ALL = (1u << 18) - 1,
+    GF_COL_RADEC = 1u << 16, GF_COL_FEHCOMP = 1u << 17, GF_COL_ABSMAGSYS = 1u << 18, GF_COL_SYSNCOMP = 1u << 19,
+    GF_COL_ALL = (1u << 20) - 1,
     /* the output catalog of the full-sky form: ra, dec, DM, Mr, true and observed
      * magnitudes, vR/vPhi/vZ, proper motions (and radial velocity) */
     GF_COL_CATALOG = GF_COL_RADEC | GF_COL_DM | GF_COL_ABSMAG | GF_COL_MAGS | GF_COL_OBSMAGS | GF_COL_VCYL | GF_COL_PM
@@ -619,6 +663,7 @@ typedef struct gf_textout_config {
     int32_t ncomp;
     const char *version;             /* galfast version for the second header line (NULL: none) */
     int32_t threads;                 /* formatting threads (0: all hardware threads) */
+    int32_t multiples;               /* unresolved multiples present: absmag + "Sys"[2] and + "SysNcomp" */
 } gf_textout_config;
 
 typedef struct gf_textout gf_textout;

@@ -1634,11 +1634,80 @@ int or_module_gaussfeh(const gf_gaussfeh_config *par, uint32_t *rng_state, int32
     return 0;
 }
 
-/* os_photometry_kernel (photometry_gpu.cu.h:87-174) for single stars (nabsmag = 1) */
+/* nearest-texel 1-D table lookup of the host build (cux.h:786-792, 849-855) */
+static float tex1(const float *tab, int n, float x0, float inv_dx, float x)
+{
+    float xi = (x - x0) * inv_dx + 0.5f;
+    if (xi < 0.f) xi = 0.f;
+    else if (xi >= (float)n) xi = (float)(n - 1);
+    return tab[(uint32_t)xi];
+}
+
+/* os_unresolvedMultiples_kernel (unresolvedMultiples_gpu.cu.h:46-123): two system
+ * components; rows the module skips hold a single-star system */
+int or_module_multiples(const gf_multiples_config *c, uint32_t *rng_state, int32_t nstreams, gf_table *t, int64_t begin,
+                        int64_t end)
+{
+    const int64_t P = t->capacity;
+    RngState rs = {rng_state, nstreams};
+    const int64_t n = end - begin, nth = n / 256 + (n % 256 ? 1 : 0);
+    if (nth > nstreams) { g_err = "unresolvedMultiples: more than 256*nstreams rows"; return -1; }
+    parallel_for((int)nth, [&](int th) {
+        Rng rng = rs.load(th);
+        const int64_t rb = begin + 256 * (int64_t)th, re = std::min(begin + 256 * ((int64_t)th + 1), end);
+        for (int64_t row = rb; row < re; row++) {
+            const float M1 = t->absmag[row];
+            t->absmagSys[row] = M1;
+            if (t->hidden[row] || !((c->comp_mask >> t->comp[row]) & 1u)) {
+                t->absmagSys[P + row] = 99.999f;
+                t->absmagSysNcomp[row] = 1;
+                continue;
+            }
+            float Ltot = OR_EXP10F(-0.4f * M1);
+            int ncomps = 1;
+            /* draw_companion */
+            bool has = false;
+            float M2 = 0.f;
+            const float psec = tex1(c->secprob, c->nsec, c->sec_x0, c->sec_inv_dx, M1);
+            float u = rng.uniform();
+            if (!(u > psec)) {
+                has = true;
+                if (c->algo == GF_MULT_EQUAL_MASS) {
+                    M2 = M1;
+                } else {
+                    const float pprim = tex1(c->cumlf, c->ncum, c->cum_x0, c->cum_inv_dx, M1);
+                    u = rng.uniform();
+                    if (c->algo == GF_MULT_LF_M2_GT_M1) u = pprim + u * (1. - pprim);
+                    M2 = tex1(c->invcumlf, c->ninv, c->inv_x0, c->inv_inv_dx, u);
+                    if (c->algo == GF_MULT_LF_M2_GT_M1 && M2 < M1) M2 = M1;
+                }
+            }
+            if (has) {
+                t->absmagSys[P + row] = M2;
+                Ltot += OR_EXP10F(-0.4f * M2);
+                ncomps++;
+            } else {
+                t->absmagSys[P + row] = 99.999f;
+            }
+            float Mtot = -2.5 * OR_LOG10F(Ltot);
+            t->absmag[row] = Mtot;
+            t->absmagSysNcomp[row] = ncomps;
+        }
+        rs.store(th, rng);
+    }, 4);
+    t->systems = 1;
+    return 0;
+}
+
+/* os_photometry_kernel (photometry_gpu.cu.h:87-174); the system's components come
+ * from absmagSys when unresolved multiples ran (photometry_host.cpp:373-376) */
 int or_module_photometry(const gf_photometry_config *lt, gf_table *t, int64_t begin, int64_t end)
 {
     const int64_t P = t->capacity;
     const int ncolors = lt->nbands - 1;
+    const bool sys = t->systems && t->absmagSys;
+    const float *Mr = sys ? t->absmagSys : t->absmag;
+    const int nabsmag = sys ? 2 : 1;
     Phot ph = {lt};
     parallel_rows(end - begin, [&](int64_t rb_, int64_t re_) {
         for (int64_t row = begin + rb_; row < begin + re_; row++) {
@@ -1648,8 +1717,9 @@ int or_module_photometry(const gf_photometry_config *lt, gf_table *t, int64_t be
             if (!((lt->comp_mask >> cmp) & 1u)) continue;
             float fFeH = t->FeH[row];
             uint32_t flag = 0;
-            float fMr = t->absmag[row];
-            if (!(fMr >= 99.999f)) {
+            for (int syscomp = 0; syscomp < nabsmag; syscomp++) {
+                float fMr = Mr[syscomp * P + row];
+                if (fMr >= 99.999f) break;
                 for (int ic = 0; ic < ncolors; ic++) {
                     bool fl;
                     c[ic] = ph.tex(ic, fFeH, fMr, fl);
@@ -1660,6 +1730,7 @@ int or_module_photometry(const gf_photometry_config *lt, gf_table *t, int64_t be
                     if (b < lt->bidx) { for (int i = b; i != lt->bidx; i++) M += c[i]; }
                     if (b > lt->bidx) { for (int i = lt->bidx; i != b; i++) M -= c[i]; }
                     float L = OR_EXP10F(-0.4f * M);
+                    if (syscomp) L += t->mags[b * P + row];
                     t->mags[b * P + row] = L;
                 }
             }

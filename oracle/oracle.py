@@ -48,6 +48,7 @@ def load(flavour="p"):
         L.or_module_bond2010.argtypes = [vp, vp, C.c_int32, vp, C.c_int64, C.c_int64]
         L.or_module_feh.argtypes = [vp, vp, C.c_int32, vp, C.c_int64, C.c_int64]
         L.or_module_gaussfeh.argtypes = [vp, vp, C.c_int32, vp, C.c_int64, C.c_int64]
+        L.or_module_multiples.argtypes = [vp, vp, C.c_int32, vp, C.c_int64, C.c_int64]
         L.or_module_photometry.argtypes = [vp, vp, C.c_int64, C.c_int64]
         L.or_module_photoerrors.argtypes = [vp, C.c_int64, vp, C.c_int64, C.c_int64]
         L.or_module_vel2pm.argtypes = [vp, vp, C.c_int64, C.c_int64]
@@ -180,8 +181,10 @@ def run_catalog(w, multipliers, flavour="p", sink=None, threads=1, table=None):
                     L.or_module_clipper(C.addressof(w.foot), None, C.addressof(t.t), 0, size)
                 if w.feh is not None:
                     L.or_module_fixedfeh(C.addressof(w.feh), C.addressof(t.t), 0, size)
+                t.t.systems = 0
                 for fm, fn in ((getattr(w, "feh_ivezic", None), L.or_module_feh),
-                               (getattr(w, "feh_gauss", None), L.or_module_gaussfeh)):
+                               (getattr(w, "feh_gauss", None), L.or_module_gaussfeh),
+                               (getattr(w, "multiples", None), L.or_module_multiples)):
                     if fm is not None and fn(C.addressof(fm), state.ctypes.data, NS, C.addressof(t.t), 0, size) != 0:
                         raise RuntimeError(L.or_last_error().decode())
                 if w.kin is not None:

@@ -26,6 +26,11 @@ int main()
         if (X < 0xffffffffll && passes((uint64_t)(X + 1), thr)) bad++;
         /* every x up to X passes: spot-check below X */
         if (X >= 0 && X >= 3 && !passes((uint64_t)(X - 3), thr)) bad++;
+        /* the cheaper threshold: never above the exact one, its x passes, at most 3.6e-7 below */
+        const int64_t Y = gfr::uniform_threshold_lower(thr);
+        if (Y > X) bad++;
+        if (Y >= 0 && !passes((uint64_t)Y, thr)) bad++;
+        if (thr > 1e-6f && thr < 1.f && (double)(X - Y) > 3.6e-7 * (double)X + 2.0) bad++;
     };
     for (int i = 0; i < 2000000; i++) check((float)U(g));
     for (int i = 0; i < 200000; i++) check((float)std::exp(-40.0 * U(g)));

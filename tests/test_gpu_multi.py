@@ -222,3 +222,26 @@ def test_metallicity_modules_in_the_batched_passes(lib):
                     y = y[: x.shape[0]]
                 np.testing.assert_array_equal(x, y, err_msg="%s request %d model %d" % (c, j, m))
     ctx.close()
+
+
+def test_unresolved_multiples_in_the_batched_passes(lib):
+    """os_unresolvedMultiples over the rows of many requests (256-row chunks on
+    each request's streams), with photometry over the systems: rows equal the
+    standalone run's."""
+    ws = requests(lib, n=4)
+    for w in ws:
+        w.multiples = W.multiples_config(lib, comp_mask=0b011, fraction=W.MULT_FRACTION, lf=W.MULT_LF)
+    ctx = G.Context(0)
+    got = {}
+    G.run_catalog_multi(ctx, ws, sink=lambda j, m, rows: got.setdefault(j, {}).setdefault(m, []).append(rows))
+    for j, w in enumerate(ws):
+        ref, st = catalog_alone(ctx, w)
+        for m in ref:
+            b = {k: np.concatenate([p[k] for p in got[j][m]], axis=-1) for k in got[j][m][0]}
+            for c in ref[m]:
+                x, y = ref[m][c], b[c]
+                if c in ("mags", "obsmags"):
+                    y = y[: x.shape[0]]
+                np.testing.assert_array_equal(x, y, err_msg="%s request %d model %d" % (c, j, m))
+        assert any((ref[m]["absmagSysNcomp"] == 2).any() for m in ref)
+    ctx.close()

@@ -241,3 +241,32 @@ def test_metallicity_modules_parity(ctx, lib, multipliers):
         assert_same(g, o, MODULE_COLS + ["FeH_comp"], exact=False)
         nonzero += int((g["FeH_comp"] == 1).sum())
     assert nonzero > 0
+
+
+@pytest.mark.parametrize("algo", [1, 2, 3])
+def test_unresolved_multiples_parity(ctx, lib, multipliers, algo):
+    """os_unresolvedMultiples between the metallicities and Bond2010 (the disks
+    only), for each secondary-magnitude algorithm: the system magnitudes, the
+    component magnitudes and counts, and the photometry summed over the
+    components equal the oracle's; the streams carry the module's uniforms into
+    Bond2010 and across 4000-row batches."""
+    w = small_patch(lib, capacity=4000)
+    w.multiples = W.multiples_config(lib, algo=algo, comp_mask=0b011, fraction=W.MULT_FRACTION, lf=W.MULT_LF)
+    gs, os_, gb, ob = run_both(ctx, w, multipliers)
+    assert len(gb) == len(ob) > 3
+    binaries = singles = 0
+    for (gm, go, g), (om, oo, o) in zip(gb, ob):
+        assert (gm, go) == (om, oo)
+        assert_same(g, o, SKY_COLS + ["absmagSys", "absmagSysNcomp"])
+        assert_same(g, o, MODULE_COLS, exact=False)
+        vis = g["hidden"] == 0
+        disk = vis & (g["comp"] != 2)
+        binaries += int((g["absmagSysNcomp"][disk] == 2).sum())
+        singles += int((g["absmagSysNcomp"][disk] == 1).sum())
+        assert (g["absmagSysNcomp"][vis & (g["comp"] == 2)] == 1).all()
+        two = g["absmagSysNcomp"] == 2
+        if algo == 1:
+            assert (g["absmagSys"][1][two] >= g["absmagSys"][0][two]).all()
+        if algo == 3:
+            assert (g["absmagSys"][1][two] == g["absmagSys"][0][two]).all()
+    assert binaries > 100 and singles > 100

@@ -60,7 +60,7 @@ def test_struct_layouts(tmp_path):
               "gf_vel2pm_config": A.Vel2pmConfig, "gf_skygen_model_info": A.ModelInfo, "gf_job": G.Job,
               "gf_catalog_stats": G.CatalogStats, "gf_precision_report": A.PrecisionReport,
               "gf_textout_config": G.TextoutConfig, "gf_textout_set": G.TextoutSet,
-              "gf_server_info": G.ServerInfo}
+              "gf_server_info": G.ServerInfo, "gf_multiples_config": A.MultiplesConfig}
     checked = 0
     for line in out.split("\n"):
         if not line.strip():
@@ -266,3 +266,56 @@ def test_uniform_threshold_integer_test_equals_float_test(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True)
     n, bad = (int(x) for x in r.stdout.split())
     assert r.returncode == 0 and bad == 0 and n > 2000000, r.stdout
+
+
+def _interp(xa, ya, x):
+    """GSL linear interpolation with linear extrapolation (the reference's spline)."""
+    n = len(xa)
+    lo, hi = 0, n - 1
+    while hi > lo + 1:
+        mid = (hi + lo) // 2
+        if xa[mid] > x:
+            hi = mid
+        else:
+            lo = mid
+    dx = xa[lo + 1] - xa[lo]
+    return ya[lo] + (x - xa[lo]) / dx * (ya[lo + 1] - ya[lo]) if dx > 0 else 0.0
+
+
+def test_multiples_tables_follow_the_reference_construction(lib):
+    """gf_multiples_build: the binary fraction resampled to 64 texels, the
+    normalised trapezoid integral of the secondaries' LF at 256 points and its
+    inverse resampled to 256 texels (unresolvedMultiples_host.cpp:120-189,
+    cux.cpp:330-350), restated here in Python double precision."""
+    from galfast_b200 import workloads as W
+    fm, fp = W.MULT_FRACTION
+    lm, lp = W.MULT_LF
+    c = W.multiples_config(lib, algo=A.GF_MULT_LF, comp_mask=5, fraction=W.MULT_FRACTION, lf=W.MULT_LF)
+    assert c.algo == A.GF_MULT_LF and c.comp_mask == 5 and c.nsec == 64 and c.ncum == c.ninv == 256
+
+    def resample(X, Y, n):
+        X0, X1 = X[0], X[-1]
+        dX = (X1 - X0) / (n - 1)
+        return [np.float32(_interp(X, Y, X0 + i * dX)) for i in range(n)], np.float32(X0), np.float32(1.0 / dX)
+    tab, x0, inv = resample(fm, fp, 64)
+    assert list(np.array(c.secprob[:64], dtype=np.float32)) == tab and c.sec_x0 == x0 and c.sec_inv_dx == inv
+    dx = (lm[-1] - lm[0]) / 255
+    xc, yc = [lm[0]], [0.0]
+    yprev = _interp(lm, lp, lm[0])
+    for i in range(1, 256):
+        xx = lm[0] + i * dx
+        yy = _interp(lm, lp, xx)
+        xc.append(xx)
+        yc.append(yc[-1] + (yprev + 0.5 * (yy - yprev)) * dx)
+        yprev = yy
+    yc = [v / yc[-1] for v in yc]
+    tab, x0, inv = resample(xc, yc, 256)
+    assert list(np.array(c.cumlf[:256], dtype=np.float32)) == tab and c.cum_x0 == x0 and c.cum_inv_dx == inv
+    tab, x0, inv = resample(yc, xc, 256)
+    assert list(np.array(c.invcumlf[:256], dtype=np.float32)) == tab and c.inv_x0 == x0 and c.inv_inv_dx == inv
+    # no fraction file: 1 over [-100, 100] (two texels); no LF: flat
+    d = W.multiples_config(lib, algo=A.GF_MULT_EQUAL_MASS)
+    assert d.nsec == 2 and list(d.secprob[:2]) == [1.0, 1.0] and d.sec_x0 == -100.0
+    assert abs(d.cumlf[128] - 128 / 255) < 1e-6
+    with pytest.raises(RuntimeError):
+        W.multiples_config(lib, algo=7)

@@ -309,3 +309,34 @@ def test_fits_catalog_structure_and_rows(tmp_path, lib):
     assert meta[0]["EXTNAME"] == "METADATA" and meta[0]["NAXIS2"] == 1 and meta[0]["TTYPE1"] == "HEADER"
     text_header = header(version="0.0.0-test")[2:-1]
     assert meta[2].rstrip(b"\0").decode() == text_header
+
+
+def test_multiples_columns_in_the_text_header(tmp_path, lib):
+    """With unresolved multiples the absolute magnitude loses its M1 alias and the
+    system columns absSDSSrSys[2] and absSDSSrSysNcomp join the name-sorted
+    columns (unresolvedMultiples_host.cpp:56-80, serialize_def order)."""
+    n = 500
+    t = random_table(n)
+    A_ = t.arrays
+    A_["absmagSys"][:, :n] = np.random.default_rng(3).uniform(-1, 16, (2, n))
+    A_["absmagSys"][1, :n:3] = 99.999
+    A_["absmagSysNcomp"][0, :n] = np.where(A_["absmagSys"][1, :n] < 99, 2, 1)
+    w = workload(lib)
+    w.multiples = W.multiples_config(lib)
+    cfg = G.textout_config(w)
+    path = tmp_path / "m.txt"
+    wr = G.TextWriter(path, cfg)
+    wr.write(t.t, 0, n)
+    wr.close()
+    lines = path.read_text().split("\n")
+    defs = lines[0][2:].split()
+    assert defs[4] == "absSDSSr{alias=absmag;band=SDSSr;}"
+    assert defs[11:13] == ["absSDSSrSys[2]{class=magnitude;fieldNames=0:M1,1:M2;alias=absmagSys;band=SDSSr;}",
+                           "absSDSSrSysNcomp{type=int;fmt=%1d;}"]
+    vis = np.nonzero(A_["hidden"][0, :n] == 0)[0]
+    first = lines[1].split(" ")
+    r = vis[0]
+    # lb 2, radec 2, XYZ 3, DM, absmag, comp, FeH, vcyl 3, pm 3, Am, AmInf = 19 fields, then the system columns
+    sysf = [f for f in first if f != ""]
+    assert printf("% 7.3f", float(A_["absmagSys"][0, r])).strip() == sysf[19]
+    assert str(int(A_["absmagSysNcomp"][0, r])) == sysf[21]
