@@ -951,7 +951,7 @@ def bench_single(args, G, W, ctx, rank, world, dist):
                 "warmup": args.warmup, "ms_per_step": float(np.mean(times)), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": desc, "pixels": w.npixels, "bins_per_step": bins,
-                           "stars_per_step": stars_step, "batch_rows": w.capacity, "nthreads": w.sky.nthreads,
+                           "stars_per_step": float(np.mean(stars)), "batch_rows": w.capacity, "nthreads": w.sky.nthreads,
                            "parallelism": "replicas" if world > 1 else "single request",
                            "l2": "inputs larger than L2 (164 MB pixel list, 10+ GB catalog per step)",
                            "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99))},

@@ -138,6 +138,8 @@ def lib():
         L.gf_footprint_pixelize.argtypes = [C.POINTER(Footprint), C.c_double, C.POINTER(Lambert),
                                             C.POINTER(Extinction), C.POINTER(PencilBeam), C.POINTER(C.c_float),
                                             C.c_int64, C.POINTER(C.c_int64)]
+        L.gf_extinction_beam_minima.argtypes = [C.POINTER(Extinction), C.POINTER(Lambert), C.POINTER(PencilBeam), C.c_int32,
+                                                C.POINTER(C.c_float), C.POINTER(C.c_int32)]
         L.gf_photometry_build.argtypes = [C.POINTER(C.c_double), C.c_int32, C.c_int32, C.c_double, C.c_double,
                                           C.POINTER(C.c_float), C.POINTER(C.c_uint8), C.POINTER(C.c_int32),
                                           C.POINTER(C.c_int32), C.POINTER(C.c_float), C.POINTER(C.c_float)]

@@ -6,10 +6,12 @@ GF_MODEL_EXP_DISK = 1
 GF_MODEL_POWER_LAW_ELLIPSOID = 2
 GF_MODEL_BROKEN_POWER_LAW = 3
 GF_MODEL_LCBULGE = 4
+GF_MODEL_DENSITY_CUBE = 5
 GF_FRAME_GALPLANE = 0
 GF_FRAME_EXPLICIT = 1
 GF_EXT_NONE = 0
 GF_EXT_SCREEN_CSCB = 1
+GF_EXT_MAPS = 2
 GF_FOOT_ALL = 0
 GF_FOOT_LAMBERT_RECT = 1
 GF_FOOT_CAP = 2
@@ -47,11 +49,16 @@ class ModelConfig(C.Structure):
                 ("T", C.c_double * 3), ("M", C.c_double * 9),
                 ("lf_l", C.c_double), ("lf_b", C.c_double), ("lf_D", C.c_double),
                 ("lf_M", C.POINTER(C.c_double)), ("lf_phi", C.POINTER(C.c_double)), ("lf_n", C.c_int32),
-                ("nbreaks", C.c_int32), ("n_brk", C.c_double * 10), ("rbreak", C.c_double * 9)]
+                ("nbreaks", C.c_int32), ("n_brk", C.c_double * 10), ("rbreak", C.c_double * 9),
+                ("cube", C.POINTER(C.c_float)), ("cube_n", C.c_int32 * 3), ("cube_tc", (C.c_float * 2) * 3)]
+
+
+class ExtMap(C.Structure):                # gf_ext_map: one hemisphere's 3-D extinction map
+    _fields_ = [("A", C.POINTER(C.c_float)), ("n", C.c_int32 * 3), ("tc", (C.c_float * 2) * 3)]
 
 
 class Extinction(C.Structure):
-    _fields_ = [("kind", C.c_int32), ("A0", C.c_float)]
+    _fields_ = [("kind", C.c_int32), ("A0", C.c_float), ("north", C.POINTER(ExtMap)), ("south", C.POINTER(ExtMap))]
 
 
 class Footprint(C.Structure):
@@ -144,7 +151,7 @@ EXPORTS = [
     "gf_photometry_create", "gf_photometry_destroy", "gf_module_photometry",
     "gf_photoerr_create", "gf_photoerr_destroy", "gf_module_photoerrors",
     "gf_module_vel2pm", "gf_module_gal2other",
-    "gf_lambert_init", "gf_footprint_pixelize", "gf_photometry_build",
+    "gf_lambert_init", "gf_footprint_pixelize", "gf_photometry_build", "gf_extinction_beam_minima",
     "gf_multipliers", "gf_rng_seed_host", "gf_mt19937_outputs", "gf_skygen_setup_host",
     "gf_skygen_integrate_static",
 ]

@@ -115,6 +115,7 @@ void set_last_error(const std::string &msg) { gfa::g_err = msg; }
 struct ModelState {
     gfh::HostModel hm;
     float *d_lf = nullptr;
+    float *d_cube = nullptr;                 /* density cube (GF_MODEL_DENSITY_CUBE) */
     float *d_Dtab = nullptr;                 /* D[im][iM] */
     bool crawl_init = false;
     bool done = false;
@@ -140,6 +141,9 @@ struct gf_skygen {
     int64_t *h_nstars = nullptr;         /* pinned [nthreads] */
     uint32_t *d_rng_snap = nullptr;      /* [3][nthreads] */
     StarRecord *d_rec = nullptr, *d_rec2 = nullptr;
+    float *d_rec_am = nullptr, *d_rec_am2 = nullptr;   /* GF_EXT_MAPS: anchor extinction per record */
+    bool maps = false;                                 /* GF_EXT_MAPS: the records carry their anchor's extinction */
+    float *d_map[2] = {nullptr, nullptr};              /* device copies of the extinction maps */
     int64_t rec_cap = 0;
     /* placement + sort buffers (rec_cap rows) */
     double *d_lb = nullptr;
@@ -187,18 +191,28 @@ gf_status ensure_rec_capacity(gf_skygen *s, int64_t need, int64_t keep)
     int64_t cap = std::max<int64_t>(need, s->rec_cap * 3 / 2);
     cap = std::max<int64_t>(cap, 4096);
     StarRecord *old = s->d_rec;
+    float *old_am = s->d_rec_am;
     s->d_rec = nullptr;
+    s->d_rec_am = nullptr;
     if (keep > 0 && old) {
         StarRecord *nr = nullptr;
         GF_TRY(dev_alloc(&nr, cap));
         GF_CUDA(cudaMemcpyAsync(nr, old, sizeof(StarRecord) * (size_t)keep, cudaMemcpyDeviceToDevice, s->ctx->stream));
+        if (s->maps && old_am) {
+            float *na = nullptr;
+            GF_TRY(dev_alloc(&na, cap));
+            GF_CUDA(cudaMemcpyAsync(na, old_am, 4 * (size_t)keep, cudaMemcpyDeviceToDevice, s->ctx->stream));
+            s->d_rec_am = na;
+        }
         GF_CUDA(cudaStreamSynchronize(s->ctx->stream));
         dev_free(old);
         s->d_rec = nr;
     } else {
         dev_free(old);
     }
+    dev_free(old_am);
     dev_free(s->d_rec2);
+    dev_free(s->d_rec_am2);
     dev_free(s->d_lb); dev_free(s->d_projIdx); dev_free(s->d_hidden);
     dev_free(s->d_projXY); dev_free(s->d_DM); dev_free(s->d_absmag); dev_free(s->d_XYZ);
     dev_free(s->d_Am); dev_free(s->d_AmInf);
@@ -208,6 +222,10 @@ gf_status ensure_rec_capacity(gf_skygen *s, int64_t need, int64_t keep)
     s->rec_cap = 0;
     if (!s->d_rec) GF_TRY(dev_alloc(&s->d_rec, cap));
     GF_TRY(dev_alloc(&s->d_rec2, cap));
+    if (s->maps) {
+        if (!s->d_rec_am) GF_TRY(dev_alloc(&s->d_rec_am, cap));
+        GF_TRY(dev_alloc(&s->d_rec_am2, cap));
+    }
     GF_TRY(dev_alloc(&s->d_lb, 2 * cap));
     GF_TRY(dev_alloc(&s->d_projIdx, cap));
     GF_TRY(dev_alloc(&s->d_hidden, cap));
@@ -244,6 +262,7 @@ gfk::LaunchCrawl crawl_launch(gf_skygen *s, ModelState &ms)
     L.stream_end = s->nthreads;
     L.limits = s->d_limits;
     L.rec = s->d_rec;
+    L.rec_am = s->d_rec_am;
     L.rec_capacity = s->rec_cap;
     L.rec_count = s->ctx->d_counters;
     L.err = s->ctx->d_counters + 2;
@@ -283,8 +302,8 @@ gf_status snapshot_range(gf_skygen *s, ModelState &ms, int a, int b, bool restor
 }
 
 /* keep the records of streams before t, and the first keep_t[0] stars of stream t */
-__global__ void filter_records(const StarRecord *in, int64_t n, int32_t t, const int64_t *keep_t, StarRecord *out,
-                               unsigned long long *count)
+__global__ void filter_records(const StarRecord *in, const float *in_am, int64_t n, int32_t t, const int64_t *keep_t,
+                               StarRecord *out, float *out_am, unsigned long long *count)
 {
     const int64_t kt = *keep_t;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -292,6 +311,7 @@ __global__ void filter_records(const StarRecord *in, int64_t n, int32_t t, const
         if (r.stream < t || (r.stream == t && (int64_t)r.seq < kt)) {
             unsigned long long k = atomicAdd(count, 1ull);
             out[k] = r;
+            if (in_am) out_am[k] = in_am[i];
         }
     }
 }
@@ -554,9 +574,41 @@ gf_status gf_skygen_create(gf_ctx *ctx, const gf_skygen_config *cfg, const gf_pe
     auto bail = [&](gf_status code) { gf_skygen_destroy(s); return code; };
     if ((st = dev_alloc(&s->d_pixels, npixels)) != GF_OK) return bail(st);
     cudaMemcpy(s->d_pixels, pixels, sizeof(gf_pencil_beam) * (size_t)npixels, cudaMemcpyHostToDevice);
+    /* 3-D extinction maps: device copies and the per-beam rows of nz minima */
+    size_t ammin_per_beam = 1;
+    if (ext && ext->kind == GF_EXT_MAPS) {
+        const gf_ext_map *mp[2] = {ext->north, ext->south};
+        int nz = 0;
+        for (int h = 0; h < 2; h++) {
+            if (!mp[h]) continue;
+            const gf_ext_map &e = *mp[h];
+            if (!e.A || e.n[0] < 1 || e.n[1] < 1 || e.n[2] < 1 || (nz && e.n[2] != nz))
+                return bail(fail(GF_E_INVALID, "invalid extinction map (or north/south depths differ)"));
+            nz = e.n[2];
+            const size_t n = (size_t)e.n[0] * e.n[1] * e.n[2];
+            if ((st = dev_alloc(&s->d_map[h], n)) != GF_OK) return bail(st);
+            cudaMemcpy(s->d_map[h], e.A, 4 * n, cudaMemcpyHostToDevice);
+            s->geom.map[h] = s->d_map[h];
+            for (int a = 0; a < 3; a++) {
+                s->geom.map_n[h][a] = e.n[a];
+                s->geom.map_tc[h][a][0] = e.tc[a][0];
+                s->geom.map_tc[h][a][1] = e.tc[a][1];
+            }
+            s->geom.ext_tcz[0] = e.tc[2][0];
+            s->geom.ext_tcz[1] = e.tc[2][1];
+        }
+        if (nz == 0) {                 /* no map: zero extinction, one texel of minima */
+            nz = 1;
+            s->geom.ext_tcz[0] = 0.f;
+            s->geom.ext_tcz[1] = 1.f;
+        }
+        s->geom.ext_nz = nz;
+        s->maps = true;
+        ammin_per_beam = (size_t)nz;
+    }
     if (beam_ammin) {
-        if ((st = dev_alloc(&s->d_ammin, npixels)) != GF_OK) return bail(st);
-        cudaMemcpy(s->d_ammin, beam_ammin, 4 * (size_t)npixels, cudaMemcpyHostToDevice);
+        if ((st = dev_alloc(&s->d_ammin, ammin_per_beam * (size_t)npixels)) != GF_OK) return bail(st);
+        cudaMemcpy(s->d_ammin, beam_ammin, 4 * ammin_per_beam * (size_t)npixels, cudaMemcpyHostToDevice);
     }
     s->geom.pixels = s->d_pixels;
     s->geom.npixels = npixels;
@@ -571,6 +623,11 @@ gf_status gf_skygen_create(gf_ctx *ctx, const gf_skygen_config *cfg, const gf_pe
         ms.hm = hms[i];
         if ((st = dev_alloc(&ms.d_lf, ms.hm.lf.size())) != GF_OK) return bail(st);
         cudaMemcpy(ms.d_lf, ms.hm.lf.data(), 4 * ms.hm.lf.size(), cudaMemcpyHostToDevice);
+        if (ms.hm.cube) {
+            if ((st = dev_alloc(&ms.d_cube, ms.hm.cube_size)) != GF_OK) return bail(st);
+            cudaMemcpy(ms.d_cube, ms.hm.cube, 4 * ms.hm.cube_size, cudaMemcpyHostToDevice);
+            ms.hm.m.cube = ms.d_cube;
+        }
         if ((st = dev_alloc(&ms.d_Dtab, (size_t)ms.hm.m.nm * ms.hm.m.nM)) != GF_OK) return bail(st);
         if (gfk::launch_dtab(ms.hm.m, ms.d_Dtab, ctx->stream) != cudaSuccess) return bail(fail(GF_E_CUDA, "distance table"));
         if ((st = alloc_crawl_state(s->nthreads, ms.st, &ms.st_mem)) != GF_OK) return bail(st);
@@ -592,13 +649,15 @@ gf_status gf_skygen_destroy(gf_skygen *s)
     cudaStreamSynchronize(s->ctx->stream);
     for (auto &ms : s->models) {
         dev_free(ms.d_lf);
+        dev_free(ms.d_cube);
         dev_free(ms.d_Dtab);
         if (ms.st_mem) cudaFree(ms.st_mem);
         if (ms.snap_mem) cudaFree(ms.snap_mem);
     }
     dev_free(s->d_pixels); dev_free(s->d_ammin); dev_free(s->d_limits); dev_free(s->d_rng_snap);
     if (s->h_nstars) cudaFreeHost(s->h_nstars);
-    dev_free(s->d_rec); dev_free(s->d_rec2);
+    dev_free(s->d_rec); dev_free(s->d_rec2); dev_free(s->d_rec_am); dev_free(s->d_rec_am2);
+    dev_free(s->d_map[0]); dev_free(s->d_map[1]);
     dev_free(s->d_lb); dev_free(s->d_projIdx); dev_free(s->d_hidden);
     dev_free(s->d_projXY); dev_free(s->d_DM); dev_free(s->d_absmag); dev_free(s->d_XYZ);
     dev_free(s->d_Am); dev_free(s->d_AmInf);
@@ -892,8 +951,11 @@ gf_status gf_skygen_draw(gf_skygen *s, int32_t model, gf_table *out, int64_t *n_
             r_hi = first_batch ? N : w_hi;
         }
         int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)gfk::sm_count() * 16);
-        if (total > 0) filter_records<<<std::max(blocks, 1), 256, 0, st>>>(s->d_rec, total, t, s->d_keep, s->d_rec2, s->ctx->d_counters);
+        if (total > 0)
+            filter_records<<<std::max(blocks, 1), 256, 0, st>>>(s->d_rec, s->d_rec_am, total, t, s->d_keep, s->d_rec2,
+                                                                s->d_rec_am2, s->ctx->d_counters);
         std::swap(s->d_rec, s->d_rec2);
+        std::swap(s->d_rec_am, s->d_rec_am2);
         set_limits<<<fb, 256, 0, st>>>(s->d_limits, N, t, Lt);
         gfk::LaunchCrawl L = crawl_launch(s, ms);
         L.stream_begin = r_lo;
@@ -920,6 +982,7 @@ gf_status gf_skygen_draw(gf_skygen *s, int32_t model, gf_table *out, int64_t *n_
     P.m.lf = ms.d_lf;
     P.g = s->geom;
     P.rec = s->d_rec;
+    P.rec_am = s->d_rec_am;
     P.n = nbatch;
     P.lb = s->d_lb; P.projIdx = s->d_projIdx; P.projXY = s->d_projXY; P.DM = s->d_DM; P.absmag = s->d_absmag;
     P.XYZ = s->d_XYZ; P.Am = s->d_Am; P.AmInf = s->d_AmInf; P.hidden = s->d_hidden; P.key = s->d_key;

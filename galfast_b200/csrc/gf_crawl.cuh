@@ -138,6 +138,51 @@ __device__ __forceinline__ float beam_extinction(const SkyGeom &g, const gf_penc
     return g.ammin[pix.extIdx];
 }
 
+/* nearest texel index of coordinate v on an axis of n texels (cux.h:800-809, 860-874) */
+__host__ __device__ __forceinline__ uint32_t tex_index(float v, float x0, float inv_dx, int n)
+{
+    float t = (v - x0) * inv_dx + 0.5f;
+    if (t < 0.f) t = 0.f;
+    else if (t >= (float)n) t = (float)(n - 1);
+    return (uint32_t)t;
+}
+
+/* the anchor's extinction at distance modulus DM (compute_pos, skygen.cu.h:216-229):
+ * the beam's row of minima at the nearest DM texel with 3-D maps, else the beam's value */
+__device__ __forceinline__ float beam_extinction_dm(const SkyGeom &g, const gf_pencil_beam &pix, float DM)
+{
+    if (g.ext_kind != GF_EXT_MAPS) return beam_extinction(g, pix);
+    if (g.ammin == nullptr) return 0.f;
+    const uint32_t k = tex_index(DM, g.ext_tcz[0], g.ext_tcz[1], g.ext_nz);
+    return g.ammin[(size_t)pix.extIdx * (size_t)g.ext_nz + k];
+}
+
+/* sampleExtinction (skygen.cu.h:199-208): the map of hemisphere proj at (X, Y, DM) */
+__device__ __forceinline__ float map_extinction(const SkyGeom &g, int proj, float X, float Y, float DM)
+{
+    const float *A = g.map[proj];
+    if (A == nullptr) return 0.f;
+    const int32_t *n = g.map_n[proj];
+    const uint32_t i = tex_index(X, g.map_tc[proj][0][0], g.map_tc[proj][0][1], n[0]);
+    const uint32_t j = tex_index(Y, g.map_tc[proj][1][0], g.map_tc[proj][1][1], n[1]);
+    const uint32_t k = tex_index(DM, g.map_tc[proj][2][0], g.map_tc[proj][2][1], n[2]);
+    return A[((size_t)k * (size_t)n[1] + j) * (size_t)n[0] + i];
+}
+
+/* nearest-texel sample of a model's density cube (cux.h:800-809, 860-874) */
+__host__ __device__ __forceinline__ float cube_sample(const SkyModel &m, float x, float y, float z)
+{
+    const float c[3] = {x, y, z};
+    uint32_t ix[3];
+    for (int a = 0; a < 3; a++) {
+        float t = (c[a] - m.cube_tc[a][0]) * m.cube_tc[a][1] + 0.5f;
+        if (t < 0.f) t = 0.f;
+        else if (t >= (float)m.cube_n[a]) t = (float)(m.cube_n[a] - 1);
+        ix[a] = (uint32_t)t;
+    }
+    return m.cube[((size_t)ix[2] * (size_t)m.cube_n[1] + ix[1]) * (size_t)m.cube_n[0] + ix[0]];
+}
+
 /* Model density at the heliocentric position (x, y, z); MODEL is the
  * compile-time model kind (GF_MODEL_EXP_DISK or GF_MODEL_POWER_LAW_ELLIPSOID). */
 template <int MODEL>
@@ -152,6 +197,10 @@ __device__ __forceinline__ float model_rho(const SkyModel &m, float x, float y, 
         if (m.r_cut2 != 0.f && r2 + wz * wz > m.r_cut2) return 0.f;
         float r = sqrtf(r2);
         return m.f * gfm::expf_(-r / m.l - fabsf(wz) / m.h);
+    } else if (m.type == GF_MODEL_DENSITY_CUBE) {
+        /* densityCube::setpos (model_densityCube.h:60-66): the frame gives (Rg - x, -y, z);
+         * nearest texel of the grid */
+        return m.f * cube_sample(m, wx, wy, wz);
     } else if (m.type == GF_MODEL_LCBULGE) {
         /* LCBulge::rho (model_LCBulge.h:79-92): no density factor (the LF carries f) */
         const float t = gfm::powf_(gfm::powf_(wx, m.n) + gfm::powf_(wy / m.ba, m.n) + gfm::powf_(wz / m.ca, m.n),
@@ -189,7 +238,15 @@ __device__ __forceinline__ AnchorX anchor_x(const SkyModel &m, const SkyGeom &g,
     const gf_pencil_beam pix = g.pixels[ilb];
     AnchorX a;
     const float D = bin_distance(m, Dtab, im, iM);
-    const float Am = beam_extinction(g, pix);
+    float Am;
+    if (g.ext_kind == GF_EXT_MAPS) {
+        /* the distance modulus as compute_pos forms it: m = m0 + im dm, DM = m - M */
+        const float M = m.M1 - (float)iM * m.dM;
+        const float mm = m.m0 + (float)im * m.dm;
+        Am = beam_extinction_dm(g, pix, mm - M);
+    } else {
+        Am = beam_extinction(g, pix);
+    }
     float x = D * pix.cl * pix.cb;
     float y = D * pix.sl * pix.cb;
     float z = D * pix.sb;

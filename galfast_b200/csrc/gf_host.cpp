@@ -14,6 +14,8 @@
 #include <dlfcn.h>
 #include <map>
 #include <mutex>
+#include <thread>
+#include <limits>
 
 namespace gfh {
 
@@ -173,7 +175,8 @@ bool setup_models(const gf_skygen_config &cfg, int npixels, const gf_model_confi
         HostModel hm;
         SkyModel &m = hm.m;
         m = base;
-        if (c.type < GF_MODEL_EXP_DISK || c.type > GF_MODEL_LCBULGE) { err = "unknown model type"; return false; }
+        if (c.type < GF_MODEL_EXP_DISK || c.type > GF_MODEL_DENSITY_CUBE) { err = "unknown model type"; return false; }
+        const bool cube = c.type == GF_MODEL_DENSITY_CUBE;
         if (c.comp < 0 || c.comp > 31) { err = "component id must be in [0, 31]"; return false; }
         m.type = c.type;
         m.comp = c.comp;
@@ -191,7 +194,28 @@ bool setup_models(const gf_skygen_config &cfg, int npixels, const gf_model_confi
             double R[9] = {-cosa, 0, sina, 0, -1, 0, sina, 0, cosa};
             for (int k = 0; k < 9; k++) m.M[k] = (float)R[k];
         }
-        if (c.type == GF_MODEL_EXP_DISK) {
+        if (cube) {
+            /* densityCube::setpos: (Rg - x, -y, z) as a frame: T = (-Rg, 0, 0), M = diag(-1, -1, 1) */
+            const float Rg = (float)c.Rg;
+            const float T[3] = {-Rg, 0.f, 0.f}, M[9] = {-1.f, 0.f, 0.f, 0.f, -1.f, 0.f, 0.f, 0.f, 1.f};
+            for (int k = 0; k < 3; k++) m.T[k] = T[k];
+            for (int k = 0; k < 9; k++) m.M[k] = M[k];
+            if (!c.cube) { err = "density cube without a grid"; return false; }
+            size_t n = 1;
+            for (int k = 0; k < 3; k++) {
+                if (c.cube_n[k] < 1 || c.cube_n[k] > 65536) { err = "density cube dimensions must be in [1, 65536]"; return false; }
+                n *= (size_t)c.cube_n[k];
+                m.cube_n[k] = c.cube_n[k];
+                m.cube_tc[k][0] = c.cube_tc[k][0];
+                m.cube_tc[k][1] = c.cube_tc[k][1];
+            }
+            if (n > ((size_t)1 << 31)) { err = "density cube above 2^31 texels"; return false; }
+            hm.cube = c.cube;
+            hm.cube_size = n;
+            m.nbreaks = 0;
+            m.nArr[0] = 0.f;
+            m.fArr[0] = 1.f;
+        } else if (c.type == GF_MODEL_EXP_DISK) {
             if (!(c.l > 0) || !(c.h > 0)) { err = "exponential disk needs l > 0 and h > 0"; return false; }
             m.l = (float)c.l;
             m.h = (float)c.h;
@@ -225,7 +249,17 @@ bool setup_models(const gf_skygen_config &cfg, int npixels, const gf_model_confi
         m.r_cut2 = 0.f;
         m.rminSq = m.rmaxSq = 0.f;
         /* luminosity function (cux.cpp:336-384) */
-        if (c.lf_n <= 0 || !c.lf_M || !c.lf_phi) {
+        if (cube && c.lf_n > 0 && c.lf_M && c.lf_phi) {
+            /* load_and_resample_texture_1D: the knots' range, 1024 texels, no clipping */
+            if (c.lf_n < 2) { err = "LF needs at least 2 knots"; return false; }
+            const std::vector<double> X(c.lf_M, c.lf_M + c.lf_n), Y(c.lf_phi, c.lf_phi + c.lf_n);
+            const int nsamp = 1024;
+            const double X0 = X[0], X1 = X.back(), dX = (X1 - X0) / (nsamp - 1);
+            hm.lf.resize(nsamp);
+            for (int k = 0; k < nsamp; k++) hm.lf[k] = (float)interp_linear(X, Y, X0 + k * dX);
+            m.lf_x0 = (float)X0;
+            m.lf_inv_dx = (float)(1. / dX);
+        } else if (c.lf_n <= 0 || !c.lf_M || !c.lf_phi) {
             hm.lf.assign(2, 1.f);
             m.lf_x0 = -100.f;
             m.lf_inv_dx = (float)(1. / (100. - -100.));
@@ -259,7 +293,9 @@ bool setup_models(const gf_skygen_config &cfg, int npixels, const gf_model_confi
         double rl = lfl * d2r, rb = lfb * d2r;
         float cl = (float)gfm::cos_d(rl), cb = (float)gfm::cos_d(rb), sl = (float)gfm::sin_d(rl), sb = (float)gfm::sin_d(rb);
         float px = lfD * cl * cb, py = lfD * sl * cb, pz = lfD * sb;
-        if (c.type != GF_MODEL_LCBULGE) {
+        if (cube) {
+            m.f = (float)c.f;                /* a plain scale factor (densityCube::load) */
+        } else if (c.type != GF_MODEL_LCBULGE) {
             m.f = 1.f;
             float norm = rho_host(m, px, py, pz);
             if (!(norm != 0.f && std::isnormal(norm))) { err = "density is zero at the LF sampling point"; return false; }
@@ -269,7 +305,7 @@ bool setup_models(const gf_skygen_config &cfg, int npixels, const gf_model_confi
         if (c.type == GF_MODEL_EXP_DISK) {
             float rc = (float)c.rcut;
             m.r_cut2 = rc * rc;
-        } else if (c.type != GF_MODEL_LCBULGE) {
+        } else if (c.type != GF_MODEL_LCBULGE && !cube) {
             float rmin = (float)c.rmin, rmax = (float)c.rmax;
             m.rminSq = rmin * rmin;
             m.rmaxSq = rmax * rmax;
@@ -286,6 +322,7 @@ bool setup_models(const gf_skygen_config &cfg, int npixels, const gf_model_confi
         if ((long long)m.nm * m.nM > 0x3fffffff) { err = "magnitude grid too large"; return false; }
         if (m.nm > 32767 || m.nM > 32767) { err = "magnitude grid dimension above 32767"; return false; }
         m.lf = nullptr;
+        m.cube = nullptr;                  /* the device copy is attached by the caller */
         out.push_back(hm);
     }
     return true;
@@ -721,6 +758,82 @@ gf_status gf_multiples_build(const double *frac_M, const double *frac_p, int32_t
     out->ncum = out->ninv = NPIX;
     resample_1d(xcum, ycum, NPIX, out->cumlf, &out->cum_x0, &out->cum_inv_dx);
     resample_1d(ycum, xcum, NPIX, out->invcumlf, &out->inv_x0, &out->inv_inv_dx);
+    return GF_OK;
+}
+
+/* lambert::project (skygen.h:123-130): float direction and pole, double intermediates */
+static void lambert_project(const gf_lambert &p, const gf_pencil_beam &d, float &x, float &y)
+{
+    const double cll0 = d.cl * p.cl + d.sl * p.sl;
+    const double sll0 = p.cl * d.sl - d.cl * p.sl;
+    const double kp = 1.414213562373095 * sqrt(1. / (1. + p.sb * d.sb + p.cb * d.cb * cll0));
+    x = (float)(kp * d.cb * sll0);
+    y = (float)(kp * (p.cb * d.sb - p.sb * d.cb * cll0));
+}
+
+gf_status gf_extinction_beam_minima(const gf_extinction *ext, const gf_lambert proj[2], const gf_pencil_beam *pixels,
+                                    int32_t npixels, float *out, int32_t *nz_out)
+{
+    if (!ext || ext->kind != GF_EXT_MAPS || !proj || npixels < 0 || (npixels && !pixels)) return GF_E_INVALID;
+    const gf_ext_map *mp[2] = {ext->north, ext->south};
+    int nz = 0;
+    for (int h = 0; h < 2; h++) {
+        if (!mp[h]) continue;
+        if (!mp[h]->A || mp[h]->n[0] < 1 || mp[h]->n[1] < 1 || mp[h]->n[2] < 1) return GF_E_INVALID;
+        if (nz && mp[h]->n[2] != nz) return GF_E_INVALID;
+        nz = mp[h]->n[2];
+    }
+    if (nz == 0) nz = 1;                                  /* no map: zero extinction */
+    if (nz_out) *nz_out = nz;
+    if (!out) return GF_OK;
+    for (int32_t i = 0; i < npixels; i++)
+        if (pixels[i].extIdx < 0 || pixels[i].extIdx >= npixels) return GF_E_INVALID;
+    const bool any = mp[0] || mp[1];
+    for (size_t q = 0; q < (size_t)npixels * nz; q++) out[q] = any ? std::numeric_limits<float>::infinity() : 0.f;
+    /* find_extinction_minima (os_skygen.cpp:285-342) for every beam and given map */
+    std::vector<std::thread> th;
+    const int nt = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    for (int w = 0; w < nt; w++) {
+        th.emplace_back([&, w] {
+            for (int32_t i = w; i < npixels; i += nt) {
+                const gf_pencil_beam &p = pixels[i];
+                float *row = out + (size_t)p.extIdx * nz;
+                for (int h = 0; h < 2; h++) {
+                    if (!mp[h]) continue;
+                    const gf_ext_map &e = *mp[h];
+                    const int width = e.n[0], height = e.n[1], depth = e.n[2];
+                    auto tex = [&](int x, int y, int z) { return e.A[((size_t)z * height + y) * width + x]; };
+                    float x, y;
+                    lambert_project(proj[h], p, x, y);
+                    const float tcxx = e.tc[0][0], tcxy = e.tc[0][1], tcyx = e.tc[1][0], tcyy = e.tc[1][1];
+                    const double dr = 1.0001 / 2. * sqrt(2) * (p.dx + std::max(1. / tcxy, 1. / tcyy));
+                    int xi = (int)((x - dr - tcxx) * tcxy);  xi = std::max(0, std::min(xi - 1, width));
+                    int yi = (int)((y - dr - tcyx) * tcyy);  yi = std::max(0, std::min(yi - 1, height));
+                    int xie = (int)((x + dr - tcxx) * tcxy); xie = std::max(0, std::min(xie + 2, width));
+                    int yie = (int)((y + dr - tcyx) * tcyy); yie = std::max(0, std::min(yie + 2, height));
+                    for (int X = xi; X != xie; X++) {
+                        if (X < 0 || X >= width) continue;
+                        for (int Y = yi; Y != yie; Y++) {
+                            if (Y < 0 || Y >= width) continue;       /* the reference compares y with the width */
+                            if (Y >= height) continue;               /* (and never reads past the map) */
+                            /* texels outside the hemisphere's disk hold zero: skip them */
+                            const double Amax = tex(X, Y, depth - 1);
+                            if (Amax == 0) {
+                                const double xx = ((double)X) / tcxy + tcxx;
+                                const double yy = ((double)Y) / tcyy + tcyx;
+                                if (xx * xx + yy * yy > 2) continue;
+                            }
+                            for (int z = 0; z < depth; z++) {
+                                const float Ar = z - 1 < 0 ? 0.f : tex(X, Y, z - 1);
+                                row[z] = std::min(row[z], Ar);
+                            }
+                        }
+                    }
+                }
+            }
+        });
+    }
+    for (auto &t : th) t.join();
     return GF_OK;
 }
 

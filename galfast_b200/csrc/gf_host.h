@@ -41,6 +41,8 @@ double interp_linear(const std::vector<double> &xa, const std::vector<double> &y
 struct HostModel {
     SkyModel m;
     std::vector<float> lf;
+    const float *cube = nullptr;       /* the caller's density grid (GF_MODEL_DENSITY_CUBE), nx*ny*nz floats */
+    size_t cube_size = 0;
 };
 bool setup_models(const gf_skygen_config &cfg, int npixels, const gf_model_config *mc, int nmodels,
                   std::vector<HostModel> &out, std::string &err);

@@ -28,16 +28,27 @@ struct SkyModel {
      * rbreakSq[k - 1] and rbreakSq[k] (a plain power law: nbreaks = 0, nArr[0] = n, fArr[0] = 1) */
     int32_t nbreaks;
     float nArr[10], fArr[10], rbreakSq[9];
+    /* density cube: device grid (x fastest) and per-axis texture coordinates (x0, inv_dx) */
+    const float *cube;
+    int32_t cube_n[3];
+    float cube_tc[3][2];
 };
 
 /* Sky geometry shared by all models of a generator. */
 struct SkyGeom {
     const gf_pencil_beam *pixels;  /* device */
     int32_t npixels;
-    const float *ammin;            /* device, per-beam minimum extinction, or null */
+    const float *ammin;            /* device, per-beam minimum extinction, or null (GF_EXT_MAPS: ext_nz per beam) */
     int32_t ext_kind;
     float A0;
     gf_lambert proj[2];
+    /* GF_EXT_MAPS: depth and DM texture coordinates of the per-beam rows, and the
+     * north/south maps (device, x fastest; null = zero extinction) */
+    int32_t ext_nz;
+    float ext_tcz[2];
+    const float *map[2];
+    int32_t map_n[2][3];
+    float map_tc[2][3][2];
 };
 
 /* A star drawn by the crawl, to be placed by the star kernel. */

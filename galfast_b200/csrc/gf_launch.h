@@ -19,6 +19,7 @@ struct LaunchCrawl {
     int32_t stream_begin, stream_end;
     const int64_t *limits;
     StarRecord *rec;
+    float *rec_am;                 /* GF_EXT_MAPS: anchor extinction per record (parallel to rec), or null */
     int64_t rec_capacity;
     unsigned long long *rec_count;
     unsigned long long *err;
@@ -35,6 +36,7 @@ struct LaunchPlace {
     SkyModel m;
     SkyGeom g;
     const StarRecord *rec;
+    const float *rec_am;           /* GF_EXT_MAPS: anchor extinction per record, or null */
     int64_t n;
     double *lb;
     int32_t *projIdx;

@@ -510,8 +510,12 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                 return fail(GF_E_INVALID, "model kinds must agree across requests (in component order)");
             const long long kmax = (long long)q.hm[i].m.nm * q.hm[i].m.nM;
             if (kmax % GF_BLOCK) q.plain = true;
+            if (q.hm[i].m.type == GF_MODEL_DENSITY_CUBE) q.plain = true;    /* its grid is uploaded by the plain path */
             if (q.hm[i].m.nm + q.hm[i].m.nM > 16384) q.plain = true;
         }
+        /* 3-D extinction maps: the anchors' extinction depends on their distance,
+         * which the slot tables do not carry; such a request takes the plain path */
+        if (J.ext.kind == GF_EXT_MAPS) q.plain = true;
         q.pix_off = pix_total;
         pix_total += J.npixels;
         q.cost = (double)J.npixels * q.hm[0].m.nm;

@@ -46,6 +46,9 @@ __device__ void anchor_fp64(const SkyModel &m, const SkyGeom &g, int ilb, int im
         const double r2 = wx * wx + wy * wy;
         if (m.r_cut2 != 0.f && r2 + wz * wz > (double)m.r_cut2) ms = 0.0;
         else ms = (double)m.f * gfm::exp_d(-sqrt(r2) / (double)m.l - fabs(wz) / (double)m.h);
+    } else if (m.type == GF_MODEL_DENSITY_CUBE) {
+        /* the grid holds float values: the same texel as the float path */
+        ms = (double)m.f * (double)gfc::cube_sample(m, (float)wx, (float)wy, (float)wz);
     } else if (m.type == GF_MODEL_LCBULGE) {
         const double n = (double)m.n;
         const double t = pow_fp64(pow_fp64(wx, n) + pow_fp64(wy / (double)m.ba, n) + pow_fp64(wz / (double)m.ca, n), 1.0 / n);

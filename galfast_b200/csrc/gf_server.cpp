@@ -50,6 +50,10 @@ struct OwnedJob {
     gf_vel2pm_config v2pm;
     gf_feh_config feh_ivezic;
     gf_gaussfeh_config feh_gauss;
+    gf_multiples_config multiples;
+    gf_ext_map maps[2];
+    std::vector<float> map_A[2];
+    std::vector<std::vector<float>> cubes;
 };
 
 template <class T>
@@ -70,8 +74,23 @@ std::shared_ptr<OwnedJob> own(const gf_job &j)
         o->pixels.assign(j.pixels, j.pixels + j.npixels);
         o->job.pixels = o->pixels.data();
     }
+    size_t per_beam = 1;
+    if (j.ext.kind == GF_EXT_MAPS) {
+        /* the maps and the per-beam rows of nz minima */
+        const gf_ext_map *mp[2] = {j.ext.north, j.ext.south};
+        const gf_ext_map **dst[2] = {&o->job.ext.north, &o->job.ext.south};
+        for (int h = 0; h < 2; h++) {
+            if (!mp[h]) continue;
+            if (!mp[h]->A || mp[h]->n[0] < 1 || mp[h]->n[1] < 1 || mp[h]->n[2] < 1) return nullptr;
+            o->maps[h] = *mp[h];
+            o->map_A[h].assign(mp[h]->A, mp[h]->A + (size_t)mp[h]->n[0] * mp[h]->n[1] * mp[h]->n[2]);
+            o->maps[h].A = o->map_A[h].data();
+            *dst[h] = &o->maps[h];
+            per_beam = (size_t)mp[h]->n[2];
+        }
+    }
     if (j.beam_ammin) {
-        o->ammin.assign(j.beam_ammin, j.beam_ammin + j.npixels);
+        o->ammin.assign(j.beam_ammin, j.beam_ammin + per_beam * (size_t)j.npixels);
         o->job.beam_ammin = o->ammin.data();
     }
     if (j.models) {
@@ -83,6 +102,11 @@ std::shared_ptr<OwnedJob> own(const gf_job &j)
             if (m.lf_n < 0) return nullptr;
             if (m.lf_M) { o->lf_M[i].assign(m.lf_M, m.lf_M + m.lf_n); m.lf_M = o->lf_M[i].data(); }
             if (m.lf_phi) { o->lf_phi[i].assign(m.lf_phi, m.lf_phi + m.lf_n); m.lf_phi = o->lf_phi[i].data(); }
+            if (m.type == GF_MODEL_DENSITY_CUBE && m.cube) {
+                if (m.cube_n[0] < 1 || m.cube_n[1] < 1 || m.cube_n[2] < 1) return nullptr;
+                o->cubes.emplace_back(m.cube, m.cube + (size_t)m.cube_n[0] * m.cube_n[1] * m.cube_n[2]);
+                m.cube = o->cubes.back().data();
+            }
         }
         o->job.models = o->models.data();
     }
@@ -92,6 +116,7 @@ std::shared_ptr<OwnedJob> own(const gf_job &j)
     o->job.v2pm = copy_one(j.v2pm, o->v2pm);
     o->job.feh_ivezic = copy_one(j.feh_ivezic, o->feh_ivezic);
     o->job.feh_gauss = copy_one(j.feh_gauss, o->feh_gauss);
+    o->job.multiples = copy_one(j.multiples, o->multiples);
     if (j.phot) {
         o->phot = *j.phot;
         if (o->phot.nbands < 1 || o->phot.nMr < 0 || o->phot.nFeH < 0) return nullptr;

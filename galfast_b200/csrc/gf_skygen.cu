@@ -41,6 +41,7 @@ struct CrawlParams {
     int32_t stream_begin;          /* single-request launch: stream of item 0 */
     JumpTables jt;
     StarRecord *rec;
+    float *rec_am;                 /* GF_EXT_MAPS: the anchor extinction of each record (parallel to rec), or null */
     int64_t rec_capacity;
     unsigned long long *rec_count;
     unsigned long long *err;       /* set when a bin's expected count is infinite */
@@ -137,6 +138,7 @@ struct CrawlSmem {
     uint16_t dense[(CW * 32) * GF_BLOCK];        /* compacted list of the window's anchor slots */
     float mu[DRAW ? CW : 1][GF_BLOCK][32]; /* mu of bin s of each thread's block */
     StarRecord recbuf[DRAW ? GF_RECBUF : 1];
+    float ambuf[DRAW ? GF_RECBUF : 1];
     int nrec;
     int wtot[CW];
     int wev[CW];
@@ -163,7 +165,10 @@ __device__ void flush_records(const CrawlParams &P, CrawlSmem<DRAW, CW> &S, int 
     base = __shfl_sync(FULLMASK, base, 0);
     for (int q = lane; q < n; q += 32) {
         const unsigned long long slot = base + q;
-        if (slot < (unsigned long long)P.rec_capacity) P.rec[slot] = S.recbuf[q];
+        if (slot < (unsigned long long)P.rec_capacity) {
+            P.rec[slot] = S.recbuf[q];
+            if (P.rec_am) P.rec_am[slot] = S.ambuf[q];
+        }
     }
     __syncwarp();
     if (lane == 0) S.nrec = 0;
@@ -176,7 +181,7 @@ __device__ void flush_records(const CrawlParams &P, CrawlSmem<DRAW, CW> &S, int 
  * warp; lane 0 writes. */
 template <int DRAW, int CW>
 __device__ void draw_stars(const CrawlParams &P, CrawlSmem<DRAW, CW> &S, int sid, int lane, gfr::Mwc &r, int &ndraw,
-                           long long &nstars, long long limit, int ilb, int im, int iM)
+                           long long &nstars, long long limit, int ilb, int im, int iM, float am)
 {
     if (!ndraw) return;
     const CrawlJob &J = S.job;
@@ -205,7 +210,7 @@ __device__ void draw_stars(const CrawlParams &P, CrawlSmem<DRAW, CW> &S, int sid
         __syncwarp();
         const int k = S.nrec;
         __syncwarp();
-        if (lane == 0) { S.recbuf[k] = rec; S.nrec = k + 1; }
+        if (lane == 0) { S.recbuf[k] = rec; S.ambuf[k] = am; S.nrec = k + 1; }
         if (k + 1 == GF_RECBUF) flush_records(P, S, lane);
     }
     nstars += todo;
@@ -287,7 +292,7 @@ __device__ __noinline__ void handle_event(const CrawlParams &P, CrawlSmem<DRAW, 
         r.set_v(vb);
         r.used = 0;
         nd = (int)r.poisson(emu);
-        draw_stars<DRAW, CW>(P, S, sid, lane, r, nd, ns, S.limit, e_ilb, e_im, e_iM);
+        draw_stars<DRAW, CW>(P, S, sid, lane, r, nd, ns, S.limit, e_ilb, e_im, e_iM, anc_es.Am);
         vnew = r.v();
         if (nd) flag = 1;             /* the stream reached its limit: pause right after the bin */
         /* The walk assumed one uniform for this bin; it drew r.used >= 1.  Every later
@@ -324,7 +329,7 @@ __device__ __noinline__ void finish_pending(const CrawlParams &P, CrawlSmem<DRAW
     r.set_v(S.v);
     int nd = S.cur.ndraw;
     long long ns = S.nstars;
-    draw_stars<DRAW, CW>(P, S, sid, lane, r, nd, ns, S.limit, S.cur.cur_ilb, S.cur.cur_im, S.cur.cur_iM);
+    draw_stars<DRAW, CW>(P, S, sid, lane, r, nd, ns, S.limit, S.cur.cur_ilb, S.cur.cur_im, S.cur.cur_iM, S.cur.anc.Am);
     __syncwarp();
     if (lane == 0) { S.v = r.v(); S.nstars = ns; S.cur.ndraw = nd; S.next_ck = (int)ns; }
     __syncwarp();
@@ -745,6 +750,7 @@ struct PlaceParams {
     SkyModel m;
     SkyGeom g;
     const StarRecord *rec;
+    const float *rec_am;    /* GF_EXT_MAPS: the anchor extinction of each record, or null */
     int64_t n;
     /* unsorted columns */
     double *lb;             /* [2][n] */
@@ -807,11 +813,20 @@ __device__ __forceinline__ int place_one(const SkyModel &m, const SkyGeom &g, co
     P.XYZ[i] = D * cl * cb;
     P.XYZ[n + i] = D * sl * cb;
     P.XYZ[2 * n + i] = D * sb;
-    float Am0 = (g.ext_kind == GF_EXT_SCREEN_CSCB) ? g.A0 / fabsf(sb) : 0.f;
-    float AmInf = Am0;
+    float Am0, AmInf;
+    if (g.ext_kind == GF_EXT_MAPS) {
+        /* sampleExtinction at the star's DM and at DM = 100 (skygen.cu.h:421-424) */
+        Am0 = gfc::map_extinction(g, pix.projIdx, x, y, DM);
+        const float Am1 = gfc::map_extinction(g, pix.projIdx, x, y, 100.f);
+        AmInf = Am1 > Am0 ? Am1 : Am0;
+    } else {
+        Am0 = (g.ext_kind == GF_EXT_SCREEN_CSCB) ? g.A0 / fabsf(sb) : 0.f;
+        AmInf = Am0;
+    }
     int hid = (mtmp + Am0 > m.m1) ? 1 : 0;
-    /* the beam extinction at the bin's anchor (draw_stars, skygen.cu.h:437-446) */
-    const float AmMin = gfc::beam_extinction(g, pix);
+    /* the extinction at the bin's anchor (draw_stars, skygen.cu.h:437-446): carried with
+     * the record for 3-D maps (it depends on the anchor's distance), else the beam's */
+    const float AmMin = (g.ext_kind == GF_EXT_MAPS && P.rec_am) ? P.rec_am[i] : gfc::beam_extinction(g, pix);
     if (AmMin > Am0) AmInf = -AmMin;
     P.Am[i] = Am0;
     P.AmInf[i] = AmInf;
@@ -974,6 +989,7 @@ cudaError_t launch_crawl(const LaunchCrawl &L, int draw, cudaStream_t s)
     P.stream_begin = L.stream_begin;
     P.jt = L.jt;
     P.rec = L.rec;
+    P.rec_am = L.rec_am;
     P.rec_capacity = L.rec_capacity;
     P.rec_count = L.rec_count;
     P.err = L.err;
@@ -994,7 +1010,7 @@ cudaError_t launch_place(const LaunchPlace &L, cudaStream_t s)
 {
     if (L.n <= 0) return cudaSuccess;
     PlaceParams P;
-    P.m = L.m; P.g = L.g; P.rec = L.rec; P.n = L.n;
+    P.m = L.m; P.g = L.g; P.rec = L.rec; P.rec_am = L.rec_am; P.n = L.n;
     P.lb = L.lb; P.projIdx = L.projIdx; P.projXY = L.projXY; P.DM = L.DM; P.absmag = L.absmag;
     P.XYZ = L.XYZ; P.Am = L.Am; P.AmInf = L.AmInf; P.hidden = L.hidden; P.key = L.key;
     P.nvis = L.nvis;

@@ -77,6 +77,10 @@ extern "C" gf_status gf_skygen_integrate_static(const gf_skygen_config *cfg, con
     std::string err;
     if (!gfh::setup_models(*cfg, npixels, model, 1, hms, err)) return sfail(GF_E_INVALID, err);
     const SkyModel &hm = hms[0].m;
+    if (ext && ext->kind == GF_EXT_MAPS)
+        return sfail(GF_E_UNSUPPORTED, "3-D extinction maps need device copies (use gf_skygen_integrate)");
+    if (hm.type == GF_MODEL_DENSITY_CUBE)
+        return sfail(GF_E_UNSUPPORTED, "the density cube needs a device copy of its grid (use gf_skygen_integrate)");
     if (hm.lf_n > kMaxLF) return sfail(GF_E_INVALID, "luminosity function above the static scratch limit of 1024 samples");
     if ((long long)hm.nm * hm.nM > kMaxBins)
         return sfail(GF_E_INVALID, "nm*nM above the static scratch limit of 65536 bins per pixel");

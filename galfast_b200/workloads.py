@@ -286,6 +286,94 @@ def _model(kind, comp, f, Rg, z0, lfM, lfphi, **kw):
     return m
 
 
+def use_extinction_maps(lib, w, nxy=96, nz=24, dm_range=(4.0, 20.0), A0=0.06, D0=1500.0):
+    """Switch a workload to 3-D extinction maps (GF_EXT_MAPS): for each hemisphere a
+    grid over its Lambert plane (X, Y in [-2, 2], nxy texels a side, texel i at
+    -2 + 4 i / (nxy - 1) as the reference's default map coordinates) and nz distance
+    moduli over dm_range, holding A0 / sin|b| (capped at 20 A0) times
+    (1 - exp(-D / D0)): extinction growing with distance, steeper towards the plane,
+    zero outside the hemisphere's disk.  The per-beam rows come from
+    gf_extinction_beam_minima."""
+    xs = np.linspace(-2.0, 2.0, nxy)
+    dms = np.linspace(dm_range[0], dm_range[1], nz)
+    X, Y = np.meshgrid(xs, xs, indexing="xy")           # [y][x]
+    r2 = X ** 2 + Y ** 2
+    sinb = np.clip(1.0 - 0.5 * r2, 0.0, None)
+    screen = np.where(r2 <= 2.0, A0 / np.maximum(sinb, 0.05), 0.0)
+    D = 10.0 ** (0.2 * dms + 1.0)
+    cube = (screen[None, :, :] * (1.0 - np.exp(-D / D0))[:, None, None]).astype(np.float32)   # [z][y][x]
+    maps = []
+    for h in range(2):
+        a = np.ascontiguousarray(cube * (1.0 if h == 0 else 1.3), dtype=np.float32)
+        e = A.ExtMap()
+        e.A = a.ctypes.data_as(C.POINTER(C.c_float))
+        e.n[0], e.n[1], e.n[2] = nxy, nxy, nz
+        for ax, (lo, hi, n) in enumerate(((-2.0, 2.0, nxy), (-2.0, 2.0, nxy), (dm_range[0], dm_range[1], nz))):
+            e.tc[ax][0] = lo
+            e.tc[ax][1] = float(np.float32((n - 1) / (hi - lo)))
+        maps.append((a, e))
+    ext = A.Extinction()
+    ext.kind = A.GF_EXT_MAPS
+    ext.A0 = 0.0
+    ext.north = C.pointer(maps[0][1])
+    ext.south = C.pointer(maps[1][1])
+    proj = (A.Lambert * 2)(w.sky.proj[0], w.sky.proj[1])
+    nzc = C.c_int32(0)
+    pix = w.pixel_array()
+    st = lib.gf_extinction_beam_minima(C.byref(ext), proj, pix, w.npixels, None, C.byref(nzc))
+    if st != 0:
+        raise RuntimeError("gf_extinction_beam_minima failed")
+    table = np.zeros(w.npixels * nzc.value, dtype=np.float32)
+    st = lib.gf_extinction_beam_minima(C.byref(ext), proj, pix, w.npixels, table.ctypes.data_as(C.POINTER(C.c_float)),
+                                       C.byref(nzc))
+    if st != 0:
+        raise RuntimeError("gf_extinction_beam_minima failed")
+    w.ext = ext
+    w.ammin = table
+    w.keep += [maps, proj]
+    return w
+
+
+def density_cube_model(comp, f=1.0, Rg=8000.0, half=(20000.0, 20000.0, 5000.0), step=(500.0, 500.0, 250.0),
+                       scale=(2600.0, 300.0), lf=None, keep=None):
+    """A density-cube model (GF_MODEL_DENSITY_CUBE) whose grid samples a galactocentric
+    exponential disk exp(-R/l - |z|/h) on a regular grid (x, y, z in [-half, half] with the
+    given step, one empty texel of padding on each side as the reference's text loader
+    adds, model_densityCube.cpp:108-150); texture coordinates map the first and last grid
+    points to texels 1 and n - 2.  keep receives the arrays that must outlive the model."""
+    l_, h_ = scale
+    axes = [np.arange(-half[a], half[a] + 0.5 * step[a], step[a]) for a in range(3)]
+    n = [len(ax) + 2 for ax in axes]
+    cube = np.zeros((n[2], n[1], n[0]), dtype=np.float32)
+    X, Y, Z = np.meshgrid(axes[0], axes[1], axes[2], indexing="ij")
+    rho = np.exp(-np.sqrt(X ** 2 + Y ** 2) / l_ - np.abs(Z) / h_).astype(np.float32)
+    cube[1:-1, 1:-1, 1:-1] = np.transpose(rho, (2, 1, 0))
+    m = A.ModelConfig()
+    m.type = A.GF_MODEL_DENSITY_CUBE
+    m.comp = comp
+    m.f = f
+    m.Rg = Rg
+    m.frame = A.GF_FRAME_GALPLANE
+    m.cube = cube.ctypes.data_as(C.POINTER(C.c_float))
+    for a in range(3):
+        m.cube_n[a] = n[a]
+        # texcoord_from_range(1, n - 2, first, last): (x0, 1/dx) with texel 1 at the first point
+        x0, x1 = float(axes[a][0]), float(axes[a][-1])
+        inv = np.float32((n[a] - 3) / (x1 - x0))
+        m.cube_tc[a][0] = float(np.float32((-(n[a] - 2) * x0 + 1 * x1) / (1 - (n[a] - 2))))
+        m.cube_tc[a][1] = float(inv)
+    keep_ = [cube]
+    if lf is not None:
+        M_, phi = (np.ascontiguousarray(np.asarray(v, dtype=np.float64)) for v in lf)
+        m.lf_M = M_.ctypes.data_as(C.POINTER(C.c_double))
+        m.lf_phi = phi.ctypes.data_as(C.POINTER(C.c_double))
+        m.lf_n = len(M_)
+        keep_ += [M_, phi]
+    if keep is not None:
+        keep.extend(keep_)
+    return m
+
+
 _TABLES = {}
 
 

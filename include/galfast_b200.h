@@ -92,7 +92,8 @@ typedef enum {
     GF_MODEL_EXP_DISK = 1,                 /* src/skygen/model_expDisk.h */
     GF_MODEL_POWER_LAW_ELLIPSOID = 2,      /* src/skygen/model_powerLawEllipsoid.h */
     GF_MODEL_BROKEN_POWER_LAW = 3,         /* src/skygen/model_brokenPowerLaw.h: power-law ellipsoid with breaks */
-    GF_MODEL_LCBULGE = 4                   /* src/skygen/model_LCBulge.h: exp(-t/l), t = (x^n + (y/ba)^n + (z/ca)^n)^(1/n) */
+    GF_MODEL_LCBULGE = 4,                  /* src/skygen/model_LCBulge.h: exp(-t/l), t = (x^n + (y/ba)^n + (z/ca)^n)^(1/n) */
+    GF_MODEL_DENSITY_CUBE = 5              /* src/skygen/model_densityCube.h: f times a density grid, galactocentric */
 } gf_model_type;
 
 typedef enum {
@@ -123,16 +124,40 @@ typedef struct gf_model_config {
     double rbreak[9];
     /* The LC bulge (model_LCBulge.cpp:33-60) uses n, l, ba, ca and the frame, and scales the
      * LF by f instead of normalising the density at (lf_l, lf_b, lf_D). */
+    /* The density cube (model_densityCube.h:34-79, .cpp:250-311): rho = f * cube(Rg - x, -y, z)
+     * sampled at the nearest texel, value(X) = cube[k][j][i] with i = clamp(trunc((X - x0) * inv_dx
+     * + 0.5), 0, nx - 1) per axis (x fastest in memory); f is not normalised at a point and the LF
+     * (lf_M, lf_phi) is resampled to 1024 texels without clipping.  Uses Rg, f, the LF and these. */
+    const float *cube;
+    int32_t cube_n[3];                 /* nx, ny, nz */
+    float cube_tc[3][2];               /* per axis (x0, inv_dx): the texture coordinates */
 } gf_model_config;
 
 typedef enum {
     GF_EXT_NONE = 0,           /* zero extinction (os_skygen.cpp:701-706) */
-    GF_EXT_SCREEN_CSCB = 1     /* Am = A0 / |sin b| in the bootstrap band at every distance */
+    GF_EXT_SCREEN_CSCB = 1,    /* Am = A0 / |sin b| in the bootstrap band at every distance */
+    GF_EXT_MAPS = 2            /* 3-D maps of the two hemispheres (os_skygen.cpp:518-579, 699-814) */
 } gf_extinction_kind;
+
+/* One hemisphere's 3-D extinction map (load_extinction_map, os_skygen.cpp:518-579):
+ * the bootstrap-band extinction on a grid of the hemisphere's Lambert coordinates
+ * (X, Y) and distance modulus, already multiplied by the map's scale (nscale or
+ * sscale).  Sampled at the nearest texel, as the reference's host build samples
+ * its textures: index = clamp(trunc((v - x0) * inv_dx + 0.5), 0, n - 1) per axis. */
+typedef struct gf_ext_map {
+    const float *A;            /* [nz][ny][nx], x fastest */
+    int32_t n[3];              /* nx (X), ny (Y), nz (DM) */
+    float tc[3][2];            /* (x0, inv_dx) of X, Y and DM */
+} gf_ext_map;
 
 typedef struct gf_extinction {
     int32_t kind;
     float A0;                  /* bootstrap-band extinction towards the pole */
+    /* GF_EXT_MAPS: the maps of the north (projection 0) and south (projection 1)
+     * hemispheres; NULL = zero extinction there.  Both present: equal nz and DM axes.
+     * The per-beam minima (beam_ammin of the requests) then hold nz values per beam,
+     * beam_ammin[extIdx * nz + k] (gf_extinction_beam_minima). */
+    const gf_ext_map *north, *south;
 } gf_extinction;
 
 /* Footprints of the analytic clipper (stars outside are flagged hidden). */
@@ -718,6 +743,15 @@ gf_status gf_lambert_init(double l0_deg, double b0_deg, gf_lambert *p);
 gf_status gf_footprint_pixelize(const gf_footprint *foot, double dx_deg, const gf_lambert proj[2],
                                 const gf_extinction *ext, gf_pencil_beam *pixels, float *beam_ammin,
                                 int64_t max_pixels, int64_t *npixels);
+/* The per-beam extinction table of GF_EXT_MAPS (find_extinction_minima,
+ * os_skygen.cpp:285-342, and load_extinction_maps, :770-800): for every beam (its
+ * extIdx) and every DM texel z of the maps, the smallest extinction one texel
+ * closer (A(x, y, z - 1), 0 at z = 0) over the map texels that may overlap the
+ * beam, in each given map projected with its hemisphere's Lambert pole; +inf where
+ * no texel qualifies.  out[npixels * nz]; *nz receives the depth (call with
+ * out == NULL to get it). */
+gf_status gf_extinction_beam_minima(const gf_extinction *ext, const gf_lambert proj[2], const gf_pencil_beam *pixels,
+                                    int32_t npixels, float *out, int32_t *nz);
 /* Resample a photometric-system table (rows: Mr, FeH, c_1..c_ncolors) to the colour
  * and extrapolation-flag grids of os_photometry::construct (photometry_host.cpp:233-344).
  * colors/eflags: [ncolors][nMr][nFeH]; call with colors == NULL for the sizes. */

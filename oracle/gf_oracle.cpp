@@ -254,6 +254,10 @@ struct Model {
     float n, ba, ca, rminSq, rmaxSq;
     int nbreaks;                       /* brokenPowerLaw (model_brokenPowerLaw.h:41-45) */
     float nArr[10], fArr[10], rbreakSq[9];
+    float Rg;                          /* densityCube (model_densityCube.h:40-44) */
+    const float *cube;
+    int cube_n[3];
+    float cube_tc[3][2];
     float T[3];
     float M[3][3];
     std::vector<float> lf;
@@ -271,6 +275,19 @@ struct Model {
         float wx = M[0][0] * vx + M[0][1] * vy + M[0][2] * vz;
         float wy = M[1][0] * vx + M[1][1] * vy + M[1][2] * vz;
         float wz = M[2][0] * vx + M[2][1] * vy + M[2][2] * vz;
+        if (type == GF_MODEL_DENSITY_CUBE) {
+            /* densityCube::setpos (model_densityCube.h:60-66): galactocentric, nearest texel */
+            float gx = Rg - x, gy = y * -1, gz = z;
+            const float c3[3] = {gx, gy, gz};
+            size_t ix[3];
+            for (int a = 0; a < 3; a++) {
+                float t = (c3[a] - cube_tc[a][0]) * cube_tc[a][1] + 0.5f;
+                if (t < 0.f) t = 0.f;
+                else if (t >= cube_n[a]) t = cube_n[a] - 1;
+                ix[a] = (uint32_t)t;
+            }
+            return f * cube[(ix[2] * cube_n[1] + ix[1]) * cube_n[0] + ix[0]];
+        }
         if (type == GF_MODEL_EXP_DISK) {
             float r2 = wx * wx + wy * wy;
             if (r_cut2 && r2 + wz * wz > r_cut2) return 0.f;
@@ -395,6 +412,8 @@ struct Sky {
     std::vector<gf_pencil_beam> pixels;
     std::vector<float> ammin;
     gf_extinction ext;
+    int ext_nz = 1;                    /* GF_EXT_MAPS: DM texels of the per-beam rows */
+    float ext_tcz[2] = {0.f, 1.f};
     std::vector<Model> models;
     std::vector<KState> ks;            /* per model draw state */
     std::vector<char> ks_alloc;
@@ -486,17 +505,40 @@ bool advance(const Launch &L, int &ilb, int &i, int &j, gf_pencil_beam &dir, con
     return true;
 }
 
-/* The minimum extinction along a beam (ext_beam texture, os_skygen.cpp:742-797). */
-float beam_extinction(const Launch &L, const gf_pencil_beam &pix)
+/* nearest-texel index of the host build's texture sampling (cux.h:778-809, 860-874) */
+static uint32_t texel(float v, const float tc[2], int n)
 {
-    if (L.sky->ext.kind == GF_EXT_NONE || L.sky->ammin.empty()) return 0.f;
-    return L.sky->ammin[pix.extIdx];
+    float t = (v - tc[0]) * tc[1] + 0.5f;
+    if (t < 0.f) t = 0.f;
+    else if (t >= n) t = n - 1;
+    return (uint32_t)t;
 }
 
-/* Extinction towards a star (sampleExtinction, skygen.cu.h:199-208) for the screen model. */
-float star_extinction(const Launch &L, const Dir &d)
+/* The minimum extinction along a beam (ext_beam texture, os_skygen.cpp:742-797):
+ * with 3-D maps the beam's row at the nearest DM texel (TEX3D(ext_beam, xidx, yidx, DM)). */
+float beam_extinction(const Launch &L, const gf_pencil_beam &pix, float DM)
 {
-    if (L.sky->ext.kind == GF_EXT_SCREEN_CSCB) return L.sky->ext.A0 / fabsf(d.sb);
+    const Sky &s = *L.sky;
+    if (s.ext.kind == GF_EXT_NONE || s.ammin.empty()) return 0.f;
+    if (s.ext.kind == GF_EXT_MAPS) {
+        const uint32_t k = texel(DM, s.ext_tcz, s.ext_nz);
+        return s.ammin[(size_t)pix.extIdx * s.ext_nz + k];
+    }
+    return s.ammin[pix.extIdx];
+}
+
+/* Extinction towards a star (sampleExtinction, skygen.cu.h:199-208): the screen,
+ * or the map of the star's hemisphere at its projected position and DM. */
+float star_extinction(const Launch &L, const Dir &d, int projIdx, float x, float y, float DM)
+{
+    const Sky &s = *L.sky;
+    if (s.ext.kind == GF_EXT_SCREEN_CSCB) return s.ext.A0 / fabsf(d.sb);
+    if (s.ext.kind == GF_EXT_MAPS) {
+        const gf_ext_map *e = projIdx == 0 ? s.ext.north : s.ext.south;
+        if (!e) return 0.f;
+        const uint32_t i = texel(x, e->tc[0], e->n[0]), j = texel(y, e->tc[1], e->n[1]), k = texel(DM, e->tc[2], e->n[2]);
+        return e->A[((size_t)k * e->n[1] + j) * e->n[0] + i];
+    }
     return 0.f;
 }
 
@@ -507,7 +549,7 @@ F3 compute_pos(const Launch &L, float &D, float &Am, float M, const int im, cons
     float mm = m.m0 + im * m.dm;
     float DM = mm - M;
     D = OR_POWF(10.f, 0.2f * DM + 1.f);
-    Am = beam_extinction(L, pix);
+    Am = beam_extinction(L, pix, DM);
     F3 p;
     p.x = D * pix.cl * pix.cb;
     p.y = D * pix.sl * pix.cb;
@@ -590,8 +632,8 @@ void draw_stars(const Launch &L, Rng &rng, int &ndraw, const float &M, const int
         r.Z = D * dir2.sb;
         r.comp = m.comp;
         float Am0, Am1;
-        r.Am = Am0 = star_extinction(L, dir2);
-        Am1 = star_extinction(L, dir2);
+        r.Am = Am0 = star_extinction(L, dir2, pix.projIdx, x, y, DM);
+        Am1 = star_extinction(L, dir2, pix.projIdx, x, y, 100);
         r.AmInf = Am1 > Am0 ? Am1 : Am0;
         r.hidden = (mtmp + Am0 > m.m1) ? 1 : 0;
         if (AmMin > Am0) r.AmInf = -AmMin;
@@ -1131,8 +1173,16 @@ void *or_skygen_create(const gf_skygen_config *cfg, const gf_pencil_beam *pixels
     Sky *s = new Sky();
     s->cfg = *cfg;
     s->pixels.assign(pixels, pixels + npixels);
-    if (beam_ammin) s->ammin.assign(beam_ammin, beam_ammin + npixels);
-    s->ext = ext ? *ext : gf_extinction{GF_EXT_NONE, 0.f};
+    s->ext = ext ? *ext : gf_extinction{GF_EXT_NONE, 0.f, nullptr, nullptr};
+    if (s->ext.kind == GF_EXT_MAPS) {
+        const gf_ext_map *e = s->ext.north ? s->ext.north : s->ext.south;
+        if (e) {
+            s->ext_nz = e->n[2];
+            s->ext_tcz[0] = e->tc[2][0];
+            s->ext_tcz[1] = e->tc[2][1];
+        }
+    }
+    if (beam_ammin) s->ammin.assign(beam_ammin, beam_ammin + (size_t)npixels * s->ext_nz);
 
     /* load_skyPixelizationConfig (os_skygen.cpp:409-430) */
     float M0 = cfg->M0, M1 = cfg->M1, m0 = cfg->m0, m1 = cfg->m1, dm = cfg->dm, dM = dm;
@@ -1167,7 +1217,27 @@ void *or_skygen_create(const gf_skygen_config *cfg, const gf_pencil_beam *pixels
         }
         /* load_lf (model_lib.h:68-95); the LC bulge: load_lf_raw times f (model_LCBulge.cpp:50-56) */
         load_lf(m, c);
-        if (c.type == GF_MODEL_LCBULGE) {
+        if (c.type == GF_MODEL_DENSITY_CUBE) {
+            /* densityCube::load (model_densityCube.cpp:250-300): f, Rg, the grid; the LF by
+             * load_and_resample_texture_1D (no clipping), no normalisation */
+            m.f = (float)c.f;
+            m.Rg = (float)c.Rg;
+            m.cube = c.cube;
+            for (int k = 0; k < 3; k++) {
+                m.cube_n[k] = c.cube_n[k];
+                m.cube_tc[k][0] = c.cube_tc[k][0];
+                m.cube_tc[k][1] = c.cube_tc[k][1];
+            }
+            if (c.lf_n > 0 && c.lf_M) {
+                std::vector<double> X(c.lf_M, c.lf_M + c.lf_n), Y(c.lf_phi, c.lf_phi + c.lf_n);
+                int ndata = (int)X.size(), nsamp = 1024;
+                m.lf.resize(nsamp);
+                double X0 = X[0], X1 = X[ndata - 1], dX = (X1 - X0) / (nsamp - 1);
+                for (int i = 0; i != nsamp; i++) m.lf[i] = (float)linear_eval(X.data(), Y.data(), ndata, X0 + i * dX);
+                m.lf_x0 = (float)X0;
+                m.lf_inv_dx = (float)(1. / dX);
+            }
+        } else if (c.type == GF_MODEL_LCBULGE) {
             float f0 = (float)c.f;
             for (auto &v : m.lf) v *= f0;
             m.f = 1.f;
@@ -1188,7 +1258,7 @@ void *or_skygen_create(const gf_skygen_config *cfg, const gf_pencil_beam *pixels
         if (c.type == GF_MODEL_EXP_DISK) {
             float rc = (float)c.rcut;
             m.r_cut2 = rc * rc;
-        } else if (c.type != GF_MODEL_LCBULGE) {
+        } else if (c.type != GF_MODEL_LCBULGE && c.type != GF_MODEL_DENSITY_CUBE) {
             float rmin = (float)c.rmin, rmax = (float)c.rmax;
             m.rminSq = rmin * rmin;
             m.rmaxSq = rmax * rmax;

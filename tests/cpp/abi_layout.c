@@ -15,7 +15,9 @@ int main(void)
     SZ(gf_skygen_config); OF(gf_skygen_config, nthreads); OF(gf_skygen_config, nstars); OF(gf_skygen_config, proj);
     SZ(gf_model_config); OF(gf_model_config, f); OF(gf_model_config, frame); OF(gf_model_config, Rg); OF(gf_model_config, M);
     OF(gf_model_config, lf_l); OF(gf_model_config, lf_M); OF(gf_model_config, lf_n); OF(gf_model_config, nbreaks);
-    OF(gf_model_config, n_brk); OF(gf_model_config, rbreak);
+    OF(gf_model_config, n_brk); OF(gf_model_config, rbreak); OF(gf_model_config, cube); OF(gf_model_config, cube_n);
+    OF(gf_model_config, cube_tc);
+    SZ(gf_ext_map); OF(gf_ext_map, n); OF(gf_ext_map, tc); OF(gf_extinction, north); OF(gf_extinction, south);
     SZ(gf_extinction); SZ(gf_footprint); OF(gf_footprint, a);
     SZ(gf_table); OF(gf_table, nbands); OF(gf_table, lb); OF(gf_table, hidden); OF(gf_table, radec); OF(gf_table, FeH_comp); OF(gf_table, absmagSysNcomp); OF(gf_table, systems);
     SZ(gf_fixedfeh_config); SZ(gf_vmoments); SZ(gf_bond2010_config); OF(gf_bond2010_config, halo); OF(gf_bond2010_config, T);

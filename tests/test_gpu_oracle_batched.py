@@ -217,3 +217,59 @@ def test_hardware_exp_brackets_the_exact_exp_for_every_float(tmp_path):
     n, bad, worst = r.stdout.split()
     assert r.returncode == 0 and int(bad) == 0 and int(n) > 2000000000, r.stdout
     assert float(worst) < 0.5e-5
+
+
+def test_density_cube_model_equals_oracle(lib, multipliers):
+    """model_densityCube (src/skygen/model_densityCube.h): f times the nearest texel
+    of a density grid at (Rg - x, -y, z), its own LF resampled without clipping and
+    no normalisation.  The grid samples an exponential disk on 500 pc cells; the
+    catalog of a request with it equals the oracle's, through gf_catalog_run and
+    through gf_catalog_run_multi (where such a request takes the plain path)."""
+    from galfast_b200 import _abi as A
+    w = W.build_workload(lib, foot=W.cap_footprint(30.0, 25.0, 1.5), dx_deg=0.25, m0=15.0, m1=20.0,
+                         capacity=1 << 20, seed48=77)
+    lfM = np.array([-1.0, 3.0, 8.0, 14.0, 16.0])
+    lfp = np.array([0.002, 0.01, 0.03, 0.08, 0.05])
+    w.models[1] = W.density_cube_model(1, f=0.2, lf=(lfM, lfp), keep=w.keep)
+    assert w.models[1].type == A.GF_MODEL_DENSITY_CUBE
+    ref, st, _ = oracle_catalog(w, multipliers)
+    assert st["generated"][1] > 1000
+    ctx = G.Context(0)
+    plain = {}
+    gst = G.run_catalog(ctx, w, sink=lambda m, t, off: plain.setdefault(m, []).append(t.as_dict()))
+    compare(ref, {m: concat(p) for m, p in plain.items()}, "plain")
+    for i in range(3):
+        assert gst.generated[i] == st["generated"][i]
+        assert gst.expected[i] == pytest.approx(st["expected"][i][0], rel=1e-12)
+    got, stats = batched_catalogs(ctx, [w, model_types_workload(lib)])
+    ctx.close()
+    compare(ref, got[0], "multi")
+
+
+def test_extinction_maps_equal_oracle(lib, multipliers):
+    """3-D extinction maps (GF_EXT_MAPS; os_skygen.cpp:518-579, 699-814): the anchors
+    take the beam's minimum row at their DM texel, the stars the nearest texel of
+    their hemisphere's map at their own DM and at DM = 100, and a star whose anchor
+    extinction exceeds its own gets AmInf = -AmMin (skygen.cu.h:421-455).  A cap
+    straddling the plane draws from both maps; the catalog equals the oracle's
+    through gf_catalog_run and through gf_catalog_run_multi (where the request takes
+    the plain path), with 20000-row batches so that reruns carry the anchor values."""
+    w = W.build_workload(lib, foot=W.cap_footprint(40.0, 1.0, 1.0), dx_deg=0.25, m0=15.0, m1=19.5, capacity=20000,
+                         seed48=5)
+    W.use_extinction_maps(lib, w)
+    ref, st, _ = oracle_catalog(w, multipliers)
+    assert sum(st["generated"].values()) > 40000
+    ctx = G.Context(0)
+    plain = {}
+    gst = G.run_catalog(ctx, w, sink=lambda m, t, off: plain.setdefault(m, []).append(t.as_dict()))
+    got = {m: concat(p) for m, p in plain.items()}
+    compare(ref, got, "plain")
+    for i in range(3):
+        assert gst.expected[i] == pytest.approx(st["expected"][i][0], rel=1e-12)
+    am = np.concatenate([got[m]["AmInf"].ravel() for m in got])
+    assert (am < 0).any() and (am > 0).any()
+    lat = np.concatenate([got[m]["lb"][1] for m in got])
+    assert (lat > 0).any() and (lat < 0).any()
+    got2, stats = batched_catalogs(ctx, [w, model_types_workload(lib)])
+    ctx.close()
+    compare(ref, got2[0], "multi")

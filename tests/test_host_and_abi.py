@@ -60,7 +60,8 @@ def test_struct_layouts(tmp_path):
               "gf_vel2pm_config": A.Vel2pmConfig, "gf_skygen_model_info": A.ModelInfo, "gf_job": G.Job,
               "gf_catalog_stats": G.CatalogStats, "gf_precision_report": A.PrecisionReport,
               "gf_textout_config": G.TextoutConfig, "gf_textout_set": G.TextoutSet,
-              "gf_server_info": G.ServerInfo, "gf_multiples_config": A.MultiplesConfig}
+              "gf_server_info": G.ServerInfo, "gf_multiples_config": A.MultiplesConfig,
+              "gf_ext_map": A.ExtMap}
     checked = 0
     for line in out.split("\n"):
         if not line.strip():
@@ -319,3 +320,52 @@ def test_multiples_tables_follow_the_reference_construction(lib):
     assert abs(d.cumlf[128] - 128 / 255) < 1e-6
     with pytest.raises(RuntimeError):
         W.multiples_config(lib, algo=7)
+
+
+def test_extinction_beam_minima_follow_the_reference(lib):
+    """gf_extinction_beam_minima restates find_extinction_minima
+    (os_skygen.cpp:285-342): for every beam and DM texel z, the smallest A(x, y, z-1)
+    (0 at z = 0) over the texels of each map within the beam's reach, skipping empty
+    texels outside the hemisphere's disk.  Checked against a Python restatement on
+    the beams of a cap that straddles the plane (both maps contribute)."""
+    import math
+    from galfast_b200 import workloads as W
+    w = W.build_workload(lib, foot=W.cap_footprint(40.0, 2.0, 2.0), dx_deg=0.5, m0=15.0, m1=17.0, with_modules=False)
+    W.use_extinction_maps(lib, w, nxy=40, nz=8)
+    nz = len(w.ammin) // w.npixels
+    assert nz == 8
+    maps = [w.ext.north.contents, w.ext.south.contents]
+    pix = w.pixel_array()
+    f32 = np.float32
+    for i in range(0, w.npixels, max(1, w.npixels // 25)):
+        p = pix[i]
+        want = np.full(nz, np.inf, dtype=np.float32)
+        for h in range(2):
+            e = maps[h]
+            nx, ny, d = e.n[0], e.n[1], e.n[2]
+            A_ = np.ctypeslib.as_array(e.A, shape=(d * ny * nx,)).reshape(d, ny, nx)
+            pr = w.sky.proj[h]
+            # float products and sums (as the reference's float expressions), widened to double
+            cll0 = float(f32(f32(p.cl * pr.cl) + f32(p.sl * pr.sl)))
+            sll0 = float(f32(f32(pr.cl * p.sl) - f32(p.cl * pr.sl)))
+            kp = 1.414213562373095 * math.sqrt(1.0 / (1.0 + float(f32(pr.sb * p.sb)) + float(f32(pr.cb * p.cb)) * cll0))
+            x = float(f32(kp * p.cb * sll0))
+            y = float(f32(kp * (pr.cb * p.sb - float(f32(pr.sb * p.cb)) * cll0)))
+            tcx0, tcxy, tcy0, tcyy = (float(e.tc[0][0]), float(e.tc[0][1]), float(e.tc[1][0]), float(e.tc[1][1]))
+            dr = 1.0001 / 2.0 * math.sqrt(2) * (float(p.dx) + max(1.0 / tcxy, 1.0 / tcyy))
+            xi = max(0, min(int((x - dr - tcx0) * tcxy) - 1, nx))
+            yi = max(0, min(int((y - dr - tcy0) * tcyy) - 1, ny))
+            xie = max(0, min(int((x + dr - tcx0) * tcxy) + 2, nx))
+            yie = max(0, min(int((y + dr - tcy0) * tcyy) + 2, ny))
+            for X in range(xi, xie):
+                for Y in range(yi, yie):
+                    if Y >= nx:
+                        continue
+                    if A_[d - 1, Y, X] == 0:
+                        xx, yy = X / tcxy + tcx0, Y / tcyy + tcy0
+                        if xx * xx + yy * yy > 2:
+                            continue
+                    col = np.concatenate([[0.0], A_[:d - 1, Y, X]]).astype(np.float32)
+                    want = np.minimum(want, col)
+        got = w.ammin[p.extIdx * nz:(p.extIdx + 1) * nz]
+        np.testing.assert_array_equal(got, want, err_msg="beam %d" % i)
