@@ -16,6 +16,7 @@ GF_FOOT_ALL = 0
 GF_FOOT_LAMBERT_RECT = 1
 GF_FOOT_CAP = 2
 GF_FOOT_LB_RECT = 4
+GF_FOOT_REGIONS = 5
 GF_FOOT_LATCUT = 3
 GF_MAX_BANDS = 17
 
@@ -61,9 +62,20 @@ class Extinction(C.Structure):
     _fields_ = [("kind", C.c_int32), ("A0", C.c_float), ("north", C.POINTER(ExtMap)), ("south", C.POINTER(ExtMap))]
 
 
+GF_REGION_BEAM, GF_REGION_RECT = 1, 2
+GF_COORD_GAL, GF_COORD_EQU = 0, 1
+GF_MAX_REGIONS = 8
+
+
+class Region(C.Structure):                # gf_region: one footprint specification
+    _fields_ = [("type", C.c_int32), ("coordsys", C.c_int32), ("a", C.c_double), ("b", C.c_double),
+                ("c", C.c_double), ("d", C.c_double), ("bmin", C.c_double)]
+
+
 class Footprint(C.Structure):
     _fields_ = [("kind", C.c_int32), ("proj", C.c_int32),
-                ("a", C.c_double), ("b", C.c_double), ("c", C.c_double), ("d", C.c_double)]
+                ("a", C.c_double), ("b", C.c_double), ("c", C.c_double), ("d", C.c_double),
+                ("nregions", C.c_int32), ("pad_", C.c_int32), ("regions", Region * GF_MAX_REGIONS)]
 
 
 class Table(C.Structure):

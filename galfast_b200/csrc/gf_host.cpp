@@ -4,6 +4,7 @@
  * pixelisation and photometric-system tables.
  */
 #include "gf_host.h"
+#include "gf_footprint.h"
 #include "gf_math.h"
 #include "gf_safeprimes.h"
 
@@ -439,10 +440,70 @@ struct FootTest {
         case GF_FOOT_CAP: return gfm::sin_d(b) * sb0 + gfm::cos_d(b) * cb0 * gfm::cos_d(l - l0) >= cosr;
         case GF_FOOT_LATCUT: return fabs(b) > f.a * kD2R;
         case GF_FOOT_LB_RECT: return lb_rect_inside(f, l / kD2R, b / kD2R);
+        case GF_FOOT_REGIONS: return gff::regions_inside(f, l / kD2R, b / kD2R);
         }
         return false;
     }
 };
+
+/* galactic samples (radians) of the boundaries of a region set, for its bounding boxes */
+template <class F>
+static void region_boundaries(const gf_footprint &f, F &&add)
+{
+    auto put = [&](const gf_region &r, double lon, double lat) {
+        if (r.coordsys == GF_COORD_EQU) gff::equ_to_gal(lon, lat, lon, lat);
+        add(lon, lat);
+    };
+    for (int q = 0; q < f.nregions && q < GF_MAX_REGIONS; q++) {
+        const gf_region &r = f.regions[q];
+        if (r.type == GF_REGION_BEAM) {
+            /* small circles about the centre c: cos(r) c + sin(r) (cos(az) u + sin(az) v)
+             * with u, v orthonormal tangents (well defined at the poles too) */
+            const double lc = r.a * kD2R, bc = r.b * kD2R;
+            const double c[3] = {gfm::cos_d(bc) * gfm::cos_d(lc), gfm::cos_d(bc) * gfm::sin_d(lc), gfm::sin_d(bc)};
+            const double u[3] = {-gfm::sin_d(lc), gfm::cos_d(lc), 0.0};
+            const double v[3] = {c[1] * u[2] - c[2] * u[1], c[2] * u[0] - c[0] * u[2], c[0] * u[1] - c[1] * u[0]};
+            const double radii[2] = {std::min(r.c, 180.0) * kD2R, r.d * kD2R};
+            for (int h = 0; h < 2; h++) {
+                const double rr = radii[h];
+                if (h == 1 && !(r.d > 0)) break;
+                for (int k = 0; k <= 4096; k++) {
+                    const double az = 2 * M_PI * k / 4096.0, r0 = (k == 4096) ? 0.0 : rr;
+                    double p[3];
+                    for (int i = 0; i < 3; i++)
+                        p[i] = gfm::cos_d(r0) * c[i] + gfm::sin_d(r0) * (gfm::cos_d(az) * u[i] + gfm::sin_d(az) * v[i]);
+                    const double b = gfm::asin_d(std::max(-1.0, std::min(1.0, p[2])));
+                    const double l = gfm::atan2_d(p[1], p[0]);
+                    put(r, l, b);
+                }
+            }
+        } else if (r.type == GF_REGION_RECT) {
+            double l0 = r.a, l1 = r.b;
+            if (l1 <= l0) l1 += 360.0;
+            const double b0 = std::max(r.c, -90.0), b1 = std::min(r.d, 90.0);
+            for (int k = 0; k <= 2048; k++) {
+                const double t = k / 2048.0;
+                const double l = (l0 + t * (l1 - l0)) * kD2R, b = (b0 + t * (b1 - b0)) * kD2R;
+                put(r, l, b0 * kD2R);
+                put(r, l, b1 * kD2R);
+                put(r, l0 * kD2R, b);
+                put(r, l1 * kD2R, b);
+                put(r, 0.5 * (l0 + l1) * kD2R, b);
+            }
+        }
+    }
+}
+
+/* does the region set hold a region smaller than s degrees across? */
+static bool regions_small(const gf_footprint &f, double s)
+{
+    for (int q = 0; q < f.nregions && q < GF_MAX_REGIONS; q++) {
+        const gf_region &r = f.regions[q];
+        if (r.type == GF_REGION_BEAM && (r.c < s || (r.d > 0 && r.c - r.d < s))) return true;
+        if (r.type == GF_REGION_RECT && (r.d - r.c < s || (r.a != r.b && fabs(fmod(r.b - r.a + 360.0, 360.0)) < s))) return true;
+    }
+    return false;
+}
 
 }  // namespace
 
@@ -470,6 +531,14 @@ gf_status gf_footprint_pixelize(const gf_footprint *foot, double dx_deg, const g
                                 int64_t max_pixels, int64_t *npixels)
 {
     if (!foot || !npixels || !(dx_deg > 0)) return GF_E_INVALID;
+    if (foot->kind == GF_FOOT_REGIONS) {
+        if (foot->nregions < 1 || foot->nregions > GF_MAX_REGIONS) return GF_E_INVALID;
+        for (int q = 0; q < foot->nregions; q++) {
+            const gf_region &r = foot->regions[q];
+            if ((r.type != GF_REGION_BEAM && r.type != GF_REGION_RECT) || (r.coordsys != GF_COORD_GAL && r.coordsys != GF_COORD_EQU))
+                return GF_E_INVALID;
+        }
+    }
     const double dx = dx_deg * kD2R;
     const float dxf = (float)dx;
     FootTest ft(*foot);
@@ -484,7 +553,7 @@ gf_status gf_footprint_pixelize(const gf_footprint *foot, double dx_deg, const g
         } else if (foot->kind == GF_FOOT_LATCUT) {
             double R = 2 * gfm::sin_d(0.5 * (90. - foot->a) * kD2R);
             xmin = ymin = -R; xmax = ymax = R;
-        } else if (foot->kind == GF_FOOT_CAP || foot->kind == GF_FOOT_LB_RECT) {
+        } else if (foot->kind == GF_FOOT_CAP || foot->kind == GF_FOOT_LB_RECT || foot->kind == GF_FOOT_REGIONS) {
             /* project boundary samples of the footprint that fall in this hemisphere */
             double bx0 = 1e9, bx1 = -1e9, by0 = 1e9, by1 = -1e9;
             bool any = false;
@@ -500,7 +569,9 @@ gf_status gf_footprint_pixelize(const gf_footprint *foot, double dx_deg, const g
                 bx0 = std::min(bx0, x); bx1 = std::max(bx1, x); by0 = std::min(by0, y); by1 = std::max(by1, y);
                 any = true;
             };
-            if (foot->kind == GF_FOOT_CAP) {
+            if (foot->kind == GF_FOOT_REGIONS) {
+                region_boundaries(*foot, add_point);
+            } else if (foot->kind == GF_FOOT_CAP) {
                 double lc = foot->a * kD2R, bc = foot->b * kD2R, r = foot->c * kD2R;
                 for (int k = 0; k <= 4096; k++) {
                     double rr = (k == 4096) ? 0.0 : r;
@@ -534,8 +605,9 @@ gf_status gf_footprint_pixelize(const gf_footprint *foot, double dx_deg, const g
             xmin = std::max(-M_SQRT2, bx0 - pad); xmax = std::min(M_SQRT2, bx1 + pad);
             ymin = std::max(-M_SQRT2, by0 - pad); ymax = std::min(M_SQRT2, by1 + pad);
             /* a footprint containing the pole covers the origin */
-            bool pole = (foot->kind == GF_FOOT_CAP) ? ((h == 0 ? 90. - foot->b : 90. + foot->b) <= foot->c)
-                                                    : (h == 0 ? foot->d >= 90. : foot->c <= -90.);
+            bool pole = (foot->kind == GF_FOOT_REGIONS) ? ft.inside(h, 0.0, 0.0, 0.0, (h == 0 ? 0.5 : -0.5) * M_PI)
+                        : (foot->kind == GF_FOOT_CAP) ? ((h == 0 ? 90. - foot->b : 90. + foot->b) <= foot->c)
+                                                      : (h == 0 ? foot->d >= 90. : foot->c <= -90.);
             if (pole) { xmin = std::min(xmin, -dx); xmax = std::max(xmax, dx); ymin = std::min(ymin, -dx); ymax = std::max(ymax, dx); }
         }
         long long i0 = (long long)floor(xmin / dx), i1 = (long long)ceil(xmax / dx);
@@ -569,7 +641,8 @@ gf_status gf_footprint_pixelize(const gf_footprint *foot, double dx_deg, const g
                     double py = (c == 4) ? cy0 + 0.5 * dx : cy0 + ((c >> 1) & 1) * dx;
                     if (in_point(px, py)) in_corners++;
                 }
-                bool tiny = foot->kind == GF_FOOT_CAP && foot->c * kD2R < 3 * dx;
+                bool tiny = (foot->kind == GF_FOOT_CAP && foot->c * kD2R < 3 * dx) ||
+                            (foot->kind == GF_FOOT_REGIONS && regions_small(*foot, 3 * dx / kD2R));
                 double cov;
                 if (foot->kind == GF_FOOT_LAMBERT_RECT) {
                     /* exact overlap of two rectangles */

@@ -17,6 +17,7 @@
 #include "gf_launch.h"
 #include "gf_math.h"
 #include "gf_rng.h"
+#include "gf_footprint.h"
 
 namespace gfk {
 
@@ -70,6 +71,8 @@ __device__ __forceinline__ void clip_row(const gf_footprint &foot, gf_table &t, 
         } else if (foot.kind == GF_FOOT_LB_RECT) {
             const double l = t.lb[row], b = t.lb[P + row];
             in = b >= foot.c && b < foot.d && ((foot.a <= foot.b) ? (l >= foot.a && l < foot.b) : (l >= foot.a || l < foot.b));
+        } else if (foot.kind == GF_FOOT_REGIONS) {
+            in = gff::regions_inside(foot, t.lb[row], t.lb[P + row]);
         }
         if (!in) t.hidden[row] = 1;
 }

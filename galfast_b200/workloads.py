@@ -560,6 +560,22 @@ def config4_workloads(lib, reqs, threads=None, **kw):
         return list(ex.map(lambda r: config4_workload(lib, r, **kw), reqs))
 
 
+def regions_footprint(regions):
+    """GF_FOOT_REGIONS: the union of up to 8 regions, each a dict
+    type ("beam" or "rect"), coordsys ("gal" or "equ"), the four values
+    (beam: lon, lat, r, rhole; rect: lon0, lon1, lat0, lat1; degrees) and bmin."""
+    foot = A.Footprint()
+    foot.kind = A.GF_FOOT_REGIONS
+    foot.nregions = len(regions)
+    for i, r in enumerate(regions):
+        g = foot.regions[i]
+        g.type = A.GF_REGION_BEAM if r["type"] == "beam" else A.GF_REGION_RECT
+        g.coordsys = A.GF_COORD_EQU if r.get("coordsys", "gal") == "equ" else A.GF_COORD_GAL
+        g.a, g.b, g.c, g.d = (float(v) for v in r["v"])
+        g.bmin = float(r.get("bmin", 0.0))
+    return foot
+
+
 def lb_rect_footprint(l0, l1, b0, b1):
     foot = A.Footprint()
     foot.kind = A.GF_FOOT_LB_RECT

@@ -166,13 +166,35 @@ typedef enum {
     GF_FOOT_LAMBERT_RECT = 1,  /* x0 <= X < x1, y0 <= Y < y1 in projection proj */
     GF_FOOT_CAP = 2,           /* angular distance from (l, b) <= r (degrees) */
     GF_FOOT_LATCUT = 3,        /* |b| > bmin (degrees) */
-    GF_FOOT_LB_RECT = 4        /* l0 <= l < l1 (degrees, through 360 when l0 > l1), b0 <= b < b1 */
+    GF_FOOT_LB_RECT = 4,       /* l0 <= l < l1 (degrees, through 360 when l0 > l1), b0 <= b < b1 */
+    GF_FOOT_REGIONS = 5        /* the union of `regions` (footprint.cpp:729-758) */
 } gf_footprint_kind;
+
+/* One footprint specification of the reference (footprint.cpp: load_footprint_beam,
+ * load_footprint_rect, clip_zone_of_avoidance): a beam (cap of radius r around
+ * (lon, lat), minus a concentric hole of radius rhole) or a lon/lat rectangle, in
+ * galactic or equatorial (J2000) coordinates, minus the galactic band |b| < bmin.
+ * The reference approximates each region by a polygon sampled every dx and clips
+ * stars against the polygon in the Lambert planes; here the regions are tested
+ * exactly (a star on the sphere is inside or not), and pixels are covered by
+ * supersampling the same test. */
+typedef enum { GF_REGION_BEAM = 1, GF_REGION_RECT = 2 } gf_region_type;
+typedef enum { GF_COORD_GAL = 0, GF_COORD_EQU = 1 } gf_coordsys;
+#define GF_MAX_REGIONS 8
+typedef struct gf_region {
+    int32_t type;              /* gf_region_type */
+    int32_t coordsys;          /* gf_coordsys */
+    double a, b, c, d;         /* BEAM: lon lat r rhole; RECT: lon0 lon1 lat0 lat1 (degrees; lon0 == lon1: all longitudes) */
+    double bmin;               /* galactic |b| < bmin removed (0: none) */
+} gf_region;
 
 typedef struct gf_footprint {
     int32_t kind;
     int32_t proj;
     double a, b, c, d;         /* RECT: x0 x1 y0 y1; CAP: l b r; LATCUT: bmin; LB_RECT: l0 l1 b0 b1 */
+    int32_t nregions;          /* GF_FOOT_REGIONS: regions[0 .. nregions), nregions <= GF_MAX_REGIONS */
+    int32_t pad_;
+    gf_region regions[GF_MAX_REGIONS];
 } gf_footprint;
 
 /* ------------------------------------------------------------------ */

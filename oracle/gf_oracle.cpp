@@ -1517,6 +1517,44 @@ int or_skygen_draw(void *h, int32_t mi, uint32_t *rng_state, int32_t nstreams, g
 /* ---- modules on a host table, rows [begin, end) ---- */
 
 /* os_clipper::process (os_skygen.cpp:999-1044) with an analytic footprint */
+/* The footprint regions (footprint.cpp: load_footprint_beam :675-704, load_footprint_rect
+ * :486-589, clip_zone_of_avoidance :706-727, the union of load_footprints :746-758), tested
+ * exactly on the sphere: equatorial coordinates through the Hipparcos (J2000) rotation. */
+static bool or_region_inside(const gf_region &r, double l, double b)
+{
+    if (r.bmin > 0.0 && fabs(b) < r.bmin) return false;
+    double lon = l * dbl_d2r, lat = b * dbl_d2r;
+    if (r.coordsys == GF_COORD_EQU) {
+        static const double A[3][3] = {{-0.0548755604162154, -0.8734370902348850, -0.4838350155487132},
+                                       {+0.4941094278755837, -0.4448296299600112, +0.7469822444972189},
+                                       {-0.8676661490190047, -0.1980763734312015, +0.4559837761750669}};
+        const double g[3] = {OR_COS(lat) * OR_COS(lon), OR_COS(lat) * OR_SIN(lon), OR_SIN(lat)};
+        double e[3];
+        for (int i = 0; i < 3; i++) e[i] = A[0][i] * g[0] + A[1][i] * g[1] + A[2][i] * g[2];
+        lon = OR_ATAN2(e[1], e[0]);
+        lat = OR_ASIN(std::max(-1.0, std::min(1.0, e[2])));
+    }
+    if (r.type == GF_REGION_BEAM) {
+        const double l0 = r.a * dbl_d2r, b0 = r.b * dbl_d2r;
+        const double cosd = OR_SIN(lat) * OR_SIN(b0) + OR_COS(lat) * OR_COS(b0) * OR_COS(lon - l0);
+        if (r.c < 180.0 && !(cosd >= OR_COS(r.c * dbl_d2r))) return false;
+        if (r.d > 0.0 && cosd > OR_COS(r.d * dbl_d2r)) return false;
+        return true;
+    }
+    if (r.type == GF_REGION_RECT) {
+        const double latd = lat / dbl_d2r;
+        if (!(latd >= r.c && latd < r.d)) return false;
+        if (r.a == r.b) return true;
+        double lond = fmod(lon / dbl_d2r, 360.0);
+        if (lond < 0) lond += 360.0;
+        double a = fmod(r.a, 360.0), e = fmod(r.b, 360.0);
+        if (a < 0) a += 360.0;
+        if (e < 0) e += 360.0;
+        return (a <= e) ? (lond >= a && lond < e) : (lond >= a || lond < e);
+    }
+    return false;
+}
+
 int or_module_clipper(const gf_footprint *foot, const gf_lambert *proj, gf_table *t, int64_t begin, int64_t end)
 {
     (void)proj;
@@ -1535,6 +1573,14 @@ int or_module_clipper(const gf_footprint *foot, const gf_lambert *proj, gf_table
                 in = cosd >= OR_COS(foot->c * dbl_d2r);
             } else if (foot->kind == GF_FOOT_LATCUT) {
                 in = fabs(t->lb[P + row]) > foot->a;
+            } else if (foot->kind == GF_FOOT_LB_RECT) {
+                const double l = t->lb[row], b = t->lb[P + row];
+                in = b >= foot->c && b < foot->d &&
+                     ((foot->a <= foot->b) ? (l >= foot->a && l < foot->b) : (l >= foot->a || l < foot->b));
+            } else if (foot->kind == GF_FOOT_REGIONS) {
+                in = false;
+                for (int q = 0; q < foot->nregions && q < GF_MAX_REGIONS && !in; q++)
+                    in = or_region_inside(foot->regions[q], t->lb[row], t->lb[P + row]);
             }
             if (!in) t->hidden[row] = 1;
         }

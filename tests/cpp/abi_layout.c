@@ -18,6 +18,7 @@ int main(void)
     OF(gf_model_config, n_brk); OF(gf_model_config, rbreak); OF(gf_model_config, cube); OF(gf_model_config, cube_n);
     OF(gf_model_config, cube_tc);
     SZ(gf_ext_map); OF(gf_ext_map, n); OF(gf_ext_map, tc); OF(gf_extinction, north); OF(gf_extinction, south);
+    SZ(gf_region); OF(gf_region, bmin); OF(gf_footprint, nregions); OF(gf_footprint, regions);
     SZ(gf_extinction); SZ(gf_footprint); OF(gf_footprint, a);
     SZ(gf_table); OF(gf_table, nbands); OF(gf_table, lb); OF(gf_table, hidden); OF(gf_table, radec); OF(gf_table, FeH_comp); OF(gf_table, absmagSysNcomp); OF(gf_table, systems);
     SZ(gf_fixedfeh_config); SZ(gf_vmoments); SZ(gf_bond2010_config); OF(gf_bond2010_config, halo); OF(gf_bond2010_config, T);

@@ -270,6 +270,7 @@ def test_extinction_maps_equal_oracle(lib, multipliers):
     assert (am < 0).any() and (am > 0).any()
     lat = np.concatenate([got[m]["lb"][1] for m in got])
     assert (lat > 0).any() and (lat < 0).any()
-    got2, stats = batched_catalogs(ctx, [w, model_types_workload(lib)])
+    other = W.build_workload(lib, foot=W.cap_footprint(60.0, 40.0, 1.0), dx_deg=0.25, m0=15.0, m1=19.5, seed48=6)
+    got2, stats = batched_catalogs(ctx, [w, other])
     ctx.close()
     compare(ref, got2[0], "multi")

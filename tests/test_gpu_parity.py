@@ -270,3 +270,28 @@ def test_unresolved_multiples_parity(ctx, lib, multipliers, algo):
         if algo == 3:
             assert (g["absmagSys"][1][two] == g["absmagSys"][0][two]).all()
     assert binaries > 100 and singles > 100
+
+
+def test_footprint_regions_parity(ctx, lib, multipliers):
+    """GF_FOOT_REGIONS on the device clipper: an equatorial beam with a hole around
+    (ra, dec) = (210, 30) and a galactic rectangle minus |b| < 52 deg; the clipped
+    catalog (hidden flags and all columns) equals the oracle's, the clipper hides
+    stars of both regions' edge pixels, and visible stars satisfy the regions."""
+    import math
+    foot = W.regions_footprint([dict(type="beam", coordsys="equ", v=(210.0, 30.0, 3.0, 1.0)),
+                                dict(type="rect", v=(40.0, 48.0, 48.0, 58.0), bmin=52.0)])
+    w = W.build_workload(lib, foot=foot, dx_deg=0.25, m0=15.0, m1=20.0, capacity=1 << 18, seed48=11)
+    gs, os_, gb, ob = run_both(ctx, w, multipliers)
+    assert len(gb) == len(ob) > 2
+    hidden = visible = 0
+    for (gm, go, g), (om, oo, o) in zip(gb, ob):
+        assert (gm, go) == (om, oo)
+        assert_same(g, o, SKY_COLS)
+        assert_same(g, o, MODULE_COLS, exact=False)
+        vis = g["hidden"] == 0
+        visible += int(vis.sum())
+        hidden += int((~vis).sum())
+        b = g["lb"][1][vis]
+        rect = (g["lb"][0][vis] >= 40.0) & (g["lb"][0][vis] < 48.0)
+        assert (np.abs(b[rect]) >= 52.0).all()
+    assert visible > 1000 and hidden > 100

@@ -61,7 +61,7 @@ def test_struct_layouts(tmp_path):
               "gf_catalog_stats": G.CatalogStats, "gf_precision_report": A.PrecisionReport,
               "gf_textout_config": G.TextoutConfig, "gf_textout_set": G.TextoutSet,
               "gf_server_info": G.ServerInfo, "gf_multiples_config": A.MultiplesConfig,
-              "gf_ext_map": A.ExtMap}
+              "gf_ext_map": A.ExtMap, "gf_region": A.Region}
     checked = 0
     for line in out.split("\n"):
         if not line.strip():
@@ -369,3 +369,41 @@ def test_extinction_beam_minima_follow_the_reference(lib):
                     want = np.minimum(want, col)
         got = w.ammin[p.extIdx * nz:(p.extIdx + 1) * nz]
         np.testing.assert_array_equal(got, want, err_msg="beam %d" % i)
+
+
+def _pixel_lb(w):
+    pix = w.pixel_array()
+    l = np.array([math.degrees(math.atan2(p.sl, p.cl)) % 360.0 for p in pix])
+    b = np.array([math.degrees(math.atan2(p.sb, p.cb)) for p in pix])
+    area = np.array([p.dA * p.coveredFraction for p in pix])
+    return l, b, area
+
+
+def test_footprint_regions_pixelise_to_their_areas(lib):
+    """GF_FOOT_REGIONS: a beam with a hole, a union of overlapping beams, a lon/lat
+    rectangle minus the |b| < bmin band, and an equatorial beam around the north
+    celestial pole, pixelised on 0.2 deg Lambert cells: the covered areas match the
+    regions' areas to 1 %, and the equatorial beam lands on the galactic position of
+    the pole (l, b) = (122.93, 27.13) deg."""
+    import math
+    from galfast_b200 import workloads as W
+    d2r = math.pi / 180
+
+    def area_of(foot):
+        w = W.build_workload(lib, foot=foot, dx_deg=0.2, m0=15.0, m1=16.0, with_modules=False)
+        l, b, a = _pixel_lb(w)
+        return a.sum(), l, b, a
+
+    cap = lambda r: 2 * math.pi * (1 - math.cos(r * d2r))
+    got, _, _, _ = area_of(W.regions_footprint([dict(type="beam", v=(40, 30, 6, 2))]))
+    assert got == pytest.approx(cap(6) - cap(2), rel=0.01)
+    got, _, _, _ = area_of(W.regions_footprint([dict(type="beam", v=(40, 30, 5, 0)), dict(type="beam", v=(40, 30, 3, 0)),
+                                                dict(type="beam", v=(200, -40, 4, 0))]))
+    assert got == pytest.approx(cap(5) + cap(4), rel=0.01)
+    got, _, _, _ = area_of(W.regions_footprint([dict(type="rect", v=(100, 130, -20, 25), bmin=10)]))
+    strip = lambda b0, b1: (math.sin(b1 * d2r) - math.sin(b0 * d2r)) * 30 * d2r
+    assert got == pytest.approx(strip(-20, -10) + strip(10, 25), rel=0.01)
+    got, l, b, a = area_of(W.regions_footprint([dict(type="beam", coordsys="equ", v=(0, 90, 3, 0))]))
+    assert got == pytest.approx(cap(3), rel=0.01)
+    assert np.average(b, weights=a) == pytest.approx(27.13, abs=0.2)
+    assert np.average(l, weights=a) == pytest.approx(122.93, abs=0.5)
