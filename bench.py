@@ -320,7 +320,7 @@ def reduce_max_sum(dist, tmax, tsum):
 # 64-request case of the batched workload (DRAM read + write over its bins);
 # traffic grows with the bins (each block reads its plan entries and slot row,
 # each star its event), so a full launch's traffic is this times its bins.
-DRAW_TRAFFIC_PER_BIN = 561.55e6 / 4.3396e9
+DRAW_TRAFFIC_PER_BIN = 852.35e6 / 4.3396e9
 DRAW_TRAFFIC_SOURCE = "ncu capture of batch_draw_kernel on 64 requests of the set, scaled by bins per launch"
 
 

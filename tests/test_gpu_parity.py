@@ -287,8 +287,11 @@ def test_footprint_regions_parity(ctx, lib, multipliers):
     for (gm, go, g), (om, oo, o) in zip(gb, ob):
         assert (gm, go) == (om, oo)
         assert_same(g, o, SKY_COLS)
-        assert_same(g, o, MODULE_COLS, exact=False)
         vis = g["hidden"] == 0
+        # module columns of the rows the clipper hid are not written (the oracle's
+        # reused table keeps an earlier batch's values there): compare the visible rows
+        assert_same({k: g[k][..., vis] for k in MODULE_COLS}, {k: o[k][..., vis] for k in MODULE_COLS}, MODULE_COLS,
+                    exact=False)
         visible += int(vis.sum())
         hidden += int((~vis).sum())
         b = g["lb"][1][vis]
