@@ -944,7 +944,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         ws.free_recorded[0] = ws.free_recorded[1] = false;
         hd.cb = hcb;
         hd.user = user;
-        hd.piece_rows = piece_rows > 0 ? piece_rows : (int64_t)4 << 20;
+        hd.piece_rows = piece_rows > 0 ? piece_rows : (int64_t)16 << 20;
         hd.nbands = nbands;
         const size_t slot_bytes = carved_bytes(hd.piece_rows, nbands, ctx->host_cols);
         GF_TRY(ws.ring.need(slot_bytes * GF_RING));

@@ -579,7 +579,7 @@ gf_status gf_multi_set_memory_budget(gf_ctx *ctx, int64_t bytes);
 /* gf_catalog_run_multi with the rows delivered in host memory.  After each model
  * pass the library copies the pass's rows to a ring of page-locked host tables on
  * a second stream while the device generates the next pass, in pieces of at most
- * piece_rows rows (0: 4M).  cb sees one piece: request j's rows are
+ * piece_rows rows (0: 16M).  cb sees one piece: request j's rows are
  * host rows row_begin[j] .. row_begin[j] + row_count[j] - 1 (count 0: none in
  * this piece); a request's rows of a model arrive in order, possibly over several
  * pieces.  The host table is valid until cb returns.  cb runs on a CUDA driver
