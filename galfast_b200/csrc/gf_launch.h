@@ -79,12 +79,8 @@ struct LaunchPlaceMulti {
     const int32_t *job_slot;       /* output position of each request */
     const StarRecord *rec;
     int64_t n;
-    double *lb;
-    int32_t *projIdx;
-    float *projXY, *DM, *absmag, *XYZ, *Am, *AmInf;
-    int32_t *hidden;
-    uint64_t *key, *key_b;
-    uint32_t *idx_a, *idx_b, *slot_a;
+    uint64_t *key, *key_b;         /* sort keys, before and after the sort */
+    uint32_t *idx_a, *idx_b;       /* record index after and before the sort */
     int slot_bits;             /* bits of the output slot at the top of the sort key */
     void *temp;
     size_t temp_bytes;
@@ -107,7 +103,7 @@ cudaError_t launch_seed_streams(const uint32_t *seeds, int njobs, const uint32_t
 cudaError_t launch_crawl_multi(const LaunchCrawlMulti &L, int draw, cudaStream_t s);
 cudaError_t sort_temp_bytes_multi(int64_t n, size_t *bytes);
 cudaError_t launch_place_sort_multi(const LaunchPlaceMulti &L, cudaStream_t s);
-cudaError_t launch_tie_gather_multi(const LaunchPlaceMulti &L, const int64_t *row_begin, const int32_t *slot_comp,
+cudaError_t launch_tie_place_multi(const LaunchPlaceMulti &L, const int64_t *row_begin, const int32_t *slot_comp,
                                     gf_table out, int32_t *row_slot, cudaStream_t s);
 
 /* modules (gf_modules.cu) */

@@ -197,11 +197,9 @@ struct MultiWS {
     Grow<int32_t> slot_job;
     Grow<int64_t> slot_rows;
     Grow<StarRecord> rec;
-    Grow<double> lb;
-    Grow<int32_t> projIdx, hidden, row_slot;
-    Grow<float> projXY, DMc, absmag, XYZ, Am, AmInf;
+    Grow<int32_t> row_slot;
     Grow<uint64_t> key, key_b;
-    Grow<uint32_t> idx_a, idx_b, slot_a;
+    Grow<uint32_t> idx_a, idx_b;
     Grow<char> temp;
     Grow<double2> pixsum, tot;              /* pixel-by-pixel integrate: per pixel, per request */
     Grow<const unsigned char *> plans;
@@ -812,10 +810,10 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
     }
 
     /* ---- requests generated together ---- */
-    /* device memory of a batched request's draw passes: records, placement, sort and
+    /* device memory of a batched request's draw passes: records, sort keys and
      * output columns take about kStarBytes per star of its largest model, events 48
      * bytes per star at most, and the slot densities of its pixels */
-    const double kStarBytes = 320.0;
+    const double kStarBytes = 256.0;
     auto need_of = [&](int j) {
         double mx = 0;
         for (int i = 0; i < nmod; i++) mx = std::max(mx, S[j].expected[i] + 8.0 * sqrt(S[j].expected[i]) + 1024.0);
@@ -923,11 +921,9 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
 
     /* growing buffers of the draw passes */
     auto &rec = ws.rec;
-    auto &lb = ws.lb;
-    auto &projIdx = ws.projIdx, &hidden = ws.hidden, &row_slot = ws.row_slot;
-    auto &projXY = ws.projXY, &DMc = ws.DMc, &absmag = ws.absmag, &XYZ = ws.XYZ, &Am = ws.Am, &AmInf = ws.AmInf;
+    auto &row_slot = ws.row_slot;
     auto &key = ws.key, &key_b = ws.key_b;
-    auto &idx_a = ws.idx_a, &idx_b = ws.idx_b, &slot_a = ws.slot_a;
+    auto &idx_a = ws.idx_a, &idx_b = ws.idx_b;
     auto &temp = ws.temp;
     std::vector<int64_t> catoff(njobs, 0);
     /* host delivery: copy stream, events and the page-locked ring */
@@ -1183,12 +1179,9 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                     cap = nrec + nrec / 8 + 65536;
                 }
             }
-            /* placement and the (request, star_comp) sort */
+            /* the (request, star_comp) sort of the records; placement follows in sorted order */
             const size_t n = (size_t)std::max<int64_t>(nrec, 1);
-            GF_TRY(lb.need(2 * n)); GF_TRY(projIdx.need(n)); GF_TRY(hidden.need(n)); GF_TRY(projXY.need(2 * n));
-            GF_TRY(DMc.need(n)); GF_TRY(absmag.need(n)); GF_TRY(XYZ.need(3 * n)); GF_TRY(Am.need(n)); GF_TRY(AmInf.need(n));
             GF_TRY(key.need(n)); GF_TRY(key_b.need(n)); GF_TRY(idx_a.need(n)); GF_TRY(idx_b.need(n));
-            GF_TRY(slot_a.need(n));
             size_t tb = 0;
             GF_CUDA(gfk::sort_temp_bytes_multi((int64_t)n, &tb));
             GF_TRY(temp.need(tb + 256));
@@ -1196,9 +1189,8 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
             gfk::LaunchPlaceMulti PL;
             memset(&PL, 0, sizeof(PL));
             PL.jobs = d_jobs; PL.job_slot = d_job_slot; PL.rec = rec.p; PL.n = nrec;
-            PL.lb = lb.p; PL.projIdx = projIdx.p; PL.projXY = projXY.p; PL.DM = DMc.p; PL.absmag = absmag.p;
-            PL.XYZ = XYZ.p; PL.Am = Am.p; PL.AmInf = AmInf.p; PL.hidden = hidden.p; PL.key = key.p; PL.key_b = key_b.p;
-            PL.idx_a = idx_a.p; PL.idx_b = idx_b.p; PL.slot_a = slot_a.p; PL.slot_bits = slot_bits;
+            PL.key = key.p; PL.key_b = key_b.p;
+            PL.idx_a = idx_a.p; PL.idx_b = idx_b.p; PL.slot_bits = slot_bits;
             PL.temp = temp.p; PL.temp_bytes = temp.n;
             PL.seg_begin = d_seg; PL.vis_end = d_seg + nslots; PL.seg_end = d_seg + 2 * nslots;
             {
@@ -1258,8 +1250,8 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
             GF_CUDA(cudaMemcpyAsync(d_slot_comp, slot_comp.data(), 4 * (size_t)nslots, cudaMemcpyHostToDevice, st));
             GF_CUDA(cudaMemcpyAsync(d_catoff, catoff.data(), 8 * (size_t)njobs, cudaMemcpyHostToDevice, st));
             {
-                ProfScope ps(ctx, GF_PROF_SORT);
-                GF_CUDA(gfk::launch_tie_gather_multi(PL, d_row_begin, d_slot_comp, out, row_slot.p, st));
+                ProfScope ps(ctx, GF_PROF_PLACE);
+                GF_CUDA(gfk::launch_tie_place_multi(PL, d_row_begin, d_slot_comp, out, row_slot.p, st));
             }
             out.size = total;
             GF_TRY(gfa::zero_module_rows(ctx, &out, total));

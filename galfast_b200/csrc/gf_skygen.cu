@@ -775,10 +775,24 @@ __device__ __forceinline__ void deproject(const gf_lambert &p, double &l, double
     l = p.l0 + gfm::atan2_d((double)x * sc, (double)p.cb * cc / ir - (double)(y * p.sb) * sc);
 }
 
-/* Placement of one star record (draw_stars, skygen.cu.h:376-456) into row i of
- * the unsorted columns; returns whether the star is visible. */
-__device__ __forceinline__ int place_one(const SkyModel &m, const SkyGeom &g, const StarRecord &rec, int64_t i, int64_t n,
-                                         const PlaceParams &P)
+/* The placed values of one star record (draw_stars, skygen.cu.h:376-456). */
+struct Placed {
+    double l, b;            /* degrees */
+    float x, y;             /* Lambert coordinates */
+    float DM, M;
+    float X, Y, Z;
+    float Am, AmInf;
+    int32_t projIdx;
+    int edge;               /* x^2 + y^2 > 2: beyond the projection edge, nothing else is set */
+    int vis;                /* visible: not beyond the edge and no fainter than m1 after extinction */
+};
+
+/* Placement of one star record (draw_stars, skygen.cu.h:376-456).  am points to
+ * the record's anchor extinction (3-D maps) or is null.  Every caller that places
+ * the same record gets the same bits: the expressions are evaluated in one order
+ * and the device code is compiled without contraction. */
+__device__ __forceinline__ void place_values(const SkyModel &m, const SkyGeom &g, const StarRecord &rec, const float *am,
+                                             Placed &v)
 {
     const double r2d = 57.2957795130823208767981548;
     const gf_pencil_beam pix = g.pixels[rec.ilb];
@@ -786,14 +800,16 @@ __device__ __forceinline__ int place_one(const SkyModel &m, const SkyGeom &g, co
     float x = pix.X, y = pix.Y;
     x += pix.dx * (rec.u[0] - 0.5f);
     y += pix.dx * (rec.u[1] - 0.5f);
+    v.x = x;
+    v.y = y;
     if (x * x + y * y > 2.f) {
-        P.hidden[i] = 1;
-        P.key[i] = ~0ull;
-        return 0;
+        v.edge = 1;
+        v.vis = 0;
+        v.l = 0.;
+        return;
     }
-    P.projIdx[i] = pix.projIdx;
-    P.projXY[i] = x;
-    P.projXY[n + i] = y;
+    v.edge = 0;
+    v.projIdx = pix.projIdx;
     double l, b;
     deproject(g.proj[pix.projIdx], l, b, x, y);
     float cl = (float)gfm::cos_d(l), cb = (float)gfm::cos_d(b);
@@ -802,17 +818,17 @@ __device__ __forceinline__ int place_one(const SkyModel &m, const SkyGeom &g, co
     if (l < 0.) l += 360.;
     if (l > 360.) l -= 360.;
     b *= r2d;
-    P.lb[i] = l;
-    P.lb[n + i] = b;
+    v.l = l;
+    v.b = b;
     float Mtmp = M + m.dM * (rec.u[2] - 0.5f);
     float mtmp = m.m0 + m.dm * ((float)rec.im + rec.u[3] - 0.5f);
     float DM = mtmp - Mtmp;
-    P.absmag[i] = Mtmp;
-    P.DM[i] = DM;
+    v.M = Mtmp;
+    v.DM = DM;
     float D = gfm::powf_(10.f, 0.2f * DM + 1.f);
-    P.XYZ[i] = D * cl * cb;
-    P.XYZ[n + i] = D * sl * cb;
-    P.XYZ[2 * n + i] = D * sb;
+    v.X = D * cl * cb;
+    v.Y = D * sl * cb;
+    v.Z = D * sb;
     float Am0, AmInf;
     if (g.ext_kind == GF_EXT_MAPS) {
         /* sampleExtinction at the star's DM and at DM = 100 (skygen.cu.h:421-424) */
@@ -823,17 +839,43 @@ __device__ __forceinline__ int place_one(const SkyModel &m, const SkyGeom &g, co
         Am0 = (g.ext_kind == GF_EXT_SCREEN_CSCB) ? g.A0 / fabsf(sb) : 0.f;
         AmInf = Am0;
     }
-    int hid = (mtmp + Am0 > m.m1) ? 1 : 0;
+    v.vis = (mtmp + Am0 > m.m1) ? 0 : 1;
     /* the extinction at the bin's anchor (draw_stars, skygen.cu.h:437-446): carried with
      * the record for 3-D maps (it depends on the anchor's distance), else the beam's */
-    const float AmMin = (g.ext_kind == GF_EXT_MAPS && P.rec_am) ? P.rec_am[i] : gfc::beam_extinction(g, pix);
+    const float AmMin = (g.ext_kind == GF_EXT_MAPS && am) ? *am : gfc::beam_extinction(g, pix);
     if (AmMin > Am0) AmInf = -AmMin;
-    P.Am[i] = Am0;
-    P.AmInf[i] = AmInf;
-    P.hidden[i] = hid;
+    v.Am = Am0;
+    v.AmInf = AmInf;
+}
+
+/* Placement of one star record into row i of the unsorted columns; returns
+ * whether the star is visible. */
+__device__ __forceinline__ int place_one(const SkyModel &m, const SkyGeom &g, const StarRecord &rec, int64_t i, int64_t n,
+                                         const PlaceParams &P)
+{
+    Placed v;
+    place_values(m, g, rec, P.rec_am ? P.rec_am + i : nullptr, v);
+    if (v.edge) {
+        P.hidden[i] = 1;
+        P.key[i] = ~0ull;
+        return 0;
+    }
+    P.projIdx[i] = v.projIdx;
+    P.projXY[i] = v.x;
+    P.projXY[n + i] = v.y;
+    P.lb[i] = v.l;
+    P.lb[n + i] = v.b;
+    P.absmag[i] = v.M;
+    P.DM[i] = v.DM;
+    P.XYZ[i] = v.X;
+    P.XYZ[n + i] = v.Y;
+    P.XYZ[2 * n + i] = v.Z;
+    P.Am[i] = v.Am;
+    P.AmInf[i] = v.AmInf;
+    P.hidden[i] = v.vis ? 0 : 1;
     /* l >= 0 here (-0.0 compares equal to 0.0 and maps to key 0) */
-    P.key[i] = hid ? ~0ull : (l == 0.0 ? 0ull : (uint64_t)__double_as_longlong(l));
-    return hid ? 0 : 1;
+    P.key[i] = v.vis ? (v.l == 0.0 ? 0ull : (uint64_t)__double_as_longlong(v.l)) : ~0ull;
+    return v.vis;
 }
 
 __global__ void __launch_bounds__(256) place_kernel(PlaceParams P)
@@ -1203,176 +1245,238 @@ cudaError_t launch_crawl_multi(const LaunchCrawlMulti &L, int draw, cudaStream_t
     return cudaGetLastError();
 }
 
-/* The sort key of a record of a many-request pass: its request's output slot in
- * the top sb bits, below them the IEEE bits 62..sb-1 of l (l >= 0, so the sign
- * bit is 0 and the order of the bits is the order of l), all ones for hidden
- * rows (after every visible row of the slot: l <= 360 never has all those bits
- * set).  The sort uses the bits from GF_SORT_LOW_BIT up; records equal there --
- * within about 2^-24 of l of each other -- are ordered by the tie pass on the
- * full (l, b, DM, M, Am), star_comp's order (skyconfig_impl.h:34-68). */
-__device__ __forceinline__ uint64_t multi_key(uint32_t slot, int sb, uint64_t lkey)
+/* Sort keys of a many-request pass.  A record's key holds its request's output
+ * slot in the top sb bits and below them l in fixed point, floor(l * 2^(lbits-9))
+ * with lbits = key bits - sb (l <= 360 < 2^9, so the all-ones value of lbits bits
+ * is never reached and marks a hidden record, which sorts after every visible
+ * record of its slot).  The floor is monotone in l, so the sorted order is l's order
+ * up to runs of equal keys (records within 2^-(lbits-9) degrees of each other),
+ * which the tie pass orders on the full (l, b, DM, M, Am): star_comp's order
+ * (skyconfig_impl.h:34-68).  The key width is sb + 32 bits rounded up to whole
+ * 8-bit radix digits, so l keeps at least 23 fractional bits (1.2e-7 deg). */
+int multi_key_bits(int sb)
 {
-    const uint64_t low = (lkey == ~0ull) ? (~0ull >> sb) : (lkey >> (sb - 1));
-    return ((uint64_t)slot << (64 - sb)) | low;
+    const int t = (sb + 32 + 7) / 8 * 8;
+    return t > 64 ? 64 : t;
 }
 
-/* placement of the records of many requests, with their combined sort keys */
-__global__ void __launch_bounds__(256) place_multi_kernel(PlaceParams P, const CrawlJob *jobs, const int32_t *job_slot,
-                                                          int sb)
+struct MultiKeyParams {
+    const StarRecord *rec;
+    int64_t n;
+    const CrawlJob *jobs;
+    const int32_t *job_slot;
+    int lbits;
+    double lscale;          /* 2^(lbits-9) */
+    uint64_t *key;
+    uint32_t *idx;
+};
+
+/* the sort key of every record, and the identity permutation beside it */
+__global__ void __launch_bounds__(256) key_multi_kernel(MultiKeyParams K)
 {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += (int64_t)gridDim.x * blockDim.x) {
-        const StarRecord rec = P.rec[i];
+    const uint64_t lmask = (1ull << K.lbits) - 1;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < K.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const StarRecord rec = K.rec[i];
         const int job = rec.stream >> 16;
-        const CrawlJob &J = jobs[job];
-        place_one(J.m, J.g, rec, i, P.n, P);
-        P.key[i] = multi_key((uint32_t)job_slot[job], sb, P.key[i]);
+        const CrawlJob &J = K.jobs[job];
+        Placed v;
+        place_values(J.m, J.g, rec, nullptr, v);
+        const uint64_t lk = v.vis ? (uint64_t)(v.l * K.lscale) : lmask;
+        K.key[i] = ((uint64_t)(uint32_t)K.job_slot[job] << K.lbits) | lk;
+        K.idx[i] = (uint32_t)i;
     }
 }
 
-/* the slot of every sorted record (the top sb bits of its key) */
-__global__ void key_slot_kernel(const uint64_t *key, int sb, uint32_t *slot, int64_t n)
+/* per output slot: first sorted position, end of its visible records (hidden
+ * records sort last within the slot) and end of the slot */
+__global__ void segment_bounds_kernel(const uint64_t *key, int lbits, int64_t n, int64_t *seg_begin, int64_t *vis_end,
+                                      int64_t *seg_end)
 {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        slot[i] = (uint32_t)(key[i] >> (64 - sb));
-}
-
-/* per output slot: first sorted position, end of its visible rows (hidden rows
- * carry all ones below the slot bits and sort last within the slot) and end of
- * the slot */
-__global__ void segment_bounds_kernel(const uint32_t *slot, const uint64_t *key, int sb, int64_t n, int64_t *seg_begin,
-                                      int64_t *vis_end, int64_t *seg_end)
-{
-    const uint64_t lmask = ~0ull >> sb;
+    const uint64_t lmask = (1ull << lbits) - 1;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t sl = slot[i];
-        const bool first = (i == 0) || slot[i - 1] != sl;
-        const bool last = (i + 1 == n) || slot[i + 1] != sl;
+        const uint64_t k = key[i];
+        const uint32_t sl = (uint32_t)(k >> lbits);
+        const bool first = (i == 0) || (uint32_t)(key[i - 1] >> lbits) != sl;
+        const bool last = (i + 1 == n) || (uint32_t)(key[i + 1] >> lbits) != sl;
         if (first) seg_begin[sl] = i;
         if (last) seg_end[sl] = i + 1;
-        const bool hid = (key[i] & lmask) == lmask;
+        const bool hid = (k & lmask) == lmask;
         if (hid && (first || (key[i - 1] & lmask) != lmask)) vis_end[sl] = i;
         if (!hid && last) vis_end[sl] = i + 1;
     }
 }
 
-/* Runs of visible records equal in the sorted key bits (one slot, l within the
- * key's resolution) ordered by (l, b, DM, M, Am) (star_comp, skyconfig_impl.h:34-68). */
-__global__ void tie_multi_kernel(const uint64_t *key, int sb, int low_bit, uint32_t *idx, int64_t n, const double *lb,
-                                 const float *DM, const float *absmag, const float *Am, int64_t pitch)
+/* star_comp's fields of a record: l, b, DM, M, Am (floats widened exactly) */
+__device__ __forceinline__ void tie_fields(const StarRecord *recs, const CrawlJob *jobs, uint32_t s, double f[5])
 {
-    const uint64_t lmask = ~0ull >> sb;
+    const StarRecord rec = recs[s];
+    const CrawlJob &J = jobs[rec.stream >> 16];
+    Placed v;
+    place_values(J.m, J.g, rec, nullptr, v);
+    f[0] = v.l; f[1] = v.b; f[2] = v.DM; f[3] = v.M; f[4] = v.Am;
+}
+
+__device__ __forceinline__ bool star_less(const double *a, const double *b)
+{
+    for (int q = 0; q < 4; q++)
+        if (a[q] != b[q]) return a[q] < b[q];
+    return a[4] < b[4];
+}
+
+/* Runs of visible records with equal keys, ordered by (l, b, DM, M, Am)
+ * (star_comp, skyconfig_impl.h:34-68) with an insertion sort of their indices;
+ * the fields are recomputed from the records (runs up to kTieCache long keep
+ * them in registers, longer ones recompute them per comparison). */
+__global__ void __launch_bounds__(256) tie_multi_kernel(const uint64_t *key, int lbits, uint32_t *idx, int64_t n,
+                                                        const StarRecord *recs, const CrawlJob *jobs)
+{
+    constexpr int kTieCache = 8;
+    const uint64_t lmask = (1ull << lbits) - 1;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        if ((key[i] & lmask) == lmask) continue;
-        const uint64_t k = key[i] >> low_bit;
-        if (i + 1 >= n || (key[i + 1] >> low_bit) != k) continue;
-        if (i > 0 && (key[i - 1] >> low_bit) == k) continue;     /* not a run start */
+        const uint64_t k = key[i];
+        if ((k & lmask) == lmask) continue;
+        if (i + 1 >= n || key[i + 1] != k) continue;
+        if (i > 0 && key[i - 1] == k) continue;     /* not a run start */
         int64_t e = i + 1;
-        while (e + 1 < n && (key[e + 1] >> low_bit) == k) e++;
-        for (int64_t q = i + 1; q <= e; q++) {
-            uint32_t cur = idx[q];
-            int64_t r = q - 1;
-            while (r >= i) {
-                uint32_t o = idx[r];
-                bool less;
-                if (lb[cur] != lb[o]) less = lb[cur] < lb[o];
-                else if (lb[pitch + cur] != lb[pitch + o]) less = lb[pitch + cur] < lb[pitch + o];
-                else if (DM[cur] != DM[o]) less = DM[cur] < DM[o];
-                else if (absmag[cur] != absmag[o]) less = absmag[cur] < absmag[o];
-                else less = Am[cur] < Am[o];
-                if (!less) break;
-                idx[r + 1] = o;
-                r--;
+        while (e + 1 < n && key[e + 1] == k) e++;
+        const int64_t len = e - i + 1;
+        if (len <= kTieCache) {
+            double f[kTieCache][5];
+            uint32_t id[kTieCache];
+#pragma unroll
+            for (int q = 0; q < kTieCache; q++) {
+                if (q < len) {
+                    id[q] = idx[i + q];
+                    tie_fields(recs, jobs, id[q], f[q]);
+                }
             }
-            idx[r + 1] = cur;
+            /* insertion sort over the cached fields (stable: equal records keep their order) */
+            int ord[kTieCache];
+#pragma unroll
+            for (int q = 0; q < kTieCache; q++) ord[q] = q;
+            for (int q = 1; q < (int)len; q++) {
+                const int cur = ord[q];
+                int r = q - 1;
+                while (r >= 0 && star_less(f[cur], f[ord[r]])) {
+                    ord[r + 1] = ord[r];
+                    r--;
+                }
+                ord[r + 1] = cur;
+            }
+            for (int q = 0; q < (int)len; q++) {
+                uint32_t v = id[0];
+#pragma unroll
+                for (int t = 1; t < kTieCache; t++)
+                    if (ord[q] == t) v = id[t];
+                idx[i + q] = v;
+            }
+        } else {
+            for (int64_t q = i + 1; q <= e; q++) {
+                const uint32_t cur = idx[q];
+                double fc[5];
+                tie_fields(recs, jobs, cur, fc);
+                int64_t r = q - 1;
+                while (r >= i) {
+                    const uint32_t o = idx[r];
+                    double fo[5];
+                    tie_fields(recs, jobs, o, fo);
+                    if (!star_less(fc, fo)) break;
+                    idx[r + 1] = o;
+                    r--;
+                }
+                idx[r + 1] = cur;
+            }
         }
     }
 }
 
-/* visible rows of each slot into the output table at row_begin[slot]; row_slot maps rows back */
-__global__ void __launch_bounds__(256) gather_multi_kernel(GatherParams G, const uint32_t *slot, const int64_t *seg_begin,
-                                                           const int64_t *vis_end, const int64_t *row_begin,
-                                                           const int32_t *slot_comp, int32_t *row_slot)
-{
-    const int64_t P = G.out.capacity, S = G.src_pitch;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < G.n; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t sl = slot[i];
-        if (i >= vis_end[sl]) continue;
-        const int64_t o = row_begin[sl] + (i - seg_begin[sl]);
-        const uint32_t s = G.idx[i];
-        G.out.lb[o] = G.lb[s];
-        G.out.lb[P + o] = G.lb[S + s];
-        G.out.projIdx[o] = G.projIdx[s];
-        G.out.projXY[o] = G.projXY[s];
-        G.out.projXY[P + o] = G.projXY[S + s];
-        G.out.DM[o] = G.DM[s];
-        G.out.absmag[o] = G.absmag[s];
-        G.out.XYZ[o] = G.XYZ[s];
-        G.out.XYZ[P + o] = G.XYZ[S + s];
-        G.out.XYZ[2 * P + o] = G.XYZ[2 * S + s];
-        G.out.comp[o] = slot_comp[sl];
-        G.out.Am[o] = G.Am[s];
-        G.out.AmInf[o] = G.AmInf[s];
-        G.out.hidden[o] = 0;
-        row_slot[o] = (int32_t)sl;
-    }
-}
+struct PlaceSortedParams {
+    const StarRecord *rec;
+    const CrawlJob *jobs;
+    const uint64_t *key;
+    const uint32_t *idx;
+    int64_t n;
+    int lbits;
+    const int64_t *seg_begin, *vis_end, *row_begin;
+    const int32_t *slot_comp;
+    gf_table out;
+    int32_t *row_slot;
+};
 
-/* lowest key bit the multi-request sort looks at: keeps the slot and l to 24
- * mantissa bits (2^-24 relative); the tie pass orders what the sort leaves equal */
-static int sort_low_bit(int sb)
+/* Placement in sorted order: the visible records of each slot, placed straight
+ * into the output table at row_begin[slot] (consecutive sorted records of a slot
+ * are consecutive rows, so the column stores coalesce); row_slot maps rows back
+ * to their slot. */
+__global__ void __launch_bounds__(256) place_sorted_multi_kernel(PlaceSortedParams S)
 {
-    const int b = 53 - sb - 24;
-    return b > 0 ? b : 0;
+    const int64_t P = S.out.capacity;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < S.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t sl = (uint32_t)(S.key[i] >> S.lbits);
+        if (i >= S.vis_end[sl]) continue;
+        const int64_t o = S.row_begin[sl] + (i - S.seg_begin[sl]);
+        const StarRecord rec = S.rec[S.idx[i]];
+        const CrawlJob &J = S.jobs[rec.stream >> 16];
+        Placed v;
+        place_values(J.m, J.g, rec, nullptr, v);
+        S.out.lb[o] = v.l;
+        S.out.lb[P + o] = v.b;
+        S.out.projIdx[o] = v.projIdx;
+        S.out.projXY[o] = v.x;
+        S.out.projXY[P + o] = v.y;
+        S.out.DM[o] = v.DM;
+        S.out.absmag[o] = v.M;
+        S.out.XYZ[o] = v.X;
+        S.out.XYZ[P + o] = v.Y;
+        S.out.XYZ[2 * P + o] = v.Z;
+        S.out.comp[o] = S.slot_comp[sl];
+        S.out.Am[o] = v.Am;
+        S.out.AmInf[o] = v.AmInf;
+        S.out.hidden[o] = 0;
+        S.row_slot[o] = (int32_t)sl;
+    }
 }
 
 cudaError_t launch_place_sort_multi(const LaunchPlaceMulti &L, cudaStream_t s)
 {
     if (L.n <= 0) return cudaSuccess;
     const int blocks = (int)std::min<int64_t>((L.n + 255) / 256, (int64_t)sm_count() * 16);
-    const int sb = L.slot_bits;
-    PlaceParams P;
-    memset(&P, 0, sizeof(P));
-    P.rec = L.rec; P.n = L.n;
-    P.lb = L.lb; P.projIdx = L.projIdx; P.projXY = L.projXY; P.DM = L.DM; P.absmag = L.absmag;
-    P.XYZ = L.XYZ; P.Am = L.Am; P.AmInf = L.AmInf; P.hidden = L.hidden; P.key = L.key;
-    place_multi_kernel<<<blocks, 256, 0, s>>>(P, L.jobs, L.job_slot, sb);
-    iota_kernel<<<blocks, 256, 0, s>>>(L.idx_b, L.n);
-    /* one radix sort by (slot, l): the records of each request in star_comp order up to ties */
+    const int kb = multi_key_bits(L.slot_bits);
+    const int lbits = kb - L.slot_bits;
+    MultiKeyParams K;
+    K.rec = L.rec; K.n = L.n; K.jobs = L.jobs; K.job_slot = L.job_slot;
+    K.lbits = lbits; K.lscale = ldexp(1.0, lbits - 9);
+    K.key = L.key; K.idx = L.idx_b;
+    key_multi_kernel<<<blocks, 256, 0, s>>>(K);
+    /* one radix sort by (slot, l) over the key's bits: each request's records in l order */
     size_t tb = L.temp_bytes;
-    cudaError_t e = cub::DeviceRadixSort::SortPairs(L.temp, tb, L.key, L.key_b, L.idx_b, L.idx_a, (int)L.n,
-                                                    sort_low_bit(sb), 64, s);
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(L.temp, tb, L.key, L.key_b, L.idx_b, L.idx_a, (int)L.n, 0, kb, s);
     if (e != cudaSuccess) return e;
-    key_slot_kernel<<<blocks, 256, 0, s>>>(L.key_b, sb, L.slot_a, L.n);
-    segment_bounds_kernel<<<blocks, 256, 0, s>>>(L.slot_a, L.key_b, sb, L.n, L.seg_begin, L.vis_end, L.seg_end);
-    count_launches(4);
+    segment_bounds_kernel<<<blocks, 256, 0, s>>>(L.key_b, lbits, L.n, L.seg_begin, L.vis_end, L.seg_end);
+    count_launches(2);
     return cudaGetLastError();
 }
 
-cudaError_t launch_tie_gather_multi(const LaunchPlaceMulti &L, const int64_t *row_begin, const int32_t *slot_comp,
-                                    gf_table out, int32_t *row_slot, cudaStream_t s)
+cudaError_t launch_tie_place_multi(const LaunchPlaceMulti &L, const int64_t *row_begin, const int32_t *slot_comp,
+                                   gf_table out, int32_t *row_slot, cudaStream_t s)
 {
     if (L.n <= 0) return cudaSuccess;
     const int blocks = (int)std::min<int64_t>((L.n + 255) / 256, (int64_t)sm_count() * 16);
-    tie_multi_kernel<<<blocks, 256, 0, s>>>(L.key_b, L.slot_bits, sort_low_bit(L.slot_bits), L.idx_a, L.n, L.lb, L.DM,
-                                            L.absmag, L.Am, L.n);
-    GatherParams G;
-    G.idx = L.idx_a; G.n = L.n; G.src_pitch = L.n;
-    G.lb = L.lb; G.projIdx = L.projIdx; G.projXY = L.projXY; G.DM = L.DM; G.absmag = L.absmag;
-    G.XYZ = L.XYZ; G.Am = L.Am; G.AmInf = L.AmInf; G.comp = 0; G.out = out;
-    gather_multi_kernel<<<blocks, 256, 0, s>>>(G, L.slot_a, L.seg_begin, L.vis_end, row_begin, slot_comp, row_slot);
+    const int lbits = multi_key_bits(L.slot_bits) - L.slot_bits;
+    tie_multi_kernel<<<blocks, 256, 0, s>>>(L.key_b, lbits, L.idx_a, L.n, L.rec, L.jobs);
+    PlaceSortedParams S;
+    S.rec = L.rec; S.jobs = L.jobs; S.key = L.key_b; S.idx = L.idx_a; S.n = L.n; S.lbits = lbits;
+    S.seg_begin = L.seg_begin; S.vis_end = L.vis_end; S.row_begin = row_begin; S.slot_comp = slot_comp;
+    S.out = out; S.row_slot = row_slot;
+    place_sorted_multi_kernel<<<blocks, 256, 0, s>>>(S);
     count_launches(2);
     return cudaGetLastError();
 }
 
 cudaError_t sort_temp_bytes_multi(int64_t n, size_t *bytes)
 {
-    size_t a = 0, b = 0;
-    cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, a, (const uint64_t *)nullptr, (uint64_t *)nullptr,
-                                                    (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)n);
-    if (e != cudaSuccess) return e;
-    *bytes = a;
-    (void)b;
-    return e;
+    *bytes = 0;
+    return cub::DeviceRadixSort::SortPairs(nullptr, *bytes, (const uint64_t *)nullptr, (uint64_t *)nullptr,
+                                           (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)n);
 }
 
 }  // namespace gfk
