@@ -169,7 +169,8 @@ COLUMNS = [  # name, dtype, components (or "bands")
     ("absmagSys", np.float32, 2), ("absmagSysNcomp", np.int32, 1),
 ]
 PROFILE_PHASES = ["integrate", "draw_window", "draw_rerun", "place", "sort", "clipper", "fixedfeh", "bond2010",
-                  "photometry", "photoerrors", "vel2pm", "gal2other", "slot_density", "expand", "batch_draw"]
+                  "photometry", "photoerrors", "vel2pm", "gal2other", "slot_density", "expand", "batch_draw",
+                  "setup", "plain_requests"]
 SKYGEN_COLUMNS = ["lb", "projIdx", "projXY", "DM", "absmag", "XYZ", "comp", "Am", "AmInf", "hidden"]
 # column bits of gf_multi_set_host_columns (GF_COL_*): bit i is COLUMNS[i]
 COL = {name: 1 << i for i, (name, _, _) in enumerate(COLUMNS)}

@@ -1276,6 +1276,38 @@ gf_status gf_photoerr_create(gf_ctx *ctx, const gf_photoerr_config *cfg, gf_phot
     cudaMemcpy(p->d_sigma, cfg->sigma, 8 * n, cudaMemcpyHostToDevice);
     p->tab.nbands = cfg->nbands; p->tab.nknots = cfg->nknots; p->tab.mag = p->d_mag; p->tab.sigma = p->d_sigma;
     p->tab.seed = cfg->seed;
+    p->tab.guide = nullptr;
+    p->tab.nguide = 0;
+    /* bracket guide: one cell per knot over each band's knot range, when every band's
+     * knots are finite and strictly increasing */
+    const int nk = cfg->nknots;
+    bool mono = true;
+    for (int b = 0; b < cfg->nbands && mono; b++) {
+        const double *xa = cfg->mag + (size_t)b * nk;
+        for (int i = 0; i < nk && mono; i++) mono = std::isfinite(xa[i]) && (i == 0 || xa[i] > xa[i - 1]);
+    }
+    if (mono) {
+        const int G = nk;
+        std::vector<int32_t> guide((size_t)cfg->nbands * G);
+        for (int b = 0; b < cfg->nbands; b++) {
+            const double *xa = cfg->mag + (size_t)b * nk;
+            const double x0 = xa[0], inv = (double)G / (xa[nk - 1] - xa[0]);
+            p->tab.gx0[b] = x0;
+            p->tab.ginv[b] = inv;
+            int last = 0, i = 0;
+            for (int g = 0; g < G; g++) {
+                while (i <= nk - 2 && gfk::perr_cell(xa[i], x0, inv, G) < g) last = i++;
+                guide[(size_t)b * G + g] = last;
+            }
+        }
+        if (dev_alloc(&p->d_guide, guide.size()) != GF_OK) {
+            dev_free(p->d_mag); dev_free(p->d_sigma); delete p;
+            return fail(GF_E_OOM, "photometric error tables");
+        }
+        cudaMemcpy(p->d_guide, guide.data(), 4 * guide.size(), cudaMemcpyHostToDevice);
+        p->tab.guide = p->d_guide;
+        p->tab.nguide = G;
+    }
     *out = p;
     return GF_OK;
 }
@@ -1283,7 +1315,7 @@ gf_status gf_photoerr_create(gf_ctx *ctx, const gf_photoerr_config *cfg, gf_phot
 gf_status gf_photoerr_destroy(gf_photoerr *p)
 {
     if (!p) return GF_OK;
-    dev_free(p->d_mag); dev_free(p->d_sigma);
+    dev_free(p->d_mag); dev_free(p->d_sigma); dev_free(p->d_guide);
     delete p;
     return GF_OK;
 }

@@ -3,6 +3,7 @@
  * helpers shared by the C ABI files (gf_api.cu, gf_multi.cu).
  */
 #pragma once
+#include <chrono>
 #include <cuda_runtime.h>
 #include <string>
 #include <utility>
@@ -90,6 +91,7 @@ struct gf_photometry {
 struct gf_photoerr {
     gfk::PerrTables tab;
     double *d_mag = nullptr, *d_sigma = nullptr;
+    int32_t *d_guide = nullptr;
 };
 
 namespace gfa {
@@ -141,6 +143,21 @@ struct ProfScope {
         cudaEventRecord(b, c->stream);
         c->prof_pending.push_back({kind, {a, b}});
     }
+};
+
+/* host wall time of a phase, added to the context's profile when it is enabled */
+struct HostScope {
+    gf_ctx *c; int kind; bool on;
+    std::chrono::steady_clock::time_point t0;
+    HostScope(gf_ctx *c_, int k) : c(c_), kind(k), on(c_->prof), t0(std::chrono::steady_clock::now()) {}
+    void stop()
+    {
+        if (!on) return;
+        on = false;
+        c->prof_ms[kind] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        c->prof_n[kind] += 1;
+    }
+    ~HostScope() { stop(); }
 };
 
 }  // namespace gfa

@@ -60,6 +60,8 @@ __device__ __forceinline__ int first_block_start(long long k0)
 
 #define GF_PLAN_REMEMBER 8          /* distinct distances remembered per diagonal */
 
+constexpr int kIntegChunk = 8;      /* pixels per run a warp takes from the shared counter */
+
 /* distinct anchor distances of diagonal d, in order of first appearance; calls
  * emit(anchor ordinal, slot ordinal on the diagonal, D, local index, i, j) for every anchor */
 template <class F>
@@ -225,7 +227,24 @@ __device__ __forceinline__ void walk_diagonals(int lane, int nd, int x, int y, i
         int t = 0, seg_end = dg.y < tl ? dg.y : tl;
         for (;;) {
             const float2 q = Q[*ap++];
-            if (q.y >= 0.f) {
+            if (!COV && q.y >= 0.f && seg_end - t == GF_BLOCK) {
+                /* a whole block: its ten products are independent; the sums take them in
+                 * the order of the loop below (even bins to c0, odd bins to c1) */
+                float mv[GF_BLOCK];
+#pragma unroll
+                for (int u = 0; u < GF_BLOCK; u++) mv[u] = lf[-(t + u)] * q.x;
+#pragma unroll
+                for (int u = 0; u < GF_BLOCK; u++) mv[u] *= norm;
+#pragma unroll
+                for (int u = 0; u < GF_BLOCK; u++) mv[u] *= q.y;
+#pragma unroll
+                for (int u = 0; u < GF_BLOCK; u++) mv[u] *= K;
+#pragma unroll
+                for (int u = 0; u < GF_BLOCK; u += 2) {
+                    c0 += (double)mv[u];
+                    c1 += (double)mv[u + 1];
+                }
+            } else if (q.y >= 0.f) {
                 for (; t + 1 < seg_end; t += 2) {
                     float m0 = lf[-t] * q.x, m1 = lf[-(t + 1)] * q.x;
                     m0 *= norm;
@@ -272,7 +291,6 @@ __global__ void __launch_bounds__(256) integrate_pixels_kernel(IntegPixParams P)
     float *LFM = (float *)(mine + P.off_lf);
     float *MMr = (float *)(mine + P.off_mr);
     float2 *Q = (float2 *)(mine + P.off_q);
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
     int job = -1;
     const unsigned char *plan = nullptr;
     const int2 *diag = nullptr;
@@ -283,14 +301,33 @@ __global__ void __launch_bounds__(256) integrate_pixels_kernel(IntegPixParams P)
     SkyGeom g;
     g.ext_kind = GF_EXT_NONE;
     g.ammin = nullptr;
-    for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < P.total_pix; p += nwarps) {
+    /* runs of kIntegChunk consecutive pixels (mostly of one request) taken from a
+     * shared counter: the request's tables are set up once per run, not per pixel */
+    int p = 0, pend = 0, job_end = 0;
+    for (;;) {
+        if (p >= pend) {
+            unsigned u0 = 0;
+            if (lane == 0) u0 = atomicAdd(P.next, (unsigned)kIntegChunk);
+            u0 = __shfl_sync(0xffffffffu, u0, 0);
+            if (u0 >= (unsigned)P.total_pix) break;
+            p = (int)u0;
+            pend = p + kIntegChunk < P.total_pix ? p + kIntegChunk : P.total_pix;
+        } else {
+            p++;
+            if (p >= pend) continue;
+        }
         /* the request of flat pixel p: pix_off is increasing */
-        int lo = 0, hi = P.njobs;
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (P.pix_off[mid] <= p) lo = mid; else hi = mid;
+        int lo = job;
+        if (job < 0 || p < P.pix_off[job] || p >= job_end) {
+            lo = 0;
+            int hi = P.njobs;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (P.pix_off[mid] <= p) lo = mid; else hi = mid;
+            }
         }
         if (lo != job) {
+            job_end = P.pix_off[lo + 1];
             job = lo;
             plan = P.plans[job];
             if (plan) {
@@ -421,6 +458,7 @@ size_t integ_warp_bytes(int nm_max, int nM_max, int slots_max, IntegPixParams *P
 cudaError_t launch_integrate_pixels(const IntegPixParams &P, int model_type, double2 *tot, cudaStream_t s)
 {
     if (P.total_pix <= 0) return cudaSuccess;
+    if (!P.next) return cudaErrorInvalidValue;
     const size_t max_smem = 200 * 1024;
     int wpb = (int)std::min<size_t>(8, max_smem / (size_t)P.warp_bytes);
     if (wpb < 1) return cudaErrorInvalidValue;
@@ -439,8 +477,10 @@ cudaError_t launch_integrate_pixels(const IntegPixParams &P, int model_type, dou
     }
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
-    const long long need = ((long long)P.total_pix + wpb - 1) / wpb;
+    const long long need = ((long long)P.total_pix + wpb * kIntegChunk - 1) / (wpb * kIntegChunk);
     const int blocks = (int)std::min<long long>(need, (long long)sm_count() * per_sm);
+    e = cudaMemsetAsync(P.next, 0, sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
     if (model_type == GF_MODEL_EXP_DISK)
         integrate_pixels_kernel<GF_MODEL_EXP_DISK><<<blocks, threads, smem, s>>>(P);
     else

@@ -130,7 +130,21 @@ struct PerrTables {
     int32_t nbands, nknots;
     const double *mag, *sigma;    /* device */
     uint64_t seed;
+    /* Bracket guide of strictly increasing knots (null otherwise): the magnitude axis
+     * of band b is cut into nguide equal cells, cell(x) = floor((x - gx0[b]) * ginv[b])
+     * clamped to [0, nguide), and guide[b * nguide + g] is the last knot index
+     * (<= nknots - 2) whose own cell is before g, or 0.  A lookup starts there and
+     * steps forward to the bisection's bracket. */
+    const int32_t *guide;
+    int32_t nguide;
+    double gx0[GF_MAX_BANDS], ginv[GF_MAX_BANDS];
 };
+/* the cell of the bracket guide (host and device evaluate it alike) */
+__host__ __device__ inline int perr_cell(double x, double x0, double inv, int n)
+{
+    const double t = (x - x0) * inv;
+    return t < 0.0 ? 0 : (t >= (double)n ? n - 1 : (int)t);
+}
 cudaError_t launch_photoerrors(const PerrTables &c, int64_t row_offset, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
 cudaError_t launch_vel2pm(const gf_vel2pm_config &c, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
 cudaError_t launch_gal2other(int32_t coordsys, gf_table t, int64_t begin, int64_t end, cudaStream_t s);
@@ -172,6 +186,7 @@ struct IntegPixParams {
     int32_t njobs, total_pix;
     double2 *pix_sum;              /* [total_pix] (expected, expected covered) */
     int32_t off_lf, off_mr, off_q, warp_bytes;   /* per-warp shared-memory layout (integ_warp_bytes) */
+    uint32_t *next;                /* device counter of the pixel runs handed out (reset by the launch) */
 };
 size_t integ_plan_bytes(int nm, int nM, int *max_anchors, int *max_slots);
 cudaError_t launch_integ_plans(const IntegPlanDesc *desc_dev, int nplans, cudaStream_t s);

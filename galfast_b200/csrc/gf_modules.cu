@@ -588,12 +588,23 @@ __device__ __forceinline__ double error_normal(uint64_t seed, uint64_t row, uint
     return r * gfm::cos_d(6.283185307179586 * u2);
 }
 
-__device__ __forceinline__ double linear_eval(const double *xa, const double *ya, int n, double x)
+/* gsl_interp_linear at x: the bisection's bracket (the last knot <= x, within
+ * [0, n-2]), found from the guide cell when the knots are strictly increasing --
+ * the same bracket, since the guide never starts past it -- and by bisection
+ * otherwise (NaN takes the bisection's answer, n - 2). */
+__device__ __forceinline__ double linear_eval(const double *xa, const double *ya, int n, double x, const int32_t *guide,
+                                              int nguide, double gx0, double ginv)
 {
-    int ilo = 0, ihi = n - 1;
-    while (ihi > ilo + 1) {
-        int i = (ihi + ilo) / 2;
-        if (xa[i] > x) ihi = i; else ilo = i;
+    int ilo = 0;
+    if (guide && x == x) {
+        ilo = guide[perr_cell(x, gx0, ginv, nguide)];
+        while (ilo < n - 2 && xa[ilo + 1] <= x) ilo++;
+    } else {
+        int ihi = n - 1;
+        while (ihi > ilo + 1) {
+            int i = (ihi + ilo) / 2;
+            if (xa[i] > x) ihi = i; else ilo = i;
+        }
     }
     double x_lo = xa[ilo], x_hi = xa[ilo + 1];
     double y_lo = ya[ilo], y_hi = ya[ilo + 1];
@@ -609,7 +620,8 @@ __device__ __forceinline__ void photoerr_row(const PerrTables &c, uint64_t seed,
     if (t.hidden[row]) return;
     for (int b = 0; b < c.nbands; b++) {
         float mag = t.mags[b * P + row];
-        float sigma = (float)linear_eval(c.mag + (size_t)b * c.nknots, c.sigma + (size_t)b * c.nknots, c.nknots, mag);
+        float sigma = (float)linear_eval(c.mag + (size_t)b * c.nknots, c.sigma + (size_t)b * c.nknots, c.nknots, mag,
+                                         c.guide ? c.guide + (size_t)b * c.nguide : nullptr, c.nguide, c.gx0[b], c.ginv[b]);
         double z = error_normal(seed, (uint64_t)catalog_row, (uint32_t)b);
         t.obsmags[b * P + row] = mag + (float)((double)sigma * z);
     }

@@ -440,6 +440,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                     int64_t piece_rows, void *user, gf_catalog_stats *stats, gfa::Admission *adm)
 {
     GF_TRY(gfa::check_ctx(ctx));
+    gfa::HostScope setup_time(ctx, GF_PROF_SETUP);
     if (!jobs || njobs <= 0 || njobs > 32767) return fail(GF_E_INVALID, "njobs must be in [1, 32767]");
     const gf_job &J0 = jobs[0];
     const int N = J0.sky.nthreads;
@@ -699,6 +700,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         GF_TRY(ws.tot.need((size_t)njobs));
         GF_TRY(ws.plans.need((size_t)njobs));
     }
+    setup_time.stop();
     for (int i = 0; i < nmod && !integ.empty(); i++) {
         for (int j = 0; j < njobs; j++) hj[j] = crawl_job(j, i);
         GF_CUDA(cudaMemcpyAsync(d_jobs, hj.data(), sizeof(CrawlJob) * (size_t)njobs, cudaMemcpyHostToDevice, st));
@@ -757,6 +759,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
                 P.njobs = njobs;
                 P.total_pix = (int32_t)pix_total;
                 P.pix_sum = ws.pixsum.p;
+                P.next = d_counter;
                 {
                     ProfScope ps(ctx, GF_PROF_INTEGRATE);
                     GF_CUDA(gfk::launch_integrate_pixels(P, model_kind(R[integ[0]].hm[i].m.type), ws.tot.p, st));
@@ -1322,6 +1325,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         GF_CUDA(cudaStreamSynchronize(ws.copy_stream));
         if (hd.stop) return fail(GF_E_STATE, "stopped by the host callback");
     }
+    gfa::ProfScope plain_time(ctx, GF_PROF_PLAIN);
     for (int j = 0; j < njobs; j++) {
         if (!R[j].plain || R[j].deferred) continue;
         if (to_host) {

@@ -363,7 +363,11 @@ enum {
     GF_PROF_SLOTS = 12,          /* batched draw: model density at the slot distances of each pixel */
     GF_PROF_EXPAND = 13,         /* batched draw: star records of the bins with stars */
     GF_PROF_BATCH_DRAW = 14,     /* batched draw: the Poisson draw of every stream (one launch per model pass) */
-    GF_PROF_NPHASES = 15
+    GF_PROF_SETUP = 15,          /* many-request calls: host wall time from the call to the integrate pass (checks,
+                                    model set-up, staging and upload of the pencil beams, stream seeding) */
+    GF_PROF_PLAIN = 16,          /* many-request calls: device time of the requests run through the plain path
+                                    inside the call (their own phases are counted as well) */
+    GF_PROF_NPHASES = 17
 };
 gf_status gf_profile_enable(gf_ctx *ctx, int32_t on);
 gf_status gf_profile_read(gf_ctx *ctx, double *ms, int64_t *launches);
