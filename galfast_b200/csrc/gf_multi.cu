@@ -672,7 +672,6 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
 
     /* ---- integrate every model of every request (os_skygen.cpp:875-880) ---- */
     std::vector<CrawlJob> hj(njobs);
-    std::vector<double> hc(2 * nall);
     std::vector<int> integ;
     for (int j : order_all)
         if (!R[j].plain) integ.push_back(j);
@@ -794,7 +793,8 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
             GF_TRY(ws.h_stage.need(16 * nall));
             GF_CUDA(cudaMemcpyAsync(ws.h_stage.p, d_counts, 16 * nall, cudaMemcpyDeviceToHost, st));
             GF_CUDA(cudaStreamSynchronize(st));
-            memcpy(hc.data(), ws.h_stage.p, 16 * nall);
+            /* the per-stream sums, read in place from the page-locked staging area */
+            const double *hc = (const double *)ws.h_stage.p;
             for (int j : integ) {
                 double e = 0, ec = 0;
                 for (int t = 0; t < N; t++) {
