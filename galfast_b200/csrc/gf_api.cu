@@ -1463,6 +1463,24 @@ gf_status gf_catalog_run(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, v
     return st;
 }
 
+}  /* extern "C" */
+
+namespace gfa {
+gf_status catalog_run_in_multi(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, void *user, gf_catalog_stats *stats)
+{
+    CountingBatch c = {cb, user, 0};
+    gf_status st = catalog_run_once(ctx, job, counting_batch, &c, stats);
+    if (st == GF_E_OOM && c.calls == 0 && job && job->nstreams > 0) {
+        cudaStreamSynchronize(ctx->stream);
+        gf_table_free(ctx, &ctx->plain_table);
+        st = catalog_run_once(ctx, job, counting_batch, &c, stats);
+    }
+    return st;
+}
+}  // namespace gfa
+
+extern "C" {
+
 gf_status gf_debug_fail_allocations(int64_t after, int64_t count)
 {
     if (count < 0) return fail(GF_E_INVALID, "negative failure count");

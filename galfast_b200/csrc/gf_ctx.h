@@ -118,6 +118,10 @@ gf_status zero_module_rows(gf_ctx *ctx, const gf_table *t, int64_t n);
 void free_multi_ws(gf_ctx *ctx);
 /* free the buffers a context keeps between calls (output table, multi-request workspace) */
 void release_caches(gf_ctx *ctx);
+/* gf_catalog_run for a request run inside a multi-request call: an out-of-memory
+ * failure before its first batch frees only the plain path's output table before the
+ * retry, so the multi-request workspace the caller is using stays in place */
+gf_status catalog_run_in_multi(gf_ctx *ctx, const gf_job *job, gf_batch_callback cb, void *user, gf_catalog_stats *stats);
 /* multipliers and jump tables of all 65536 streams on the context's device */
 gf_status ensure_multipliers(gf_ctx *ctx);
 

@@ -323,14 +323,17 @@ gf_table carve_table(char *p, int64_t cap, int nb, uint32_t mask)
 
 size_t carved_bytes(int64_t cap, int nb, uint32_t mask) { return row_bytes(nb, mask) * (size_t)cap + 23 * 256; }
 
-/* rows [r0, r1) of the device table d into the host table h, on stream cs */
-gf_status copy_rows_async(const gf_table &d, int64_t r0, int64_t r1, gf_table &h, cudaStream_t cs)
+/* rows [r0, r1) of the device table d into the table h (host memory, or device
+ * memory with kind = cudaMemcpyDeviceToDevice) at its row 0, on stream cs; the
+ * columns that either table lacks are not copied */
+gf_status copy_rows_async(const gf_table &d, int64_t r0, int64_t r1, gf_table &h, cudaStream_t cs,
+                          cudaMemcpyKind kind = cudaMemcpyDeviceToHost)
 {
     const size_t n = (size_t)(r1 - r0), P = (size_t)d.capacity, H = (size_t)h.capacity;
     auto cp = [&](void *hp, const void *dp, size_t elem, int ncomp) -> gf_status {
         if (!hp || !dp || n == 0 || ncomp <= 0) return GF_OK;
         GF_CUDA(cudaMemcpy2DAsync(hp, H * elem, (const char *)dp + (size_t)r0 * elem, P * elem, n * elem, (size_t)ncomp,
-                                  cudaMemcpyDeviceToHost, cs));
+                                  kind, cs));
         return GF_OK;
     };
     GF_TRY(cp(h.lb, d.lb, 8, 2)); GF_TRY(cp(h.projIdx, d.projIdx, 4, 1)); GF_TRY(cp(h.projXY, d.projXY, 4, 2));
@@ -345,6 +348,20 @@ gf_status copy_rows_async(const gf_table &d, int64_t r0, int64_t r1, gf_table &h
     return GF_OK;
 }
 
+/* the columns of t in mask (GF_COL_*); the others NULL */
+gf_table masked_view(const gf_table &t, uint32_t mask)
+{
+    gf_table v = t;
+    auto keep = [&](auto *&p, uint32_t col) { if (!(mask & col)) p = nullptr; };
+    keep(v.lb, GF_COL_LB); keep(v.projIdx, GF_COL_PROJIDX); keep(v.projXY, GF_COL_PROJXY); keep(v.DM, GF_COL_DM);
+    keep(v.absmag, GF_COL_ABSMAG); keep(v.XYZ, GF_COL_XYZ); keep(v.comp, GF_COL_COMP); keep(v.Am, GF_COL_AM);
+    keep(v.AmInf, GF_COL_AMINF); keep(v.hidden, GF_COL_HIDDEN); keep(v.FeH, GF_COL_FEH); keep(v.vcyl, GF_COL_VCYL);
+    keep(v.mags, GF_COL_MAGS); keep(v.photoflags, GF_COL_PHOTOFLAGS); keep(v.obsmags, GF_COL_OBSMAGS);
+    keep(v.pm, GF_COL_PM); keep(v.radec, GF_COL_RADEC); keep(v.FeH_comp, GF_COL_FEHCOMP);
+    keep(v.absmagSys, GF_COL_ABSMAGSYS); keep(v.absmagSysNcomp, GF_COL_SYSNCOMP);
+    return v;
+}
+
 /* one delivered piece: run by the copy stream after its rows have arrived */
 struct Piece {
     gf_multi_host_callback cb;
@@ -352,14 +369,14 @@ struct Piece {
     int32_t model;
     gf_table host;
     std::vector<int64_t> begin, count;
-    int *stop;
+    std::atomic<int> *stop;
 };
 
 void CUDART_CB deliver_piece(void *arg)
 {
     Piece *p = (Piece *)arg;
-    if (*p->stop || !p->cb) return;
-    if (p->cb(p->user, p->model, &p->host, p->begin.data(), p->count.data()) != 0) *p->stop = 1;
+    if (p->stop->load() || !p->cb) return;
+    if (p->cb(p->user, p->model, &p->host, p->begin.data(), p->count.data()) != 0) p->stop->store(1);
 }
 
 struct HostDelivery {
@@ -369,7 +386,7 @@ struct HostDelivery {
     int nbands = 0;
     int64_t next = 0;                    /* pieces enqueued */
     std::deque<Piece> pieces;
-    int stop = 0;
+    std::atomic<int> stop{0};
     gf_table ring[GF_RING];
 };
 
@@ -409,30 +426,58 @@ gf_status deliver_pass(MultiWS &ws, HostDelivery &hd, int b, cudaStream_t st, co
 
 struct PlainHostForward {
     HostDelivery *hd;
+    MultiWS *ws;
+    int *pass;                         /* model passes delivered so far (selects the staging table) */
     gf_ctx *ctx;
     int32_t njobs, job;
+    int64_t capacity;                  /* the request's batch capacity */
     std::vector<int32_t> skip;         /* components already delivered by batched passes */
+    gf_status err = GF_OK;             /* a failure inside the callback, and its message */
+    std::string msg;
 };
 
-/* a plain-path batch of a request run inside the multi call, delivered to the host
- * through the ring on the calling thread */
+/* A plain-path batch of a request run inside the multi call.  Its delivered
+ * columns are staged on the device, in the batched passes' alternating output
+ * tables, and leave through the copy stream behind the batched passes' rows, so
+ * the plain path generates its next batch while the copies drain. */
 int forward_plain_host(void *u, int32_t model, const gf_table *dev, int64_t row_offset)
 {
     (void)row_offset;
     PlainHostForward *f = (PlainHostForward *)u;
     HostDelivery &hd = *f->hd;
-    if (skipped(f->skip, model)) return 0;
-    for (int64_t r0 = 0; r0 < dev->size; r0 += hd.piece_rows) {
-        const int64_t r1 = std::min(dev->size, r0 + hd.piece_rows);
-        gf_table h = hd.ring[0];
-        if (copy_rows_async(*dev, r0, r1, h, f->ctx->stream) != GF_OK) return 1;
-        if (cudaStreamSynchronize(f->ctx->stream) != cudaSuccess) return 1;
-        h.size = r1 - r0;
-        h.nbands = dev->nbands;
-        std::vector<int64_t> b(f->njobs, 0), c(f->njobs, 0);
-        c[f->job] = r1 - r0;
-        if (hd.cb && hd.cb(hd.user, model, &h, b.data(), c.data()) != 0) return 1;
+    MultiWS &ws = *f->ws;
+    auto failed = [&](gf_status e, const char *what) {
+        f->err = e;
+        f->msg = std::string(what) + ": " + gf_last_error();
+        return 1;
+    };
+    if (hd.stop.load()) return 1;
+    if (skipped(f->skip, model) || dev->size <= 0) return 0;
+    cudaStream_t st = f->ctx->stream;
+    const int b = *f->pass & 1;
+    gf_table &T = b ? ws.out2 : ws.out;
+    /* the staging table's previous rows have been copied out */
+    cudaError_t ce = ws.free_recorded[b] ? cudaStreamWaitEvent(st, ws.ev_free[b], 0) : cudaSuccess;
+    if (ce == cudaSuccess && (T.capacity < dev->size || T.nbands < dev->nbands)) {
+        ce = cudaStreamSynchronize(ws.copy_stream);
+        if (ce == cudaSuccess) {
+            gf_table_free(f->ctx, &T);
+            const gf_status as = gf_table_alloc(f->ctx, std::max(dev->size, f->capacity), dev->nbands, &T);
+            if (as != GF_OK) return failed(as, "staging table");
+        }
     }
+    if (ce != cudaSuccess) return failed(GF_E_CUDA, cudaGetErrorString(ce));
+    gf_table V = masked_view(T, f->ctx->host_cols);
+    V.nbands = dev->nbands;
+    gf_status cs = copy_rows_async(*dev, 0, dev->size, V, st, cudaMemcpyDeviceToDevice);
+    if (cs != GF_OK) return failed(cs, "staging copy");
+    V.size = dev->size;
+    V.systems = dev->systems;
+    const std::vector<int> slot_job(1, f->job);
+    const std::vector<int64_t> row_begin = {0, dev->size}, rows(1, dev->size);
+    cs = deliver_pass(ws, hd, b, st, V, model, slot_job, row_begin, rows, f->njobs);
+    if (cs != GF_OK) return failed(cs, "host delivery");
+    (*f->pass)++;
     return 0;
 }
 
@@ -1304,7 +1349,7 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
             }
             if (to_host) {
                 GF_TRY(deliver_pass(ws, hd, ob, st, out, R[batched[0]].hm[i].m.comp, slot_job, row_begin, slot_rows, njobs));
-                if (hd.stop) return fail(GF_E_STATE, "stopped by the host callback");
+                if (hd.stop.load()) return fail(GF_E_STATE, "stopped by the host callback");
             } else {
                 GF_CUDA(cudaStreamSynchronize(st));
                 if (cb) {
@@ -1319,28 +1364,35 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
         }
     }
 
-    /* ---- requests that need the batch rules of the plain path ---- */
-    if (to_host) {
-        /* deliveries stay in order: the batched passes first */
-        GF_CUDA(cudaStreamSynchronize(ws.copy_stream));
-        if (hd.stop) return fail(GF_E_STATE, "stopped by the host callback");
-    }
-    gfa::ProfScope plain_time(ctx, GF_PROF_PLAIN);
-    for (int j = 0; j < njobs; j++) {
-        if (!R[j].plain || R[j].deferred) continue;
-        if (to_host) {
-            PlainHostForward f;
-            f.hd = &hd; f.ctx = ctx; f.njobs = njobs; f.job = j;
-            f.skip = R[j].delivered;
-            GF_TRY(gf_catalog_run(ctx, &jobs[j], forward_plain_host, &f, &S[j]));
-        } else {
-            PlainForward f;
-            f.cb = cb; f.user = user; f.njobs = njobs; f.job = j;
-            f.skip = R[j].delivered;
-            f.begin.assign(njobs, 0);
-            f.count.assign(njobs, 0);
-            GF_TRY(gf_catalog_run(ctx, &jobs[j], forward_plain_batch, &f, &S[j]));
+    /* ---- requests that need the batch rules of the plain path ----
+     * With host delivery their rows follow the batched passes' rows through the copy
+     * stream (deliveries stay in order) while the device generates them. */
+    {
+        gfa::ProfScope plain_time(ctx, GF_PROF_PLAIN);
+        for (int j = 0; j < njobs; j++) {
+            if (!R[j].plain || R[j].deferred) continue;
+            if (to_host) {
+                if (hd.stop.load()) break;
+                PlainHostForward f;
+                f.hd = &hd; f.ws = &ws; f.pass = &pass; f.ctx = ctx; f.njobs = njobs; f.job = j;
+                f.capacity = jobs[j].capacity;
+                f.skip = R[j].delivered;
+                const gf_status rs = gfa::catalog_run_in_multi(ctx, &jobs[j], forward_plain_host, &f, &S[j]);
+                if (f.err != GF_OK) return fail(f.err, f.msg);
+                if (rs != GF_OK && !hd.stop.load()) return rs;
+            } else {
+                PlainForward f;
+                f.cb = cb; f.user = user; f.njobs = njobs; f.job = j;
+                f.skip = R[j].delivered;
+                f.begin.assign(njobs, 0);
+                f.count.assign(njobs, 0);
+                GF_TRY(gfa::catalog_run_in_multi(ctx, &jobs[j], forward_plain_batch, &f, &S[j]));
+            }
         }
+    }
+    if (to_host) {
+        GF_CUDA(cudaStreamSynchronize(ws.copy_stream));
+        if (hd.stop.load()) return fail(GF_E_STATE, "stopped by the host callback");
     }
     return GF_OK;
 }

@@ -587,9 +587,12 @@ gf_status gf_multi_set_memory_budget(gf_ctx *ctx, int64_t bytes);
  * host rows row_begin[j] .. row_begin[j] + row_count[j] - 1 (count 0: none in
  * this piece); a request's rows of a model arrive in order, possibly over several
  * pieces.  The host table is valid until cb returns.  cb runs on a CUDA driver
- * thread (or, for requests that need several output batches, on the calling
- * thread) and must not call CUDA or this library; a nonzero return stops the run
- * (GF_E_STATE).  All callbacks have returned when this function returns. */
+ * thread, one piece at a time in delivery order, and must not call CUDA or this
+ * library; a nonzero return stops the run (GF_E_STATE) and no later piece reaches
+ * cb.  Requests that need several output batches run through the plain path after
+ * the batched passes; their batches are staged on the device and follow the
+ * batched rows through the same copy stream.  All callbacks have returned when
+ * this function returns. */
 typedef int (*gf_multi_host_callback)(void *user, int32_t model, const gf_table *host, const int64_t *row_begin,
                                       const int64_t *row_count);
 gf_status gf_catalog_run_multi_host(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, int64_t piece_rows,

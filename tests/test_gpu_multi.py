@@ -169,6 +169,41 @@ def test_host_delivery_equals_device_rows(lib):
     ctx.close()
 
 
+def test_host_delivery_stops_when_the_callback_asks(lib):
+    """A nonzero return of the host callback ends gf_catalog_run_multi_host with
+    GF_E_STATE, whether it comes during the batched passes' rows or during the rows
+    of the request that takes the plain path (whose batches follow the batched
+    rows through the same copy stream); no piece reaches the callback after it,
+    and the context runs the next call as before."""
+    ws = requests(lib, n=5)
+    ctx = G.Context(0)
+    ref = {}
+
+    def sink(j, model, rows):
+        ref.setdefault((j, model), []).append(rows)
+    G.run_catalog_multi_host(ctx, ws, sink, piece_rows=1000)
+    for stop_job in (0, 1):                     # request 1 takes the plain path
+        seen = []
+
+        def stopper(j, model, rows):
+            seen.append(j)
+            return j == stop_job
+        with pytest.raises(G.GalfastError, match="stopped"):
+            G.run_catalog_multi_host(ctx, ws, stopper, piece_rows=1000)
+        assert seen and seen[-1] == stop_job and seen.count(stop_job) == 1
+    got = {}
+
+    def again(j, model, rows):
+        got.setdefault((j, model), []).append(rows)
+    G.run_catalog_multi_host(ctx, ws, again, piece_rows=1000)
+    assert sorted(got) == sorted(ref)
+    for k in ref:
+        for a, b in zip(ref[k], got[k]):
+            for c in a:
+                np.testing.assert_array_equal(a[c], b[c], err_msg="%s %s" % (c, k))
+    ctx.close()
+
+
 def test_request_that_fills_a_batch_runs_alone(lib):
     """Admission lets every request into the batched passes (margin -1000 sigma);
     the first request's halo stars (about 2850) then fill its 2000-row batch while
