@@ -227,12 +227,17 @@ __device__ __forceinline__ void walk_diagonals(int lane, int nd, int x, int y, i
         int t = 0, seg_end = dg.y < tl ? dg.y : tl;
         for (;;) {
             const float2 q = Q[*ap++];
-            if (!COV && q.y >= 0.f && seg_end - t == GF_BLOCK) {
-                /* a whole block: its ten products are independent; the sums take them in
-                 * the order of the loop below (even bins to c0, odd bins to c1) */
+            if (q.y >= 0.f) {
+                /* One code path for whole and partial segments (no divergence between
+                 * lanes whose segments differ in length): bins u >= len read no LF and
+                 * add an exact +0.0, so the sums take the segment's bins in the order
+                 * of the plain loop (even offsets to c0, odd ones to c1). */
+                const int len = seg_end - t;
                 float mv[GF_BLOCK];
 #pragma unroll
-                for (int u = 0; u < GF_BLOCK; u++) mv[u] = lf[-(t + u)] * q.x;
+                for (int u = 0; u < GF_BLOCK; u++) mv[u] = u < len ? lf[-(t + u)] : 0.f;
+#pragma unroll
+                for (int u = 0; u < GF_BLOCK; u++) mv[u] *= q.x;
 #pragma unroll
                 for (int u = 0; u < GF_BLOCK; u++) mv[u] *= norm;
 #pragma unroll
@@ -240,33 +245,15 @@ __device__ __forceinline__ void walk_diagonals(int lane, int nd, int x, int y, i
 #pragma unroll
                 for (int u = 0; u < GF_BLOCK; u++) mv[u] *= K;
 #pragma unroll
+                for (int u = 0; u < GF_BLOCK; u++) mv[u] = u < len ? mv[u] : 0.f;    /* 0 * inf would be NaN */
+#pragma unroll
                 for (int u = 0; u < GF_BLOCK; u += 2) {
                     c0 += (double)mv[u];
                     c1 += (double)mv[u + 1];
-                }
-            } else if (q.y >= 0.f) {
-                for (; t + 1 < seg_end; t += 2) {
-                    float m0 = lf[-t] * q.x, m1 = lf[-(t + 1)] * q.x;
-                    m0 *= norm;
-                    m1 *= norm;
-                    m0 *= q.y;
-                    m1 *= q.y;
-                    m0 *= K;
-                    m1 *= K;
-                    c0 += (double)m0;
-                    c1 += (double)m1;
                     if (COV) {
-                        v0 += (double)(m0 * cf);
-                        v1 += (double)(m1 * cf);
+                        v0 += (double)(mv[u] * cf);
+                        v1 += (double)(mv[u + 1] * cf);
                     }
-                }
-                if (t < seg_end) {
-                    float m0 = lf[-t] * q.x;
-                    m0 *= norm;
-                    m0 *= q.y;
-                    m0 *= K;
-                    c0 += (double)m0;
-                    if (COV) v0 += (double)(m0 * cf);
                 }
             }
             t = seg_end;
