@@ -222,6 +222,11 @@ struct MultiWS {
     cudaEvent_t ev_pass[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
     bool free_recorded[2] = {false, false};
     HostGrow<char> ring;
+    /* host delivery of plain-path batches: two device staging tables of the delivered
+     * columns only, each free again once its copy-stream event has passed */
+    Grow<char> stage;
+    cudaEvent_t ev_stage[2] = {nullptr, nullptr}, ev_stage_free[2] = {nullptr, nullptr};
+    bool stage_recorded[2] = {false, false};
     MultiWS()
     {
         memset(&out, 0, sizeof(out));
@@ -233,6 +238,8 @@ struct MultiWS {
         for (int b = 0; b < 2; b++) {
             if (ev_pass[b]) cudaEventDestroy(ev_pass[b]);
             if (ev_free[b]) cudaEventDestroy(ev_free[b]);
+            if (ev_stage[b]) cudaEventDestroy(ev_stage[b]);
+            if (ev_stage_free[b]) cudaEventDestroy(ev_stage_free[b]);
         }
         if (copy_stream) cudaStreamDestroy(copy_stream);
     }
@@ -348,20 +355,6 @@ gf_status copy_rows_async(const gf_table &d, int64_t r0, int64_t r1, gf_table &h
     return GF_OK;
 }
 
-/* the columns of t in mask (GF_COL_*); the others NULL */
-gf_table masked_view(const gf_table &t, uint32_t mask)
-{
-    gf_table v = t;
-    auto keep = [&](auto *&p, uint32_t col) { if (!(mask & col)) p = nullptr; };
-    keep(v.lb, GF_COL_LB); keep(v.projIdx, GF_COL_PROJIDX); keep(v.projXY, GF_COL_PROJXY); keep(v.DM, GF_COL_DM);
-    keep(v.absmag, GF_COL_ABSMAG); keep(v.XYZ, GF_COL_XYZ); keep(v.comp, GF_COL_COMP); keep(v.Am, GF_COL_AM);
-    keep(v.AmInf, GF_COL_AMINF); keep(v.hidden, GF_COL_HIDDEN); keep(v.FeH, GF_COL_FEH); keep(v.vcyl, GF_COL_VCYL);
-    keep(v.mags, GF_COL_MAGS); keep(v.photoflags, GF_COL_PHOTOFLAGS); keep(v.obsmags, GF_COL_OBSMAGS);
-    keep(v.pm, GF_COL_PM); keep(v.radec, GF_COL_RADEC); keep(v.FeH_comp, GF_COL_FEHCOMP);
-    keep(v.absmagSys, GF_COL_ABSMAGSYS); keep(v.absmagSysNcomp, GF_COL_SYSNCOMP);
-    return v;
-}
-
 /* one delivered piece: run by the copy stream after its rows have arrived */
 struct Piece {
     gf_multi_host_callback cb;
@@ -392,13 +385,13 @@ struct HostDelivery {
 
 /* Enqueue the delivery of rows [0, total) of the device table d, whose slot s holds
  * request slot_job[s] at rows [row_begin[s], row_begin[s] + rows[s]). */
-gf_status deliver_pass(MultiWS &ws, HostDelivery &hd, int b, cudaStream_t st, const gf_table &d, int32_t model,
-                       const std::vector<int> &slot_job, const std::vector<int64_t> &row_begin,
-                       const std::vector<int64_t> &rows, int njobs)
+gf_status deliver_rows(MultiWS &ws, HostDelivery &hd, cudaEvent_t ev_ready, cudaEvent_t ev_done, cudaStream_t st,
+                       const gf_table &d, int32_t model, const std::vector<int> &slot_job,
+                       const std::vector<int64_t> &row_begin, const std::vector<int64_t> &rows, int njobs)
 {
     cudaStream_t cs = ws.copy_stream;
-    GF_CUDA(cudaEventRecord(ws.ev_pass[b], st));
-    GF_CUDA(cudaStreamWaitEvent(cs, ws.ev_pass[b], 0));
+    GF_CUDA(cudaEventRecord(ev_ready, st));
+    GF_CUDA(cudaStreamWaitEvent(cs, ev_ready, 0));
     const int64_t total = row_begin[slot_job.size()];
     for (int64_t r0 = 0; r0 < total; r0 += hd.piece_rows) {
         const int64_t r1 = std::min(total, r0 + hd.piece_rows);
@@ -419,7 +412,15 @@ gf_status deliver_pass(MultiWS &ws, HostDelivery &hd, int b, cudaStream_t st, co
         }
         GF_CUDA(cudaLaunchHostFunc(cs, deliver_piece, &p));
     }
-    GF_CUDA(cudaEventRecord(ws.ev_free[b], cs));
+    GF_CUDA(cudaEventRecord(ev_done, cs));
+    return GF_OK;
+}
+
+gf_status deliver_pass(MultiWS &ws, HostDelivery &hd, int b, cudaStream_t st, const gf_table &d, int32_t model,
+                       const std::vector<int> &slot_job, const std::vector<int64_t> &row_begin,
+                       const std::vector<int64_t> &rows, int njobs)
+{
+    GF_TRY(deliver_rows(ws, hd, ws.ev_pass[b], ws.ev_free[b], st, d, model, slot_job, row_begin, rows, njobs));
     ws.free_recorded[b] = true;
     return GF_OK;
 }
@@ -437,9 +438,10 @@ struct PlainHostForward {
 };
 
 /* A plain-path batch of a request run inside the multi call.  Its delivered
- * columns are staged on the device, in the batched passes' alternating output
- * tables, and leave through the copy stream behind the batched passes' rows, so
- * the plain path generates its next batch while the copies drain. */
+ * columns are staged on the device, in two alternating staging tables of their
+ * own, and leave through the copy stream behind the batched passes' rows, so the
+ * plain path generates its next batch while the copies drain; it waits only for
+ * the copy of the batch before last. */
 int forward_plain_host(void *u, int32_t model, const gf_table *dev, int64_t row_offset)
 {
     (void)row_offset;
@@ -455,28 +457,33 @@ int forward_plain_host(void *u, int32_t model, const gf_table *dev, int64_t row_
     if (skipped(f->skip, model) || dev->size <= 0) return 0;
     cudaStream_t st = f->ctx->stream;
     const int b = *f->pass & 1;
-    gf_table &T = b ? ws.out2 : ws.out;
-    /* the staging table's previous rows have been copied out */
-    cudaError_t ce = ws.free_recorded[b] ? cudaStreamWaitEvent(st, ws.ev_free[b], 0) : cudaSuccess;
-    if (ce == cudaSuccess && (T.capacity < dev->size || T.nbands < dev->nbands)) {
-        ce = cudaStreamSynchronize(ws.copy_stream);
+    /* staging table b: the delivered columns of up to `capacity` rows */
+    const int64_t cap = std::max(dev->size, f->capacity);
+    const size_t bytes = (carved_bytes(cap, dev->nbands, f->ctx->host_cols) + 255) & ~(size_t)255;
+    cudaError_t ce = cudaSuccess;
+    if (ws.stage.n < 2 * bytes) {
+        ce = cudaStreamSynchronize(ws.copy_stream);            /* nothing reads the old staging tables */
         if (ce == cudaSuccess) {
-            gf_table_free(f->ctx, &T);
-            const gf_status as = gf_table_alloc(f->ctx, std::max(dev->size, f->capacity), dev->nbands, &T);
-            if (as != GF_OK) return failed(as, "staging table");
+            const gf_status as = ws.stage.need(2 * bytes);
+            if (as != GF_OK) return failed(as, "staging tables");
+            ws.stage_recorded[0] = ws.stage_recorded[1] = false;
         }
     }
+    /* its previous rows have been copied out */
+    if (ce == cudaSuccess && ws.stage_recorded[b]) ce = cudaStreamWaitEvent(st, ws.ev_stage_free[b], 0);
     if (ce != cudaSuccess) return failed(GF_E_CUDA, cudaGetErrorString(ce));
-    gf_table V = masked_view(T, f->ctx->host_cols);
-    V.nbands = dev->nbands;
+    /* each half of the staging buffer holds at least `bytes`, the carving of cap rows */
+    const size_t half = (ws.stage.n / 2) & ~(size_t)255;
+    gf_table V = carve_table(ws.stage.p + (size_t)b * half, cap, dev->nbands, f->ctx->host_cols);
     gf_status cs = copy_rows_async(*dev, 0, dev->size, V, st, cudaMemcpyDeviceToDevice);
     if (cs != GF_OK) return failed(cs, "staging copy");
     V.size = dev->size;
     V.systems = dev->systems;
     const std::vector<int> slot_job(1, f->job);
     const std::vector<int64_t> row_begin = {0, dev->size}, rows(1, dev->size);
-    cs = deliver_pass(ws, hd, b, st, V, model, slot_job, row_begin, rows, f->njobs);
+    cs = deliver_rows(ws, hd, ws.ev_stage[b], ws.ev_stage_free[b], st, V, model, slot_job, row_begin, rows, f->njobs);
     if (cs != GF_OK) return failed(cs, "host delivery");
+    ws.stage_recorded[b] = true;
     (*f->pass)++;
     return 0;
 }
@@ -983,9 +990,12 @@ gf_status run_multi(gf_ctx *ctx, const gf_job *jobs, int32_t njobs, gf_multi_cal
             for (int b = 0; b < 2; b++) {
                 GF_CUDA(cudaEventCreateWithFlags(&ws.ev_pass[b], cudaEventDisableTiming));
                 GF_CUDA(cudaEventCreateWithFlags(&ws.ev_free[b], cudaEventDisableTiming));
+                GF_CUDA(cudaEventCreateWithFlags(&ws.ev_stage[b], cudaEventDisableTiming));
+                GF_CUDA(cudaEventCreateWithFlags(&ws.ev_stage_free[b], cudaEventDisableTiming));
             }
         }
         ws.free_recorded[0] = ws.free_recorded[1] = false;
+        ws.stage_recorded[0] = ws.stage_recorded[1] = false;
         hd.cb = hcb;
         hd.user = user;
         hd.piece_rows = piece_rows > 0 ? piece_rows : (int64_t)16 << 20;
