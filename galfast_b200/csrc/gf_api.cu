@@ -38,6 +38,7 @@ void release_caches(gf_ctx *ctx)
     cudaStreamSynchronize(ctx->stream);
     gf_table_free(ctx, &ctx->plain_table);
     free_multi_ws(ctx);
+    free_rec_cache(ctx);
 }
 
 cudaError_t device_malloc(void **p, size_t bytes)
@@ -185,9 +186,76 @@ gf_status alloc_crawl_state(int n, CrawlState &st, void **mem)
     return GF_OK;
 }
 
+/* The record and placement buffers of a finished generator, kept by its context:
+ * every gf_catalog_run creates a generator, and allocating and freeing these
+ * gigabytes per request costs device synchronisations and, now and then, much more. */
+/* move the buffer set of src (a generator or a cached set) to dst */
+template <class A, class B>
+void move_recs(A &dst, B &src)
+{
+    dst.d_rec = src.d_rec; dst.d_rec2 = src.d_rec2; dst.d_rec_am = src.d_rec_am; dst.d_rec_am2 = src.d_rec_am2;
+    dst.d_lb = src.d_lb; dst.d_projIdx = src.d_projIdx; dst.d_hidden = src.d_hidden; dst.d_projXY = src.d_projXY;
+    dst.d_DM = src.d_DM; dst.d_absmag = src.d_absmag; dst.d_XYZ = src.d_XYZ; dst.d_Am = src.d_Am; dst.d_AmInf = src.d_AmInf;
+    dst.d_key = src.d_key; dst.d_key2 = src.d_key2; dst.d_idx = src.d_idx; dst.d_idx2 = src.d_idx2;
+    dst.d_sort_temp = src.d_sort_temp; dst.sort_temp_bytes = src.sort_temp_bytes; dst.rec_cap = src.rec_cap;
+    src.d_rec = src.d_rec2 = nullptr; src.d_rec_am = src.d_rec_am2 = nullptr; src.d_lb = nullptr;
+    src.d_projIdx = src.d_hidden = nullptr; src.d_projXY = src.d_DM = src.d_absmag = src.d_XYZ = src.d_Am = src.d_AmInf = nullptr;
+    src.d_key = src.d_key2 = nullptr; src.d_idx = src.d_idx2 = nullptr; src.d_sort_temp = nullptr;
+    src.sort_temp_bytes = 0; src.rec_cap = 0;
+}
+
+/* a cached buffer set, with the generator's field names */
+struct RecView {
+    StarRecord *d_rec = nullptr, *d_rec2 = nullptr;
+    float *d_rec_am = nullptr, *d_rec_am2 = nullptr;
+    double *d_lb = nullptr;
+    int32_t *d_projIdx = nullptr, *d_hidden = nullptr;
+    float *d_projXY = nullptr, *d_DM = nullptr, *d_absmag = nullptr, *d_XYZ = nullptr, *d_Am = nullptr, *d_AmInf = nullptr;
+    uint64_t *d_key = nullptr, *d_key2 = nullptr;
+    uint32_t *d_idx = nullptr, *d_idx2 = nullptr;
+    void *d_sort_temp = nullptr;
+    size_t sort_temp_bytes = 0;
+    int64_t rec_cap = 0;
+};
+
+void free_recs(RecView &v)
+{
+    dev_free(v.d_rec); dev_free(v.d_rec2); dev_free(v.d_rec_am); dev_free(v.d_rec_am2);
+    dev_free(v.d_lb); dev_free(v.d_projIdx); dev_free(v.d_hidden);
+    dev_free(v.d_projXY); dev_free(v.d_DM); dev_free(v.d_absmag); dev_free(v.d_XYZ);
+    dev_free(v.d_Am); dev_free(v.d_AmInf);
+    dev_free(v.d_key); dev_free(v.d_key2); dev_free(v.d_idx); dev_free(v.d_idx2);
+    if (v.d_sort_temp) cudaFree(v.d_sort_temp);
+    v.d_sort_temp = nullptr;
+    v.rec_cap = 0;
+}
+
+}  // namespace
+
+namespace gfa {
+void free_rec_cache(gf_ctx *ctx)
+{
+    if (!ctx || !ctx->rec_cache) return;
+    RecView *c = (RecView *)ctx->rec_cache;
+    free_recs(*c);
+    delete c;
+    ctx->rec_cache = nullptr;
+}
+}  // namespace gfa
+
+namespace {
+
 gf_status ensure_rec_capacity(gf_skygen *s, int64_t need, int64_t keep)
 {
     if (need <= s->rec_cap) return GF_OK;
+    if (s->rec_cap == 0 && !s->d_rec && keep == 0 && s->ctx->rec_cache) {
+        /* a fresh generator adopts its context's buffers when they are large enough */
+        RecView &c = *(RecView *)s->ctx->rec_cache;
+        if (c.rec_cap >= need && (!s->maps || (c.d_rec_am && c.d_rec_am2))) {
+            move_recs(*s, c);
+            return GF_OK;
+        }
+    }
     int64_t cap = std::max<int64_t>(need, s->rec_cap * 3 / 2);
     cap = std::max<int64_t>(cap, 4096);
     StarRecord *old = s->d_rec;
@@ -414,6 +482,7 @@ gf_status gf_ctx_destroy(gf_ctx *ctx)
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     gfa::free_multi_ws(ctx);
+    gfa::free_rec_cache(ctx);
     gf_table_free(ctx, &ctx->plain_table);
     dev_free(ctx->d_rng);
     dev_free(ctx->d_mult);
@@ -656,13 +725,15 @@ gf_status gf_skygen_destroy(gf_skygen *s)
     }
     dev_free(s->d_pixels); dev_free(s->d_ammin); dev_free(s->d_limits); dev_free(s->d_rng_snap);
     if (s->h_nstars) cudaFreeHost(s->h_nstars);
-    dev_free(s->d_rec); dev_free(s->d_rec2); dev_free(s->d_rec_am); dev_free(s->d_rec_am2);
     dev_free(s->d_map[0]); dev_free(s->d_map[1]);
-    dev_free(s->d_lb); dev_free(s->d_projIdx); dev_free(s->d_hidden);
-    dev_free(s->d_projXY); dev_free(s->d_DM); dev_free(s->d_absmag); dev_free(s->d_XYZ);
-    dev_free(s->d_Am); dev_free(s->d_AmInf);
-    dev_free(s->d_key); dev_free(s->d_key2); dev_free(s->d_idx); dev_free(s->d_idx2);
-    if (s->d_sort_temp) cudaFree(s->d_sort_temp);
+    /* the record and placement buffers go to the context for its next generator
+     * (the larger set is kept) */
+    if (!s->ctx->rec_cache) s->ctx->rec_cache = new RecView();
+    RecView &c = *(RecView *)s->ctx->rec_cache;
+    RecView mine;
+    move_recs(mine, *s);
+    if (mine.rec_cap > c.rec_cap) std::swap(mine, c);
+    free_recs(mine);
     dev_free(s->d_ck); dev_free(s->d_ck_count); dev_free(s->d_ck_sel); dev_free(s->d_keep);
     delete s;
     return GF_OK;
@@ -1473,6 +1544,7 @@ gf_status catalog_run_in_multi(gf_ctx *ctx, const gf_job *job, gf_batch_callback
     if (st == GF_E_OOM && c.calls == 0 && job && job->nstreams > 0) {
         cudaStreamSynchronize(ctx->stream);
         gf_table_free(ctx, &ctx->plain_table);
+        free_rec_cache(ctx);
         st = catalog_run_once(ctx, job, counting_batch, &c, stats);
     }
     return st;

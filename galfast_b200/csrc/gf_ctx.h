@@ -77,6 +77,7 @@ struct gf_ctx {
     int64_t multi_budget = 0;            /* device bytes per multi-request chunk (0: 60% of free memory) */
     MultiWS *multi_ws = nullptr;         /* buffers of gf_catalog_run_multi kept between calls */
     gf_table plain_table = {};           /* output table of gf_catalog_run, kept for the next call of the same shape */
+    void *rec_cache = nullptr;           /* star-record and placement buffers of a finished generator, for the next one */
     int32_t draw_wpc[3] = {0, 0, 0};      /* warps per CTA of the batched draw, by model kind (0: not tuned yet) */
     uint32_t host_cols = GF_COL_ALL;     /* columns gf_catalog_run_multi_host copies to host memory */
     double admit_sigma = 8.0;            /* batched if expected + admit_sigma sqrt(expected) + 1024 < capacity */
@@ -118,6 +119,8 @@ gf_status zero_module_rows(gf_ctx *ctx, const gf_table *t, int64_t n);
 void free_multi_ws(gf_ctx *ctx);
 /* free the buffers a context keeps between calls (output table, multi-request workspace) */
 void release_caches(gf_ctx *ctx);
+/* free the cached generator buffers (rec_cache) */
+void free_rec_cache(gf_ctx *ctx);
 /* gf_catalog_run for a request run inside a multi-request call: an out-of-memory
  * failure before its first batch frees only the plain path's output table before the
  * retry, so the multi-request workspace the caller is using stays in place */
